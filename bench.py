@@ -1,0 +1,343 @@
+"""Benchmark of the CKKS evaluation hot path: key-switched HMult/s.
+
+Workload (one step): HMult + relinearisation + rescale of B resident
+ciphertext pairs at N=2^16, 30 moduli (one 60-bit + 29 x 50-bit), K=10
+special 60-bit moduli, dnum=3, top level (29).  Inputs are seeded synthetic
+residues (bit patterns uniform in [0, q)), which is all the kernels see; the
+B pairs occupy 480 MB (> the 126 MB L2), so no L2 flush is needed between
+steps.
+
+  value  = HMult/s with inputs resident in HBM (device time, CUDA events on
+           the library's stream, max over ranks).
+  e2e    = the same metric through the C ABI with host buffers: per step the
+           pinned-host upload of B pairs, B HMults and the download of the B
+           results are inside the timed region.
+  roofline = the forward NTT (two kernels) over 30 limbs timed live:
+           algorithmic bytes 16*N*30 (one read + one write of each limb).
+  cpu_baseline = the CPU oracle (C, OpenMP over limbs) on one HMult of the
+           same shape on this host's cores.
+
+`--impl reference` times the CPU implementation of the path (the oracle port:
+FIDESlib's own CPU path is OpenFHE, which is not available) on rank 0.
+Multi-GPU: independent replicas, one per rank (the path has no exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "key-switched HMult/s at N=2^16 L=30 (batched vs per-op), bootstrap ms, NTT HBM GB/s"
+LOGN, L, K, DNUM = 16, 30, 10, 3
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_hmult(max_seconds=30.0):
+    """One HMult+Relin+Rescale of the workload's shape on the host cores (oracle port)."""
+    import numpy as np
+
+    from oracle import oracle as O
+    from pyfideslib_b200.host_params import generated_moduli
+
+    q, p = generated_moduli(LOGN, L, K)
+    oc = O.Ctx(LOGN, q, p, DNUM)
+    lv = L - 1
+    pid = list(range(lv + 1))
+    np_ = L + K
+    kb = oc.random(list(range(np_)) * DNUM, 1).reshape(DNUM, np_, oc.N)
+    ka = oc.random(list(range(np_)) * DNUM, 2).reshape(DNUM, np_, oc.N)
+    a0, a1, b0, b1 = (oc.random(pid, s) for s in (3, 4, 5, 6))
+    n, t0 = 0, time.perf_counter()
+    while True:
+        oc.hmult(lv, a0, a1, b0, b1, kb, ka, rescale=True)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > max_seconds / 3 or n >= 3:
+            break
+    return n / el, O.get_threads(), "%d HMult+Relin+Rescale at N=2^16 L=30 K=10 dnum=3 (%.1f s)" % (n, el)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    v, cores, sample = cpu_baseline_hmult(max_seconds=20.0)
+    # each timed step is one bounded sample of the workload
+    import numpy as np  # noqa: F401
+    from oracle import oracle as O
+    from pyfideslib_b200.host_params import generated_moduli
+
+    q, p = generated_moduli(LOGN, L, K)
+    oc = O.Ctx(LOGN, q, p, DNUM)
+    lv = L - 1
+    pid = list(range(lv + 1))
+    np_ = L + K
+    kb = oc.random(list(range(np_)) * DNUM, 1).reshape(DNUM, np_, oc.N)
+    ka = oc.random(list(range(np_)) * DNUM, 2).reshape(DNUM, np_, oc.N)
+    a0, a1, b0, b1 = (oc.random(pid, s) for s in (3, 4, 5, 6))
+    for _ in range(args.warmup):
+        oc.hmult(lv, a0, a1, b0, b1, kb, ka, rescale=True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oc.hmult(lv, a0, a1, b0, b1, kb, ka, rescale=True)
+    el = time.perf_counter() - t0
+    val = args.steps / el
+    out = {"impl": "reference", "metric": METRIC, "value": val, "unit": "HMult/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+           "data": "synthetic", "config": {"workload": "HMult+Relin+Rescale N=2^16 L=30 K=10 dnum=3, level 29",
+                                           "batch_pairs": 1, "parallelism": "host threads"},
+           "cpu_baseline": {"value": val, "unit": "HMult/s", "cores": O.get_threads(), "kind": "port",
+                            "sample": "1 HMult per step; FIDESlib's CPU path is OpenFHE (not available), so the "
+                                      "C restatement of the path (oracle/oracle.c) is timed"},
+           "e2e": {"value": val, "unit": "HMult/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    import pyfideslib_b200 as F
+    from pyfideslib_b200._capi import lib
+
+    cc = F.CryptoContext(log_n=LOGN, num_q=L, dnum=DNUM, num_p=K, device=local)
+    stream_ptr = C.c_void_p()
+    lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))
+    st = torch.cuda.ExternalStream(stream_ptr.value, device=local)
+    N = cc.N
+    lv = L - 1
+    B = args.batch
+    rng = np.random.default_rng(1234 + rank)
+    qs = np.array(cc.q, dtype=np.uint64)
+
+    def rand_poly(nl, primes):
+        x = rng.integers(0, 2 ** 63, size=(nl, N), dtype=np.uint64)
+        return (x % np.asarray(primes, dtype=np.uint64)[:, None]).astype(np.uint64)
+
+    np_ = L + K
+    allp = cc.primes()
+    kb = np.stack([rand_poly(np_, allp) for _ in range(DNUM)])
+    ka = np.stack([rand_poly(np_, allp) for _ in range(DNUM)])
+    cc.upload_relin_key(kb, ka)
+    # pinned host inputs (e2e) and resident device inputs (value)
+    host_in = []
+    for i in range(B):
+        pair = []
+        for _ in range(2):
+            t0 = torch.empty((2, lv + 1, N), dtype=torch.int64, pin_memory=True)
+            arr = t0.numpy().view(np.uint64)
+            arr[0] = rand_poly(lv + 1, qs[:lv + 1])
+            arr[1] = rand_poly(lv + 1, qs[:lv + 1])
+            pair.append((t0, arr))
+        host_in.append(pair)
+    host_out = [torch.empty((2, lv, N), dtype=torch.int64, pin_memory=True) for _ in range(B)]
+    dev_a = [cc.upload(p[0][1][0], p[0][1][1]) for p in host_in]
+    dev_b = [cc.upload(p[1][1][0], p[1][1][1]) for p in host_in]
+    outs = [F.Ciphertext(cc) for _ in range(B)]
+
+    def step_resident():
+        for i in range(B):
+            cc.EvalMult(dev_a[i], dev_b[i], rescale=True, out=outs[i])
+
+    u64p = C.POINTER(C.c_uint64)
+    vp = C.c_void_p
+
+    def step_e2e():
+        for i in range(B):
+            a, b = host_in[i]
+            ha, hb = vp(), vp()
+            lib.fides_ct_upload(cc._h, a[1][0].ctypes.data_as(u64p), a[1][1].ctypes.data_as(u64p), lv, cc.scale, 1,
+                                N // 2, C.byref(ha))
+            lib.fides_ct_upload(cc._h, b[1][0].ctypes.data_as(u64p), b[1][1].ctypes.data_as(u64p), lv, cc.scale, 1,
+                                N // 2, C.byref(hb))
+            lib.fides_hmult(cc._h, ha, hb, outs[i]._h, 1)
+            ho = host_out[i].numpy().view(np.uint64)
+            lib.fides_ct_download_async(cc._h, outs[i]._h, ho[0].ctypes.data_as(u64p), ho[1].ctypes.data_as(u64p))
+            lib.fides_ct_free(cc._h, ha)
+            lib.fides_ct_free(cc._h, hb)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        cc.Synchronize()
+        if pg:
+            pg.barrier()
+        n0 = lib.fides_kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st):
+            e0.record(st)
+        for _ in range(steps):
+            fn()
+        with torch.cuda.stream(st):
+            e1.record(st)
+        e1.synchronize()
+        cc.Synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        launches = lib.fides_kernel_launches() - n0
+        if pg:
+            t = torch.tensor([ms], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches
+
+    with ClockSampler(local) as clk:
+        ms, launches = timed(step_resident, args.steps, args.warmup)
+    ms_e2e, _ = timed(step_e2e, max(1, args.steps // 2), 1)
+
+    # roofline: forward NTT over 30 limbs (2 kernels), resident, > L2 traffic per launch is 31 MB
+    nl = 30
+    buf = torch.empty((4, nl, N), dtype=torch.int64, device="cuda")
+    bp = [buf[i].data_ptr() for i in range(4)]
+    for i in range(4):
+        lib.fides_ntt(cc._h, bp[i], 0, nl, 1)  # any residues < p work; inverse first keeps them canonical
+    reps = 40
+    cc.Synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        e0.record(st)
+    for r in range(reps):
+        lib.fides_ntt(cc._h, bp[r % 4], 0, nl, 0)
+    with torch.cuda.stream(st):
+        e1.record(st)
+    e1.synchronize()
+    ntt_ms = e0.elapsed_time(e1) / reps
+    ntt_bytes = 16.0 * N * nl
+    hbm, peak_kind = peaks()
+    achieved = ntt_bytes / (ntt_ms * 1e-3) / 1e9
+
+    total = B * args.steps * world
+    value = total / (ms * 1e-3)
+    e2e_steps = max(1, args.steps // 2)
+    e2e_val = B * e2e_steps * world / (ms_e2e * 1e-3)
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            v, cores, sample = cpu_baseline_hmult(max_seconds=20.0)
+            cpu = {"value": v, "unit": "HMult/s", "cores": cores, "kind": "port", "sample": sample}
+        out = {"metric": METRIC, "value": value, "unit": "HMult/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+               "config": {"workload": "HMult+Relin+Rescale N=2^16 L=30 (60+29x50-bit) K=10 dnum=3, level 29",
+                          "batch_pairs": B, "per_op": True, "l2": "inputs larger than L2 (%d MB resident)" %
+                          int(B * 2 * 2 * (lv + 1) * N * 8 / 1e6), "parallelism": "replicas%d" % world},
+               "e2e": {"value": e2e_val, "unit": "HMult/s",
+                       "h2d_bytes_per_step": int(B * 2 * 2 * (lv + 1) * N * 8),
+                       "d2h_bytes_per_step": int(B * 2 * lv * N * 8)},
+               "roofline": {"kernel": "ntt_forward(30 limbs, 2 kernels)", "bound": "hbm", "achieved": achieved,
+                            "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                            "traffic": None, "algorithmic_bytes": ntt_bytes, "us_per_launch": ntt_ms * 1e3},
+               "ntt_gbs": achieved,
+               "gpu_launches": int(launches),
+               "clocks": clk.summary(),
+               "cpu_baseline": cpu}
+        print(json.dumps(out), flush=True)
+    for o in outs:
+        del o
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

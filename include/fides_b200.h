@@ -1,0 +1,177 @@
+/*
+ * fides_b200.h -- C ABI of the B200 CKKS evaluation core.
+ *
+ * Plain pointers and sizes only.  Every call returns a fides_status and never
+ * throws or exits.  Residue arrays are uint64, limb-major ([limb][N]), in the
+ * evaluation (NTT, bit-reversed) representation that OpenFHE calls
+ * EVALUATION and FIDESlib exchanges through RawCipherText
+ * (src/CKKS/openfhe-interface/RawCiphertext.cuh:19-93).
+ *
+ * Prime indices: 0..L-1 are the ciphertext moduli q_0..q_{L-1}, L..L+K-1 the
+ * special (key-switching) moduli p_0..p_{K-1}.  A ciphertext at level l has
+ * l+1 limbs (q_0..q_l).  Switching keys are dnum polynomials over all L+K
+ * primes: arrays of dnum*(L+K)*N words.  Digits are contiguous groups of
+ * alpha = ceil(L/dnum) moduli (OpenFHE's HYBRID key-switching partition).
+ *
+ * Each function names the FIDESlib interface it replaces.
+ */
+#ifndef FIDES_B200_H
+#define FIDES_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    FIDES_OK = 0,
+    FIDES_BAD_ARG = 1,
+    FIDES_OOM = 2,
+    FIDES_LEVEL_MISMATCH = 3,
+    FIDES_KEY_MISSING = 4,
+    FIDES_TIMEOUT = 5,
+    FIDES_CUDA_ERR = 6,
+    FIDES_UNSUPPORTED = 7,
+    FIDES_BUSY = 8
+} fides_status;
+
+typedef struct fides_ctx fides_ctx;
+typedef struct fides_ct fides_ct; /* device-resident ciphertext */
+typedef struct fides_pt fides_pt; /* device-resident plaintext  */
+typedef struct fides_sk fides_sk; /* secret key (client side)   */
+
+typedef struct {
+    int log_n;            /* ring dimension N = 2^log_n, 8 <= log_n <= 16 */
+    int num_q;            /* L: number of ciphertext moduli (levels 0..L-1) */
+    int num_p;            /* K: number of special moduli (0 = derive from the digit size) */
+    int dnum;             /* number of key-switching digits */
+    const uint64_t* q;    /* optional explicit moduli (num_q entries), NULL to generate */
+    const uint64_t* p;    /* optional explicit special moduli (num_p entries) */
+    int q0_bits;          /* generated moduli sizes (defaults 60 / 50 / 60 when 0) */
+    int qi_bits;
+    int p_bits;
+    int device;           /* CUDA device ordinal */
+    double default_scale; /* encoding scale, default 2^qi_bits */
+} fides_params;
+
+/* ---- context (replaces CKKS::GenCryptoContextGPU / ContextData ctor,
+ *      src/CKKS/Context.cu:37-98, and SetupConstants, src/ConstantsGPU.cu:127-708) ---- */
+fides_status fides_ctx_create(const fides_params* params, fides_ctx** out);
+fides_status fides_ctx_destroy(fides_ctx* ctx);
+/* Host-only: the moduli fides_ctx_create would generate for these parameters
+ * (descending search for primes = 1 mod 2N; Parameters / computeK,
+ * src/CKKS/Context.cu:275-295).  q gets num_q entries, p up to 64; *num_p_out
+ * receives K. */
+fides_status fides_generate_moduli(const fides_params* params, uint64_t* q, uint64_t* p, int* num_p_out);
+/* moduli actually used: q[0..L-1], p[0..K-1]; any pointer may be NULL */
+fides_status fides_ctx_info(const fides_ctx* ctx, int* log_n, int* num_q, int* num_p, int* dnum, uint64_t* q,
+                            uint64_t* p);
+/* wait for all queued work of this context (CryptoContextImpl::Synchronize, api/CryptoContext.hpp:242) */
+fides_status fides_ctx_synchronize(fides_ctx* ctx);
+/* last error message of this context (static storage owned by the context) */
+const char* fides_ctx_last_error(const fides_ctx* ctx);
+/* The CUDA stream (cudaStream_t) all work of this context is queued on, for
+ * callers that time or order work around it (FIDESlib keeps per-partition
+ * streams in ContextData, src/CKKS/Context.cuh:85-98). */
+fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream);
+/* Number of kernels this library has launched so far (process-wide). */
+uint64_t fides_kernel_launches(void);
+
+/* ---- keys (replaces KeySwitchingKey::Initialize, src/CKKS/KeySwitchingKey.cu:20-35,
+ *      and the GetEvalKeySwitchKey / GetRotationKeySwitchKey imports,
+ *      RawCiphertext.cu:468-602) ---- */
+/* Relinearisation key: b, a are dnum*(L+K)*N words each (host memory). */
+fides_status fides_key_upload_relin(fides_ctx* ctx, const uint64_t* b, const uint64_t* a);
+/* Rotation / conjugation key for the automorphism X -> X^galois (galois odd, < 2N). */
+fides_status fides_key_upload_galois(fides_ctx* ctx, uint32_t galois, const uint64_t* b, const uint64_t* a);
+/* Galois element of a slot rotation by `index` with `slots` slots
+ * (Ciphertext::normalyzeIndex, Ciphertext.cpp:157; RNSPoly.cpp:559 gives the
+ * inverse element used by the permutation). */
+uint32_t fides_rotation_galois(const fides_ctx* ctx, int32_t index, int slots);
+
+/* ---- ciphertexts (replaces Ciphertext::load / store, Ciphertext.cpp:270-309) ---- */
+fides_status fides_ct_upload(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level, double scale,
+                             int noise_deg, int slots, fides_ct** out);
+fides_status fides_ct_download(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1);
+/* Queue the download without waiting; the host buffers (pinned for overlap)
+ * are valid after fides_ctx_synchronize. */
+fides_status fides_ct_download_async(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1);
+fides_status fides_ct_info(const fides_ct* ct, int* level, double* scale, int* noise_deg, int* slots);
+fides_status fides_ct_create(fides_ctx* ctx, fides_ct** out); /* empty, filled by an operation */
+fides_status fides_ct_copy(fides_ctx* ctx, const fides_ct* src, fides_ct* dst);
+fides_status fides_ct_free(fides_ctx* ctx, fides_ct* ct);
+/* Device residues of a ciphertext: (l+1)*N words each, valid until the next
+ * operation that writes this ciphertext. */
+fides_status fides_ct_device_ptrs(const fides_ct* ct, uint64_t** c0, uint64_t** c1);
+/* Drop to a lower level by discarding limbs (CryptoContextImpl::SetLevel). */
+fides_status fides_ct_set_level(fides_ctx* ctx, fides_ct* ct, int level);
+
+fides_status fides_pt_upload(fides_ctx* ctx, const uint64_t* m, int level, double scale, int noise_deg, int slots,
+                             fides_pt** out);
+fides_status fides_pt_free(fides_ctx* ctx, fides_pt* pt);
+
+/* ---- evaluation (api/CryptoContext.hpp:110-181 -> CKKS::Ciphertext, Ciphertext.cuh:34-500) ---- */
+/* EvalMult + relinearisation (+ Rescale when `rescale` != 0): Ciphertext::mult, Ciphertext.cpp:409-622 */
+fides_status fides_hmult(fides_ctx* ctx, const fides_ct* a, const fides_ct* b, fides_ct* out, int rescale);
+/* EvalSquare: Ciphertext::square, Ciphertext.cpp:624 */
+fides_status fides_square(fides_ctx* ctx, const fides_ct* a, fides_ct* out, int rescale);
+/* Rescale: Ciphertext::rescale, Ciphertext.cpp:379-398 */
+fides_status fides_rescale(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
+/* EvalRotate: Ciphertext::rotate, Ciphertext.cpp:756-926 */
+fides_status fides_rotate(fides_ctx* ctx, const fides_ct* a, int32_t index, fides_ct* out);
+/* EvalFastRotation (hoisted, one shared ModUp): Ciphertext::rotate_hoisted, Ciphertext.cpp:1053-1226 */
+fides_status fides_rotate_hoisted(fides_ctx* ctx, const fides_ct* a, int n, const int32_t* indices, fides_ct** outs);
+/* EvalConjugate: Ciphertext::conjugate, Ciphertext.cpp:933 */
+fides_status fides_conjugate(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
+/* Apply an automorphism whose key was uploaded with fides_key_upload_galois */
+fides_status fides_automorphism(fides_ctx* ctx, const fides_ct* a, uint32_t galois, fides_ct* out);
+/* EvalAdd / EvalSub / EvalNegate: Ciphertext::add/sub, Ciphertext.cpp:177-230 */
+fides_status fides_add(fides_ctx* ctx, const fides_ct* a, const fides_ct* b, fides_ct* out);
+fides_status fides_sub(fides_ctx* ctx, const fides_ct* a, const fides_ct* b, fides_ct* out);
+fides_status fides_negate(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
+/* EvalAdd(ct, pt) / EvalMult(ct, pt): Ciphertext::addPt / multPt, Ciphertext.cpp:232,329 */
+fides_status fides_add_pt(fides_ctx* ctx, const fides_ct* a, const fides_pt* p, fides_ct* out);
+fides_status fides_mult_pt(fides_ctx* ctx, const fides_ct* a, const fides_pt* p, fides_ct* out, int rescale);
+/* EvalAdd(ct, double) / EvalMult(ct, double): Ciphertext::addScalar / multScalar */
+fides_status fides_add_scalar(fides_ctx* ctx, const fides_ct* a, double v, fides_ct* out);
+fides_status fides_mult_scalar(fides_ctx* ctx, const fides_ct* a, double v, fides_ct* out, int rescale);
+
+/* ---- raw limb kernels on device memory (LimbPartition NTT/INTT entry points,
+ *      src/CKKS/LimbPartition.cu; used for the plain RNS polynomial multiply) ---- */
+/* In-place forward / inverse NTT of `nlimbs` limbs at `data` (device pointer),
+ * limb i using prime index prime0 + i. */
+fides_status fides_ntt(fides_ctx* ctx, uint64_t* data, int prime0, int nlimbs, int inverse);
+/* c = a * b in R_q for nlimbs limbs of coefficient-form inputs (device
+ * pointers): NTT of a and b into a_ntt / b_ntt (caller-provided device
+ * scratch), then one INTT with the product fused into its load.  `c` may
+ * alias a or b. */
+fides_status fides_polymul(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, uint64_t* c, uint64_t* a_ntt,
+                           uint64_t* b_ntt, int prime0, int nlimbs);
+
+/* ---- client side (OpenFHE's role in FIDESlib: KeyGen, Encrypt, Decrypt,
+ *      MakeCKKSPackedPlaintext; api/CryptoContext.hpp:71-106) ---- */
+/* Secret key with `hamming_weight` nonzero ternary coefficients (0 = uniform ternary). */
+fides_status fides_keygen(fides_ctx* ctx, uint64_t seed, int hamming_weight, fides_sk** out);
+fides_status fides_sk_free(fides_ctx* ctx, fides_sk* sk);
+/* Generate and upload the relinearisation key (EvalMultKeyGen). */
+fides_status fides_keygen_relin(fides_ctx* ctx, const fides_sk* sk, uint64_t seed);
+/* Generate and upload rotation keys for the given slot indices (EvalRotateKeyGen). */
+fides_status fides_keygen_rotations(fides_ctx* ctx, const fides_sk* sk, int n, const int32_t* indices, int slots,
+                                    uint64_t seed);
+fides_status fides_keygen_conjugate(fides_ctx* ctx, const fides_sk* sk, uint64_t seed);
+/* Export generated switching keys (dnum*(L+K)*N words each) for interop tests. */
+fides_status fides_key_export(fides_ctx* ctx, uint32_t galois, uint64_t* b, uint64_t* a);
+/* Encode `slots` complex values (re, im interleaved) at `level` and `scale`
+ * into evaluation-form residues m[(level+1)*N]. */
+fides_status fides_encode(fides_ctx* ctx, const double* values, int slots, int level, double scale, uint64_t* m);
+/* Encrypt with the secret key (symmetric CKKS encryption). */
+fides_status fides_encrypt(fides_ctx* ctx, const fides_sk* sk, const double* values, int slots, int level,
+                           double scale, uint64_t seed, fides_ct** out);
+/* Decrypt and decode into `slots` complex values (re, im interleaved). */
+fides_status fides_decrypt(fides_ctx* ctx, const fides_sk* sk, const fides_ct* ct, double* values, int slots);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,298 @@
+"""pyfideslib_b200 -- B200-native CKKS evaluation core with the FIDESlib
+evaluation surface (api/fideslib.hpp: CryptoContext, Ciphertext, EvalAdd,
+EvalMult, EvalRotate, EvalFastRotation, Rescale ...), driven through the C ABI
+in include/fides_b200.h.
+
+This Python layer is a thin host-side mirror used by tests and benchmarks; the
+C++ mirror of the same surface is pyfideslib_b200/csrc/api/fideslib.hpp.
+Residues cross the boundary as numpy uint64 arrays in evaluation
+(bit-reversed NTT) order, limb-major.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._capi import FidesError, FidesParams, check, lib, u64p, vp
+
+__all__ = ["CryptoContext", "Ciphertext", "Plaintext", "PrivateKey", "FidesError", "lib"]
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(u64p)
+
+
+class Ciphertext:
+    """Device-resident ciphertext handle (FIDESlib CiphertextImpl)."""
+
+    def __init__(self, ctx: "CryptoContext", handle=None):
+        self.ctx = ctx
+        if handle is None:
+            h = vp()
+            check(lib.fides_ct_create(ctx._h, C.byref(h)), ctx._h)
+            handle = h.value
+        self._h = handle
+
+    def __del__(self):
+        h, ctx = getattr(self, "_h", None), getattr(self, "ctx", None)
+        if h and ctx is not None and ctx._h:
+            lib.fides_ct_free(ctx._h, h)
+        self._h = None
+
+    def info(self):
+        lv, sc, nd, sl = C.c_int(), C.c_double(), C.c_int(), C.c_int()
+        check(lib.fides_ct_info(self._h, C.byref(lv), C.byref(sc), C.byref(nd), C.byref(sl)))
+        return {"level": lv.value, "scale": sc.value, "noise_deg": nd.value, "slots": sl.value}
+
+    @property
+    def level(self):
+        return self.info()["level"]
+
+    def GetLevel(self):
+        return self.level
+
+    def download(self):
+        lv = self.level
+        c0 = np.empty((lv + 1, self.ctx.N), dtype=np.uint64)
+        c1 = np.empty_like(c0)
+        check(lib.fides_ct_download(self.ctx._h, self._h, _p(c0), _p(c1)), self.ctx._h)
+        return c0, c1
+
+
+class Plaintext:
+    def __init__(self, ctx, handle, values=None, slots=0):
+        self.ctx, self._h, self.values, self.slots = ctx, handle, values, slots
+
+    def __del__(self):
+        h, ctx = getattr(self, "_h", None), getattr(self, "ctx", None)
+        if h and ctx is not None and ctx._h:
+            lib.fides_pt_free(ctx._h, h)
+        self._h = None
+
+
+class PrivateKey:
+    def __init__(self, ctx, handle):
+        self.ctx, self._h = ctx, handle
+
+    def __del__(self):
+        h, ctx = getattr(self, "_h", None), getattr(self, "ctx", None)
+        if h and ctx is not None and ctx._h:
+            lib.fides_sk_free(ctx._h, h)
+        self._h = None
+
+
+class CryptoContext:
+    """Mirror of fideslib::CryptoContextImpl<DCRTPoly> (api/CryptoContext.hpp:24-245)."""
+
+    def __init__(self, log_n=16, num_q=30, dnum=3, num_p=0, q=None, p=None, q0_bits=60, qi_bits=50, p_bits=60,
+                 device=0, scale=None):
+        prm = FidesParams()
+        prm.log_n, prm.num_q, prm.num_p, prm.dnum = log_n, num_q, num_p, dnum
+        self._qa = np.ascontiguousarray(q, dtype=np.uint64) if q is not None else None
+        self._pa = np.ascontiguousarray(p, dtype=np.uint64) if p is not None else None
+        prm.q = _p(self._qa)
+        prm.p = _p(self._pa)
+        if self._pa is not None:
+            prm.num_p = len(self._pa)
+        prm.q0_bits, prm.qi_bits, prm.p_bits = q0_bits, qi_bits, p_bits
+        prm.device = device
+        prm.default_scale = float(scale) if scale else 0.0
+        h = vp()
+        check(lib.fides_ctx_create(C.byref(prm), C.byref(h)))
+        self._h = h.value
+        ln, nq, npp, dn = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        lib.fides_ctx_info(self._h, C.byref(ln), C.byref(nq), C.byref(npp), C.byref(dn), None, None)
+        self.logN, self.L, self.K, self.dnum = ln.value, nq.value, npp.value, dn.value
+        self.N = 1 << self.logN
+        qq = np.zeros(self.L, dtype=np.uint64)
+        pp = np.zeros(max(self.K, 1), dtype=np.uint64)
+        lib.fides_ctx_info(self._h, None, None, None, None, _p(qq), _p(pp))
+        self.q = [int(x) for x in qq]
+        self.p = [int(x) for x in pp[:self.K]]
+        self.scale = float(scale) if scale else float(2 ** qi_bits)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.fides_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    # ---- info ----
+    def GetRingDimension(self):
+        return self.N
+
+    def GetCyclotomicOrder(self):
+        return 2 * self.N
+
+    def primes(self):
+        return self.q + self.p
+
+    def Synchronize(self):
+        check(lib.fides_ctx_synchronize(self._h), self._h)
+
+    # ---- raw residue interop (RawCipherText-shaped) ----
+    def upload(self, c0, c1, level=None, scale=None, noise_deg=1, slots=None):
+        c0 = np.ascontiguousarray(c0, dtype=np.uint64)
+        c1 = np.ascontiguousarray(c1, dtype=np.uint64)
+        lv = c0.shape[0] - 1 if level is None else level
+        h = vp()
+        check(lib.fides_ct_upload(self._h, _p(c0), _p(c1), lv, float(scale or self.scale), noise_deg,
+                                  slots or self.N // 2, C.byref(h)), self._h)
+        return Ciphertext(self, h.value)
+
+    def upload_relin_key(self, b, a):
+        check(lib.fides_key_upload_relin(self._h, _p(np.ascontiguousarray(b, dtype=np.uint64)),
+                                         _p(np.ascontiguousarray(a, dtype=np.uint64))), self._h)
+
+    def upload_galois_key(self, galois, b, a):
+        check(lib.fides_key_upload_galois(self._h, galois, _p(np.ascontiguousarray(b, dtype=np.uint64)),
+                                          _p(np.ascontiguousarray(a, dtype=np.uint64))), self._h)
+
+    def export_key(self, galois=0):
+        shape = (self.dnum, self.L + self.K, self.N)
+        b = np.empty(shape, dtype=np.uint64)
+        a = np.empty(shape, dtype=np.uint64)
+        check(lib.fides_key_export(self._h, galois, _p(b), _p(a)), self._h)
+        return b, a
+
+    def rotation_galois(self, index, slots=None):
+        return lib.fides_rotation_galois(self._h, index, slots or self.N // 2)
+
+    # ---- client side ----
+    def KeyGen(self, seed=1, hamming_weight=0):
+        h = vp()
+        check(lib.fides_keygen(self._h, seed, hamming_weight, C.byref(h)), self._h)
+        return PrivateKey(self, h.value)
+
+    def EvalMultKeyGen(self, sk, seed=2):
+        check(lib.fides_keygen_relin(self._h, sk._h, seed), self._h)
+
+    def EvalRotateKeyGen(self, sk, indices, slots=None, seed=3):
+        arr = (C.c_int32 * len(indices))(*indices)
+        check(lib.fides_keygen_rotations(self._h, sk._h, len(indices), arr, slots or self.N // 2, seed), self._h)
+
+    def EvalConjugateKeyGen(self, sk, seed=4):
+        check(lib.fides_keygen_conjugate(self._h, sk._h, seed), self._h)
+
+    @staticmethod
+    def _vals(values, slots):
+        v = np.zeros(2 * slots, dtype=np.float64)
+        z = np.asarray(values, dtype=np.complex128)
+        v[0:2 * len(z):2] = z.real
+        v[1:2 * len(z):2] = z.imag
+        return v
+
+    def encode(self, values, slots=None, level=None, scale=None):
+        slots = slots or self.N // 2
+        lv = self.L - 1 if level is None else level
+        v = self._vals(values, slots)
+        m = np.empty((lv + 1, self.N), dtype=np.uint64)
+        check(lib.fides_encode(self._h, v.ctypes.data_as(C.POINTER(C.c_double)), slots, lv,
+                               float(scale or self.scale), _p(m)), self._h)
+        return m
+
+    def MakeCKKSPackedPlaintext(self, values, noise_deg=1, level=None, slots=None, scale=None):
+        slots = slots or self.N // 2
+        lv = self.L - 1 if level is None else level
+        sc = float(scale or self.scale) if noise_deg == 1 else float(scale or self.scale) ** noise_deg
+        m = self.encode(values, slots, lv, sc)
+        h = vp()
+        check(lib.fides_pt_upload(self._h, _p(m), lv, sc, noise_deg, slots, C.byref(h)), self._h)
+        return Plaintext(self, h.value, values, slots)
+
+    def Encrypt(self, sk, values, slots=None, level=None, scale=None, seed=5):
+        slots = slots or self.N // 2
+        lv = self.L - 1 if level is None else level
+        v = self._vals(values, slots)
+        h = vp()
+        check(lib.fides_encrypt(self._h, sk._h, v.ctypes.data_as(C.POINTER(C.c_double)), slots, lv,
+                                float(scale or self.scale), seed, C.byref(h)), self._h)
+        return Ciphertext(self, h.value)
+
+    def Decrypt(self, sk, ct, slots=None):
+        slots = slots or ct.info()["slots"] or self.N // 2
+        v = np.empty(2 * slots, dtype=np.float64)
+        check(lib.fides_decrypt(self._h, sk._h, ct._h, v.ctypes.data_as(C.POINTER(C.c_double)), slots), self._h)
+        return v[0::2] + 1j * v[1::2]
+
+    # ---- evaluation ----
+    def _out(self, out):
+        return out if out is not None else Ciphertext(self)
+
+    def EvalMult(self, a, b, rescale=False, out=None):
+        out = self._out(out)
+        if isinstance(b, Plaintext):
+            check(lib.fides_mult_pt(self._h, a._h, b._h, out._h, int(rescale)), self._h)
+        elif isinstance(b, (int, float)):
+            check(lib.fides_mult_scalar(self._h, a._h, float(b), out._h, int(rescale)), self._h)
+        else:
+            check(lib.fides_hmult(self._h, a._h, b._h, out._h, int(rescale)), self._h)
+        return out
+
+    def EvalSquare(self, a, rescale=False, out=None):
+        out = self._out(out)
+        check(lib.fides_square(self._h, a._h, out._h, int(rescale)), self._h)
+        return out
+
+    def Rescale(self, a, out=None):
+        out = self._out(out)
+        check(lib.fides_rescale(self._h, a._h, out._h), self._h)
+        return out
+
+    def EvalAdd(self, a, b, out=None):
+        out = self._out(out)
+        if isinstance(b, Plaintext):
+            check(lib.fides_add_pt(self._h, a._h, b._h, out._h), self._h)
+        elif isinstance(b, (int, float)):
+            check(lib.fides_add_scalar(self._h, a._h, float(b), out._h), self._h)
+        else:
+            check(lib.fides_add(self._h, a._h, b._h, out._h), self._h)
+        return out
+
+    def EvalSub(self, a, b, out=None):
+        out = self._out(out)
+        check(lib.fides_sub(self._h, a._h, b._h, out._h), self._h)
+        return out
+
+    def EvalNegate(self, a, out=None):
+        out = self._out(out)
+        check(lib.fides_negate(self._h, a._h, out._h), self._h)
+        return out
+
+    def EvalRotate(self, a, index, out=None):
+        out = self._out(out)
+        check(lib.fides_rotate(self._h, a._h, index, out._h), self._h)
+        return out
+
+    def EvalFastRotation(self, a, indices):
+        outs = [Ciphertext(self) for _ in indices]
+        arr = (C.c_int32 * len(indices))(*indices)
+        hs = (vp * len(outs))(*[o._h for o in outs])
+        check(lib.fides_rotate_hoisted(self._h, a._h, len(indices), arr, hs), self._h)
+        return outs
+
+    def EvalConjugate(self, a, out=None):
+        out = self._out(out)
+        check(lib.fides_conjugate(self._h, a._h, out._h), self._h)
+        return out
+
+    def EvalAutomorphism(self, a, galois, out=None):
+        out = self._out(out)
+        check(lib.fides_automorphism(self._h, a._h, galois, out._h), self._h)
+        return out
+
+    def SetLevel(self, ct, level):
+        check(lib.fides_ct_set_level(self._h, ct._h, level), self._h)
+
+    # ---- raw device kernels (device pointers as ints) ----
+    def ntt(self, dev_ptr, prime0, nlimbs, inverse=False):
+        check(lib.fides_ntt(self._h, dev_ptr, prime0, nlimbs, int(inverse)), self._h)
+
+    def polymul(self, a, b, c, a_ntt, b_ntt, prime0, nlimbs):
+        check(lib.fides_polymul(self._h, a, b, c, a_ntt, b_ntt, prime0, nlimbs), self._h)

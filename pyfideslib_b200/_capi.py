@@ -1,0 +1,110 @@
+"""ctypes bindings of include/fides_b200.h (libfidesb200.so, built in-tree).
+
+There is no fallback: importing this module without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfidesb200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        "pyfideslib_b200: %s is missing; build it with `make -C pyfideslib_b200/csrc` "
+        "(or __graft_entry__.build())" % LIB_PATH)
+
+lib = C.CDLL(LIB_PATH)
+
+u64 = C.c_uint64
+u64p = C.POINTER(C.c_uint64)
+i32p = C.POINTER(C.c_int32)
+vp = C.c_void_p
+
+STATUS = {0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "LEVEL_MISMATCH", 4: "KEY_MISSING", 5: "TIMEOUT",
+          6: "CUDA_ERR", 7: "UNSUPPORTED", 8: "BUSY"}
+
+
+class FidesParams(C.Structure):
+    _fields_ = [("log_n", C.c_int), ("num_q", C.c_int), ("num_p", C.c_int), ("dnum", C.c_int),
+                ("q", u64p), ("p", u64p), ("q0_bits", C.c_int), ("qi_bits", C.c_int), ("p_bits", C.c_int),
+                ("device", C.c_int), ("default_scale", C.c_double)]
+
+
+def _sig(name, args, res=C.c_int):
+    f = getattr(lib, name)
+    f.argtypes = args
+    f.restype = res
+    return f
+
+
+EXPORTS = {
+    "fides_ctx_create": ([C.POINTER(FidesParams), C.POINTER(vp)], C.c_int),
+    "fides_ctx_destroy": ([vp], C.c_int),
+    "fides_generate_moduli": ([C.POINTER(FidesParams), u64p, u64p, C.POINTER(C.c_int)], C.c_int),
+    "fides_ctx_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), u64p,
+                        u64p], C.c_int),
+    "fides_ctx_synchronize": ([vp], C.c_int),
+    "fides_ctx_last_error": ([vp], C.c_char_p),
+    "fides_ctx_stream": ([vp, C.POINTER(vp)], C.c_int),
+    "fides_kernel_launches": ([], C.c_uint64),
+    "fides_key_upload_relin": ([vp, u64p, u64p], C.c_int),
+    "fides_key_upload_galois": ([vp, C.c_uint32, u64p, u64p], C.c_int),
+    "fides_rotation_galois": ([vp, C.c_int32, C.c_int], C.c_uint32),
+    "fides_ct_upload": ([vp, u64p, u64p, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+    "fides_ct_download": ([vp, vp, u64p, u64p], C.c_int),
+    "fides_ct_download_async": ([vp, vp, u64p, u64p], C.c_int),
+    "fides_ct_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+                      C.c_int),
+    "fides_ct_create": ([vp, C.POINTER(vp)], C.c_int),
+    "fides_ct_copy": ([vp, vp, vp], C.c_int),
+    "fides_ct_free": ([vp, vp], C.c_int),
+    "fides_ct_device_ptrs": ([vp, C.POINTER(u64p), C.POINTER(u64p)], C.c_int),
+    "fides_ct_set_level": ([vp, vp, C.c_int], C.c_int),
+    "fides_pt_upload": ([vp, u64p, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+    "fides_pt_free": ([vp, vp], C.c_int),
+    "fides_hmult": ([vp, vp, vp, vp, C.c_int], C.c_int),
+    "fides_square": ([vp, vp, vp, C.c_int], C.c_int),
+    "fides_rescale": ([vp, vp, vp], C.c_int),
+    "fides_rotate": ([vp, vp, C.c_int32, vp], C.c_int),
+    "fides_rotate_hoisted": ([vp, vp, C.c_int, i32p, C.POINTER(vp)], C.c_int),
+    "fides_conjugate": ([vp, vp, vp], C.c_int),
+    "fides_automorphism": ([vp, vp, C.c_uint32, vp], C.c_int),
+    "fides_add": ([vp, vp, vp, vp], C.c_int),
+    "fides_sub": ([vp, vp, vp, vp], C.c_int),
+    "fides_negate": ([vp, vp, vp], C.c_int),
+    "fides_add_pt": ([vp, vp, vp, vp], C.c_int),
+    "fides_mult_pt": ([vp, vp, vp, vp, C.c_int], C.c_int),
+    "fides_add_scalar": ([vp, vp, C.c_double, vp], C.c_int),
+    "fides_mult_scalar": ([vp, vp, C.c_double, vp, C.c_int], C.c_int),
+    "fides_ntt": ([vp, vp, C.c_int, C.c_int, C.c_int], C.c_int),
+    "fides_polymul": ([vp, vp, vp, vp, vp, vp, C.c_int, C.c_int], C.c_int),
+    "fides_keygen": ([vp, u64, C.c_int, C.POINTER(vp)], C.c_int),
+    "fides_sk_free": ([vp, vp], C.c_int),
+    "fides_keygen_relin": ([vp, vp, u64], C.c_int),
+    "fides_keygen_rotations": ([vp, vp, C.c_int, i32p, C.c_int, u64], C.c_int),
+    "fides_keygen_conjugate": ([vp, vp, u64], C.c_int),
+    "fides_key_export": ([vp, C.c_uint32, u64p, u64p], C.c_int),
+    "fides_encode": ([vp, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_double, u64p], C.c_int),
+    "fides_encrypt": ([vp, vp, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_double, u64, C.POINTER(vp)], C.c_int),
+    "fides_decrypt": ([vp, vp, vp, C.POINTER(C.c_double), C.c_int], C.c_int),
+}
+
+for _n, (_a, _r) in EXPORTS.items():
+    _sig(_n, _a, _r)
+
+
+class FidesError(RuntimeError):
+    def __init__(self, status, msg=""):
+        super().__init__("%s%s" % (STATUS.get(status, status), (": " + msg) if msg else ""))
+        self.status = status
+
+
+def check(status, ctx=None):
+    if status != 0:
+        msg = ""
+        if ctx is not None:
+            m = lib.fides_ctx_last_error(ctx)
+            msg = m.decode() if m else ""
+        raise FidesError(status, msg)

@@ -1,0 +1,750 @@
+// api.cpp -- the C ABI of the evaluation core (include/fides_b200.h).
+//
+// Operations are queued on the context's stream and return immediately;
+// downloads synchronise.  Every result is computed into a fresh buffer from
+// the stream-ordered pool and then swapped into the output object, so an
+// output may alias an input.
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "context.hpp"
+
+using namespace fides;
+
+namespace {
+
+struct Guard {
+    std::lock_guard<std::recursive_mutex> lk;
+    explicit Guard(fides_ctx* c) : lk(c->mu) { cudaSetDevice(c->device); }
+};
+
+// Swap a freshly computed buffer into `out` and release the old one.
+void commit(fides_ctx* c, fides_ct* out, fides_ct& tmp) {
+    std::swap(out->buf, tmp.buf);
+    std::swap(out->cap, tmp.cap);
+    std::swap(out->ring, tmp.ring);
+    if (tmp.buf) cudaFreeAsync(tmp.buf, c->st);
+    tmp.buf = nullptr;
+    tmp.cap = 0;
+}
+
+// ModUp of x (n evaluation limbs at `level`): scaled INTT into XT, base
+// conversion into DIG, NTT of every digit target.
+void ks_modup(fides_ctx* c, int level, const uint64_t* x) {
+    const int n = level + 1, N = c->N;
+    ntt_inverse(c->dev, map_single(x, c->XT, n, n, 0, level), IL_PLAIN, IS_MODUP, c->st);
+    launch_modup_conv(c->dev, level, c->XT, c->DIG, c->dig_stride, c->st);
+    LimbMap dm{};
+    const int nd = level / c->alpha + 1;
+    dm.nseg = nd;
+    for (int d = 0; d < nd; ++d) {
+        const int lo = d * c->alpha, hi = std::min(lo + c->alpha - 1, level), cnt = hi - lo + 1;
+        LimbSeg& s = dm.seg[d];
+        s.in = s.out = c->DIG + (size_t)d * c->dig_stride * N;
+        s.count = n - cnt + c->K;
+        s.skip_lo = lo;
+        s.skip_cnt = cnt;
+        s.nq = n;
+        s.q0 = 0;
+        s.level = level;
+        dm.total += s.count;
+    }
+    ntt_forward(c->dev, dm, FL_PLAIN, FS_PLAIN, c->st);
+}
+
+// INTT (scaled by (P/p_k)^-1) of the special limbs of XB and XA, in place.
+void special_intt(fides_ctx* c, int level, bool both) {
+    const int n = level + 1, N = c->N;
+    LimbMap m{};
+    m.nseg = both ? 2 : 1;
+    uint64_t* bufs[2] = {c->XB, c->XA};
+    for (int s = 0; s < m.nseg; ++s) {
+        LimbSeg& g = m.seg[s];
+        g.in = g.out = bufs[s] + (size_t)n * N;
+        g.count = c->K;
+        g.skip_lo = c->K;
+        g.nq = 0;
+        g.q0 = 0;
+        g.level = level;
+        m.total += c->K;
+    }
+    ntt_inverse(c->dev, m, IL_PLAIN, IS_MODDOWN, c->st);
+}
+
+// ModDown of XB -> out0 and XA -> out1 (optionally adding e0/e1), no rescale.
+void moddown_pair(fides_ctx* c, int level, uint64_t* out0, uint64_t* out1, const uint64_t* e0, const uint64_t* e1) {
+    const int n = level + 1, N = c->N, L = c->L;
+    special_intt(c, level, true);
+    launch_moddown_conv(c->dev, level, c->XB + (size_t)n * N, c->W, nullptr, c->st);
+    launch_moddown_conv(c->dev, level, c->XA + (size_t)n * N, c->W + (size_t)L * N, nullptr, c->st);
+    LimbMap m{};
+    m.nseg = 2;
+    const uint64_t* xs[2] = {c->XB, c->XA};
+    const uint64_t* es[2] = {e0, e1};
+    uint64_t* os[2] = {out0, out1};
+    for (int s = 0; s < 2; ++s) {
+        LimbSeg& g = m.seg[s];
+        g.in = c->W + (size_t)s * L * N;
+        g.out = os[s];
+        g.in2 = xs[s];
+        g.in3 = es[s];
+        g.count = n;
+        g.skip_lo = n;
+        g.nq = n;
+        g.level = level;
+        m.total += n;
+    }
+    ntt_forward(c->dev, m, FL_PLAIN, FS_MODDOWN, c->st);
+}
+
+// ModDown fused with Rescale:  out = Rescale(e + ModDown(x)) for both halves.
+void moddown_rescale_pair(fides_ctx* c, int level, uint64_t* out0, uint64_t* out1, const uint64_t* e0,
+                          const uint64_t* e1) {
+    const int n = level + 1, N = c->N, L = c->L;
+    special_intt(c, level, true);
+    LimbMap t{};
+    t.nseg = 2;
+    const uint64_t* es[2] = {e0, e1};
+    const uint64_t* xs[2] = {c->XB, c->XA};
+    for (int s = 0; s < 2; ++s) {
+        LimbSeg& g = t.seg[s];
+        g.in = es[s] + (size_t)level * N;
+        g.in2 = xs[s] + (size_t)level * N;
+        g.out = c->T + (size_t)s * N;
+        g.count = 1;
+        g.skip_lo = 1;
+        g.nq = 1;
+        g.q0 = level;
+        g.level = level;
+        t.total += 1;
+    }
+    ntt_inverse(c->dev, t, IL_AXPY_PINV, IS_PLAIN, c->st);
+    launch_moddown_conv(c->dev, level, c->XB + (size_t)n * N, c->W, c->T, c->st);
+    launch_moddown_conv(c->dev, level, c->XA + (size_t)n * N, c->W + (size_t)L * N, c->T + N, c->st);
+    LimbMap m{};
+    m.nseg = 2;
+    uint64_t* os[2] = {out0, out1};
+    for (int s = 0; s < 2; ++s) {
+        LimbSeg& g = m.seg[s];
+        g.in = c->W + (size_t)s * L * N;
+        g.out = os[s];
+        g.in2 = xs[s];
+        g.in3 = es[s];
+        g.count = level;
+        g.skip_lo = level;
+        g.nq = level;
+        g.level = level;
+        m.total += level;
+    }
+    ntt_forward(c->dev, m, FL_PLAIN, FS_MDRS, c->st);
+}
+
+bool valid_ct(const fides_ctx* c, const fides_ct* a) { return a && a->buf && a->level >= 0 && a->level < c->L; }
+
+uint64_t round_to_mod(long double v, uint64_t p) {
+    // v rounded to the nearest integer, reduced mod p (|v| < 2^126)
+    const bool neg = v < 0;
+    long double a = neg ? -v : v;
+    a = floorl(a + 0.5L);
+    const unsigned __int128 big = (unsigned __int128)a;
+    uint64_t r = (uint64_t)(big % p);
+    return neg ? (r ? p - r : 0) : r;
+}
+
+}  // namespace
+
+namespace fides {
+void keyswitch_core(fides_ctx* c, int level, const uint64_t* e2, const SwitchKey& k, const uint64_t* c0_for_rot,
+                    uint32_t galois) {
+    ks_modup(c, level, e2);
+    launch_ks_inner(c->dev, level, e2, c->DIG, c->dig_stride, k.b, k.a, c->XB, c->XA, c0_for_rot, galois, c->st);
+}
+}  // namespace fides
+
+extern "C" {
+
+fides_status fides_ctx_create(const fides_params* params, fides_ctx** out) {
+    if (!params || !out) return FIDES_BAD_ARG;
+    *out = nullptr;
+    if (!ntt_supported(params->log_n) || params->num_q < 1 || params->dnum < 1 || params->dnum > params->num_q ||
+        (params->p && params->num_p < 1))
+        return FIDES_BAD_ARG;
+    fides_ctx* c = new (std::nothrow) fides_ctx();
+    if (!c) return FIDES_OOM;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || params->device < 0 || params->device >= ndev) {
+        cudaGetLastError();
+        delete c;
+        return FIDES_CUDA_ERR;
+    }
+    cudaSetDevice(params->device);
+    {
+        cudaMemPool_t mp;
+        if (cudaDeviceGetDefaultMemPool(&mp, params->device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    fides_status s = build_context(c, params);
+    if (s != FIDES_OK) {
+        free_context(c);
+        delete c;
+        return s;
+    }
+    *out = c;
+    return FIDES_OK;
+}
+
+fides_status fides_generate_moduli(const fides_params* params, uint64_t* q, uint64_t* p, int* num_p_out) {
+    if (!params || !q || !p || !num_p_out || !ntt_supported(params->log_n) || params->num_q < 1 || params->dnum < 1 ||
+        params->dnum > params->num_q)
+        return FIDES_BAD_ARG;
+    std::vector<uint64_t> qq, pp;
+    if (!select_moduli(params, qq, pp)) return FIDES_BAD_ARG;
+    std::copy(qq.begin(), qq.end(), q);
+    std::copy(pp.begin(), pp.end(), p);
+    *num_p_out = (int)pp.size();
+    return FIDES_OK;
+}
+
+fides_status fides_ctx_destroy(fides_ctx* ctx) {
+    if (!ctx) return FIDES_BAD_ARG;
+    free_context(ctx);
+    delete ctx;
+    return FIDES_OK;
+}
+
+fides_status fides_ctx_info(const fides_ctx* ctx, int* log_n, int* num_q, int* num_p, int* dnum, uint64_t* q,
+                            uint64_t* p) {
+    if (!ctx) return FIDES_BAD_ARG;
+    if (log_n) *log_n = ctx->logN;
+    if (num_q) *num_q = ctx->L;
+    if (num_p) *num_p = ctx->K;
+    if (dnum) *dnum = ctx->dnum;
+    if (q) memcpy(q, ctx->host.prime.data(), sizeof(uint64_t) * ctx->L);
+    if (p) memcpy(p, ctx->host.prime.data() + ctx->L, sizeof(uint64_t) * ctx->K);
+    return FIDES_OK;
+}
+
+fides_status fides_ctx_synchronize(fides_ctx* ctx) {
+    if (!ctx) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    if (cudaStreamSynchronize(ctx->st) != cudaSuccess) return check_cuda(ctx, "synchronize");
+    return check_cuda(ctx, "synchronize");
+}
+
+const char* fides_ctx_last_error(const fides_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return FIDES_BAD_ARG;
+    *stream = (void*)ctx->st;
+    return FIDES_OK;
+}
+
+uint64_t fides_kernel_launches(void) { return fides::launch_count(); }
+
+static fides_status upload_key(fides_ctx* c, SwitchKey& k, const uint64_t* b, const uint64_t* a) {
+    const size_t words = (size_t)c->dnum * (c->L + c->K) * c->N;
+    if (!k.b) {
+        if (cudaMalloc((void**)&k.b, 2 * words * sizeof(uint64_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(c, FIDES_OOM, "key allocation failed");
+        }
+        k.a = k.b + words;
+    }
+    cudaMemcpyAsync(k.b, b, words * 8, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(k.a, a, words * 8, cudaMemcpyHostToDevice, c->st);
+    cudaStreamSynchronize(c->st);
+    return check_cuda(c, "key upload");
+}
+
+fides_status fides_key_upload_relin(fides_ctx* ctx, const uint64_t* b, const uint64_t* a) {
+    if (!ctx || !b || !a) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    fides_status s = upload_key(ctx, ctx->relin, b, a);
+    if (s == FIDES_OK) ctx->has_relin = true;
+    return s;
+}
+
+fides_status fides_key_upload_galois(fides_ctx* ctx, uint32_t galois, const uint64_t* b, const uint64_t* a) {
+    if (!ctx || !b || !a || !(galois & 1) || galois >= 2u * (uint32_t)ctx->N) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    SwitchKey& k = ctx->galois_keys[galois];
+    return upload_key(ctx, k, b, a);
+}
+
+uint32_t fides_rotation_galois(const fides_ctx* ctx, int32_t index, int slots) {
+    if (!ctx || slots <= 0) return 0;
+    const int N = ctx->N;
+    int idx = index % slots;
+    if (idx < 0) idx += slots;
+    if (idx > slots / 2) idx += N / 2 - slots;
+    return (uint32_t)powmod(5, (uint64_t)idx, 2ull * N);
+}
+
+fides_status fides_ct_create(fides_ctx* ctx, fides_ct** out) {
+    if (!ctx || !out) return FIDES_BAD_ARG;
+    *out = new (std::nothrow) fides_ct();
+    return *out ? FIDES_OK : FIDES_OOM;
+}
+
+fides_status fides_ct_upload(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level, double scale,
+                             int noise_deg, int slots, fides_ct** out) {
+    if (!ctx || !c0 || !c1 || !out || level < 0 || level >= ctx->L) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    fides_ct* ct = new (std::nothrow) fides_ct();
+    if (!ct) return FIDES_OOM;
+    fides_status s = ct_reserve(ctx, ct, level);
+    if (s != FIDES_OK) {
+        delete ct;
+        return s;
+    }
+    const size_t bytes = (size_t)(level + 1) * ctx->limb_bytes();
+    cudaMemcpyAsync(ct->c0(), c0, bytes, cudaMemcpyHostToDevice, ctx->st);
+    cudaMemcpyAsync(ct->c1(ctx->N), c1, bytes, cudaMemcpyHostToDevice, ctx->st);
+    ct->level = level;
+    ct->scale = scale;
+    ct->noise_deg = noise_deg;
+    ct->slots = slots;
+    *out = ct;
+    return check_cuda(ctx, "ct upload");
+}
+
+fides_status fides_ct_download(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1) {
+    if (!ctx || !valid_ct(ctx, ct)) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    const size_t bytes = (size_t)(ct->level + 1) * ctx->limb_bytes();
+    if (c0) cudaMemcpyAsync(c0, ct->c0(), bytes, cudaMemcpyDeviceToHost, ctx->st);
+    if (c1) cudaMemcpyAsync(c1, ct->c1(ctx->N), bytes, cudaMemcpyDeviceToHost, ctx->st);
+    cudaStreamSynchronize(ctx->st);
+    return check_cuda(ctx, "ct download");
+}
+
+fides_status fides_ct_download_async(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1) {
+    if (!ctx || !valid_ct(ctx, ct)) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    const size_t bytes = (size_t)(ct->level + 1) * ctx->limb_bytes();
+    if (c0) cudaMemcpyAsync(c0, ct->c0(), bytes, cudaMemcpyDeviceToHost, ctx->st);
+    if (c1) cudaMemcpyAsync(c1, ct->c1(ctx->N), bytes, cudaMemcpyDeviceToHost, ctx->st);
+    return check_cuda(ctx, "ct download");
+}
+
+fides_status fides_ct_info(const fides_ct* ct, int* level, double* scale, int* noise_deg, int* slots) {
+    if (!ct) return FIDES_BAD_ARG;
+    if (level) *level = ct->level;
+    if (scale) *scale = ct->scale;
+    if (noise_deg) *noise_deg = ct->noise_deg;
+    if (slots) *slots = ct->slots;
+    return FIDES_OK;
+}
+
+fides_status fides_ct_device_ptrs(const fides_ct* ct, uint64_t** c0, uint64_t** c1) {
+    if (!ct || !ct->buf) return FIDES_BAD_ARG;
+    if (c0) *c0 = ct->c0();
+    if (c1) *c1 = ct->c1(ct->ring);
+    return FIDES_OK;
+}
+
+fides_status fides_ct_copy(fides_ctx* ctx, const fides_ct* src, fides_ct* dst) {
+    if (!ctx || !valid_ct(ctx, src) || !dst) return FIDES_BAD_ARG;
+    if (src == dst) return FIDES_OK;
+    Guard g(ctx);
+    fides_status s = ct_reserve(ctx, dst, src->level);
+    if (s != FIDES_OK) return s;
+    const size_t bytes = (size_t)(src->level + 1) * ctx->limb_bytes();
+    cudaMemcpyAsync(dst->c0(), src->c0(), bytes, cudaMemcpyDeviceToDevice, ctx->st);
+    cudaMemcpyAsync(dst->c1(ctx->N), src->c1(ctx->N), bytes, cudaMemcpyDeviceToDevice, ctx->st);
+    dst->level = src->level;
+    dst->scale = src->scale;
+    dst->noise_deg = src->noise_deg;
+    dst->slots = src->slots;
+    return check_cuda(ctx, "ct copy");
+}
+
+fides_status fides_ct_free(fides_ctx* ctx, fides_ct* ct) {
+    if (!ctx || !ct) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    if (ct->buf) cudaFreeAsync(ct->buf, ctx->st);
+    delete ct;
+    return FIDES_OK;
+}
+
+fides_status fides_ct_set_level(fides_ctx* ctx, fides_ct* ct, int level) {
+    if (!ctx || !valid_ct(ctx, ct) || level < 0 || level > ct->level) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    if (level == ct->level) return FIDES_OK;
+    fides_ct tmp;
+    fides_status s = ct_reserve(ctx, &tmp, level);
+    if (s != FIDES_OK) return s;
+    const size_t bytes = (size_t)(level + 1) * ctx->limb_bytes();
+    cudaMemcpyAsync(tmp.c0(), ct->c0(), bytes, cudaMemcpyDeviceToDevice, ctx->st);
+    cudaMemcpyAsync(tmp.c1(ctx->N), ct->c1(ctx->N), bytes, cudaMemcpyDeviceToDevice, ctx->st);
+    commit(ctx, ct, tmp);
+    ct->level = level;
+    return check_cuda(ctx, "set level");
+}
+
+fides_status fides_pt_upload(fides_ctx* ctx, const uint64_t* m, int level, double scale, int noise_deg, int slots,
+                             fides_pt** out) {
+    if (!ctx || !m || !out || level < 0 || level >= ctx->L) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    fides_pt* pt = new (std::nothrow) fides_pt();
+    if (!pt) return FIDES_OOM;
+    pt->cap = level + 1;
+    if (cudaMallocAsync((void**)&pt->m, (size_t)pt->cap * ctx->limb_bytes(), ctx->st) != cudaSuccess) {
+        cudaGetLastError();
+        delete pt;
+        return set_err(ctx, FIDES_OOM, "plaintext allocation failed");
+    }
+    cudaMemcpyAsync(pt->m, m, (size_t)pt->cap * ctx->limb_bytes(), cudaMemcpyHostToDevice, ctx->st);
+    pt->level = level;
+    pt->scale = scale;
+    pt->noise_deg = noise_deg;
+    pt->slots = slots;
+    *out = pt;
+    return check_cuda(ctx, "pt upload");
+}
+
+fides_status fides_pt_free(fides_ctx* ctx, fides_pt* pt) {
+    if (!ctx || !pt) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    if (pt->m) cudaFreeAsync(pt->m, ctx->st);
+    delete pt;
+    return FIDES_OK;
+}
+
+// ---------------------------------------------------------------------------
+
+static fides_status hmult_impl(fides_ctx* c, const fides_ct* a, const fides_ct* b, fides_ct* out, int rescale) {
+    if (!valid_ct(c, a) || !valid_ct(c, b) || !out) return FIDES_BAD_ARG;
+    if (!c->has_relin) return set_err(c, FIDES_KEY_MISSING, "no relinearisation key");
+    const int level = std::min(a->level, b->level);
+    const bool rs = rescale && level > 0;
+    const int n = level + 1, N = c->N;
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, rs ? level - 1 : level);
+    if (s != FIDES_OK) return s;
+    launch_tensor(c->dev, n, a->c0(), a->c1(N), b->c0(), b->c1(N), c->E0, c->E1, c->E2, c->st);
+    keyswitch_core(c, level, c->E2, c->relin, nullptr, 0);
+    if (rs)
+        moddown_rescale_pair(c, level, tmp.c0(), tmp.c1(N), c->E0, c->E1);
+    else
+        moddown_pair(c, level, tmp.c0(), tmp.c1(N), c->E0, c->E1);
+    const double sc = a->scale * b->scale;
+    const int nd = a->noise_deg + b->noise_deg;
+    const int sl = std::max(a->slots, b->slots);
+    commit(c, out, tmp);
+    out->level = rs ? level - 1 : level;
+    out->scale = rs ? sc / (double)c->host.prime[level] : sc;
+    out->noise_deg = rs ? nd - 1 : nd;
+    out->slots = sl;
+    return check_cuda(c, "hmult");
+}
+
+fides_status fides_hmult(fides_ctx* ctx, const fides_ct* a, const fides_ct* b, fides_ct* out, int rescale) {
+    if (!ctx) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    return hmult_impl(ctx, a, b, out, rescale);
+}
+
+fides_status fides_square(fides_ctx* ctx, const fides_ct* a, fides_ct* out, int rescale) {
+    if (!ctx) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    return hmult_impl(ctx, a, a, out, rescale);
+}
+
+fides_status fides_rescale(fides_ctx* c, const fides_ct* a, fides_ct* out) {
+    if (!c || !valid_ct(c, a) || !out || a->level < 1) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int l = a->level, N = c->N;
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, l - 1);
+    if (s != FIDES_OK) return s;
+    LimbMap t{};
+    t.nseg = 2;
+    const uint64_t* ins[2] = {a->c0(), a->c1(N)};
+    for (int i = 0; i < 2; ++i) {
+        LimbSeg& g2 = t.seg[i];
+        g2.in = ins[i] + (size_t)l * N;
+        g2.out = c->T + (size_t)i * N;
+        g2.count = 1;
+        g2.skip_lo = 1;
+        g2.nq = 1;
+        g2.q0 = l;
+        g2.level = l;
+        t.total += 1;
+    }
+    ntt_inverse(c->dev, t, IL_PLAIN, IS_PLAIN, c->st);
+    LimbMap m{};
+    m.nseg = 2;
+    uint64_t* os[2] = {tmp.c0(), tmp.c1(N)};
+    for (int i = 0; i < 2; ++i) {
+        LimbSeg& g2 = m.seg[i];
+        g2.in = c->T + (size_t)i * N;
+        g2.in_stride_zero = 1;
+        g2.in2 = ins[i];
+        g2.out = os[i];
+        g2.count = l;
+        g2.skip_lo = l;
+        g2.nq = l;
+        g2.level = l;
+        m.total += l;
+    }
+    ntt_forward(c->dev, m, FL_SWITCHMOD, FS_RESCALE, c->st);
+    const double sc = a->scale / (double)c->host.prime[l];
+    const int nd = a->noise_deg - 1, sl = a->slots;
+    commit(c, out, tmp);
+    out->level = l - 1;
+    out->scale = sc;
+    out->noise_deg = nd;
+    out->slots = sl;
+    return check_cuda(c, "rescale");
+}
+
+static fides_status rotate_many(fides_ctx* c, const fides_ct* a, int n, const uint32_t* galois, fides_ct** outs) {
+    if (!valid_ct(c, a) || n < 1) return FIDES_BAD_ARG;
+    std::vector<const SwitchKey*> keys(n);
+    for (int r = 0; r < n; ++r) {
+        if (!outs[r]) return FIDES_BAD_ARG;
+        auto it = c->galois_keys.find(galois[r]);
+        if (it == c->galois_keys.end())
+            return set_err(c, FIDES_KEY_MISSING, "no key for galois element " + std::to_string(galois[r]));
+        keys[r] = &it->second;
+    }
+    const int level = a->level, N = c->N;
+    std::vector<fides_ct> tmp(n);
+    for (int r = 0; r < n; ++r) {
+        fides_status s = ct_reserve(c, &tmp[r], level);
+        if (s != FIDES_OK) return s;
+    }
+    ks_modup(c, level, a->c1(N));
+    for (int r = 0; r < n; ++r) {
+        launch_ks_inner(c->dev, level, a->c1(N), c->DIG, c->dig_stride, keys[r]->b, keys[r]->a, c->XB, c->XA,
+                        a->c0(), galois[r], c->st);
+        moddown_pair(c, level, tmp[r].c0(), tmp[r].c1(N), nullptr, nullptr);
+    }
+    const double sc = a->scale;
+    const int nd = a->noise_deg, sl = a->slots;
+    for (int r = 0; r < n; ++r) {
+        commit(c, outs[r], tmp[r]);
+        outs[r]->level = level;
+        outs[r]->scale = sc;
+        outs[r]->noise_deg = nd;
+        outs[r]->slots = sl;
+    }
+    return check_cuda(c, "rotate");
+}
+
+fides_status fides_rotate(fides_ctx* ctx, const fides_ct* a, int32_t index, fides_ct* out) {
+    if (!ctx || !valid_ct(ctx, a) || !out) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    const int slots = a->slots > 0 ? a->slots : ctx->N / 2;
+    const uint32_t gal = fides_rotation_galois(ctx, index, slots);
+    if (gal == 1) return fides_ct_copy(ctx, a, out);
+    return rotate_many(ctx, a, 1, &gal, &out);
+}
+
+fides_status fides_rotate_hoisted(fides_ctx* ctx, const fides_ct* a, int n, const int32_t* indices, fides_ct** outs) {
+    if (!ctx || !valid_ct(ctx, a) || n < 1 || !indices || !outs) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    const int slots = a->slots > 0 ? a->slots : ctx->N / 2;
+    std::vector<uint32_t> gal;
+    std::vector<fides_ct*> o;
+    for (int r = 0; r < n; ++r) {
+        const uint32_t ge = fides_rotation_galois(ctx, indices[r], slots);
+        if (ge == 1) {
+            fides_status s = fides_ct_copy(ctx, a, outs[r]);
+            if (s != FIDES_OK) return s;
+            continue;
+        }
+        gal.push_back(ge);
+        o.push_back(outs[r]);
+    }
+    if (gal.empty()) return FIDES_OK;
+    return rotate_many(ctx, a, (int)gal.size(), gal.data(), o.data());
+}
+
+fides_status fides_conjugate(fides_ctx* ctx, const fides_ct* a, fides_ct* out) {
+    if (!ctx || !valid_ct(ctx, a) || !out) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    const uint32_t gal = 2u * (uint32_t)ctx->N - 1;
+    return rotate_many(ctx, a, 1, &gal, &out);
+}
+
+fides_status fides_automorphism(fides_ctx* ctx, const fides_ct* a, uint32_t galois, fides_ct* out) {
+    if (!ctx || !valid_ct(ctx, a) || !out) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    return rotate_many(ctx, a, 1, &galois, &out);
+}
+
+static fides_status binary_op(fides_ctx* c, int op, const fides_ct* a, const fides_ct* b, fides_ct* out) {
+    if (!valid_ct(c, a) || (op != EW_NEG && !valid_ct(c, b)) || !out) return FIDES_BAD_ARG;
+    const int level = op == EW_NEG ? a->level : std::min(a->level, b->level);
+    const int n = level + 1, N = c->N;
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, level);
+    if (s != FIDES_OK) return s;
+    launch_elementwise(c->dev, op, n, 0, a->c0(), b ? b->c0() : nullptr, tmp.c0(), c->st);
+    launch_elementwise(c->dev, op, n, 0, a->c1(N), b ? b->c1(N) : nullptr, tmp.c1(N), c->st);
+    const double sc = a->scale;
+    const int nd = a->noise_deg, sl = std::max(a->slots, b ? b->slots : 0);
+    commit(c, out, tmp);
+    out->level = level;
+    out->scale = sc;
+    out->noise_deg = nd;
+    out->slots = sl;
+    return check_cuda(c, "elementwise");
+}
+
+fides_status fides_add(fides_ctx* ctx, const fides_ct* a, const fides_ct* b, fides_ct* out) {
+    if (!ctx) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    return binary_op(ctx, EW_ADD, a, b, out);
+}
+fides_status fides_sub(fides_ctx* ctx, const fides_ct* a, const fides_ct* b, fides_ct* out) {
+    if (!ctx) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    return binary_op(ctx, EW_SUB, a, b, out);
+}
+fides_status fides_negate(fides_ctx* ctx, const fides_ct* a, fides_ct* out) {
+    if (!ctx) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    return binary_op(ctx, EW_NEG, a, nullptr, out);
+}
+
+fides_status fides_add_pt(fides_ctx* c, const fides_ct* a, const fides_pt* p, fides_ct* out) {
+    if (!c || !valid_ct(c, a) || !p || !p->m || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int level = std::min(a->level, p->level), n = level + 1, N = c->N;
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, level);
+    if (s != FIDES_OK) return s;
+    launch_elementwise(c->dev, EW_ADD, n, 0, a->c0(), p->m, tmp.c0(), c->st);
+    launch_elementwise(c->dev, EW_COPY, n, 0, a->c1(N), nullptr, tmp.c1(N), c->st);
+    const double sc = a->scale;
+    const int nd = a->noise_deg, sl = std::max(a->slots, p->slots);
+    commit(c, out, tmp);
+    out->level = level;
+    out->scale = sc;
+    out->noise_deg = nd;
+    out->slots = sl;
+    return check_cuda(c, "add_pt");
+}
+
+fides_status fides_mult_pt(fides_ctx* c, const fides_ct* a, const fides_pt* p, fides_ct* out, int rescale) {
+    if (!c || !valid_ct(c, a) || !p || !p->m || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int level = std::min(a->level, p->level), n = level + 1, N = c->N;
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, level);
+    if (s != FIDES_OK) return s;
+    launch_elementwise(c->dev, EW_MUL, n, 0, a->c0(), p->m, tmp.c0(), c->st);
+    launch_elementwise(c->dev, EW_MUL, n, 0, a->c1(N), p->m, tmp.c1(N), c->st);
+    const double sc = a->scale * p->scale;
+    const int nd = a->noise_deg + p->noise_deg, sl = std::max(a->slots, p->slots);
+    commit(c, out, tmp);
+    out->level = level;
+    out->scale = sc;
+    out->noise_deg = nd;
+    out->slots = sl;
+    fides_status st = check_cuda(c, "mult_pt");
+    if (st == FIDES_OK && rescale && level > 0) st = fides_rescale(c, out, out);
+    return st;
+}
+
+fides_status fides_add_scalar(fides_ctx* c, const fides_ct* a, double v, fides_ct* out) {
+    if (!c || !valid_ct(c, a) || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int n = a->level + 1, N = c->N;
+    std::vector<uint64_t> k(n);
+    for (int j = 0; j < n; ++j) k[j] = round_to_mod((long double)v * a->scale, c->host.prime[j]);
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, a->level);
+    if (s != FIDES_OK) return s;
+    uint64_t* dk = nullptr;
+    if (cudaMallocAsync((void**)&dk, n * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "scalar table");
+    cudaMemcpyAsync(dk, k.data(), n * 8, cudaMemcpyHostToDevice, c->st);
+    launch_scalar_add(c->dev, n, a->c0(), dk, tmp.c0(), c->st);
+    launch_elementwise(c->dev, EW_COPY, n, 0, a->c1(N), nullptr, tmp.c1(N), c->st);
+    cudaStreamSynchronize(c->st);
+    cudaFreeAsync(dk, c->st);
+    const fides_ct meta = *a;
+    commit(c, out, tmp);
+    out->level = meta.level;
+    out->scale = meta.scale;
+    out->noise_deg = meta.noise_deg;
+    out->slots = meta.slots;
+    return check_cuda(c, "add_scalar");
+}
+
+fides_status fides_mult_scalar(fides_ctx* c, const fides_ct* a, double v, fides_ct* out, int rescale) {
+    if (!c || !valid_ct(c, a) || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int n = a->level + 1, N = c->N;
+    const double delta = c->default_scale;
+    std::vector<uint64_t> k(2 * n);
+    for (int j = 0; j < n; ++j) {
+        const uint64_t p = c->host.prime[j];
+        k[2 * j] = round_to_mod((long double)v * delta, p);
+        k[2 * j + 1] = shoup_precompute(k[2 * j], p);
+    }
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, a->level);
+    if (s != FIDES_OK) return s;
+    uint64_t* dk = nullptr;
+    if (cudaMallocAsync((void**)&dk, 2 * n * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "scalar table");
+    cudaMemcpyAsync(dk, k.data(), 2 * n * 8, cudaMemcpyHostToDevice, c->st);
+    launch_scalar_mac(c->dev, n, a->c0(), dk, nullptr, tmp.c0(), c->st);
+    launch_scalar_mac(c->dev, n, a->c1(N), dk, nullptr, tmp.c1(N), c->st);
+    cudaStreamSynchronize(c->st);
+    cudaFreeAsync(dk, c->st);
+    const fides_ct meta = *a;
+    commit(c, out, tmp);
+    out->level = meta.level;
+    out->scale = meta.scale * delta;
+    out->noise_deg = meta.noise_deg + 1;
+    out->slots = meta.slots;
+    fides_status st = check_cuda(c, "mult_scalar");
+    if (st == FIDES_OK && rescale && out->level > 0) st = fides_rescale(c, out, out);
+    return st;
+}
+
+fides_status fides_ntt(fides_ctx* ctx, uint64_t* data, int prime0, int nlimbs, int inverse) {
+    if (!ctx || !data || prime0 < 0 || nlimbs < 1 || prime0 + nlimbs > ctx->L + ctx->K || nlimbs > 65535)
+        return FIDES_BAD_ARG;
+    Guard g(ctx);
+    LimbMap m = map_single(data, data, nlimbs, nlimbs, prime0);
+    if (inverse)
+        ntt_inverse(ctx->dev, m, IL_PLAIN, IS_PLAIN, ctx->st);
+    else
+        ntt_forward(ctx->dev, m, FL_PLAIN, FS_PLAIN, ctx->st);
+    return check_cuda(ctx, "ntt");
+}
+
+fides_status fides_polymul(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, uint64_t* c, uint64_t* a_ntt,
+                           uint64_t* b_ntt, int prime0, int nlimbs) {
+    if (!ctx || !a || !b || !c || !a_ntt || !b_ntt || prime0 < 0 || nlimbs < 1 ||
+        prime0 + nlimbs > ctx->L + ctx->K || nlimbs > 32767)
+        return FIDES_BAD_ARG;
+    Guard g(ctx);
+    LimbMap m{};
+    m.nseg = 2;
+    const uint64_t* ins[2] = {a, b};
+    uint64_t* outs[2] = {a_ntt, b_ntt};
+    for (int s = 0; s < 2; ++s) {
+        LimbSeg& g2 = m.seg[s];
+        g2.in = ins[s];
+        g2.out = outs[s];
+        g2.count = nlimbs;
+        g2.skip_lo = nlimbs;
+        g2.nq = nlimbs;
+        g2.q0 = prime0;
+        m.total += nlimbs;
+    }
+    ntt_forward(ctx->dev, m, FL_PLAIN, FS_PLAIN, ctx->st);
+    ntt_inverse(ctx->dev, map_single(a_ntt, c, nlimbs, nlimbs, prime0, -1, b_ntt), IL_MUL, IS_PLAIN, ctx->st);
+    return check_cuda(ctx, "polymul");
+}
+
+}  // extern "C"

@@ -1,0 +1,480 @@
+// client.cu -- the client-side half of CKKS that FIDESlib delegates to OpenFHE
+// (api/CryptoContext.cpp:475-626: KeyGen, EvalMultKeyGen, EvalRotateKeyGen,
+// MakeCKKSPackedPlaintext, Encrypt, Decrypt).  It is provided so that the
+// evaluation core can be exercised end to end without OpenFHE; the
+// evaluation path does not depend on it.
+//
+//   * encoding: canonical embedding with slot j at the root zeta^(5^j)
+//     (zeta = e^{i pi / N}); sparse packings repeat the slots with period n.
+//     Evaluated with one complex FFT of size N over the odd powers of zeta.
+//   * secrets: ternary, uniform or with a fixed Hamming weight; errors:
+//     rounded Gaussian, sigma 3.2; uniform polynomials drawn on the device
+//     from a counter-based hash.
+//   * switching keys (hybrid, digits of alpha moduli):
+//       b_d = -a_d * s_b + e_d + [P]_{q_i} * s_g   on the moduli of digit d,
+//       b_d = -a_d * s_b + e_d                    elsewhere,
+//     with (s_b, s_g) = (s, s^2) for relinearisation and
+//     (sigma_g^-1(s), s) for the automorphism sigma_g: X -> X^g, matching the
+//     order in which the evaluation applies the permutation (after the inner
+//     product, before ModDown).
+//   * decryption: c0 + c1 s on the device, INTT, then a mixed-radix CRT of the
+//     first three moduli on the host (values of decryptable ciphertexts are
+//     far below q0 q1 q2 / 2).
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <new>
+#include <random>
+#include <vector>
+
+#include "context.hpp"
+
+using namespace fides;
+using cplx = std::complex<double>;
+
+namespace {
+
+struct Xoshiro {
+    uint64_t s[4];
+    explicit Xoshiro(uint64_t seed) {
+        for (int i = 0; i < 4; ++i) {
+            uint64_t z = (seed += 0x9E3779B97F4A7C15ull);
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            s[i] = z ^ (z >> 31);
+        }
+    }
+    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next() {
+        const uint64_t r = rotl(s[1] * 5, 7) * 9;
+        const uint64_t t = s[1] << 17;
+        s[2] ^= s[0];
+        s[3] ^= s[1];
+        s[1] ^= s[2];
+        s[0] ^= s[3];
+        s[2] ^= t;
+        s[3] = rotl(s[3], 45);
+        return r;
+    }
+    double uniform01() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
+};
+
+std::vector<int64_t> gaussian(int N, uint64_t seed, double sigma = 3.2) {
+    Xoshiro r(seed);
+    std::vector<int64_t> e(N);
+    for (int i = 0; i < N; i += 2) {
+        double u1 = r.uniform01(), u2 = r.uniform01();
+        if (u1 < 1e-300) u1 = 1e-300;
+        const double rad = sqrt(-2.0 * log(u1)) * sigma;
+        e[i] = llround(rad * cos(2 * M_PI * u2));
+        if (i + 1 < N) e[i + 1] = llround(rad * sin(2 * M_PI * u2));
+    }
+    return e;
+}
+
+// ---- device helpers ----
+__global__ void k_small_to_rns(const int64_t* __restrict__ v, uint64_t* __restrict__ out, int N, int q0,
+                               const PrimeConst* __restrict__ pcs) {
+    const int limb = blockIdx.y;
+    const PrimeConst pc = pcs[q0 + limb];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t x = v[j];
+    uint64_t a = x < 0 ? (uint64_t)(-x) : (uint64_t)x;
+    a = csub(reduce64_lazy(a, pc), pc.p);
+    out[(size_t)limb * N + j] = x < 0 ? neg_mod(a, pc.p) : a;
+}
+
+__device__ __forceinline__ uint64_t hash64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+__global__ void k_fill_uniform(uint64_t* __restrict__ out, int N, int q0, const PrimeConst* __restrict__ pcs,
+                               uint64_t seed) {
+    const int limb = blockIdx.y;
+    const uint64_t p = pcs[q0 + limb].p;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t h = hash64(seed ^ hash64(((uint64_t)(q0 + limb) << 32) | (uint64_t)j));
+    out[(size_t)limb * N + j] = __umul64hi(h, p);
+}
+
+// b = -a * sb + e (+ pmod_i * sg on limbs with lo <= prime < hi)
+__global__ void k_key_combine(uint64_t* __restrict__ b, const uint64_t* __restrict__ a,
+                              const uint64_t* __restrict__ sb, const uint64_t* __restrict__ e,
+                              const uint64_t* __restrict__ sg, const PrimeConst* __restrict__ pcs,
+                              const uint64_t* __restrict__ pmod, int N, int lo, int hi) {
+    const int limb = blockIdx.y;
+    const PrimeConst pc = pcs[limb];
+    const size_t i = (size_t)limb * N + blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t v = sub_mod(e[i], mul_mod(a[i], sb[i], pc), pc.p);
+    if (limb >= lo && limb < hi) v = add_mod(v, mul_shoup(sg[i], pmod[2 * limb], pmod[2 * limb + 1], pc.p), pc.p);
+    b[i] = v;
+}
+
+// ---- host FFT ----
+void fft(std::vector<cplx>& a, bool inverse) {
+    const int n = (int)a.size();
+    for (int i = 1, j = 0; i < n; ++i) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) std::swap(a[i], a[j]);
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        const double ang = 2 * M_PI / len * (inverse ? -1 : 1);
+        const cplx wl(cos(ang), sin(ang));
+        std::vector<cplx> w(len / 2);
+        w[0] = 1;
+        for (int k = 1; k < len / 2; ++k) w[k] = (k % 64 == 0) ? cplx(cos(ang * k), sin(ang * k)) : w[k - 1] * wl;
+        for (int i = 0; i < n; i += len)
+            for (int k = 0; k < len / 2; ++k) {
+                const cplx u = a[i + k], v = a[i + k + len / 2] * w[k];
+                a[i + k] = u + v;
+                a[i + k + len / 2] = u - v;
+            }
+    }
+}
+
+// index t in [0, N) of the odd exponent 2t+1 = 5^j mod 2N (and its conjugate)
+void slot_indices(int N, std::vector<int>& pos, std::vector<int>& neg) {
+    pos.resize(N / 2);
+    neg.resize(N / 2);
+    uint64_t g = 1;
+    for (int j = 0; j < N / 2; ++j) {
+        pos[j] = (int)((g - 1) / 2);
+        neg[j] = (int)((2 * N - g - 1) / 2);
+        g = (g * 5) % (2 * N);
+    }
+}
+
+// slots (n complex) -> real coefficients (not yet scaled)
+std::vector<double> embed_inverse(int N, const double* values, int slots) {
+    std::vector<int> pos, neg;
+    slot_indices(N, pos, neg);
+    std::vector<cplx> M(N);
+    for (int j = 0; j < N / 2; ++j) {
+        const int k = j % slots;
+        const cplx z(values[2 * k], values[2 * k + 1]);
+        M[pos[j]] = z;
+        M[neg[j]] = std::conj(z);
+    }
+    fft(M, true);  // sum_t M_t w^{-t i}
+    std::vector<double> m(N);
+    for (int i = 0; i < N; ++i) {
+        const double ang = -M_PI * i / N;
+        m[i] = (M[i] * cplx(cos(ang), sin(ang))).real() / N;
+    }
+    return m;
+}
+
+// real coefficients -> slots
+void embed(int N, const std::vector<long double>& m, double* values, int slots) {
+    std::vector<cplx> A(N);
+    for (int i = 0; i < N; ++i) {
+        const double ang = M_PI * i / N;
+        A[i] = (double)m[i] * cplx(cos(ang), sin(ang));
+    }
+    fft(A, false);  // sum_i a_i w^{t i}
+    std::vector<int> pos, neg;
+    slot_indices(N, pos, neg);
+    for (int k = 0; k < slots; ++k) {
+        values[2 * k] = A[pos[k]].real();
+        values[2 * k + 1] = A[pos[k]].imag();
+    }
+}
+
+fides_status upload_small(fides_ctx* c, const std::vector<int64_t>& v, uint64_t* out, int q0, int nlimbs) {
+    int64_t* dv = nullptr;
+    if (cudaMallocAsync((void**)&dv, sizeof(int64_t) * c->N, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "small");
+    cudaMemcpyAsync(dv, v.data(), sizeof(int64_t) * c->N, cudaMemcpyHostToDevice, c->st);
+    count_launches(1);
+    k_small_to_rns<<<dim3(c->N / 256, nlimbs), 256, 0, c->st>>>(dv, out, c->N, q0, c->dev.pc);
+    cudaStreamSynchronize(c->st);
+    cudaFreeAsync(dv, c->st);
+    return check_cuda(c, "small_to_rns");
+}
+
+fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg, uint64_t seed, SwitchKey& key) {
+    const int N = c->N, NP = c->L + c->K;
+    const size_t words = (size_t)c->dnum * NP * N;
+    if (!key.b) {
+        if (cudaMalloc((void**)&key.b, 2 * words * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(c, FIDES_OOM, "key allocation");
+        }
+        key.a = key.b + words;
+    }
+    uint64_t* e = nullptr;
+    if (cudaMallocAsync((void**)&e, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "key tmp");
+    for (int d = 0; d < c->dnum; ++d) {
+        uint64_t* kb = key.b + (size_t)d * NP * N;
+        uint64_t* ka = key.a + (size_t)d * NP * N;
+        count_launches(1);
+        k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(ka, N, 0, c->dev.pc, seed * 1315423911ull + d + 1);
+        fides_status s = upload_small(c, gaussian(N, seed ^ (0xABCDull + d)), e, 0, NP);
+        if (s != FIDES_OK) return s;
+        ntt_forward(c->dev, map_single(e, e, NP, NP, 0), FL_PLAIN, FS_PLAIN, c->st);
+        const int lo = d * c->alpha, hi = std::min(c->L, lo + c->alpha);
+        count_launches(1);
+        k_key_combine<<<dim3(N / 256, NP), 256, 0, c->st>>>(kb, ka, sb, e, sg, c->dev.pc, c->dev.md_pmod, N, lo, hi);
+    }
+    cudaStreamSynchronize(c->st);
+    cudaFreeAsync(e, c->st);
+    return check_cuda(c, "switch key");
+}
+
+}  // namespace
+
+extern "C" {
+
+fides_status fides_keygen(fides_ctx* c, uint64_t seed, int hamming_weight, fides_sk** out) {
+    if (!c || !out || hamming_weight < 0 || hamming_weight > c->N) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    fides_sk* sk = new (std::nothrow) fides_sk();
+    if (!sk) return FIDES_OOM;
+    const int N = c->N, NP = c->L + c->K;
+    sk->coeff.assign(N, 0);
+    Xoshiro r(seed);
+    if (hamming_weight == 0) {
+        for (int i = 0; i < N; ++i) sk->coeff[i] = (int8_t)((int)(r.next() % 3) - 1);
+    } else {
+        int placed = 0;
+        while (placed < hamming_weight) {
+            const int i = (int)(r.next() % N);
+            if (sk->coeff[i]) continue;
+            sk->coeff[i] = (r.next() & 1) ? 1 : -1;
+            ++placed;
+        }
+    }
+    if (cudaMalloc((void**)&sk->s, (size_t)NP * N * 8) != cudaSuccess) {
+        cudaGetLastError();
+        delete sk;
+        return set_err(c, FIDES_OOM, "secret key");
+    }
+    std::vector<int64_t> v(sk->coeff.begin(), sk->coeff.end());
+    fides_status s = upload_small(c, v, sk->s, 0, NP);
+    if (s != FIDES_OK) return s;
+    ntt_forward(c->dev, map_single(sk->s, sk->s, NP, NP, 0), FL_PLAIN, FS_PLAIN, c->st);
+    cudaStreamSynchronize(c->st);
+    *out = sk;
+    return check_cuda(c, "keygen");
+}
+
+fides_status fides_sk_free(fides_ctx* c, fides_sk* sk) {
+    if (!c || !sk) return FIDES_BAD_ARG;
+    cudaSetDevice(c->device);
+    if (sk->s) cudaFree(sk->s);
+    delete sk;
+    return FIDES_OK;
+}
+
+fides_status fides_keygen_relin(fides_ctx* c, const fides_sk* sk, uint64_t seed) {
+    if (!c || !sk || !sk->s) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    const int NP = c->L + c->K;
+    uint64_t* s2 = nullptr;
+    if (cudaMallocAsync((void**)&s2, (size_t)NP * c->N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "s^2");
+    launch_elementwise(c->dev, EW_MUL, NP, 0, sk->s, sk->s, s2, c->st);
+    fides_status s = gen_switch_key(c, sk->s, s2, seed, c->relin);
+    cudaFreeAsync(s2, c->st);
+    if (s == FIDES_OK) c->has_relin = true;
+    return s;
+}
+
+// inverse of an odd g modulo 2N (extended Euclid; 2N is not prime)
+static uint32_t inv_mod_2n(uint32_t g, uint32_t m) {
+    int64_t t = 0, nt = 1, r = m, nr = g % m;
+    while (nr) {
+        const int64_t q = r / nr;
+        const int64_t t2 = t - q * nt, r2 = r - q * nr;
+        t = nt;
+        nt = t2;
+        r = nr;
+        nr = r2;
+    }
+    return (uint32_t)(t < 0 ? t + m : t);
+}
+
+static fides_status keygen_galois(fides_ctx* c, const fides_sk* sk, uint32_t g, uint64_t seed) {
+    const int NP = c->L + c->K, N = c->N;
+    // sigma_g^-1(s) = s(X^{g^-1}): gather with the inverse element
+    const uint32_t ginv = inv_mod_2n(g, 2u * (uint32_t)N);
+    uint64_t* sr = nullptr;
+    if (cudaMallocAsync((void**)&sr, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "s rot");
+    launch_automorph(c->dev, NP, sk->s, sr, ginv, c->st);
+    fides_status s = gen_switch_key(c, sr, sk->s, seed ^ ((uint64_t)g << 20), c->galois_keys[g]);
+    cudaFreeAsync(sr, c->st);
+    return s;
+}
+
+fides_status fides_keygen_rotations(fides_ctx* c, const fides_sk* sk, int n, const int32_t* indices, int slots,
+                                    uint64_t seed) {
+    if (!c || !sk || !sk->s || n < 0 || (n && !indices)) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    if (slots <= 0) slots = c->N / 2;
+    for (int i = 0; i < n; ++i) {
+        const uint32_t g = fides_rotation_galois(c, indices[i], slots);
+        if (g == 1 || c->galois_keys.count(g)) continue;
+        fides_status s = keygen_galois(c, sk, g, seed + 7919ull * (uint64_t)i);
+        if (s != FIDES_OK) return s;
+    }
+    return FIDES_OK;
+}
+
+fides_status fides_keygen_conjugate(fides_ctx* c, const fides_sk* sk, uint64_t seed) {
+    if (!c || !sk || !sk->s) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    return keygen_galois(c, sk, 2u * (uint32_t)c->N - 1, seed);
+}
+
+fides_status fides_key_export(fides_ctx* c, uint32_t galois, uint64_t* b, uint64_t* a) {
+    if (!c || !b || !a) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    const SwitchKey* k = nullptr;
+    if (galois == 0) {
+        if (!c->has_relin) return FIDES_KEY_MISSING;
+        k = &c->relin;
+    } else {
+        auto it = c->galois_keys.find(galois);
+        if (it == c->galois_keys.end()) return FIDES_KEY_MISSING;
+        k = &it->second;
+    }
+    const size_t words = (size_t)c->dnum * (c->L + c->K) * c->N;
+    cudaMemcpyAsync(b, k->b, words * 8, cudaMemcpyDeviceToHost, c->st);
+    cudaMemcpyAsync(a, k->a, words * 8, cudaMemcpyDeviceToHost, c->st);
+    cudaStreamSynchronize(c->st);
+    return check_cuda(c, "key export");
+}
+
+static fides_status encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm) {
+    const int N = c->N;
+    std::vector<double> m = embed_inverse(N, values, slots);
+    std::vector<int64_t> v(N);
+    for (int i = 0; i < N; ++i) {
+        const double x = m[i] * scale;
+        if (!(fabs(x) < 9.0e18)) return set_err(c, FIDES_BAD_ARG, "encoded coefficient exceeds 2^63");
+        v[i] = llround(x);
+    }
+    fides_status s = upload_small(c, v, dm, 0, level + 1);
+    if (s != FIDES_OK) return s;
+    ntt_forward(c->dev, map_single(dm, dm, level + 1, level + 1, 0), FL_PLAIN, FS_PLAIN, c->st);
+    return check_cuda(c, "encode");
+}
+
+fides_status fides_encode(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* m) {
+    if (!c || !values || !m || slots < 1 || slots > c->N / 2 || (slots & (slots - 1)) || level < 0 || level >= c->L)
+        return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    uint64_t* dm = nullptr;
+    if (cudaMallocAsync((void**)&dm, (size_t)(level + 1) * c->N * 8, c->st) != cudaSuccess)
+        return set_err(c, FIDES_OOM, "encode");
+    fides_status s = encode_dev(c, values, slots, level, scale > 0 ? scale : c->default_scale, dm);
+    if (s == FIDES_OK) {
+        cudaMemcpyAsync(m, dm, (size_t)(level + 1) * c->N * 8, cudaMemcpyDeviceToHost, c->st);
+        cudaStreamSynchronize(c->st);
+    }
+    cudaFreeAsync(dm, c->st);
+    return s == FIDES_OK ? check_cuda(c, "encode") : s;
+}
+
+fides_status fides_encrypt(fides_ctx* c, const fides_sk* sk, const double* values, int slots, int level,
+                           double scale, uint64_t seed, fides_ct** out) {
+    if (!c || !sk || !sk->s || !values || !out || slots < 1 || slots > c->N / 2 || (slots & (slots - 1)) ||
+        level < 0 || level >= c->L)
+        return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    if (scale <= 0) scale = c->default_scale;
+    const int n = level + 1, N = c->N;
+    fides_ct* ct = new (std::nothrow) fides_ct();
+    if (!ct) return FIDES_OOM;
+    fides_status s = ct_reserve(c, ct, level);
+    if (s != FIDES_OK) {
+        delete ct;
+        return s;
+    }
+    uint64_t *m = nullptr, *e = nullptr;
+    cudaMallocAsync((void**)&m, (size_t)n * N * 8, c->st);
+    cudaMallocAsync((void**)&e, (size_t)n * N * 8, c->st);
+    s = encode_dev(c, values, slots, level, scale, m);
+    if (s == FIDES_OK) s = upload_small(c, gaussian(N, seed ^ 0x5EED), e, 0, n);
+    if (s == FIDES_OK) {
+        ntt_forward(c->dev, map_single(e, e, n, n, 0), FL_PLAIN, FS_PLAIN, c->st);
+        count_launches(1);
+        k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c1(N), N, 0, c->dev.pc, seed * 2654435761ull + 17);
+        launch_elementwise(c->dev, EW_ADD, n, 0, e, m, e, c->st);  // e + m
+        // c0 = -a s + (e + m): key_combine with no gadget term
+        count_launches(1);
+        k_key_combine<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c0(), ct->c1(N), sk->s, e, sk->s, c->dev.pc,
+                                                           c->dev.md_pmod, N, 0, 0);
+        cudaStreamSynchronize(c->st);
+    }
+    cudaFreeAsync(m, c->st);
+    cudaFreeAsync(e, c->st);
+    if (s != FIDES_OK) {
+        fides_ct_free(c, ct);
+        return s;
+    }
+    ct->level = level;
+    ct->scale = scale;
+    ct->noise_deg = 1;
+    ct->slots = slots;
+    *out = ct;
+    return check_cuda(c, "encrypt");
+}
+
+fides_status fides_decrypt(fides_ctx* c, const fides_sk* sk, const fides_ct* ct, double* values, int slots) {
+    if (!c || !sk || !sk->s || !ct || !ct->buf || !values || slots < 1 || slots > c->N / 2) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    const int n = ct->level + 1, N = c->N;
+    uint64_t* m = nullptr;
+    if (cudaMallocAsync((void**)&m, (size_t)n * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "decrypt");
+    launch_elementwise(c->dev, EW_MUL, n, 0, ct->c1(N), sk->s, m, c->st);
+    launch_elementwise(c->dev, EW_ADD, n, 0, m, ct->c0(), m, c->st);
+    ntt_inverse(c->dev, map_single(m, m, n, n, 0), IL_PLAIN, IS_PLAIN, c->st);
+    const int use = std::min(n, 3);
+    std::vector<uint64_t> h((size_t)use * N);
+    cudaMemcpyAsync(h.data(), m, (size_t)use * N * 8, cudaMemcpyDeviceToHost, c->st);
+    cudaStreamSynchronize(c->st);
+    cudaFreeAsync(m, c->st);
+    fides_status s = check_cuda(c, "decrypt");
+    if (s != FIDES_OK) return s;
+    // mixed-radix CRT over q0..q_{use-1}, centred
+    const uint64_t* q = c->host.prime.data();
+    std::vector<long double> coef(N);
+    uint64_t inv01 = use > 1 ? invmod(q[0] % q[1], q[1]) : 0;
+    uint64_t inv02 = use > 2 ? invmod(q[0] % q[2], q[2]) : 0;
+    uint64_t inv12 = use > 2 ? invmod(q[1] % q[2], q[2]) : 0;
+    for (int i = 0; i < N; ++i) {
+        uint64_t v[3] = {h[i], 0, 0};
+        if (use > 1) v[1] = mulmod(sub_mod(h[(size_t)N + i], v[0] % q[1], q[1]), inv01, q[1]);
+        if (use > 2) {
+            uint64_t t = mulmod(sub_mod(h[(size_t)2 * N + i], v[0] % q[2], q[2]), inv02, q[2]);
+            v[2] = mulmod(sub_mod(t, v[1] % q[2], q[2]), inv12, q[2]);
+        }
+        const bool negv = v[use - 1] > q[use - 1] / 2;
+        long double acc = 0, w = 1;
+        for (int k = 0; k < use; ++k) {
+            const uint64_t dk = negv ? q[k] - 1 - v[k] : v[k];
+            acc += (long double)dk * w;
+            w *= (long double)q[k];
+        }
+        coef[i] = negv ? -(acc + 1) : acc;
+        coef[i] /= (long double)ct->scale;
+    }
+    embed(N, coef, values, slots);
+    return FIDES_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// common.cuh -- device-side context view and limb addressing shared by all
+// kernels of the evaluation core.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "modarith.cuh"
+
+namespace fides {
+
+constexpr int kMaxPrimes = 128;
+constexpr int kMaxSeg = 8;
+
+// Read-only view of the context tables in HBM, passed by value to kernels.
+// Index conventions: prime ids 0..L-1 are the Q primes, L..L+K-1 the special
+// primes.  Every table entry with a Shoup companion stores (value, companion)
+// adjacently.
+struct DevCtx {
+    int logN, N, L, K, dnum, alpha;
+    const PrimeConst* pc;        // [L+K]
+    const uint64_t* fwd_tw;      // [L+K][N][2]  psi^{bitrev(i)}, companion
+    const uint64_t* inv_tw;      // [L+K][N][2]  psi^{-bitrev(i)}, companion
+    const uint64_t* intt_scale;  // [L+K][4]     s=N^-1, s', s*w1, (s*w1)'  (w1 = inverse twiddle 1)
+    const uint64_t* modup_scale; // [L][L][4]    same with s = N^-1 * (Q'/q_i)^-1 for level, prime
+    const uint64_t* modup_mat;   // [L][L][L+K]  (Q'/q_i) mod t for level, input prime i, target prime t
+    const uint64_t* md_scale;    // [K][4]       same with s = N^-1 * (P/p_k)^-1
+    const uint64_t* md_mat;      // [K][L]       (P/p_k) mod q_j
+    const uint64_t* md_pinv;     // [L][2]       P^-1 mod q_j
+    const uint64_t* md_pmod;     // [L][2]       P mod q_j
+    const uint64_t* rs_qinv;     // [L][L][2]    q_l^-1 mod q_j (row l, column j < l)
+};
+
+// A launch covers up to kMaxSeg segments of contiguous limbs.  Within a
+// segment, limb i (0 <= i < count) sits at in/out + i*N and maps to prime
+//   j = i < skip_lo ? i : i + skip_cnt;   prime = j < nq ? q0 + j : L + (j - nq).
+struct LimbSeg {
+    const uint64_t* in;
+    const uint64_t* in2;
+    const uint64_t* in3;
+    uint64_t* out;
+    int count;
+    int skip_lo, skip_cnt;
+    int nq, q0;
+    int level;  // level used by level-dependent tables (-1 if unused)
+    int in_stride_zero;  // 1: every limb reads the same input limb
+    int pad;
+};
+
+struct LimbMap {
+    int nseg;
+    int total;
+    LimbSeg seg[kMaxSeg];
+};
+
+struct LimbRef {
+    const uint64_t* in;
+    const uint64_t* in2;
+    const uint64_t* in3;
+    uint64_t* out;
+    int prime;
+    int level;
+};
+
+__device__ __forceinline__ LimbRef resolve_limb(const LimbMap& m, int f, int N, int L) {
+    int s = 0;
+#pragma unroll 1
+    while (s < m.nseg - 1 && f >= m.seg[s].count) {
+        f -= m.seg[s].count;
+        ++s;
+    }
+    const LimbSeg& g = m.seg[s];
+    LimbRef r;
+    const size_t off = (size_t)f * N;
+    r.in = g.in ? g.in + (g.in_stride_zero ? 0 : off) : nullptr;
+    r.in2 = g.in2 ? g.in2 + off : nullptr;
+    r.in3 = g.in3 ? g.in3 + off : nullptr;
+    r.out = g.out ? g.out + off : nullptr;
+    const int j = f < g.skip_lo ? f : f + g.skip_cnt;
+    r.prime = j < g.nq ? g.q0 + j : L + (j - g.nq);
+    r.level = g.level;
+    return r;
+}
+
+}  // namespace fides

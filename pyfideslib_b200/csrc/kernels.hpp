@@ -1,0 +1,58 @@
+// kernels.hpp -- host-side launchers of the sm_100a kernels.
+#pragma once
+#include "common.cuh"
+
+namespace fides {
+
+// forward-NTT prologues (pass 1 loads)
+enum { FL_PLAIN = 0, FL_SWITCHMOD = 1 };
+// forward-NTT epilogues (pass 2 stores); v = NTT value, j = prime, l = level
+enum {
+    FS_PLAIN = 0,    // out = v
+    FS_MODDOWN = 1,  // out = (in2 - v) * P^-1 (+ in3)
+    FS_RESCALE = 2,  // out = (in2 - v) * q_l^-1
+    FS_MDRS = 3,     // out = (in3 + in2 * P^-1 - v) * q_l^-1
+};
+// inverse-NTT prologues (pass A loads)
+enum { IL_PLAIN = 0, IL_MUL = 1, IL_AXPY_PINV = 2 };
+// inverse-NTT epilogues (pass B scale): N^-1 times 1 / ModUp hat-inverse / ModDown hat-inverse
+enum { IS_PLAIN = 0, IS_MODUP = 1, IS_MODDOWN = 2 };
+
+// process-wide count of kernels launched by this library
+uint64_t launch_count();
+void count_launches(int n);
+
+bool ntt_supported(int logN);
+// Forward NTT of every limb in `map`: pass 1 reads seg.in (writes seg.out),
+// pass 2 transforms seg.out in place and applies the epilogue.
+void ntt_forward(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st);
+// Inverse NTT: pass A reads seg.in (+in2 for the prologue), writes seg.out;
+// pass B finishes seg.out in place.
+void ntt_inverse(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st);
+
+// ---- element-wise and base-conversion kernels (ks.cu) ----
+void launch_tensor(const DevCtx& ctx, int n, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0,
+                   const uint64_t* b1, uint64_t* e0, uint64_t* e1, uint64_t* e2, cudaStream_t st);
+void launch_modup_conv(const DevCtx& ctx, int level, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
+                       cudaStream_t st);
+void launch_ks_inner(const DevCtx& ctx, int level, const uint64_t* e2, const uint64_t* dig, size_t dig_stride,
+                     const uint64_t* kb, const uint64_t* ka, uint64_t* xb, uint64_t* xa, const uint64_t* c0,
+                     uint32_t galois_inv, cudaStream_t st);
+void launch_moddown_conv(const DevCtx& ctx, int level, const uint64_t* y, uint64_t* w, const uint64_t* ttop,
+                         cudaStream_t st);
+
+// element-wise helpers; limbs 0..n-1 use primes q0..q0+n-1
+enum { EW_ADD = 0, EW_SUB = 1, EW_NEG = 2, EW_MUL = 3, EW_COPY = 4 };
+void launch_elementwise(const DevCtx& ctx, int op, int n, int q0, const uint64_t* a, const uint64_t* b,
+                        uint64_t* out, cudaStream_t st);
+// out = a * c_j (+ b) with one constant per limb from a device table [n][2] (value, Shoup)
+void launch_scalar_mac(const DevCtx& ctx, int n, const uint64_t* a, const uint64_t* cj, const uint64_t* b,
+                       uint64_t* out, cudaStream_t st);
+// out = a + c_j with one constant per limb (device table [n])
+void launch_scalar_add(const DevCtx& ctx, int n, const uint64_t* a, const uint64_t* cj, uint64_t* out,
+                       cudaStream_t st);
+// automorphism gather over nlimbs limbs (any primes): out[j] = in[slot(galois_inv, j)]
+void launch_automorph(const DevCtx& ctx, int nlimbs, const uint64_t* in, uint64_t* out, uint32_t galois_inv,
+                      cudaStream_t st);
+
+}  // namespace fides

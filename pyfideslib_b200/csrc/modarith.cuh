@@ -1,0 +1,97 @@
+// modarith.cuh -- 64-bit modular arithmetic for residues modulo NTT primes
+// p < 2^62, shared by the CUDA kernels and the host code.
+//
+// All products are on the integer pipes (IMAD); nothing is approximated.
+// Canonical residues live in [0, p); the transforms keep Harvey's lazy
+// ranges [0, 2p) / [0, 4p) internally and reduce at the end.
+//
+// Role in the reference: src/ModMult.cuh:46-313 (Shoup_mult_64, Neal_mult_64,
+// modreduce on 128-bit values) and src/AddSub.cuh:37-49.  The formulations
+// below are independent: Shoup's precomputed-quotient product (V. Shoup,
+// NTL; D. Harvey, "Faster arithmetic for number-theoretic transforms", 2014)
+// for products by a constant, and a two-step reduction of 128-bit values
+// (high word by Shoup with 2^64 mod p, low word by a one-word Barrett
+// quotient) for products of two variables and for 128-bit accumulators.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define FHD __host__ __device__ __forceinline__
+#else
+#define FHD inline
+#endif
+
+namespace fides {
+
+FHD uint64_t mulhi64(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+    return __umul64hi(a, b);
+#else
+    return (uint64_t)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+// Per-prime constants needed by the reductions.
+struct PrimeConst {
+    uint64_t p;
+    uint64_t two_p;
+    uint64_t mu64;    // floor(2^64 / p)
+    uint64_t r64;     // 2^64 mod p
+    uint64_t r64_sh;  // Shoup companion of r64
+    uint64_t ninv;    // N^-1 mod p
+    uint64_t ninv_sh;
+    uint64_t pad;
+};
+
+// floor(w * 2^64 / p), host only (needs a 128-bit division).
+inline uint64_t shoup_precompute(uint64_t w, uint64_t p) {
+    return (uint64_t)(((unsigned __int128)w << 64) / p);
+}
+
+FHD uint64_t csub(uint64_t x, uint64_t m) { return x >= m ? x - m : x; }
+
+FHD uint64_t add_mod(uint64_t a, uint64_t b, uint64_t p) { return csub(a + b, p); }
+FHD uint64_t sub_mod(uint64_t a, uint64_t b, uint64_t p) { return a >= b ? a - b : a + p - b; }
+FHD uint64_t neg_mod(uint64_t a, uint64_t p) { return a ? p - a : 0; }
+
+// a * w mod p in [0, 2p) for any a < 2^64 (w < p, w_sh = floor(w 2^64 / p)).
+FHD uint64_t mul_shoup_lazy(uint64_t a, uint64_t w, uint64_t w_sh, uint64_t p) {
+    const uint64_t q = mulhi64(a, w_sh);
+    return a * w - q * p;
+}
+FHD uint64_t mul_shoup(uint64_t a, uint64_t w, uint64_t w_sh, uint64_t p) {
+    return csub(mul_shoup_lazy(a, w, w_sh, p), p);
+}
+
+// x mod p for x < 2^64 via q = floor(x * mu64 / 2^64) (q >= floor(x/p) - 1).
+FHD uint64_t reduce64_lazy(uint64_t x, const PrimeConst& c) {  // result in [0, 2p)
+    return x - mulhi64(x, c.mu64) * c.p;
+}
+
+// (hi*2^64 + lo) mod p, any 128-bit value, canonical result.
+FHD uint64_t reduce128(uint64_t hi, uint64_t lo, const PrimeConst& c) {
+    uint64_t a = mul_shoup_lazy(hi, c.r64, c.r64_sh, c.p);  // [0, 2p)
+    uint64_t b = reduce64_lazy(lo, c);                       // [0, 2p)
+    uint64_t s = a + b;                                      // [0, 4p) < 2^64 for p < 2^62
+    s = csub(s, c.two_p);
+    return csub(s, c.p);
+}
+
+// 128-bit accumulator of 64x64 products.
+struct Acc128 {
+    uint64_t lo, hi;
+    FHD Acc128() : lo(0), hi(0) {}
+    FHD void mac(uint64_t a, uint64_t b) {
+        const uint64_t l = a * b;
+        const uint64_t h = mulhi64(a, b);
+        lo += l;
+        hi += h + (lo < l ? 1 : 0);
+    }
+    FHD uint64_t reduce(const PrimeConst& c) const { return reduce128(hi, lo, c); }
+};
+
+FHD uint64_t mul_mod(uint64_t a, uint64_t b, const PrimeConst& c) {
+    return reduce128(mulhi64(a, b), a * b, c);
+}
+
+}  // namespace fides

@@ -1,0 +1,115 @@
+"""Bit-exact parity of the CUDA path with the CPU oracle, through the C ABI.
+
+Shapes follow FIDESlib's own tests: per-limb NTT against the CPU transform at
+logN 13..16 (test/NTTtests.cu), Mult/Square/MultRescale at every level
+(test/OpenFheInterfaceTests.cu), rotations and hoisted rotations, on the
+reference's own prime lists (test/ParametrizedTest.cuh p64/sp64) and on the
+generated moduli of the HMult workload (N=2^16, L=30, K=10, dnum=3).
+"""
+import numpy as np
+import pytest
+
+from gpu_helpers import from_dev, make_pair, rand_ct, rand_key, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("logN", [10, 12, 13, 14, 15, 16])
+def test_ntt_roundtrip_and_parity(logN):
+    cc, oc = make_pair(logN, 4, 2, 2, ref_primes=True)
+    nl = 6
+    x = oc.random(list(range(nl)), 100 + logN)
+    d = to_dev(x)
+    cc.ntt(d.data_ptr(), 0, nl)
+    got = from_dev(d)
+    want = oc.ntt(x, list(range(nl)))
+    assert np.array_equal(got, want)
+    cc.ntt(d.data_ptr(), 0, nl, inverse=True)
+    assert np.array_equal(from_dev(d), x)
+
+
+def test_polymul_30_limbs_n16():
+    """Plain RNS polynomial multiply: N=2^16, 30 limbs (fwd NTT x2, product, INTT)."""
+    import torch
+
+    cc, oc = make_pair(16, 30, 10, 3)
+    pid = list(range(30))
+    a, b = oc.random(pid, 1), oc.random(pid, 2)
+    da, db = to_dev(a), to_dev(b)
+    dc = torch.empty_like(da)
+    sa, sb = torch.empty_like(da), torch.empty_like(da)
+    cc.polymul(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sa.data_ptr(), sb.data_ptr(), 0, 30)
+    want = oc.ntt(oc.polymul(oc.ntt(a, pid), oc.ntt(b, pid), pid), pid, inverse=True)
+    assert np.array_equal(from_dev(dc), want)
+
+
+@pytest.mark.parametrize("ref", [True, False])
+def test_hmult_all_levels_small(ref):
+    cc, oc = make_pair(12, 8, 3, 3, ref_primes=ref)
+    kb, ka = rand_key(oc, 50)
+    cc.upload_relin_key(kb, ka)
+    for level in range(0, 8):
+        a0, a1 = rand_ct(oc, level, 10 * level + 1)
+        b0, b1 = rand_ct(oc, level, 10 * level + 5)
+        A, B = cc.upload(a0, a1), cc.upload(b0, b1)
+        for rs in ([False, True] if level > 0 else [False]):
+            got = cc.EvalMult(A, B, rescale=rs).download()
+            want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=rs)
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (level, rs)
+
+
+def test_square_matches_mult_self():
+    cc, oc = make_pair(12, 6, 2, 2)
+    kb, ka = rand_key(oc, 7)
+    cc.upload_relin_key(kb, ka)
+    a0, a1 = rand_ct(oc, 5, 3)
+    A = cc.upload(a0, a1)
+    got = cc.EvalSquare(A, rescale=True).download()
+    want = oc.hmult(5, a0, a1, a0, a1, kb, ka, rescale=True)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+def test_rescale_parity():
+    cc, oc = make_pair(13, 6, 2, 2, ref_primes=True)
+    for level in (1, 3, 5):
+        c0, c1 = rand_ct(oc, level, 77 + level)
+        got = cc.Rescale(cc.upload(c0, c1)).download()
+        assert np.array_equal(got[0], oc.rescale(level, c0))
+        assert np.array_equal(got[1], oc.rescale(level, c1))
+
+
+def test_rotate_and_hoisted_parity():
+    cc, oc = make_pair(12, 8, 3, 3)
+    idx = [1, -1, 5, 100]
+    keys = {}
+    for i, r in enumerate(idx):
+        g = cc.rotation_galois(r)
+        keys[g] = rand_key(oc, 300 + 2 * i)
+        cc.upload_galois_key(g, *keys[g])
+    for level in (7, 4, 0):
+        c0, c1 = rand_ct(oc, level, 900 + level)
+        A = cc.upload(c0, c1)
+        for r in idx:
+            g = cc.rotation_galois(r)
+            got = cc.EvalRotate(A, r).download()
+            want = oc.rotate(level, c0, c1, pow(g, -1, 2 * oc.N), *keys[g])
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (level, r)
+        outs = cc.EvalFastRotation(A, idx)
+        gals = [cc.rotation_galois(r) for r in idx]
+        w0, w1 = oc.rotate_hoisted(level, c0, c1, [pow(g, -1, 2 * oc.N) for g in gals],
+                                   [keys[g][0] for g in gals], [keys[g][1] for g in gals])
+        for o, x0, x1 in zip(outs, w0, w1):
+            g0, g1 = o.download()
+            assert np.array_equal(g0, x0) and np.array_equal(g1, x1)
+
+
+def test_hmult_c2_shape_bitexact():
+    """HMult+Relin+Rescale at N=2^16, L=30, K=10, dnum=3, top level, one pair."""
+    cc, oc = make_pair(16, 30, 10, 3)
+    kb, ka = rand_key(oc, 1234)
+    cc.upload_relin_key(kb, ka)
+    a0, a1 = rand_ct(oc, 29, 11)
+    b0, b1 = rand_ct(oc, 29, 13)
+    got = cc.EvalMult(cc.upload(a0, a1), cc.upload(b0, b1), rescale=True).download()
+    want = oc.hmult(29, a0, a1, b0, b1, kb, ka, rescale=True)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
