@@ -185,6 +185,10 @@ def run_ours(args):
     from pyfideslib_b200._capi import lib
 
     cc = F.CryptoContext(log_n=LOGN, num_q=L, dnum=DNUM, num_p=K, device=local)
+    tv, nv = C.c_int(), C.c_int()
+    tms = (C.c_float * 8)()
+    lib.fides_autotune(cc._h, C.byref(tv), tms, C.byref(nv))
+    autotune = {"ntt_variant": tv.value, "fwd_inv_30limb_us": [round(1e3 * tms[i], 2) for i in range(nv.value)]}
     stream_ptr = C.c_void_p()
     lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))
     st = torch.cuda.ExternalStream(stream_ptr.value, device=local)
@@ -314,6 +318,7 @@ def run_ours(args):
                             "traffic": None, "algorithmic_bytes": ntt_bytes, "us_per_launch": ntt_ms * 1e3},
                "ntt_gbs": achieved,
                "gpu_launches": int(launches),
+               "autotune": autotune,
                "clocks": clk.summary(),
                "cpu_baseline": cpu}
         print(json.dumps(out), flush=True)

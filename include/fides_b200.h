@@ -75,6 +75,13 @@ const char* fides_ctx_last_error(const fides_ctx* ctx);
  * callers that time or order work around it (FIDESlib keeps per-partition
  * streams in ContextData, src/CKKS/Context.cuh:85-98). */
 fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream);
+/* Autotuner: time every NTT kernel variant (occupancy / twiddle-fetch
+ * policy) on this context's limb shapes and keep the fastest.  Runs once in
+ * fides_ctx_create; call again to re-tune.  *variant and times_ms (one entry
+ * per variant) may be NULL.  Results never depend on the variant. */
+fides_status fides_autotune(fides_ctx* ctx, int* variant, float* times_ms, int* num_variants);
+/* Force an NTT variant (for measurements); -1 restores the tuned choice. */
+fides_status fides_set_ntt_variant(fides_ctx* ctx, int variant);
 /* Number of kernels this library has launched so far (process-wide). */
 uint64_t fides_kernel_launches(void);
 

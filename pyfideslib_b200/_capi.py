@@ -49,6 +49,8 @@ EXPORTS = {
     "fides_ctx_last_error": ([vp], C.c_char_p),
     "fides_ctx_stream": ([vp, C.POINTER(vp)], C.c_int),
     "fides_kernel_launches": ([], C.c_uint64),
+    "fides_autotune": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
+    "fides_set_ntt_variant": ([vp, C.c_int], C.c_int),
     "fides_key_upload_relin": ([vp, u64p, u64p], C.c_int),
     "fides_key_upload_galois": ([vp, C.c_uint32, u64p, u64p], C.c_int),
     "fides_rotation_galois": ([vp, C.c_int32, C.c_int], C.c_uint32),

@@ -53,31 +53,33 @@ void ks_modup(fides_ctx* c, int level, const uint64_t* x) {
     ntt_forward(c->dev, dm, FL_PLAIN, FS_PLAIN, c->st);
 }
 
-// INTT (scaled by (P/p_k)^-1) of the special limbs of XB and XA, in place.
-void special_intt(fides_ctx* c, int level, bool both) {
+// Segments for the INTT (scaled by (P/p_k)^-1) of the special limbs of XB and
+// XA, in place.
+void add_special_segs(fides_ctx* c, int level, LimbMap& m) {
     const int n = level + 1, N = c->N;
-    LimbMap m{};
-    m.nseg = both ? 2 : 1;
     uint64_t* bufs[2] = {c->XB, c->XA};
-    for (int s = 0; s < m.nseg; ++s) {
-        LimbSeg& g = m.seg[s];
+    for (int s = 0; s < 2; ++s) {
+        LimbSeg& g = m.seg[m.nseg++];
+        g = LimbSeg{};
         g.in = g.out = bufs[s] + (size_t)n * N;
         g.count = c->K;
         g.skip_lo = c->K;
         g.nq = 0;
-        g.q0 = 0;
         g.level = level;
+        g.lmode = IL_PLAIN;
+        g.smode = IS_MODDOWN;
         m.total += c->K;
     }
-    ntt_inverse(c->dev, m, IL_PLAIN, IS_MODDOWN, c->st);
 }
 
 // ModDown of XB -> out0 and XA -> out1 (optionally adding e0/e1), no rescale.
 void moddown_pair(fides_ctx* c, int level, uint64_t* out0, uint64_t* out1, const uint64_t* e0, const uint64_t* e1) {
     const int n = level + 1, N = c->N, L = c->L;
-    special_intt(c, level, true);
-    launch_moddown_conv(c->dev, level, c->XB + (size_t)n * N, c->W, nullptr, c->st);
-    launch_moddown_conv(c->dev, level, c->XA + (size_t)n * N, c->W + (size_t)L * N, nullptr, c->st);
+    LimbMap sp{};
+    add_special_segs(c, level, sp);
+    ntt_inverse(c->dev, sp, -1, -1, c->st);
+    launch_moddown_conv2(c->dev, level, c->XB + (size_t)n * N, c->W, nullptr, c->XA + (size_t)n * N,
+                         c->W + (size_t)L * N, nullptr, c->st);
     LimbMap m{};
     m.nseg = 2;
     const uint64_t* xs[2] = {c->XB, c->XA};
@@ -99,16 +101,18 @@ void moddown_pair(fides_ctx* c, int level, uint64_t* out0, uint64_t* out1, const
 }
 
 // ModDown fused with Rescale:  out = Rescale(e + ModDown(x)) for both halves.
+// One INTT launch covers the special limbs of both halves and the two top
+// limbs (e_l + P^-1 x_l); one conversion launch covers both halves.
 void moddown_rescale_pair(fides_ctx* c, int level, uint64_t* out0, uint64_t* out1, const uint64_t* e0,
                           const uint64_t* e1) {
     const int n = level + 1, N = c->N, L = c->L;
-    special_intt(c, level, true);
-    LimbMap t{};
-    t.nseg = 2;
     const uint64_t* es[2] = {e0, e1};
     const uint64_t* xs[2] = {c->XB, c->XA};
+    LimbMap t{};
+    add_special_segs(c, level, t);
     for (int s = 0; s < 2; ++s) {
-        LimbSeg& g = t.seg[s];
+        LimbSeg& g = t.seg[t.nseg++];
+        g = LimbSeg{};
         g.in = es[s] + (size_t)level * N;
         g.in2 = xs[s] + (size_t)level * N;
         g.out = c->T + (size_t)s * N;
@@ -117,11 +121,13 @@ void moddown_rescale_pair(fides_ctx* c, int level, uint64_t* out0, uint64_t* out
         g.nq = 1;
         g.q0 = level;
         g.level = level;
+        g.lmode = IL_AXPY_PINV;
+        g.smode = IS_PLAIN;
         t.total += 1;
     }
-    ntt_inverse(c->dev, t, IL_AXPY_PINV, IS_PLAIN, c->st);
-    launch_moddown_conv(c->dev, level, c->XB + (size_t)n * N, c->W, c->T, c->st);
-    launch_moddown_conv(c->dev, level, c->XA + (size_t)n * N, c->W + (size_t)L * N, c->T + N, c->st);
+    ntt_inverse(c->dev, t, -1, -1, c->st);
+    launch_moddown_conv2(c->dev, level, c->XB + (size_t)n * N, c->W, c->T, c->XA + (size_t)n * N,
+                         c->W + (size_t)L * N, c->T + N, c->st);
     LimbMap m{};
     m.nseg = 2;
     uint64_t* os[2] = {out0, out1};
@@ -187,6 +193,7 @@ fides_status fides_ctx_create(const fides_params* params, fides_ctx** out) {
         }
     }
     fides_status s = build_context(c, params);
+    if (s == FIDES_OK) s = fides_autotune(c, nullptr, nullptr, nullptr);
     if (s != FIDES_OK) {
         free_context(c);
         delete c;
@@ -243,6 +250,55 @@ fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream) {
 }
 
 uint64_t fides_kernel_launches(void) { return fides::launch_count(); }
+
+fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* num_variants) {
+    if (!c) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int nv = ntt_num_variants();
+    const int nl = std::min(c->L, 30);
+    // any residues work for timing; start from canonical zeros
+    cudaMemsetAsync(c->E0, 0, (size_t)nl * c->limb_bytes(), c->st);
+    LimbMap m = map_single(c->E0, c->E0, nl, nl, 0);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    c->tune_ms.assign(nv, 0.f);
+    int best = 0;
+    for (int v = 0; v < nv; ++v) {
+        c->dev.ntt_variant = v;
+        for (int w = 0; w < 2; ++w) {
+            ntt_forward(c->dev, m, FL_PLAIN, FS_PLAIN, c->st);
+            ntt_inverse(c->dev, m, IL_PLAIN, IS_PLAIN, c->st);
+        }
+        cudaEventRecord(e0, c->st);
+        for (int r = 0; r < 10; ++r) {
+            ntt_forward(c->dev, m, FL_PLAIN, FS_PLAIN, c->st);
+            ntt_inverse(c->dev, m, IL_PLAIN, IS_PLAIN, c->st);
+        }
+        cudaEventRecord(e1, c->st);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        c->tune_ms[v] = ms / 10;
+        if (c->tune_ms[v] < c->tune_ms[best]) best = v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tuned_variant = best;
+    c->dev.ntt_variant = best;
+    if (variant) *variant = best;
+    if (num_variants) *num_variants = nv;
+    if (times_ms)
+        for (int v = 0; v < nv; ++v) times_ms[v] = c->tune_ms[v];
+    return check_cuda(c, "autotune");
+}
+
+fides_status fides_set_ntt_variant(fides_ctx* c, int variant) {
+    if (!c || variant >= ntt_num_variants() || variant < -1) return FIDES_BAD_ARG;
+    Guard g(c);
+    c->dev.ntt_variant = variant < 0 ? c->tuned_variant : variant;
+    return FIDES_OK;
+}
 
 static fides_status upload_key(fides_ctx* c, SwitchKey& k, const uint64_t* b, const uint64_t* a) {
     const size_t words = (size_t)c->dnum * (c->L + c->K) * c->N;

@@ -17,6 +17,7 @@ constexpr int kMaxSeg = 8;
 // adjacently.
 struct DevCtx {
     int logN, N, L, K, dnum, alpha;
+    int ntt_variant;             // NTT kernel variant chosen by the autotuner
     const PrimeConst* pc;        // [L+K]
     const uint64_t* fwd_tw;      // [L+K][N][2]  psi^{bitrev(i)}, companion
     const uint64_t* inv_tw;      // [L+K][N][2]  psi^{-bitrev(i)}, companion
@@ -43,7 +44,9 @@ struct LimbSeg {
     int nq, q0;
     int level;  // level used by level-dependent tables (-1 if unused)
     int in_stride_zero;  // 1: every limb reads the same input limb
-    int pad;
+    int8_t lmode;  // transform prologue mode (FL_* forward, IL_* inverse)
+    int8_t smode;  // transform epilogue mode (FS_* forward, IS_* inverse)
+    int16_t pad;
 };
 
 struct LimbMap {
@@ -59,6 +62,7 @@ struct LimbRef {
     uint64_t* out;
     int prime;
     int level;
+    int lmode, smode;
 };
 
 __device__ __forceinline__ LimbRef resolve_limb(const LimbMap& m, int f, int N, int L) {
@@ -78,6 +82,8 @@ __device__ __forceinline__ LimbRef resolve_limb(const LimbMap& m, int f, int N, 
     const int j = f < g.skip_lo ? f : f + g.skip_cnt;
     r.prime = j < g.nq ? g.q0 + j : L + (j - g.nq);
     r.level = g.level;
+    r.lmode = g.lmode;
+    r.smode = g.smode;
     return r;
 }
 

@@ -252,6 +252,8 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     const int K = (int)p.size();
     c->K = K;
     const int NP = L + K;
+    if (c->alpha > 16 || K > 16 || c->dnum > 8)
+        return set_err(c, FIDES_UNSUPPORTED, "need digit size <= 16, special moduli <= 16, dnum <= 8");
     if (NP > kMaxPrimes) return set_err(c, FIDES_BAD_ARG, "too many primes");
     for (int i = 0; i < NP; ++i) {
         uint64_t x = i < L ? q[i] : p[i - L];

@@ -84,6 +84,8 @@ struct fides_ctx {
     std::map<uint32_t, fides::SwitchKey> galois_keys;
     std::map<uint32_t, fides::SwitchKey> host_generated;  // galois 0 = relin (for export)
 
+    int tuned_variant = 0;
+    std::vector<float> tune_ms;
     std::string last_error;
     std::recursive_mutex mu;
 

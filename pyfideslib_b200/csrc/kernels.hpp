@@ -23,8 +23,10 @@ uint64_t launch_count();
 void count_launches(int n);
 
 bool ntt_supported(int logN);
+int ntt_num_variants();
 // Forward NTT of every limb in `map`: pass 1 reads seg.in (writes seg.out),
-// pass 2 transforms seg.out in place and applies the epilogue.
+// pass 2 transforms seg.out in place and applies the epilogue.  load / store
+// >= 0 override the per-segment modes.
 void ntt_forward(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st);
 // Inverse NTT: pass A reads seg.in (+in2 for the prologue), writes seg.out;
 // pass B finishes seg.out in place.
@@ -40,6 +42,13 @@ void launch_ks_inner(const DevCtx& ctx, int level, const uint64_t* e2, const uin
                      uint32_t galois_inv, cudaStream_t st);
 void launch_moddown_conv(const DevCtx& ctx, int level, const uint64_t* y, uint64_t* w, const uint64_t* ttop,
                          cudaStream_t st);
+// both halves (b, a) of a key-switch result in one launch
+void launch_moddown_conv2(const DevCtx& ctx, int level, const uint64_t* y0, uint64_t* w0, const uint64_t* ttop0,
+                          const uint64_t* y1, uint64_t* w1, const uint64_t* ttop1, cudaStream_t st);
+// the conversion kernels keep up to 16 inputs (digit moduli / special moduli) in registers
+bool conv_supported(const DevCtx& ctx);
+// override every segment's prologue / epilogue mode (-1 keeps the segment's own)
+void set_modes(LimbMap& map, int lmode, int smode);
 
 // element-wise helpers; limbs 0..n-1 use primes q0..q0+n-1
 enum { EW_ADD = 0, EW_SUB = 1, EW_NEG = 2, EW_MUL = 3, EW_COPY = 4 };

@@ -73,55 +73,87 @@ void launch_tensor(const DevCtx& ctx, int n, const uint64_t* a0, const uint64_t*
 // target prime t outside the digit gets  sum_i xt_i * [Q'/q_i]_t  mod t.
 // Digit d's targets are stored at dig + (d*dig_stride + m)*N, m = target index
 // (Q primes below the digit, Q primes above it up to `level`, then P).
+//
+// Each thread owns two adjacent coefficients and keeps the digit's inputs in
+// registers; the block stages its slice of the conversion matrix and the
+// target constants in shared memory.  Sums of up to 16 products of residues
+// below 2^62 stay below 2^128, so one reduction per output suffices.
 // ---------------------------------------------------------------------------
 constexpr int kConvThreads = 128;
-constexpr int kTargetsPerBlock = 8;
+constexpr int kConvTargets = 32;  // targets per block
+constexpr int kMaxConvIn = 16;    // digit size / special count handled in registers
+
+__device__ __forceinline__ void conv_store(uint64_t* out, const Acc128& a, const Acc128& b, const PrimeConst& pc) {
+    ulonglong2 o;
+    o.x = a.reduce(pc);
+    o.y = b.reduce(pc);
+    *reinterpret_cast<ulonglong2*>(out) = o;
+}
 
 __global__ void __launch_bounds__(kConvThreads) k_modup_conv(const __grid_constant__ DevCtx ctx, int level,
                                                              const uint64_t* __restrict__ xt,
                                                              uint64_t* __restrict__ dig, size_t dig_stride) {
-    extern __shared__ uint64_t xs[];  // [cnt][kConvThreads]
+    __shared__ uint64_t sM[kMaxConvIn][kConvTargets];
+    __shared__ PrimeConst sP[kConvTargets];
     const int d = blockIdx.y;
     const int n = level + 1;
     const int lo = d * ctx.alpha;
-    int hi = lo + ctx.alpha - 1;
-    if (hi > level) hi = level;
+    const int hi = min(lo + ctx.alpha - 1, level);
     const int cnt = hi - lo + 1;
     const int ntar = n - cnt + ctx.K;
-    const int m0 = blockIdx.z * kTargetsPerBlock;
+    const int m0 = blockIdx.z * kConvTargets;
     if (m0 >= ntar) return;
-    const int m1 = min(m0 + kTargetsPerBlock, ntar);
-    const int j = blockIdx.x * kConvThreads + threadIdx.x;
-    for (int i = 0; i < cnt; ++i) xs[i * kConvThreads + threadIdx.x] = xt[(size_t)(lo + i) * ctx.N + j];
-    const uint64_t* mat = ctx.modup_mat + (size_t)level * ctx.L * (ctx.L + ctx.K);
+    const int nt = min(kConvTargets, ntar - m0);
     const int NP = ctx.L + ctx.K;
-    for (int m = m0; m < m1; ++m) {
+    const uint64_t* mat = ctx.modup_mat + (size_t)level * ctx.L * NP;
+    for (int e = threadIdx.x; e < cnt * nt; e += kConvThreads) {
+        const int i = e / nt, mm = e % nt, m = m0 + mm;
         const int jj = m < lo ? m : m + cnt;
         const int t = jj < n ? jj : ctx.L + (jj - n);
-        const PrimeConst pc = ctx.pc[t];
-        Acc128 acc;
-        int run = 0;
-        for (int i = 0; i < cnt; ++i) {
-            acc.mac(xs[i * kConvThreads + threadIdx.x], __ldg(mat + (size_t)(lo + i) * NP + t));
-            if (++run == 15 && i + 1 < cnt) {  // keep the 128-bit sum from overflowing
-                const uint64_t v = acc.reduce(pc);
-                acc = Acc128();
-                acc.lo = v;
-                run = 1;
+        sM[i][mm] = mat[(size_t)(lo + i) * NP + t];
+        if (i == 0) sP[mm] = ctx.pc[t];
+    }
+    const size_t j = ((size_t)blockIdx.x * kConvThreads + threadIdx.x) * 2;
+    uint64_t x0[kMaxConvIn], x1[kMaxConvIn];
+#pragma unroll
+    for (int i = 0; i < kMaxConvIn; ++i) {
+        if (i < cnt) {
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(xt + (size_t)(lo + i) * ctx.N + j);
+            x0[i] = v.x;
+            x1[i] = v.y;
+        }
+    }
+    __syncthreads();
+    uint64_t* out = dig + ((size_t)d * dig_stride + m0) * ctx.N + j;
+    // two targets per iteration: four independent 128-bit accumulators
+#pragma unroll 1
+    for (int mm = 0; mm < nt; mm += 2) {
+        const int m2 = mm + 1 < nt ? mm + 1 : mm;
+        Acc128 a, b, c2, d2;
+#pragma unroll
+        for (int i = 0; i < kMaxConvIn; ++i) {
+            if (i < cnt) {
+                const uint64_t M = sM[i][mm], M2 = sM[i][m2];
+                a.mac(x0[i], M);
+                b.mac(x1[i], M);
+                c2.mac(x0[i], M2);
+                d2.mac(x1[i], M2);
             }
         }
-        dig[((size_t)d * dig_stride + m) * ctx.N + j] = acc.reduce(pc);
+        conv_store(out + (size_t)mm * ctx.N, a, b, sP[mm]);
+        if (m2 != mm) conv_store(out + (size_t)m2 * ctx.N, c2, d2, sP[m2]);
     }
 }
+
+bool conv_supported(const DevCtx& ctx) { return ctx.alpha <= kMaxConvIn && ctx.K <= kMaxConvIn; }
 
 void launch_modup_conv(const DevCtx& ctx, int level, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
                        cudaStream_t st) {
     const int nd = level / ctx.alpha + 1;
     const int maxtar = level + 1 + ctx.K;
-    dim3 g(ctx.N / kConvThreads, nd, (maxtar + kTargetsPerBlock - 1) / kTargetsPerBlock);
-    const size_t smem = sizeof(uint64_t) * kConvThreads * ctx.alpha;
+    dim3 g(ctx.N / (2 * kConvThreads), nd, (maxtar + kConvTargets - 1) / kConvTargets);
     count_launches(1);
-    k_modup_conv<<<g, kConvThreads, smem, st>>>(ctx, level, xt, dig, dig_stride);
+    k_modup_conv<<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride);
 }
 
 // ---------------------------------------------------------------------------
@@ -133,53 +165,94 @@ void launch_modup_conv(const DevCtx& ctx, int level, const uint64_t* xt, uint64_
 // ModUp output.  With galois_inv != 0 the result is written permuted:
 // out[j] = value at slot(galois_inv, j).
 // ---------------------------------------------------------------------------
+template <int VEC>
 __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx ctx, int level,
                                                   const uint64_t* __restrict__ e2, const uint64_t* __restrict__ dig,
                                                   size_t dig_stride, const uint64_t* __restrict__ kb,
                                                   const uint64_t* __restrict__ ka, uint64_t* __restrict__ xb,
                                                   uint64_t* __restrict__ xa, const uint64_t* __restrict__ c0,
-                                                  uint32_t galois_inv) {
+                                                  uint32_t galois) {
     const int n = level + 1;
     const int m = blockIdx.y;
     const int t = m < n ? m : ctx.L + (m - n);
     const PrimeConst pc = ctx.pc[t];
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t src = galois_inv ? automorph_slot(ctx.logN, galois_inv, j) : (uint32_t)j;
     const int nd = level / ctx.alpha + 1;
     const size_t kstride = (size_t)(ctx.L + ctx.K) * ctx.N;
-    Acc128 sb, sa;
-    for (int d = 0; d < nd; ++d) {
-        const int lo = d * ctx.alpha;
-        const int hi = min(lo + ctx.alpha - 1, level);
-        const int cnt = hi - lo + 1;
-        uint64_t x;
-        if (m < n && t >= lo && t <= hi) {
-            x = e2[(size_t)t * ctx.N + src];
-        } else {
-            const int md = m < n ? (t < lo ? t : t - cnt) : (n - cnt) + (m - n);
-            x = dig[((size_t)d * dig_stride + md) * ctx.N + src];
+    // source limb of each digit for this prime
+    const uint64_t* srcs[8];
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+        if (d < nd) {
+            const int lo = d * ctx.alpha;
+            const int hi = min(lo + ctx.alpha - 1, level);
+            const int cnt = hi - lo + 1;
+            if (m < n && t >= lo && t <= hi) {
+                srcs[d] = e2 + (size_t)t * ctx.N;
+            } else {
+                const int md = m < n ? (t < lo ? t : t - cnt) : (n - cnt) + (m - n);
+                srcs[d] = dig + ((size_t)d * dig_stride + md) * ctx.N;
+            }
         }
-        sb.mac(x, kb[d * kstride + (size_t)t * ctx.N + src]);
-        sa.mac(x, ka[d * kstride + (size_t)t * ctx.N + src]);
     }
-    if (c0 && m < n) {
-        const ulonglong2 pm = __ldg(reinterpret_cast<const ulonglong2*>(ctx.md_pmod) + t);
-        sb.mac(mul_shoup(c0[(size_t)m * ctx.N + src], pm.x, pm.y, pc.p), 1);
+    if constexpr (VEC) {
+        const size_t j = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 2;
+        Acc128 sb0, sb1, sa0, sa1;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            if (d < nd) {
+                const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(srcs[d] + j);
+                const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(kb + d * kstride + (size_t)t * ctx.N + j);
+                const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(ka + d * kstride + (size_t)t * ctx.N + j);
+                sb0.mac(x.x, b.x);
+                sb1.mac(x.y, b.y);
+                sa0.mac(x.x, a.x);
+                sa1.mac(x.y, a.y);
+            }
+        }
+        ulonglong2 ob, oa;
+        ob.x = sb0.reduce(pc);
+        ob.y = sb1.reduce(pc);
+        oa.x = sa0.reduce(pc);
+        oa.y = sa1.reduce(pc);
+        *reinterpret_cast<ulonglong2*>(xb + (size_t)m * ctx.N + j) = ob;
+        *reinterpret_cast<ulonglong2*>(xa + (size_t)m * ctx.N + j) = oa;
+    } else {
+        const int j = blockIdx.x * blockDim.x + threadIdx.x;
+        const uint32_t src = galois ? automorph_slot(ctx.logN, galois, j) : (uint32_t)j;
+        Acc128 sb, sa;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            if (d < nd) {
+                const uint64_t x = srcs[d][src];
+                sb.mac(x, kb[d * kstride + (size_t)t * ctx.N + src]);
+                sa.mac(x, ka[d * kstride + (size_t)t * ctx.N + src]);
+            }
+        }
+        if (c0 && m < n) {
+            const ulonglong2 pm = __ldg(reinterpret_cast<const ulonglong2*>(ctx.md_pmod) + t);
+            sb.mac(mul_shoup(c0[(size_t)m * ctx.N + src], pm.x, pm.y, pc.p), 1);
+        }
+        xb[(size_t)m * ctx.N + j] = sb.reduce(pc);
+        xa[(size_t)m * ctx.N + j] = sa.reduce(pc);
     }
-    xb[(size_t)m * ctx.N + j] = sb.reduce(pc);
-    xa[(size_t)m * ctx.N + j] = sa.reduce(pc);
 }
 
 void launch_ks_inner(const DevCtx& ctx, int level, const uint64_t* e2, const uint64_t* dig, size_t dig_stride,
                      const uint64_t* kb, const uint64_t* ka, uint64_t* xb, uint64_t* xa, const uint64_t* c0,
                      uint32_t galois_inv, cudaStream_t st) {
-    dim3 g(ctx.N / 256, level + 1 + ctx.K);
     count_launches(1);
-    k_ks_inner<<<g, 256, 0, st>>>(ctx, level, e2, dig, dig_stride, kb, ka, xb, xa, c0, galois_inv);
+    if (!c0 && !galois_inv) {
+        dim3 g(ctx.N / 512, level + 1 + ctx.K);
+        k_ks_inner<1><<<g, 256, 0, st>>>(ctx, level, e2, dig, dig_stride, kb, ka, xb, xa, c0, galois_inv);
+    } else {
+        dim3 g(ctx.N / 256, level + 1 + ctx.K);
+        k_ks_inner<0><<<g, 256, 0, st>>>(ctx, level, e2, dig, dig_stride, kb, ka, xb, xa, c0, galois_inv);
+    }
 }
 
 // ---------------------------------------------------------------------------
-// ModDown base conversion (ModDown2).  y = special limbs already scaled by
+// ModDown base conversion (ModDown2), both halves of a key-switch result in
+// one launch (blockIdx.z = half).  y = special limbs already scaled by
 // (P/p_k)^-1 (scaled INTT).  Without ttop: w_j = sum_k y_k [P/p_k]_{q_j} for
 // j = 0..level.  With ttop (fused rescale; ttop = INTT(e_l + P^-1 x_l)):
 //   conv_l = sum_k y_k [P/p_k]_{q_l};  tl = ttop - P^-1 conv_l  (mod q_l)
@@ -193,53 +266,114 @@ __device__ __forceinline__ uint64_t switch_modulus_d(uint64_t a, uint64_t om, co
     return csub(reduce64_lazy(v, nc), nm);
 }
 
+struct MdArgs {
+    const uint64_t* y[2];
+    uint64_t* w[2];
+    const uint64_t* ttop[2];
+};
+
 __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_constant__ DevCtx ctx, int level,
-                                                               const uint64_t* __restrict__ y,
-                                                               uint64_t* __restrict__ w,
-                                                               const uint64_t* __restrict__ ttop) {
-    extern __shared__ uint64_t ys[];  // [K][kConvThreads]
-    const int j = blockIdx.x * kConvThreads + threadIdx.x;
+                                                               const __grid_constant__ MdArgs args) {
+    __shared__ uint64_t sM[kMaxConvIn][kConvTargets];
+    __shared__ PrimeConst sP[kConvTargets];
+    __shared__ ulonglong2 sPinv[kConvTargets];
+    const int half = blockIdx.z;
+    const uint64_t* __restrict__ y = args.y[half];
+    uint64_t* __restrict__ w = args.w[half];
+    const uint64_t* __restrict__ ttop = args.ttop[half];
     const int K = ctx.K, L = ctx.L;
-    for (int k = 0; k < K; ++k) ys[k * kConvThreads + threadIdx.x] = y[(size_t)k * ctx.N + j];
-    auto conv = [&](int q) -> uint64_t {
-        const PrimeConst pc = ctx.pc[q];
-        Acc128 acc;
-        int run = 0;
-        for (int k = 0; k < K; ++k) {
-            acc.mac(ys[k * kConvThreads + threadIdx.x], __ldg(ctx.md_mat + (size_t)k * L + q));
-            if (++run == 15 && k + 1 < K) {
-                const uint64_t v = acc.reduce(pc);
-                acc = Acc128();
-                acc.lo = v;
-                run = 1;
+    const int nout = ttop ? level : level + 1;
+    const int q0 = blockIdx.y * kConvTargets;
+    const int nt = min(kConvTargets, nout - q0);
+    if (nt <= 0) return;
+    for (int e = threadIdx.x; e < K * nt; e += kConvThreads) {
+        const int k = e / nt, qq = e % nt;
+        sM[k][qq] = ctx.md_mat[(size_t)k * L + q0 + qq];
+        if (k == 0) {
+            sP[qq] = ctx.pc[q0 + qq];
+            sPinv[qq] = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[q0 + qq];
+        }
+    }
+    const size_t j = ((size_t)blockIdx.x * kConvThreads + threadIdx.x) * 2;
+    uint64_t y0[kMaxConvIn], y1[kMaxConvIn];
+#pragma unroll
+    for (int k = 0; k < kMaxConvIn; ++k) {
+        if (k < K) {
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(y + (size_t)k * ctx.N + j);
+            y0[k] = v.x;
+            y1[k] = v.y;
+        }
+    }
+    uint64_t tl0 = 0, tl1 = 0;
+    uint64_t ql = 0;
+    if (ttop) {
+        const PrimeConst pl = ctx.pc[level];
+        const ulonglong2 pinv_l = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[level];
+        Acc128 a, b;
+#pragma unroll
+        for (int k = 0; k < kMaxConvIn; ++k) {
+            if (k < K) {
+                const uint64_t M = ctx.md_mat[(size_t)k * L + level];
+                a.mac(y0[k], M);
+                b.mac(y1[k], M);
             }
         }
-        return acc.reduce(pc);
+        const ulonglong2 tv = *reinterpret_cast<const ulonglong2*>(ttop + j);
+        tl0 = sub_mod(tv.x, mul_shoup(a.reduce(pl), pinv_l.x, pinv_l.y, pl.p), pl.p);
+        tl1 = sub_mod(tv.y, mul_shoup(b.reduce(pl), pinv_l.x, pinv_l.y, pl.p), pl.p);
+        ql = pl.p;
+    }
+    __syncthreads();
+    auto finish = [&](int qq, const Acc128& a, const Acc128& b) {
+        const PrimeConst pc = sP[qq];
+        ulonglong2 o;
+        o.x = a.reduce(pc);
+        o.y = b.reduce(pc);
+        if (ttop) {
+            const ulonglong2 pinv = sPinv[qq];
+            o.x = add_mod(mul_shoup(o.x, pinv.x, pinv.y, pc.p), switch_modulus_d(tl0, ql, pc), pc.p);
+            o.y = add_mod(mul_shoup(o.y, pinv.x, pinv.y, pc.p), switch_modulus_d(tl1, ql, pc), pc.p);
+        }
+        *reinterpret_cast<ulonglong2*>(w + (size_t)(q0 + qq) * ctx.N + j) = o;
     };
-    if (!ttop) {
-        for (int q = blockIdx.y * kTargetsPerBlock; q < min((int)(blockIdx.y + 1) * kTargetsPerBlock, level + 1); ++q)
-            w[(size_t)q * ctx.N + j] = conv(q);
-        return;
+#pragma unroll 1
+    for (int qq = 0; qq < nt; qq += 2) {
+        const int q2 = qq + 1 < nt ? qq + 1 : qq;
+        Acc128 a, b, c2, d2;
+#pragma unroll
+        for (int k = 0; k < kMaxConvIn; ++k) {
+            if (k < K) {
+                const uint64_t M = sM[k][qq], M2 = sM[k][q2];
+                a.mac(y0[k], M);
+                b.mac(y1[k], M);
+                c2.mac(y0[k], M2);
+                d2.mac(y1[k], M2);
+            }
+        }
+        finish(qq, a, b);
+        if (q2 != qq) finish(q2, c2, d2);
     }
-    const PrimeConst pl = ctx.pc[level];
-    const ulonglong2 pinv_l = __ldg(reinterpret_cast<const ulonglong2*>(ctx.md_pinv) + level);
-    const uint64_t tl = sub_mod(ttop[j], mul_shoup(conv(level), pinv_l.x, pinv_l.y, pl.p), pl.p);
-    for (int q = blockIdx.y * kTargetsPerBlock; q < min((int)(blockIdx.y + 1) * kTargetsPerBlock, level); ++q) {
-        const PrimeConst pc = ctx.pc[q];
-        const ulonglong2 pinv = __ldg(reinterpret_cast<const ulonglong2*>(ctx.md_pinv) + q);
-        const uint64_t a = mul_shoup(conv(q), pinv.x, pinv.y, pc.p);
-        w[(size_t)q * ctx.N + j] = add_mod(a, switch_modulus_d(tl, pl.p, pc), pc.p);
-    }
+}
+
+void launch_moddown_conv2(const DevCtx& ctx, int level, const uint64_t* y0, uint64_t* w0, const uint64_t* ttop0,
+                          const uint64_t* y1, uint64_t* w1, const uint64_t* ttop1, cudaStream_t st) {
+    const int nout = ttop0 ? level : level + 1;
+    if (nout <= 0) return;
+    MdArgs a;
+    a.y[0] = y0;
+    a.y[1] = y1;
+    a.w[0] = w0;
+    a.w[1] = w1;
+    a.ttop[0] = ttop0;
+    a.ttop[1] = ttop1;
+    dim3 g(ctx.N / (2 * kConvThreads), (nout + kConvTargets - 1) / kConvTargets, y1 ? 2 : 1);
+    count_launches(1);
+    k_moddown_conv<<<g, kConvThreads, 0, st>>>(ctx, level, a);
 }
 
 void launch_moddown_conv(const DevCtx& ctx, int level, const uint64_t* y, uint64_t* w, const uint64_t* ttop,
                          cudaStream_t st) {
-    const int nout = ttop ? level : level + 1;
-    if (nout <= 0) return;
-    dim3 g(ctx.N / kConvThreads, (nout + kTargetsPerBlock - 1) / kTargetsPerBlock);
-    const size_t smem = sizeof(uint64_t) * kConvThreads * ctx.K;
-    count_launches(1);
-    k_moddown_conv<<<g, kConvThreads, smem, st>>>(ctx, level, y, w, ttop);
+    launch_moddown_conv2(ctx, level, y, w, ttop, nullptr, nullptr, nullptr, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -12,16 +12,22 @@
 //     first LR stages only pair elements of one column, the last LC stages
 //     only elements of one row.  Pass 1 runs the column stages, pass 2 the
 //     row stages; the intermediate limb (512 KiB at N=2^16) stays in L2.
-//   * Each thread owns 16 elements of one column/row in registers and runs 4
-//     butterfly stages on them (radix-16 register blocking); the next group
-//     of stages follows one shared-memory exchange.  Column passes move 16
-//     consecutive columns per CTA (128-byte coalesced rows); row passes stage
-//     through shared memory so that global stores are coalesced.
+//   * Each thread owns 16 elements of one column/row in registers and runs up
+//     to 4 butterfly stages on them (radix-16 register blocking); the next
+//     group of stages follows one shared-memory exchange.  Column passes move
+//     16 consecutive columns per CTA (128-byte coalesced rows); row passes
+//     stage through padded shared memory so that global stores are coalesced.
+//   * In a group of stages the twiddle of a butterfly only depends on the
+//     high bits of its register index, so every group needs 1+2+4+8 = 15
+//     twiddles per thread; they are fetched together (16-byte (w, Shoup)
+//     pairs) before the butterflies, keeping 15 loads in flight instead of
+//     one dependent load per butterfly.
 //   * Harvey lazy butterflies: values stay in [0,4p) (forward) or [0,2p)
-//     (inverse) and are reduced once at the end; twiddles are read as
-//     16-byte (w, Shoup companion) pairs.
+//     (inverse) and are reduced once at the end.
 //   * Prologues/epilogues fuse the surrounding element-wise work (products of
-//     two inputs, ModDown/Rescale combinations, per-limb CRT scalings).
+//     two inputs, ModDown/Rescale combinations, per-limb CRT scalings).  The
+//     mode is a per-segment field, so one launch can mix limbs with different
+//     fusions.
 #include <atomic>
 
 #include "kernels.hpp"
@@ -59,28 +65,89 @@ __device__ __forceinline__ ulonglong2 ldg2(const uint64_t* base, size_t idx) {
     return __ldg(reinterpret_cast<const ulonglong2*>(base) + idx);
 }
 
+// A stage whose register partner bit is kb pairs k and k | (1 << kb) and uses
+// twiddle  (B << t) + (th_hi << (3 - kb)) + (k >> (kb + 1)),  t = t_of_kb0 - kb;
+// its 8 >> kb twiddles sit at offset (8 >> kb) - 1 of the group's block.
+__device__ __forceinline__ constexpr int tw_off(int kb) { return (8 >> kb) - 1; }
+
+template <int KB, class Tab>
+__device__ __forceinline__ void load_stage_tw(ulonglong2 (&w)[15], Tab tab, int t_of_kb0, size_t B, int th_hi) {
+    const int t = t_of_kb0 - KB;
+    const size_t base = (B << t) + ((size_t)th_hi << (3 - KB));
+#pragma unroll
+    for (int g = 0; g < (8 >> KB); ++g) w[tw_off(KB) + g] = tab(base + g);
+}
+
+// Twiddle-fetch policy of a group: PF = true fetches the 15 twiddles of the
+// whole group up front (more loads in flight, +30 registers); PF = false
+// fetches each stage's twiddles right before the stage (fewer registers,
+// higher occupancy).  The autotuner picks per context.
+template <int KB, int KB_END, int STEP, bool PF, bool FWD, class Tab>
+__device__ __forceinline__ void run_stages(uint64_t (&x)[16], ulonglong2 (&w)[15], Tab tab, int t_of_kb0, size_t B,
+                                           int th_hi, uint64_t p, uint64_t two_p) {
+    if constexpr (!PF) load_stage_tw<KB>(w, tab, t_of_kb0, B, th_hi);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        if (k & (1 << KB)) continue;
+        if constexpr (FWD)
+            ct_bfly(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
+        else
+            gs_bfly(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
+    }
+    if constexpr (KB != KB_END) run_stages<KB + STEP, KB_END, STEP, PF, FWD>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
+}
+
+template <int KB_FIRST, int KB_LAST, bool PF, bool FWD, class Tab>
+__device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi, uint64_t p,
+                                          uint64_t two_p) {
+    ulonglong2 w[15];
+    constexpr int STEP = KB_FIRST > KB_LAST ? -1 : 1;
+    if constexpr (PF) {
+#pragma unroll
+        for (int kb = 0; kb < 4; ++kb) {
+            if ((kb < KB_FIRST && kb < KB_LAST) || (kb > KB_FIRST && kb > KB_LAST)) continue;
+            const int t = t_of_kb0 - kb;
+            const size_t base = (B << t) + ((size_t)th_hi << (3 - kb));
+#pragma unroll
+            for (int g = 0; g < (8 >> kb); ++g) w[tw_off(kb) + g] = tab(base + g);
+        }
+    }
+    run_stages<KB_FIRST, KB_LAST, STEP, PF, FWD>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
+}
+
+// Tile geometry shared by kernels and launchers.
+template <int LR, int LC>
+struct Geo {
+    static constexpr int R = 1 << LR, C = 1 << LC;
+    static constexpr int TPC = 1 << (LR - 4);                       // threads per column
+    static constexpr int TC = (256 / TPC) < C ? (256 / TPC) : C;    // columns per CTA
+    static constexpr int NTC = TPC * TC;
+    static constexpr int TPR = 1 << (LC - 4);                       // threads per row
+    static constexpr int TR = (256 / TPR) < R ? (256 / TPR) : R;    // rows per CTA
+    static constexpr int NTR = TPR * TR;
+    static constexpr int CP = C + C / 16;                           // padded row stride
+};
+
 // ---------------------------------------------------------------------------
 // forward, pass 1: column stages 0..LR-1
 // ---------------------------------------------------------------------------
-template <int LR, int LC, int LOAD>
-__global__ void __launch_bounds__(256, 2) k_ntt_fwd_cols(const __grid_constant__ DevCtx ctx,
-                                                         const __grid_constant__ LimbMap map) {
-    constexpr int R = 1 << LR, C = 1 << LC;
-    constexpr int TPL = 1 << (LR - 4);
-    constexpr int TC = (256 / TPL) < C ? (256 / TPL) : C;
-    constexpr int NT = TPL * TC;
-    __shared__ __align__(16) uint64_t sm[R * TC];
-    __shared__ ulonglong2 tw[R];
+template <int LR, int LC, int MINB, bool PF>
+__global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constant__ DevCtx ctx,
+                                                            const __grid_constant__ LimbMap map) {
+    using G = Geo<LR, LC>;
+    constexpr int C = G::C, TC = G::TC;
+    __shared__ __align__(16) uint64_t sm[G::R * TC];
+    __shared__ ulonglong2 tws[G::R];
 
     const LimbRef lr = resolve_limb(map, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const ulonglong2* twg = reinterpret_cast<const ulonglong2*>(ctx.fwd_tw) + (size_t)lr.prime * ctx.N;
-    for (int i = threadIdx.x; i < R; i += NT) tw[i] = twg[i];
+    for (int i = threadIdx.x; i < G::R; i += G::NTC) tws[i] = twg[i];
 
     const int c = threadIdx.x % TC, th = threadIdx.x / TC;
     const int col = blockIdx.x * TC + c;
     uint64_t x[16];
-    if constexpr (LOAD == FL_SWITCHMOD) {
+    if (lr.lmode == FL_SWITCHMOD) {
         const uint64_t om = ctx.pc[lr.level].p;
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = switch_modulus(lr.in[(size_t)(th + (k << (LR - 4))) * C + col], om, pc);
@@ -89,33 +156,17 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_cols(const __grid_constant__
         for (int k = 0; k < 16; ++k) x[k] = lr.in[(size_t)(th + (k << (LR - 4))) * C + col];
     }
     __syncthreads();
-
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const int kb = 3 - t;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            if (k & (1 << kb)) continue;
-            const int r = th + (k << (LR - 4));
-            ct_bfly(x[k], x[k | (1 << kb)], tw[(1 << t) + (r >> (LR - t))], pc.p, pc.two_p);
-        }
-    }
+    auto tab = [&](size_t i) { return tws[i]; };
+    // stages 0..3: r = th + (k << (LR - 4)), twiddle (1 << t) + (k >> (4 - t))
+    run_group<3, 0, PF, true>(x, tab, 3, 1, 0, pc.p, pc.two_p);
     if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) sm[(th + (k << (LR - 4))) * TC + c] = x[k];
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = sm[((th << 4) + k) * TC + c];
-#pragma unroll
-        for (int t = 4; t < LR; ++t) {
-            const int kb = LR - 1 - t;
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                if (k & (1 << kb)) continue;
-                const int r = (th << 4) + k;
-                ct_bfly(x[k], x[k | (1 << kb)], tw[(1 << t) + (r >> (LR - t))], pc.p, pc.two_p);
-            }
-        }
+        // stages 4..LR-1: r = 16 th + k
+        run_group<LR - 5, 0, PF, true>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
 #pragma unroll
         for (int k = 0; k < 16; ++k) lr.out[(size_t)((th << 4) + k) * C + col] = x[k];
     } else {
@@ -127,25 +178,28 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_cols(const __grid_constant__
 // ---------------------------------------------------------------------------
 // forward, pass 2: row stages LR..logN-1, with fused epilogue
 // ---------------------------------------------------------------------------
-template <int STORE>
-__device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRef& lr, const PrimeConst& pc,
-                                                 size_t g, uint64_t v) {
+__device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRef& lr, const PrimeConst& pc, size_t g,
+                                                 uint64_t v) {
     v = reduce4p(v, pc);
-    if constexpr (STORE == FS_PLAIN) {
-        return v;
-    } else if constexpr (STORE == FS_MODDOWN) {
-        const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
-        uint64_t r = mul_shoup(sub_mod(lr.in2[g], v, pc.p), pinv.x, pinv.y, pc.p);
-        if (lr.in3) r = add_mod(r, lr.in3[g], pc.p);
-        return r;
-    } else if constexpr (STORE == FS_RESCALE) {
-        const ulonglong2 qi = ldg2(ctx.rs_qinv, (size_t)lr.level * ctx.L + lr.prime);
-        return mul_shoup(sub_mod(lr.in2[g], v, pc.p), qi.x, qi.y, pc.p);
-    } else {  // FS_MDRS
-        const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
-        const ulonglong2 qi = ldg2(ctx.rs_qinv, (size_t)lr.level * ctx.L + lr.prime);
-        const uint64_t u = add_mod(lr.in3[g], mul_shoup(lr.in2[g], pinv.x, pinv.y, pc.p), pc.p);
-        return mul_shoup(sub_mod(u, v, pc.p), qi.x, qi.y, pc.p);
+    switch (lr.smode) {
+        case FS_MODDOWN: {
+            const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
+            uint64_t r = mul_shoup(sub_mod(lr.in2[g], v, pc.p), pinv.x, pinv.y, pc.p);
+            if (lr.in3) r = add_mod(r, lr.in3[g], pc.p);
+            return r;
+        }
+        case FS_RESCALE: {
+            const ulonglong2 qi = ldg2(ctx.rs_qinv, (size_t)lr.level * ctx.L + lr.prime);
+            return mul_shoup(sub_mod(lr.in2[g], v, pc.p), qi.x, qi.y, pc.p);
+        }
+        case FS_MDRS: {
+            const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
+            const ulonglong2 qi = ldg2(ctx.rs_qinv, (size_t)lr.level * ctx.L + lr.prime);
+            const uint64_t u = add_mod(lr.in3[g], mul_shoup(lr.in2[g], pinv.x, pinv.y, pc.p), pc.p);
+            return mul_shoup(sub_mod(u, v, pc.p), qi.x, qi.y, pc.p);
+        }
+        default:
+            return v;
     }
 }
 
@@ -154,37 +208,25 @@ __device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRe
 // mappings hit 16 distinct bank pairs.
 __device__ __forceinline__ int padi(int r) { return r + (r >> 4); }
 
-template <int LR, int LC, int STORE>
-__global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows(const __grid_constant__ DevCtx ctx,
-                                                         const __grid_constant__ LimbMap map) {
-    constexpr int R = 1 << LR, C = 1 << LC;
-    constexpr int CP = C + C / 16;  // padded row stride
-    constexpr int TPL = 1 << (LC - 4);
-    constexpr int TR = (256 / TPL) < R ? (256 / TPL) : R;
-    constexpr int NT = TPL * TR;
+template <int LR, int LC, int MINB, bool PF>
+__global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constant__ DevCtx ctx,
+                                                            const __grid_constant__ LimbMap map) {
+    using G = Geo<LR, LC>;
+    constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     __shared__ __align__(16) uint64_t sm[TR * CP];
 
     const LimbRef lr = resolve_limb(map, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const uint64_t* twg = ctx.fwd_tw + (size_t)lr.prime * 2 * ctx.N;
+    auto tab = [&](size_t i) { return ldg2(twg, i); };
 
-    const int th = threadIdx.x % TPL, rl = threadIdx.x / TPL;
+    const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int row = blockIdx.x * TR + rl;
     const uint64_t* src = lr.out + (size_t)row * C;
     uint64_t x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
-
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const int kb = 3 - t;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            if (k & (1 << kb)) continue;
-            const int r = th + (k << (LC - 4));
-            ct_bfly(x[k], x[k | (1 << kb)], ldg2(twg, ((size_t)(R + row) << t) + (r >> (LC - t))), pc.p, pc.two_p);
-        }
-    }
+    run_group<3, 0, PF, true>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
 #pragma unroll
@@ -192,17 +234,7 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows(const __grid_constant__
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-#pragma unroll
-        for (int t = 4; t < LC; ++t) {
-            const int kb = LC - 1 - t;
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                if (k & (1 << kb)) continue;
-                const int r = (th << 4) + k;
-                ct_bfly(x[k], x[k | (1 << kb)], ldg2(twg, ((size_t)(R + row) << t) + (r >> (LC - t))), pc.p,
-                        pc.two_p);
-            }
-        }
+        run_group<LC - 5, 0, PF, true>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
         // each thread rewrites exactly the slots it read
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
@@ -214,10 +246,10 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows(const __grid_constant__
     const size_t base = (size_t)blockIdx.x * TR * C;
 #pragma unroll 4
     for (int i = threadIdx.x * 2; i < TR * C; i += NT * 2) {
-        const int w = (i / C) * CP + padi(i % C);
+        const int wi = (i / C) * CP + padi(i % C);
         ulonglong2 o;
-        o.x = fwd_epilogue<STORE>(ctx, lr, pc, base + i, sm[w]);
-        o.y = fwd_epilogue<STORE>(ctx, lr, pc, base + i + 1, sm[w + 1]);
+        o.x = fwd_epilogue(ctx, lr, pc, base + i, sm[wi]);
+        o.y = fwd_epilogue(ctx, lr, pc, base + i + 1, sm[wi + 1]);
         *reinterpret_cast<ulonglong2*>(lr.out + base + i) = o;
     }
 }
@@ -225,76 +257,56 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows(const __grid_constant__
 // ---------------------------------------------------------------------------
 // inverse, pass A: row stages logN-1..LR (GS), with fused prologue
 // ---------------------------------------------------------------------------
-template <int LOAD>
 __device__ __forceinline__ uint64_t inv_prologue(const DevCtx& ctx, const LimbRef& lr, const PrimeConst& pc,
                                                  size_t g) {
-    if constexpr (LOAD == IL_PLAIN) {
-        return lr.in[g];
-    } else if constexpr (LOAD == IL_MUL) {
-        return mul_mod(lr.in[g], lr.in2[g], pc);
-    } else {  // IL_AXPY_PINV: in + in2 * P^-1
-        const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
-        return add_mod(lr.in[g], mul_shoup(lr.in2[g], pinv.x, pinv.y, pc.p), pc.p);
+    switch (lr.lmode) {
+        case IL_MUL:
+            return mul_mod(lr.in[g], lr.in2[g], pc);
+        case IL_AXPY_PINV: {  // in + in2 * P^-1
+            const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
+            return add_mod(lr.in[g], mul_shoup(lr.in2[g], pinv.x, pinv.y, pc.p), pc.p);
+        }
+        default:
+            return lr.in[g];
     }
 }
 
-template <int LR, int LC, int LOAD>
-__global__ void __launch_bounds__(256, 2) k_ntt_inv_rows(const __grid_constant__ DevCtx ctx,
-                                                         const __grid_constant__ LimbMap map) {
-    constexpr int R = 1 << LR, C = 1 << LC;
-    constexpr int CP = C + C / 16;
-    constexpr int TPL = 1 << (LC - 4);
-    constexpr int TR = (256 / TPL) < R ? (256 / TPL) : R;
-    constexpr int NT = TPL * TR;
+template <int LR, int LC, int MINB, bool PF>
+__global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constant__ DevCtx ctx,
+                                                            const __grid_constant__ LimbMap map) {
+    using G = Geo<LR, LC>;
+    constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     __shared__ __align__(16) uint64_t sm[TR * CP];
 
     const LimbRef lr = resolve_limb(map, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const uint64_t* twg = ctx.inv_tw + (size_t)lr.prime * 2 * ctx.N;
+    auto tab = [&](size_t i) { return ldg2(twg, i); };
 
+    const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int row = blockIdx.x * TR + rl;
     const size_t base = (size_t)blockIdx.x * TR * C;
 #pragma unroll 4
     for (int i = threadIdx.x * 2; i < TR * C; i += NT * 2) {
-        const int w = (i / C) * CP + padi(i % C);
-        sm[w] = inv_prologue<LOAD>(ctx, lr, pc, base + i);
-        sm[w + 1] = inv_prologue<LOAD>(ctx, lr, pc, base + i + 1);
+        const int wi = (i / C) * CP + padi(i % C);
+        sm[wi] = inv_prologue(ctx, lr, pc, base + i);
+        sm[wi + 1] = inv_prologue(ctx, lr, pc, base + i + 1);
     }
     __syncthreads();
 
-    const int th = threadIdx.x % TPL, rl = threadIdx.x / TPL;
-    const int row = blockIdx.x * TR + rl;
     uint64_t* srow = sm + rl * CP;
     uint64_t x[16];
     if constexpr (LC > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-#pragma unroll
-        for (int t = LC - 1; t >= 4; --t) {
-            const int kb = LC - 1 - t;
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                if (k & (1 << kb)) continue;
-                const int r = (th << 4) + k;
-                gs_bfly(x[k], x[k | (1 << kb)], ldg2(twg, ((size_t)(R + row) << t) + (r >> (LC - t))), pc.p,
-                        pc.two_p);
-            }
-        }
+        run_group<0, LC - 5, PF, false>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
         __syncthreads();
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = srow[padi(th + (k << (LC - 4)))];
-#pragma unroll
-    for (int t = 3; t >= 0; --t) {
-        const int kb = 3 - t;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            if (k & (1 << kb)) continue;
-            const int r = th + (k << (LC - 4));
-            gs_bfly(x[k], x[k | (1 << kb)], ldg2(twg, ((size_t)(R + row) << t) + (r >> (LC - t))), pc.p, pc.two_p);
-        }
-    }
+    run_group<0, 3, PF, false>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
     uint64_t* dst = lr.out + (size_t)row * C;
 #pragma unroll
     for (int k = 0; k < 16; ++k) dst[th + (k << (LC - 4))] = x[k];
@@ -303,33 +315,29 @@ __global__ void __launch_bounds__(256, 2) k_ntt_inv_rows(const __grid_constant__
 // ---------------------------------------------------------------------------
 // inverse, pass B: column stages LR-1..0 (GS), N^-1 and CRT scale folded in
 // ---------------------------------------------------------------------------
-template <int STORE>
 __device__ __forceinline__ const uint64_t* inv_scale_entry(const DevCtx& ctx, const LimbRef& lr) {
-    if constexpr (STORE == IS_PLAIN) {
-        return ctx.intt_scale + (size_t)lr.prime * 4;
-    } else if constexpr (STORE == IS_MODUP) {
-        return ctx.modup_scale + ((size_t)lr.level * ctx.L + lr.prime) * 4;
-    } else {  // IS_MODDOWN
-        return ctx.md_scale + (size_t)(lr.prime - ctx.L) * 4;
+    switch (lr.smode) {
+        case IS_MODUP: return ctx.modup_scale + ((size_t)lr.level * ctx.L + lr.prime) * 4;
+        case IS_MODDOWN: return ctx.md_scale + (size_t)(lr.prime - ctx.L) * 4;
+        default: return ctx.intt_scale + (size_t)lr.prime * 4;
     }
 }
 
-template <int LR, int LC, int STORE>
-__global__ void __launch_bounds__(256, 2) k_ntt_inv_cols(const __grid_constant__ DevCtx ctx,
-                                                         const __grid_constant__ LimbMap map) {
-    constexpr int R = 1 << LR, C = 1 << LC;
-    constexpr int TPL = 1 << (LR - 4);
-    constexpr int TC = (256 / TPL) < C ? (256 / TPL) : C;
-    constexpr int NT = TPL * TC;
-    __shared__ __align__(16) uint64_t sm[R * TC];
-    __shared__ ulonglong2 tw[R];
+template <int LR, int LC, int MINB, bool PF>
+__global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constant__ DevCtx ctx,
+                                                            const __grid_constant__ LimbMap map) {
+    using G = Geo<LR, LC>;
+    constexpr int C = G::C, TC = G::TC;
+    __shared__ __align__(16) uint64_t sm[G::R * TC];
+    __shared__ ulonglong2 tws[G::R];
 
     const LimbRef lr = resolve_limb(map, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const ulonglong2* twg = reinterpret_cast<const ulonglong2*>(ctx.inv_tw) + (size_t)lr.prime * ctx.N;
-    for (int i = threadIdx.x; i < R; i += NT) tw[i] = twg[i];
-    const uint64_t* se = inv_scale_entry<STORE>(ctx, lr);
+    for (int i = threadIdx.x; i < G::R; i += G::NTC) tws[i] = twg[i];
+    const uint64_t* se = inv_scale_entry(ctx, lr);
     const ulonglong2 s0 = ldg2(se, 0), s1 = ldg2(se, 1);
+    auto tab = [&](size_t i) { return tws[i]; };
 
     const int c = threadIdx.x % TC, th = threadIdx.x / TC;
     const int col = blockIdx.x * TC + c;
@@ -338,16 +346,7 @@ __global__ void __launch_bounds__(256, 2) k_ntt_inv_cols(const __grid_constant__
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = lr.out[(size_t)((th << 4) + k) * C + col];
         __syncthreads();
-#pragma unroll
-        for (int t = LR - 1; t >= 4; --t) {
-            const int kb = LR - 1 - t;
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                if (k & (1 << kb)) continue;
-                const int r = (th << 4) + k;
-                gs_bfly(x[k], x[k | (1 << kb)], tw[(1 << t) + (r >> (LR - t))], pc.p, pc.two_p);
-            }
-        }
+        run_group<0, LR - 5, PF, false>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
 #pragma unroll
         for (int k = 0; k < 16; ++k) sm[((th << 4) + k) * TC + c] = x[k];
         __syncthreads();
@@ -358,16 +357,7 @@ __global__ void __launch_bounds__(256, 2) k_ntt_inv_cols(const __grid_constant__
         for (int k = 0; k < 16; ++k) x[k] = lr.out[(size_t)(th + k) * C + col];
         __syncthreads();
     }
-#pragma unroll
-    for (int t = 3; t >= 1; --t) {
-        const int kb = 3 - t;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            if (k & (1 << kb)) continue;
-            const int r = th + (k << (LR - 4));
-            gs_bfly(x[k], x[k | (1 << kb)], tw[(1 << t) + (r >> (LR - t))], pc.p, pc.two_p);
-        }
-    }
+    run_group<0, 2, PF, false>(x, tab, 3, 1, 0, pc.p, pc.two_p);
     // last stage (twiddle index 1) with the N^-1 * scale fold
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -380,84 +370,87 @@ __global__ void __launch_bounds__(256, 2) k_ntt_inv_cols(const __grid_constant__
 }
 
 // ---------------------------------------------------------------------------
-// host launchers
+// host launchers and variant dispatch
 // ---------------------------------------------------------------------------
-template <int LR, int LC>
-static void launch_fwd(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st) {
-    constexpr int R = 1 << LR, C = 1 << LC;
-    constexpr int TC = (256 >> (LR - 4)) < C ? (256 >> (LR - 4)) : C;
-    constexpr int TR = (256 >> (LC - 4)) < R ? (256 >> (LC - 4)) : R;
-    dim3 g1(C / TC, map.total), g2(R / TR, map.total);
-    const int nt1 = (1 << (LR - 4)) * TC, nt2 = (1 << (LC - 4)) * TR;
-    if (load == FL_SWITCHMOD)
-        k_ntt_fwd_cols<LR, LC, FL_SWITCHMOD><<<g1, nt1, 0, st>>>(ctx, map);
-    else
-        k_ntt_fwd_cols<LR, LC, FL_PLAIN><<<g1, nt1, 0, st>>>(ctx, map);
-    switch (store) {
-        case FS_MODDOWN: k_ntt_fwd_rows<LR, LC, FS_MODDOWN><<<g2, nt2, 0, st>>>(ctx, map); break;
-        case FS_RESCALE: k_ntt_fwd_rows<LR, LC, FS_RESCALE><<<g2, nt2, 0, st>>>(ctx, map); break;
-        case FS_MDRS: k_ntt_fwd_rows<LR, LC, FS_MDRS><<<g2, nt2, 0, st>>>(ctx, map); break;
-        default: k_ntt_fwd_rows<LR, LC, FS_PLAIN><<<g2, nt2, 0, st>>>(ctx, map); break;
-    }
-}
-
-template <int LR, int LC>
-static void launch_inv(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st) {
-    constexpr int R = 1 << LR, C = 1 << LC;
-    constexpr int TC = (256 >> (LR - 4)) < C ? (256 >> (LR - 4)) : C;
-    constexpr int TR = (256 >> (LC - 4)) < R ? (256 >> (LC - 4)) : R;
-    dim3 g1(C / TC, map.total), g2(R / TR, map.total);
-    const int nt1 = (1 << (LR - 4)) * TC, nt2 = (1 << (LC - 4)) * TR;
-    switch (load) {
-        case IL_MUL: k_ntt_inv_rows<LR, LC, IL_MUL><<<g2, nt2, 0, st>>>(ctx, map); break;
-        case IL_AXPY_PINV: k_ntt_inv_rows<LR, LC, IL_AXPY_PINV><<<g2, nt2, 0, st>>>(ctx, map); break;
-        default: k_ntt_inv_rows<LR, LC, IL_PLAIN><<<g2, nt2, 0, st>>>(ctx, map); break;
-    }
-    switch (store) {
-        case IS_MODUP: k_ntt_inv_cols<LR, LC, IS_MODUP><<<g1, nt1, 0, st>>>(ctx, map); break;
-        case IS_MODDOWN: k_ntt_inv_cols<LR, LC, IS_MODDOWN><<<g1, nt1, 0, st>>>(ctx, map); break;
-        default: k_ntt_inv_cols<LR, LC, IS_PLAIN><<<g1, nt1, 0, st>>>(ctx, map); break;
-    }
-}
-
 static std::atomic<uint64_t> g_launches{0};
 uint64_t launch_count() { return g_launches.load(); }
 void count_launches(int n) { g_launches.fetch_add((uint64_t)n); }
 
 bool ntt_supported(int logN) { return logN >= 8 && logN <= 16; }
 
-void ntt_forward(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st) {
-    if (map.total <= 0) return;
-    count_launches(2);
-    switch (ctx.logN) {
-        case 8: launch_fwd<4, 4>(ctx, map, load, store, st); break;
-        case 9: launch_fwd<4, 5>(ctx, map, load, store, st); break;
-        case 10: launch_fwd<5, 5>(ctx, map, load, store, st); break;
-        case 11: launch_fwd<5, 6>(ctx, map, load, store, st); break;
-        case 12: launch_fwd<6, 6>(ctx, map, load, store, st); break;
-        case 13: launch_fwd<6, 7>(ctx, map, load, store, st); break;
-        case 14: launch_fwd<7, 7>(ctx, map, load, store, st); break;
-        case 15: launch_fwd<7, 8>(ctx, map, load, store, st); break;
-        case 16: launch_fwd<8, 8>(ctx, map, load, store, st); break;
-        default: break;
+// Variants: (min CTAs per SM, twiddle policy).  0: (2, group prefetch),
+// 1: (3, per-stage), 2: (4, per-stage).
+int ntt_num_variants() { return 3; }
+
+template <int LR, int LC, int MINB, bool PF>
+static void launch_fwd_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
+    using G = Geo<LR, LC>;
+    dim3 g1(G::C / G::TC, map.total), g2(G::R / G::TR, map.total);
+    k_ntt_fwd_cols<LR, LC, MINB, PF><<<g1, G::NTC, 0, st>>>(ctx, map);
+    k_ntt_fwd_rows<LR, LC, MINB, PF><<<g2, G::NTR, 0, st>>>(ctx, map);
+}
+
+template <int LR, int LC, int MINB, bool PF>
+static void launch_inv_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
+    using G = Geo<LR, LC>;
+    dim3 g1(G::C / G::TC, map.total), g2(G::R / G::TR, map.total);
+    k_ntt_inv_rows<LR, LC, MINB, PF><<<g2, G::NTR, 0, st>>>(ctx, map);
+    k_ntt_inv_cols<LR, LC, MINB, PF><<<g1, G::NTC, 0, st>>>(ctx, map);
+}
+
+template <int LR, int LC>
+static void launch_fwd(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
+    switch (ctx.ntt_variant) {
+        case 1: launch_fwd_v<LR, LC, 3, false>(ctx, map, st); break;
+        case 2: launch_fwd_v<LR, LC, 4, false>(ctx, map, st); break;
+        default: launch_fwd_v<LR, LC, 2, true>(ctx, map, st); break;
     }
 }
 
-void ntt_inverse(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st) {
-    if (map.total <= 0) return;
-    count_launches(2);
-    switch (ctx.logN) {
-        case 8: launch_inv<4, 4>(ctx, map, load, store, st); break;
-        case 9: launch_inv<4, 5>(ctx, map, load, store, st); break;
-        case 10: launch_inv<5, 5>(ctx, map, load, store, st); break;
-        case 11: launch_inv<5, 6>(ctx, map, load, store, st); break;
-        case 12: launch_inv<6, 6>(ctx, map, load, store, st); break;
-        case 13: launch_inv<6, 7>(ctx, map, load, store, st); break;
-        case 14: launch_inv<7, 7>(ctx, map, load, store, st); break;
-        case 15: launch_inv<7, 8>(ctx, map, load, store, st); break;
-        case 16: launch_inv<8, 8>(ctx, map, load, store, st); break;
-        default: break;
+template <int LR, int LC>
+static void launch_inv(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
+    switch (ctx.ntt_variant) {
+        case 1: launch_inv_v<LR, LC, 3, false>(ctx, map, st); break;
+        case 2: launch_inv_v<LR, LC, 4, false>(ctx, map, st); break;
+        default: launch_inv_v<LR, LC, 2, true>(ctx, map, st); break;
     }
+}
+
+#define FIDES_NTT_DISPATCH(FN)                        \
+    switch (ctx.logN) {                               \
+        case 8: FN<4, 4>(ctx, map, st); break;        \
+        case 9: FN<4, 5>(ctx, map, st); break;        \
+        case 10: FN<5, 5>(ctx, map, st); break;       \
+        case 11: FN<5, 6>(ctx, map, st); break;       \
+        case 12: FN<6, 6>(ctx, map, st); break;       \
+        case 13: FN<6, 7>(ctx, map, st); break;       \
+        case 14: FN<7, 7>(ctx, map, st); break;       \
+        case 15: FN<7, 8>(ctx, map, st); break;       \
+        case 16: FN<8, 8>(ctx, map, st); break;       \
+        default: return;                              \
+    }
+
+void set_modes(LimbMap& map, int lmode, int smode) {
+    for (int s = 0; s < map.nseg; ++s) {
+        if (lmode >= 0) map.seg[s].lmode = (int8_t)lmode;
+        if (smode >= 0) map.seg[s].smode = (int8_t)smode;
+    }
+}
+
+void ntt_forward(const DevCtx& ctx, const LimbMap& m, int load, int store, cudaStream_t st) {
+    if (m.total <= 0) return;
+    LimbMap map = m;
+    set_modes(map, load, store);
+    count_launches(2);
+    FIDES_NTT_DISPATCH(launch_fwd)
+}
+
+void ntt_inverse(const DevCtx& ctx, const LimbMap& m, int load, int store, cudaStream_t st) {
+    if (m.total <= 0) return;
+    LimbMap map = m;
+    set_modes(map, load, store);
+    count_launches(2);
+    FIDES_NTT_DISPATCH(launch_inv)
 }
 
 }  // namespace fides
