@@ -40,6 +40,7 @@ typedef struct fides_ctx fides_ctx;
 typedef struct fides_ct fides_ct; /* device-resident ciphertext */
 typedef struct fides_pt fides_pt; /* device-resident plaintext  */
 typedef struct fides_sk fides_sk; /* secret key (client side)   */
+typedef struct fides_pk fides_pk; /* public key (client side)   */
 
 typedef struct {
     int log_n;            /* ring dimension N = 2^log_n, 8 <= log_n <= 16 */
@@ -161,6 +162,12 @@ fides_status fides_polymul(fides_ctx* ctx, const uint64_t* a, const uint64_t* b,
 /* Secret key with `hamming_weight` nonzero ternary coefficients (0 = uniform ternary). */
 fides_status fides_keygen(fides_ctx* ctx, uint64_t seed, int hamming_weight, fides_sk** out);
 fides_status fides_sk_free(fides_ctx* ctx, fides_sk* sk);
+/* Public key (b = -a s + e, a) over the ciphertext moduli (KeyGen's publicKey). */
+fides_status fides_keygen_public(fides_ctx* ctx, const fides_sk* sk, uint64_t seed, fides_pk** out);
+fides_status fides_pk_free(fides_ctx* ctx, fides_pk* pk);
+/* Public-key encryption: c = (v b + e0 + m, v a + e1), v uniform ternary. */
+fides_status fides_encrypt_pk(fides_ctx* ctx, const fides_pk* pk, const double* values, int slots, int level,
+                              double scale, uint64_t seed, fides_ct** out);
 /* Generate and upload the relinearisation key (EvalMultKeyGen). */
 fides_status fides_keygen_relin(fides_ctx* ctx, const fides_sk* sk, uint64_t seed);
 /* Generate and upload rotation keys for the given slot indices (EvalRotateKeyGen). */

@@ -84,6 +84,9 @@ EXPORTS = {
     "fides_polymul": ([vp, vp, vp, vp, vp, vp, C.c_int, C.c_int], C.c_int),
     "fides_keygen": ([vp, u64, C.c_int, C.POINTER(vp)], C.c_int),
     "fides_sk_free": ([vp, vp], C.c_int),
+    "fides_keygen_public": ([vp, vp, u64, C.POINTER(vp)], C.c_int),
+    "fides_pk_free": ([vp, vp], C.c_int),
+    "fides_encrypt_pk": ([vp, vp, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_double, u64, C.POINTER(vp)], C.c_int),
     "fides_keygen_relin": ([vp, vp, u64], C.c_int),
     "fides_keygen_rotations": ([vp, vp, C.c_int, i32p, C.c_int, u64], C.c_int),
     "fides_keygen_conjugate": ([vp, vp, u64], C.c_int),

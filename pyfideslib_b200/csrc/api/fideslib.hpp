@@ -1,0 +1,429 @@
+// fideslib.hpp -- C++ mirror of FIDESlib's public API (api/fideslib.hpp) over
+// the C ABI in include/fides_b200.h.  Header-only; link libfidesb200.so.
+//
+// The names, argument meanings and ownership follow the reference surface
+// (api/CryptoContext.hpp:24-245, api/Ciphertext.hpp:13-56,
+// api/Plaintext.hpp:15-58, api/CCParams.hpp, api/Definitions.hpp):
+//   * CryptoContext / Ciphertext / Plaintext are shared_ptr handles; the
+//     device objects live behind C-ABI handles owned by the context.
+//   * Operations return new ciphertexts; the *InPlace variants overwrite.
+//   * Errors throw fideslib::Exception (the reference throws OPENFHE_THROW at
+//     the API; its CUDA errors exit, ours come back as a status).
+// The client-side operations (KeyGen, Encrypt, Decrypt, encoding) that the
+// reference delegates to OpenFHE are served by the library's own client half.
+// Scaling: FIXEDMANUAL (explicit Rescale) and FLEXIBLEAUTO / FIXEDAUTO (inputs
+// of degree 2 are rescaled before the next multiplication; levels aligned
+// before additions), as Ciphertext.cpp:409-423 / adjustForMult does.
+#pragma once
+#include <complex>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../../include/fides_b200.h"
+
+namespace fideslib {
+
+class Exception : public std::runtime_error {
+  public:
+    Exception(fides_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+    fides_status status;
+};
+
+enum ScalingTechnique { FIXEDMANUAL = 0, FIXEDAUTO, FLEXIBLEAUTO, FLEXIBLEAUTOEXT, NORESCALE };
+enum KeySwitchTechnique { INVALID_KS_TECH = 0, BV, HYBRID };
+enum SecretKeyDist { GAUSSIAN = 0, UNIFORM_TERNARY = 1, SPARSE_TERNARY = 2 };
+enum PKESchemeFeature { PKE = 0x01, KEYSWITCH = 0x02, LEVELEDSHE = 0x08, ADVANCEDSHE = 0x10, FHE = 0x40 };
+struct DCRTPoly {};
+struct CryptoContextCKKSRNS {};
+
+template <typename T>
+class CCParams;
+
+template <>
+class CCParams<CryptoContextCKKSRNS> {
+  public:
+    void SetMultiplicativeDepth(uint32_t d) { depth = d; }
+    void SetScalingModSize(uint32_t s) { scaleBits = s; }
+    void SetFirstModSize(uint32_t s) { firstBits = s; }
+    void SetBatchSize(uint32_t b) { batch = b; }
+    void SetRingDim(uint32_t n) { ringDim = n; }
+    void SetScalingTechnique(ScalingTechnique t) { tech = t; }
+    void SetNumLargeDigits(uint32_t d) { dnum = d; }
+    void SetKeySwitchTechnique(KeySwitchTechnique) {}
+    void SetSecretKeyDist(SecretKeyDist d) { keyDist = d; }
+    void SetSecretKeyHammingWeight(uint32_t h) { hamming = h; }
+    void SetDevices(std::vector<int>&& d) { devices = std::move(d); }
+    uint32_t GetMultiplicativeDepth() const { return depth; }
+    uint32_t GetBatchSize() const { return batch; }
+    SecretKeyDist GetSecretKeyDist() const { return keyDist; }
+
+    uint32_t depth = 1, scaleBits = 50, firstBits = 60, batch = 0, ringDim = 1 << 16, dnum = 3, hamming = 192;
+    ScalingTechnique tech = FLEXIBLEAUTO;
+    SecretKeyDist keyDist = UNIFORM_TERNARY;
+    std::vector<int> devices = {0};
+};
+
+inline void check(fides_status s, const fides_ctx* c = nullptr) {
+    if (s != FIDES_OK) throw Exception(s, std::string("fides status ") + std::to_string((int)s) + ": " +
+                                              (c ? fides_ctx_last_error(c) : ""));
+}
+
+template <typename T>
+class CryptoContextImpl;
+
+class CiphertextImpl {
+  public:
+    CiphertextImpl(fides_ctx* c, fides_ct* h) : ctx(c), handle(h) {}
+    ~CiphertextImpl() {
+        if (handle) fides_ct_free(ctx, handle);
+    }
+    CiphertextImpl(const CiphertextImpl&) = delete;
+    CiphertextImpl& operator=(const CiphertextImpl&) = delete;
+    uint32_t GetLevel() const {
+        int l = 0;
+        fides_ct_info(handle, &l, nullptr, nullptr, nullptr);
+        return (uint32_t)l;
+    }
+    size_t GetNoiseScaleDeg() const {
+        int d = 0;
+        fides_ct_info(handle, nullptr, nullptr, &d, nullptr);
+        return (size_t)d;
+    }
+    double GetScalingFactor() const {
+        double s = 0;
+        fides_ct_info(handle, nullptr, &s, nullptr, nullptr);
+        return s;
+    }
+    uint32_t GetSlots() const {
+        int s = 0;
+        fides_ct_info(handle, nullptr, nullptr, nullptr, &s);
+        return (uint32_t)s;
+    }
+    fides_ctx* ctx;
+    fides_ct* handle;
+};
+template <typename T = DCRTPoly>
+using Ciphertext = std::shared_ptr<CiphertextImpl>;
+
+class PlaintextImpl {
+  public:
+    PlaintextImpl(fides_ctx* c, fides_pt* h, uint32_t s) : ctx(c), handle(h), slots(s) {}
+    ~PlaintextImpl() {
+        if (handle) fides_pt_free(ctx, handle);
+    }
+    void SetLength(size_t n) { length = n; }
+    void SetSlots(uint32_t s) { slots = s; }
+    std::vector<std::complex<double>> GetCKKSPackedValue() const {
+        return std::vector<std::complex<double>>(values.begin(), values.begin() + std::min(length, values.size()));
+    }
+    std::vector<double> GetRealPackedValue() const {
+        std::vector<double> r;
+        for (size_t i = 0; i < std::min(length, values.size()); ++i) r.push_back(values[i].real());
+        return r;
+    }
+    fides_ctx* ctx;
+    fides_pt* handle;
+    uint32_t slots;
+    size_t length = 0;
+    std::vector<std::complex<double>> values;
+};
+using Plaintext = std::shared_ptr<PlaintextImpl>;
+
+template <typename T>
+struct PrivateKeyImpl {
+    fides_ctx* ctx = nullptr;
+    fides_sk* handle = nullptr;
+    ~PrivateKeyImpl() {
+        if (handle) fides_sk_free(ctx, handle);
+    }
+};
+template <typename T>
+using PrivateKey = std::shared_ptr<PrivateKeyImpl<T>>;
+template <typename T>
+struct PublicKeyImpl {
+    fides_ctx* ctx = nullptr;
+    fides_pk* handle = nullptr;
+    ~PublicKeyImpl() {
+        if (handle) fides_pk_free(ctx, handle);
+    }
+};
+template <typename T>
+using PublicKey = std::shared_ptr<PublicKeyImpl<T>>;
+template <typename T>
+struct KeyPair {
+    PublicKey<T> publicKey;
+    PrivateKey<T> secretKey;
+};
+using DecryptResult = bool;
+
+template <>
+class CryptoContextImpl<DCRTPoly> {
+  public:
+    explicit CryptoContextImpl(const CCParams<CryptoContextCKKSRNS>& p) : tech(p.tech), hamming(p.hamming) {
+        fides_params prm{};
+        prm.log_n = 0;
+        for (uint32_t n = p.ringDim; n > 1; n >>= 1) ++prm.log_n;
+        prm.num_q = (int)p.depth + 1;
+        prm.dnum = (int)p.dnum;
+        prm.q0_bits = (int)p.firstBits;
+        prm.qi_bits = (int)p.scaleBits;
+        prm.p_bits = 60;
+        prm.device = p.devices.empty() ? 0 : p.devices[0];
+        check(fides_ctx_create(&prm, &ctx));
+        slots = p.batch ? p.batch : (1u << prm.log_n) / 2;
+        sparse = p.keyDist == SPARSE_TERNARY;
+    }
+    ~CryptoContextImpl() {
+        if (ctx) fides_ctx_destroy(ctx);
+    }
+    CryptoContextImpl(const CryptoContextImpl&) = delete;
+
+    void Enable(PKESchemeFeature) {}
+    uint32_t GetRingDimension() const {
+        int l = 0;
+        fides_ctx_info(ctx, &l, nullptr, nullptr, nullptr, nullptr, nullptr);
+        return 1u << l;
+    }
+    uint32_t GetCyclotomicOrder() const { return 2 * GetRingDimension(); }
+
+    KeyPair<DCRTPoly> KeyGen() {
+        KeyPair<DCRTPoly> kp;
+        kp.secretKey = std::make_shared<PrivateKeyImpl<DCRTPoly>>();
+        kp.secretKey->ctx = ctx;
+        check(fides_keygen(ctx, seed++, sparse ? (int)hamming : 0, &kp.secretKey->handle), ctx);
+        kp.publicKey = std::make_shared<PublicKeyImpl<DCRTPoly>>();
+        kp.publicKey->ctx = ctx;
+        check(fides_keygen_public(ctx, kp.secretKey->handle, seed++, &kp.publicKey->handle), ctx);
+        return kp;
+    }
+    void EvalMultKeyGen(const PrivateKey<DCRTPoly>& sk) { check(fides_keygen_relin(ctx, sk->handle, seed++), ctx); }
+    void EvalRotateKeyGen(const PrivateKey<DCRTPoly>& sk, const std::vector<int32_t>& steps) {
+        check(fides_keygen_rotations(ctx, sk->handle, (int)steps.size(), steps.data(), (int)slots, seed++), ctx);
+    }
+    void EvalConjugateKeyGen(const PrivateKey<DCRTPoly>& sk) { check(fides_keygen_conjugate(ctx, sk->handle, seed++), ctx); }
+    void LoadContext(const PublicKey<DCRTPoly>&) {}
+
+    Plaintext MakeCKKSPackedPlaintext(const std::vector<std::complex<double>>& v, size_t noiseScaleDeg = 1,
+                                      uint32_t level = 0, std::shared_ptr<void> = nullptr, uint32_t nslots = 0) {
+        const uint32_t s = nslots ? nslots : slots;
+        int L = 0;
+        fides_ctx_info(ctx, nullptr, &L, nullptr, nullptr, nullptr, nullptr);
+        const int lv = L - 1 - (int)level;  // OpenFHE's level counts consumed levels
+        std::vector<double> iv(2 * s, 0.0);
+        for (size_t i = 0; i < v.size() && i < s; ++i) {
+            iv[2 * i] = v[i].real();
+            iv[2 * i + 1] = v[i].imag();
+        }
+        const double sc = scale_for(noiseScaleDeg);
+        std::vector<uint64_t> m((size_t)(lv + 1) * GetRingDimension());
+        check(fides_encode(ctx, iv.data(), (int)s, lv, sc, m.data()), ctx);
+        fides_pt* h = nullptr;
+        check(fides_pt_upload(ctx, m.data(), lv, sc, (int)noiseScaleDeg, (int)s, &h), ctx);
+        auto pt = std::make_shared<PlaintextImpl>(ctx, h, s);
+        pt->values = v;
+        pt->length = v.size();
+        return pt;
+    }
+    Plaintext MakeCKKSPackedPlaintext(const std::vector<double>& v, size_t noiseScaleDeg = 1, uint32_t level = 0,
+                                      std::shared_ptr<void> params = nullptr, uint32_t nslots = 0) {
+        std::vector<std::complex<double>> c(v.begin(), v.end());
+        return MakeCKKSPackedPlaintext(c, noiseScaleDeg, level, params, nslots);
+    }
+
+    Ciphertext<DCRTPoly> Encrypt(const PublicKey<DCRTPoly>& pk, Plaintext& pt) {
+        fides_ct* h = nullptr;
+        auto iv = interleave(pt);
+        check(fides_encrypt_pk(ctx, pk->handle, iv.data(), (int)pt->slots, top_level(), scale_for(1), seed++, &h), ctx);
+        return wrap(h);
+    }
+    Ciphertext<DCRTPoly> Encrypt(Plaintext& pt, const PublicKey<DCRTPoly>& pk) { return Encrypt(pk, pt); }
+    Ciphertext<DCRTPoly> Encrypt(const PrivateKey<DCRTPoly>& sk, Plaintext& pt) {
+        fides_ct* h = nullptr;
+        auto iv = interleave(pt);
+        check(fides_encrypt(ctx, sk->handle, iv.data(), (int)pt->slots, top_level(), scale_for(1), seed++, &h), ctx);
+        return wrap(h);
+    }
+    DecryptResult Decrypt(const PrivateKey<DCRTPoly>& sk, Ciphertext<DCRTPoly>& ct, Plaintext* out) {
+        const uint32_t s = ct->GetSlots() ? ct->GetSlots() : slots;
+        std::vector<double> v(2 * s);
+        check(fides_decrypt(ctx, sk->handle, ct->handle, v.data(), (int)s), ctx);
+        auto pt = std::make_shared<PlaintextImpl>(ctx, nullptr, s);
+        for (uint32_t i = 0; i < s; ++i) pt->values.emplace_back(v[2 * i], v[2 * i + 1]);
+        pt->length = s;
+        *out = pt;
+        return true;
+    }
+    DecryptResult Decrypt(Ciphertext<DCRTPoly>& ct, const PrivateKey<DCRTPoly>& sk, Plaintext* out) {
+        return Decrypt(sk, ct, out);
+    }
+
+    // ---- evaluation ----
+    Ciphertext<DCRTPoly> EvalAdd(const Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) {
+        auto x = match(a, b);
+        return op2(fides_add, x.first, x.second);
+    }
+    Ciphertext<DCRTPoly> EvalSub(const Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) {
+        auto x = match(a, b);
+        return op2(fides_sub, x.first, x.second);
+    }
+    Ciphertext<DCRTPoly> EvalAdd(const Ciphertext<DCRTPoly>& a, Plaintext& p) {
+        auto o = empty();
+        check(fides_add_pt(ctx, a->handle, p->handle, o->handle), ctx);
+        return o;
+    }
+    Ciphertext<DCRTPoly> EvalAdd(const Ciphertext<DCRTPoly>& a, double v) {
+        auto o = empty();
+        check(fides_add_scalar(ctx, a->handle, v, o->handle), ctx);
+        return o;
+    }
+    Ciphertext<DCRTPoly> EvalNegate(const Ciphertext<DCRTPoly>& a) {
+        auto o = empty();
+        check(fides_negate(ctx, a->handle, o->handle), ctx);
+        return o;
+    }
+    Ciphertext<DCRTPoly> EvalMult(const Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) {
+        auto x = align(prepare(a), prepare(b));
+        auto o = empty();
+        check(fides_hmult(ctx, x.first->handle, x.second->handle, o->handle, 0), ctx);
+        return o;
+    }
+    Ciphertext<DCRTPoly> EvalMult(const Ciphertext<DCRTPoly>& a, Plaintext& p) {
+        auto o = empty();
+        check(fides_mult_pt(ctx, prepare(a)->handle, p->handle, o->handle, 0), ctx);
+        return o;
+    }
+    Ciphertext<DCRTPoly> EvalMult(const Ciphertext<DCRTPoly>& a, double v) {
+        auto o = empty();
+        check(fides_mult_scalar(ctx, prepare(a)->handle, v, o->handle, 0), ctx);
+        return o;
+    }
+    Ciphertext<DCRTPoly> EvalSquare(const Ciphertext<DCRTPoly>& a) {
+        auto o = empty();
+        check(fides_square(ctx, prepare(a)->handle, o->handle, 0), ctx);
+        return o;
+    }
+    void EvalMultInPlace(Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) { a = EvalMult(a, b); }
+    void EvalAddInPlace(Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) { a = EvalAdd(a, b); }
+    Ciphertext<DCRTPoly> Rescale(const Ciphertext<DCRTPoly>& a) {
+        auto o = empty();
+        check(fides_rescale(ctx, a->handle, o->handle), ctx);
+        return o;
+    }
+    void RescaleInPlace(Ciphertext<DCRTPoly>& a) { a = Rescale(a); }
+    Ciphertext<DCRTPoly> EvalRotate(const Ciphertext<DCRTPoly>& a, int32_t index) {
+        auto o = empty();
+        check(fides_rotate(ctx, a->handle, index, o->handle), ctx);
+        return o;
+    }
+    void EvalRotateInPlace(Ciphertext<DCRTPoly>& a, int32_t index) { a = EvalRotate(a, index); }
+    // The hoisted ModUp happens inside EvalFastRotation; the precomputation
+    // handle is kept for signature compatibility (the reference returns
+    // nullptr on GPU too, api/CryptoContext.cpp:1360-1373).
+    std::shared_ptr<void> EvalFastRotationPrecompute(const Ciphertext<DCRTPoly>&) { return nullptr; }
+    Ciphertext<DCRTPoly> EvalFastRotation(const Ciphertext<DCRTPoly>& a, int32_t index, uint32_t,
+                                          const std::shared_ptr<void>&) {
+        return EvalRotate(a, index);
+    }
+    std::vector<Ciphertext<DCRTPoly>> EvalFastRotation(const Ciphertext<DCRTPoly>& a, const std::vector<int32_t>& idx,
+                                                       uint32_t, const std::shared_ptr<void>&) {
+        std::vector<Ciphertext<DCRTPoly>> outs;
+        std::vector<fides_ct*> hs;
+        for (size_t i = 0; i < idx.size(); ++i) {
+            outs.push_back(empty());
+            hs.push_back(outs.back()->handle);
+        }
+        check(fides_rotate_hoisted(ctx, a->handle, (int)idx.size(), idx.data(), hs.data()), ctx);
+        return outs;
+    }
+    Ciphertext<DCRTPoly> EvalConjugate(const Ciphertext<DCRTPoly>& a) {
+        auto o = empty();
+        check(fides_conjugate(ctx, a->handle, o->handle), ctx);
+        return o;
+    }
+    static void SetLevel(Ciphertext<DCRTPoly>& ct, size_t level) {
+        int L = 0;
+        fides_ctx_info(ct->ctx, nullptr, &L, nullptr, nullptr, nullptr, nullptr);
+        check(fides_ct_set_level(ct->ctx, ct->handle, L - 1 - (int)level), ct->ctx);
+    }
+    void Synchronize() const { check(fides_ctx_synchronize(ctx), ctx); }
+
+    fides_ctx* ctx = nullptr;
+
+  private:
+    ScalingTechnique tech;
+    uint32_t hamming;
+    uint32_t slots = 0;
+    bool sparse = false;
+    uint64_t seed = 0x5EEDull;
+
+    int top_level() const {
+        int L = 0;
+        fides_ctx_info(ctx, nullptr, &L, nullptr, nullptr, nullptr, nullptr);
+        return L - 1;
+    }
+    double scale_for(size_t deg) const {
+        const double base = 1125899906842624.0;  // 2^50, the context's default scale
+        double s = 1;
+        for (size_t i = 0; i < deg; ++i) s *= base;
+        return s;
+    }
+    std::vector<double> interleave(const Plaintext& pt) const {
+        std::vector<double> iv(2 * pt->slots, 0.0);
+        for (size_t i = 0; i < pt->values.size() && i < pt->slots; ++i) {
+            iv[2 * i] = pt->values[i].real();
+            iv[2 * i + 1] = pt->values[i].imag();
+        }
+        return iv;
+    }
+    Ciphertext<DCRTPoly> wrap(fides_ct* h) { return std::make_shared<CiphertextImpl>(ctx, h); }
+    Ciphertext<DCRTPoly> empty() {
+        fides_ct* h = nullptr;
+        check(fides_ct_create(ctx, &h), ctx);
+        return wrap(h);
+    }
+    Ciphertext<DCRTPoly> op2(fides_status (*f)(fides_ctx*, const fides_ct*, const fides_ct*, fides_ct*),
+                             const Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) {
+        auto o = empty();
+        check(f(ctx, a->handle, b->handle, o->handle), ctx);
+        return o;
+    }
+    // FLEXIBLEAUTO / FIXEDAUTO: rescale a degree-2 input before multiplying.
+    Ciphertext<DCRTPoly> prepare(const Ciphertext<DCRTPoly>& a) {
+        if (tech != FIXEDMANUAL && a->GetNoiseScaleDeg() >= 2) return Rescale(a);
+        return a;
+    }
+    // Automatic modes before an addition: bring both operands to the same
+    // noise degree (rescaling the degree-2 one) and the same level
+    // (adjustForAddOrSub, Ciphertext.cpp:177-230).
+    std::pair<Ciphertext<DCRTPoly>, Ciphertext<DCRTPoly>> match(Ciphertext<DCRTPoly> a, Ciphertext<DCRTPoly> b) {
+        if (tech != FIXEDMANUAL) {
+            if (a->GetNoiseScaleDeg() > b->GetNoiseScaleDeg()) a = Rescale(a);
+            if (b->GetNoiseScaleDeg() > a->GetNoiseScaleDeg()) b = Rescale(b);
+        }
+        return align(a, b);
+    }
+    // Drop the higher-level operand to the lower level (automatic modes).
+    std::pair<Ciphertext<DCRTPoly>, Ciphertext<DCRTPoly>> align(Ciphertext<DCRTPoly> a, Ciphertext<DCRTPoly> b) {
+        if (a->GetLevel() == b->GetLevel()) return {a, b};
+        auto& hi = a->GetLevel() > b->GetLevel() ? a : b;
+        const int target = (int)std::min(a->GetLevel(), b->GetLevel());
+        auto c = empty();
+        check(fides_ct_copy(ctx, hi->handle, c->handle), ctx);
+        check(fides_ct_set_level(ctx, c->handle, target), ctx);
+        hi = c;
+        return {a, b};
+    }
+};
+
+template <typename T = DCRTPoly>
+using CryptoContext = std::shared_ptr<CryptoContextImpl<DCRTPoly>>;
+
+inline CryptoContext<DCRTPoly> GenCryptoContext(const CCParams<CryptoContextCKKSRNS>& p) {
+    return std::make_shared<CryptoContextImpl<DCRTPoly>>(p);
+}
+
+}  // namespace fideslib

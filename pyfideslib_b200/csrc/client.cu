@@ -433,6 +433,115 @@ fides_status fides_encrypt(fides_ctx* c, const fides_sk* sk, const double* value
     return check_cuda(c, "encrypt");
 }
 
+fides_status fides_keygen_public(fides_ctx* c, const fides_sk* sk, uint64_t seed, fides_pk** out) {
+    if (!c || !sk || !sk->s || !out) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    const int N = c->N, L = c->L;
+    fides_pk* pk = new (std::nothrow) fides_pk();
+    if (!pk) return FIDES_OOM;
+    if (cudaMalloc((void**)&pk->b, 2 * (size_t)L * N * 8) != cudaSuccess) {
+        cudaGetLastError();
+        delete pk;
+        return set_err(c, FIDES_OOM, "public key");
+    }
+    pk->a = pk->b + (size_t)L * N;
+    uint64_t* e = nullptr;
+    if (cudaMallocAsync((void**)&e, (size_t)L * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "pk tmp");
+    count_launches(1);
+    k_fill_uniform<<<dim3(N / 256, L), 256, 0, c->st>>>(pk->a, N, 0, c->dev.pc, seed * 0x9E3779B97F4A7C15ull + 99);
+    fides_status s = upload_small(c, gaussian(N, seed ^ 0x7EA5), e, 0, L);
+    if (s == FIDES_OK) {
+        ntt_forward(c->dev, map_single(e, e, L, L, 0), FL_PLAIN, FS_PLAIN, c->st);
+        count_launches(1);
+        k_key_combine<<<dim3(N / 256, L), 256, 0, c->st>>>(pk->b, pk->a, sk->s, e, sk->s, c->dev.pc, c->dev.md_pmod, N,
+                                                           0, 0);
+        cudaStreamSynchronize(c->st);
+    }
+    cudaFreeAsync(e, c->st);
+    if (s != FIDES_OK) {
+        cudaFree(pk->b);
+        delete pk;
+        return s;
+    }
+    *out = pk;
+    return check_cuda(c, "public key");
+}
+
+fides_status fides_pk_free(fides_ctx* c, fides_pk* pk) {
+    if (!c || !pk) return FIDES_BAD_ARG;
+    cudaSetDevice(c->device);
+    if (pk->b) cudaFree(pk->b);
+    delete pk;
+    return FIDES_OK;
+}
+
+fides_status fides_encrypt_pk(fides_ctx* c, const fides_pk* pk, const double* values, int slots, int level,
+                              double scale, uint64_t seed, fides_ct** out) {
+    if (!c || !pk || !pk->b || !values || !out || slots < 1 || slots > c->N / 2 || (slots & (slots - 1)) ||
+        level < 0 || level >= c->L)
+        return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    if (scale <= 0) scale = c->default_scale;
+    const int n = level + 1, N = c->N, L = c->L;
+    fides_ct* ct = new (std::nothrow) fides_ct();
+    if (!ct) return FIDES_OOM;
+    fides_status s = ct_reserve(c, ct, level);
+    if (s != FIDES_OK) {
+        delete ct;
+        return s;
+    }
+    uint64_t* tmp = nullptr;  // m, v, e0, e1
+    if (cudaMallocAsync((void**)&tmp, 4 * (size_t)n * N * 8, c->st) != cudaSuccess) {
+        fides_ct_free(c, ct);
+        return set_err(c, FIDES_OOM, "encrypt tmp");
+    }
+    uint64_t *m = tmp, *v = tmp + (size_t)n * N, *e0 = tmp + 2 * (size_t)n * N, *e1 = tmp + 3 * (size_t)n * N;
+    s = encode_dev(c, values, slots, level, scale, m);
+    std::vector<int64_t> vt(N);
+    {
+        Xoshiro r(seed ^ 0xC0FFEE);
+        for (int i = 0; i < N; ++i) vt[i] = (int64_t)(r.next() % 3) - 1;
+    }
+    if (s == FIDES_OK) s = upload_small(c, vt, v, 0, n);
+    if (s == FIDES_OK) s = upload_small(c, gaussian(N, seed ^ 0xE0), e0, 0, n);
+    if (s == FIDES_OK) s = upload_small(c, gaussian(N, seed ^ 0xE1), e1, 0, n);
+    if (s == FIDES_OK) {
+        LimbMap mm{};
+        mm.nseg = 3;
+        uint64_t* bufs[3] = {v, e0, e1};
+        for (int i = 0; i < 3; ++i) {
+            LimbSeg& g = mm.seg[i];
+            g.in = g.out = bufs[i];
+            g.count = n;
+            g.skip_lo = n;
+            g.nq = n;
+            mm.total += n;
+        }
+        ntt_forward(c->dev, mm, FL_PLAIN, FS_PLAIN, c->st);
+        launch_elementwise(c->dev, EW_ADD, n, 0, e0, m, e0, c->st);
+        // c0 = v b + (e0 + m), c1 = v a + e1  (pk limbs 0..level)
+        launch_elementwise(c->dev, EW_MUL, n, 0, pk->b, v, ct->c0(), c->st);
+        launch_elementwise(c->dev, EW_ADD, n, 0, ct->c0(), e0, ct->c0(), c->st);
+        launch_elementwise(c->dev, EW_MUL, n, 0, pk->a, v, ct->c1(N), c->st);
+        launch_elementwise(c->dev, EW_ADD, n, 0, ct->c1(N), e1, ct->c1(N), c->st);
+        cudaStreamSynchronize(c->st);
+    }
+    (void)L;
+    cudaFreeAsync(tmp, c->st);
+    if (s != FIDES_OK) {
+        fides_ct_free(c, ct);
+        return s;
+    }
+    ct->level = level;
+    ct->scale = scale;
+    ct->noise_deg = 1;
+    ct->slots = slots;
+    *out = ct;
+    return check_cuda(c, "encrypt_pk");
+}
+
 fides_status fides_decrypt(fides_ctx* c, const fides_sk* sk, const fides_ct* ct, double* values, int slots) {
     if (!c || !sk || !sk->s || !ct || !ct->buf || !values || slots < 1 || slots > c->N / 2) return FIDES_BAD_ARG;
     std::lock_guard<std::recursive_mutex> lk(c->mu);

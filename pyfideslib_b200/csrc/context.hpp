@@ -39,6 +39,11 @@ struct fides_sk {
     uint64_t* s = nullptr;       // device, evaluation form over all L+K primes
 };
 
+struct fides_pk {
+    uint64_t* b = nullptr;  // device, evaluation form over the L ciphertext moduli
+    uint64_t* a = nullptr;
+};
+
 namespace fides {
 
 struct SwitchKey {

@@ -257,20 +257,8 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
 // ---------------------------------------------------------------------------
 // inverse, pass A: row stages logN-1..LR (GS), with fused prologue
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t inv_prologue(const DevCtx& ctx, const LimbRef& lr, const PrimeConst& pc,
-                                                 size_t g) {
-    switch (lr.lmode) {
-        case IL_MUL:
-            return mul_mod(lr.in[g], lr.in2[g], pc);
-        case IL_AXPY_PINV: {  // in + in2 * P^-1
-            const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
-            return add_mod(lr.in[g], mul_shoup(lr.in2[g], pinv.x, pinv.y, pc.p), pc.p);
-        }
-        default:
-            return lr.in[g];
-    }
-}
-
+// Prologue modes of the inverse row pass (per segment): IL_PLAIN reads `in`,
+// IL_MUL the product in*in2, IL_AXPY_PINV in + in2*P^-1.
 template <int LR, int LC, int MINB, bool PF>
 __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
@@ -285,17 +273,34 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
 
     const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int row = blockIdx.x * TR + rl;
+    // all 16 elements of the thread are loaded before any is used, so the
+    // 16 global loads (32 with a second operand) are in flight together
     const size_t base = (size_t)blockIdx.x * TR * C;
-#pragma unroll 4
-    for (int i = threadIdx.x * 2; i < TR * C; i += NT * 2) {
-        const int wi = (i / C) * CP + padi(i % C);
-        sm[wi] = inv_prologue(ctx, lr, pc, base + i);
-        sm[wi + 1] = inv_prologue(ctx, lr, pc, base + i + 1);
+    constexpr int PER = TR * C / NT;  // elements per thread (16)
+    static_assert(PER == 16, "row tile holds 16 elements per thread");
+    uint64_t x[16];
+    {
+        uint64_t v[16];
+#pragma unroll
+        for (int q = 0; q < PER; ++q) v[q] = lr.in[base + threadIdx.x + q * NT];
+        if (lr.lmode == IL_MUL) {
+#pragma unroll
+            for (int q = 0; q < PER; ++q) v[q] = mul_mod(v[q], lr.in2[base + threadIdx.x + q * NT], pc);
+        } else if (lr.lmode == IL_AXPY_PINV) {
+            const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
+#pragma unroll
+            for (int q = 0; q < PER; ++q)
+                v[q] = add_mod(v[q], mul_shoup(lr.in2[base + threadIdx.x + q * NT], pinv.x, pinv.y, pc.p), pc.p);
+        }
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int i = threadIdx.x + q * NT;
+            sm[(i / C) * CP + padi(i % C)] = v[q];
+        }
     }
     __syncthreads();
 
     uint64_t* srow = sm + rl * CP;
-    uint64_t x[16];
     if constexpr (LC > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
