@@ -157,6 +157,19 @@ fides_status fides_ntt(fides_ctx* ctx, uint64_t* data, int prime0, int nlimbs, i
 fides_status fides_polymul(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, uint64_t* c, uint64_t* a_ntt,
                            uint64_t* b_ntt, int prime0, int nlimbs);
 
+/* Same product as fides_polymul, but allocating nothing and asking for no
+ * scratch: for callers that cannot obtain device memory when they multiply
+ * (inside CUDA stream capture, under a host allocator that owns the device,
+ * in loops that must not call cudaMalloc/cudaFree).  No counterpart in the
+ * reference.  The scratch is a fixed 8 MiB device array inside the library
+ * (2^19 words per operand): nlimbs * N must not exceed 2^19, larger calls
+ * return FIDES_BAD_ARG.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and should precede any stream capture.  All calls
+ * share the array; calls that overlap on the GPU race and must be serialised
+ * by the caller.  `c` may alias a or b. */
+fides_status fides_polymul_noalloc(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, uint64_t* c, int prime0,
+                                   int nlimbs);
+
 /* ---- client side (OpenFHE's role in FIDESlib: KeyGen, Encrypt, Decrypt,
  *      MakeCKKSPackedPlaintext; api/CryptoContext.hpp:71-106) ---- */
 /* Secret key with `hamming_weight` nonzero ternary coefficients (0 = uniform ternary). */

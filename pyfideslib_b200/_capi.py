@@ -82,6 +82,7 @@ EXPORTS = {
     "fides_mult_scalar": ([vp, vp, C.c_double, vp, C.c_int], C.c_int),
     "fides_ntt": ([vp, vp, C.c_int, C.c_int, C.c_int], C.c_int),
     "fides_polymul": ([vp, vp, vp, vp, vp, vp, C.c_int, C.c_int], C.c_int),
+    "fides_polymul_noalloc": ([vp, vp, vp, vp, C.c_int, C.c_int], C.c_int),
     "fides_keygen": ([vp, u64, C.c_int, C.POINTER(vp)], C.c_int),
     "fides_sk_free": ([vp, vp], C.c_int),
     "fides_keygen_public": ([vp, vp, u64, C.POINTER(vp)], C.c_int),
