@@ -130,6 +130,16 @@ fides_status fides_rescale(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
 fides_status fides_rotate(fides_ctx* ctx, const fides_ct* a, int32_t index, fides_ct* out);
 /* EvalFastRotation (hoisted, one shared ModUp): Ciphertext::rotate_hoisted, Ciphertext.cpp:1053-1226 */
 fides_status fides_rotate_hoisted(fides_ctx* ctx, const fides_ct* a, int n, const int32_t* indices, fides_ct** outs);
+/* Batched EvalMult (+ Rescale) of n independent pairs (a[i], b[i]) -> out[i],
+ * levels may differ between pairs.  Pairs at one level share every launch,
+ * up to 32 per launch, so the relinearisation key is read once per batch
+ * from HBM (the reference's batched path is LimbPartitionBatch.cu:21-604).
+ * Results are identical to n calls of fides_hmult. */
+fides_status fides_hmult_batch(fides_ctx* ctx, int n, const fides_ct* const* a, const fides_ct* const* b,
+                               fides_ct* const* out, int rescale);
+/* Batched EvalRotate: out[i] = rotation of a[i] by indices[i] (own keys). */
+fides_status fides_rotate_batch(fides_ctx* ctx, int n, const fides_ct* const* a, const int32_t* indices,
+                                fides_ct* const* out);
 /* EvalConjugate: Ciphertext::conjugate, Ciphertext.cpp:933 */
 fides_status fides_conjugate(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
 /* Apply an automorphism whose key was uploaded with fides_key_upload_galois */

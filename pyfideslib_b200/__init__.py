@@ -235,6 +235,26 @@ class CryptoContext:
             check(lib.fides_hmult(self._h, a._h, b._h, out._h, int(rescale)), self._h)
         return out
 
+    def EvalMultBatch(self, a_list, b_list, rescale=False, outs=None):
+        """Batched HMult (+ rescale) of independent pairs; levels may differ."""
+        n = len(a_list)
+        outs = outs or [Ciphertext(self) for _ in range(n)]
+        A = (vp * n)(*[x._h for x in a_list])
+        B = (vp * n)(*[x._h for x in b_list])
+        O = (vp * n)(*[o._h for o in outs])
+        check(lib.fides_hmult_batch(self._h, n, A, B, O, int(rescale)), self._h)
+        return outs
+
+    def EvalRotateBatch(self, a_list, indices, outs=None):
+        """Rotation of each ciphertext by its own index (own keys)."""
+        n = len(a_list)
+        outs = outs or [Ciphertext(self) for _ in range(n)]
+        A = (vp * n)(*[x._h for x in a_list])
+        I = (C.c_int32 * n)(*indices)
+        O = (vp * n)(*[o._h for o in outs])
+        check(lib.fides_rotate_batch(self._h, n, A, I, O), self._h)
+        return outs
+
     def EvalSquare(self, a, rescale=False, out=None):
         out = self._out(out)
         check(lib.fides_square(self._h, a._h, out._h, int(rescale)), self._h)

@@ -72,6 +72,8 @@ EXPORTS = {
     "fides_rotate": ([vp, vp, C.c_int32, vp], C.c_int),
     "fides_rotate_hoisted": ([vp, vp, C.c_int, i32p, C.POINTER(vp)], C.c_int),
     "fides_conjugate": ([vp, vp, vp], C.c_int),
+    "fides_hmult_batch": ([vp, C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_int], C.c_int),
+    "fides_rotate_batch": ([vp, C.c_int, C.POINTER(vp), i32p, C.POINTER(vp)], C.c_int),
     "fides_automorphism": ([vp, vp, C.c_uint32, vp], C.c_int),
     "fides_add": ([vp, vp, vp, vp], C.c_int),
     "fides_sub": ([vp, vp, vp, vp], C.c_int),

@@ -29,123 +29,6 @@ void commit(fides_ctx* c, fides_ct* out, fides_ct& tmp) {
     tmp.cap = 0;
 }
 
-// ModUp of x (n evaluation limbs at `level`): scaled INTT into XT, base
-// conversion into DIG, NTT of every digit target.
-void ks_modup(fides_ctx* c, int level, const uint64_t* x) {
-    const int n = level + 1, N = c->N;
-    ntt_inverse(c->dev, map_single(x, c->XT, n, n, 0, level), IL_PLAIN, IS_MODUP, c->st);
-    launch_modup_conv(c->dev, level, c->XT, c->DIG, c->dig_stride, c->st);
-    LimbMap dm{};
-    const int nd = level / c->alpha + 1;
-    dm.nseg = nd;
-    for (int d = 0; d < nd; ++d) {
-        const int lo = d * c->alpha, hi = std::min(lo + c->alpha - 1, level), cnt = hi - lo + 1;
-        LimbSeg& s = dm.seg[d];
-        s.in = s.out = c->DIG + (size_t)d * c->dig_stride * N;
-        s.count = n - cnt + c->K;
-        s.skip_lo = lo;
-        s.skip_cnt = cnt;
-        s.nq = n;
-        s.q0 = 0;
-        s.level = level;
-        dm.total += s.count;
-    }
-    ntt_forward(c->dev, dm, FL_PLAIN, FS_PLAIN, c->st);
-}
-
-// Segments for the INTT (scaled by (P/p_k)^-1) of the special limbs of XB and
-// XA, in place.
-void add_special_segs(fides_ctx* c, int level, LimbMap& m) {
-    const int n = level + 1, N = c->N;
-    uint64_t* bufs[2] = {c->XB, c->XA};
-    for (int s = 0; s < 2; ++s) {
-        LimbSeg& g = m.seg[m.nseg++];
-        g = LimbSeg{};
-        g.in = g.out = bufs[s] + (size_t)n * N;
-        g.count = c->K;
-        g.skip_lo = c->K;
-        g.nq = 0;
-        g.level = level;
-        g.lmode = IL_PLAIN;
-        g.smode = IS_MODDOWN;
-        m.total += c->K;
-    }
-}
-
-// ModDown of XB -> out0 and XA -> out1 (optionally adding e0/e1), no rescale.
-void moddown_pair(fides_ctx* c, int level, uint64_t* out0, uint64_t* out1, const uint64_t* e0, const uint64_t* e1) {
-    const int n = level + 1, N = c->N, L = c->L;
-    LimbMap sp{};
-    add_special_segs(c, level, sp);
-    ntt_inverse(c->dev, sp, -1, -1, c->st);
-    launch_moddown_conv2(c->dev, level, c->XB + (size_t)n * N, c->W, nullptr, c->XA + (size_t)n * N,
-                         c->W + (size_t)L * N, nullptr, c->st);
-    LimbMap m{};
-    m.nseg = 2;
-    const uint64_t* xs[2] = {c->XB, c->XA};
-    const uint64_t* es[2] = {e0, e1};
-    uint64_t* os[2] = {out0, out1};
-    for (int s = 0; s < 2; ++s) {
-        LimbSeg& g = m.seg[s];
-        g.in = c->W + (size_t)s * L * N;
-        g.out = os[s];
-        g.in2 = xs[s];
-        g.in3 = es[s];
-        g.count = n;
-        g.skip_lo = n;
-        g.nq = n;
-        g.level = level;
-        m.total += n;
-    }
-    ntt_forward(c->dev, m, FL_PLAIN, FS_MODDOWN, c->st);
-}
-
-// ModDown fused with Rescale:  out = Rescale(e + ModDown(x)) for both halves.
-// One INTT launch covers the special limbs of both halves and the two top
-// limbs (e_l + P^-1 x_l); one conversion launch covers both halves.
-void moddown_rescale_pair(fides_ctx* c, int level, uint64_t* out0, uint64_t* out1, const uint64_t* e0,
-                          const uint64_t* e1) {
-    const int n = level + 1, N = c->N, L = c->L;
-    const uint64_t* es[2] = {e0, e1};
-    const uint64_t* xs[2] = {c->XB, c->XA};
-    LimbMap t{};
-    add_special_segs(c, level, t);
-    for (int s = 0; s < 2; ++s) {
-        LimbSeg& g = t.seg[t.nseg++];
-        g = LimbSeg{};
-        g.in = es[s] + (size_t)level * N;
-        g.in2 = xs[s] + (size_t)level * N;
-        g.out = c->T + (size_t)s * N;
-        g.count = 1;
-        g.skip_lo = 1;
-        g.nq = 1;
-        g.q0 = level;
-        g.level = level;
-        g.lmode = IL_AXPY_PINV;
-        g.smode = IS_PLAIN;
-        t.total += 1;
-    }
-    ntt_inverse(c->dev, t, -1, -1, c->st);
-    launch_moddown_conv2(c->dev, level, c->XB + (size_t)n * N, c->W, c->T, c->XA + (size_t)n * N,
-                         c->W + (size_t)L * N, c->T + N, c->st);
-    LimbMap m{};
-    m.nseg = 2;
-    uint64_t* os[2] = {out0, out1};
-    for (int s = 0; s < 2; ++s) {
-        LimbSeg& g = m.seg[s];
-        g.in = c->W + (size_t)s * L * N;
-        g.out = os[s];
-        g.in2 = xs[s];
-        g.in3 = es[s];
-        g.count = level;
-        g.skip_lo = level;
-        g.nq = level;
-        g.level = level;
-        m.total += level;
-    }
-    ntt_forward(c->dev, m, FL_PLAIN, FS_MDRS, c->st);
-}
-
 bool valid_ct(const fides_ctx* c, const fides_ct* a) { return a && a->buf && a->level >= 0 && a->level < c->L; }
 
 uint64_t round_to_mod(long double v, uint64_t p) {
@@ -159,14 +42,6 @@ uint64_t round_to_mod(long double v, uint64_t p) {
 }
 
 }  // namespace
-
-namespace fides {
-void keyswitch_core(fides_ctx* c, int level, const uint64_t* e2, const SwitchKey& k, const uint64_t* c0_for_rot,
-                    uint32_t galois) {
-    ks_modup(c, level, e2);
-    launch_ks_inner(c->dev, level, e2, c->DIG, c->dig_stride, k.b, k.a, c->XB, c->XA, c0_for_rot, galois, c->st);
-}
-}  // namespace fides
 
 extern "C" {
 
@@ -257,8 +132,8 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
     const int nv = ntt_num_variants();
     const int nl = std::min(c->L, 30);
     // any residues work for timing; start from canonical zeros
-    cudaMemsetAsync(c->E0, 0, (size_t)nl * c->limb_bytes(), c->st);
-    LimbMap m = map_single(c->E0, c->E0, nl, nl, 0);
+    cudaMemsetAsync(c->ws1.E0, 0, (size_t)nl * c->limb_bytes(), c->st);
+    LimbMap m = map_single(c->ws1.E0, c->ws1.E0, nl, nl, 0);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -477,16 +352,13 @@ static fides_status hmult_impl(fides_ctx* c, const fides_ct* a, const fides_ct* 
     if (!c->has_relin) return set_err(c, FIDES_KEY_MISSING, "no relinearisation key");
     const int level = std::min(a->level, b->level);
     const bool rs = rescale && level > 0;
-    const int n = level + 1, N = c->N;
+    const int N = c->N;
     fides_ct tmp;
     fides_status s = ct_reserve(c, &tmp, rs ? level - 1 : level);
     if (s != FIDES_OK) return s;
-    launch_tensor(c->dev, n, a->c0(), a->c1(N), b->c0(), b->c1(N), c->E0, c->E1, c->E2, c->st);
-    keyswitch_core(c, level, c->E2, c->relin, nullptr, 0);
-    if (rs)
-        moddown_rescale_pair(c, level, tmp.c0(), tmp.c1(N), c->E0, c->E1);
-    else
-        moddown_pair(c, level, tmp.c0(), tmp.c1(N), c->E0, c->E1);
+    const uint64_t *a0 = a->c0(), *a1 = a->c1(N), *b0 = b->c0(), *b1 = b->c1(N);
+    uint64_t *o0 = tmp.c0(), *o1 = tmp.c1(N);
+    eng_hmult(c, c->ws1, level, 1, &a0, &a1, &b0, &b1, &o0, &o1, rs, c->relin);
     const double sc = a->scale * b->scale;
     const int nd = a->noise_deg + b->noise_deg;
     const int sl = std::max(a->slots, b->slots);
@@ -523,7 +395,7 @@ fides_status fides_rescale(fides_ctx* c, const fides_ct* a, fides_ct* out) {
     for (int i = 0; i < 2; ++i) {
         LimbSeg& g2 = t.seg[i];
         g2.in = ins[i] + (size_t)l * N;
-        g2.out = c->T + (size_t)i * N;
+        g2.out = c->ws1.T + (size_t)i * N;
         g2.count = 1;
         g2.skip_lo = 1;
         g2.nq = 1;
@@ -537,7 +409,7 @@ fides_status fides_rescale(fides_ctx* c, const fides_ct* a, fides_ct* out) {
     uint64_t* os[2] = {tmp.c0(), tmp.c1(N)};
     for (int i = 0; i < 2; ++i) {
         LimbSeg& g2 = m.seg[i];
-        g2.in = c->T + (size_t)i * N;
+        g2.in = c->ws1.T + (size_t)i * N;
         g2.in_stride_zero = 1;
         g2.in2 = ins[i];
         g2.out = os[i];
@@ -558,6 +430,8 @@ fides_status fides_rescale(fides_ctx* c, const fides_ct* a, fides_ct* out) {
     return check_cuda(c, "rescale");
 }
 
+// n rotations of one ciphertext sharing one ModUp (hoisted); n = 1 is a plain
+// rotation.  Rotations are processed in batches of up to kMaxBatch.
 static fides_status rotate_many(fides_ctx* c, const fides_ct* a, int n, const uint32_t* galois, fides_ct** outs) {
     if (!valid_ct(c, a) || n < 1) return FIDES_BAD_ARG;
     std::vector<const SwitchKey*> keys(n);
@@ -574,11 +448,21 @@ static fides_status rotate_many(fides_ctx* c, const fides_ct* a, int n, const ui
         fides_status s = ct_reserve(c, &tmp[r], level);
         if (s != FIDES_OK) return s;
     }
-    ks_modup(c, level, a->c1(N));
-    for (int r = 0; r < n; ++r) {
-        launch_ks_inner(c->dev, level, a->c1(N), c->DIG, c->dig_stride, keys[r]->b, keys[r]->a, c->XB, c->XA,
-                        a->c0(), galois[r], c->st);
-        moddown_pair(c, level, tmp[r].c0(), tmp[r].c1(N), nullptr, nullptr);
+    Workspace* w = &c->ws1;
+    if (n > 1) {
+        fides_status s = ws_reserve(c, c->wsb, std::min(n, kMaxBatch));
+        if (s != FIDES_OK) return s;
+        w = &c->wsb;
+    }
+    const uint64_t *c0 = a->c0(), *c1 = a->c1(N);
+    for (int r0 = 0; r0 < n; r0 += w->cap) {
+        const int nb = std::min(w->cap, n - r0);
+        std::vector<uint64_t*> o0(nb), o1(nb);
+        for (int b = 0; b < nb; ++b) {
+            o0[b] = tmp[r0 + b].c0();
+            o1[b] = tmp[r0 + b].c1(N);
+        }
+        eng_rotate(c, *w, level, nb, &c0, &c1, keys.data() + r0, galois + r0, o0.data(), o1.data(), true);
     }
     const double sc = a->scale;
     const int nd = a->noise_deg, sl = a->slots;
@@ -764,6 +648,141 @@ fides_status fides_mult_scalar(fides_ctx* c, const fides_ct* a, double v, fides_
     fides_status st = check_cuda(c, "mult_scalar");
     if (st == FIDES_OK && rescale && out->level > 0) st = fides_rescale(c, out, out);
     return st;
+}
+
+// Elements grouped by level (stable), each group processed in chunks of the
+// batch workspace's capacity.
+static std::vector<std::vector<int>> level_groups(const fides_ctx* c, int n, const int* levels) {
+    std::vector<std::vector<int>> g(c->L);
+    for (int i = 0; i < n; ++i) g[levels[i]].push_back(i);
+    std::vector<std::vector<int>> out;
+    for (int l = c->L - 1; l >= 0; --l)
+        if (!g[l].empty()) out.push_back(std::move(g[l]));
+    return out;
+}
+
+fides_status fides_hmult_batch(fides_ctx* c, int n, const fides_ct* const* a, const fides_ct* const* b,
+                               fides_ct* const* out, int rescale) {
+    if (!c || n < 0 || (n && (!a || !b || !out))) return FIDES_BAD_ARG;
+    Guard g(c);
+    if (!c->has_relin) return set_err(c, FIDES_KEY_MISSING, "no relinearisation key");
+    for (int i = 0; i < n; ++i)
+        if (!valid_ct(c, a[i]) || !valid_ct(c, b[i]) || !out[i]) return FIDES_BAD_ARG;
+    if (n == 0) return FIDES_OK;
+    fides_status s = ws_reserve(c, c->wsb, std::min(n, kMaxBatch));
+    if (s != FIDES_OK) return s;
+    const int N = c->N;
+    std::vector<int> lv(n);
+    for (int i = 0; i < n; ++i) lv[i] = std::min(a[i]->level, b[i]->level);
+    std::vector<fides_ct> tmp(n);
+    for (auto& grp : level_groups(c, n, lv.data())) {
+        const int level = lv[grp[0]];
+        const bool rs = rescale && level > 0;
+        for (int i : grp) {
+            s = ct_reserve(c, &tmp[i], rs ? level - 1 : level);
+            if (s != FIDES_OK) return s;
+        }
+        for (size_t k0 = 0; k0 < grp.size(); k0 += c->wsb.cap) {
+            const int nb = (int)std::min(grp.size() - k0, (size_t)c->wsb.cap);
+            std::vector<const uint64_t*> a0(nb), a1(nb), b0(nb), b1(nb);
+            std::vector<uint64_t*> o0(nb), o1(nb);
+            for (int j = 0; j < nb; ++j) {
+                const int i = grp[k0 + j];
+                a0[j] = a[i]->c0();
+                a1[j] = a[i]->c1(N);
+                b0[j] = b[i]->c0();
+                b1[j] = b[i]->c1(N);
+                o0[j] = tmp[i].c0();
+                o1[j] = tmp[i].c1(N);
+            }
+            eng_hmult(c, c->wsb, level, nb, a0.data(), a1.data(), b0.data(), b1.data(), o0.data(), o1.data(), rs,
+                      c->relin);
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        const int level = lv[i];
+        const bool rs = rescale && level > 0;
+        const double sc = a[i]->scale * b[i]->scale;
+        const int nd = a[i]->noise_deg + b[i]->noise_deg;
+        const int sl = std::max(a[i]->slots, b[i]->slots);
+        commit(c, out[i], tmp[i]);
+        out[i]->level = rs ? level - 1 : level;
+        out[i]->scale = rs ? sc / (double)c->host.prime[level] : sc;
+        out[i]->noise_deg = rs ? nd - 1 : nd;
+        out[i]->slots = sl;
+    }
+    return check_cuda(c, "hmult_batch");
+}
+
+fides_status fides_rotate_batch(fides_ctx* c, int n, const fides_ct* const* a, const int32_t* indices,
+                                fides_ct* const* out) {
+    if (!c || n < 0 || (n && (!a || !indices || !out))) return FIDES_BAD_ARG;
+    Guard g(c);
+    for (int i = 0; i < n; ++i)
+        if (!valid_ct(c, a[i]) || !out[i]) return FIDES_BAD_ARG;
+    if (n == 0) return FIDES_OK;
+    const int N = c->N;
+    std::vector<uint32_t> gal(n);
+    std::vector<const SwitchKey*> keys(n, nullptr);
+    std::vector<int> lv(n);
+    for (int i = 0; i < n; ++i) {
+        gal[i] = fides_rotation_galois(c, indices[i], a[i]->slots > 0 ? a[i]->slots : N / 2);
+        lv[i] = a[i]->level;
+        if (gal[i] == 1) continue;
+        auto it = c->galois_keys.find(gal[i]);
+        if (it == c->galois_keys.end())
+            return set_err(c, FIDES_KEY_MISSING, "no key for galois element " + std::to_string(gal[i]));
+        keys[i] = &it->second;
+    }
+    fides_status s = ws_reserve(c, c->wsb, std::min(n, kMaxBatch));
+    if (s != FIDES_OK) return s;
+    std::vector<fides_ct> tmp(n);
+    for (auto& grp0 : level_groups(c, n, lv.data())) {
+        std::vector<int> grp;
+        for (int i : grp0) {
+            if (gal[i] == 1) {
+                s = ct_reserve(c, &tmp[i], lv[i]);
+                if (s != FIDES_OK) return s;
+                const size_t bytes = (size_t)(lv[i] + 1) * c->limb_bytes();
+                cudaMemcpyAsync(tmp[i].c0(), a[i]->c0(), bytes, cudaMemcpyDeviceToDevice, c->st);
+                cudaMemcpyAsync(tmp[i].c1(N), a[i]->c1(N), bytes, cudaMemcpyDeviceToDevice, c->st);
+            } else {
+                grp.push_back(i);
+            }
+        }
+        if (grp.empty()) continue;
+        const int level = lv[grp[0]];
+        for (int i : grp) {
+            s = ct_reserve(c, &tmp[i], level);
+            if (s != FIDES_OK) return s;
+        }
+        for (size_t k0 = 0; k0 < grp.size(); k0 += c->wsb.cap) {
+            const int nb = (int)std::min(grp.size() - k0, (size_t)c->wsb.cap);
+            std::vector<const uint64_t*> c0(nb), c1(nb);
+            std::vector<uint64_t*> o0(nb), o1(nb);
+            std::vector<const SwitchKey*> kk(nb);
+            std::vector<uint32_t> gg(nb);
+            for (int j = 0; j < nb; ++j) {
+                const int i = grp[k0 + j];
+                c0[j] = a[i]->c0();
+                c1[j] = a[i]->c1(N);
+                o0[j] = tmp[i].c0();
+                o1[j] = tmp[i].c1(N);
+                kk[j] = keys[i];
+                gg[j] = gal[i];
+            }
+            eng_rotate(c, c->wsb, level, nb, c0.data(), c1.data(), kk.data(), gg.data(), o0.data(), o1.data(), false);
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        const fides_ct meta = *a[i];
+        commit(c, out[i], tmp[i]);
+        out[i]->level = meta.level;
+        out[i]->scale = meta.scale;
+        out[i]->noise_deg = meta.noise_deg;
+        out[i]->slots = meta.slots;
+    }
+    return check_cuda(c, "rotate_batch");
 }
 
 fides_status fides_ntt(fides_ctx* ctx, uint64_t* data, int prime0, int nlimbs, int inverse) {

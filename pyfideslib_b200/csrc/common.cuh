@@ -10,6 +10,7 @@ namespace fides {
 
 constexpr int kMaxPrimes = 128;
 constexpr int kMaxSeg = 8;
+constexpr int kMaxBatch = 32;  // ciphertexts per batched launch (blockIdx.z)
 
 // Read-only view of the context tables in HBM, passed by value to kernels.
 // Index conventions: prime ids 0..L-1 are the Q primes, L..L+K-1 the special
@@ -46,13 +47,17 @@ struct LimbSeg {
     int in_stride_zero;  // 1: every limb reads the same input limb
     int8_t lmode;  // transform prologue mode (FL_* forward, IL_* inverse)
     int8_t smode;  // transform epilogue mode (FS_* forward, IS_* inverse)
-    int16_t pad;
+    int8_t out_tab;  // t > 0: batch element b writes to LimbMap::bout[t - 1][b] (+ limb offset)
+    int8_t pad;
+    size_t bstride;  // batch element b adds b * bstride words to in/in2/in3/out
 };
 
 struct LimbMap {
     int nseg;
     int total;
+    int nb;  // batch elements (gridDim.z); 0 means 1
     LimbSeg seg[kMaxSeg];
+    uint64_t* bout[2][kMaxBatch];
 };
 
 struct LimbRef {
@@ -65,7 +70,7 @@ struct LimbRef {
     int lmode, smode;
 };
 
-__device__ __forceinline__ LimbRef resolve_limb(const LimbMap& m, int f, int N, int L) {
+__device__ __forceinline__ LimbRef resolve_limb(const LimbMap& m, int f, int b, int N, int L) {
     int s = 0;
 #pragma unroll 1
     while (s < m.nseg - 1 && f >= m.seg[s].count) {
@@ -75,10 +80,14 @@ __device__ __forceinline__ LimbRef resolve_limb(const LimbMap& m, int f, int N, 
     const LimbSeg& g = m.seg[s];
     LimbRef r;
     const size_t off = (size_t)f * N;
-    r.in = g.in ? g.in + (g.in_stride_zero ? 0 : off) : nullptr;
-    r.in2 = g.in2 ? g.in2 + off : nullptr;
-    r.in3 = g.in3 ? g.in3 + off : nullptr;
-    r.out = g.out ? g.out + off : nullptr;
+    const size_t bo = (size_t)b * g.bstride;
+    r.in = g.in ? g.in + bo + (g.in_stride_zero ? 0 : off) : nullptr;
+    r.in2 = g.in2 ? g.in2 + bo + off : nullptr;
+    r.in3 = g.in3 ? g.in3 + bo + off : nullptr;
+    if (g.out_tab > 0)
+        r.out = m.bout[g.out_tab - 1][b] + off;
+    else
+        r.out = g.out ? g.out + bo + off : nullptr;
     const int j = f < g.skip_lo ? f : f + g.skip_cnt;
     r.prime = j < g.nq ? g.q0 + j : L + (j - g.nq);
     r.level = g.level;

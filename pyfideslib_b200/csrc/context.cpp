@@ -423,28 +423,45 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.md_pmod = (const uint64_t*)(base + parts[i_dq].off);
     d.rs_qinv = (const uint64_t*)(base + parts[i_rq].off);
 
-    // ---- key-switch workspace ----
-    c->dig_stride = (size_t)(L + K);
-    const size_t lim = (size_t)L * 4 /*E0,E1,E2,XT*/ + c->dnum * c->dig_stride /*DIG*/ + 2 * (size_t)(L + K) /*XB,XA*/ +
-                       2 * (size_t)L /*W*/ + 2 /*T*/;
-    c->ws_limbs = lim;
-    if (cudaMalloc(&c->ws, lim * c->limb_bytes()) != cudaSuccess) return set_err(c, FIDES_OOM, "workspace allocation failed");
-    uint64_t* w = c->ws;
-    auto take = [&](size_t limbs) {
-        uint64_t* r = w;
-        w += limbs * N;
+    // ---- key-switch workspace for single operations ----
+    return ws_reserve(c, c->ws1, 1);
+}
+
+fides_status ws_reserve(fides_ctx* c, Workspace& w, int cap) {
+    if (w.base && w.cap >= cap) return FIDES_OK;
+    ws_free(w);
+    const size_t L = c->L, K = c->K, N = c->N;
+    w.dig_stride = L + K;
+    const size_t limbs = 4 * L /*E0,E1,E2,XT*/ + c->dnum * w.dig_stride /*DIG*/ + 2 * (L + K) /*XB,XA*/ +
+                         2 * L /*W*/ + 2 /*T*/;
+    w.stride = limbs * N;
+    if (cudaMalloc((void**)&w.base, w.stride * 8 * (size_t)cap) != cudaSuccess) {
+        cudaGetLastError();
+        w.base = nullptr;
+        return set_err(c, FIDES_OOM, "workspace allocation failed");
+    }
+    w.cap = cap;
+    uint64_t* p = w.base;
+    auto take = [&](size_t n) {
+        uint64_t* r = p;
+        p += n * N;
         return r;
     };
-    c->E0 = take(L);
-    c->E1 = take(L);
-    c->E2 = take(L);
-    c->XT = take(L);
-    c->DIG = take(c->dnum * c->dig_stride);
-    c->XB = take(L + K);
-    c->XA = take(L + K);
-    c->W = take(2 * (size_t)L);
-    c->T = take(2);
+    w.E0 = take(L);
+    w.E1 = take(L);
+    w.E2 = take(L);
+    w.XT = take(L);
+    w.DIG = take(c->dnum * w.dig_stride);
+    w.XB = take(L + K);
+    w.XA = take(L + K);
+    w.W = take(2 * L);
+    w.T = take(2);
     return FIDES_OK;
+}
+
+void ws_free(Workspace& w) {
+    if (w.base) cudaFree(w.base);
+    w = Workspace{};
 }
 
 void free_context(fides_ctx* c) {
@@ -458,10 +475,10 @@ void free_context(fides_ctx* c) {
     if (c->has_relin) freek(c->relin);
     for (auto& kv : c->galois_keys) freek(kv.second);
     c->galois_keys.clear();
-    if (c->ws) cudaFree(c->ws);
+    ws_free(c->ws1);
+    ws_free(c->wsb);
     if (c->table_mem) cudaFree(c->table_mem);
     if (c->st) cudaStreamDestroy(c->st);
-    c->ws = nullptr;
     c->table_mem = nullptr;
     c->st = nullptr;
 }

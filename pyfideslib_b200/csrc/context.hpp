@@ -51,6 +51,17 @@ struct SwitchKey {
     uint64_t* a = nullptr;
 };
 
+// Key-switch workspace for `cap` batch elements; element b's buffers sit at
+// the element-0 pointers + b*stride words.  Sized for the top level.
+struct Workspace {
+    uint64_t* base = nullptr;
+    size_t stride = 0;  // words per element
+    int cap = 0;
+    size_t dig_stride = 0;  // limbs per digit in DIG
+    uint64_t *E0 = nullptr, *E1 = nullptr, *E2 = nullptr, *XT = nullptr, *DIG = nullptr, *XB = nullptr,
+             *XA = nullptr, *W = nullptr, *T = nullptr;
+};
+
 // Moduli and host copies of the per-prime constants.
 struct HostTables {
     std::vector<uint64_t> prime;  // L+K
@@ -77,12 +88,10 @@ struct fides_ctx {
     void* table_mem = nullptr;
     size_t table_bytes = 0;
 
-    // key-switch workspace (per context, sized for the top level)
-    uint64_t* ws = nullptr;
-    size_t ws_limbs = 0;
-    uint64_t *E0 = nullptr, *E1 = nullptr, *E2 = nullptr, *XT = nullptr, *DIG = nullptr, *XB = nullptr,
-             *XA = nullptr, *W = nullptr, *T = nullptr;
-    size_t dig_stride = 0;  // limbs per digit in DIG
+    // key-switch workspaces: one element for single operations, a larger one
+    // (allocated on first use) for batches
+    fides::Workspace ws1;
+    fides::Workspace wsb;
 
     fides::SwitchKey relin;
     bool has_relin = false;
@@ -107,6 +116,19 @@ bool select_moduli(const fides_params* prm, std::vector<uint64_t>& q, std::vecto
 void free_context(fides_ctx* c);
 LimbMap map_single(const uint64_t* in, uint64_t* out, int count, int nq, int q0, int level = -1,
                    const uint64_t* in2 = nullptr, const uint64_t* in3 = nullptr);
-void keyswitch_core(fides_ctx* c, int level, const uint64_t* e2, const SwitchKey& k, const uint64_t* c0_for_rot,
-                    uint32_t galois);
+fides_status ws_reserve(fides_ctx* c, Workspace& w, int cap);
+void ws_free(Workspace& w);
+
+// ---- engine (engine.cpp): batched evaluation steps over nb <= kMaxBatch elements ----
+// ModUp of x[b] (level+1 evaluation limbs each) into w.XT / w.DIG.
+void eng_modup(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* x);
+// HMult + relinearisation (+ rescale) of pairs (a0,a1)x(b0,b1) into (out0,out1).
+void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* a0, const uint64_t* const* a1,
+               const uint64_t* const* b0, const uint64_t* const* b1, uint64_t* const* out0, uint64_t* const* out1,
+               bool rescale, const SwitchKey& key);
+// Rotation of element b by galois[b] with keys[b]; hoisted=true: all elements
+// rotate the same ciphertext (c0[0], c1[0]) and share one ModUp.
+void eng_rotate(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* c0, const uint64_t* const* c1,
+                const SwitchKey* const* keys, const uint32_t* galois, uint64_t* const* out0, uint64_t* const* out1,
+                bool hoisted);
 }  // namespace fides

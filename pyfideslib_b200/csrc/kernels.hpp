@@ -33,18 +33,43 @@ void ntt_forward(const DevCtx& ctx, const LimbMap& map, int load, int store, cud
 void ntt_inverse(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st);
 
 // ---- element-wise and base-conversion kernels (ks.cu) ----
-void launch_tensor(const DevCtx& ctx, int n, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0,
-                   const uint64_t* b1, uint64_t* e0, uint64_t* e1, uint64_t* e2, cudaStream_t st);
-void launch_modup_conv(const DevCtx& ctx, int level, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
-                       cudaStream_t st);
-void launch_ks_inner(const DevCtx& ctx, int level, const uint64_t* e2, const uint64_t* dig, size_t dig_stride,
-                     const uint64_t* kb, const uint64_t* ka, uint64_t* xb, uint64_t* xa, const uint64_t* c0,
-                     uint32_t galois_inv, cudaStream_t st);
-void launch_moddown_conv(const DevCtx& ctx, int level, const uint64_t* y, uint64_t* w, const uint64_t* ttop,
-                         cudaStream_t st);
-// both halves (b, a) of a key-switch result in one launch
-void launch_moddown_conv2(const DevCtx& ctx, int level, const uint64_t* y0, uint64_t* w0, const uint64_t* ttop0,
-                          const uint64_t* y1, uint64_t* w1, const uint64_t* ttop1, cudaStream_t st);
+// Batched kernels take per-element pointers in kernel parameters (up to
+// kMaxBatch elements); workspace buffers of element b sit at ptr + b*bstride.
+struct TensorArgs {
+    const uint64_t* a0[kMaxBatch];
+    const uint64_t* a1[kMaxBatch];
+    const uint64_t* b0[kMaxBatch];
+    const uint64_t* b1[kMaxBatch];
+    uint64_t* e0;
+    uint64_t* e1;
+    uint64_t* e2;
+    size_t bstride;
+};
+void launch_tensor(const DevCtx& ctx, int n, int nb, const TensorArgs& args, cudaStream_t st);
+void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
+                       size_t bstride, cudaStream_t st);
+struct KsArgs {
+    const uint64_t* own[kMaxBatch];  // evaluation values of the key-switched polynomial (own-digit limbs)
+    const uint64_t* kb[kMaxBatch];   // switching key halves of each element
+    const uint64_t* ka[kMaxBatch];
+    const uint64_t* c0[kMaxBatch];   // rotations: c0 of the input (P*c0 added), else null
+    uint32_t galois[kMaxBatch];      // rotations: automorphism X -> X^g applied as a gather, else 0
+    const uint64_t* dig;             // ModUp digits of element 0
+    uint64_t* xb;                    // outputs of element 0 (extended basis)
+    uint64_t* xa;
+    size_t dig_stride;               // limbs per digit in dig
+    size_t bstride;                  // words between consecutive elements' xb / xa
+    size_t dig_bstride;              // words between consecutive elements' dig (0: shared ModUp)
+};
+// plain: no rotation in any element (vectorised variant)
+void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, bool plain, cudaStream_t st);
+struct MdArgs {
+    const uint64_t* y[2];     // scaled special limbs of the two halves (element 0)
+    uint64_t* w[2];           // conversion outputs
+    const uint64_t* ttop[2];  // fused rescale: INTT(e_l + P^-1 x_l) of each half, else null
+    size_t bstride;
+};
+void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& args, cudaStream_t st);
 // the conversion kernels keep up to 16 inputs (digit moduli / special moduli) in registers
 bool conv_supported(const DevCtx& ctx);
 // override every segment's prologue / epilogue mode (-1 keeps the segment's own)

@@ -27,19 +27,18 @@ __device__ __forceinline__ uint32_t automorph_slot(int logN, uint32_t k, uint32_
 }
 
 // ---------------------------------------------------------------------------
-// tensor product (binomialMult_): e0 = a0 b0, e1 = a0 b1 + a1 b0, e2 = a1 b1
+// tensor product (binomialMult_): e0 = a0 b0, e1 = a0 b1 + a1 b0, e2 = a1 b1,
+// for every batch element (blockIdx.z)
 // ---------------------------------------------------------------------------
-__global__ void k_tensor(const __grid_constant__ DevCtx ctx, const uint64_t* __restrict__ a0,
-                         const uint64_t* __restrict__ a1, const uint64_t* __restrict__ b0,
-                         const uint64_t* __restrict__ b1, uint64_t* __restrict__ e0, uint64_t* __restrict__ e1,
-                         uint64_t* __restrict__ e2) {
-    const int limb = blockIdx.y;
+__global__ void k_tensor(const __grid_constant__ DevCtx ctx, const __grid_constant__ TensorArgs args) {
+    const int limb = blockIdx.y, bi = blockIdx.z;
     const PrimeConst pc = ctx.pc[limb];
     const size_t i = ((size_t)limb * ctx.N + (size_t)(blockIdx.x * blockDim.x + threadIdx.x) * 2);
-    const ulonglong2 x0 = *reinterpret_cast<const ulonglong2*>(a0 + i);
-    const ulonglong2 x1 = *reinterpret_cast<const ulonglong2*>(a1 + i);
-    const ulonglong2 y0 = *reinterpret_cast<const ulonglong2*>(b0 + i);
-    const ulonglong2 y1 = *reinterpret_cast<const ulonglong2*>(b1 + i);
+    const size_t o = i + (size_t)bi * args.bstride;
+    const ulonglong2 x0 = *reinterpret_cast<const ulonglong2*>(args.a0[bi] + i);
+    const ulonglong2 x1 = *reinterpret_cast<const ulonglong2*>(args.a1[bi] + i);
+    const ulonglong2 y0 = *reinterpret_cast<const ulonglong2*>(args.b0[bi] + i);
+    const ulonglong2 y1 = *reinterpret_cast<const ulonglong2*>(args.b1[bi] + i);
     ulonglong2 r0, r1, r2;
     r0.x = mul_mod(x0.x, y0.x, pc);
     r0.y = mul_mod(x0.y, y0.y, pc);
@@ -55,16 +54,15 @@ __global__ void k_tensor(const __grid_constant__ DevCtx ctx, const uint64_t* __r
     }
     r2.x = mul_mod(x1.x, y1.x, pc);
     r2.y = mul_mod(x1.y, y1.y, pc);
-    *reinterpret_cast<ulonglong2*>(e0 + i) = r0;
-    *reinterpret_cast<ulonglong2*>(e1 + i) = r1;
-    *reinterpret_cast<ulonglong2*>(e2 + i) = r2;
+    *reinterpret_cast<ulonglong2*>(args.e0 + o) = r0;
+    *reinterpret_cast<ulonglong2*>(args.e1 + o) = r1;
+    *reinterpret_cast<ulonglong2*>(args.e2 + o) = r2;
 }
 
-void launch_tensor(const DevCtx& ctx, int n, const uint64_t* a0, const uint64_t* a1, const uint64_t* b0,
-                   const uint64_t* b1, uint64_t* e0, uint64_t* e1, uint64_t* e2, cudaStream_t st) {
-    dim3 g(ctx.N / 256, n);
+void launch_tensor(const DevCtx& ctx, int n, int nb, const TensorArgs& args, cudaStream_t st) {
+    dim3 g(ctx.N / 256, n, nb);
     count_launches(1);
-    k_tensor<<<g, 128, 0, st>>>(ctx, a0, a1, b0, b1, e0, e1, e2);
+    k_tensor<<<g, 128, 0, st>>>(ctx, args);
 }
 
 // ---------------------------------------------------------------------------
@@ -92,10 +90,15 @@ __device__ __forceinline__ void conv_store(uint64_t* out, const Acc128& a, const
 
 __global__ void __launch_bounds__(kConvThreads) k_modup_conv(const __grid_constant__ DevCtx ctx, int level,
                                                              const uint64_t* __restrict__ xt,
-                                                             uint64_t* __restrict__ dig, size_t dig_stride) {
+                                                             uint64_t* __restrict__ dig, size_t dig_stride,
+                                                             size_t bstride) {
     __shared__ uint64_t sM[kMaxConvIn][kConvTargets];
     __shared__ PrimeConst sP[kConvTargets];
-    const int d = blockIdx.y;
+    const int ndig = level / ctx.alpha + 1;
+    const int d = blockIdx.y % ndig;
+    const size_t boff = (size_t)(blockIdx.y / ndig) * bstride;
+    xt += boff;
+    dig += boff;
     const int n = level + 1;
     const int lo = d * ctx.alpha;
     const int hi = min(lo + ctx.alpha - 1, level);
@@ -147,13 +150,13 @@ __global__ void __launch_bounds__(kConvThreads) k_modup_conv(const __grid_consta
 
 bool conv_supported(const DevCtx& ctx) { return ctx.alpha <= kMaxConvIn && ctx.K <= kMaxConvIn; }
 
-void launch_modup_conv(const DevCtx& ctx, int level, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
-                       cudaStream_t st) {
+void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
+                       size_t bstride, cudaStream_t st) {
     const int nd = level / ctx.alpha + 1;
     const int maxtar = level + 1 + ctx.K;
-    dim3 g(ctx.N / (2 * kConvThreads), nd, (maxtar + kConvTargets - 1) / kConvTargets);
+    dim3 g(ctx.N / (2 * kConvThreads), nd * nb, (maxtar + kConvTargets - 1) / kConvTargets);
     count_launches(1);
-    k_modup_conv<<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride);
+    k_modup_conv<<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride, bstride);
 }
 
 // ---------------------------------------------------------------------------
@@ -165,19 +168,23 @@ void launch_modup_conv(const DevCtx& ctx, int level, const uint64_t* xt, uint64_
 // ModUp output.  With galois_inv != 0 the result is written permuted:
 // out[j] = value at slot(galois_inv, j).
 // ---------------------------------------------------------------------------
+// Batch element b = blockIdx.x % nb varies fastest, so the blocks that read
+// one key tile for the different elements run back to back and the key is
+// fetched from HBM once and served from L2 to the rest of the batch.
 template <int VEC>
-__global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx ctx, int level,
-                                                  const uint64_t* __restrict__ e2, const uint64_t* __restrict__ dig,
-                                                  size_t dig_stride, const uint64_t* __restrict__ kb,
-                                                  const uint64_t* __restrict__ ka, uint64_t* __restrict__ xb,
-                                                  uint64_t* __restrict__ xa, const uint64_t* __restrict__ c0,
-                                                  uint32_t galois) {
+__global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx ctx, int level, int nb,
+                                                  const __grid_constant__ KsArgs args) {
     const int n = level + 1;
     const int m = blockIdx.y;
+    const int bi = blockIdx.x % nb;
+    const int bx = blockIdx.x / nb;
     const int t = m < n ? m : ctx.L + (m - n);
     const PrimeConst pc = ctx.pc[t];
     const int nd = level / ctx.alpha + 1;
     const size_t kstride = (size_t)(ctx.L + ctx.K) * ctx.N;
+    const size_t boff = (size_t)bi * args.bstride;
+    const uint64_t* kb = args.kb[bi];
+    const uint64_t* ka = args.ka[bi];
     // source limb of each digit for this prime
     const uint64_t* srcs[8];
 #pragma unroll
@@ -187,15 +194,17 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
             const int hi = min(lo + ctx.alpha - 1, level);
             const int cnt = hi - lo + 1;
             if (m < n && t >= lo && t <= hi) {
-                srcs[d] = e2 + (size_t)t * ctx.N;
+                srcs[d] = args.own[bi] + (size_t)t * ctx.N;
             } else {
                 const int md = m < n ? (t < lo ? t : t - cnt) : (n - cnt) + (m - n);
-                srcs[d] = dig + ((size_t)d * dig_stride + md) * ctx.N;
+                srcs[d] = args.dig + (size_t)bi * args.dig_bstride + ((size_t)d * args.dig_stride + md) * ctx.N;
             }
         }
     }
+    uint64_t* xb = args.xb + boff + (size_t)m * ctx.N;
+    uint64_t* xa = args.xa + boff + (size_t)m * ctx.N;
     if constexpr (VEC) {
-        const size_t j = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 2;
+        const size_t j = ((size_t)bx * blockDim.x + threadIdx.x) * 2;
         Acc128 sb0, sb1, sa0, sa1;
 #pragma unroll
         for (int d = 0; d < 8; ++d) {
@@ -214,11 +223,12 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
         ob.y = sb1.reduce(pc);
         oa.x = sa0.reduce(pc);
         oa.y = sa1.reduce(pc);
-        *reinterpret_cast<ulonglong2*>(xb + (size_t)m * ctx.N + j) = ob;
-        *reinterpret_cast<ulonglong2*>(xa + (size_t)m * ctx.N + j) = oa;
+        *reinterpret_cast<ulonglong2*>(xb + j) = ob;
+        *reinterpret_cast<ulonglong2*>(xa + j) = oa;
     } else {
-        const int j = blockIdx.x * blockDim.x + threadIdx.x;
-        const uint32_t src = galois ? automorph_slot(ctx.logN, galois, j) : (uint32_t)j;
+        const int j = bx * blockDim.x + threadIdx.x;
+        const uint32_t g = args.galois[bi];
+        const uint32_t src = g ? automorph_slot(ctx.logN, g, j) : (uint32_t)j;
         Acc128 sb, sa;
 #pragma unroll
         for (int d = 0; d < 8; ++d) {
@@ -228,25 +238,24 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                 sa.mac(x, ka[d * kstride + (size_t)t * ctx.N + src]);
             }
         }
+        const uint64_t* c0 = args.c0[bi];
         if (c0 && m < n) {
             const ulonglong2 pm = __ldg(reinterpret_cast<const ulonglong2*>(ctx.md_pmod) + t);
             sb.mac(mul_shoup(c0[(size_t)m * ctx.N + src], pm.x, pm.y, pc.p), 1);
         }
-        xb[(size_t)m * ctx.N + j] = sb.reduce(pc);
-        xa[(size_t)m * ctx.N + j] = sa.reduce(pc);
+        xb[j] = sb.reduce(pc);
+        xa[j] = sa.reduce(pc);
     }
 }
 
-void launch_ks_inner(const DevCtx& ctx, int level, const uint64_t* e2, const uint64_t* dig, size_t dig_stride,
-                     const uint64_t* kb, const uint64_t* ka, uint64_t* xb, uint64_t* xa, const uint64_t* c0,
-                     uint32_t galois_inv, cudaStream_t st) {
+void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, bool plain, cudaStream_t st) {
     count_launches(1);
-    if (!c0 && !galois_inv) {
-        dim3 g(ctx.N / 512, level + 1 + ctx.K);
-        k_ks_inner<1><<<g, 256, 0, st>>>(ctx, level, e2, dig, dig_stride, kb, ka, xb, xa, c0, galois_inv);
+    if (plain) {
+        dim3 g(ctx.N / 512 * nb, level + 1 + ctx.K);
+        k_ks_inner<1><<<g, 256, 0, st>>>(ctx, level, nb, args);
     } else {
-        dim3 g(ctx.N / 256, level + 1 + ctx.K);
-        k_ks_inner<0><<<g, 256, 0, st>>>(ctx, level, e2, dig, dig_stride, kb, ka, xb, xa, c0, galois_inv);
+        dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
+        k_ks_inner<0><<<g, 256, 0, st>>>(ctx, level, nb, args);
     }
 }
 
@@ -266,21 +275,17 @@ __device__ __forceinline__ uint64_t switch_modulus_d(uint64_t a, uint64_t om, co
     return csub(reduce64_lazy(v, nc), nm);
 }
 
-struct MdArgs {
-    const uint64_t* y[2];
-    uint64_t* w[2];
-    const uint64_t* ttop[2];
-};
 
 __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_constant__ DevCtx ctx, int level,
                                                                const __grid_constant__ MdArgs args) {
     __shared__ uint64_t sM[kMaxConvIn][kConvTargets];
     __shared__ PrimeConst sP[kConvTargets];
     __shared__ ulonglong2 sPinv[kConvTargets];
-    const int half = blockIdx.z;
-    const uint64_t* __restrict__ y = args.y[half];
-    uint64_t* __restrict__ w = args.w[half];
-    const uint64_t* __restrict__ ttop = args.ttop[half];
+    const int half = blockIdx.z & 1;
+    const size_t boff = (size_t)(blockIdx.z >> 1) * args.bstride;
+    const uint64_t* __restrict__ y = args.y[half] + boff;
+    uint64_t* __restrict__ w = args.w[half] + boff;
+    const uint64_t* __restrict__ ttop = args.ttop[half] ? args.ttop[half] + boff : nullptr;
     const int K = ctx.K, L = ctx.L;
     const int nout = ttop ? level : level + 1;
     const int q0 = blockIdx.y * kConvTargets;
@@ -355,25 +360,12 @@ __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_cons
     }
 }
 
-void launch_moddown_conv2(const DevCtx& ctx, int level, const uint64_t* y0, uint64_t* w0, const uint64_t* ttop0,
-                          const uint64_t* y1, uint64_t* w1, const uint64_t* ttop1, cudaStream_t st) {
-    const int nout = ttop0 ? level : level + 1;
+void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& a, cudaStream_t st) {
+    const int nout = a.ttop[0] ? level : level + 1;
     if (nout <= 0) return;
-    MdArgs a;
-    a.y[0] = y0;
-    a.y[1] = y1;
-    a.w[0] = w0;
-    a.w[1] = w1;
-    a.ttop[0] = ttop0;
-    a.ttop[1] = ttop1;
-    dim3 g(ctx.N / (2 * kConvThreads), (nout + kConvTargets - 1) / kConvTargets, y1 ? 2 : 1);
+    dim3 g(ctx.N / (2 * kConvThreads), (nout + kConvTargets - 1) / kConvTargets, 2 * nb);
     count_launches(1);
     k_moddown_conv<<<g, kConvThreads, 0, st>>>(ctx, level, a);
-}
-
-void launch_moddown_conv(const DevCtx& ctx, int level, const uint64_t* y, uint64_t* w, const uint64_t* ttop,
-                         cudaStream_t st) {
-    launch_moddown_conv2(ctx, level, y, w, ttop, nullptr, nullptr, nullptr, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
     __shared__ __align__(16) uint64_t sm[G::R * TC];
     __shared__ ulonglong2 tws[G::R];
 
-    const LimbRef lr = resolve_limb(map, blockIdx.y, ctx.N, ctx.L);
+    const LimbRef lr = resolve_limb(map, blockIdx.y, blockIdx.z, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const ulonglong2* twg = reinterpret_cast<const ulonglong2*>(ctx.fwd_tw) + (size_t)lr.prime * ctx.N;
     for (int i = threadIdx.x; i < G::R; i += G::NTC) tws[i] = twg[i];
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     __shared__ __align__(16) uint64_t sm[TR * CP];
 
-    const LimbRef lr = resolve_limb(map, blockIdx.y, ctx.N, ctx.L);
+    const LimbRef lr = resolve_limb(map, blockIdx.y, blockIdx.z, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const uint64_t* twg = ctx.fwd_tw + (size_t)lr.prime * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     __shared__ __align__(16) uint64_t sm[TR * CP];
 
-    const LimbRef lr = resolve_limb(map, blockIdx.y, ctx.N, ctx.L);
+    const LimbRef lr = resolve_limb(map, blockIdx.y, blockIdx.z, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const uint64_t* twg = ctx.inv_tw + (size_t)lr.prime * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
     __shared__ __align__(16) uint64_t sm[G::R * TC];
     __shared__ ulonglong2 tws[G::R];
 
-    const LimbRef lr = resolve_limb(map, blockIdx.y, ctx.N, ctx.L);
+    const LimbRef lr = resolve_limb(map, blockIdx.y, blockIdx.z, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const ulonglong2* twg = reinterpret_cast<const ulonglong2*>(ctx.inv_tw) + (size_t)lr.prime * ctx.N;
     for (int i = threadIdx.x; i < G::R; i += G::NTC) tws[i] = twg[i];
@@ -390,7 +390,7 @@ int ntt_num_variants() { return 3; }
 template <int LR, int LC, int MINB, bool PF>
 static void launch_fwd_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
-    dim3 g1(G::C / G::TC, map.total), g2(G::R / G::TR, map.total);
+    dim3 g1(G::C / G::TC, map.total, map.nb > 0 ? map.nb : 1), g2(G::R / G::TR, map.total, map.nb > 0 ? map.nb : 1);
     k_ntt_fwd_cols<LR, LC, MINB, PF><<<g1, G::NTC, 0, st>>>(ctx, map);
     k_ntt_fwd_rows<LR, LC, MINB, PF><<<g2, G::NTR, 0, st>>>(ctx, map);
 }
@@ -398,7 +398,7 @@ static void launch_fwd_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st)
 template <int LR, int LC, int MINB, bool PF>
 static void launch_inv_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
-    dim3 g1(G::C / G::TC, map.total), g2(G::R / G::TR, map.total);
+    dim3 g1(G::C / G::TC, map.total, map.nb > 0 ? map.nb : 1), g2(G::R / G::TR, map.total, map.nb > 0 ? map.nb : 1);
     k_ntt_inv_rows<LR, LC, MINB, PF><<<g2, G::NTR, 0, st>>>(ctx, map);
     k_ntt_inv_cols<LR, LC, MINB, PF><<<g1, G::NTC, 0, st>>>(ctx, map);
 }

@@ -1,0 +1,88 @@
+"""Batched evaluation (config 4 shape, scaled down): results of the batched
+entry points are identical to the per-operation path and to the oracle."""
+import numpy as np
+import pytest
+
+from gpu_helpers import make_pair, rand_ct, rand_key
+
+pytestmark = pytest.mark.gpu
+
+
+def test_hmult_batch_uneven_levels_equals_per_op():
+    cc, oc = make_pair(12, 10, 4, 3)
+    kb, ka = rand_key(oc, 77)
+    cc.upload_relin_key(kb, ka)
+    rng = np.random.default_rng(3)
+    levels = [int(x) for x in rng.integers(0, 10, size=40)]  # > 32 per level group would chunk too
+    A, B, raw = [], [], []
+    for i, lv in enumerate(levels):
+        a0, a1 = rand_ct(oc, lv, 1000 + 4 * i)
+        b0, b1 = rand_ct(oc, lv, 1002 + 4 * i)
+        A.append(cc.upload(a0, a1))
+        B.append(cc.upload(b0, b1))
+        raw.append((a0, a1, b0, b1))
+    for rs in (True, False):
+        outs = cc.EvalMultBatch(A, B, rescale=rs)
+        for i, lv in enumerate(levels):
+            got = outs[i].download()
+            want = cc.EvalMult(A[i], B[i], rescale=rs).download()
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (i, lv, rs)
+        # spot-check against the oracle
+        for i in (0, 7, 23):
+            w = oc.hmult(levels[i], *raw[i], kb, ka, rescale=rs and levels[i] > 0)
+            g = outs[i].download()
+            assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1])
+
+
+def test_hmult_batch_same_level_more_than_32():
+    cc, oc = make_pair(11, 6, 2, 2)
+    kb, ka = rand_key(oc, 5)
+    cc.upload_relin_key(kb, ka)
+    A, B = [], []
+    for i in range(37):
+        A.append(cc.upload(*rand_ct(oc, 5, 10 * i)))
+        B.append(cc.upload(*rand_ct(oc, 5, 10 * i + 5)))
+    outs = cc.EvalMultBatch(A, B, rescale=True)
+    for i in (0, 31, 32, 36):
+        want = cc.EvalMult(A[i], B[i], rescale=True).download()
+        got = outs[i].download()
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+def test_rotate_batch_equals_per_op_and_oracle():
+    cc, oc = make_pair(12, 8, 3, 3)
+    idx = [1, 3, -2, 17, 1, 100]
+    keys = {}
+    for i, r in enumerate(sorted(set(idx))):
+        g = cc.rotation_galois(r)
+        keys[g] = rand_key(oc, 400 + 2 * i)
+        cc.upload_galois_key(g, *keys[g])
+    levels = [7, 7, 4, 2, 4, 7]
+    cts, raw = [], []
+    for i, lv in enumerate(levels):
+        c0, c1 = rand_ct(oc, lv, 50 + 3 * i)
+        cts.append(cc.upload(c0, c1))
+        raw.append((c0, c1))
+    outs = cc.EvalRotateBatch(cts, idx)
+    for i, r in enumerate(idx):
+        g = cc.rotation_galois(r)
+        want = oc.rotate(levels[i], *raw[i], pow(g, -1, 2 * oc.N), *keys[g])
+        got = outs[i].download()
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), i
+
+
+def test_hoisted_more_than_32_rotations():
+    cc, oc = make_pair(11, 5, 2, 2)
+    idx = list(range(1, 41))
+    cc_keys = {}
+    for i, r in enumerate(idx):
+        g = cc.rotation_galois(r)
+        cc_keys[g] = rand_key(oc, 900 + 2 * i)
+        cc.upload_galois_key(g, *cc_keys[g])
+    c0, c1 = rand_ct(oc, 4, 8)
+    ct = cc.upload(c0, c1)
+    outs = cc.EvalFastRotation(ct, idx)
+    for i in (0, 31, 32, 39):
+        want = cc.EvalRotate(ct, idx[i]).download()
+        got = outs[i].download()
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
