@@ -41,6 +41,8 @@ typedef struct fides_ct fides_ct; /* device-resident ciphertext */
 typedef struct fides_pt fides_pt; /* device-resident plaintext  */
 typedef struct fides_sk fides_sk; /* secret key (client side)   */
 typedef struct fides_pk fides_pk; /* public key (client side)   */
+typedef struct fides_plan fides_plan; /* captured CUDA graph of a batched evaluation */
+typedef struct fides_server fides_server; /* continuous-batching request loop */
 
 typedef struct {
     int log_n;            /* ring dimension N = 2^log_n, 8 <= log_n <= 16 */
@@ -107,6 +109,9 @@ fides_status fides_ct_download(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0,
 fides_status fides_ct_download_async(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1);
 fides_status fides_ct_info(const fides_ct* ct, int* level, double* scale, int* noise_deg, int* slots);
 fides_status fides_ct_create(fides_ctx* ctx, fides_ct** out); /* empty, filled by an operation */
+/* Overwrite the residues of an existing ciphertext (same level, buffer kept):
+ * refreshes the inputs of a captured plan without re-capturing it. */
+fides_status fides_ct_write(fides_ctx* ctx, fides_ct* ct, const uint64_t* c0, const uint64_t* c1);
 fides_status fides_ct_copy(fides_ctx* ctx, const fides_ct* src, fides_ct* dst);
 fides_status fides_ct_free(fides_ctx* ctx, fides_ct* ct);
 /* Device residues of a ciphertext: (l+1)*N words each, valid until the next
@@ -140,6 +145,19 @@ fides_status fides_hmult_batch(fides_ctx* ctx, int n, const fides_ct* const* a, 
 /* Batched EvalRotate: out[i] = rotation of a[i] by indices[i] (own keys). */
 fides_status fides_rotate_batch(fides_ctx* ctx, int n, const fides_ct* const* a, const int32_t* indices,
                                 fides_ct* const* out);
+/* Plan of a batched evaluation captured into one CUDA graph: n independent
+ * pairs (levels may differ) go through HMult + relinearisation (+ rescale)
+ * and then, if `indices` is not NULL, a rotation of each product by
+ * indices[i]; results land in out[i].  Creating the plan allocates every
+ * output and intermediate buffer and captures the kernel sequence once;
+ * fides_plan_launch replays it (a single graph launch) on the context
+ * stream, reading the inputs' current residues (fides_ct_write refreshes
+ * them).  No counterpart in the reference, which captures per-level graphs
+ * of one key switch (LimbPartitionMGPU.cu:581-640, FIDESLIB_USE_GRAPH_CAPTURE). */
+fides_status fides_plan_hmult_rotate(fides_ctx* ctx, int n, const fides_ct* const* a, const fides_ct* const* b,
+                                     const int32_t* indices, int rescale, fides_ct* const* out, fides_plan** plan);
+fides_status fides_plan_launch(fides_ctx* ctx, fides_plan* plan);
+fides_status fides_plan_free(fides_ctx* ctx, fides_plan* plan);
 /* EvalConjugate: Ciphertext::conjugate, Ciphertext.cpp:933 */
 fides_status fides_conjugate(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
 /* Apply an automorphism whose key was uploaded with fides_key_upload_galois */
@@ -154,6 +172,35 @@ fides_status fides_mult_pt(fides_ctx* ctx, const fides_ct* a, const fides_pt* p,
 /* EvalAdd(ct, double) / EvalMult(ct, double): Ciphertext::addScalar / multScalar */
 fides_status fides_add_scalar(fides_ctx* ctx, const fides_ct* a, double v, fides_ct* out);
 fides_status fides_mult_scalar(fides_ctx* ctx, const fides_ct* a, double v, fides_ct* out, int rescale);
+
+/* ---- serving: continuous batching over one context (no counterpart in the
+ *      reference, which has no serving layer) ---- */
+typedef enum { FIDES_OP_HMULT = 0, FIDES_OP_ROTATE = 1, FIDES_OP_BOOTSTRAP = 2 } fides_op;
+typedef struct {
+    uint64_t completed;    /* requests finished since the last reset */
+    uint64_t batches;      /* batches launched */
+    double p50_ms;         /* latency submit -> completion, median */
+    double p99_ms;         /* 99th percentile */
+    double mean_queue_ms;  /* submit -> batch launch */
+    double throughput;     /* completed requests per second (first submit -> last completion) */
+    size_t reserved_bytes; /* HBM currently charged against the budget */
+} fides_srv_stats_t;
+/* Start the loop: `num_streams` streams, each with a workspace for
+ * `max_batch` requests, and a fixed HBM budget (bytes) that the workspaces
+ * and the outputs of admitted requests are charged against. */
+fides_status fides_srv_create(fides_ctx* ctx, size_t hbm_budget, int max_batch, int num_streams,
+                              fides_server** out);
+/* Queue a request: FIDES_OP_HMULT (a*b, relinearised and rescaled) or
+ * FIDES_OP_ROTATE (a rotated by index).  a, b and out must stay alive until
+ * the request completes; the result lands in out. */
+fides_status fides_srv_submit(fides_server* srv, int op, const fides_ct* a, const fides_ct* b, int32_t index,
+                              fides_ct* out, uint64_t* request_id);
+/* Wait for a request (FIDES_TIMEOUT after timeout_s); returns its status. */
+fides_status fides_srv_wait(fides_server* srv, uint64_t request_id, double timeout_s);
+fides_status fides_srv_stats(fides_server* srv, fides_srv_stats_t* out);
+fides_status fides_srv_reset_stats(fides_server* srv);
+/* Drain the queue, stop the loop, release its streams and workspaces. */
+fides_status fides_srv_destroy(fides_server* srv);
 
 /* ---- raw limb kernels on device memory (LimbPartition NTT/INTT entry points,
  *      src/CKKS/LimbPartition.cu; used for the plain RNS polynomial multiply) ---- */

@@ -14,9 +14,9 @@ import ctypes as C
 
 import numpy as np
 
-from ._capi import FidesError, FidesParams, check, lib, u64p, vp
+from ._capi import FidesError, FidesParams, SrvStats, check, lib, u64p, vp
 
-__all__ = ["CryptoContext", "Ciphertext", "Plaintext", "PrivateKey", "FidesError", "lib"]
+__all__ = ["CryptoContext", "Ciphertext", "Plaintext", "PrivateKey", "Server", "Plan", "FidesError", "lib"]
 
 
 def _p(a):
@@ -72,6 +72,61 @@ class Plaintext:
         if h and ctx is not None and ctx._h:
             lib.fides_pt_free(ctx._h, h)
         self._h = None
+
+
+class Plan:
+    """A captured CUDA graph of a batched evaluation (fides_plan)."""
+
+    def __init__(self, ctx, handle, keep):
+        self.ctx, self._h, self._keep = ctx, handle, keep
+
+    def launch(self):
+        check(lib.fides_plan_launch(self.ctx._h, self._h), self.ctx._h)
+
+    def __del__(self):
+        h, ctx = getattr(self, "_h", None), getattr(self, "ctx", None)
+        if h and ctx is not None and ctx._h:
+            lib.fides_plan_free(ctx._h, h)
+        self._h = None
+
+
+class Server:
+    """Continuous-batching request loop (fides_srv_*): submit HMult / Rotate
+    requests from any thread, wait on request ids, read p50 / p99."""
+
+    HMULT, ROTATE = 0, 1
+
+    def __init__(self, ctx, hbm_budget, max_batch=16, num_streams=2):
+        self.ctx = ctx
+        h = vp()
+        check(lib.fides_srv_create(ctx._h, int(hbm_budget), max_batch, num_streams, C.byref(h)), ctx._h)
+        self._h = h.value
+
+    def submit(self, op, a, b=None, index=0, out=None):
+        out = out if out is not None else Ciphertext(self.ctx)
+        rid = C.c_uint64()
+        check(lib.fides_srv_submit(self._h, op, a._h, b._h if b is not None else None, index, out._h,
+                                   C.byref(rid)), self.ctx._h)
+        return rid.value, out
+
+    def wait(self, rid, timeout=60.0):
+        check(lib.fides_srv_wait(self._h, rid, timeout), self.ctx._h)
+
+    def stats(self):
+        st = SrvStats()
+        check(lib.fides_srv_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in SrvStats._fields_}
+
+    def reset_stats(self):
+        check(lib.fides_srv_reset_stats(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.fides_srv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 class PrivateKey:
@@ -254,6 +309,24 @@ class CryptoContext:
         O = (vp * n)(*[o._h for o in outs])
         check(lib.fides_rotate_batch(self._h, n, A, I, O), self._h)
         return outs
+
+    def plan_hmult_rotate(self, a_list, b_list, indices=None, rescale=True, outs=None):
+        """Capture batched HMult(+rescale)(+rotation) into one CUDA graph.
+        Returns (plan, outs); plan.launch() replays it."""
+        n = len(a_list)
+        outs = outs or [Ciphertext(self) for _ in range(n)]
+        A = (vp * n)(*[x._h for x in a_list])
+        B = (vp * n)(*[x._h for x in b_list])
+        O = (vp * n)(*[o._h for o in outs])
+        I = (C.c_int32 * n)(*indices) if indices is not None else None
+        h = vp()
+        check(lib.fides_plan_hmult_rotate(self._h, n, A, B, I, int(rescale), O, C.byref(h)), self._h)
+        return Plan(self, h.value, (a_list, b_list, outs)), outs
+
+    def write(self, ct, c0, c1):
+        check(lib.fides_ct_write(self._h, ct._h, _p(np.ascontiguousarray(c0, dtype=np.uint64)),
+                                 _p(np.ascontiguousarray(c1, dtype=np.uint64))), self._h)
+        self.Synchronize()
 
     def EvalSquare(self, a, rescale=False, out=None):
         out = self._out(out)

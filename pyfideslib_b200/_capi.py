@@ -26,6 +26,11 @@ STATUS = {0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "LEVEL_MISMATCH", 4: "KEY_MISSING"
           6: "CUDA_ERR", 7: "UNSUPPORTED", 8: "BUSY"}
 
 
+class SrvStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("batches", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double),
+                ("mean_queue_ms", C.c_double), ("throughput", C.c_double), ("reserved_bytes", C.c_size_t)]
+
+
 class FidesParams(C.Structure):
     _fields_ = [("log_n", C.c_int), ("num_q", C.c_int), ("num_p", C.c_int), ("dnum", C.c_int),
                 ("q", u64p), ("p", u64p), ("q0_bits", C.c_int), ("qi_bits", C.c_int), ("p_bits", C.c_int),
@@ -60,6 +65,7 @@ EXPORTS = {
     "fides_ct_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_int)],
                       C.c_int),
     "fides_ct_create": ([vp, C.POINTER(vp)], C.c_int),
+    "fides_ct_write": ([vp, vp, u64p, u64p], C.c_int),
     "fides_ct_copy": ([vp, vp, vp], C.c_int),
     "fides_ct_free": ([vp, vp], C.c_int),
     "fides_ct_device_ptrs": ([vp, C.POINTER(u64p), C.POINTER(u64p)], C.c_int),
@@ -74,6 +80,10 @@ EXPORTS = {
     "fides_conjugate": ([vp, vp, vp], C.c_int),
     "fides_hmult_batch": ([vp, C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.c_int], C.c_int),
     "fides_rotate_batch": ([vp, C.c_int, C.POINTER(vp), i32p, C.POINTER(vp)], C.c_int),
+    "fides_plan_hmult_rotate": ([vp, C.c_int, C.POINTER(vp), C.POINTER(vp), i32p, C.c_int, C.POINTER(vp),
+                                 C.POINTER(vp)], C.c_int),
+    "fides_plan_launch": ([vp, vp], C.c_int),
+    "fides_plan_free": ([vp, vp], C.c_int),
     "fides_automorphism": ([vp, vp, C.c_uint32, vp], C.c_int),
     "fides_add": ([vp, vp, vp, vp], C.c_int),
     "fides_sub": ([vp, vp, vp, vp], C.c_int),
@@ -82,6 +92,12 @@ EXPORTS = {
     "fides_mult_pt": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "fides_add_scalar": ([vp, vp, C.c_double, vp], C.c_int),
     "fides_mult_scalar": ([vp, vp, C.c_double, vp, C.c_int], C.c_int),
+    "fides_srv_create": ([vp, C.c_size_t, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
+    "fides_srv_submit": ([vp, C.c_int, vp, vp, C.c_int32, vp, C.POINTER(C.c_uint64)], C.c_int),
+    "fides_srv_wait": ([vp, C.c_uint64, C.c_double], C.c_int),
+    "fides_srv_stats": ([vp, C.POINTER(SrvStats)], C.c_int),
+    "fides_srv_reset_stats": ([vp], C.c_int),
+    "fides_srv_destroy": ([vp], C.c_int),
     "fides_ntt": ([vp, vp, C.c_int, C.c_int, C.c_int], C.c_int),
     "fides_polymul": ([vp, vp, vp, vp, vp, vp, C.c_int, C.c_int], C.c_int),
     "fides_polymul_noalloc": ([vp, vp, vp, vp, C.c_int, C.c_int], C.c_int),

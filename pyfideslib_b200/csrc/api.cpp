@@ -277,6 +277,15 @@ fides_status fides_ct_device_ptrs(const fides_ct* ct, uint64_t** c0, uint64_t** 
     return FIDES_OK;
 }
 
+fides_status fides_ct_write(fides_ctx* ctx, fides_ct* ct, const uint64_t* c0, const uint64_t* c1) {
+    if (!ctx || !valid_ct(ctx, ct) || !c0 || !c1) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    const size_t bytes = (size_t)(ct->level + 1) * ctx->limb_bytes();
+    cudaMemcpyAsync(ct->c0(), c0, bytes, cudaMemcpyHostToDevice, ctx->st);
+    cudaMemcpyAsync(ct->c1(ctx->N), c1, bytes, cudaMemcpyHostToDevice, ctx->st);
+    return check_cuda(ctx, "ct write");
+}
+
 fides_status fides_ct_copy(fides_ctx* ctx, const fides_ct* src, fides_ct* dst) {
     if (!ctx || !valid_ct(ctx, src) || !dst) return FIDES_BAD_ARG;
     if (src == dst) return FIDES_OK;
@@ -783,6 +792,161 @@ fides_status fides_rotate_batch(fides_ctx* c, int n, const fides_ct* const* a, c
         out[i]->slots = meta.slots;
     }
     return check_cuda(c, "rotate_batch");
+}
+
+}  // extern "C"
+
+struct fides_plan {
+    uint64_t nkernels = 0;  // kernels per replay
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<fides_ct> inter;  // products feeding the rotations
+};
+
+extern "C" {
+
+fides_status fides_plan_hmult_rotate(fides_ctx* c, int n, const fides_ct* const* a, const fides_ct* const* b,
+                                     const int32_t* indices, int rescale, fides_ct* const* out, fides_plan** plan) {
+    if (!c || n < 1 || !a || !b || !out || !plan) return FIDES_BAD_ARG;
+    Guard g(c);
+    *plan = nullptr;
+    if (!c->has_relin) return set_err(c, FIDES_KEY_MISSING, "no relinearisation key");
+    const int N = c->N;
+    std::vector<int> lv(n), lv2(n);
+    std::vector<uint32_t> gal(n, 1);
+    std::vector<const SwitchKey*> keys(n, nullptr);
+    for (int i = 0; i < n; ++i) {
+        if (!valid_ct(c, a[i]) || !valid_ct(c, b[i]) || !out[i]) return FIDES_BAD_ARG;
+        lv[i] = std::min(a[i]->level, b[i]->level);
+        lv2[i] = (rescale && lv[i] > 0) ? lv[i] - 1 : lv[i];
+        if (indices) {
+            gal[i] = fides_rotation_galois(c, indices[i], std::max(a[i]->slots, b[i]->slots));
+            if (gal[i] != 1) {
+                auto it = c->galois_keys.find(gal[i]);
+                if (it == c->galois_keys.end())
+                    return set_err(c, FIDES_KEY_MISSING, "no key for galois element " + std::to_string(gal[i]));
+                keys[i] = &it->second;
+            }
+        }
+    }
+    fides_status s = ws_reserve(c, c->wsb, std::min(n, kMaxBatch));
+    if (s != FIDES_OK) return s;
+    auto* p = new (std::nothrow) fides_plan();
+    if (!p) return FIDES_OOM;
+    const bool rot = indices != nullptr;
+    if (rot) p->inter.resize(n);
+    for (int i = 0; i < n; ++i) {
+        if (rot) s = ct_reserve(c, &p->inter[i], lv2[i]);
+        if (s == FIDES_OK) s = ct_reserve(c, out[i], lv2[i]);
+        if (s != FIDES_OK) {
+            fides_plan_free(c, p);
+            return s;
+        }
+    }
+    cudaStreamSynchronize(c->st);
+    // capture: kernels and device-to-device copies only, no allocation
+    const uint64_t k0count = launch_count();
+    if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        fides_plan_free(c, p);
+        return check_cuda(c, "begin capture");
+    }
+    auto stage_out = [&](int i) -> fides_ct* { return rot ? &p->inter[i] : out[i]; };
+    for (auto& grp : level_groups(c, n, lv.data())) {
+        const int level = lv[grp[0]];
+        for (size_t k0 = 0; k0 < grp.size(); k0 += c->wsb.cap) {
+            const int nb = (int)std::min(grp.size() - k0, (size_t)c->wsb.cap);
+            std::vector<const uint64_t*> a0(nb), a1(nb), b0(nb), b1(nb);
+            std::vector<uint64_t*> o0(nb), o1(nb);
+            for (int j = 0; j < nb; ++j) {
+                const int i = grp[k0 + j];
+                a0[j] = a[i]->c0();
+                a1[j] = a[i]->c1(N);
+                b0[j] = b[i]->c0();
+                b1[j] = b[i]->c1(N);
+                o0[j] = stage_out(i)->c0();
+                o1[j] = stage_out(i)->c1(N);
+            }
+            eng_hmult(c, c->wsb, level, nb, a0.data(), a1.data(), b0.data(), b1.data(), o0.data(), o1.data(),
+                      rescale && level > 0, c->relin);
+        }
+    }
+    if (rot) {
+        for (auto& grp0 : level_groups(c, n, lv2.data())) {
+            std::vector<int> grp;
+            for (int i : grp0) {
+                if (gal[i] == 1) {
+                    const size_t bytes = (size_t)(lv2[i] + 1) * c->limb_bytes();
+                    cudaMemcpyAsync(out[i]->c0(), p->inter[i].c0(), bytes, cudaMemcpyDeviceToDevice, c->st);
+                    cudaMemcpyAsync(out[i]->c1(N), p->inter[i].c1(N), bytes, cudaMemcpyDeviceToDevice, c->st);
+                } else {
+                    grp.push_back(i);
+                }
+            }
+            if (grp.empty()) continue;
+            const int level = lv2[grp[0]];
+            for (size_t k0 = 0; k0 < grp.size(); k0 += c->wsb.cap) {
+                const int nb = (int)std::min(grp.size() - k0, (size_t)c->wsb.cap);
+                std::vector<const uint64_t*> c0(nb), c1(nb);
+                std::vector<uint64_t*> o0(nb), o1(nb);
+                std::vector<const SwitchKey*> kk(nb);
+                std::vector<uint32_t> gg(nb);
+                for (int j = 0; j < nb; ++j) {
+                    const int i = grp[k0 + j];
+                    c0[j] = p->inter[i].c0();
+                    c1[j] = p->inter[i].c1(N);
+                    o0[j] = out[i]->c0();
+                    o1[j] = out[i]->c1(N);
+                    kk[j] = keys[i];
+                    gg[j] = gal[i];
+                }
+                eng_rotate(c, c->wsb, level, nb, c0.data(), c1.data(), kk.data(), gg.data(), o0.data(), o1.data(),
+                           false);
+            }
+        }
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e1 = cudaStreamEndCapture(c->st, &graph);
+    if (e1 != cudaSuccess || !graph) {
+        fides_plan_free(c, p);
+        return set_err(c, FIDES_CUDA_ERR, std::string("end capture: ") + cudaGetErrorString(e1));
+    }
+    p->graph = graph;
+    p->nkernels = launch_count() - k0count;
+    const cudaError_t e2 = cudaGraphInstantiate(&p->exec, graph, 0);
+    if (e2 != cudaSuccess) {
+        fides_plan_free(c, p);
+        return set_err(c, FIDES_CUDA_ERR, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+    }
+    for (int i = 0; i < n; ++i) {
+        const double sc = a[i]->scale * b[i]->scale;
+        const bool rs = rescale && lv[i] > 0;
+        out[i]->level = lv2[i];
+        out[i]->scale = rs ? sc / (double)c->host.prime[lv[i]] : sc;
+        out[i]->noise_deg = a[i]->noise_deg + b[i]->noise_deg - (rs ? 1 : 0);
+        out[i]->slots = std::max(a[i]->slots, b[i]->slots);
+    }
+    *plan = p;
+    return check_cuda(c, "plan");
+}
+
+fides_status fides_plan_launch(fides_ctx* c, fides_plan* plan) {
+    if (!c || !plan || !plan->exec) return FIDES_BAD_ARG;
+    Guard g(c);
+    count_launches((int)plan->nkernels);
+    if (cudaGraphLaunch(plan->exec, c->st) != cudaSuccess) return check_cuda(c, "graph launch");
+    return FIDES_OK;
+}
+
+fides_status fides_plan_free(fides_ctx* c, fides_plan* plan) {
+    if (!c || !plan) return FIDES_BAD_ARG;
+    Guard g(c);
+    cudaStreamSynchronize(c->st);
+    if (plan->exec) cudaGraphExecDestroy(plan->exec);
+    if (plan->graph) cudaGraphDestroy(plan->graph);
+    for (auto& t : plan->inter)
+        if (t.buf) cudaFreeAsync(t.buf, c->st);
+    delete plan;
+    return FIDES_OK;
 }
 
 fides_status fides_ntt(fides_ctx* ctx, uint64_t* data, int prime0, int nlimbs, int inverse) {

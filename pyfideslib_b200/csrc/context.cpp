@@ -428,8 +428,11 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
 }
 
 fides_status ws_reserve(fides_ctx* c, Workspace& w, int cap) {
+    if (!w.st) w.st = c->st;
     if (w.base && w.cap >= cap) return FIDES_OK;
+    cudaStream_t keep = w.st;
     ws_free(w);
+    w.st = keep;
     const size_t L = c->L, K = c->K, N = c->N;
     w.dig_stride = L + K;
     const size_t limbs = 4 * L /*E0,E1,E2,XT*/ + c->dnum * w.dig_stride /*DIG*/ + 2 * (L + K) /*XB,XA*/ +
@@ -483,13 +486,14 @@ void free_context(fides_ctx* c) {
     c->st = nullptr;
 }
 
-fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level) {
+fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st) {
+    if (!st) st = c->st;
     if (ct->buf && ct->cap >= level + 1) return FIDES_OK;
-    if (ct->buf) cudaFreeAsync(ct->buf, c->st);
+    if (ct->buf) cudaFreeAsync(ct->buf, st);
     ct->buf = nullptr;
     ct->cap = level + 1;
     ct->ring = c->N;
-    if (cudaMallocAsync((void**)&ct->buf, 2 * (size_t)ct->cap * c->limb_bytes(), c->st) != cudaSuccess) {
+    if (cudaMallocAsync((void**)&ct->buf, 2 * (size_t)ct->cap * c->limb_bytes(), st) != cudaSuccess) {
         ct->cap = 0;
         cudaGetLastError();
         return set_err(c, FIDES_OOM, "ciphertext allocation failed");

@@ -54,6 +54,7 @@ struct SwitchKey {
 // Key-switch workspace for `cap` batch elements; element b's buffers sit at
 // the element-0 pointers + b*stride words.  Sized for the top level.
 struct Workspace {
+    cudaStream_t st = nullptr;  // stream the engine queues this workspace's work on
     uint64_t* base = nullptr;
     size_t stride = 0;  // words per element
     int cap = 0;
@@ -110,7 +111,7 @@ namespace fides {
 // helpers shared by api.cpp / client.cpp
 fides_status set_err(fides_ctx* c, fides_status s, const std::string& msg);
 fides_status check_cuda(fides_ctx* c, const char* where);
-fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level);
+fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st = nullptr);
 fides_status build_context(fides_ctx* c, const fides_params* p);
 bool select_moduli(const fides_params* prm, std::vector<uint64_t>& q, std::vector<uint64_t>& p);
 void free_context(fides_ctx* c);

@@ -1,5 +1,5 @@
 // engine.cpp -- the key-switching pipeline over a batch of nb <= kMaxBatch
-// elements at one level.  A single operation is a batch of one; batches
+// elements at one level, queued on the workspace's stream.  A single operation is a batch of one; batches
 // share every launch (blockIdx.z or an interleaved grid dimension), so wave
 // tails, launch overheads and, for HMult, switching-key reads are amortised.
 //
@@ -53,7 +53,7 @@ void special_intt(fides_ctx* c, Workspace& w, int level, int nb, bool with_top) 
             m.total += 1;
         }
     }
-    ntt_inverse(c->dev, m, -1, -1, c->st);
+    ntt_inverse(c->dev, m, -1, -1, w.st);
 }
 
 // ModDown of XB -> out0, XA -> out1 for every element, adding e0/e1 (E0/E1 of
@@ -71,7 +71,7 @@ void moddown_finish(fides_ctx* c, Workspace& w, int level, int nb, uint64_t* con
     md.ttop[0] = rescale ? w.T : nullptr;
     md.ttop[1] = rescale ? w.T + N : nullptr;
     md.bstride = w.stride;
-    launch_moddown_conv(c->dev, level, nb, md, c->st);
+    launch_moddown_conv(c->dev, level, nb, md, w.st);
     LimbMap m{};
     m.nb = nb;
     m.nseg = 2;
@@ -90,7 +90,7 @@ void moddown_finish(fides_ctx* c, Workspace& w, int level, int nb, uint64_t* con
         m.bout[0][b] = out0[b];
         m.bout[1][b] = out1[b];
     }
-    ntt_forward(c->dev, m, FL_PLAIN, rescale ? FS_MDRS : FS_MODDOWN, c->st);
+    ntt_forward(c->dev, m, FL_PLAIN, rescale ? FS_MDRS : FS_MODDOWN, w.st);
 }
 
 }  // namespace
@@ -98,7 +98,7 @@ void moddown_finish(fides_ctx* c, Workspace& w, int level, int nb, uint64_t* con
 // ModUp conversion + NTT of the digits, from the scaled coefficients in XT.
 static void modup_from_xt(fides_ctx* c, Workspace& w, int level, int nb) {
     const int n = level + 1, N = c->N;
-    launch_modup_conv(c->dev, level, nb, w.XT, w.DIG, w.dig_stride, w.stride, c->st);
+    launch_modup_conv(c->dev, level, nb, w.XT, w.DIG, w.dig_stride, w.stride, w.st);
     LimbMap dm{};
     dm.nb = nb;
     const int nd = level / c->alpha + 1;
@@ -111,7 +111,7 @@ static void modup_from_xt(fides_ctx* c, Workspace& w, int level, int nb) {
         dm.seg[dm.nseg++] = g;
         dm.total += g.count;
     }
-    ntt_forward(c->dev, dm, FL_PLAIN, FS_PLAIN, c->st);
+    ntt_forward(c->dev, dm, FL_PLAIN, FS_PLAIN, w.st);
 }
 
 void eng_modup(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* x) {
@@ -126,7 +126,7 @@ void eng_modup(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
             im.seg[im.nseg++] = seg_ws(x[done], w.XT + (size_t)done * w.stride, n, n, 0, level, 0);
             im.total += n;
         }
-        ntt_inverse(c->dev, im, IL_PLAIN, IS_MODUP, c->st);
+        ntt_inverse(c->dev, im, IL_PLAIN, IS_MODUP, w.st);
     }
     modup_from_xt(c, w, level, nb);
 }
@@ -146,13 +146,13 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
     ta.e1 = w.E1;
     ta.e2 = w.E2;
     ta.bstride = w.stride;
-    launch_tensor(c->dev, n, nb, ta, c->st);
+    launch_tensor(c->dev, n, nb, ta, w.st);
     // scaled INTT of E2 (workspace: batch dimension with the element stride)
     LimbMap im{};
     im.nb = nb;
     im.seg[im.nseg++] = seg_ws(w.E2, w.XT, n, n, 0, level, w.stride);
     im.total = n;
-    ntt_inverse(c->dev, im, IL_PLAIN, IS_MODUP, c->st);
+    ntt_inverse(c->dev, im, IL_PLAIN, IS_MODUP, w.st);
     modup_from_xt(c, w, level, nb);
     KsArgs ka{};
     for (int b = 0; b < nb; ++b) {
@@ -166,7 +166,7 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
     ka.dig_stride = w.dig_stride;
     ka.bstride = w.stride;
     ka.dig_bstride = w.stride;
-    launch_ks_inner(c->dev, level, nb, ka, true, c->st);
+    launch_ks_inner(c->dev, level, nb, ka, true, w.st);
     moddown_finish(c, w, level, nb, out0, out1, true, rescale && level > 0);
 }
 
@@ -192,7 +192,7 @@ void eng_rotate(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* c
     ka.dig_stride = w.dig_stride;
     ka.bstride = w.stride;
     ka.dig_bstride = hoisted ? 0 : w.stride;
-    launch_ks_inner(c->dev, level, nb, ka, false, c->st);
+    launch_ks_inner(c->dev, level, nb, ka, false, w.st);
     moddown_finish(c, w, level, nb, out0, out1, false, false);
 }
 

@@ -86,3 +86,32 @@ def test_hoisted_more_than_32_rotations():
         want = cc.EvalRotate(ct, idx[i]).download()
         got = outs[i].download()
         assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+def test_graph_plan_matches_eager_and_replays_new_inputs():
+    """Config-4 shape, scaled down: uneven levels, HMult+Relin+Rescale then one
+    rotation per pair, captured once and replayed."""
+    cc, oc = make_pair(12, 8, 3, 3)
+    kb, ka = rand_key(oc, 31)
+    cc.upload_relin_key(kb, ka)
+    rng = np.random.default_rng(9)
+    n = 12
+    levels = [int(x) for x in rng.integers(1, 8, size=n)]
+    idx = [int(x) for x in rng.integers(1, cc.N // 2, size=n)]
+    for i, r in enumerate(sorted(set(idx))):
+        cc.upload_galois_key(cc.rotation_galois(r), *rand_key(oc, 600 + 2 * i))
+    A = [cc.upload(*rand_ct(oc, lv, 7 * i)) for i, lv in enumerate(levels)]
+    B = [cc.upload(*rand_ct(oc, lv, 7 * i + 3)) for i, lv in enumerate(levels)]
+    plan, outs = cc.plan_hmult_rotate(A, B, idx, rescale=True)
+    for rep in range(2):
+        if rep == 1:  # new inputs through the same captured graph
+            for i, lv in enumerate(levels):
+                cc.write(A[i], *rand_ct(oc, lv, 999 + i))
+        plan.launch()
+        cc.Synchronize()
+        prod = cc.EvalMultBatch(A, B, rescale=True)
+        want = cc.EvalRotateBatch(prod, idx)
+        for i in range(n):
+            g0, g1 = outs[i].download()
+            w0, w1 = want[i].download()
+            assert np.array_equal(g0, w0) and np.array_equal(g1, w1), (rep, i)
