@@ -126,6 +126,99 @@ def cpu_baseline_hmult(max_seconds=30.0):
     return n / el, O.get_threads(), "%d HMult+Relin+Rescale at N=2^16 L=30 K=10 dnum=3 (%.1f s)" % (n, el)
 
 
+def measure_c4(cc, lib, st, n=256, reps=3, seed=4):
+    """Config 4: n pairs at levels uniform in 4..29 (5..30 limbs), HMult+Relin+
+    Rescale then one rotation by a random index in [1, 2^15) (one key per
+    pair), captured once as a CUDA graph and replayed; compared with the same
+    work through per-operation calls."""
+    import numpy as np
+    import torch
+
+    import pyfideslib_b200 as F
+
+    rng = np.random.default_rng(seed)
+    levels = [int(x) for x in rng.integers(4, 30, size=n)]
+    idx = [int(x) for x in rng.integers(1, 2 ** 15, size=n)]
+    sk = cc.KeyGen(seed=77, hamming_weight=192)
+    cc.EvalRotateKeyGen(sk, idx)
+    A = [cc.random_ct(lv, 2 * i + 1) for i, lv in enumerate(levels)]
+    B = [cc.random_ct(lv, 2 * i + 2) for i, lv in enumerate(levels)]
+    plan, outs = cc.plan_hmult_rotate(A, B, idx, rescale=True)
+    plan.launch()
+    cc.Synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        plan.launch()
+    e1.record(st)
+    e1.synchronize()
+    graph_ms = e0.elapsed_time(e1) / reps
+    # the same work, one operation per call
+    tmp = [F.Ciphertext(cc) for _ in range(n)]
+    outs2 = [F.Ciphertext(cc) for _ in range(n)]
+    for i in range(2):
+        cc.EvalRotate(cc.EvalMult(A[i], B[i], rescale=True, out=tmp[i]), idx[i], out=outs2[i])
+    cc.Synchronize()
+    e0.record(st)
+    for i in range(n):
+        cc.EvalMult(A[i], B[i], rescale=True, out=tmp[i])
+        cc.EvalRotate(tmp[i], idx[i], out=outs2[i])
+    e1.record(st)
+    e1.synchronize()
+    op_ms = e0.elapsed_time(e1)
+    same = all(np.array_equal(outs[i].download()[0], outs2[i].download()[0]) for i in (0, n // 2, n - 1))
+    del plan
+    return {"pairs": n, "levels": "uniform 4..29", "rotations": "one per pair, random index in [1, 2^15)",
+            "graph_ms": graph_ms, "graph_pairs_per_s": n / (graph_ms * 1e-3),
+            "per_op_ms": op_ms, "per_op_pairs_per_s": n / (op_ms * 1e-3), "results_equal": bool(same)}
+
+
+def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_streams=2):
+    """Poisson arrivals at each rate for `duration` seconds: 2/3 HMult+Relin+
+    Rescale, 1/3 Rotate on resident ciphertexts at random levels (the
+    bootstrap share of the mix is not served yet)."""
+    import numpy as np
+
+    import pyfideslib_b200 as F
+
+    rng = np.random.default_rng(seed)
+    pool = {}
+    for lv in (29, 22, 15, 8):
+        pool[lv] = [cc.random_ct(lv, 1000 * lv + i) for i in range(4)]
+    out = []
+    srv = F.Server(cc, hbm_budget=40 << 30, max_batch=max_batch, num_streams=num_streams)
+    for rate in rates:
+        srv.reset_stats()
+        reqs = []
+        t_end = time.perf_counter() + duration
+        t_next = time.perf_counter()
+        while True:
+            now = time.perf_counter()
+            if now >= t_end:
+                break
+            if now < t_next:
+                time.sleep(min(t_next - now, 0.002))
+                continue
+            t_next += float(rng.exponential(1.0 / rate))
+            lv = list(pool)[int(rng.integers(0, len(pool)))]
+            a = pool[lv][int(rng.integers(0, 4))]
+            if rng.uniform() < 2.0 / 3.0:
+                reqs.append(srv.submit(F.Server.HMULT, a, pool[lv][int(rng.integers(0, 4))]))
+            else:
+                reqs.append(srv.submit(F.Server.ROTATE, a, None, rot_indices[int(rng.integers(0, len(rot_indices)))]))
+        for rid, _ in reqs:
+            srv.wait(rid, 120.0)
+        st = srv.stats()
+        out.append({"rate": rate, "offered": len(reqs) / duration, "throughput": st["throughput"],
+                    "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_queue_ms": st["mean_queue_ms"],
+                    "batches": st["batches"], "completed": st["completed"]})
+        del reqs
+    srv.close()
+    return {"mix": "2/3 HMult+Relin+Rescale, 1/3 Rotate (EvalBootstrap share not served)",
+            "params": "N=2^16 L=30 K=10 dnum=3, levels 29/22/15/8", "streams": num_streams, "max_batch": max_batch,
+            "sweep": out}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -305,6 +398,15 @@ def run_ours(args):
     hbm, peak_kind = peaks()
     achieved = ntt_bytes / (ntt_ms * 1e-3) / 1e9
 
+    c4 = None
+    serving = None
+    if not args.no_c4:
+        c4 = measure_c4(cc, lib, st)
+    if not args.no_serve:
+        rot_idx = [1, 2, 4, 8, 16, 33]
+        cc.EvalRotateKeyGen(cc.KeyGen(seed=91, hamming_weight=192), rot_idx)
+        serving = {"continuous_batching": measure_serving(cc, [500.0, 2000.0], 2.0, rot_idx),
+                   "per_op": measure_serving(cc, [500.0, 2000.0], 2.0, rot_idx, max_batch=1, num_streams=1)}
     total = B * args.steps * world
     value = total / (ms * 1e-3)
     per_op_value = B * max(1, args.steps // 2) * world / (ms_op * 1e-3)
@@ -332,6 +434,8 @@ def run_ours(args):
                "ntt_gbs": achieved,
                "gpu_launches": int(launches),
                "autotune": autotune,
+               "batched_uneven_c4": c4,
+               "serving_c5": serving,
                "clocks": clk.summary(),
                "cpu_baseline": cpu}
         print(json.dumps(out), flush=True)
@@ -350,6 +454,8 @@ def main():
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the config-4 graph-plan measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -252,6 +252,9 @@ fides_status fides_encode(fides_ctx* ctx, const double* values, int slots, int l
 /* Encrypt with the secret key (symmetric CKKS encryption). */
 fides_status fides_encrypt(fides_ctx* ctx, const fides_sk* sk, const double* values, int slots, int level,
                            double scale, uint64_t seed, fides_ct** out);
+/* Synthetic ciphertext with residues drawn uniformly on the device (seeded):
+ * benchmark and test input without a host round trip. */
+fides_status fides_ct_random(fides_ctx* ctx, int level, uint64_t seed, fides_ct** out);
 /* Decrypt and decode into `slots` complex values (re, im interleaved). */
 fides_status fides_decrypt(fides_ctx* ctx, const fides_sk* sk, const fides_ct* ct, double* values, int slots);
 

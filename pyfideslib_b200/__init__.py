@@ -201,6 +201,11 @@ class CryptoContext:
                                   slots or self.N // 2, C.byref(h)), self._h)
         return Ciphertext(self, h.value)
 
+    def random_ct(self, level, seed):
+        h = vp()
+        check(lib.fides_ct_random(self._h, level, seed, C.byref(h)), self._h)
+        return Ciphertext(self, h.value)
+
     def upload_relin_key(self, b, a):
         check(lib.fides_key_upload_relin(self._h, _p(np.ascontiguousarray(b, dtype=np.uint64)),
                                          _p(np.ascontiguousarray(a, dtype=np.uint64))), self._h)

@@ -113,6 +113,7 @@ EXPORTS = {
     "fides_encode": ([vp, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_double, u64p], C.c_int),
     "fides_encrypt": ([vp, vp, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_double, u64, C.POINTER(vp)], C.c_int),
     "fides_decrypt": ([vp, vp, vp, C.POINTER(C.c_double), C.c_int], C.c_int),
+    "fides_ct_random": ([vp, C.c_int, u64, C.POINTER(vp)], C.c_int),
 }
 
 for _n, (_a, _r) in EXPORTS.items():

@@ -542,6 +542,29 @@ fides_status fides_encrypt_pk(fides_ctx* c, const fides_pk* pk, const double* va
     return check_cuda(c, "encrypt_pk");
 }
 
+fides_status fides_ct_random(fides_ctx* c, int level, uint64_t seed, fides_ct** out) {
+    if (!c || !out || level < 0 || level >= c->L) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    fides_ct* ct = new (std::nothrow) fides_ct();
+    if (!ct) return FIDES_OOM;
+    fides_status s = ct_reserve(c, ct, level);
+    if (s != FIDES_OK) {
+        delete ct;
+        return s;
+    }
+    const int N = c->N, n = level + 1;
+    count_launches(2);
+    k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c0(), N, 0, c->dev.pc, seed * 0x9E3779B97F4A7C15ull + 1);
+    k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c1(N), N, 0, c->dev.pc, seed * 0x9E3779B97F4A7C15ull + 2);
+    ct->level = level;
+    ct->scale = c->default_scale;
+    ct->noise_deg = 1;
+    ct->slots = N / 2;
+    *out = ct;
+    return check_cuda(c, "ct random");
+}
+
 fides_status fides_decrypt(fides_ctx* c, const fides_sk* sk, const fides_ct* ct, double* values, int slots) {
     if (!c || !sk || !sk->s || !ct || !ct->buf || !values || slots < 1 || slots > c->N / 2) return FIDES_BAD_ARG;
     std::lock_guard<std::recursive_mutex> lk(c->mu);
