@@ -173,10 +173,112 @@ def measure_c4(cc, lib, st, n=256, reps=3, seed=4):
             "per_op_ms": op_ms, "per_op_pairs_per_s": n / (op_ms * 1e-3), "results_equal": bool(same)}
 
 
-def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_streams=2):
-    """Poisson arrivals at each rate for `duration` seconds: 2/3 HMult+Relin+
-    Rescale, 1/3 Rotate on resident ciphertexts at random levels (the
-    bootstrap share of the mix is not served yet)."""
+def measure_c3(reps=5, seed=3):
+    """Config 3: N=2^16, 20 moduli (60 + 19 x 40-bit, scale 2^40), dnum=3, one
+    ciphertext; 32 hoisted rotations (+-2^k, k < 15, and 3, 5) sharing one
+    ModUp, and a 64-diagonal plaintext matrix (offsets 0..63, entries uniform
+    in [-1, 1]) applied by baby-step giant-step with 8 baby steps; the
+    transform's error is taken against the FP64 product."""
+    import numpy as np
+    import torch
+
+    import pyfideslib_b200 as F
+
+    cc = F.CryptoContext(log_n=16, num_q=20, dnum=3, qi_bits=40)
+    slots = cc.N // 2
+    rng = np.random.default_rng(seed)
+    idx = sorted({s * (1 << k) for k in range(15) for s in (1, -1)} | {3, 5})
+    offsets, bstep = list(range(64)), 8
+    sk = cc.KeyGen(seed=21, hamming_weight=192)
+    cc.EvalRotateKeyGen(sk, sorted(set(idx) | set(F.CryptoContext.linear_transform_rotations(offsets, bstep))))
+    x = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+    ct = cc.Encrypt(sk, x, slots=slots)
+    diags = {o: rng.uniform(-1, 1, slots) for o in offsets}
+    offs, pts = cc.prepare_linear_transform(diags, bstep, level=ct.level, slots=slots)
+    st = torch.cuda.ExternalStream(cc.stream_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        fn()
+        cc.Synchronize()
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    keep = [None]
+
+    def hoist():
+        keep[0] = cc.EvalFastRotation(ct, idx)
+
+    hoist_ms = timed(hoist)
+    lt_ms = timed(lambda: cc.EvalLinearTransform(ct, offs, pts, bstep, rescale=True))
+    y = cc.EvalLinearTransform(ct, offs, pts, bstep, rescale=True)
+    want = np.zeros(slots, dtype=np.complex128)
+    for o, d in diags.items():
+        want += d * np.roll(x, -o)
+    err = float(np.max(np.abs(cc.Decrypt(sk, y, slots=slots) - want)))
+    del keep
+    cc.close()
+    return {"params": "N=2^16 L=20 (60+19x40-bit) K=%d dnum=3, scale 2^40, level 19" % cc.K,
+            "hoisted_rotations": len(idx), "hoisted_ms": hoist_ms, "rotations_per_s": len(idx) / (hoist_ms * 1e-3),
+            "bsgs_diagonals": len(offs), "bsgs_baby_step": bstep, "bsgs_ms": lt_ms,
+            "bsgs_max_abs_err_vs_fp64": err}
+
+
+def measure_bootstrap(cc, reps=3, seed=101, degree=119):
+    """Config 5's bootstrap: N=2^16, L=30, dnum=3, full packing (2^15 slots),
+    sparse ternary secret h=32, level budget {3,3}, degree-119 Chebyshev
+    EvalMod with 3 double-angle steps.  Time of one EvalBootstrap (host
+    orchestration included, CUDA events on the context stream) and its
+    precision in bits against the FP64 message.  Returns (result, sk, inputs)."""
+    import numpy as np
+    import torch
+
+    sk = cc.KeyGen(seed=seed, hamming_weight=32)
+    cc.EvalMultKeyGen(sk)
+    t0 = time.perf_counter()
+    cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=degree)
+    cc.EvalBootstrapKeyGen(sk)
+    cc.Synchronize()
+    setup_s = time.perf_counter() - t0
+    out_level, rots = cc.bootstrap_info()
+    slots = cc.N // 2
+    rng = np.random.default_rng(seed)
+    msgs = [rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots) for _ in range(2)]
+    cts = [cc.Encrypt(sk, m, slots=slots, level=0, seed=7 + i) for i, m in enumerate(msgs)]
+    bt = cc.EvalBootstrap(cts[0])
+    cc.Synchronize()
+    st = torch.cuda.ExternalStream(cc.stream_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(st)
+    for r in range(reps):
+        bt = cc.EvalBootstrap(cts[r % 2])
+    e1.record(st)
+    e1.synchronize()
+    wall_ms = (time.perf_counter() - w0) * 1e3 / reps
+    ms = e0.elapsed_time(e1) / reps
+    got = cc.Decrypt(sk, bt, slots=slots)
+    err = float(np.max(np.abs(got - msgs[(reps - 1) % 2])))
+    res = {"bootstrap_ms": ms, "wall_ms": wall_ms, "precision_bits": -float(np.log2(err)), "max_abs_err": err,
+           "output_level": out_level, "rotation_keys": len(rots), "setup_s": setup_s,
+           "params": "N=2^16 L=30 K=%d dnum=3, 2^15 slots, h=32, budget {3,3}, Chebyshev degree %d, K=16, "
+                     "3 double-angle steps" % (cc.K, degree)}
+    return res, sk, cts
+
+
+def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_streams=2, boot_share=0.0,
+                    boot_inputs=None):
+    """Poisson arrivals at each rate for `duration` seconds on resident
+    ciphertexts at random levels: HMult+Relin+Rescale, Rotate and (share
+    `boot_share`) EvalBootstrap.  A waiter thread retires requests in arrival
+    order and drops their outputs, so device memory stays bounded by the
+    requests in flight."""
+    import queue
+
     import numpy as np
 
     import pyfideslib_b200 as F
@@ -187,9 +289,26 @@ def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_
         pool[lv] = [cc.random_ct(lv, 1000 * lv + i) for i in range(4)]
     out = []
     srv = F.Server(cc, hbm_budget=40 << 30, max_batch=max_batch, num_streams=num_streams)
-    for rate in rates:
+    p_rot = (1.0 - boot_share) / 3.0
+    # the first pass warms the server's pool and the output allocations; not reported
+    for k, rate in enumerate([rates[0]] + list(rates)):
         srv.reset_stats()
-        reqs = []
+        q = queue.Queue()
+        failures = []
+
+        def waiter():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                try:
+                    srv.wait(item[0], 300.0)
+                except Exception as e:  # reported, not raised from the thread
+                    failures.append(str(e))
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        n_sub = 0
         t_end = time.perf_counter() + duration
         t_next = time.perf_counter()
         while True:
@@ -200,23 +319,33 @@ def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_
                 time.sleep(min(t_next - now, 0.002))
                 continue
             t_next += float(rng.exponential(1.0 / rate))
-            lv = list(pool)[int(rng.integers(0, len(pool)))]
-            a = pool[lv][int(rng.integers(0, 4))]
-            if rng.uniform() < 2.0 / 3.0:
-                reqs.append(srv.submit(F.Server.HMULT, a, pool[lv][int(rng.integers(0, 4))]))
+            u = rng.uniform()
+            if u < boot_share:
+                q.put(srv.submit(F.Server.BOOTSTRAP, boot_inputs[int(rng.integers(0, len(boot_inputs)))]))
             else:
-                reqs.append(srv.submit(F.Server.ROTATE, a, None, rot_indices[int(rng.integers(0, len(rot_indices)))]))
-        for rid, _ in reqs:
-            srv.wait(rid, 120.0)
+                lv = list(pool)[int(rng.integers(0, len(pool)))]
+                a = pool[lv][int(rng.integers(0, 4))]
+                if u < 1.0 - p_rot:
+                    q.put(srv.submit(F.Server.HMULT, a, pool[lv][int(rng.integers(0, 4))]))
+                else:
+                    q.put(srv.submit(F.Server.ROTATE, a, None,
+                                     rot_indices[int(rng.integers(0, len(rot_indices)))]))
+            n_sub += 1
+        q.put(None)
+        th.join()
+        if failures:
+            raise RuntimeError("serving request failed: " + failures[0])
         st = srv.stats()
-        out.append({"rate": rate, "offered": len(reqs) / duration, "throughput": st["throughput"],
+        if k == 0:
+            continue
+        out.append({"rate": rate, "offered": n_sub / duration, "throughput": st["throughput"],
                     "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_queue_ms": st["mean_queue_ms"],
                     "batches": st["batches"], "completed": st["completed"]})
-        del reqs
     srv.close()
-    return {"mix": "2/3 HMult+Relin+Rescale, 1/3 Rotate (EvalBootstrap share not served)",
-            "params": "N=2^16 L=30 K=10 dnum=3, levels 29/22/15/8", "streams": num_streams, "max_batch": max_batch,
-            "sweep": out}
+    mix = "%.0f%% HMult+Relin+Rescale, %.0f%% Rotate, %.0f%% EvalBootstrap" % (
+        100 * (1 - boot_share - p_rot), 100 * p_rot, 100 * boot_share)
+    return {"mix": mix, "params": "N=2^16 L=30 K=10 dnum=3, levels 29/22/15/8 (bootstrap inputs at level 0)",
+            "streams": num_streams, "max_batch": max_batch, "sweep": out}
 
 
 def run_reference(args):
@@ -377,22 +506,28 @@ def run_ours(args):
     ms_op, _ = timed(step_per_op, max(1, args.steps // 2), 2)
     ms_e2e, _ = timed(step_e2e, max(1, args.steps // 2), 1)
 
-    # roofline: forward NTT over 30 limbs (2 kernels), resident, > L2 traffic per launch is 31 MB
-    nl = 30
-    buf = torch.empty((4, nl, N), dtype=torch.int64, device="cuda")
-    bp = [buf[i].data_ptr() for i in range(4)]
-    for i in range(4):
-        lib.fides_ntt(cc._h, bp[i], 0, nl, 1)  # any residues < p work; inverse first keeps them canonical
+    # roofline: forward NTT over 30 limbs (2 kernels) cycling through 10
+    # resident polynomials (157 MB > L2), algorithmic traffic 31.5 MB per launch
+    nl, nbuf = 30, 10
+    # values below 2^40 are canonical residues of every modulus
+    buf = torch.randint(0, 2 ** 40, (nbuf, nl, N), dtype=torch.int64, device="cuda")
+    bp = [buf[i].data_ptr() for i in range(nbuf)]
     reps = 40
+    for r in range(nbuf):
+        lib.fides_ntt(cc._h, bp[r], 0, nl, 0)
     cc.Synchronize()
+    # the region between the profiler marks is what an ncu capture started with
+    # --profile-from-start off sees (no effect otherwise)
+    torch.cuda.profiler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(st):
         e0.record(st)
     for r in range(reps):
-        lib.fides_ntt(cc._h, bp[r % 4], 0, nl, 0)
+        lib.fides_ntt(cc._h, bp[r % nbuf], 0, nl, 0)
     with torch.cuda.stream(st):
         e1.record(st)
     e1.synchronize()
+    torch.cuda.profiler.stop()
     ntt_ms = e0.elapsed_time(e1) / reps
     ntt_bytes = 16.0 * N * nl
     hbm, peak_kind = peaks()
@@ -400,13 +535,31 @@ def run_ours(args):
 
     c4 = None
     serving = None
+    c3 = None
     if not args.no_c4:
         c4 = measure_c4(cc, lib, st)
+    boot = None
+    boot_sk, boot_cts = None, None
+    if not args.no_boot:
+        boot, boot_sk, boot_cts = measure_bootstrap(cc)
     if not args.no_serve:
         rot_idx = [1, 2, 4, 8, 16, 33]
-        cc.EvalRotateKeyGen(cc.KeyGen(seed=91, hamming_weight=192), rot_idx)
-        serving = {"continuous_batching": measure_serving(cc, [500.0, 2000.0], 2.0, rot_idx),
-                   "per_op": measure_serving(cc, [500.0, 2000.0], 2.0, rot_idx, max_batch=1, num_streams=1)}
+        cc.EvalRotateKeyGen(boot_sk or cc.KeyGen(seed=91, hamming_weight=192), rot_idx)
+        rates = [1000.0, 3000.0, 5000.0]
+        serving = {"hmult_rotate": {
+            "continuous_batching": measure_serving(cc, rates, 2.0, rot_idx, max_batch=8, num_streams=3),
+            "per_op": measure_serving(cc, rates, 2.0, rot_idx, max_batch=1, num_streams=1)}}
+        if boot is not None:
+            # rates at 20 / 40 / 70% of the bootstrap lane's capacity
+            cap = 1.0 / (0.1 * boot["bootstrap_ms"] * 1e-3)
+            brates = [round(f * cap, 1) for f in (0.2, 0.4, 0.7)]
+            serving["c5_mix_with_bootstrap"] = {
+                "continuous_batching": measure_serving(cc, brates, 4.0, rot_idx, max_batch=8, num_streams=3,
+                                                       boot_share=0.1, boot_inputs=boot_cts),
+                "per_op": measure_serving(cc, brates, 4.0, rot_idx, max_batch=1, num_streams=1, boot_share=0.1,
+                                          boot_inputs=boot_cts)}
+    if not args.no_c3:
+        c3 = measure_c3()
     total = B * args.steps * world
     value = total / (ms * 1e-3)
     per_op_value = B * max(1, args.steps // 2) * world / (ms_op * 1e-3)
@@ -435,6 +588,8 @@ def run_ours(args):
                "gpu_launches": int(launches),
                "autotune": autotune,
                "batched_uneven_c4": c4,
+               "hoisted_bsgs_c3": c3,
+               "bootstrap_c5": boot,
                "serving_c5": serving,
                "clocks": clk.summary(),
                "cpu_baseline": cpu}
@@ -456,6 +611,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the config-4 graph-plan measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--no-c3", action="store_true", help="skip the config-3 hoisted/BSGS measurement")
+    ap.add_argument("--no-boot", action="store_true", help="skip the bootstrap measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -158,6 +158,19 @@ fides_status fides_plan_hmult_rotate(fides_ctx* ctx, int n, const fides_ct* cons
                                      const int32_t* indices, int rescale, fides_ct* const* out, fides_plan** plan);
 fides_status fides_plan_launch(fides_ctx* ctx, fides_plan* plan);
 fides_status fides_plan_free(fides_ctx* ctx, fides_plan* plan);
+/* Diagonal-form plaintext matrix times ciphertext, baby-step giant-step:
+ *   out = sum_k pt_k' (.) Rot(x, offsets[k])
+ * computed as  sum_g Rot( sum_{b} pts[k] (.) Rot(x, b), g*bstep )  with
+ * offsets[k] = g*bstep + b, g = floor(offsets[k] / bstep), 0 <= b < bstep.
+ * pts[k] must hold diagonal k pre-rotated by g*bstep slots (slot j holds
+ * diag_k[j - g*bstep]), encoded at x's level or above.  Baby steps share one
+ * hoisted ModUp, each giant's inner sum is one fused dot-product launch, the
+ * giant rotations are one batched key switch.  Rescales when `rescale` != 0.
+ * Rotation keys: every nonzero b and every nonzero g*bstep.
+ * Reference: LinearTransform (CKKS/LinearTransform.cu:67-258) with
+ * dotProductPt_ (CKKS/ElemenwiseBatchKernels.cu:651). */
+fides_status fides_linear_transform(fides_ctx* ctx, const fides_ct* x, int n, const int32_t* offsets,
+                                    const fides_pt* const* pts, int bstep, int rescale, fides_ct* out);
 /* EvalConjugate: Ciphertext::conjugate, Ciphertext.cpp:933 */
 fides_status fides_conjugate(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
 /* Apply an automorphism whose key was uploaded with fides_key_upload_galois */
@@ -172,6 +185,43 @@ fides_status fides_mult_pt(fides_ctx* ctx, const fides_ct* a, const fides_pt* p,
 /* EvalAdd(ct, double) / EvalMult(ct, double): Ciphertext::addScalar / multScalar */
 fides_status fides_add_scalar(fides_ctx* ctx, const fides_ct* a, double v, fides_ct* out);
 fides_status fides_mult_scalar(fides_ctx* ctx, const fides_ct* a, double v, fides_ct* out, int rescale);
+
+/* Integer scalar product out = z * a (value times z, scale kept): multIntScalar,
+ * src/CKKS/ApproxModEval.cu (multIntScalar). */
+fides_status fides_mult_int(fides_ctx* ctx, const fides_ct* a, int64_t z, fides_ct* out);
+/* Multiplication by the monomial X^power (0 <= power < 2N): Ciphertext::multMonomial,
+ * used by src/CKKS/Bootstrap.cu:268 and ApproxModEval.cu.  X^(N/2) multiplies every
+ * slot by i. */
+fides_status fides_mult_monomial(fides_ctx* ctx, const fides_ct* a, uint32_t power, fides_ct* out);
+/* ModRaise: limb 0 of a (mod q_0), lifted to (-q_0/2, q_0/2] and re-expressed
+ * over all L ciphertext moduli (level L-1): src/CKKS/Bootstrap.cu:380. */
+fides_status fides_mod_raise(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
+/* EvalChebyshevSeries (api/CryptoContext.hpp:171-173, src/CKKS/ApproxModEval.cu:370):
+ * sum_k coeffs[k] T_k(y), y = (2x - (lo + hi)) / (hi - lo), degree <= 2047.
+ * Consumes ceil(log2(degree + 1)) + 1 levels (+1 when [lo, hi] != [-1, 1]). */
+fides_status fides_chebyshev_series(fides_ctx* ctx, const fides_ct* a, const double* coeffs, int degree, double lo,
+                                    double hi, fides_ct* out);
+
+/* ---- bootstrapping (api/CryptoContext.hpp:80-82,180-181 EvalBootstrapSetup /
+ *      EvalBootstrapKeyGen / EvalBootstrap; src/CKKS/Bootstrap.cu:169-320) ---- */
+typedef struct {
+    int slots;           /* N/2 (full packing; 0 means N/2) */
+    int level_budget[2]; /* levels of CoeffsToSlots and SlotsToCoeffs (0 means 3) */
+    int cheb_degree;     /* degree of the EvalMod Chebyshev series (0 means 119) */
+    double K;            /* EvalMod input range [-K, K] in units of q_0 (0 means 16) */
+    int double_angle;    /* double-angle iterations (0 means 3) */
+} fides_boot_params;
+/* Precompute the CoeffsToSlots / SlotsToCoeffs diagonals (device-resident)
+ * and the EvalMod series.  The keys it needs: relinearisation, conjugation
+ * and the rotations listed by fides_bootstrap_info. */
+fides_status fides_bootstrap_setup(fides_ctx* ctx, const fides_boot_params* params);
+/* Output level of a bootstrapped ciphertext and the rotation indices the
+ * bootstrap needs keys for (rotations may be NULL to query the count). */
+fides_status fides_bootstrap_info(fides_ctx* ctx, int slots, int* output_level, int* num_rotations,
+                                  int32_t* rotations);
+/* EvalBootstrap: refresh a ciphertext (only its limb 0 is read) to the
+ * output level, same slots and message. */
+fides_status fides_bootstrap(fides_ctx* ctx, const fides_ct* in, fides_ct* out);
 
 /* ---- serving: continuous batching over one context (no counterpart in the
  *      reference, which has no serving layer) ---- */

@@ -14,7 +14,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._capi import FidesError, FidesParams, SrvStats, check, lib, u64p, vp
+from ._capi import BootParams, FidesError, FidesParams, SrvStats, check, lib, u64p, vp
 
 __all__ = ["CryptoContext", "Ciphertext", "Plaintext", "PrivateKey", "Server", "Plan", "FidesError", "lib"]
 
@@ -91,10 +91,10 @@ class Plan:
 
 
 class Server:
-    """Continuous-batching request loop (fides_srv_*): submit HMult / Rotate
-    requests from any thread, wait on request ids, read p50 / p99."""
+    """Continuous-batching request loop (fides_srv_*): submit HMult / Rotate /
+    Bootstrap requests from any thread, wait on request ids, read p50 / p99."""
 
-    HMULT, ROTATE = 0, 1
+    HMULT, ROTATE, BOOTSTRAP = 0, 1, 2
 
     def __init__(self, ctx, hbm_budget, max_batch=16, num_streams=2):
         self.ctx = ctx
@@ -187,6 +187,12 @@ class CryptoContext:
 
     def primes(self):
         return self.q + self.p
+
+    def stream_ptr(self):
+        """The context's CUDA stream (cudaStream_t as an int)."""
+        h = vp()
+        check(lib.fides_ctx_stream(self._h, C.byref(h)), self._h)
+        return h.value
 
     def Synchronize(self):
         check(lib.fides_ctx_synchronize(self._h), self._h)
@@ -374,6 +380,90 @@ class CryptoContext:
         hs = (vp * len(outs))(*[o._h for o in outs])
         check(lib.fides_rotate_hoisted(self._h, a._h, len(indices), arr, hs), self._h)
         return outs
+
+    # ---- scalar / monomial / polynomial evaluation ----
+    def EvalMultInt(self, a, z, out=None):
+        """a times the integer z (scale kept)."""
+        out = self._out(out)
+        check(lib.fides_mult_int(self._h, a._h, int(z), out._h), self._h)
+        return out
+
+    def EvalMultMonomial(self, a, power, out=None):
+        out = self._out(out)
+        check(lib.fides_mult_monomial(self._h, a._h, int(power) % (2 * self.N), out._h), self._h)
+        return out
+
+    def ModRaise(self, a, out=None):
+        out = self._out(out)
+        check(lib.fides_mod_raise(self._h, a._h, out._h), self._h)
+        return out
+
+    def EvalChebyshevSeries(self, a, coeffs, lo=-1.0, hi=1.0, out=None):
+        out = self._out(out)
+        cf = np.ascontiguousarray(coeffs, dtype=np.float64)
+        check(lib.fides_chebyshev_series(self._h, a._h, cf.ctypes.data_as(C.POINTER(C.c_double)), len(cf) - 1,
+                                         float(lo), float(hi), out._h), self._h)
+        return out
+
+    # ---- bootstrapping (EvalBootstrapSetup / EvalBootstrapKeyGen / EvalBootstrap) ----
+    def EvalBootstrapSetup(self, level_budget=(3, 3), slots=None, cheb_degree=119, K=16.0, double_angle=3):
+        prm = BootParams()
+        prm.slots = slots or self.N // 2
+        prm.level_budget[0], prm.level_budget[1] = level_budget
+        prm.cheb_degree, prm.K, prm.double_angle = cheb_degree, K, double_angle
+        check(lib.fides_bootstrap_setup(self._h, C.byref(prm)), self._h)
+
+    def bootstrap_info(self, slots=None):
+        lv, n = C.c_int(), C.c_int()
+        check(lib.fides_bootstrap_info(self._h, slots or self.N // 2, C.byref(lv), C.byref(n), None), self._h)
+        rot = (C.c_int32 * max(1, n.value))()
+        check(lib.fides_bootstrap_info(self._h, slots or self.N // 2, None, None, rot), self._h)
+        return lv.value, [int(rot[i]) for i in range(n.value)]
+
+    def EvalBootstrapKeyGen(self, sk, slots=None, seed=11):
+        _, rots = self.bootstrap_info(slots)
+        self.EvalRotateKeyGen(sk, rots, slots=slots, seed=seed)
+        self.EvalConjugateKeyGen(sk, seed=seed + 1)
+
+    def EvalBootstrap(self, a, out=None):
+        out = self._out(out)
+        check(lib.fides_bootstrap(self._h, a._h, out._h), self._h)
+        return out
+
+    # ---- diagonal-form linear transforms (baby-step giant-step) ----
+    @staticmethod
+    def linear_transform_rotations(offsets, bstep):
+        """Rotation indices a BSGS transform over `offsets` needs keys for."""
+        need = set()
+        for o in offsets:
+            g = o // bstep
+            b = o - g * bstep
+            if b:
+                need.add(b)
+            if g:
+                need.add(g * bstep)
+        return sorted(need)
+
+    def prepare_linear_transform(self, diags, bstep, level=None, slots=None, scale=None):
+        """Encode the diagonals {offset: vector of `slots` values} of a slot
+        matrix M (M[i, (i + offset) % slots] = diags[offset][i]) as the
+        plaintexts EvalLinearTransform consumes: diagonal o = g*bstep + b is
+        pre-rotated by g*bstep slots."""
+        slots = slots or self.N // 2
+        offs = sorted(diags)
+        pts = []
+        for o in offs:
+            g = o // bstep
+            v = np.roll(np.asarray(diags[o], dtype=np.complex128), g * bstep)
+            pts.append(self.MakeCKKSPackedPlaintext(v, level=level, slots=slots, scale=scale))
+        return offs, pts
+
+    def EvalLinearTransform(self, x, offsets, pts, bstep, rescale=True, out=None):
+        out = self._out(out)
+        n = len(offsets)
+        check(lib.fides_linear_transform(self._h, x._h, n, (C.c_int32 * n)(*offsets),
+                                         (vp * n)(*[p._h for p in pts]), bstep, int(rescale), out._h), self._h)
+        return out
 
     def EvalConjugate(self, a, out=None):
         out = self._out(out)

@@ -37,6 +37,11 @@ class FidesParams(C.Structure):
                 ("device", C.c_int), ("default_scale", C.c_double)]
 
 
+class BootParams(C.Structure):
+    _fields_ = [("slots", C.c_int), ("level_budget", C.c_int * 2), ("cheb_degree", C.c_int), ("K", C.c_double),
+                ("double_angle", C.c_int)]
+
+
 def _sig(name, args, res=C.c_int):
     f = getattr(lib, name)
     f.argtypes = args
@@ -90,6 +95,14 @@ EXPORTS = {
     "fides_negate": ([vp, vp, vp], C.c_int),
     "fides_add_pt": ([vp, vp, vp, vp], C.c_int),
     "fides_mult_pt": ([vp, vp, vp, vp, C.c_int], C.c_int),
+    "fides_mult_int": ([vp, vp, C.c_int64, vp], C.c_int),
+    "fides_mult_monomial": ([vp, vp, C.c_uint32, vp], C.c_int),
+    "fides_mod_raise": ([vp, vp, vp], C.c_int),
+    "fides_chebyshev_series": ([vp, vp, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp], C.c_int),
+    "fides_bootstrap_setup": ([vp, C.POINTER(BootParams)], C.c_int),
+    "fides_bootstrap_info": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), i32p], C.c_int),
+    "fides_bootstrap": ([vp, vp, vp], C.c_int),
+    "fides_linear_transform": ([vp, vp, C.c_int, i32p, C.POINTER(vp), C.c_int, C.c_int, vp], C.c_int),
     "fides_add_scalar": ([vp, vp, C.c_double, vp], C.c_int),
     "fides_mult_scalar": ([vp, vp, C.c_double, vp, C.c_int], C.c_int),
     "fides_srv_create": ([vp, C.c_size_t, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),

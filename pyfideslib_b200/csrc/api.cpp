@@ -4,7 +4,9 @@
 // downloads synchronise.  Every result is computed into a fresh buffer from
 // the stream-ordered pool and then swapped into the output object, so an
 // output may alias an input.
+#include <algorithm>
 #include <cmath>
+#include <map>
 #include <cstring>
 #include <new>
 
@@ -792,6 +794,227 @@ fides_status fides_rotate_batch(fides_ctx* c, int n, const fides_ct* const* a, c
         out[i]->slots = meta.slots;
     }
     return check_cuda(c, "rotate_batch");
+}
+
+// out = z * a (integer z), both components, level and scale of a.
+fides_status fides_mult_int(fides_ctx* c, const fides_ct* a, int64_t z, fides_ct* out) {
+    if (!c || !valid_ct(c, a) || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int n = a->level + 1, N = c->N;
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, a->level);
+    if (s != FIDES_OK) return s;
+    for (int j0 = 0; j0 < n; j0 += kMaxLinLimbs) {
+        const int nl = std::min(kMaxLinLimbs, n - j0);
+        LinArgs la{};
+        la.n = 1;
+        la.q0 = j0;
+        la.in0[0] = a->c0() + (size_t)j0 * N;
+        la.in1[0] = a->c1(N) + (size_t)j0 * N;
+        la.out0 = tmp.c0() + (size_t)j0 * N;
+        la.out1 = tmp.c1(N) + (size_t)j0 * N;
+        uint64_t zz[kMaxPrimes][2];
+        int_const_limbs(c, z, n, zz);
+        for (int j = 0; j < nl; ++j) {
+            la.z[0][j][0] = zz[j0 + j][0];
+            la.z[0][j][1] = zz[j0 + j][1];
+        }
+        launch_lincomb(c->dev, nl, la, c->st);
+    }
+    const fides_ct meta = *a;
+    commit(c, out, tmp);
+    out->level = meta.level;
+    out->scale = meta.scale;
+    out->noise_deg = meta.noise_deg;
+    out->slots = meta.slots;
+    return check_cuda(c, "mult_int");
+}
+
+fides_status fides_mult_monomial(fides_ctx* c, const fides_ct* a, uint32_t power, fides_ct* out) {
+    if (!c || !valid_ct(c, a) || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int N = c->N;
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, a->level);
+    if (s != FIDES_OK) return s;
+    launch_mult_monomial(c->dev, a->level + 1, a->c0(), a->c1(N), tmp.c0(), tmp.c1(N), power % (2u * (uint32_t)N),
+                         c->st);
+    const fides_ct meta = *a;
+    commit(c, out, tmp);
+    out->level = meta.level;
+    out->scale = meta.scale;
+    out->noise_deg = meta.noise_deg;
+    out->slots = meta.slots;
+    return check_cuda(c, "mult_monomial");
+}
+
+// ModRaise: the residues of limb 0 (mod q_0), lifted to (-q_0/2, q_0/2] in
+// coefficient form, reduced modulo every ciphertext modulus and transformed
+// back: one INTT of 2 limbs, one forward NTT of 2L limbs whose prologue does
+// the centred lift (the SwitchModulus of the rescale with source prime q_0).
+fides_status fides_mod_raise(fides_ctx* c, const fides_ct* a, fides_ct* out) {
+    if (!c || !valid_ct(c, a) || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int N = c->N, top = c->L - 1;
+    fides_ct tmp;
+    fides_status s = ct_reserve(c, &tmp, top);
+    if (s != FIDES_OK) return s;
+    LimbMap t{};
+    t.nseg = 2;
+    const uint64_t* ins[2] = {a->c0(), a->c1(N)};
+    for (int i = 0; i < 2; ++i) {
+        LimbSeg& g2 = t.seg[i];
+        g2.in = ins[i];
+        g2.out = c->ws1.T + (size_t)i * N;
+        g2.count = 1;
+        g2.skip_lo = 1;
+        g2.nq = 1;
+        g2.q0 = 0;
+        g2.level = 0;
+        t.total += 1;
+    }
+    ntt_inverse(c->dev, t, IL_PLAIN, IS_PLAIN, c->st);
+    LimbMap m{};
+    m.nseg = 2;
+    uint64_t* os[2] = {tmp.c0(), tmp.c1(N)};
+    for (int i = 0; i < 2; ++i) {
+        LimbSeg& g2 = m.seg[i];
+        g2.in = c->ws1.T + (size_t)i * N;
+        g2.in_stride_zero = 1;
+        g2.out = os[i];
+        g2.count = top + 1;
+        g2.skip_lo = top + 1;
+        g2.nq = top + 1;
+        g2.q0 = 0;
+        g2.level = 0;  // source prime of the centred lift
+        m.total += top + 1;
+    }
+    ntt_forward(c->dev, m, FL_SWITCHMOD, FS_PLAIN, c->st);
+    const fides_ct meta = *a;
+    commit(c, out, tmp);
+    out->level = top;
+    out->scale = meta.scale;
+    out->noise_deg = meta.noise_deg;
+    out->slots = meta.slots;
+    return check_cuda(c, "mod_raise");
+}
+
+// Offsets split as o = g*bstep + b with g = floor(o / bstep), 0 <= b < bstep.
+static int floor_div(int a, int b) {
+    int q = a / b;
+    if ((a % b) != 0 && ((a < 0) != (b < 0))) --q;
+    return q;
+}
+
+namespace {
+// Temporary ciphertexts released on the context stream when the call ends.
+struct CtTemps {
+    fides_ctx* c;
+    std::vector<fides_ct*> v;
+    fides_ct* make() {
+        v.push_back(new fides_ct());
+        return v.back();
+    }
+    ~CtTemps() {
+        for (fides_ct* t : v) {
+            if (t->buf) cudaFreeAsync(t->buf, c->st);
+            delete t;
+        }
+    }
+};
+}  // namespace
+
+fides_status fides_linear_transform(fides_ctx* c, const fides_ct* x, int n, const int32_t* offsets,
+                                    const fides_pt* const* pts, int bstep, int rescale, fides_ct* out) {
+    if (!c || !valid_ct(c, x) || n < 1 || !offsets || !pts || bstep < 1 || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int level = x->level, nl = level + 1, N = c->N;
+    for (int k = 0; k < n; ++k)
+        if (!pts[k] || !pts[k]->m || pts[k]->level < level) return FIDES_BAD_ARG;
+    std::vector<int> baby(n);
+    std::vector<int32_t> babies;
+    std::map<int, std::vector<int>> groups;  // giant step -> terms
+    for (int k = 0; k < n; ++k) {
+        const int gs = floor_div(offsets[k], bstep);
+        baby[k] = offsets[k] - gs * bstep;
+        if (baby[k] && std::find(babies.begin(), babies.end(), baby[k]) == babies.end()) babies.push_back(baby[k]);
+        groups[gs].push_back(k);
+    }
+    CtTemps tmp{c, {}};
+    std::map<int, const fides_ct*> bct;
+    bct[0] = x;
+    fides_status s = FIDES_OK;
+    if (!babies.empty()) {
+        std::vector<fides_ct*> outs;
+        for (size_t i = 0; i < babies.size(); ++i) outs.push_back(tmp.make());
+        s = fides_rotate_hoisted(c, x, (int)babies.size(), babies.data(), outs.data());
+        if (s != FIDES_OK) return s;
+        for (size_t i = 0; i < babies.size(); ++i) bct[babies[i]] = outs[i];
+    }
+    const double sc = x->scale * pts[0]->scale;
+    const int nd = x->noise_deg + pts[0]->noise_deg, sl = x->slots;
+    fides_ct* acc = tmp.make();
+    bool have_acc = false;
+    std::vector<const fides_ct*> inner;
+    std::vector<int32_t> gidx;
+    for (auto& kv : groups) {
+        const int gs = kv.first;
+        const std::vector<int>& ks = kv.second;
+        fides_ct* dst = gs == 0 ? acc : tmp.make();
+        s = ct_reserve(c, dst, level);
+        if (s != FIDES_OK) return s;
+        for (size_t k0 = 0; k0 < ks.size(); k0 += kMaxBatch) {
+            DotArgs d{};
+            d.n = (int)std::min(ks.size() - k0, (size_t)kMaxBatch);
+            d.accumulate = k0 > 0;
+            for (int j = 0; j < d.n; ++j) {
+                const fides_ct* b = bct[baby[ks[k0 + j]]];
+                d.c0[j] = b->c0();
+                d.c1[j] = b->c1(N);
+                d.p[j] = pts[ks[k0 + j]]->m;
+            }
+            d.o0 = dst->c0();
+            d.o1 = dst->c1(N);
+            launch_dot_pt(c->dev, nl, d, c->st);
+        }
+        dst->level = level;
+        dst->scale = sc;
+        dst->noise_deg = nd;
+        dst->slots = sl;
+        if (gs == 0) {
+            have_acc = true;
+        } else {
+            inner.push_back(dst);
+            gidx.push_back(gs * bstep);
+        }
+    }
+    if (!inner.empty()) {
+        std::vector<fides_ct*> rot;
+        for (size_t i = 0; i < inner.size(); ++i) rot.push_back(tmp.make());
+        s = fides_rotate_batch(c, (int)inner.size(), inner.data(), gidx.data(), rot.data());
+        if (s != FIDES_OK) return s;
+        size_t i0 = 0;
+        if (!have_acc) {
+            s = ct_reserve(c, acc, level);
+            if (s != FIDES_OK) return s;
+            const size_t bytes = (size_t)nl * c->limb_bytes();
+            cudaMemcpyAsync(acc->c0(), rot[0]->c0(), bytes, cudaMemcpyDeviceToDevice, c->st);
+            cudaMemcpyAsync(acc->c1(N), rot[0]->c1(N), bytes, cudaMemcpyDeviceToDevice, c->st);
+            i0 = 1;
+        }
+        for (size_t i = i0; i < rot.size(); ++i) {
+            launch_elementwise(c->dev, EW_ADD, nl, 0, acc->c0(), rot[i]->c0(), acc->c0(), c->st);
+            launch_elementwise(c->dev, EW_ADD, nl, 0, acc->c1(N), rot[i]->c1(N), acc->c1(N), c->st);
+        }
+    }
+    commit(c, out, *acc);
+    out->level = level;
+    out->scale = sc;
+    out->noise_deg = nd;
+    out->slots = sl;
+    s = check_cuda(c, "linear_transform");
+    if (s == FIDES_OK && rescale && level > 0) s = fides_rescale(c, out, out);
+    return s;
 }
 
 }  // extern "C"

@@ -344,6 +344,38 @@ class CryptoContextImpl<DCRTPoly> {
         check(fides_conjugate(ctx, a->handle, o->handle), ctx);
         return o;
     }
+    // EvalChebyshevSeries (api/CryptoContext.hpp:171-173)
+    Ciphertext<DCRTPoly> EvalChebyshevSeries(const Ciphertext<DCRTPoly>& a, const std::vector<double>& coeffs,
+                                             double lo, double hi) {
+        auto o = empty();
+        check(fides_chebyshev_series(ctx, prepare(a)->handle, coeffs.data(), (int)coeffs.size() - 1, lo, hi,
+                                     o->handle),
+              ctx);
+        return o;
+    }
+    // EvalBootstrapSetup / EvalBootstrapKeyGen / EvalBootstrap (api/CryptoContext.hpp:80-82,180-181)
+    void EvalBootstrapSetup(const std::vector<uint32_t>& levelBudget = {3, 3}, const std::vector<uint32_t>& = {0, 0},
+                            uint32_t numSlots = 0) {
+        fides_boot_params bp{};
+        bp.slots = (int)(numSlots ? numSlots : slots);
+        bp.level_budget[0] = levelBudget.size() > 0 ? (int)levelBudget[0] : 3;
+        bp.level_budget[1] = levelBudget.size() > 1 ? (int)levelBudget[1] : 3;
+        check(fides_bootstrap_setup(ctx, &bp), ctx);
+    }
+    void EvalBootstrapKeyGen(const PrivateKey<DCRTPoly>& sk, uint32_t numSlots = 0) {
+        const int s = (int)(numSlots ? numSlots : slots);
+        int n = 0;
+        check(fides_bootstrap_info(ctx, s, nullptr, &n, nullptr), ctx);
+        std::vector<int32_t> rot(n);
+        check(fides_bootstrap_info(ctx, s, nullptr, nullptr, rot.data()), ctx);
+        check(fides_keygen_rotations(ctx, sk->handle, n, rot.data(), s, seed++), ctx);
+        check(fides_keygen_conjugate(ctx, sk->handle, seed++), ctx);
+    }
+    Ciphertext<DCRTPoly> EvalBootstrap(const Ciphertext<DCRTPoly>& a) {
+        auto o = empty();
+        check(fides_bootstrap(ctx, prepare(a)->handle, o->handle), ctx);
+        return o;
+    }
     static void SetLevel(Ciphertext<DCRTPoly>& ct, size_t level) {
         int L = 0;
         fides_ctx_info(ct->ctx, nullptr, &L, nullptr, nullptr, nullptr, nullptr);

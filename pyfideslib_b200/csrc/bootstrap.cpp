@@ -1,0 +1,632 @@
+// bootstrap.cpp -- CKKS bootstrapping and Chebyshev series evaluation over the
+// evaluation core.
+//
+// Reference flow (src/CKKS/Bootstrap.cu:169-320 Bootstrap, :380 ModRaise;
+// src/CKKS/CoeffsToSlots.cu:26,161 EvalCoeffsToSlots / EvalLinearTransform;
+// src/CKKS/ApproxModEval.cu:24-93 approxModReduction, :370 evalChebyshevSeries,
+// :747 applyDoubleAngleIterations):
+//   ModRaise -> CoeffsToSlots -> split into real and imaginary parts with the
+//   conjugation -> approximate modular reduction (Chebyshev series of a scaled
+//   cosine, then double-angle iterations) on both parts -> recombine ->
+//   SlotsToCoeffs.
+//
+// Formulation used here (own derivation, checked numerically in the tests):
+//   * After ModRaise the polynomial is p = D*mu + q0*I with small integers I.
+//     Declaring its scale K*q0 makes the slot values of CoeffsToSlots
+//     t = (D*mu/q0 + I)/K in [-1, 1]; one integer multiply + rescale then
+//     brings the scale near the 2^50 moduli without touching t (exact: the
+//     multiplier is an integer and the scale is tracked).
+//   * Decoding of n = N/2 slots is the special FFT  z = A_logn ... A_1 P_br w
+//     (w_k = p_k + i p_{k+n}, P_br the bit reversal, A_s a butterfly stage with
+//     diagonals 0, +-2^(s-1) and twiddles zeta^(5^j mod 2^(s+2))).
+//     CoeffsToSlots applies A_1^-1 ... A_logn^-1 (output in bit-reversed
+//     order), SlotsToCoeffs applies A_logn ... A_1 to that order, so the bit
+//     reversal never has to be applied.  Stages are merged into `level
+//     budget` groups; each group is one diagonal-form matrix applied by
+//     baby-step giant-step (fides_linear_transform), one level each.
+//   * EvalMod evaluates g(t) = cos(2 pi (K t - 1/4) / 2^r) by its Chebyshev
+//     interpolant on [-1, 1], then r double-angle steps c <- 2c^2 - 1 give
+//     sin(2 pi K t) = sin(2 pi D mu / q0) ~ 2 pi D mu / q0; the factor
+//     q0 / (2 pi D) is folded into the first SlotsToCoeffs group.
+//   * The Chebyshev series is evaluated by recursive splitting
+//     p = T_n Q + R (T_{n+k} = 2 T_n T_k - T_{n-k}) down to leaves of degree
+//     < 8, which are integer linear combinations of T_1..T_7 computed in one
+//     launch and one rescale.  Every product lands on a target level and
+//     scale chosen top-down, so no operand ever needs a scale correction
+//     beyond the integer rounding of its multiplier (relative 2^-50).
+// Real and imaginary parts run in lockstep: every HMult of the series is one
+// batched call over both.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <map>
+#include <memory>
+#include <new>
+
+#include "context.hpp"
+
+using namespace fides;
+using cplx = std::complex<double>;
+
+namespace fides {
+
+struct BootStage {
+    int level = 0;
+    int bstep = 1;
+    std::vector<int32_t> offsets;
+    std::vector<fides_pt*> pts;
+};
+
+struct BootPrecomp {
+    fides_ctx* c = nullptr;
+    int slots = 0;
+    double K = 16.0;
+    int double_angle = 3;
+    int degree = 119;
+    std::vector<double> cheb;
+    std::vector<BootStage> cts, stc;
+    int level_after_cts = 0, level_after_mod = 0, level_out = 0;
+    std::vector<int32_t> rotations;
+    ~BootPrecomp() {
+        for (auto* v : {&cts, &stc})
+            for (auto& s : *v)
+                for (fides_pt* p : s.pts) {
+                    if (p && p->m) cudaFree(p->m);
+                    delete p;
+                }
+    }
+};
+
+}  // namespace fides
+
+namespace {
+
+struct Guard {
+    std::lock_guard<std::recursive_mutex> lk;
+    explicit Guard(fides_ctx* c) : lk(c->mu) { cudaSetDevice(c->device); }
+};
+
+int floor_div(int a, int b) {
+    int q = a / b;
+    if ((a % b) != 0 && ((a < 0) != (b < 0))) --q;
+    return q;
+}
+
+// (x mod p) of a real value rounded to the nearest integer, |x| < 2^126.
+uint64_t real_mod(long double x, uint64_t p) {
+    const bool neg = x < 0;
+    long double a = floorl((neg ? -x : x) + 0.5L);
+    const unsigned __int128 big = (unsigned __int128)a;
+    const uint64_t r = (uint64_t)(big % p);
+    return neg ? (r ? p - r : 0) : r;
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal-form slot matrices: (M x)[i] = sum_o d_o[i] x[(i + o) mod n].
+// ---------------------------------------------------------------------------
+using Diag = std::map<int, std::vector<cplx>>;
+
+// Butterfly stage s (block length 2^s) of the special FFT or its inverse.
+Diag fft_stage(int n, int s, bool inverse) {
+    const int len = 1 << s, h = len >> 1, lenq = len << 2;
+    Diag d;
+    auto& d0 = d[0];
+    d0.assign(n, 0.0);
+    std::vector<cplx> dp(n, 0.0), dm(n, 0.0), tw(h);
+    uint64_t g = 1;  // 5^j mod 4*len
+    for (int j = 0; j < h; ++j) {
+        const double ang = 2.0 * M_PI * (double)g / (double)lenq;
+        tw[j] = cplx(cos(ang), sin(ang));
+        g = (g * 5) % (uint64_t)lenq;
+    }
+    for (int p = 0; p < n; ++p) {
+        const int jj = p & (len - 1);
+        const int j = jj < h ? jj : jj - h;
+        const cplx t = tw[j];
+        if (jj < h) {
+            d0[p] += inverse ? 0.5 : 1.0;
+            dp[p] += inverse ? cplx(0.5) : t;
+        } else {
+            dm[p] += inverse ? 1.0 / (2.0 * t) : cplx(1.0);
+            d0[p] += inverse ? -1.0 / (2.0 * t) : -t;
+        }
+    }
+    auto acc = [&](int off, const std::vector<cplx>& v) {
+        auto& t = d[((off % n) + n) % n];
+        if (t.empty()) t.assign(n, 0.0);
+        for (int i = 0; i < n; ++i) t[i] += v[i];
+    };
+    acc(h, dp);
+    acc(-h, dm);
+    return d;
+}
+
+// A * B (B applied first).
+Diag diag_mul(int n, const Diag& A, const Diag& B) {
+    Diag C;
+    for (const auto& a : A)
+        for (const auto& b : B) {
+            auto& t = C[(a.first + b.first) % n];
+            if (t.empty()) t.assign(n, 0.0);
+            for (int i = 0; i < n; ++i) t[i] += a.second[i] * b.second[(i + a.first) % n];
+        }
+    for (auto it = C.begin(); it != C.end();) {
+        double mx = 0;
+        for (const cplx& v : it->second) mx = std::max(mx, std::abs(v));
+        it = mx < 1e-300 ? C.erase(it) : std::next(it);
+    }
+    return C;
+}
+
+// Stage groups: `budget` contiguous groups of the logn butterfly stages,
+// sizes as equal as possible.
+std::vector<std::vector<int>> stage_groups(int logn, int budget, bool descending) {
+    budget = std::max(1, std::min(budget, logn));
+    std::vector<std::vector<int>> g(budget);
+    int s = descending ? logn : 1;
+    for (int b = 0; b < budget; ++b) {
+        const int cnt = logn / budget + (b < logn % budget ? 1 : 0);
+        for (int k = 0; k < cnt; ++k) {
+            g[b].push_back(s);
+            s += descending ? -1 : 1;
+        }
+    }
+    return g;
+}
+
+fides_status encode_stage(fides_ctx* c, int n, const Diag& M, int level, double factor, BootStage& st) {
+    st.level = level;
+    // offsets centred in (-n/2, n/2]; baby step ~ sqrt(#diagonals) in units of
+    // the smallest offset step
+    std::vector<int> offs;
+    int unit = n;
+    for (const auto& kv : M) {
+        int o = kv.first > n / 2 ? kv.first - n : kv.first;
+        offs.push_back(o);
+        if (o) unit = std::min(unit, std::abs(o) & -std::abs(o));
+    }
+    if (unit == n) unit = 1;
+    const int nd = (int)offs.size();
+    int bk = 1;
+    while (bk * bk < nd) bk <<= 1;
+    st.bstep = bk * unit;
+    const double scale = (double)c->host.prime[level];
+    std::vector<double> vals(2 * (size_t)n);
+    for (int o : offs) {
+        const auto& d = M.at(((o % n) + n) % n);
+        const int G = floor_div(o, st.bstep) * st.bstep;
+        for (int j = 0; j < n; ++j) {
+            const cplx v = d[(size_t)((((j - G) % n) + n) % n)] * factor;
+            vals[2 * (size_t)j] = v.real();
+            vals[2 * (size_t)j + 1] = v.imag();
+        }
+        fides_pt* pt = new (std::nothrow) fides_pt();
+        if (!pt) return FIDES_OOM;
+        pt->cap = level + 1;
+        if (cudaMalloc((void**)&pt->m, (size_t)pt->cap * c->limb_bytes()) != cudaSuccess) {
+            cudaGetLastError();
+            delete pt;
+            return set_err(c, FIDES_OOM, "bootstrap plaintext");
+        }
+        st.pts.push_back(pt);
+        st.offsets.push_back(o);
+        fides_status s = encode_dev(c, vals.data(), n, level, scale, pt->m);
+        if (s != FIDES_OK) return s;
+        pt->level = level;
+        pt->scale = scale;
+        pt->noise_deg = 1;
+        pt->slots = n;
+    }
+    return FIDES_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Lockstep ciphertext arithmetic with exact (level, scale) bookkeeping.
+// ---------------------------------------------------------------------------
+constexpr int kBaby = 8;
+
+using Lanes = std::vector<fides_ct*>;
+
+class Arith {
+   public:
+    fides_ctx* c;
+    fides_status st = FIDES_OK;
+    explicit Arith(fides_ctx* cc) : c(cc) {}
+    ~Arith() {
+        for (fides_ct* t : owned) {
+            if (t->buf) cudaFreeAsync(t->buf, c->st);
+            delete t;
+        }
+    }
+    Arith(const Arith&) = delete;
+    Arith& operator=(const Arith&) = delete;
+
+    Lanes fresh(size_t nl) {
+        Lanes v;
+        for (size_t i = 0; i < nl; ++i) {
+            owned.push_back(new fides_ct());
+            v.push_back(owned.back());
+        }
+        return v;
+    }
+    bool ok() const { return st == FIDES_OK; }
+
+    // HMult + relinearisation + rescale, all lanes in one batched call
+    Lanes mul(const Lanes& a, const Lanes& b) {
+        Lanes o = fresh(a.size());
+        if (ok()) st = fides_hmult_batch(c, (int)a.size(), a.data(), b.data(), o.data(), 1);
+        return o;
+    }
+
+    // sum_k z_k x_k + cst (at the result's scale) on limbs 0..level, integer
+    // z_k, no rescale; the x_k carry the result's scale (that of the first)
+    Lanes ilin(const std::vector<std::pair<const Lanes*, int64_t>>& terms, double cst, int level) {
+        const size_t nl = terms[0].first->size();
+        Lanes o = fresh(nl);
+        for (size_t l = 0; l < nl && ok(); ++l) {
+            const double sc = (*terms[0].first)[l]->scale;
+            std::vector<const fides_ct*> xs;
+            for (size_t k = 0; k < terms.size(); ++k) {
+                int_const_limbs(c, terms[k].second, level + 1, zbuf[k]);
+                xs.push_back((*terms[k].first)[l]);
+            }
+            if ((st = ct_reserve(c, o[l], level)) != FIDES_OK) break;
+            launch(xs, level, (long double)cst * sc, o[l]);
+            meta(o[l], level, sc, xs[0]->slots);
+        }
+        return o;
+    }
+
+    // sum_k c_k x_k + cst with real c_k, landing on (level - 1, target) after
+    // one rescale: x_k of any scale s_k is multiplied by the integer
+    // round(c_k * target * q_level / s_k), the constant enters as
+    // round(cst * target * q_level).  `like` gives the lanes and slots.
+    Lanes lin(const std::vector<std::pair<const Lanes*, double>>& terms, double cst, int level, double target,
+              const Lanes& like) {
+        Lanes o = fresh(like.size());
+        const long double tq = (long double)target * (long double)c->host.prime[level];
+        for (size_t l = 0; l < like.size() && ok(); ++l) {
+            std::vector<const fides_ct*> xs;
+            for (size_t k = 0; k < terms.size(); ++k) {
+                const fides_ct* x = (*terms[k].first)[l];
+                const long double z = (long double)terms[k].second * tq / (long double)x->scale;
+                if (!(fabsl(z) < 4.0e18L)) {
+                    st = set_err(c, FIDES_BAD_ARG, "coefficient too large for the ciphertext scale");
+                    return o;
+                }
+                int_const_limbs(c, (int64_t)llroundl(z), level + 1, zbuf[k]);
+                xs.push_back(x);
+            }
+            if ((st = ct_reserve(c, o[l], level)) != FIDES_OK) break;
+            launch(xs, level, (long double)cst * tq, o[l]);
+            meta(o[l], level, (double)tq, like[l]->slots);
+            if ((st = fides_rescale(c, o[l], o[l])) != FIDES_OK) break;
+            o[l]->scale = target;
+        }
+        return o;
+    }
+
+    Lanes monomial(const Lanes& a, uint32_t k) {
+        Lanes o = fresh(a.size());
+        for (size_t l = 0; l < a.size() && ok(); ++l) st = fides_mult_monomial(c, a[l], k, o[l]);
+        return o;
+    }
+
+   private:
+    std::vector<fides_ct*> owned;
+    uint64_t zbuf[kMaxLin][kMaxPrimes][2];
+
+    static void meta(fides_ct* o, int level, double scale, int slots) {
+        o->level = level;
+        o->scale = scale;
+        o->noise_deg = 1;
+        o->slots = slots;
+    }
+    // one lincomb launch per chunk of kMaxLinLimbs limbs, constants from zbuf
+    void launch(const std::vector<const fides_ct*>& xs, int level, long double add_value, fides_ct* out) {
+        const int N = c->N, n = level + 1;
+        for (int j0 = 0; j0 < n; j0 += kMaxLinLimbs) {
+            const int nlb = std::min(kMaxLinLimbs, n - j0);
+            LinArgs la{};
+            la.n = (int)xs.size();
+            la.q0 = j0;
+            for (size_t k = 0; k < xs.size(); ++k) {
+                la.in0[k] = xs[k]->c0() + (size_t)j0 * N;
+                la.in1[k] = xs[k]->c1(N) + (size_t)j0 * N;
+                for (int j = 0; j < nlb; ++j) {
+                    la.z[k][j][0] = zbuf[k][j0 + j][0];
+                    la.z[k][j][1] = zbuf[k][j0 + j][1];
+                }
+            }
+            la.has_add = add_value != 0;
+            for (int j = 0; j < nlb && la.has_add; ++j) la.add0[j] = real_mod(add_value, c->host.prime[j0 + j]);
+            la.out0 = out->c0() + (size_t)j0 * N;
+            la.out1 = out->c1(N) + (size_t)j0 * N;
+            launch_lincomb(c->dev, nlb, la, c->st);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Chebyshev series  sum_k c_k T_k(x),  x in [-1, 1]
+// ---------------------------------------------------------------------------
+class Chebyshev {
+   public:
+    Chebyshev(Arith& a, const Lanes& x, int degree) : A(a), deg(degree) {
+        T[1] = x;
+        lvl[1] = x[0]->level;
+        lvl[0] = 1 << 30;
+    }
+
+    // levels of T_k if built (dry run: no GPU work)
+    static std::map<int, int> plan_levels(int top, int degree) {
+        std::map<int, int> L;
+        L[1] = top;
+        auto need = [&](auto&& self, int k) -> int {
+            auto it = L.find(k);
+            if (it != L.end()) return it->second;
+            int v = (k % 2 == 0) ? self(self, k / 2) - 1 : std::min(self(self, k / 2), self(self, k / 2 + 1)) - 1;
+            L[k] = v;
+            return v;
+        };
+        for (int k = 1; k < std::min(kBaby, degree + 1); ++k) need(need, k);
+        for (int n = kBaby; n <= degree; n <<= 1) need(need, n);
+        return L;
+    }
+    // highest level at which the series of degree d can be delivered
+    static int feasible(const std::map<int, int>& L, int d) {
+        if (d < kBaby) {
+            int m = 1 << 30;
+            for (int k = 1; k <= d; ++k) m = std::min(m, L.at(k));
+            return m - 1;
+        }
+        int n = kBaby;
+        while (2 * n <= d) n <<= 1;
+        return std::min({L.at(n) - 1, feasible(L, d - n) - 1, feasible(L, n - 1)});
+    }
+
+    Lanes eval(const std::vector<double>& coeffs, int level, double scale) { return rec(coeffs, level, scale); }
+
+   private:
+    Arith& A;
+    int deg;
+    std::map<int, Lanes> T;
+    std::map<int, int> lvl;
+
+    const Lanes& get(int k) {
+        auto it = T.find(k);
+        if (it != T.end()) return it->second;
+        Lanes r;
+        if (k % 2 == 0) {
+            const Lanes& h = get(k / 2);
+            Lanes sq = A.mul(h, h);
+            // 2 T_{k/2}^2 - 1
+            r = A.ilin({{&sq, 2}}, -1.0, sq[0]->level);
+        } else {
+            const Lanes& a = get(k / 2);
+            const Lanes& b = get(k / 2 + 1);
+            Lanes p = A.mul(a, b);
+            // T_1 brought to the product's (level, scale)
+            Lanes t1 = A.lin({{&T[1], 1.0}}, 0.0, p[0]->level + 1, p[0]->scale, p);
+            r = A.ilin({{&p, 2}, {&t1, -1}}, 0.0, p[0]->level);
+        }
+        T[k] = r;
+        return T[k];
+    }
+
+    Lanes rec(const std::vector<double>& c, int level, double scale) {
+        const int d = (int)c.size() - 1;
+        if (d < kBaby) {
+            std::vector<std::pair<const Lanes*, double>> terms;
+            for (int k = 1; k <= d; ++k)
+                if (c[k] != 0.0) terms.push_back({&get(k), c[k]});
+            return A.lin(terms, c[0], level + 1, scale, T[1]);
+        }
+        int n = kBaby;
+        while (2 * n <= d) n <<= 1;
+        std::vector<double> q(d - n + 1), r(c.begin(), c.begin() + n);
+        q[0] = c[n];
+        for (int k = 1; k <= d - n; ++k) {
+            q[k] = 2.0 * c[n + k];
+            r[n - k] -= c[n + k];
+        }
+        const Lanes& Tn = get(n);
+        const double sq = scale * (double)A.c->host.prime[level + 1] / Tn[0]->scale;
+        Lanes Q = rec(q, level + 1, sq);
+        Lanes P = A.mul(Tn, Q);
+        Lanes R = rec(r, level, scale);
+        return A.ilin({{&P, 1}, {&R, 1}}, 0.0, level);
+    }
+};
+
+std::vector<double> cheb_coeffs(int degree, double K, int r) {
+    const int m = degree + 1;
+    std::vector<double> fx(m), c(m, 0.0);
+    for (int j = 0; j < m; ++j) {
+        const double x = cos(M_PI * (j + 0.5) / m);
+        fx[j] = cos(2.0 * M_PI * (K * x - 0.25) / (double)(1 << r));
+    }
+    for (int k = 0; k < m; ++k) {
+        double s = 0;
+        for (int j = 0; j < m; ++j) s += fx[j] * cos(M_PI * k * (j + 0.5) / m);
+        c[k] = 2.0 * s / m;
+    }
+    c[0] *= 0.5;
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+fides_status fides_chebyshev_series(fides_ctx* c, const fides_ct* a, const double* coeffs, int degree, double lo,
+                                    double hi, fides_ct* out) {
+    if (!c || !a || !a->buf || !coeffs || degree < 0 || degree > 2047 || !(hi > lo) || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    if (!c->has_relin) return set_err(c, FIDES_KEY_MISSING, "no relinearisation key");
+    Arith A(c);
+    Lanes x = {const_cast<fides_ct*>(a)};
+    std::vector<double> cf(coeffs, coeffs + degree + 1);
+    int top = a->level;
+    if (lo != -1.0 || hi != 1.0) {
+        // y = (2x - (lo + hi)) / (hi - lo): one rescale
+        if (top < 1) return FIDES_BAD_ARG;
+        x = A.lin({{&x, 2.0 / (hi - lo)}}, -(lo + hi) / (hi - lo), top, a->scale, x);
+        top -= 1;
+    }
+    if (!A.ok()) return A.st;
+    const auto L = Chebyshev::plan_levels(top, degree);
+    const int lv = Chebyshev::feasible(L, degree);
+    if (lv < 0) return set_err(c, FIDES_BAD_ARG, "not enough levels for the Chebyshev series");
+    Chebyshev ch(A, x, degree);
+    Lanes y = ch.eval(cf, lv, a->scale);
+    if (!A.ok()) return A.st;
+    fides_status s = fides_ct_copy(c, y[0], out);
+    if (s == FIDES_OK) out->slots = a->slots;
+    return s;
+}
+
+fides_status fides_bootstrap_setup(fides_ctx* c, const fides_boot_params* prm) {
+    if (!c || !prm) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int n = prm->slots > 0 ? prm->slots : c->N / 2;
+    if (n != c->N / 2) return set_err(c, FIDES_UNSUPPORTED, "bootstrapping is implemented for full packing (N/2 slots)");
+    int logn = 0;
+    while ((1 << logn) < n) ++logn;
+    auto bp = std::make_shared<BootPrecomp>();
+    bp->c = c;
+    bp->slots = n;
+    bp->K = prm->K > 0 ? prm->K : 16.0;
+    bp->double_angle = prm->double_angle > 0 ? prm->double_angle : 3;
+    bp->degree = prm->cheb_degree > 0 ? prm->cheb_degree : 119;
+    bp->cheb = cheb_coeffs(bp->degree, bp->K, bp->double_angle);
+    const int bc = prm->level_budget[0] > 0 ? prm->level_budget[0] : 3;
+    const int bs = prm->level_budget[1] > 0 ? prm->level_budget[1] : 3;
+    const int top = c->L - 1;
+    // levels: ModRaise at top, scale-down to top-1, CoeffsToSlots, EvalMod, SlotsToCoeffs
+    const auto gc = stage_groups(logn, bc, true);
+    const auto gs = stage_groups(logn, bs, false);
+    bp->level_after_cts = top - 1 - (int)gc.size();
+    const auto Lv = Chebyshev::plan_levels(bp->level_after_cts, bp->degree);
+    const int after_cheb = Chebyshev::feasible(Lv, bp->degree);
+    bp->level_after_mod = after_cheb - bp->double_angle;
+    bp->level_out = bp->level_after_mod - (int)gs.size();
+    if (bp->level_out < 0)
+        return set_err(c, FIDES_BAD_ARG, "not enough levels for bootstrapping (need " +
+                                             std::to_string(top - bp->level_out) + " of " + std::to_string(top) + ")");
+    // CoeffsToSlots: A_1^-1 ... A_logn^-1, highest stages applied first
+    for (size_t b = 0; b < gc.size(); ++b) {
+        Diag M;
+        M[0] = std::vector<cplx>(n, 1.0);
+        for (int s : gc[b]) M = diag_mul(n, fft_stage(n, s, true), M);
+        BootStage st;
+        fides_status e = encode_stage(c, n, M, top - 1 - (int)b, 1.0, st);
+        bp->cts.push_back(std::move(st));
+        if (e != FIDES_OK) return e;
+    }
+    // SlotsToCoeffs: A_logn ... A_1, with q0 / (2 pi D) in the first group
+    const double fac = (double)c->host.prime[0] / (2.0 * M_PI * c->default_scale);
+    for (size_t b = 0; b < gs.size(); ++b) {
+        Diag M;
+        M[0] = std::vector<cplx>(n, 1.0);
+        for (int s : gs[b]) M = diag_mul(n, fft_stage(n, s, false), M);
+        BootStage st;
+        fides_status e = encode_stage(c, n, M, bp->level_after_mod - (int)b, b == 0 ? fac : 1.0, st);
+        bp->stc.push_back(std::move(st));
+        if (e != FIDES_OK) return e;
+    }
+    std::vector<int32_t> rot;
+    for (auto* v : {&bp->cts, &bp->stc})
+        for (auto& st : *v)
+            for (int o : st.offsets) {
+                const int G = floor_div(o, st.bstep) * st.bstep, b = o - G;
+                for (int r : {b, G})
+                    if (r && std::find(rot.begin(), rot.end(), r) == rot.end()) rot.push_back(r);
+            }
+    std::sort(rot.begin(), rot.end());
+    bp->rotations = rot;
+    c->boot[n] = bp;
+    return check_cuda(c, "bootstrap setup");
+}
+
+fides_status fides_bootstrap_info(fides_ctx* c, int slots, int* output_level, int* num_rotations, int32_t* rotations) {
+    if (!c) return FIDES_BAD_ARG;
+    Guard g(c);
+    auto it = c->boot.find(slots > 0 ? slots : c->N / 2);
+    if (it == c->boot.end()) return set_err(c, FIDES_BAD_ARG, "bootstrapping not set up for these slots");
+    const BootPrecomp& b = *it->second;
+    if (output_level) *output_level = b.level_out;
+    if (num_rotations) *num_rotations = (int)b.rotations.size();
+    if (rotations) std::copy(b.rotations.begin(), b.rotations.end(), rotations);
+    return FIDES_OK;
+}
+
+fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
+    if (!c || !in || !in->buf || !out) return FIDES_BAD_ARG;
+    Guard g(c);
+    const int n = in->slots > 0 ? in->slots : c->N / 2;
+    auto it = c->boot.find(n);
+    if (it == c->boot.end()) return set_err(c, FIDES_BAD_ARG, "bootstrapping not set up for these slots");
+    const BootPrecomp& B = *it->second;
+    if (!c->has_relin) return set_err(c, FIDES_KEY_MISSING, "no relinearisation key");
+    const int top = c->L - 1, N = c->N;
+    const double d_in = in->scale;
+    Arith A(c);
+    Lanes x = A.fresh(1);
+    fides_status s = fides_mod_raise(c, in, x[0]);
+    if (s != FIDES_OK) return s;
+    x[0]->scale = B.K * (double)c->host.prime[0];
+    x[0]->slots = n;
+    // integer multiply + rescale: scale K q0 -> about the default scale, values unchanged
+    x = A.lin({{&x, 1.0}}, 0.0, top, c->default_scale, x);
+    if (!A.ok()) return A.st;
+    for (const BootStage& st : B.cts) {
+        Lanes y = A.fresh(1);
+        s = fides_linear_transform(c, x[0], (int)st.offsets.size(), st.offsets.data(),
+                                   (const fides_pt* const*)st.pts.data(), st.bstep, 1, y[0]);
+        if (s != FIDES_OK) return s;
+        x = y;
+    }
+    // real and imaginary parts: (x + conj x), -i (x - conj x), each twice the part
+    Lanes cj = A.fresh(1);
+    if ((s = fides_conjugate(c, x[0], cj[0])) != FIDES_OK) return s;
+    Lanes re = A.ilin({{&x, 1}, {&cj, 1}}, 0.0, x[0]->level);
+    Lanes df = A.ilin({{&x, 1}, {&cj, -1}}, 0.0, x[0]->level);
+    Lanes im = A.monomial(df, 3u * (uint32_t)N / 2u);
+    if (!A.ok()) return A.st;
+    re[0]->scale *= 2.0;
+    im[0]->scale *= 2.0;
+    Lanes v = {re[0], im[0]};
+    {
+        const auto Lv = Chebyshev::plan_levels(v[0]->level, B.degree);
+        const int lv = Chebyshev::feasible(Lv, B.degree);
+        Chebyshev ch(A, v, B.degree);
+        v = ch.eval(B.cheb, lv, v[0]->scale);
+        for (int r = 0; r < B.double_angle && A.ok(); ++r) {
+            Lanes sq = A.mul(v, v);
+            v = A.ilin({{&sq, 2}}, -1.0, sq[0]->level);
+        }
+    }
+    if (!A.ok()) return A.st;
+    if (v[0]->level != B.level_after_mod) return set_err(c, FIDES_CUDA_ERR, "bootstrap level plan mismatch");
+    Lanes y0 = {v[0]}, y1 = {v[1]};
+    Lanes iy = A.monomial(y1, (uint32_t)N / 2u);
+    Lanes w = A.ilin({{&y0, 1}, {&iy, 1}}, 0.0, v[0]->level);
+    if (!A.ok()) return A.st;
+    for (const BootStage& st : B.stc) {
+        Lanes y = A.fresh(1);
+        s = fides_linear_transform(c, w[0], (int)st.offsets.size(), st.offsets.data(),
+                                   (const fides_pt* const*)st.pts.data(), st.bstep, 1, y[0]);
+        if (s != FIDES_OK) return s;
+        w = y;
+    }
+    const double sc = w[0]->scale * d_in / c->default_scale;
+    s = fides_ct_copy(c, w[0], out);
+    if (s != FIDES_OK) return s;
+    out->scale = sc;
+    out->slots = in->slots;
+    out->noise_deg = 1;
+    return check_cuda(c, "bootstrap");
+}
+
+}  // extern "C"

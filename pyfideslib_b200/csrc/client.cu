@@ -229,6 +229,21 @@ fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg
 
 }  // namespace
 
+fides_status fides::encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm) {
+    const int N = c->N;
+    std::vector<double> m = embed_inverse(N, values, slots);
+    std::vector<int64_t> v(N);
+    for (int i = 0; i < N; ++i) {
+        const double x = m[i] * scale;
+        if (!(fabs(x) < 9.0e18)) return set_err(c, FIDES_BAD_ARG, "encoded coefficient exceeds 2^63");
+        v[i] = llround(x);
+    }
+    fides_status s = upload_small(c, v, dm, 0, level + 1);
+    if (s != FIDES_OK) return s;
+    ntt_forward(c->dev, map_single(dm, dm, level + 1, level + 1, 0), FL_PLAIN, FS_PLAIN, c->st);
+    return check_cuda(c, "encode");
+}
+
 extern "C" {
 
 fides_status fides_keygen(fides_ctx* c, uint64_t seed, int hamming_weight, fides_sk** out) {
@@ -355,20 +370,6 @@ fides_status fides_key_export(fides_ctx* c, uint32_t galois, uint64_t* b, uint64
     return check_cuda(c, "key export");
 }
 
-static fides_status encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm) {
-    const int N = c->N;
-    std::vector<double> m = embed_inverse(N, values, slots);
-    std::vector<int64_t> v(N);
-    for (int i = 0; i < N; ++i) {
-        const double x = m[i] * scale;
-        if (!(fabs(x) < 9.0e18)) return set_err(c, FIDES_BAD_ARG, "encoded coefficient exceeds 2^63");
-        v[i] = llround(x);
-    }
-    fides_status s = upload_small(c, v, dm, 0, level + 1);
-    if (s != FIDES_OK) return s;
-    ntt_forward(c->dev, map_single(dm, dm, level + 1, level + 1, 0), FL_PLAIN, FS_PLAIN, c->st);
-    return check_cuda(c, "encode");
-}
 
 fides_status fides_encode(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* m) {
     if (!c || !values || !m || slots < 1 || slots > c->N / 2 || (slots & (slots - 1)) || level < 0 || level >= c->L)

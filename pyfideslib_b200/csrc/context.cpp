@@ -471,6 +471,7 @@ void free_context(fides_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
+    c->boot.clear();
     auto freek = [](SwitchKey& k) {
         if (k.b) cudaFree(k.b);
         k.b = k.a = nullptr;
@@ -486,14 +487,28 @@ void free_context(fides_ctx* c) {
     c->st = nullptr;
 }
 
-fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st) {
+void int_const_limbs(const fides_ctx* c, int64_t z, int nlimbs, uint64_t (*out)[2]) {
+    const uint64_t mag = z < 0 ? (uint64_t)(-(z + 1)) + 1 : (uint64_t)z;
+    for (int j = 0; j < nlimbs; ++j) {
+        const uint64_t p = c->host.prime[j];
+        uint64_t r = mag % p;
+        if (z < 0 && r) r = p - r;
+        out[j][0] = r;
+        out[j][1] = shoup_precompute(r, p);
+    }
+}
+
+fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st, cudaMemPool_t pool) {
     if (!st) st = c->st;
     if (ct->buf && ct->cap >= level + 1) return FIDES_OK;
     if (ct->buf) cudaFreeAsync(ct->buf, st);
     ct->buf = nullptr;
     ct->cap = level + 1;
     ct->ring = c->N;
-    if (cudaMallocAsync((void**)&ct->buf, 2 * (size_t)ct->cap * c->limb_bytes(), st) != cudaSuccess) {
+    const size_t bytes = 2 * (size_t)ct->cap * c->limb_bytes();
+    const cudaError_t e = pool ? cudaMallocFromPoolAsync((void**)&ct->buf, bytes, pool, st)
+                               : cudaMallocAsync((void**)&ct->buf, bytes, st);
+    if (e != cudaSuccess) {
         ct->cap = 0;
         cudaGetLastError();
         return set_err(c, FIDES_OOM, "ciphertext allocation failed");

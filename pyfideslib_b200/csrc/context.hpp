@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -77,6 +78,8 @@ uint64_t mulmod(uint64_t a, uint64_t b, uint64_t p);
 uint64_t invmod(uint64_t a, uint64_t p);
 bool is_prime(uint64_t n);
 
+struct BootPrecomp;  // bootstrap.cpp
+
 }  // namespace fides
 
 struct fides_ctx {
@@ -99,6 +102,9 @@ struct fides_ctx {
     std::map<uint32_t, fides::SwitchKey> galois_keys;
     std::map<uint32_t, fides::SwitchKey> host_generated;  // galois 0 = relin (for export)
 
+    // bootstrapping precomputation (diagonal plaintexts, series), by slot count
+    std::map<int, std::shared_ptr<fides::BootPrecomp>> boot;
+
     int tuned_variant = 0;
     std::vector<float> tune_ms;
     std::string last_error;
@@ -111,7 +117,15 @@ namespace fides {
 // helpers shared by api.cpp / client.cpp
 fides_status set_err(fides_ctx* c, fides_status s, const std::string& msg);
 fides_status check_cuda(fides_ctx* c, const char* where);
-fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st = nullptr);
+// Canonical-embedding encode of `slots` complex values (interleaved re, im)
+// at `scale` into level+1 evaluation limbs at dm (device), on the context stream.
+fides_status encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm);
+// Per-limb integer constant z mod q_j with its Shoup companion, z of any sign.
+void int_const_limbs(const fides_ctx* c, int64_t z, int nlimbs, uint64_t (*out)[2]);
+// Output buffer of `level`+1 limbs per component, stream-ordered on `st`
+// (default: the context stream), from `pool` when given.
+fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st = nullptr,
+                        cudaMemPool_t pool = nullptr);
 fides_status build_context(fides_ctx* c, const fides_params* p);
 bool select_moduli(const fides_params* prm, std::vector<uint64_t>& q, std::vector<uint64_t>& p);
 void free_context(fides_ctx* c);

@@ -85,6 +85,41 @@ void launch_scalar_mac(const DevCtx& ctx, int n, const uint64_t* a, const uint64
 // out = a + c_j with one constant per limb (device table [n])
 void launch_scalar_add(const DevCtx& ctx, int n, const uint64_t* a, const uint64_t* cj, uint64_t* out,
                        cudaStream_t st);
+// Plaintext dot product of ciphertexts (BSGS inner sums):
+//   o0 = sum_k c0[k] * p[k],  o1 = sum_k c1[k] * p[k]   (+ o0 / o1 when accumulate)
+// over limbs 0..nlimbs-1 with one 128-bit accumulator per output, n <= kMaxBatch.
+struct DotArgs {
+    const uint64_t* c0[kMaxBatch];
+    const uint64_t* c1[kMaxBatch];
+    const uint64_t* p[kMaxBatch];
+    int n;
+    int accumulate;
+    uint64_t* o0;
+    uint64_t* o1;
+};
+void launch_dot_pt(const DevCtx& ctx, int nlimbs, const DotArgs& args, cudaStream_t st);
+// Integer linear combination over ciphertext components, with per-limb
+// integer constants z[k][j] (value, Shoup companion) and an optional constant
+// added to component 0:
+//   out0 = sum_k z_k in0_k + add0_j,   out1 = sum_k z_k in1_k   over limbs 0..nlimbs-1.
+constexpr int kMaxLin = 8;
+constexpr int kMaxLinLimbs = 64;
+struct LinArgs {
+    const uint64_t* in0[kMaxLin];
+    const uint64_t* in1[kMaxLin];
+    int n;
+    int has_add;
+    int q0;  // prime of limb 0
+    uint64_t* out0;
+    uint64_t* out1;
+    uint64_t z[kMaxLin][kMaxLinLimbs][2];
+    uint64_t add0[kMaxLinLimbs];
+};
+void launch_lincomb(const DevCtx& ctx, int nlimbs, const LinArgs& args, cudaStream_t st);
+// Multiplication by the monomial X^k (0 <= k < 2N) of both components of a
+// ciphertext in evaluation form: slot i scales by psi^((2 brev(i) + 1) k).
+void launch_mult_monomial(const DevCtx& ctx, int nlimbs, const uint64_t* in0, const uint64_t* in1, uint64_t* out0,
+                          uint64_t* out1, uint32_t k, cudaStream_t st);
 // automorphism gather over nlimbs limbs (any primes): out[j] = in[slot(galois_inv, j)]
 void launch_automorph(const DevCtx& ctx, int nlimbs, const uint64_t* in, uint64_t* out, uint32_t galois_inv,
                       cudaStream_t st);

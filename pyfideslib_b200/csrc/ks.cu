@@ -461,6 +461,119 @@ void launch_scalar_add(const DevCtx& ctx, int n, const uint64_t* a, const uint64
     k_scalar_add<<<g, 128, 0, st>>>(ctx, a, cj, out);
 }
 
+// Plaintext dot product: each thread owns two coefficients of both halves,
+// reads each plaintext term once for c0 and c1.  Products of residues below
+// 2^62 are below 2^124, so 15 of them plus a folded residue fit in 128 bits;
+// the accumulators are folded back to one residue every 15 terms.
+// Role in the reference: dotProductPt_ (CKKS/ElemenwiseBatchKernels.cu:651).
+__global__ void k_dot_pt(const __grid_constant__ DevCtx ctx, const __grid_constant__ DotArgs args) {
+    const int limb = blockIdx.y;
+    const PrimeConst pc = ctx.pc[limb];
+    const size_t i = (size_t)limb * ctx.N + (size_t)(blockIdx.x * blockDim.x + threadIdx.x) * 2;
+    Acc128 a0, a1, b0, b1;
+    if (args.accumulate) {
+        const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(args.o0 + i);
+        const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(args.o1 + i);
+        a0.lo = x.x;
+        a1.lo = x.y;
+        b0.lo = y.x;
+        b1.lo = y.y;
+    }
+    int since = 0;
+#pragma unroll 1
+    for (int k = 0; k < args.n; ++k) {
+        const ulonglong2 w = __ldg(reinterpret_cast<const ulonglong2*>(args.p[k] + i));
+        const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(args.c0[k] + i);
+        const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(args.c1[k] + i);
+        a0.mac(x.x, w.x);
+        a1.mac(x.y, w.y);
+        b0.mac(y.x, w.x);
+        b1.mac(y.y, w.y);
+        if (++since == 15) {
+            a0.lo = a0.reduce(pc), a0.hi = 0;
+            a1.lo = a1.reduce(pc), a1.hi = 0;
+            b0.lo = b0.reduce(pc), b0.hi = 0;
+            b1.lo = b1.reduce(pc), b1.hi = 0;
+            since = 0;
+        }
+    }
+    ulonglong2 r;
+    r.x = a0.reduce(pc);
+    r.y = a1.reduce(pc);
+    *reinterpret_cast<ulonglong2*>(args.o0 + i) = r;
+    r.x = b0.reduce(pc);
+    r.y = b1.reduce(pc);
+    *reinterpret_cast<ulonglong2*>(args.o1 + i) = r;
+}
+
+void launch_dot_pt(const DevCtx& ctx, int nlimbs, const DotArgs& args, cudaStream_t st) {
+    if (nlimbs <= 0 || args.n <= 0 || args.n > kMaxBatch) return;
+    dim3 g(ctx.N / 256, nlimbs);
+    count_launches(1);
+    k_dot_pt<<<g, 128, 0, st>>>(ctx, args);
+}
+
+// Integer linear combination (leaf sums of polynomial evaluation, integer
+// scalar products): each thread owns two coefficients of both components.
+__global__ void k_lincomb(const __grid_constant__ DevCtx ctx, const __grid_constant__ LinArgs args) {
+    const int limb = blockIdx.y;
+    const PrimeConst pc = ctx.pc[args.q0 + limb];
+    const size_t i = (size_t)limb * ctx.N + (size_t)(blockIdx.x * blockDim.x + threadIdx.x) * 2;
+    ulonglong2 r0 = make_ulonglong2(0, 0), r1 = make_ulonglong2(0, 0);
+#pragma unroll 1
+    for (int k = 0; k < args.n; ++k) {
+        const uint64_t z = args.z[k][limb][0], zs = args.z[k][limb][1];
+        const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(args.in0[k] + i);
+        const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(args.in1[k] + i);
+        r0.x = add_mod(r0.x, mul_shoup(x.x, z, zs, pc.p), pc.p);
+        r0.y = add_mod(r0.y, mul_shoup(x.y, z, zs, pc.p), pc.p);
+        r1.x = add_mod(r1.x, mul_shoup(y.x, z, zs, pc.p), pc.p);
+        r1.y = add_mod(r1.y, mul_shoup(y.y, z, zs, pc.p), pc.p);
+    }
+    if (args.has_add) {
+        r0.x = add_mod(r0.x, args.add0[limb], pc.p);
+        r0.y = add_mod(r0.y, args.add0[limb], pc.p);
+    }
+    *reinterpret_cast<ulonglong2*>(args.out0 + i) = r0;
+    *reinterpret_cast<ulonglong2*>(args.out1 + i) = r1;
+}
+
+void launch_lincomb(const DevCtx& ctx, int nlimbs, const LinArgs& args, cudaStream_t st) {
+    if (nlimbs <= 0 || nlimbs > kMaxLinLimbs || args.n < 0 || args.n > kMaxLin) return;
+    dim3 g(ctx.N / 256, nlimbs);
+    count_launches(1);
+    k_lincomb<<<g, 128, 0, st>>>(ctx, args);
+}
+
+// X^k in evaluation form: slot i of prime j holds psi_j^e, e = (2 brev(i) + 1) k
+// mod 2N; psi^m = fwd_tw[j][brev(m)] for m < N and psi^N = -1.
+// Role in the reference: Ciphertext::multMonomial (used by Bootstrap.cu:268).
+__global__ void k_mult_monomial(const __grid_constant__ DevCtx ctx, const uint64_t* __restrict__ in0,
+                                const uint64_t* __restrict__ in1, uint64_t* __restrict__ out0,
+                                uint64_t* __restrict__ out1, uint32_t k) {
+    const int limb = blockIdx.y;
+    const uint64_t* in = blockIdx.z ? in1 : in0;
+    uint64_t* out = blockIdx.z ? out1 : out0;
+    const uint64_t p = ctx.pc[limb].p;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t mask2n = (2u << ctx.logN) - 1;
+    const uint32_t e = (((brev_bits(i, ctx.logN) << 1) + 1) * k) & mask2n;
+    const uint32_t m = e & ((uint32_t)ctx.N - 1);
+    const ulonglong2 w = __ldg(reinterpret_cast<const ulonglong2*>(ctx.fwd_tw) + (size_t)limb * ctx.N +
+                               brev_bits(m, ctx.logN));
+    const size_t o = (size_t)limb * ctx.N + i;
+    const uint64_t v = mul_shoup(in[o], w.x, w.y, p);
+    out[o] = (e >= (uint32_t)ctx.N) ? neg_mod(v, p) : v;
+}
+
+void launch_mult_monomial(const DevCtx& ctx, int nlimbs, const uint64_t* in0, const uint64_t* in1, uint64_t* out0,
+                          uint64_t* out1, uint32_t k, cudaStream_t st) {
+    if (nlimbs <= 0) return;
+    dim3 g(ctx.N / 256, nlimbs, 2);
+    count_launches(1);
+    k_mult_monomial<<<g, 256, 0, st>>>(ctx, in0, in1, out0, out1, k);
+}
+
 __global__ void k_automorph(const __grid_constant__ DevCtx ctx, const uint64_t* __restrict__ in,
                             uint64_t* __restrict__ out, uint32_t galois_inv) {
     const size_t base = (size_t)blockIdx.y * ctx.N;

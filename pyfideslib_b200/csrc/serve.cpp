@@ -1,11 +1,12 @@
 // serve.cpp -- continuous-batching request loop over one context.
 //
-// Requests (HMult+Relin+Rescale, Rotate) are queued by any thread.  A
-// scheduler thread keeps forming batches from whatever is pending -- grouped
-// by operation and level, up to max_batch per batch -- and launches each
-// batch on the next free stream; every stream owns a key-switch workspace,
-// so a batch admitted while others are still running overlaps them on the
-// device.  Admission is against a fixed HBM budget: the workspaces are
+// Requests (HMult+Relin+Rescale, Rotate, Bootstrap) are queued by any
+// thread.  A scheduler thread keeps forming batches from whatever is pending
+// -- HMult / Rotate grouped by operation and level, up to max_batch per
+// batch -- and launches each batch on the next free stream; every stream owns
+// a key-switch workspace, so a batch admitted while others are still running
+// overlaps them on the device.  Bootstraps run one at a time on their own
+// lane (the context stream and workspaces), beside the batches.  Admission is against a fixed HBM budget: the workspaces are
 // charged once at start-up, and every admitted request reserves its output
 // buffer until the request completes.  Completion is detected with one CUDA
 // event per batch; the caller waits on a request id.  Ciphertexts and keys
@@ -51,13 +52,20 @@ struct Lane {
     bool busy = false;
 };
 
+bool is_boot(const Request* r) { return r->op == FIDES_OP_BOOTSTRAP; }
+
 }  // namespace
 
 struct fides_server {
     fides_ctx* c = nullptr;
     size_t budget = 0, reserved = 0, ws_bytes = 0;
     int max_batch = 16;
+    // outputs of admitted requests come from this pool, which keeps up to the
+    // budget cached once touched, so admission never waits on the driver
+    cudaMemPool_t pool = nullptr;
     std::vector<Lane> lanes;
+    Lane boot;                // bootstrap lane: context stream, one request at a time
+    size_t boot_scratch = 0;  // HBM charged per bootstrap besides its output
     std::mutex mu;
     std::condition_variable cv_sched, cv_done;
     std::deque<Request*> pending;
@@ -74,24 +82,39 @@ namespace {
 
 size_t out_bytes(const fides_ctx* c, int level) { return 2 * (size_t)(level + 1) * c->limb_bytes(); }
 
-// Launch one batch of same-op, same-level requests on a lane.
+// Launch one batch of same-op, same-level requests on a lane.  A request
+// whose output cannot be allocated fails alone; the rest of the batch runs.
 void launch_batch(fides_server* s, Lane& ln) {
     fides_ctx* c = s->c;
     const int N = c->N;
-    auto& b = ln.batch;
-    const int nb = (int)b.size();
-    const int op = b[0]->op;
-    const int level = b[0]->level;
-    std::vector<uint64_t*> o0(nb), o1(nb);
-    for (int j = 0; j < nb; ++j) {
-        Request* r = b[j];
+    const int op = ln.batch[0]->op;
+    const int level = ln.batch[0]->level;
+    if (op == FIDES_OP_BOOTSTRAP) {
+        // one request; queued on the context stream by the host-side orchestration
+        Request* r = ln.batch[0];
+        r->t_start = clk::now();
+        r->status = fides_bootstrap(c, r->a, r->out);
+        cudaEventRecord(ln.ev, ln.st);
+        ln.busy = true;
+        return;
+    }
+    std::vector<Request*> b;
+    for (Request* r : ln.batch) {
         r->t_start = clk::now();
         const int out_level = (op == FIDES_OP_HMULT && level > 0) ? level - 1 : level;
-        if (ct_reserve(c, r->out, out_level, ln.st) != FIDES_OK) r->status = FIDES_OOM;
-        o0[j] = r->out->c0();
-        o1[j] = r->out->c1(N);
+        if (ct_reserve(c, r->out, out_level, ln.st, s->pool) != FIDES_OK) {
+            r->status = FIDES_OOM;
+            continue;
+        }
+        b.push_back(r);
     }
-    if (op == FIDES_OP_HMULT) {
+    const int nb = (int)b.size();
+    std::vector<uint64_t*> o0(nb), o1(nb);
+    for (int j = 0; j < nb; ++j) {
+        o0[j] = b[j]->out->c0();
+        o1[j] = b[j]->out->c1(N);
+    }
+    if (nb > 0 && op == FIDES_OP_HMULT) {
         std::vector<const uint64_t*> a0(nb), a1(nb), b0(nb), b1(nb);
         for (int j = 0; j < nb; ++j) {
             a0[j] = b[j]->a->c0();
@@ -101,7 +124,7 @@ void launch_batch(fides_server* s, Lane& ln) {
         }
         eng_hmult(c, ln.ws, level, nb, a0.data(), a1.data(), b0.data(), b1.data(), o0.data(), o1.data(), level > 0,
                   c->relin);
-    } else {
+    } else if (nb > 0) {
         std::vector<const uint64_t*> c0(nb), c1(nb);
         std::vector<const SwitchKey*> keys(nb);
         std::vector<uint32_t> gal(nb);
@@ -117,12 +140,14 @@ void launch_batch(fides_server* s, Lane& ln) {
     ln.busy = true;
 }
 
-void finish_lane(fides_server* s, Lane& ln, clk::time_point now) {
+void finish_lane(fides_server* s, Lane& ln, clk::time_point now, cudaError_t q) {
     const cudaError_t e = cudaGetLastError();
     for (Request* r : ln.batch) {
-        if (e != cudaSuccess) r->status = FIDES_CUDA_ERR;
+        if (e != cudaSuccess || q != cudaSuccess) r->status = FIDES_CUDA_ERR;
         const fides_ct* a = r->a;
-        if (r->op == FIDES_OP_HMULT) {
+        if (r->status != FIDES_OK || r->op == FIDES_OP_BOOTSTRAP) {
+            // failed, or metadata set by fides_bootstrap
+        } else if (r->op == FIDES_OP_HMULT) {
             const bool rs = r->level > 0;
             const double sc = a->scale * r->b->scale;
             r->out->level = rs ? r->level - 1 : r->level;
@@ -152,23 +177,28 @@ void scheduler(fides_server* s) {
     while (true) {
         // retire finished batches
         bool any_busy = false;
-        for (auto& ln : s->lanes) {
-            if (!ln.busy) continue;
-            if (cudaEventQuery(ln.ev) == cudaSuccess) {
-                finish_lane(s, ln, clk::now());
+        auto retire = [&](Lane& ln) {
+            if (!ln.busy) return;
+            const cudaError_t q = cudaEventQuery(ln.ev);
+            if (q != cudaErrorNotReady) {  // done, or failed: either way the batch ends here
+                finish_lane(s, ln, clk::now(), q);
                 s->cv_done.notify_all();
             } else {
                 any_busy = true;
             }
-        }
+        };
+        for (auto& ln : s->lanes) retire(ln);
+        retire(s->boot);
         if (s->stop && s->pending.empty() && !any_busy) break;
         // admit: form one batch per free lane from the head of the queue
         for (auto& ln : s->lanes) {
             if (ln.busy || s->pending.empty()) continue;
-            Request* head = s->pending.front();
+            auto hit = std::find_if(s->pending.begin(), s->pending.end(), [](Request* r) { return !is_boot(r); });
+            if (hit == s->pending.end()) break;
+            Request* head = *hit;
             std::vector<Request*> pick;
             size_t need = 0;
-            for (auto it = s->pending.begin(); it != s->pending.end() && (int)pick.size() < s->max_batch;) {
+            for (auto it = hit; it != s->pending.end() && (int)pick.size() < s->max_batch;) {
                 Request* r = *it;
                 if (r->op == head->op && r->level == head->level && s->reserved + need + r->bytes <= s->budget) {
                     need += r->bytes;
@@ -182,12 +212,34 @@ void scheduler(fides_server* s) {
             s->reserved += need;
             ln.batch = std::move(pick);
             s->batches++;
+            // submitters are not held up while the batch is queued
+            lk.unlock();
             {
                 std::lock_guard<std::recursive_mutex> g(s->c->mu);
                 cudaSetDevice(s->c->device);
                 launch_batch(s, ln);
             }
+            lk.lock();
             any_busy = true;
+        }
+        // the oldest bootstrap, when its lane is free and the budget allows
+        if (!s->boot.busy) {
+            auto hit = std::find_if(s->pending.begin(), s->pending.end(), [](Request* r) { return is_boot(r); });
+            if (hit != s->pending.end() && s->reserved + (*hit)->bytes <= s->budget) {
+                Request* r = *hit;
+                s->pending.erase(hit);
+                s->reserved += r->bytes;
+                s->boot.batch = {r};
+                s->batches++;
+                lk.unlock();
+                {
+                    std::lock_guard<std::recursive_mutex> g(s->c->mu);
+                    cudaSetDevice(s->c->device);
+                    launch_batch(s, s->boot);
+                }
+                lk.lock();
+                any_busy = true;
+            }
         }
         if (any_busy) {
             s->cv_sched.wait_for(lk, std::chrono::microseconds(50));
@@ -230,6 +282,33 @@ fides_status fides_srv_create(fides_ctx* c, size_t hbm_budget, int max_batch, in
         return set_err(c, FIDES_OOM, "HBM budget smaller than the serving workspaces");
     }
     s->reserved = s->ws_bytes;
+    s->boot.st = c->st;
+    cudaEventCreateWithFlags(&s->boot.ev, cudaEventDisableTiming);
+    // a bootstrap holds about 64 top-level ciphertexts of intermediates
+    s->boot_scratch = 64 * out_bytes(c, c->L - 1);
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = c->device;
+        if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            s->pool = nullptr;
+            fides_srv_destroy(s);
+            return set_err(c, FIDES_CUDA_ERR, "serving memory pool");
+        }
+        uint64_t keep = s->budget - s->ws_bytes;
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        // touch part of the budget once so the first requests find it mapped
+        const size_t warm = std::min<size_t>(keep, (size_t)4 << 30);
+        void* w = nullptr;
+        if (cudaMallocFromPoolAsync(&w, warm, s->pool, s->lanes[0].st) == cudaSuccess) {
+            cudaFreeAsync(w, s->lanes[0].st);
+        } else {
+            cudaGetLastError();
+        }
+        cudaStreamSynchronize(s->lanes[0].st);
+    }
     s->th = std::thread(scheduler, s);
     *out = s;
     return FIDES_OK;
@@ -245,6 +324,10 @@ fides_status fides_srv_submit(fides_server* s, int op, const fides_ct* a, const 
         std::lock_guard<std::recursive_mutex> g(c->mu);
         const uint32_t gal = fides_rotation_galois(c, index, a->slots > 0 ? a->slots : c->N / 2);
         if (gal == 1 || !c->galois_keys.count(gal)) return set_err(c, FIDES_KEY_MISSING, "no rotation key");
+    } else if (op == FIDES_OP_BOOTSTRAP) {
+        std::lock_guard<std::recursive_mutex> g(c->mu);
+        if (!c->boot.count(a->slots > 0 ? a->slots : c->N / 2))
+            return set_err(c, FIDES_BAD_ARG, "bootstrapping not set up for these slots");
     } else {
         return FIDES_UNSUPPORTED;
     }
@@ -256,7 +339,7 @@ fides_status fides_srv_submit(fides_server* s, int op, const fides_ct* a, const 
     r->index = index;
     r->out = out;
     r->level = a->level;
-    r->bytes = out_bytes(c, a->level);
+    r->bytes = op == FIDES_OP_BOOTSTRAP ? out_bytes(c, c->L - 1) + s->boot_scratch : out_bytes(c, a->level);
     std::lock_guard<std::mutex> lk(s->mu);
     if (r->bytes + s->ws_bytes > s->budget) {
         delete r;
@@ -335,7 +418,11 @@ fides_status fides_srv_destroy(fides_server* s) {
         if (ln.ev) cudaEventDestroy(ln.ev);
         if (ln.st) cudaStreamDestroy(ln.st);
     }
+    if (s->boot.st) cudaStreamSynchronize(s->boot.st);  // the context's stream: not destroyed here
+    if (s->boot.ev) cudaEventDestroy(s->boot.ev);
     for (auto& kv : s->all) delete kv.second;
+    // outputs still held by the caller keep their memory until freed
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return FIDES_OK;
 }

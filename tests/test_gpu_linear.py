@@ -1,0 +1,104 @@
+"""Diagonal-form linear transform (baby-step giant-step) through the C ABI.
+
+* Bit-exact: the CUDA path equals the oracle composition of the same steps
+  (hoisted baby rotations, plaintext products summed per giant step, giant
+  rotations, sum, rescale) on random residues and random switching keys; the
+  reference's LinearTransform (CKKS/LinearTransform.cu:67-258) has this shape.
+* Numerically: with real keys and encoded diagonals the decrypted result
+  matches the FP64 matrix-vector product (the reference's tests bound the
+  error of rotations the same way, test/ParametrizedTest.cuh:517-530).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from gpu_helpers import make_pair, rand_ct, rand_key
+
+pytestmark = pytest.mark.gpu
+
+
+def _upload_pt(cc, m, level):
+    import pyfideslib_b200 as F
+    from pyfideslib_b200._capi import check, lib, u64p, vp
+
+    h = vp()
+    m = np.ascontiguousarray(m, dtype=np.uint64)
+    check(lib.fides_pt_upload(cc._h, m.ctypes.data_as(u64p), level, 1.0, 1, cc.N // 2, C.byref(h)), cc._h)
+    return F.Plaintext(cc, h.value)
+
+
+def _oracle_bsgs(oc, level, c0, c1, offsets, pts, bstep, keys, gal_of):
+    pid = list(range(level + 1))
+    p = np.array(oc.primes[:level + 1], dtype=np.uint64)[:, None]
+    babies = sorted({o - (o // bstep) * bstep for o in offsets} - {0})
+    rot = {0: (c0, c1)}
+    if babies:
+        ks = [pow(gal_of(b), -1, 2 * oc.N) for b in babies]
+        h0, h1 = oc.rotate_hoisted(level, c0, c1, ks, [keys[b][0] for b in babies], [keys[b][1] for b in babies])
+        for i, b in enumerate(babies):
+            rot[b] = (h0[i], h1[i])
+    groups = {}
+    for k, o in enumerate(offsets):
+        groups.setdefault(o // bstep, []).append(k)
+    acc = None
+    for g in sorted(groups):
+        s0 = np.zeros_like(c0)
+        s1 = np.zeros_like(c1)
+        for k in groups[g]:
+            b = offsets[k] - g * bstep
+            s0 = (s0 + oc.polymul(rot[b][0], pts[k], pid)) % p
+            s1 = (s1 + oc.polymul(rot[b][1], pts[k], pid)) % p
+        if g:
+            G = g * bstep
+            s0, s1 = oc.rotate(level, s0, s1, pow(gal_of(G), -1, 2 * oc.N), *keys[G])
+        acc = (s0, s1) if acc is None else ((acc[0] + s0) % p, (acc[1] + s1) % p)
+    return acc
+
+
+@pytest.mark.parametrize("offsets,bstep", [(list(range(16)), 4), ([-7, -3, -1, 0, 2, 5, 9, 13], 4), ([0], 4)])
+def test_linear_transform_bitexact_vs_oracle(offsets, bstep):
+    import pyfideslib_b200 as F
+
+    cc, oc = make_pair(12, 8, 3, 3)
+    level = 6
+    rots = F.CryptoContext.linear_transform_rotations(offsets, bstep)
+    keys = {}
+    for i, r in enumerate(rots):
+        g = cc.rotation_galois(r)
+        keys[r] = rand_key(oc, 500 + 2 * i)
+        cc.upload_galois_key(g, *keys[r])
+    c0, c1 = rand_ct(oc, level, 71)
+    x = cc.upload(c0, c1)
+    pts_r = [oc.random(list(range(level + 1)), 900 + k) for k in range(len(offsets))]
+    pts = [_upload_pt(cc, m, level) for m in pts_r]
+    for rescale in (False, True):
+        got = cc.EvalLinearTransform(x, offsets, pts, bstep, rescale=rescale).download()
+        w0, w1 = _oracle_bsgs(oc, level, c0, c1, offsets, pts_r, bstep, keys, cc.rotation_galois)
+        if rescale:
+            w0, w1 = oc.rescale(level, w0), oc.rescale(level, w1)
+        assert np.array_equal(got[0], w0) and np.array_equal(got[1], w1), (offsets, rescale)
+
+
+@pytest.mark.parametrize("offsets,bstep", [(list(range(16)), 4), ([-9, -4, -1, 0, 3, 6, 11], 4),
+                                           (list(range(-20, 44)), 8)])
+def test_linear_transform_matches_fp64(offsets, bstep):
+    import pyfideslib_b200 as F
+
+    cc = F.CryptoContext(log_n=12, num_q=6, dnum=2)
+    slots = cc.N // 2
+    sk = cc.KeyGen(seed=3, hamming_weight=64)
+    cc.EvalRotateKeyGen(sk, F.CryptoContext.linear_transform_rotations(offsets, bstep))
+    rng = np.random.default_rng(len(offsets))
+    x = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+    diags = {o: rng.uniform(-1, 1, slots) for o in offsets}
+    ct = cc.Encrypt(sk, x, slots=slots)
+    offs, pts = cc.prepare_linear_transform(diags, bstep, level=ct.level, slots=slots)
+    y = cc.EvalLinearTransform(ct, offs, pts, bstep, rescale=True)
+    got = cc.Decrypt(sk, y, slots=slots)
+    want = np.zeros(slots, dtype=np.complex128)
+    for o, d in diags.items():
+        want += d * np.roll(x, -o)
+    err = np.max(np.abs(got - want))
+    assert err < 1e-6, err
+    assert y.level == ct.level - 1
