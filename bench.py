@@ -38,6 +38,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "key-switched HMult/s at N=2^16 L=30 (batched vs per-op), bootstrap ms, NTT HBM GB/s"
 LOGN, L, K, DNUM = 16, 30, 10, 3
+# DRAM bytes (read + write) of one forward NTT over 30 limbs at N=2^16, from an
+# ncu capture of these two launches (dram__bytes_read.sum + dram__bytes_write.sum
+# of k_ntt_fwd_cols and k_ntt_fwd_rows; ncu flushes the caches before each
+# kernel).  Twice the algorithmic bytes: the row pass reads about one
+# (psi^k, Shoup) table of N entries per limb.
+NTT30_TRAFFIC_BYTES = 63.08e6
 
 
 def peaks():
@@ -583,7 +589,8 @@ def run_ours(args):
                        "d2h_bytes_per_step": int(B * 2 * lv * N * 8)},
                "roofline": {"kernel": "ntt_forward(30 limbs, 2 kernels)", "bound": "hbm", "achieved": achieved,
                             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                            "traffic": None, "algorithmic_bytes": ntt_bytes, "us_per_launch": ntt_ms * 1e3},
+                            "traffic": NTT30_TRAFFIC_BYTES, "traffic_source": "ncu capture, caches flushed",
+                            "algorithmic_bytes": ntt_bytes, "us_per_launch": ntt_ms * 1e3},
                "ntt_gbs": achieved,
                "gpu_launches": int(launches),
                "autotune": autotune,

@@ -468,10 +468,14 @@ fides_status fides_chebyshev_series(fides_ctx* c, const fides_ct* a, const doubl
     Lanes x = {const_cast<fides_ct*>(a)};
     std::vector<double> cf(coeffs, coeffs + degree + 1);
     int top = a->level;
-    if (lo != -1.0 || hi != 1.0) {
-        // y = (2x - (lo + hi)) / (hi - lo): one rescale
+    // The squarings T_2k = 2 T_k^2 - 1 map a scale s to s^2 / q: unless the
+    // input's scale sits at its level's modulus the scales run away (doubly
+    // exponentially in the depth).  An input off by more than 2^-20 is first
+    // brought there, together with the affine map to [-1, 1] (one rescale).
+    const double rel = a->scale / (double)c->host.prime[top];
+    if (lo != -1.0 || hi != 1.0 || std::fabs(rel - 1.0) > 1.0 / (1 << 20)) {
         if (top < 1) return FIDES_BAD_ARG;
-        x = A.lin({{&x, 2.0 / (hi - lo)}}, -(lo + hi) / (hi - lo), top, a->scale, x);
+        x = A.lin({{&x, 2.0 / (hi - lo)}}, -(lo + hi) / (hi - lo), top, (double)c->host.prime[top - 1], x);
         top -= 1;
     }
     if (!A.ok()) return A.st;
@@ -577,8 +581,11 @@ fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
     if (s != FIDES_OK) return s;
     x[0]->scale = B.K * (double)c->host.prime[0];
     x[0]->slots = n;
-    // integer multiply + rescale: scale K q0 -> about the default scale, values unchanged
-    x = A.lin({{&x, 1.0}}, 0.0, top, c->default_scale, x);
+    // integer multiply + rescale: scale K q0 -> half the modulus EvalMod starts
+    // at, values unchanged; the real / imaginary split doubles it, so the
+    // Chebyshev input's scale equals its own level's modulus and the squarings
+    // of the series keep their scales next to the moduli they are divided by
+    x = A.lin({{&x, 1.0}}, 0.0, top, 0.5 * (double)c->host.prime[B.level_after_cts], x);
     if (!A.ok()) return A.st;
     for (const BootStage& st : B.cts) {
         Lanes y = A.fresh(1);

@@ -20,6 +20,7 @@
 //   * decryption: c0 + c1 s on the device, INTT, then a mixed-radix CRT of the
 //     first three moduli on the host (values of decryptable ciphertexts are
 //     far below q0 q1 q2 / 2).
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -334,9 +335,13 @@ fides_status fides_keygen_rotations(fides_ctx* c, const fides_sk* sk, int n, con
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     cudaSetDevice(c->device);
     if (slots <= 0) slots = c->N / 2;
+    // a key already held for an element is regenerated: it may belong to
+    // another secret key; repeats within this call are generated once
+    std::vector<uint32_t> done;
     for (int i = 0; i < n; ++i) {
         const uint32_t g = fides_rotation_galois(c, indices[i], slots);
-        if (g == 1 || c->galois_keys.count(g)) continue;
+        if (g == 1 || std::find(done.begin(), done.end(), g) != done.end()) continue;
+        done.push_back(g);
         fides_status s = keygen_galois(c, sk, g, seed + 7919ull * (uint64_t)i);
         if (s != FIDES_OK) return s;
     }

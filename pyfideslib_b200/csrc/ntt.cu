@@ -34,9 +34,17 @@
 
 namespace fides {
 
+// Forward butterfly.  Harvey's form keeps X in [0, 4p) with one conditional
+// subtraction per butterfly; for primes below 2^57 (LAZY) the subtraction is
+// dropped: each stage adds at most 2p to the bound, so after the 16 stages of
+// a 2^16 transform values stay below 33p < 2^63 (the Shoup product accepts any
+// 64-bit input) and one reduction in the epilogue suffices.
+constexpr uint64_t kLazyPrimeBound = 1ull << 57;
+
+template <bool LAZY>
 __device__ __forceinline__ void ct_bfly(uint64_t& X, uint64_t& Y, const ulonglong2 w, const uint64_t p,
                                         const uint64_t two_p) {
-    const uint64_t x = csub(X, two_p);
+    const uint64_t x = LAZY ? X : csub(X, two_p);
     const uint64_t t = mul_shoup_lazy(Y, w.x, w.y, p);
     X = x + t;
     Y = x - t + two_p;
@@ -51,6 +59,10 @@ __device__ __forceinline__ void gs_bfly(uint64_t& X, uint64_t& Y, const ulonglon
 }
 
 __device__ __forceinline__ uint64_t reduce4p(uint64_t v, const PrimeConst& c) { return csub(csub(v, c.two_p), c.p); }
+// canonical residue of any forward-NTT output (below 33p, see ct_bfly)
+__device__ __forceinline__ uint64_t reduce_fwd(uint64_t v, const PrimeConst& c) {
+    return csub(reduce64_lazy(v, c), c.p);
+}
 
 // Centred lift of a residue mod om into nm (src/CKKS/Rescale.cuh:45-62).
 __device__ __forceinline__ uint64_t switch_modulus(uint64_t a, uint64_t om, const PrimeConst& nc) {
@@ -82,22 +94,23 @@ __device__ __forceinline__ void load_stage_tw(ulonglong2 (&w)[15], Tab tab, int 
 // whole group up front (more loads in flight, +30 registers); PF = false
 // fetches each stage's twiddles right before the stage (fewer registers,
 // higher occupancy).  The autotuner picks per context.
-template <int KB, int KB_END, int STEP, bool PF, bool FWD, class Tab>
+template <int KB, int KB_END, int STEP, bool PF, int MODE, class Tab>
 __device__ __forceinline__ void run_stages(uint64_t (&x)[16], ulonglong2 (&w)[15], Tab tab, int t_of_kb0, size_t B,
                                            int th_hi, uint64_t p, uint64_t two_p) {
     if constexpr (!PF) load_stage_tw<KB>(w, tab, t_of_kb0, B, th_hi);
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
         if (k & (1 << KB)) continue;
-        if constexpr (FWD)
-            ct_bfly(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
+        if constexpr (MODE < 2)
+            ct_bfly<MODE == 1>(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
         else
             gs_bfly(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
     }
-    if constexpr (KB != KB_END) run_stages<KB + STEP, KB_END, STEP, PF, FWD>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
+    if constexpr (KB != KB_END) run_stages<KB + STEP, KB_END, STEP, PF, MODE>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
 }
 
-template <int KB_FIRST, int KB_LAST, bool PF, bool FWD, class Tab>
+// MODE: 0 forward, 1 forward without the per-butterfly reduction, 2 inverse
+template <int KB_FIRST, int KB_LAST, bool PF, int MODE, class Tab>
 __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi, uint64_t p,
                                           uint64_t two_p) {
     ulonglong2 w[15];
@@ -112,7 +125,7 @@ __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_k
             for (int g = 0; g < (8 >> kb); ++g) w[tw_off(kb) + g] = tab(base + g);
         }
     }
-    run_stages<KB_FIRST, KB_LAST, STEP, PF, FWD>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
+    run_stages<KB_FIRST, KB_LAST, STEP, PF, MODE>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
 }
 
 // Tile geometry shared by kernels and launchers.
@@ -139,7 +152,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
     __shared__ __align__(16) uint64_t sm[G::R * TC];
     __shared__ ulonglong2 tws[G::R];
 
-    const LimbRef lr = resolve_limb(map, blockIdx.y, blockIdx.z, ctx.N, ctx.L);
+    const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const ulonglong2* twg = reinterpret_cast<const ulonglong2*>(ctx.fwd_tw) + (size_t)lr.prime * ctx.N;
     for (int i = threadIdx.x; i < G::R; i += G::NTC) tws[i] = twg[i];
@@ -158,7 +171,11 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
     __syncthreads();
     auto tab = [&](size_t i) { return tws[i]; };
     // stages 0..3: r = th + (k << (LR - 4)), twiddle (1 << t) + (k >> (4 - t))
-    run_group<3, 0, PF, true>(x, tab, 3, 1, 0, pc.p, pc.two_p);
+    const bool lazy = pc.p < kLazyPrimeBound;
+    if (lazy)
+        run_group<3, 0, PF, 1>(x, tab, 3, 1, 0, pc.p, pc.two_p);
+    else
+        run_group<3, 0, PF, 0>(x, tab, 3, 1, 0, pc.p, pc.two_p);
     if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) sm[(th + (k << (LR - 4))) * TC + c] = x[k];
@@ -166,7 +183,10 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = sm[((th << 4) + k) * TC + c];
         // stages 4..LR-1: r = 16 th + k
-        run_group<LR - 5, 0, PF, true>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
+        if (lazy)
+            run_group<LR - 5, 0, PF, 1>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
+        else
+            run_group<LR - 5, 0, PF, 0>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
 #pragma unroll
         for (int k = 0; k < 16; ++k) lr.out[(size_t)((th << 4) + k) * C + col] = x[k];
     } else {
@@ -180,7 +200,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRef& lr, const PrimeConst& pc, size_t g,
                                                  uint64_t v) {
-    v = reduce4p(v, pc);
+    v = reduce_fwd(v, pc);
     switch (lr.smode) {
         case FS_MODDOWN: {
             const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
@@ -215,7 +235,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     __shared__ __align__(16) uint64_t sm[TR * CP];
 
-    const LimbRef lr = resolve_limb(map, blockIdx.y, blockIdx.z, ctx.N, ctx.L);
+    const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const uint64_t* twg = ctx.fwd_tw + (size_t)lr.prime * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
@@ -226,7 +246,11 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
     uint64_t x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
-    run_group<3, 0, PF, true>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
+    const bool lazy = pc.p < kLazyPrimeBound;
+    if (lazy)
+        run_group<3, 0, PF, 1>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
+    else
+        run_group<3, 0, PF, 0>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
 #pragma unroll
@@ -234,7 +258,10 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        run_group<LC - 5, 0, PF, true>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
+        if (lazy)
+            run_group<LC - 5, 0, PF, 1>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
+        else
+            run_group<LC - 5, 0, PF, 0>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
         // each thread rewrites exactly the slots it read
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
@@ -266,7 +293,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     __shared__ __align__(16) uint64_t sm[TR * CP];
 
-    const LimbRef lr = resolve_limb(map, blockIdx.y, blockIdx.z, ctx.N, ctx.L);
+    const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const uint64_t* twg = ctx.inv_tw + (size_t)lr.prime * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
@@ -304,14 +331,14 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
     if constexpr (LC > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        run_group<0, LC - 5, PF, false>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
+        run_group<0, LC - 5, PF, 2>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
         __syncthreads();
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = srow[padi(th + (k << (LC - 4)))];
-    run_group<0, 3, PF, false>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
+    run_group<0, 3, PF, 2>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
     uint64_t* dst = lr.out + (size_t)row * C;
 #pragma unroll
     for (int k = 0; k < 16; ++k) dst[th + (k << (LC - 4))] = x[k];
@@ -336,7 +363,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
     __shared__ __align__(16) uint64_t sm[G::R * TC];
     __shared__ ulonglong2 tws[G::R];
 
-    const LimbRef lr = resolve_limb(map, blockIdx.y, blockIdx.z, ctx.N, ctx.L);
+    const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const ulonglong2* twg = reinterpret_cast<const ulonglong2*>(ctx.inv_tw) + (size_t)lr.prime * ctx.N;
     for (int i = threadIdx.x; i < G::R; i += G::NTC) tws[i] = twg[i];
@@ -351,7 +378,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = lr.out[(size_t)((th << 4) + k) * C + col];
         __syncthreads();
-        run_group<0, LR - 5, PF, false>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
+        run_group<0, LR - 5, PF, 2>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
 #pragma unroll
         for (int k = 0; k < 16; ++k) sm[((th << 4) + k) * TC + c] = x[k];
         __syncthreads();
@@ -362,7 +389,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
         for (int k = 0; k < 16; ++k) x[k] = lr.out[(size_t)(th + k) * C + col];
         __syncthreads();
     }
-    run_group<0, 2, PF, false>(x, tab, 3, 1, 0, pc.p, pc.two_p);
+    run_group<0, 2, PF, 2>(x, tab, 3, 1, 0, pc.p, pc.two_p);
     // last stage (twiddle index 1) with the N^-1 * scale fold
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -390,7 +417,10 @@ int ntt_num_variants() { return 3; }
 template <int LR, int LC, int MINB, bool PF>
 static void launch_fwd_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
-    dim3 g1(G::C / G::TC, map.total, map.nb > 0 ? map.nb : 1), g2(G::R / G::TR, map.total, map.nb > 0 ? map.nb : 1);
+    // grid (tiles, batch element, limb): CTAs run x fastest, then y, so the
+    // elements of a batch that share a prime run together and its twiddle
+    // table is fetched from HBM once per launch rather than once per element
+    dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
     k_ntt_fwd_cols<LR, LC, MINB, PF><<<g1, G::NTC, 0, st>>>(ctx, map);
     k_ntt_fwd_rows<LR, LC, MINB, PF><<<g2, G::NTR, 0, st>>>(ctx, map);
 }
@@ -398,7 +428,10 @@ static void launch_fwd_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st)
 template <int LR, int LC, int MINB, bool PF>
 static void launch_inv_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
-    dim3 g1(G::C / G::TC, map.total, map.nb > 0 ? map.nb : 1), g2(G::R / G::TR, map.total, map.nb > 0 ? map.nb : 1);
+    // grid (tiles, batch element, limb): CTAs run x fastest, then y, so the
+    // elements of a batch that share a prime run together and its twiddle
+    // table is fetched from HBM once per launch rather than once per element
+    dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
     k_ntt_inv_rows<LR, LC, MINB, PF><<<g2, G::NTR, 0, st>>>(ctx, map);
     k_ntt_inv_cols<LR, LC, MINB, PF><<<g1, G::NTC, 0, st>>>(ctx, map);
 }

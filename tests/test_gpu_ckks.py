@@ -114,3 +114,18 @@ def test_hmult_c2_decrypted_error():
     c = cc.EvalMult(a, b, rescale=True)
     err = np.max(np.abs(cc.Decrypt(sk, c) - z1 * z2))
     assert err < 2.0 ** -30, err
+
+
+def test_rotation_keys_regenerated_for_new_secret():
+    """EvalRotateKeyGen with a second secret key replaces the keys the first
+    one left for the same indices (OpenFHE keeps keys per secret key)."""
+    cc = F.CryptoContext(log_n=12, num_q=4, dnum=2)
+    sk1 = cc.KeyGen(seed=1, hamming_weight=64)
+    cc.EvalRotateKeyGen(sk1, [1, 5])
+    sk2 = cc.KeyGen(seed=2, hamming_weight=64)
+    cc.EvalRotateKeyGen(sk2, [5, 5, 7])
+    rng = np.random.default_rng(0)
+    z = rng.uniform(-1, 1, cc.N // 2)
+    ct = cc.Encrypt(sk2, z)
+    got = cc.Decrypt(sk2, cc.EvalRotate(ct, 5))
+    assert np.max(np.abs(got - np.roll(z, -5))) < 1e-6
