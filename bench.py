@@ -13,8 +13,10 @@ residues (uniform in [0, q)), which is all the kernels see; the pairs occupy
   e2e    = the batched metric through the C ABI with host buffers: per step
            the pinned-host upload of the B pairs, the batched HMult and the
            download of the B results are inside the timed region.
-  roofline = the forward NTT (two kernels) over 30 limbs timed live:
-           algorithmic bytes 16*N*30 (one read + one write of each limb).
+  roofline = the forward NTT (two kernels) as the key-switch pipeline
+           launches it, batched over 32 polynomials x 30 limbs, timed live:
+           algorithmic bytes 16*N*30*32 (one read + one write of each limb);
+           the single 30-limb polynomial is reported beside it.
   cpu_baseline = the CPU oracle (C, OpenMP over limbs) on one HMult of the
            same shape on this host's cores.
 
@@ -38,12 +40,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "key-switched HMult/s at N=2^16 L=30 (batched vs per-op), bootstrap ms, NTT HBM GB/s"
 LOGN, L, K, DNUM = 16, 30, 10, 3
-# DRAM bytes (read + write) of one forward NTT over 30 limbs at N=2^16, from an
-# ncu capture of these two launches (dram__bytes_read.sum + dram__bytes_write.sum
-# of k_ntt_fwd_cols and k_ntt_fwd_rows; ncu flushes the caches before each
-# kernel).  Twice the algorithmic bytes: the row pass reads about one
-# (psi^k, Shoup) table of N entries per limb.
-NTT30_TRAFFIC_BYTES = 63.08e6
+# DRAM bytes (read + write) of one batched forward NTT (32 polynomials x 30
+# limbs at N=2^16), from an ncu capture of that launch pair
+# (dram__bytes_read.sum + dram__bytes_write.sum of k_ntt_fwd_cols and
+# k_ntt_fwd_rows; ncu flushes the caches before each kernel).  About twice the
+# algorithmic bytes: the column pass writes the 960 intermediate limbs
+# (480 MB, more than L2) and the row pass reads them back; twiddles add 32 MB
+# (read once per prime for the whole batch).
+NTT_BATCH_TRAFFIC_BYTES = 1927.28e6
 
 
 def peaks():
@@ -162,7 +166,9 @@ def measure_c4(cc, lib, st, n=256, reps=3, seed=4):
     # the same work, one operation per call
     tmp = [F.Ciphertext(cc) for _ in range(n)]
     outs2 = [F.Ciphertext(cc) for _ in range(n)]
-    for i in range(2):
+    # one untimed pass, so that the memory pool already holds buffers of every
+    # size (the plan allocates all of its buffers when it is created)
+    for i in range(n):
         cc.EvalRotate(cc.EvalMult(A[i], B[i], rescale=True, out=tmp[i]), idx[i], out=outs2[i])
     cc.Synchronize()
     e0.record(st)
@@ -269,7 +275,14 @@ def measure_bootstrap(cc, reps=3, seed=101, degree=119):
     ms = e0.elapsed_time(e1) / reps
     got = cc.Decrypt(sk, bt, slots=slots)
     err = float(np.max(np.abs(got - msgs[(reps - 1) % 2])))
+    # the same with the message scaled by 2^6 through EvalMod (correction
+    # factor; valid for these messages, whose coefficients are below 2^-5)
+    cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=degree, correction=6)
+    bt6 = cc.EvalBootstrap(cts[0])
+    err6 = float(np.max(np.abs(cc.Decrypt(sk, bt6, slots=slots) - msgs[0])))
+    cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=degree)
     res = {"bootstrap_ms": ms, "wall_ms": wall_ms, "precision_bits": -float(np.log2(err)), "max_abs_err": err,
+           "precision_bits_correction6": -float(np.log2(err6)),
            "output_level": out_level, "rotation_keys": len(rots), "setup_s": setup_s,
            "params": "N=2^16 L=30 K=%d dnum=3, 2^15 slots, h=32, budget {3,3}, Chebyshev degree %d, K=16, "
                      "3 double-angle steps" % (cc.K, degree)}
@@ -417,7 +430,12 @@ def run_ours(args):
     tv, nv = C.c_int(), C.c_int()
     tms = (C.c_float * 8)()
     lib.fides_autotune(cc._h, C.byref(tv), tms, C.byref(nv))
-    autotune = {"ntt_variant": tv.value, "fwd_inv_30limb_us": [round(1e3 * tms[i], 2) for i in range(nv.value)]}
+    cacc = C.c_int()
+    cms = (C.c_float * 2)()
+    lib.fides_autotune_conv_info(cc._h, C.byref(cacc), cms)
+    autotune = {"ntt_variant": tv.value, "fwd_inv_30limb_us": [round(1e3 * tms[i], 2) for i in range(nv.value)],
+                "conv_accumulator": ["128-bit", "split 32-bit"][cacc.value],
+                "modup_conv_one_element_us": [round(1e3 * cms[i], 2) for i in range(2)]}
     stream_ptr = C.c_void_p()
     lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))
     st = torch.cuda.ExternalStream(stream_ptr.value, device=local)
@@ -512,30 +530,46 @@ def run_ours(args):
     ms_op, _ = timed(step_per_op, max(1, args.steps // 2), 2)
     ms_e2e, _ = timed(step_e2e, max(1, args.steps // 2), 1)
 
-    # roofline: forward NTT over 30 limbs (2 kernels) cycling through 10
-    # resident polynomials (157 MB > L2), algorithmic traffic 31.5 MB per launch
-    nl, nbuf = 30, 10
+    # roofline: the forward NTT as the key-switch pipeline launches it, batched
+    # over 32 polynomials of 30 limbs (one launch pair, 1.0 GB algorithmic
+    # traffic), alternating between two resident batches (2 x 1 GB > L2); and
+    # the single 30-limb polynomial for reference
+    nl, nb_ntt = 30, 32
     # values below 2^40 are canonical residues of every modulus
-    buf = torch.randint(0, 2 ** 40, (nbuf, nl, N), dtype=torch.int64, device="cuda")
-    bp = [buf[i].data_ptr() for i in range(nbuf)]
-    reps = 40
-    for r in range(nbuf):
-        lib.fides_ntt(cc._h, bp[r], 0, nl, 0)
+    bufs = [torch.randint(0, 2 ** 40, (nb_ntt, nl, N), dtype=torch.int64, device="cuda") for _ in range(2)]
+    stride = nl * N
+    reps = 20
+    for b in bufs:
+        lib.fides_ntt_batch(cc._h, b.data_ptr(), stride, nb_ntt, 0, nl, 0)
     cc.Synchronize()
-    # the region between the profiler marks is what an ncu capture started with
-    # --profile-from-start off sees (no effect otherwise)
-    torch.cuda.profiler.start()
+    # with --profile-roofline the region between the profiler marks is what an
+    # ncu capture started with --profile-from-start off sees
+    if args.profile_roofline:
+        torch.cuda.profiler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(st):
         e0.record(st)
     for r in range(reps):
-        lib.fides_ntt(cc._h, bp[r % nbuf], 0, nl, 0)
+        lib.fides_ntt_batch(cc._h, bufs[r % 2].data_ptr(), stride, nb_ntt, 0, nl, 0)
     with torch.cuda.stream(st):
         e1.record(st)
     e1.synchronize()
-    torch.cuda.profiler.stop()
+    if args.profile_roofline:
+        torch.cuda.profiler.stop()
     ntt_ms = e0.elapsed_time(e1) / reps
-    ntt_bytes = 16.0 * N * nl
+    # single polynomial, 30 limbs, cycling through 10 polynomials (157 MB)
+    single = bufs[0].view(-1)
+    cc.Synchronize()
+    with torch.cuda.stream(st):
+        e0.record(st)
+    for r in range(40):
+        lib.fides_ntt(cc._h, single.data_ptr() + (r % 10) * stride * 8, 0, nl, 0)
+    with torch.cuda.stream(st):
+        e1.record(st)
+    e1.synchronize()
+    single_us = e0.elapsed_time(e1) / 40 * 1e3
+    del bufs, single
+    ntt_bytes = 16.0 * N * nl * nb_ntt
     hbm, peak_kind = peaks()
     achieved = ntt_bytes / (ntt_ms * 1e-3) / 1e9
 
@@ -587,10 +621,13 @@ def run_ours(args):
                "e2e": {"value": e2e_val, "unit": "HMult/s",
                        "h2d_bytes_per_step": int(B * 2 * 2 * (lv + 1) * N * 8),
                        "d2h_bytes_per_step": int(B * 2 * lv * N * 8)},
-               "roofline": {"kernel": "ntt_forward(30 limbs, 2 kernels)", "bound": "hbm", "achieved": achieved,
+               "roofline": {"kernel": "ntt_forward batched (32 polynomials x 30 limbs, k_ntt_fwd_cols + k_ntt_fwd_rows)",
+                            "bound": "hbm", "achieved": achieved,
                             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                            "traffic": NTT30_TRAFFIC_BYTES, "traffic_source": "ncu capture, caches flushed",
-                            "algorithmic_bytes": ntt_bytes, "us_per_launch": ntt_ms * 1e3},
+                            "traffic": NTT_BATCH_TRAFFIC_BYTES, "traffic_source": "ncu capture, caches flushed",
+                            "algorithmic_bytes": ntt_bytes, "us_per_launch": ntt_ms * 1e3,
+                            "single_30limb_us": single_us,
+                            "single_30limb_gbs": 16.0 * N * nl / (single_us * 1e-6) / 1e9},
                "ntt_gbs": achieved,
                "gpu_launches": int(launches),
                "autotune": autotune,
@@ -620,6 +657,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-c3", action="store_true", help="skip the config-3 hoisted/BSGS measurement")
     ap.add_argument("--no-boot", action="store_true", help="skip the bootstrap measurement")
+    ap.add_argument("--profile-roofline", action="store_true",
+                    help="mark the roofline NTT loop for ncu --profile-from-start off")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -83,6 +83,13 @@ fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream);
  * fides_ctx_create; call again to re-tune.  *variant and times_ms (one entry
  * per variant) may be NULL.  Results never depend on the variant. */
 fides_status fides_autotune(fides_ctx* ctx, int* variant, float* times_ms, int* num_variants);
+/* The base-conversion accumulator the autotuner chose (0: 128-bit sums,
+ * 1: split 32-bit partial products, for moduli below 2^60) and the ModUp
+ * conversion time of each (times_ms: 2 entries, 0 when not eligible). */
+fides_status fides_autotune_conv_info(const fides_ctx* ctx, int* accumulator, float* times_ms);
+/* Force the conversion accumulator (0 or 1, for measurements and tests);
+ * -1 restores the tuned choice. */
+fides_status fides_set_conv_accumulator(fides_ctx* ctx, int accumulator);
 /* Force an NTT variant (for measurements); -1 restores the tuned choice. */
 fides_status fides_set_ntt_variant(fides_ctx* ctx, int variant);
 /* Number of kernels this library has launched so far (process-wide). */
@@ -210,6 +217,11 @@ typedef struct {
     int cheb_degree;     /* degree of the EvalMod Chebyshev series (0 means 119) */
     double K;            /* EvalMod input range [-K, K] in units of q_0 (0 means 16) */
     int double_angle;    /* double-angle iterations (0 means 3) */
+    int correction;      /* the input is multiplied by 2^correction before ModRaise and the
+                            result's scale corrected after (exact): EvalMod's noise then
+                            weighs 2^correction times less against the message, valid while
+                            every message coefficient times D 2^correction stays below
+                            2^-8 q_0 (0: none) */
 } fides_boot_params;
 /* Precompute the CoeffsToSlots / SlotsToCoeffs diagonals (device-resident)
  * and the EvalMod series.  The keys it needs: relinearisation, conjugation
@@ -257,6 +269,11 @@ fides_status fides_srv_destroy(fides_server* srv);
 /* In-place forward / inverse NTT of `nlimbs` limbs at `data` (device pointer),
  * limb i using prime index prime0 + i. */
 fides_status fides_ntt(fides_ctx* ctx, uint64_t* data, int prime0, int nlimbs, int inverse);
+/* The same transform over npoly polynomials of nlimbs limbs each, polynomial k
+ * at data + k * poly_stride words, in one launch pair (the batched form the
+ * key-switch pipeline uses; LimbPartitionBatch.cu runs NTT_ per partition). */
+fides_status fides_ntt_batch(fides_ctx* ctx, uint64_t* data, size_t poly_stride, int npoly, int prime0, int nlimbs,
+                             int inverse);
 /* c = a * b in R_q for nlimbs limbs of coefficient-form inputs (device
  * pointers): NTT of a and b into a_ntt / b_ntt (caller-provided device
  * scratch), then one INTT with the product fused into its load.  `c` may

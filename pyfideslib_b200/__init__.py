@@ -406,11 +406,12 @@ class CryptoContext:
         return out
 
     # ---- bootstrapping (EvalBootstrapSetup / EvalBootstrapKeyGen / EvalBootstrap) ----
-    def EvalBootstrapSetup(self, level_budget=(3, 3), slots=None, cheb_degree=119, K=16.0, double_angle=3):
+    def EvalBootstrapSetup(self, level_budget=(3, 3), slots=None, cheb_degree=119, K=16.0, double_angle=3,
+                           correction=0):
         prm = BootParams()
         prm.slots = slots or self.N // 2
         prm.level_budget[0], prm.level_budget[1] = level_budget
-        prm.cheb_degree, prm.K, prm.double_angle = cheb_degree, K, double_angle
+        prm.cheb_degree, prm.K, prm.double_angle, prm.correction = cheb_degree, K, double_angle, correction
         check(lib.fides_bootstrap_setup(self._h, C.byref(prm)), self._h)
 
     def bootstrap_info(self, slots=None):
@@ -478,9 +479,20 @@ class CryptoContext:
     def SetLevel(self, ct, level):
         check(lib.fides_ct_set_level(self._h, ct._h, level), self._h)
 
-    # ---- raw device kernels (device pointers as ints) ----
+    # ---- raw device kernels (device pointers as ints, memory the caller owns
+    #      and may touch from other streams: these return after completion) ----
     def ntt(self, dev_ptr, prime0, nlimbs, inverse=False):
         check(lib.fides_ntt(self._h, dev_ptr, prime0, nlimbs, int(inverse)), self._h)
+        self.Synchronize()
+
+    def ntt_batch(self, dev_ptr, poly_stride, npoly, prime0, nlimbs, inverse=False):
+        check(lib.fides_ntt_batch(self._h, dev_ptr, poly_stride, npoly, prime0, nlimbs, int(inverse)), self._h)
+        self.Synchronize()
+
+    def set_ntt_variant(self, variant):
+        """Force an NTT kernel variant (-1: back to the autotuned one)."""
+        check(lib.fides_set_ntt_variant(self._h, variant), self._h)
 
     def polymul(self, a, b, c, a_ntt, b_ntt, prime0, nlimbs):
         check(lib.fides_polymul(self._h, a, b, c, a_ntt, b_ntt, prime0, nlimbs), self._h)
+        self.Synchronize()

@@ -39,7 +39,7 @@ class FidesParams(C.Structure):
 
 class BootParams(C.Structure):
     _fields_ = [("slots", C.c_int), ("level_budget", C.c_int * 2), ("cheb_degree", C.c_int), ("K", C.c_double),
-                ("double_angle", C.c_int)]
+                ("double_angle", C.c_int), ("correction", C.c_int)]
 
 
 def _sig(name, args, res=C.c_int):
@@ -60,6 +60,8 @@ EXPORTS = {
     "fides_ctx_stream": ([vp, C.POINTER(vp)], C.c_int),
     "fides_kernel_launches": ([], C.c_uint64),
     "fides_autotune": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
+    "fides_autotune_conv_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_float)], C.c_int),
+    "fides_set_conv_accumulator": ([vp, C.c_int], C.c_int),
     "fides_set_ntt_variant": ([vp, C.c_int], C.c_int),
     "fides_key_upload_relin": ([vp, u64p, u64p], C.c_int),
     "fides_key_upload_galois": ([vp, C.c_uint32, u64p, u64p], C.c_int),
@@ -112,6 +114,7 @@ EXPORTS = {
     "fides_srv_reset_stats": ([vp], C.c_int),
     "fides_srv_destroy": ([vp], C.c_int),
     "fides_ntt": ([vp, vp, C.c_int, C.c_int, C.c_int], C.c_int),
+    "fides_ntt_batch": ([vp, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
     "fides_polymul": ([vp, vp, vp, vp, vp, vp, C.c_int, C.c_int], C.c_int),
     "fides_polymul_noalloc": ([vp, vp, vp, vp, C.c_int, C.c_int], C.c_int),
     "fides_keygen": ([vp, u64, C.c_int, C.POINTER(vp)], C.c_int),

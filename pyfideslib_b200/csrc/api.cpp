@@ -159,6 +159,32 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
         c->tune_ms[v] = ms / 10;
         if (c->tune_ms[v] < c->tune_ms[best]) best = v;
     }
+    // base-conversion accumulators: 128-bit, or split 32-bit partial products
+    // (eligible when every modulus is below 2^60); timed on the ModUp of one
+    // top-level element
+    bool split_ok = true;
+    for (uint64_t q : c->host.prime) split_ok = split_ok && q < (1ull << 60);
+    c->conv_ms.assign(2, 0.f);
+    int conv_best = 0;
+    if (conv_supported(c->dev)) {
+        const int top = c->L - 1;
+        cudaMemsetAsync(c->ws1.XT, 0, (size_t)(top + 1) * c->limb_bytes(), c->st);
+        for (int v = 0; v < (split_ok ? 2 : 1); ++v) {
+            c->dev.split_conv = v;
+            launch_modup_conv(c->dev, top, 1, c->ws1.XT, c->ws1.DIG, c->ws1.dig_stride, c->ws1.stride, c->st);
+            cudaEventRecord(e0, c->st);
+            for (int r = 0; r < 10; ++r)
+                launch_modup_conv(c->dev, top, 1, c->ws1.XT, c->ws1.DIG, c->ws1.dig_stride, c->ws1.stride, c->st);
+            cudaEventRecord(e1, c->st);
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            c->conv_ms[v] = ms / 10;
+            if (c->conv_ms[v] < c->conv_ms[conv_best]) conv_best = v;
+        }
+    }
+    c->dev.split_conv = conv_best;
+    c->tuned_conv = conv_best;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->tuned_variant = best;
@@ -168,6 +194,24 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
     if (times_ms)
         for (int v = 0; v < nv; ++v) times_ms[v] = c->tune_ms[v];
     return check_cuda(c, "autotune");
+}
+
+fides_status fides_autotune_conv_info(const fides_ctx* c, int* accumulator, float* times_ms) {
+    if (!c) return FIDES_BAD_ARG;
+    if (accumulator) *accumulator = c->tuned_conv;
+    if (times_ms)
+        for (size_t v = 0; v < 2; ++v) times_ms[v] = v < c->conv_ms.size() ? c->conv_ms[v] : 0.f;
+    return FIDES_OK;
+}
+
+fides_status fides_set_conv_accumulator(fides_ctx* c, int accumulator) {
+    if (!c || accumulator < -1 || accumulator > 1) return FIDES_BAD_ARG;
+    Guard g(c);
+    if (accumulator == 1)
+        for (uint64_t q : c->host.prime)
+            if (q >= (1ull << 60)) return set_err(c, FIDES_UNSUPPORTED, "split products need moduli below 2^60");
+    c->dev.split_conv = accumulator < 0 ? c->tuned_conv : accumulator;
+    return FIDES_OK;
 }
 
 fides_status fides_set_ntt_variant(fides_ctx* c, int variant) {
@@ -1182,6 +1226,22 @@ fides_status fides_ntt(fides_ctx* ctx, uint64_t* data, int prime0, int nlimbs, i
     else
         ntt_forward(ctx->dev, m, FL_PLAIN, FS_PLAIN, ctx->st);
     return check_cuda(ctx, "ntt");
+}
+
+fides_status fides_ntt_batch(fides_ctx* ctx, uint64_t* data, size_t poly_stride, int npoly, int prime0, int nlimbs,
+                             int inverse) {
+    if (!ctx || !data || npoly < 1 || npoly > 65535 || prime0 < 0 || nlimbs < 1 ||
+        prime0 + nlimbs > ctx->L + ctx->K || poly_stride < (size_t)nlimbs * ctx->N)
+        return FIDES_BAD_ARG;
+    Guard g(ctx);
+    LimbMap m = map_single(data, data, nlimbs, nlimbs, prime0);
+    m.nb = npoly;
+    m.seg[0].bstride = poly_stride;
+    if (inverse)
+        ntt_inverse(ctx->dev, m, IL_PLAIN, IS_PLAIN, ctx->st);
+    else
+        ntt_forward(ctx->dev, m, FL_PLAIN, FS_PLAIN, ctx->st);
+    return check_cuda(ctx, "ntt batch");
 }
 
 fides_status fides_polymul(fides_ctx* ctx, const uint64_t* a, const uint64_t* b, uint64_t* c, uint64_t* a_ntt,

@@ -13,9 +13,10 @@
 // Formulation used here (own derivation, checked numerically in the tests):
 //   * After ModRaise the polynomial is p = D*mu + q0*I with small integers I.
 //     Declaring its scale K*q0 makes the slot values of CoeffsToSlots
-//     t = (D*mu/q0 + I)/K in [-1, 1]; one integer multiply + rescale then
-//     brings the scale near the 2^50 moduli without touching t (exact: the
-//     multiplier is an integer and the scale is tracked).
+//     t = (D*mu/q0 + I)/K in [-1, 1]; CoeffsToSlots runs at that scale (about
+//     2^64, so its noise is small against t), then one integer multiply +
+//     rescale brings the scale near the 2^50 moduli without touching t
+//     (exact: the multiplier is an integer and the scale is tracked).
 //   * Decoding of n = N/2 slots is the special FFT  z = A_logn ... A_1 P_br w
 //     (w_k = p_k + i p_{k+n}, P_br the bit reversal, A_s a butterfly stage with
 //     diagonals 0, +-2^(s-1) and twiddles zeta^(5^j mod 2^(s+2))).
@@ -63,6 +64,7 @@ struct BootPrecomp {
     double K = 16.0;
     int double_angle = 3;
     int degree = 119;
+    int correction = 0;
     std::vector<double> cheb;
     std::vector<BootStage> cts, stc;
     int level_after_cts = 0, level_after_mod = 0, level_out = 0;
@@ -174,7 +176,9 @@ std::vector<std::vector<int>> stage_groups(int logn, int budget, bool descending
     return g;
 }
 
-fides_status encode_stage(fides_ctx* c, int n, const Diag& M, int level, double factor, BootStage& st) {
+// scale 0: the modulus of `level`, so the transform keeps the ciphertext's scale
+fides_status encode_stage(fides_ctx* c, int n, const Diag& M, int level, double factor, double enc_scale,
+                          BootStage& st) {
     st.level = level;
     // offsets centred in (-n/2, n/2]; baby step ~ sqrt(#diagonals) in units of
     // the smallest offset step
@@ -190,7 +194,7 @@ fides_status encode_stage(fides_ctx* c, int n, const Diag& M, int level, double 
     int bk = 1;
     while (bk * bk < nd) bk <<= 1;
     st.bstep = bk * unit;
-    const double scale = (double)c->host.prime[level];
+    const double scale = enc_scale > 0 ? enc_scale : (double)c->host.prime[level];
     std::vector<double> vals(2 * (size_t)n);
     for (int o : offs) {
         const auto& d = M.at(((o % n) + n) % n);
@@ -224,6 +228,11 @@ fides_status encode_stage(fides_ctx* c, int n, const Diag& M, int level, double 
 // Lockstep ciphertext arithmetic with exact (level, scale) bookkeeping.
 // ---------------------------------------------------------------------------
 constexpr int kBaby = 8;
+// CoeffsToSlots diagonals are encoded at 2^58: they multiply slot values of
+// magnitude ~sqrt(N) |t|, so their rounding error (about sqrt(N) / scale per
+// entry) is what bounds the precision of t; each of the three transforms
+// grows the ciphertext's scale by 2^8, undone by the normalisation after.
+constexpr double kCtsDiagScale = 288230376151711744.0;  // 2^58
 
 using Lanes = std::vector<fides_ct*>;
 
@@ -302,6 +311,28 @@ class Arith {
             meta(o[l], level, (double)tq, like[l]->slots);
             if ((st = fides_rescale(c, o[l], o[l])) != FIDES_OK) break;
             o[l]->scale = target;
+        }
+        return o;
+    }
+
+    // x times the integer z = round(target q / s) and rescaled: level - 1,
+    // scale s z / q (exact, within a factor 1 +- 1/(2z) of target)
+    Lanes normalize(const Lanes& x, double target) {
+        const int level = x[0]->level;
+        const long double q = (long double)c->host.prime[level];
+        Lanes o = fresh(x.size());
+        for (size_t l = 0; l < x.size() && ok(); ++l) {
+            const long double zr = (long double)target * q / (long double)x[l]->scale;
+            if (!(zr >= 1.0L && zr < 4.0e18L)) {
+                st = set_err(c, FIDES_BAD_ARG, "scale out of range for normalisation");
+                break;
+            }
+            const int64_t z = (int64_t)llroundl(zr);
+            int_const_limbs(c, z, level + 1, zbuf[0]);
+            if ((st = ct_reserve(c, o[l], level)) != FIDES_OK) break;
+            launch({x[l]}, level, 0.0L, o[l]);
+            meta(o[l], level, (double)((long double)x[l]->scale * (long double)z), x[l]->slots);
+            if ((st = fides_rescale(c, o[l], o[l])) != FIDES_OK) break;
         }
         return o;
     }
@@ -503,11 +534,13 @@ fides_status fides_bootstrap_setup(fides_ctx* c, const fides_boot_params* prm) {
     bp->K = prm->K > 0 ? prm->K : 16.0;
     bp->double_angle = prm->double_angle > 0 ? prm->double_angle : 3;
     bp->degree = prm->cheb_degree > 0 ? prm->cheb_degree : 119;
+    if (prm->correction < 0 || prm->correction > 20) return FIDES_BAD_ARG;
+    bp->correction = prm->correction;
     bp->cheb = cheb_coeffs(bp->degree, bp->K, bp->double_angle);
     const int bc = prm->level_budget[0] > 0 ? prm->level_budget[0] : 3;
     const int bs = prm->level_budget[1] > 0 ? prm->level_budget[1] : 3;
     const int top = c->L - 1;
-    // levels: ModRaise at top, scale-down to top-1, CoeffsToSlots, EvalMod, SlotsToCoeffs
+    // levels: ModRaise at top, CoeffsToSlots, scale normalisation, EvalMod, SlotsToCoeffs
     const auto gc = stage_groups(logn, bc, true);
     const auto gs = stage_groups(logn, bs, false);
     bp->level_after_cts = top - 1 - (int)gc.size();
@@ -524,7 +557,7 @@ fides_status fides_bootstrap_setup(fides_ctx* c, const fides_boot_params* prm) {
         M[0] = std::vector<cplx>(n, 1.0);
         for (int s : gc[b]) M = diag_mul(n, fft_stage(n, s, true), M);
         BootStage st;
-        fides_status e = encode_stage(c, n, M, top - 1 - (int)b, 1.0, st);
+        fides_status e = encode_stage(c, n, M, top - (int)b, 1.0, kCtsDiagScale, st);
         bp->cts.push_back(std::move(st));
         if (e != FIDES_OK) return e;
     }
@@ -535,7 +568,7 @@ fides_status fides_bootstrap_setup(fides_ctx* c, const fides_boot_params* prm) {
         M[0] = std::vector<cplx>(n, 1.0);
         for (int s : gs[b]) M = diag_mul(n, fft_stage(n, s, false), M);
         BootStage st;
-        fides_status e = encode_stage(c, n, M, bp->level_after_mod - (int)b, b == 0 ? fac : 1.0, st);
+        fides_status e = encode_stage(c, n, M, bp->level_after_mod - (int)b, b == 0 ? fac : 1.0, 0.0, st);
         bp->stc.push_back(std::move(st));
         if (e != FIDES_OK) return e;
     }
@@ -573,20 +606,26 @@ fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
     if (it == c->boot.end()) return set_err(c, FIDES_BAD_ARG, "bootstrapping not set up for these slots");
     const BootPrecomp& B = *it->second;
     if (!c->has_relin) return set_err(c, FIDES_KEY_MISSING, "no relinearisation key");
-    const int top = c->L - 1, N = c->N;
+    const int N = c->N;
     const double d_in = in->scale;
     Arith A(c);
     Lanes x = A.fresh(1);
-    fides_status s = fides_mod_raise(c, in, x[0]);
+    fides_status s = FIDES_OK;
+    if (B.correction > 0) {
+        // message times 2^correction (exact integer product of limb 0 and up)
+        Lanes pre = A.fresh(1);
+        if ((s = fides_mult_int(c, in, (int64_t)1 << B.correction, pre[0])) != FIDES_OK) return s;
+        s = fides_mod_raise(c, pre[0], x[0]);
+    } else {
+        s = fides_mod_raise(c, in, x[0]);
+    }
     if (s != FIDES_OK) return s;
     x[0]->scale = B.K * (double)c->host.prime[0];
     x[0]->slots = n;
-    // integer multiply + rescale: scale K q0 -> half the modulus EvalMod starts
-    // at, values unchanged; the real / imaginary split doubles it, so the
-    // Chebyshev input's scale equals its own level's modulus and the squarings
-    // of the series keep their scales next to the moduli they are divided by
-    x = A.lin({{&x, 1.0}}, 0.0, top, 0.5 * (double)c->host.prime[B.level_after_cts], x);
-    if (!A.ok()) return A.st;
+    // CoeffsToSlots from the scale K q0 (about 2^64, growing by 2^8 per
+    // transform): its rescaling and key-switching noise and the rounding of
+    // its diagonals stay small against t, whose error EvalMod multiplies by
+    // 2 pi K and SlotsToCoeffs by about sqrt(n) q0 / (2 pi D)
     for (const BootStage& st : B.cts) {
         Lanes y = A.fresh(1);
         s = fides_linear_transform(c, x[0], (int)st.offsets.size(), st.offsets.data(),
@@ -594,6 +633,13 @@ fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
         if (s != FIDES_OK) return s;
         x = y;
     }
+    // integer multiply + rescale: scale -> about half the modulus EvalMod
+    // starts at (exactly tracked), values unchanged; the real / imaginary split
+    // doubles it, so the Chebyshev input's scale sits at its own level's
+    // modulus and the squarings of the series keep their scales next to the
+    // moduli they are divided by
+    x = A.normalize(x, 0.5 * (double)c->host.prime[B.level_after_cts]);
+    if (!A.ok()) return A.st;
     // real and imaginary parts: (x + conj x), -i (x - conj x), each twice the part
     Lanes cj = A.fresh(1);
     if ((s = fides_conjugate(c, x[0], cj[0])) != FIDES_OK) return s;
@@ -627,7 +673,7 @@ fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
         if (s != FIDES_OK) return s;
         w = y;
     }
-    const double sc = w[0]->scale * d_in / c->default_scale;
+    const double sc = w[0]->scale * d_in / c->default_scale * (double)(1ll << B.correction);
     s = fides_ct_copy(c, w[0], out);
     if (s != FIDES_OK) return s;
     out->scale = sc;

@@ -19,6 +19,7 @@ constexpr int kMaxBatch = 32;  // ciphertexts per batched launch (blockIdx.z)
 struct DevCtx {
     int logN, N, L, K, dnum, alpha;
     int ntt_variant;             // NTT kernel variant chosen by the autotuner
+    int split_conv;              // 1: every modulus < 2^60, conversions use split 32-bit products
     const PrimeConst* pc;        // [L+K]
     const uint64_t* fwd_tw;      // [L+K][N][2]  psi^{bitrev(i)}, companion
     const uint64_t* inv_tw;      // [L+K][N][2]  psi^{-bitrev(i)}, companion

@@ -411,6 +411,7 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.K = K;
     d.dnum = c->dnum;
     d.alpha = c->alpha;
+    d.split_conv = 0;  // chosen by the autotuner
     d.pc = (const PrimeConst*)(base + parts[i_pc].off);
     d.fwd_tw = (const uint64_t*)(base + parts[i_fwd].off);
     d.inv_tw = (const uint64_t*)(base + parts[i_inv].off);
@@ -498,7 +499,7 @@ void int_const_limbs(const fides_ctx* c, int64_t z, int nlimbs, uint64_t (*out)[
     }
 }
 
-fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st, cudaMemPool_t pool) {
+fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st) {
     if (!st) st = c->st;
     if (ct->buf && ct->cap >= level + 1) return FIDES_OK;
     if (ct->buf) cudaFreeAsync(ct->buf, st);
@@ -506,8 +507,7 @@ fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st, 
     ct->cap = level + 1;
     ct->ring = c->N;
     const size_t bytes = 2 * (size_t)ct->cap * c->limb_bytes();
-    const cudaError_t e = pool ? cudaMallocFromPoolAsync((void**)&ct->buf, bytes, pool, st)
-                               : cudaMallocAsync((void**)&ct->buf, bytes, st);
+    const cudaError_t e = cudaMallocAsync((void**)&ct->buf, bytes, st);
     if (e != cudaSuccess) {
         ct->cap = 0;
         cudaGetLastError();

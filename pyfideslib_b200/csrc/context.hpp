@@ -107,6 +107,8 @@ struct fides_ctx {
 
     int tuned_variant = 0;
     std::vector<float> tune_ms;
+    int tuned_conv = 0;  // base-conversion accumulator: 0 128-bit, 1 split 32-bit products
+    std::vector<float> conv_ms;
     std::string last_error;
     std::recursive_mutex mu;
 
@@ -123,9 +125,8 @@ fides_status encode_dev(fides_ctx* c, const double* values, int slots, int level
 // Per-limb integer constant z mod q_j with its Shoup companion, z of any sign.
 void int_const_limbs(const fides_ctx* c, int64_t z, int nlimbs, uint64_t (*out)[2]);
 // Output buffer of `level`+1 limbs per component, stream-ordered on `st`
-// (default: the context stream), from `pool` when given.
-fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st = nullptr,
-                        cudaMemPool_t pool = nullptr);
+// (default: the context stream).
+fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st = nullptr);
 fides_status build_context(fides_ctx* c, const fides_params* p);
 bool select_moduli(const fides_params* prm, std::vector<uint64_t>& q, std::vector<uint64_t>& p);
 void free_context(fides_ctx* c);

@@ -81,18 +81,24 @@ constexpr int kConvThreads = 128;
 constexpr int kConvTargets = 32;  // targets per block
 constexpr int kMaxConvIn = 16;    // digit size / special count handled in registers
 
-__device__ __forceinline__ void conv_store(uint64_t* out, const Acc128& a, const Acc128& b, const PrimeConst& pc) {
+template <class ACC>
+__device__ __forceinline__ void conv_store(uint64_t* out, const ACC& a, const ACC& b, const PrimeConst& pc) {
     ulonglong2 o;
     o.x = a.reduce(pc);
     o.y = b.reduce(pc);
     *reinterpret_cast<ulonglong2*>(out) = o;
 }
 
+// MAXIN: the register arrays and unrolled loops cover MAXIN inputs (the digit
+// size rounded up to a multiple of 4), so no issue slot goes to inputs that
+// do not exist.  ACC: Acc128, or AccSplit when every modulus is below 2^60;
+// the autotuner picks per context (identical sums).
+template <int MAXIN, class ACC>
 __global__ void __launch_bounds__(kConvThreads) k_modup_conv(const __grid_constant__ DevCtx ctx, int level,
                                                              const uint64_t* __restrict__ xt,
                                                              uint64_t* __restrict__ dig, size_t dig_stride,
                                                              size_t bstride) {
-    __shared__ uint64_t sM[kMaxConvIn][kConvTargets];
+    __shared__ uint64_t sM[MAXIN][kConvTargets];
     __shared__ PrimeConst sP[kConvTargets];
     const int ndig = level / ctx.alpha + 1;
     const int d = blockIdx.y % ndig;
@@ -117,9 +123,9 @@ __global__ void __launch_bounds__(kConvThreads) k_modup_conv(const __grid_consta
         if (i == 0) sP[mm] = ctx.pc[t];
     }
     const size_t j = ((size_t)blockIdx.x * kConvThreads + threadIdx.x) * 2;
-    uint64_t x0[kMaxConvIn], x1[kMaxConvIn];
+    uint64_t x0[MAXIN], x1[MAXIN];
 #pragma unroll
-    for (int i = 0; i < kMaxConvIn; ++i) {
+    for (int i = 0; i < MAXIN; ++i) {
         if (i < cnt) {
             const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(xt + (size_t)(lo + i) * ctx.N + j);
             x0[i] = v.x;
@@ -132,9 +138,9 @@ __global__ void __launch_bounds__(kConvThreads) k_modup_conv(const __grid_consta
 #pragma unroll 1
     for (int mm = 0; mm < nt; mm += 2) {
         const int m2 = mm + 1 < nt ? mm + 1 : mm;
-        Acc128 a, b, c2, d2;
+        ACC a, b, c2, d2;
 #pragma unroll
-        for (int i = 0; i < kMaxConvIn; ++i) {
+        for (int i = 0; i < MAXIN; ++i) {
             if (i < cnt) {
                 const uint64_t M = sM[i][mm], M2 = sM[i][m2];
                 a.mac(x0[i], M);
@@ -156,7 +162,21 @@ void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt,
     const int maxtar = level + 1 + ctx.K;
     dim3 g(ctx.N / (2 * kConvThreads), nd * nb, (maxtar + kConvTargets - 1) / kConvTargets);
     count_launches(1);
-    k_modup_conv<<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride, bstride);
+#define FIDES_MODUP(M)                                                                                    \
+    if (ctx.split_conv)                                                                                  \
+        k_modup_conv<M, AccSplit><<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride, bstride); \
+    else                                                                                                 \
+        k_modup_conv<M, Acc128><<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride, bstride);
+    if (ctx.alpha <= 4) {
+        FIDES_MODUP(4)
+    } else if (ctx.alpha <= 8) {
+        FIDES_MODUP(8)
+    } else if (ctx.alpha <= 12) {
+        FIDES_MODUP(12)
+    } else {
+        FIDES_MODUP(16)
+    }
+#undef FIDES_MODUP
 }
 
 // ---------------------------------------------------------------------------
@@ -171,7 +191,7 @@ void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt,
 // Batch element b = blockIdx.x % nb varies fastest, so the blocks that read
 // one key tile for the different elements run back to back and the key is
 // fetched from HBM once and served from L2 to the rest of the batch.
-template <int VEC>
+template <int VEC, class ACC>
 __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx ctx, int level, int nb,
                                                   const __grid_constant__ KsArgs args) {
     const int n = level + 1;
@@ -205,7 +225,7 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
     uint64_t* xa = args.xa + boff + (size_t)m * ctx.N;
     if constexpr (VEC) {
         const size_t j = ((size_t)bx * blockDim.x + threadIdx.x) * 2;
-        Acc128 sb0, sb1, sa0, sa1;
+        ACC sb0, sb1, sa0, sa1;
 #pragma unroll
         for (int d = 0; d < 8; ++d) {
             if (d < nd) {
@@ -229,7 +249,7 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
         const int j = bx * blockDim.x + threadIdx.x;
         const uint32_t g = args.galois[bi];
         const uint32_t src = g ? automorph_slot(ctx.logN, g, j) : (uint32_t)j;
-        Acc128 sb, sa;
+        ACC sb, sa;
 #pragma unroll
         for (int d = 0; d < 8; ++d) {
             if (d < nd) {
@@ -252,10 +272,16 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
     count_launches(1);
     if (plain) {
         dim3 g(ctx.N / 512 * nb, level + 1 + ctx.K);
-        k_ks_inner<1><<<g, 256, 0, st>>>(ctx, level, nb, args);
+        if (ctx.split_conv)
+            k_ks_inner<1, AccSplit><<<g, 256, 0, st>>>(ctx, level, nb, args);
+        else
+            k_ks_inner<1, Acc128><<<g, 256, 0, st>>>(ctx, level, nb, args);
     } else {
         dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
-        k_ks_inner<0><<<g, 256, 0, st>>>(ctx, level, nb, args);
+        if (ctx.split_conv)
+            k_ks_inner<0, AccSplit><<<g, 256, 0, st>>>(ctx, level, nb, args);
+        else
+            k_ks_inner<0, Acc128><<<g, 256, 0, st>>>(ctx, level, nb, args);
     }
 }
 
@@ -276,9 +302,10 @@ __device__ __forceinline__ uint64_t switch_modulus_d(uint64_t a, uint64_t om, co
 }
 
 
+template <int MAXIN, class ACC>
 __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_constant__ DevCtx ctx, int level,
                                                                const __grid_constant__ MdArgs args) {
-    __shared__ uint64_t sM[kMaxConvIn][kConvTargets];
+    __shared__ uint64_t sM[MAXIN][kConvTargets];
     __shared__ PrimeConst sP[kConvTargets];
     __shared__ ulonglong2 sPinv[kConvTargets];
     const int half = blockIdx.z & 1;
@@ -300,9 +327,9 @@ __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_cons
         }
     }
     const size_t j = ((size_t)blockIdx.x * kConvThreads + threadIdx.x) * 2;
-    uint64_t y0[kMaxConvIn], y1[kMaxConvIn];
+    uint64_t y0[MAXIN], y1[MAXIN];
 #pragma unroll
-    for (int k = 0; k < kMaxConvIn; ++k) {
+    for (int k = 0; k < MAXIN; ++k) {
         if (k < K) {
             const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(y + (size_t)k * ctx.N + j);
             y0[k] = v.x;
@@ -314,9 +341,9 @@ __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_cons
     if (ttop) {
         const PrimeConst pl = ctx.pc[level];
         const ulonglong2 pinv_l = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[level];
-        Acc128 a, b;
+        ACC a, b;
 #pragma unroll
-        for (int k = 0; k < kMaxConvIn; ++k) {
+        for (int k = 0; k < MAXIN; ++k) {
             if (k < K) {
                 const uint64_t M = ctx.md_mat[(size_t)k * L + level];
                 a.mac(y0[k], M);
@@ -329,7 +356,7 @@ __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_cons
         ql = pl.p;
     }
     __syncthreads();
-    auto finish = [&](int qq, const Acc128& a, const Acc128& b) {
+    auto finish = [&](int qq, const ACC& a, const ACC& b) {
         const PrimeConst pc = sP[qq];
         ulonglong2 o;
         o.x = a.reduce(pc);
@@ -344,9 +371,9 @@ __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_cons
 #pragma unroll 1
     for (int qq = 0; qq < nt; qq += 2) {
         const int q2 = qq + 1 < nt ? qq + 1 : qq;
-        Acc128 a, b, c2, d2;
+        ACC a, b, c2, d2;
 #pragma unroll
-        for (int k = 0; k < kMaxConvIn; ++k) {
+        for (int k = 0; k < MAXIN; ++k) {
             if (k < K) {
                 const uint64_t M = sM[k][qq], M2 = sM[k][q2];
                 a.mac(y0[k], M);
@@ -365,7 +392,21 @@ void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& a, 
     if (nout <= 0) return;
     dim3 g(ctx.N / (2 * kConvThreads), (nout + kConvTargets - 1) / kConvTargets, 2 * nb);
     count_launches(1);
-    k_moddown_conv<<<g, kConvThreads, 0, st>>>(ctx, level, a);
+#define FIDES_MODDOWN(M)                                                      \
+    if (ctx.split_conv)                                                       \
+        k_moddown_conv<M, AccSplit><<<g, kConvThreads, 0, st>>>(ctx, level, a); \
+    else                                                                      \
+        k_moddown_conv<M, Acc128><<<g, kConvThreads, 0, st>>>(ctx, level, a);
+    if (ctx.K <= 4) {
+        FIDES_MODDOWN(4)
+    } else if (ctx.K <= 8) {
+        FIDES_MODDOWN(8)
+    } else if (ctx.K <= 12) {
+        FIDES_MODDOWN(12)
+    } else {
+        FIDES_MODDOWN(16)
+    }
+#undef FIDES_MODDOWN
 }
 
 // ---------------------------------------------------------------------------

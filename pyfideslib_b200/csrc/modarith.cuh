@@ -90,6 +90,45 @@ struct Acc128 {
     FHD uint64_t reduce(const PrimeConst& c) const { return reduce128(hi, lo, c); }
 };
 
+// Sum of up to 16 products of residues below 2^60 kept as 32-bit partial
+// products (a = a1 2^32 + a0, b = b1 2^32 + b0, a1, b1 < 2^28):
+//   s11 = sum a1 b1 < 2^60,  s10 = sum a1 b0 < 2^64,  s01 = sum a0 b1 < 2^64,
+//   w = sum a0 b0 < 2^68 in three 32-bit words.
+// Each product costs four multiply-adds and no carry handling between 64-bit
+// halves; the 128-bit total is formed once, in reduce().  Same value as Acc128.
+struct AccSplit {
+    uint64_t s11, s10, s01;
+    uint32_t w0, w1, w2;
+    FHD AccSplit() : s11(0), s10(0), s01(0), w0(0), w1(0), w2(0) {}
+    FHD void mac(uint64_t a, uint64_t b) {
+        const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+        s11 += (uint64_t)a1 * b1;
+        s10 += (uint64_t)a1 * b0;
+        s01 += (uint64_t)a0 * b1;
+#if defined(__CUDA_ARCH__)
+        asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+            "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+            "addc.u32 %2, %2, 0;"
+            : "+r"(w0), "+r"(w1), "+r"(w2)
+            : "r"(a0), "r"(b0));
+#else
+        const unsigned __int128 w = (((unsigned __int128)w2 << 64) | ((uint64_t)w1 << 32) | w0) + (uint64_t)a0 * b0;
+        w0 = (uint32_t)w;
+        w1 = (uint32_t)(w >> 32);
+        w2 = (uint32_t)(w >> 64);
+#endif
+    }
+    // total = s11 2^64 + (s10 + s01) 2^32 + (w2 2^64 + w1 2^32 + w0)
+    FHD uint64_t reduce(const PrimeConst& c) const {
+        const uint64_t mid = s10 + s01;
+        const uint64_t mid_carry = mid < s10 ? 1 : 0;  // bit 64 of s10 + s01
+        const uint64_t lo0 = ((uint64_t)w1 << 32) | w0;
+        const uint64_t lo = lo0 + (mid << 32);
+        const uint64_t hi = s11 + (mid >> 32) + (mid_carry << 32) + w2 + (lo < lo0 ? 1 : 0);
+        return reduce128(hi, lo, c);
+    }
+};
+
 FHD uint64_t mul_mod(uint64_t a, uint64_t b, const PrimeConst& c) {
     return reduce128(mulhi64(a, b), a * b, c);
 }

@@ -34,20 +34,40 @@
 
 namespace fides {
 
-// Forward butterfly.  Harvey's form keeps X in [0, 4p) with one conditional
-// subtraction per butterfly; for primes below 2^57 (LAZY) the subtraction is
-// dropped: each stage adds at most 2p to the bound, so after the 16 stages of
-// a 2^16 transform values stay below 33p < 2^63 (the Shoup product accepts any
-// 64-bit input) and one reduction in the epilogue suffices.
+// Forward butterfly.  MODE 0 is Harvey's form: X kept in [0, 4p) with one
+// conditional subtraction per butterfly.  For primes below 2^57, MODE 1 drops
+// the subtraction: each stage adds at most 2p to the bound, so after the 16
+// stages of a 2^16 transform values stay below 33p < 2^63 (the Shoup product
+// accepts any 64-bit input) and one reduction in the epilogue suffices.
+// MODE 3 (primes below 2^56) also forms the Shoup quotient from three of the
+// four 32x32 partial products: it is low by at most 2, the product lands in
+// [0, 4p), and the bound after 16 stages is 65p < 2^63.
 constexpr uint64_t kLazyPrimeBound = 1ull << 57;
+constexpr uint64_t kApproxPrimeBound = 1ull << 56;
 
-template <bool LAZY>
+// floor(a * b / 2^64) - d with d in {0, 1, 2}
+__device__ __forceinline__ uint64_t mulhi64_approx(uint64_t a, uint64_t b) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    uint64_t h = (uint64_t)a1 * b1;
+    h += __umulhi(a1, b0);
+    h += __umulhi(a0, b1);
+    return h;
+}
+
+template <int MODE>
 __device__ __forceinline__ void ct_bfly(uint64_t& X, uint64_t& Y, const ulonglong2 w, const uint64_t p,
                                         const uint64_t two_p) {
-    const uint64_t x = LAZY ? X : csub(X, two_p);
-    const uint64_t t = mul_shoup_lazy(Y, w.x, w.y, p);
-    X = x + t;
-    Y = x - t + two_p;
+    if constexpr (MODE == 3) {
+        const uint64_t t = Y * w.x - mulhi64_approx(Y, w.y) * p;  // [0, 4p)
+        const uint64_t x = X;
+        X = x + t;
+        Y = x - t + 2 * two_p;
+    } else {
+        const uint64_t x = MODE == 1 ? X : csub(X, two_p);
+        const uint64_t t = mul_shoup_lazy(Y, w.x, w.y, p);
+        X = x + t;
+        Y = x - t + two_p;
+    }
 }
 
 __device__ __forceinline__ void gs_bfly(uint64_t& X, uint64_t& Y, const ulonglong2 w, const uint64_t p,
@@ -101,15 +121,16 @@ __device__ __forceinline__ void run_stages(uint64_t (&x)[16], ulonglong2 (&w)[15
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
         if (k & (1 << KB)) continue;
-        if constexpr (MODE < 2)
-            ct_bfly<MODE == 1>(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
+        if constexpr (MODE != 2)
+            ct_bfly<MODE>(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
         else
             gs_bfly(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
     }
     if constexpr (KB != KB_END) run_stages<KB + STEP, KB_END, STEP, PF, MODE>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
 }
 
-// MODE: 0 forward, 1 forward without the per-butterfly reduction, 2 inverse
+// MODE: 0 forward, 1 forward without the per-butterfly reduction, 2 inverse,
+// 3 forward lazy with the approximate Shoup quotient
 template <int KB_FIRST, int KB_LAST, bool PF, int MODE, class Tab>
 __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi, uint64_t p,
                                           uint64_t two_p) {
@@ -128,6 +149,30 @@ __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_k
     run_stages<KB_FIRST, KB_LAST, STEP, PF, MODE>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
 }
 
+// Forward group in the mode of this limb's prime (uniform per CTA).
+template <int KF, int KL, bool PF, bool AQ, class Tab>
+__device__ __forceinline__ void fwd_group(int fmode, uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi,
+                                          uint64_t p, uint64_t two_p) {
+    if constexpr (AQ) {
+        if (fmode == 3) {
+            run_group<KF, KL, PF, 3>(x, tab, t_of_kb0, B, th_hi, p, two_p);
+            return;
+        }
+    } else {
+        if (fmode == 1) {
+            run_group<KF, KL, PF, 1>(x, tab, t_of_kb0, B, th_hi, p, two_p);
+            return;
+        }
+    }
+    run_group<KF, KL, PF, 0>(x, tab, t_of_kb0, B, th_hi, p, two_p);
+}
+
+template <bool AQ>
+__device__ __forceinline__ int fwd_mode(uint64_t p) {
+    if constexpr (AQ) return p < kApproxPrimeBound ? 3 : 0;
+    return p < kLazyPrimeBound ? 1 : 0;
+}
+
 // Tile geometry shared by kernels and launchers.
 template <int LR, int LC>
 struct Geo {
@@ -144,7 +189,7 @@ struct Geo {
 // ---------------------------------------------------------------------------
 // forward, pass 1: column stages 0..LR-1
 // ---------------------------------------------------------------------------
-template <int LR, int LC, int MINB, bool PF>
+template <int LR, int LC, int MINB, bool PF, bool AQ>
 __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
@@ -171,11 +216,8 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
     __syncthreads();
     auto tab = [&](size_t i) { return tws[i]; };
     // stages 0..3: r = th + (k << (LR - 4)), twiddle (1 << t) + (k >> (4 - t))
-    const bool lazy = pc.p < kLazyPrimeBound;
-    if (lazy)
-        run_group<3, 0, PF, 1>(x, tab, 3, 1, 0, pc.p, pc.two_p);
-    else
-        run_group<3, 0, PF, 0>(x, tab, 3, 1, 0, pc.p, pc.two_p);
+    const int fmode = fwd_mode<AQ>(pc.p);
+    fwd_group<3, 0, PF, AQ>(fmode, x, tab, 3, 1, 0, pc.p, pc.two_p);
     if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) sm[(th + (k << (LR - 4))) * TC + c] = x[k];
@@ -183,10 +225,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = sm[((th << 4) + k) * TC + c];
         // stages 4..LR-1: r = 16 th + k
-        if (lazy)
-            run_group<LR - 5, 0, PF, 1>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
-        else
-            run_group<LR - 5, 0, PF, 0>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
+        fwd_group<LR - 5, 0, PF, AQ>(fmode, x, tab, LR - 1, 1, th, pc.p, pc.two_p);
 #pragma unroll
         for (int k = 0; k < 16; ++k) lr.out[(size_t)((th << 4) + k) * C + col] = x[k];
     } else {
@@ -228,7 +267,7 @@ __device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRe
 // mappings hit 16 distinct bank pairs.
 __device__ __forceinline__ int padi(int r) { return r + (r >> 4); }
 
-template <int LR, int LC, int MINB, bool PF>
+template <int LR, int LC, int MINB, bool PF, bool AQ>
 __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
@@ -246,11 +285,8 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
     uint64_t x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
-    const bool lazy = pc.p < kLazyPrimeBound;
-    if (lazy)
-        run_group<3, 0, PF, 1>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
-    else
-        run_group<3, 0, PF, 0>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
+    const int fmode = fwd_mode<AQ>(pc.p);
+    fwd_group<3, 0, PF, AQ>(fmode, x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
 #pragma unroll
@@ -258,10 +294,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        if (lazy)
-            run_group<LC - 5, 0, PF, 1>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
-        else
-            run_group<LC - 5, 0, PF, 0>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
+        fwd_group<LC - 5, 0, PF, AQ>(fmode, x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
         // each thread rewrites exactly the slots it read
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
@@ -412,17 +445,17 @@ bool ntt_supported(int logN) { return logN >= 8 && logN <= 16; }
 
 // Variants: (min CTAs per SM, twiddle policy).  0: (2, group prefetch),
 // 1: (3, per-stage), 2: (4, per-stage).
-int ntt_num_variants() { return 3; }
+int ntt_num_variants() { return 5; }
 
-template <int LR, int LC, int MINB, bool PF>
+template <int LR, int LC, int MINB, bool PF, bool AQ>
 static void launch_fwd_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
     // grid (tiles, batch element, limb): CTAs run x fastest, then y, so the
     // elements of a batch that share a prime run together and its twiddle
     // table is fetched from HBM once per launch rather than once per element
     dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
-    k_ntt_fwd_cols<LR, LC, MINB, PF><<<g1, G::NTC, 0, st>>>(ctx, map);
-    k_ntt_fwd_rows<LR, LC, MINB, PF><<<g2, G::NTR, 0, st>>>(ctx, map);
+    k_ntt_fwd_cols<LR, LC, MINB, PF, AQ><<<g1, G::NTC, 0, st>>>(ctx, map);
+    k_ntt_fwd_rows<LR, LC, MINB, PF, AQ><<<g2, G::NTR, 0, st>>>(ctx, map);
 }
 
 template <int LR, int LC, int MINB, bool PF>
@@ -439,16 +472,19 @@ static void launch_inv_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st)
 template <int LR, int LC>
 static void launch_fwd(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     switch (ctx.ntt_variant) {
-        case 1: launch_fwd_v<LR, LC, 3, false>(ctx, map, st); break;
-        case 2: launch_fwd_v<LR, LC, 4, false>(ctx, map, st); break;
-        default: launch_fwd_v<LR, LC, 2, true>(ctx, map, st); break;
+        case 1: launch_fwd_v<LR, LC, 3, false, false>(ctx, map, st); break;
+        case 2: launch_fwd_v<LR, LC, 4, false, false>(ctx, map, st); break;
+        case 3: launch_fwd_v<LR, LC, 3, false, true>(ctx, map, st); break;
+        case 4: launch_fwd_v<LR, LC, 2, true, true>(ctx, map, st); break;
+        default: launch_fwd_v<LR, LC, 2, true, false>(ctx, map, st); break;
     }
 }
 
 template <int LR, int LC>
 static void launch_inv(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     switch (ctx.ntt_variant) {
-        case 1: launch_inv_v<LR, LC, 3, false>(ctx, map, st); break;
+        case 1:
+        case 3: launch_inv_v<LR, LC, 3, false>(ctx, map, st); break;
         case 2: launch_inv_v<LR, LC, 4, false>(ctx, map, st); break;
         default: launch_inv_v<LR, LC, 2, true>(ctx, map, st); break;
     }

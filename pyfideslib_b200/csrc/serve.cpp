@@ -60,9 +60,6 @@ struct fides_server {
     fides_ctx* c = nullptr;
     size_t budget = 0, reserved = 0, ws_bytes = 0;
     int max_batch = 16;
-    // outputs of admitted requests come from this pool, which keeps up to the
-    // budget cached once touched, so admission never waits on the driver
-    cudaMemPool_t pool = nullptr;
     std::vector<Lane> lanes;
     Lane boot;                // bootstrap lane: context stream, one request at a time
     size_t boot_scratch = 0;  // HBM charged per bootstrap besides its output
@@ -102,7 +99,7 @@ void launch_batch(fides_server* s, Lane& ln) {
     for (Request* r : ln.batch) {
         r->t_start = clk::now();
         const int out_level = (op == FIDES_OP_HMULT && level > 0) ? level - 1 : level;
-        if (ct_reserve(c, r->out, out_level, ln.st, s->pool) != FIDES_OK) {
+        if (ct_reserve(c, r->out, out_level, ln.st) != FIDES_OK) {
             r->status = FIDES_OOM;
             continue;
         }
@@ -286,29 +283,6 @@ fides_status fides_srv_create(fides_ctx* c, size_t hbm_budget, int max_batch, in
     cudaEventCreateWithFlags(&s->boot.ev, cudaEventDisableTiming);
     // a bootstrap holds about 64 top-level ciphertexts of intermediates
     s->boot_scratch = 64 * out_bytes(c, c->L - 1);
-    {
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = c->device;
-        if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
-            cudaGetLastError();
-            s->pool = nullptr;
-            fides_srv_destroy(s);
-            return set_err(c, FIDES_CUDA_ERR, "serving memory pool");
-        }
-        uint64_t keep = s->budget - s->ws_bytes;
-        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-        // touch part of the budget once so the first requests find it mapped
-        const size_t warm = std::min<size_t>(keep, (size_t)4 << 30);
-        void* w = nullptr;
-        if (cudaMallocFromPoolAsync(&w, warm, s->pool, s->lanes[0].st) == cudaSuccess) {
-            cudaFreeAsync(w, s->lanes[0].st);
-        } else {
-            cudaGetLastError();
-        }
-        cudaStreamSynchronize(s->lanes[0].st);
-    }
     s->th = std::thread(scheduler, s);
     *out = s;
     return FIDES_OK;
@@ -421,8 +395,6 @@ fides_status fides_srv_destroy(fides_server* s) {
     if (s->boot.st) cudaStreamSynchronize(s->boot.st);  // the context's stream: not destroyed here
     if (s->boot.ev) cudaEventDestroy(s->boot.ev);
     for (auto& kv : s->all) delete kv.second;
-    // outputs still held by the caller keep their memory until freed
-    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return FIDES_OK;
 }

@@ -60,7 +60,8 @@ using namespace fides;
 int main(int argc, char** argv) {
     std::mt19937_64 r(1);
     const uint64_t primes[] = {17ull, 2305843009218281473ull, 2251799661248513ull, 2305843009247641601ull,
-                               (1ull << 61) - 1, 4611686018427387847ull /* < 2^62 */};
+                               (1ull << 61) - 1, 4611686018427387847ull /* < 2^62 */,
+                               1152921504606830593ull /* < 2^60 */};
     for (uint64_t p : primes) {
         PrimeConst c{};
         c.p = p; c.two_p = 2 * p;
@@ -78,6 +79,14 @@ int main(int argc, char** argv) {
             Acc128 acc; unsigned __int128 ref = 0;
             for (int k = 0; k < 15; ++k) { uint64_t x = r() % p, y = r() % p; acc.mac(x, y); ref += (unsigned __int128)x * y; }
             if (acc.reduce(c) != (uint64_t)(ref % p)) { printf("acc\n"); return 1; }
+            if (p < (1ull << 60)) {
+                AccSplit sa; unsigned __int128 sref = 0;
+                for (int k = 0; k < 16; ++k) {
+                    uint64_t x = (t & 1) ? p - 1 - (r() & 7) : r() % p, y = (t & 2) ? p - 1 : r() % p;
+                    sa.mac(x, y); sref += (unsigned __int128)x * y;
+                }
+                if (sa.reduce(c) != (uint64_t)(sref % p)) { printf("accsplit\n"); return 1; }
+            }
         }
     }
     printf("ok\n");

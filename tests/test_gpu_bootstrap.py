@@ -106,6 +106,14 @@ def test_bootstrap_precision():
         sq = cc.EvalMult(bt, bt, rescale=True)
         err2 = np.max(np.abs(cc.Decrypt(sk, sq, slots=slots) - m * m))
         assert err2 < 2 ** -10, err2
+    # the correction factor lifts the message against EvalMod's noise (2^3:
+    # beyond that, at N = 2^12, the sine's cubic term on the largest message
+    # coefficients takes over)
+    cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=63, correction=3)
+    m = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+    ct = cc.Encrypt(sk, m, slots=slots, level=0)
+    err5 = np.max(np.abs(cc.Decrypt(sk, cc.EvalBootstrap(ct), slots=slots) - m))
+    assert -np.log2(err5) > bits + 1.5, (err5, err)
 
 
 def test_bootstrap_requests_served_in_mix():

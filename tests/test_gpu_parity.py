@@ -6,6 +6,8 @@ logN 13..16 (test/NTTtests.cu), Mult/Square/MultRescale at every level
 reference's own prime lists (test/ParametrizedTest.cuh p64/sp64) and on the
 generated moduli of the HMult workload (N=2^16, L=30, K=10, dnum=3).
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -26,6 +28,36 @@ def test_ntt_roundtrip_and_parity(logN):
     assert np.array_equal(got, want)
     cc.ntt(d.data_ptr(), 0, nl, inverse=True)
     assert np.array_equal(from_dev(d), x)
+
+
+@pytest.mark.parametrize("logN", [12, 16])
+def test_every_ntt_variant_bitexact(logN):
+    """Every autotuner variant (occupancy, twiddle fetch, lazy or approximate
+    quotient butterflies) gives the oracle's residues, forward and inverse,
+    single and batched, on 50- and 60-bit primes."""
+    from pyfideslib_b200._capi import lib
+
+    cc, oc = make_pair(logN, 8, 3, 3)
+    nl = 11  # 8 ciphertext moduli (60 + 7 x 50 bits) and 3 special 60-bit moduli
+    pid = list(range(nl))
+    x = oc.random(pid, 900 + logN)
+    want = oc.ntt(x, pid)
+    xs = np.stack([x, oc.random(pid, 901 + logN)])
+    want_b = [want, oc.ntt(xs[1], pid)]
+    nv = C.c_int()
+    lib.fides_autotune(cc._h, None, None, C.byref(nv))
+    for v in range(nv.value):
+        cc.set_ntt_variant(v)
+        d = to_dev(x)
+        cc.ntt(d.data_ptr(), 0, nl)
+        assert np.array_equal(from_dev(d), want), v
+        cc.ntt(d.data_ptr(), 0, nl, inverse=True)
+        assert np.array_equal(from_dev(d), x), v
+        db = to_dev(np.ascontiguousarray(xs))
+        cc.ntt_batch(db.data_ptr(), nl * cc.N, 2, 0, nl)
+        got = from_dev(db)
+        assert np.array_equal(got[0], want_b[0]) and np.array_equal(got[1], want_b[1]), v
+    cc.set_ntt_variant(-1)
 
 
 def test_polymul_30_limbs_n16():
@@ -101,6 +133,33 @@ def test_rotate_and_hoisted_parity():
         for o, x0, x1 in zip(outs, w0, w1):
             g0, g1 = o.download()
             assert np.array_equal(g0, x0) and np.array_equal(g1, x1)
+
+
+def test_both_conversion_accumulators_bitexact():
+    """The 128-bit and the split 32-bit-product accumulators of the base
+    conversions and the key-switch inner product give the oracle's residues
+    (HMult with rescale and a rotation at two levels, moduli below 2^60)."""
+    from pyfideslib_b200._capi import lib
+
+    cc, oc = make_pair(12, 9, 3, 3)
+    kb, ka = rand_key(oc, 61)
+    cc.upload_relin_key(kb, ka)
+    g = cc.rotation_galois(3)
+    rk = rand_key(oc, 63)
+    cc.upload_galois_key(g, *rk)
+    for acc in (0, 1):
+        assert lib.fides_set_conv_accumulator(cc._h, acc) == 0
+        for level in (8, 4):
+            a0, a1 = rand_ct(oc, level, 70 + level)
+            b0, b1 = rand_ct(oc, level, 80 + level)
+            A, B = cc.upload(a0, a1), cc.upload(b0, b1)
+            got = cc.EvalMult(A, B, rescale=True).download()
+            want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=True)
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (acc, level)
+            got = cc.EvalRotate(A, 3).download()
+            want = oc.rotate(level, a0, a1, pow(g, -1, 2 * oc.N), *rk)
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (acc, level)
+    assert lib.fides_set_conv_accumulator(cc._h, -1) == 0
 
 
 def test_hmult_c2_shape_bitexact():
