@@ -107,12 +107,16 @@ fides_status fides_key_upload_galois(fides_ctx* ctx, uint32_t galois, const uint
  * inverse element used by the permutation). */
 uint32_t fides_rotation_galois(const fides_ctx* ctx, int32_t index, int slots);
 
-/* ---- ciphertexts (replaces Ciphertext::load / store, Ciphertext.cpp:270-309) ---- */
+/* ---- ciphertexts (replaces Ciphertext::load / store, Ciphertext.cpp:270-309) ----
+ * Uploads run on a copy stream beside the kernels already queued (the host
+ * buffers must stay unchanged until fides_ctx_synchronize; pinned memory lets
+ * the copy overlap); later operations on the ciphertext wait for them. */
 fides_status fides_ct_upload(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level, double scale,
                              int noise_deg, int slots, fides_ct** out);
 fides_status fides_ct_download(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1);
-/* Queue the download without waiting; the host buffers (pinned for overlap)
- * are valid after fides_ctx_synchronize. */
+/* Queue the download without waiting, on the download stream after the
+ * kernels queued so far; the host buffers (pinned for overlap) are valid after
+ * fides_ctx_synchronize.  Freeing or overwriting the ciphertext waits for it. */
 fides_status fides_ct_download_async(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1);
 fides_status fides_ct_info(const fides_ct* ct, int* level, double* scale, int* noise_deg, int* slots);
 fides_status fides_ct_create(fides_ctx* ctx, fides_ct** out); /* empty, filled by an operation */
@@ -159,8 +163,9 @@ fides_status fides_rotate_batch(fides_ctx* ctx, int n, const fides_ct* const* a,
  * output and intermediate buffer and captures the kernel sequence once;
  * fides_plan_launch replays it (a single graph launch) on the context
  * stream, reading the inputs' current residues (fides_ct_write refreshes
- * them).  No counterpart in the reference, which captures per-level graphs
- * of one key switch (LimbPartitionMGPU.cu:581-640, FIDESLIB_USE_GRAPH_CAPTURE). */
+ * them).  a, b and out must outlive the plan.  No counterpart in the
+ * reference, which captures per-level graphs of one key switch
+ * (LimbPartitionMGPU.cu:581-640, FIDESLIB_USE_GRAPH_CAPTURE). */
 fides_status fides_plan_hmult_rotate(fides_ctx* ctx, int n, const fides_ct* const* a, const fides_ct* const* b,
                                      const int32_t* indices, int rescale, fides_ct* const* out, fides_plan** plan);
 fides_status fides_plan_launch(fides_ctx* ctx, fides_plan* plan);

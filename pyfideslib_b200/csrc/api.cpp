@@ -23,6 +23,7 @@ struct Guard {
 
 // Swap a freshly computed buffer into `out` and release the old one.
 void commit(fides_ctx* c, fides_ct* out, fides_ct& tmp) {
+    ct_quiesce(c, out);
     std::swap(out->buf, tmp.buf);
     std::swap(out->cap, tmp.cap);
     std::swap(out->ring, tmp.ring);
@@ -114,7 +115,9 @@ fides_status fides_ctx_info(const fides_ctx* ctx, int* log_n, int* num_q, int* n
 fides_status fides_ctx_synchronize(fides_ctx* ctx) {
     if (!ctx) return FIDES_BAD_ARG;
     Guard g(ctx);
-    if (cudaStreamSynchronize(ctx->st) != cudaSuccess) return check_cuda(ctx, "synchronize");
+    if (cudaStreamSynchronize(ctx->st) != cudaSuccess || cudaStreamSynchronize(ctx->h2d) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->d2h) != cudaSuccess)
+        return check_cuda(ctx, "synchronize");
     return check_cuda(ctx, "synchronize");
 }
 
@@ -272,14 +275,21 @@ fides_status fides_ct_upload(fides_ctx* ctx, const uint64_t* c0, const uint64_t*
     Guard g(ctx);
     fides_ct* ct = new (std::nothrow) fides_ct();
     if (!ct) return FIDES_OOM;
-    fides_status s = ct_reserve(ctx, ct, level);
+    // allocated and filled on the upload stream, so that the copy runs beside
+    // kernels already queued on the context stream, which then waits for it
+    fides_status s = ct_reserve(ctx, ct, level, ctx->h2d);
     if (s != FIDES_OK) {
         delete ct;
         return s;
     }
     const size_t bytes = (size_t)(level + 1) * ctx->limb_bytes();
-    cudaMemcpyAsync(ct->c0(), c0, bytes, cudaMemcpyHostToDevice, ctx->st);
-    cudaMemcpyAsync(ct->c1(ctx->N), c1, bytes, cudaMemcpyHostToDevice, ctx->st);
+    cudaMemcpyAsync(ct->c0(), c0, bytes, cudaMemcpyHostToDevice, ctx->h2d);
+    cudaMemcpyAsync(ct->c1(ctx->N), c1, bytes, cudaMemcpyHostToDevice, ctx->h2d);
+    cudaEvent_t ev;
+    cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    cudaEventRecord(ev, ctx->h2d);
+    cudaStreamWaitEvent(ctx->st, ev, 0);
+    cudaEventDestroy(ev);
     ct->level = level;
     ct->scale = scale;
     ct->noise_deg = noise_deg;
@@ -301,9 +311,19 @@ fides_status fides_ct_download(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0,
 fides_status fides_ct_download_async(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1) {
     if (!ctx || !valid_ct(ctx, ct)) return FIDES_BAD_ARG;
     Guard g(ctx);
+    // on the download stream after the kernels queued so far; later work that
+    // releases or overwrites the buffer waits for the copy (ct_quiesce)
+    cudaEvent_t ready;
+    cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    cudaEventRecord(ready, ctx->st);
+    cudaStreamWaitEvent(ctx->d2h, ready, 0);
+    cudaEventDestroy(ready);
     const size_t bytes = (size_t)(ct->level + 1) * ctx->limb_bytes();
-    if (c0) cudaMemcpyAsync(c0, ct->c0(), bytes, cudaMemcpyDeviceToHost, ctx->st);
-    if (c1) cudaMemcpyAsync(c1, ct->c1(ctx->N), bytes, cudaMemcpyDeviceToHost, ctx->st);
+    if (c0) cudaMemcpyAsync(c0, ct->c0(), bytes, cudaMemcpyDeviceToHost, ctx->d2h);
+    if (c1) cudaMemcpyAsync(c1, ct->c1(ctx->N), bytes, cudaMemcpyDeviceToHost, ctx->d2h);
+    if (ct->d2h_ev) cudaEventDestroy(ct->d2h_ev);  // superseded: same stream, later copy
+    cudaEventCreateWithFlags(&ct->d2h_ev, cudaEventDisableTiming);
+    cudaEventRecord(ct->d2h_ev, ctx->d2h);
     return check_cuda(ctx, "ct download");
 }
 
@@ -326,6 +346,7 @@ fides_status fides_ct_device_ptrs(const fides_ct* ct, uint64_t** c0, uint64_t** 
 fides_status fides_ct_write(fides_ctx* ctx, fides_ct* ct, const uint64_t* c0, const uint64_t* c1) {
     if (!ctx || !valid_ct(ctx, ct) || !c0 || !c1) return FIDES_BAD_ARG;
     Guard g(ctx);
+    ct_quiesce(ctx, ct);
     const size_t bytes = (size_t)(ct->level + 1) * ctx->limb_bytes();
     cudaMemcpyAsync(ct->c0(), c0, bytes, cudaMemcpyHostToDevice, ctx->st);
     cudaMemcpyAsync(ct->c1(ctx->N), c1, bytes, cudaMemcpyHostToDevice, ctx->st);
@@ -351,6 +372,7 @@ fides_status fides_ct_copy(fides_ctx* ctx, const fides_ct* src, fides_ct* dst) {
 fides_status fides_ct_free(fides_ctx* ctx, fides_ct* ct) {
     if (!ctx || !ct) return FIDES_BAD_ARG;
     Guard g(ctx);
+    ct_quiesce(ctx, ct);
     if (ct->buf) cudaFreeAsync(ct->buf, ctx->st);
     delete ct;
     return FIDES_OK;
@@ -1068,6 +1090,7 @@ struct fides_plan {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<fides_ct> inter;  // products feeding the rotations
+    std::vector<fides_ct*> outs;  // written by every replay
 };
 
 extern "C" {
@@ -1102,6 +1125,7 @@ fides_status fides_plan_hmult_rotate(fides_ctx* c, int n, const fides_ct* const*
     if (!p) return FIDES_OOM;
     const bool rot = indices != nullptr;
     if (rot) p->inter.resize(n);
+    p->outs.assign(out, out + n);
     for (int i = 0; i < n; ++i) {
         if (rot) s = ct_reserve(c, &p->inter[i], lv2[i]);
         if (s == FIDES_OK) s = ct_reserve(c, out[i], lv2[i]);
@@ -1199,6 +1223,7 @@ fides_status fides_plan_hmult_rotate(fides_ctx* c, int n, const fides_ct* const*
 fides_status fides_plan_launch(fides_ctx* c, fides_plan* plan) {
     if (!c || !plan || !plan->exec) return FIDES_BAD_ARG;
     Guard g(c);
+    for (fides_ct* o : plan->outs) ct_quiesce(c, o);  // pending downloads of the last replay's results
     count_launches((int)plan->nkernels);
     if (cudaGraphLaunch(plan->exec, c->st) != cudaSuccess) return check_cuda(c, "graph launch");
     return FIDES_OK;

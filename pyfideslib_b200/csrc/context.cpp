@@ -372,6 +372,9 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     // ---- upload ----
     if (cudaSetDevice(prm->device) != cudaSuccess) return set_err(c, FIDES_CUDA_ERR, "cudaSetDevice failed");
     c->device = prm->device;
+    if (cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking) != cudaSuccess)
+        return set_err(c, FIDES_CUDA_ERR, "copy stream creation failed");
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
         return set_err(c, FIDES_CUDA_ERR, "stream create failed");
     struct Part {
@@ -484,8 +487,11 @@ void free_context(fides_ctx* c) {
     ws_free(c->wsb);
     if (c->table_mem) cudaFree(c->table_mem);
     if (c->st) cudaStreamDestroy(c->st);
+    if (c->h2d) cudaStreamSynchronize(c->h2d), cudaStreamDestroy(c->h2d);
+    if (c->d2h) cudaStreamSynchronize(c->d2h), cudaStreamDestroy(c->d2h);
     c->table_mem = nullptr;
     c->st = nullptr;
+    c->h2d = c->d2h = nullptr;
 }
 
 void int_const_limbs(const fides_ctx* c, int64_t z, int nlimbs, uint64_t (*out)[2]) {
@@ -499,8 +505,16 @@ void int_const_limbs(const fides_ctx* c, int64_t z, int nlimbs, uint64_t (*out)[
     }
 }
 
+void ct_quiesce(fides_ctx* c, const fides_ct* ct, cudaStream_t st) {
+    if (!ct->d2h_ev) return;
+    cudaStreamWaitEvent(st ? st : c->st, ct->d2h_ev, 0);
+    cudaEventDestroy(ct->d2h_ev);
+    ct->d2h_ev = nullptr;
+}
+
 fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st) {
     if (!st) st = c->st;
+    ct_quiesce(c, ct, st);
     if (ct->buf && ct->cap >= level + 1) return FIDES_OK;
     if (ct->buf) cudaFreeAsync(ct->buf, st);
     ct->buf = nullptr;

@@ -22,6 +22,9 @@ struct fides_ct {
     uint64_t* buf = nullptr;  // c0 at buf, c1 at buf + cap*N
     int cap = 0;              // limbs per component
     int ring = 0;             // N
+    // completion of the last asynchronous download of this buffer: the buffer
+    // is released or overwritten only after it
+    mutable cudaEvent_t d2h_ev = nullptr;
     uint64_t* c0() const { return buf; }
     uint64_t* c1(size_t N) const { return buf + (size_t)cap * N; }
 };
@@ -85,6 +88,9 @@ struct BootPrecomp;  // bootstrap.cpp
 struct fides_ctx {
     int device = 0;
     cudaStream_t st = nullptr;
+    // copy streams: uploads and asynchronous downloads run on the copy
+    // engines beside the kernels queued on `st`, ordered by events
+    cudaStream_t h2d = nullptr, d2h = nullptr;
     int logN = 0, N = 0, L = 0, K = 0, dnum = 0, alpha = 0;
     double default_scale = 0;
     fides::HostTables host;
@@ -127,6 +133,9 @@ void int_const_limbs(const fides_ctx* c, int64_t z, int nlimbs, uint64_t (*out)[
 // Output buffer of `level`+1 limbs per component, stream-ordered on `st`
 // (default: the context stream).
 fides_status ct_reserve(fides_ctx* c, fides_ct* ct, int level, cudaStream_t st = nullptr);
+// `st` (default: the context stream) waits for a pending asynchronous
+// download of the ciphertext's buffer.
+void ct_quiesce(fides_ctx* c, const fides_ct* ct, cudaStream_t st = nullptr);
 fides_status build_context(fides_ctx* c, const fides_params* p);
 bool select_moduli(const fides_params* prm, std::vector<uint64_t>& q, std::vector<uint64_t>& p);
 void free_context(fides_ctx* c);

@@ -115,3 +115,58 @@ def test_graph_plan_matches_eager_and_replays_new_inputs():
             g0, g1 = outs[i].download()
             w0, w1 = want[i].download()
             assert np.array_equal(g0, w0) and np.array_equal(g1, w1), (rep, i)
+
+
+def test_async_upload_download_pipeline_equals_sync():
+    """Uploads on the copy stream, batched HMult, asynchronous downloads into
+    pinned memory and frees, three rounds queued back to back (the pattern of
+    the end-to-end benchmark): every result equals the synchronous path."""
+    import ctypes as C
+
+    import torch
+
+    from pyfideslib_b200._capi import check, lib, u64p, vp
+
+    cc, oc = make_pair(12, 6, 2, 3)
+    kb, ka = rand_key(oc, 5)
+    cc.upload_relin_key(kb, ka)
+    lv, B, N = 5, 4, cc.N
+    rounds = []
+    for r in range(3):
+        pins = []
+        for i in range(B):
+            pair = []
+            for s in range(2):
+                t = torch.empty((2, lv + 1, N), dtype=torch.int64, pin_memory=True)
+                a = t.numpy().view(np.uint64)
+                a[0], a[1] = rand_ct(oc, lv, 1000 * r + 10 * i + 2 * s)
+                pair.append((t, a))
+            pins.append(pair)
+        rounds.append(pins)
+    outs = [__import__("pyfideslib_b200").Ciphertext(cc) for _ in range(B)]
+    O = (vp * B)(*[o._h for o in outs])
+    host_out = [[torch.empty((2, lv, N), dtype=torch.int64, pin_memory=True) for _ in range(B)] for _ in range(3)]
+    for r in range(3):
+        ha = [vp() for _ in range(B)]
+        hb = [vp() for _ in range(B)]
+        for i in range(B):
+            a, b = rounds[r][i][0][1], rounds[r][i][1][1]
+            check(lib.fides_ct_upload(cc._h, a[0].ctypes.data_as(u64p), a[1].ctypes.data_as(u64p), lv, cc.scale, 1,
+                                      N // 2, C.byref(ha[i])), cc._h)
+            check(lib.fides_ct_upload(cc._h, b[0].ctypes.data_as(u64p), b[1].ctypes.data_as(u64p), lv, cc.scale, 1,
+                                      N // 2, C.byref(hb[i])), cc._h)
+        check(lib.fides_hmult_batch(cc._h, B, (vp * B)(*[h.value for h in ha]), (vp * B)(*[h.value for h in hb]),
+                                    O, 1), cc._h)
+        for i in range(B):
+            ho = host_out[r][i].numpy().view(np.uint64)
+            check(lib.fides_ct_download_async(cc._h, outs[i]._h, ho[0].ctypes.data_as(u64p),
+                                              ho[1].ctypes.data_as(u64p)), cc._h)
+            lib.fides_ct_free(cc._h, ha[i])
+            lib.fides_ct_free(cc._h, hb[i])
+    cc.Synchronize()
+    for r in range(3):
+        for i in range(B):
+            a, b = rounds[r][i][0][1], rounds[r][i][1][1]
+            want = oc.hmult(lv, a[0], a[1], b[0], b[1], kb, ka, rescale=True)
+            got = host_out[r][i].numpy().view(np.uint64)
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (r, i)
