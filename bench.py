@@ -431,11 +431,12 @@ def run_ours(args):
     tms = (C.c_float * 8)()
     lib.fides_autotune(cc._h, C.byref(tv), tms, C.byref(nv))
     cacc = C.c_int()
-    cms = (C.c_float * 2)()
+    cms = (C.c_float * 3)()
     lib.fides_autotune_conv_info(cc._h, C.byref(cacc), cms)
     autotune = {"ntt_variant": tv.value, "fwd_inv_30limb_us": [round(1e3 * tms[i], 2) for i in range(nv.value)],
-                "conv_accumulator": ["128-bit", "split 32-bit"][cacc.value],
-                "modup_conv_one_element_us": [round(1e3 * cms[i], 2) for i in range(2)]}
+                "conv_variant": ["2 coefficients/thread, 128-bit sums", "2 coefficients/thread, split 32-bit products",
+                                 "1 coefficient/thread, 128-bit sums"][cacc.value],
+                "modup_conv_one_element_us": [round(1e3 * cms[i], 2) for i in range(3)]}
     stream_ptr = C.c_void_p()
     lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))
     st = torch.cuda.ExternalStream(stream_ptr.value, device=local)

@@ -83,12 +83,13 @@ fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream);
  * fides_ctx_create; call again to re-tune.  *variant and times_ms (one entry
  * per variant) may be NULL.  Results never depend on the variant. */
 fides_status fides_autotune(fides_ctx* ctx, int* variant, float* times_ms, int* num_variants);
-/* The base-conversion accumulator the autotuner chose (0: 128-bit sums,
- * 1: split 32-bit partial products, for moduli below 2^60) and the ModUp
- * conversion time of each (times_ms: 2 entries, 0 when not eligible). */
+/* The base-conversion variant the autotuner chose (0: two coefficients per
+ * thread with 128-bit sums, 1: the same with split 32-bit partial products,
+ * for moduli below 2^60, 2: one coefficient per thread) and the ModUp
+ * conversion time of each (times_ms: 3 entries, 0 when not eligible). */
 fides_status fides_autotune_conv_info(const fides_ctx* ctx, int* accumulator, float* times_ms);
-/* Force the conversion accumulator (0 or 1, for measurements and tests);
- * -1 restores the tuned choice. */
+/* Force the conversion variant (0..2, for measurements and tests); -1
+ * restores the tuned choice. */
 fides_status fides_set_conv_accumulator(fides_ctx* ctx, int accumulator);
 /* Force an NTT variant (for measurements); -1 restores the tuned choice. */
 fides_status fides_set_ntt_variant(fides_ctx* ctx, int variant);

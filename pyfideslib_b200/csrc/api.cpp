@@ -167,13 +167,14 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
     // top-level element
     bool split_ok = true;
     for (uint64_t q : c->host.prime) split_ok = split_ok && q < (1ull << 60);
-    c->conv_ms.assign(2, 0.f);
+    c->conv_ms.assign(kConvVariants, 0.f);
     int conv_best = 0;
     if (conv_supported(c->dev)) {
         const int top = c->L - 1;
         cudaMemsetAsync(c->ws1.XT, 0, (size_t)(top + 1) * c->limb_bytes(), c->st);
-        for (int v = 0; v < (split_ok ? 2 : 1); ++v) {
-            c->dev.split_conv = v;
+        for (int v = 0; v < kConvVariants; ++v) {
+            if (v == 1 && !split_ok) continue;
+            c->dev.conv_variant = v;
             launch_modup_conv(c->dev, top, 1, c->ws1.XT, c->ws1.DIG, c->ws1.dig_stride, c->ws1.stride, c->st);
             cudaEventRecord(e0, c->st);
             for (int r = 0; r < 10; ++r)
@@ -186,7 +187,7 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
             if (c->conv_ms[v] < c->conv_ms[conv_best]) conv_best = v;
         }
     }
-    c->dev.split_conv = conv_best;
+    c->dev.conv_variant = conv_best;
     c->tuned_conv = conv_best;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -203,17 +204,17 @@ fides_status fides_autotune_conv_info(const fides_ctx* c, int* accumulator, floa
     if (!c) return FIDES_BAD_ARG;
     if (accumulator) *accumulator = c->tuned_conv;
     if (times_ms)
-        for (size_t v = 0; v < 2; ++v) times_ms[v] = v < c->conv_ms.size() ? c->conv_ms[v] : 0.f;
+        for (size_t v = 0; v < (size_t)kConvVariants; ++v) times_ms[v] = v < c->conv_ms.size() ? c->conv_ms[v] : 0.f;
     return FIDES_OK;
 }
 
 fides_status fides_set_conv_accumulator(fides_ctx* c, int accumulator) {
-    if (!c || accumulator < -1 || accumulator > 1) return FIDES_BAD_ARG;
+    if (!c || accumulator < -1 || accumulator >= kConvVariants) return FIDES_BAD_ARG;
     Guard g(c);
     if (accumulator == 1)
         for (uint64_t q : c->host.prime)
             if (q >= (1ull << 60)) return set_err(c, FIDES_UNSUPPORTED, "split products need moduli below 2^60");
-    c->dev.split_conv = accumulator < 0 ? c->tuned_conv : accumulator;
+    c->dev.conv_variant = accumulator < 0 ? c->tuned_conv : accumulator;
     return FIDES_OK;
 }
 

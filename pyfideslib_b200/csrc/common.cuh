@@ -19,7 +19,8 @@ constexpr int kMaxBatch = 32;  // ciphertexts per batched launch (blockIdx.z)
 struct DevCtx {
     int logN, N, L, K, dnum, alpha;
     int ntt_variant;             // NTT kernel variant chosen by the autotuner
-    int split_conv;              // 1: every modulus < 2^60, conversions use split 32-bit products
+    int conv_variant;            // base conversions: 0 2 coefficients/thread 128-bit sums, 1 the same with
+                                 // split 32-bit products (moduli < 2^60), 2 one coefficient/thread
     const PrimeConst* pc;        // [L+K]
     const uint64_t* fwd_tw;      // [L+K][N][2]  psi^{bitrev(i)}, companion
     const uint64_t* inv_tw;      // [L+K][N][2]  psi^{-bitrev(i)}, companion

@@ -72,6 +72,7 @@ struct MdArgs {
 void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& args, cudaStream_t st);
 // the conversion kernels keep up to 16 inputs (digit moduli / special moduli) in registers
 bool conv_supported(const DevCtx& ctx);
+constexpr int kConvVariants = 3;  // see DevCtx::conv_variant
 // override every segment's prologue / epilogue mode (-1 keeps the segment's own)
 void set_modes(LimbMap& map, int lmode, int smode);
 

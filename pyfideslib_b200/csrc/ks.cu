@@ -154,6 +154,63 @@ __global__ void __launch_bounds__(kConvThreads) k_modup_conv(const __grid_consta
     }
 }
 
+// One coefficient per thread, four targets per iteration: half the input
+// registers of k_modup_conv (twice the resident warps), the same products.
+template <int MAXIN>
+__global__ void __launch_bounds__(kConvThreads) k_modup_conv_c1(const __grid_constant__ DevCtx ctx, int level,
+                                                                const uint64_t* __restrict__ xt,
+                                                                uint64_t* __restrict__ dig, size_t dig_stride,
+                                                                size_t bstride) {
+    __shared__ uint64_t sM[MAXIN][kConvTargets];
+    __shared__ PrimeConst sP[kConvTargets];
+    const int ndig = level / ctx.alpha + 1;
+    const int d = blockIdx.y % ndig;
+    const size_t boff = (size_t)(blockIdx.y / ndig) * bstride;
+    xt += boff;
+    dig += boff;
+    const int n = level + 1;
+    const int lo = d * ctx.alpha;
+    const int hi = min(lo + ctx.alpha - 1, level);
+    const int cnt = hi - lo + 1;
+    const int ntar = n - cnt + ctx.K;
+    const int m0 = blockIdx.z * kConvTargets;
+    if (m0 >= ntar) return;
+    const int nt = min(kConvTargets, ntar - m0);
+    const int NP = ctx.L + ctx.K;
+    const uint64_t* mat = ctx.modup_mat + (size_t)level * ctx.L * NP;
+    for (int e = threadIdx.x; e < cnt * nt; e += kConvThreads) {
+        const int i = e / nt, mm = e % nt, m = m0 + mm;
+        const int jj = m < lo ? m : m + cnt;
+        const int t = jj < n ? jj : ctx.L + (jj - n);
+        sM[i][mm] = mat[(size_t)(lo + i) * NP + t];
+        if (i == 0) sP[mm] = ctx.pc[t];
+    }
+    const size_t j = (size_t)blockIdx.x * kConvThreads + threadIdx.x;
+    uint64_t x[MAXIN];
+#pragma unroll
+    for (int i = 0; i < MAXIN; ++i)
+        if (i < cnt) x[i] = xt[(size_t)(lo + i) * ctx.N + j];
+    __syncthreads();
+    uint64_t* out = dig + ((size_t)d * dig_stride + m0) * ctx.N + j;
+#pragma unroll 1
+    for (int mm = 0; mm < nt; mm += 4) {
+        int m[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) m[u] = min(mm + u, nt - 1);
+        Acc128 acc[4];
+#pragma unroll
+        for (int i = 0; i < MAXIN; ++i) {
+            if (i < cnt) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[u].mac(x[i], sM[i][m[u]]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (mm + u < nt) out[(size_t)(mm + u) * ctx.N] = acc[u].reduce(sP[mm + u]);
+    }
+}
+
 bool conv_supported(const DevCtx& ctx) { return ctx.alpha <= kMaxConvIn && ctx.K <= kMaxConvIn; }
 
 void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
@@ -162,10 +219,13 @@ void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt,
     const int maxtar = level + 1 + ctx.K;
     dim3 g(ctx.N / (2 * kConvThreads), nd * nb, (maxtar + kConvTargets - 1) / kConvTargets);
     count_launches(1);
-#define FIDES_MODUP(M)                                                                                    \
-    if (ctx.split_conv)                                                                                  \
-        k_modup_conv<M, AccSplit><<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride, bstride); \
-    else                                                                                                 \
+    const dim3 g1(ctx.N / kConvThreads, g.y, g.z);
+#define FIDES_MODUP(M)                                                                                       \
+    if (ctx.conv_variant == 2)                                                                              \
+        k_modup_conv_c1<M><<<g1, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride, bstride);          \
+    else if (ctx.conv_variant == 1)                                                                         \
+        k_modup_conv<M, AccSplit><<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride, bstride);    \
+    else                                                                                                    \
         k_modup_conv<M, Acc128><<<g, kConvThreads, 0, st>>>(ctx, level, xt, dig, dig_stride, bstride);
     if (ctx.alpha <= 4) {
         FIDES_MODUP(4)
@@ -272,13 +332,13 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
     count_launches(1);
     if (plain) {
         dim3 g(ctx.N / 512 * nb, level + 1 + ctx.K);
-        if (ctx.split_conv)
+        if (ctx.conv_variant == 1)
             k_ks_inner<1, AccSplit><<<g, 256, 0, st>>>(ctx, level, nb, args);
         else
             k_ks_inner<1, Acc128><<<g, 256, 0, st>>>(ctx, level, nb, args);
     } else {
         dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
-        if (ctx.split_conv)
+        if (ctx.conv_variant == 1)
             k_ks_inner<0, AccSplit><<<g, 256, 0, st>>>(ctx, level, nb, args);
         else
             k_ks_inner<0, Acc128><<<g, 256, 0, st>>>(ctx, level, nb, args);
@@ -393,7 +453,7 @@ void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& a, 
     dim3 g(ctx.N / (2 * kConvThreads), (nout + kConvTargets - 1) / kConvTargets, 2 * nb);
     count_launches(1);
 #define FIDES_MODDOWN(M)                                                      \
-    if (ctx.split_conv)                                                       \
+    if (ctx.conv_variant == 1)                                                \
         k_moddown_conv<M, AccSplit><<<g, kConvThreads, 0, st>>>(ctx, level, a); \
     else                                                                      \
         k_moddown_conv<M, Acc128><<<g, kConvThreads, 0, st>>>(ctx, level, a);

@@ -135,10 +135,11 @@ def test_rotate_and_hoisted_parity():
             assert np.array_equal(g0, x0) and np.array_equal(g1, x1)
 
 
-def test_both_conversion_accumulators_bitexact():
-    """The 128-bit and the split 32-bit-product accumulators of the base
-    conversions and the key-switch inner product give the oracle's residues
-    (HMult with rescale and a rotation at two levels, moduli below 2^60)."""
+def test_every_conversion_variant_bitexact():
+    """Every base-conversion variant (two coefficients per thread with 128-bit
+    or split 32-bit-product sums, one coefficient per thread) gives the
+    oracle's residues (HMult with rescale and a rotation at two levels, moduli
+    below 2^60)."""
     from pyfideslib_b200._capi import lib
 
     cc, oc = make_pair(12, 9, 3, 3)
@@ -147,7 +148,7 @@ def test_both_conversion_accumulators_bitexact():
     g = cc.rotation_galois(3)
     rk = rand_key(oc, 63)
     cc.upload_galois_key(g, *rk)
-    for acc in (0, 1):
+    for acc in (0, 1, 2):
         assert lib.fides_set_conv_accumulator(cc._h, acc) == 0
         for level in (8, 4):
             a0, a1 = rand_ct(oc, level, 70 + level)
