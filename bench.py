@@ -47,7 +47,7 @@ LOGN, L, K, DNUM = 16, 30, 10, 3
 # algorithmic bytes: the column pass writes the 960 intermediate limbs
 # (480 MB, more than L2) and the row pass reads them back; twiddles add 32 MB
 # (read once per prime for the whole batch).
-NTT_BATCH_TRAFFIC_BYTES = 1927.28e6
+NTT_BATCH_TRAFFIC_BYTES = 1941.7e6
 
 
 def peaks():
@@ -433,10 +433,11 @@ def run_ours(args):
     cacc = C.c_int()
     cms = (C.c_float * 3)()
     lib.fides_autotune_conv_info(cc._h, C.byref(cacc), cms)
-    autotune = {"ntt_variant": tv.value, "fwd_inv_30limb_us": [round(1e3 * tms[i], 2) for i in range(nv.value)],
+    autotune = {"ntt_variant": tv.value,
+                "fwd_inv_us_3x40_limbs": [round(1e3 * tms[i], 2) for i in range(nv.value)],
                 "conv_variant": ["2 coefficients/thread, 128-bit sums", "2 coefficients/thread, split 32-bit products",
                                  "1 coefficient/thread, 128-bit sums"][cacc.value],
-                "modup_conv_one_element_us": [round(1e3 * cms[i], 2) for i in range(3)]}
+                "modup_conv_4_elements_us": [round(1e3 * cms[i], 2) for i in range(3)]}
     stream_ptr = C.c_void_p()
     lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))
     st = torch.cuda.ExternalStream(stream_ptr.value, device=local)

@@ -85,8 +85,9 @@ fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream);
 fides_status fides_autotune(fides_ctx* ctx, int* variant, float* times_ms, int* num_variants);
 /* The base-conversion variant the autotuner chose (0: two coefficients per
  * thread with 128-bit sums, 1: the same with split 32-bit partial products,
- * for moduli below 2^60, 2: one coefficient per thread) and the ModUp
- * conversion time of each (times_ms: 3 entries, 0 when not eligible). */
+ * for moduli below 2^60, 2: one coefficient per thread) and the time of each
+ * on the ModUp conversion of four top-level elements (times_ms: 3 entries,
+ * 0 when not eligible). */
 fides_status fides_autotune_conv_info(const fides_ctx* ctx, int* accumulator, float* times_ms);
 /* Force the conversion variant (0..2, for measurements and tests); -1
  * restores the tuned choice. */
