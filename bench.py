@@ -428,16 +428,17 @@ def run_ours(args):
 
     cc = F.CryptoContext(log_n=LOGN, num_q=L, dnum=DNUM, num_p=K, device=local)
     tv, nv = C.c_int(), C.c_int()
-    tms = (C.c_float * 8)()
+    tms = (C.c_float * 16)()
     lib.fides_autotune(cc._h, C.byref(tv), tms, C.byref(nv))
     cacc = C.c_int()
-    cms = (C.c_float * 3)()
+    cms = (C.c_float * 8)()
     lib.fides_autotune_conv_info(cc._h, C.byref(cacc), cms)
     autotune = {"ntt_variant": tv.value,
                 "fwd_inv_us_3x40_limbs": [round(1e3 * tms[i], 2) for i in range(nv.value)],
                 "conv_variant": ["2 coefficients/thread, 128-bit sums", "2 coefficients/thread, split 32-bit products",
-                                 "1 coefficient/thread, 128-bit sums"][cacc.value],
-                "modup_conv_4_elements_us": [round(1e3 * cms[i], 2) for i in range(3)]}
+                                 "1 coefficient/thread, 128-bit sums", "tensor cores (int8 split), 16 targets/MMA",
+                                 "tensor cores (int8 split), 8 targets/MMA"][cacc.value],
+                "modup_conv_4_elements_us": [round(1e3 * cms[i], 2) for i in range(5)]}
     stream_ptr = C.c_void_p()
     lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))
     st = torch.cuda.ExternalStream(stream_ptr.value, device=local)

@@ -78,21 +78,31 @@ const char* fides_ctx_last_error(const fides_ctx* ctx);
  * callers that time or order work around it (FIDESlib keeps per-partition
  * streams in ContextData, src/CKKS/Context.cuh:85-98). */
 fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream);
-/* Autotuner: time every NTT kernel variant (occupancy / twiddle-fetch
- * policy) on this context's limb shapes and keep the fastest.  Runs once in
- * fides_ctx_create; call again to re-tune.  *variant and times_ms (one entry
- * per variant) may be NULL.  Results never depend on the variant. */
+/* Autotuner: time every forward NTT variant (occupancy, twiddle-fetch
+ * policy, integer or double-precision butterflies) and every inverse
+ * configuration on this context's limb shapes and keep the fastest of each.
+ * Runs once in fides_ctx_create; call again to re-tune.  *variant receives
+ * the forward variant, times_ms[v] (num_variants entries, at most 16) the
+ * forward time of variant v plus that of its paired inverse configuration;
+ * any pointer may be NULL.  Results never depend on the variant. */
 fides_status fides_autotune(fides_ctx* ctx, int* variant, float* times_ms, int* num_variants);
 /* The base-conversion variant the autotuner chose (0: two coefficients per
  * thread with 128-bit sums, 1: the same with split 32-bit partial products,
- * for moduli below 2^60, 2: one coefficient per thread) and the time of each
- * on the ModUp conversion of four top-level elements (times_ms: 3 entries,
- * 0 when not eligible). */
+ * for moduli below 2^60, 2: one coefficient per thread, 3 and 4: ModUp on
+ * the tensor cores as an exact int8-split contraction with 16 or 8 targets
+ * per matrix product) and the time of each on the ModUp conversion of four
+ * top-level elements (times_ms: 5 entries, 0 when not eligible). */
 fides_status fides_autotune_conv_info(const fides_ctx* ctx, int* accumulator, float* times_ms);
-/* Force the conversion variant (0..2, for measurements and tests); -1
- * restores the tuned choice. */
+/* Force the conversion variant (0..4, for measurements and tests; 3 and 4
+ * run the ModUp conversion on the tensor cores as an exact int8-split
+ * contraction with 16 or 8 targets per matrix product, digits of at most 16
+ * moduli); -1 restores the tuned choice. */
 fides_status fides_set_conv_accumulator(fides_ctx* ctx, int accumulator);
-/* Force an NTT variant (for measurements); -1 restores the tuned choice. */
+/* 1 once a tensor-core conversion gave up waiting for its matrix products
+ * (bounded wait; its outputs are then invalid), else 0.  Process-wide. */
+int fides_tensor_conv_status(void);
+/* Force forward NTT variant `variant` with its paired inverse configuration
+ * (for measurements and tests); -1 restores the tuned choices. */
 fides_status fides_set_ntt_variant(fides_ctx* ctx, int variant);
 /* Number of kernels this library has launched so far (process-wide). */
 uint64_t fides_kernel_launches(void);

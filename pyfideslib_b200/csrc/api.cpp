@@ -160,27 +160,39 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
         m.seg[m.nseg++] = one.seg[0];
         m.total += np;
     }
-    c->tune_ms.assign(nv, 1e30f);
-    for (int r = 0; r < kRounds; ++r)
+    // forward variants and inverse configurations are timed (and chosen)
+    // separately; tune_ms[v] reports forward v plus its paired inverse
+    const int niv = ntt_num_inverse_variants();
+    std::vector<float> fwd_ms(nv, 1e30f), inv_ms(niv, 1e30f);
+    for (int r = 0; r < kRounds; ++r) {
         for (int v = 0; v < nv; ++v) {
             c->dev.ntt_variant = v;
             ntt_forward(c->dev, m, FL_PLAIN, FS_PLAIN, c->st);
+            cudaEventRecord(e0, c->st);
+            for (int k = 0; k < kReps; ++k) ntt_forward(c->dev, m, FL_PLAIN, FS_PLAIN, c->st);
+            fwd_ms[v] = std::min(fwd_ms[v], elapsed() / kReps);
+        }
+        for (int v = 0; v < niv; ++v) {
+            c->dev.intt_variant = v;
             ntt_inverse(c->dev, m, IL_PLAIN, IS_PLAIN, c->st);
             cudaEventRecord(e0, c->st);
-            for (int k = 0; k < kReps; ++k) {
-                ntt_forward(c->dev, m, FL_PLAIN, FS_PLAIN, c->st);
-                ntt_inverse(c->dev, m, IL_PLAIN, IS_PLAIN, c->st);
-            }
-            c->tune_ms[v] = std::min(c->tune_ms[v], elapsed() / kReps);
+            for (int k = 0; k < kReps; ++k) ntt_inverse(c->dev, m, IL_PLAIN, IS_PLAIN, c->st);
+            inv_ms[v] = std::min(inv_ms[v], elapsed() / kReps);
         }
-    int best = 0;
+    }
+    c->tune_ms.assign(nv, 0.f);
+    for (int v = 0; v < nv; ++v) c->tune_ms[v] = fwd_ms[v] + inv_ms[ntt_inverse_of(v)];
+    int best = 0, best_inv = 0;
     for (int v = 1; v < nv; ++v)
-        if (c->tune_ms[v] < c->tune_ms[best]) best = v;
+        if (fwd_ms[v] < fwd_ms[best]) best = v;
+    for (int v = 1; v < niv; ++v)
+        if (inv_ms[v] < inv_ms[best_inv]) best_inv = v;
     // base-conversion variants (split products need every modulus below
     // 2^60): the ModUp conversion of four top-level elements in one launch,
     // as the batched key switch runs it, in a scratch buffer freed after
     bool split_ok = true;
     for (uint64_t q : c->host.prime) split_ok = split_ok && q < (1ull << 60);
+    const bool tc_tune = conv_tc_supported(c->dev);  // tensor-core ModUp (int8 split)
     c->conv_ms.assign(kConvVariants, 0.f);
     int conv_best = 0;
     constexpr int kTuneElems = 4;
@@ -197,6 +209,7 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
         for (int r = 0; r < kRounds; ++r)
             for (int v = 0; v < kConvVariants; ++v) {
                 if (v == 1 && !split_ok) continue;
+                if (v >= 3 && !tc_tune) continue;
                 c->dev.conv_variant = v;
                 launch_modup_conv(c->dev, top, kTuneElems, xt, dig, dstride, elem, c->st);
                 cudaEventRecord(e0, c->st);
@@ -216,7 +229,9 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->tuned_variant = best;
+    c->tuned_inverse = best_inv;
     c->dev.ntt_variant = best;
+    c->dev.intt_variant = best_inv;
     if (variant) *variant = best;
     if (num_variants) *num_variants = nv;
     if (times_ms)
@@ -238,14 +253,19 @@ fides_status fides_set_conv_accumulator(fides_ctx* c, int accumulator) {
     if (accumulator == 1)
         for (uint64_t q : c->host.prime)
             if (q >= (1ull << 60)) return set_err(c, FIDES_UNSUPPORTED, "split products need moduli below 2^60");
+    if (accumulator >= 3 && !conv_tc_supported(c->dev))
+        return set_err(c, FIDES_UNSUPPORTED, "tensor-core conversion needs digits of at most 16 moduli and at most 48 targets");
     c->dev.conv_variant = accumulator < 0 ? c->tuned_conv : accumulator;
     return FIDES_OK;
 }
+
+int fides_tensor_conv_status(void) { return conv_tc_error(); }
 
 fides_status fides_set_ntt_variant(fides_ctx* c, int variant) {
     if (!c || variant >= ntt_num_variants() || variant < -1) return FIDES_BAD_ARG;
     Guard g(c);
     c->dev.ntt_variant = variant < 0 ? c->tuned_variant : variant;
+    c->dev.intt_variant = variant < 0 ? c->tuned_inverse : ntt_inverse_of(variant);
     return FIDES_OK;
 }
 

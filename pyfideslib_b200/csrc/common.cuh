@@ -18,12 +18,18 @@ constexpr int kMaxBatch = 32;  // ciphertexts per batched launch (blockIdx.z)
 // adjacently.
 struct DevCtx {
     int logN, N, L, K, dnum, alpha;
-    int ntt_variant;             // NTT kernel variant chosen by the autotuner
+    int ntt_variant;             // forward NTT kernel variant chosen by the autotuner
+    int intt_variant;            // inverse NTT kernel configuration (0..2)
     int conv_variant;            // base conversions: 0 2 coefficients/thread 128-bit sums, 1 the same with
-                                 // split 32-bit products (moduli < 2^60), 2 one coefficient/thread
+                                 // split 32-bit products (moduli < 2^60), 2 one coefficient/thread,
+                                 // 3 and 4 ModUp on the tensor cores (int8 split, 16 or 8 targets
+                                 // per MMA), ModDown as 0
     const PrimeConst* pc;        // [L+K]
     const uint64_t* fwd_tw;      // [L+K][N][2]  psi^{bitrev(i)}, companion
     const uint64_t* inv_tw;      // [L+K][N][2]  psi^{-bitrev(i)}, companion
+    const uint64_t* fwd_twf;     // [L+K][N][2]  bit patterns of the doubles w = psi^{bitrev(i)} and w / p
+                                 //              (primes below 2^50; zero rows otherwise)
+    const uint64_t* inv_twf;     // [L+K][N][2]  the same for psi^{-bitrev(i)}
     const uint64_t* intt_scale;  // [L+K][4]     s=N^-1, s', s*w1, (s*w1)'  (w1 = inverse twiddle 1)
     const uint64_t* modup_scale; // [L][L][4]    same with s = N^-1 * (Q'/q_i)^-1 for level, prime
     const uint64_t* modup_mat;   // [L][L][L+K]  (Q'/q_i) mod t for level, input prime i, target prime t

@@ -8,6 +8,7 @@
 // (~0.3 MiB of CRT data at L=30, K=10) and the twiddles are stored as
 // (value, Shoup companion) pairs so that a butterfly reads one 16-byte word.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <numeric>
 #include <random>
@@ -20,6 +21,24 @@ namespace fides {
 using u128 = unsigned __int128;
 
 uint64_t mulmod(uint64_t a, uint64_t b, uint64_t p) { return (uint64_t)((u128)a * b % p); }
+
+static uint64_t f64_bits(double x) {
+    uint64_t u;
+    std::memcpy(&u, &x, 8);
+    return u;
+}
+
+// The double nearest above 1/p (p < 2^50): x = m 2^e with a 53-bit m, and
+// x >= 1/p  <=>  m p >= 2^-e, checked in exact integer arithmetic.
+static double recip_up(uint64_t p) {
+    double x = 1.0 / (double)p;
+    int e = 0;
+    const double f = std::frexp(x, &e);                  // x = f 2^e, f in [0.5, 1)
+    const uint64_t m = (uint64_t)std::ldexp(f, 53);      // x = m 2^(e - 53)
+    const int sh = 53 - e;                               // 2^-(e-53) = 2^sh, sh <= 104 for p < 2^50
+    if (sh < 128 && (u128)m * p < ((u128)1 << sh)) x = std::nextafter(x, 1.0);
+    return x;
+}
 
 uint64_t powmod(uint64_t a, uint64_t e, uint64_t p) {
     uint64_t r = 1 % p;
@@ -268,7 +287,8 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     // ---- per-prime constants and twiddles (host) ----
     c->host.pc.resize(NP);
     c->host.root.resize(NP);
-    std::vector<uint64_t> fwd((size_t)NP * N * 2), inv((size_t)NP * N * 2);
+    std::vector<uint64_t> fwd((size_t)NP * N * 2), inv((size_t)NP * N * 2), fwdf((size_t)NP * N * 2, 0),
+        invf((size_t)NP * N * 2, 0);
     auto work = [&](int i) {
         const uint64_t pr = c->host.prime[i];
         PrimeConst& k = c->host.pc[i];
@@ -297,6 +317,20 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
             F[2 * j + 1] = shoup_precompute(a[r], pr);
             I[2 * j] = b[r];
             I[2 * j + 1] = shoup_precompute(b[r], pr);
+        }
+        // double-precision butterflies (primes below 2^50): w and the
+        // correctly rounded quotient w / p
+        if (pr < kFpPrimeBound) {
+            k.pinv_f64 = f64_bits(recip_up(pr));
+            uint64_t* D = fwdf.data() + (size_t)i * N * 2;
+            uint64_t* E = invf.data() + (size_t)i * N * 2;
+            for (int j = 0; j < N; ++j) {
+                const double w = (double)F[2 * j], v = (double)I[2 * j];
+                D[2 * j] = f64_bits(w);
+                D[2 * j + 1] = f64_bits(w / (double)pr);
+                E[2 * j] = f64_bits(v);
+                E[2 * j + 1] = f64_bits(v / (double)pr);
+            }
         }
     };
     {
@@ -393,6 +427,8 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     size_t i_pc = add(c->host.pc.data(), sizeof(PrimeConst) * NP);
     size_t i_fwd = add(fwd.data(), fwd.size() * 8);
     size_t i_inv = add(inv.data(), inv.size() * 8);
+    size_t i_fwdf = add(fwdf.data(), fwdf.size() * 8);
+    size_t i_invf = add(invf.data(), invf.size() * 8);
     size_t i_is = add(intt_scale.data(), intt_scale.size() * 8);
     size_t i_ms = add(modup_scale.data(), modup_scale.size() * 8);
     size_t i_mm = add(modup_mat.data(), modup_mat.size() * 8);
@@ -414,10 +450,12 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.K = K;
     d.dnum = c->dnum;
     d.alpha = c->alpha;
-    d.conv_variant = 0;  // chosen by the autotuner
+    d.ntt_variant = d.intt_variant = d.conv_variant = 0;  // chosen by the autotuner
     d.pc = (const PrimeConst*)(base + parts[i_pc].off);
     d.fwd_tw = (const uint64_t*)(base + parts[i_fwd].off);
     d.inv_tw = (const uint64_t*)(base + parts[i_inv].off);
+    d.fwd_twf = (const uint64_t*)(base + parts[i_fwdf].off);
+    d.inv_twf = (const uint64_t*)(base + parts[i_invf].off);
     d.intt_scale = (const uint64_t*)(base + parts[i_is].off);
     d.modup_scale = (const uint64_t*)(base + parts[i_ms].off);
     d.modup_mat = (const uint64_t*)(base + parts[i_mm].off);

@@ -111,7 +111,8 @@ struct fides_ctx {
     // bootstrapping precomputation (diagonal plaintexts, series), by slot count
     std::map<int, std::shared_ptr<fides::BootPrecomp>> boot;
 
-    int tuned_variant = 0;
+    int tuned_variant = 0;   // forward NTT variant
+    int tuned_inverse = 0;   // inverse NTT configuration
     std::vector<float> tune_ms;
     int tuned_conv = 0;  // base-conversion accumulator: 0 128-bit, 1 split 32-bit products
     std::vector<float> conv_ms;

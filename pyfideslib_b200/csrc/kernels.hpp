@@ -24,6 +24,8 @@ void count_launches(int n);
 
 bool ntt_supported(int logN);
 int ntt_num_variants();
+int ntt_num_inverse_variants();
+int ntt_inverse_of(int forward_variant);
 // Forward NTT of every limb in `map`: pass 1 reads seg.in (writes seg.out),
 // pass 2 transforms seg.out in place and applies the epilogue.  load / store
 // >= 0 override the per-segment modes.
@@ -72,7 +74,13 @@ struct MdArgs {
 void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& args, cudaStream_t st);
 // the conversion kernels keep up to 16 inputs (digit moduli / special moduli) in registers
 bool conv_supported(const DevCtx& ctx);
-constexpr int kConvVariants = 3;  // see DevCtx::conv_variant
+constexpr int kConvVariants = 5;  // see DevCtx::conv_variant
+// ModUp conversion as an exact int8-split tcgen05 contraction (conv_tc.cu);
+// chunk = targets per MMA (16 or 8)
+bool conv_tc_supported(const DevCtx& ctx);
+void launch_modup_conv_tc(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
+                          size_t bstride, cudaStream_t st, int chunk);
+int conv_tc_error();  // 1 once a tensor-core conversion timed out waiting for its MMAs
 // override every segment's prologue / epilogue mode (-1 keeps the segment's own)
 void set_modes(LimbMap& map, int lmode, int smode);
 

@@ -215,6 +215,10 @@ bool conv_supported(const DevCtx& ctx) { return ctx.alpha <= kMaxConvIn && ctx.K
 
 void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
                        size_t bstride, cudaStream_t st) {
+    if ((ctx.conv_variant == 3 || ctx.conv_variant == 4) && conv_tc_supported(ctx)) {
+        launch_modup_conv_tc(ctx, level, nb, xt, dig, dig_stride, bstride, st, ctx.conv_variant == 3 ? 16 : 8);
+        return;
+    }
     const int nd = level / ctx.alpha + 1;
     const int maxtar = level + 1 + ctx.K;
     dim3 g(ctx.N / (2 * kConvThreads), nd * nb, (maxtar + kConvTargets - 1) / kConvTargets);

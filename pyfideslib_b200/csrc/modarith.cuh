@@ -1,7 +1,9 @@
 // modarith.cuh -- 64-bit modular arithmetic for residues modulo NTT primes
 // p < 2^62, shared by the CUDA kernels and the host code.
 //
-// All products are on the integer pipes (IMAD); nothing is approximated.
+// All products here are on the integer pipes (IMAD); nothing is approximated.
+// (The NTT also has exact double-precision butterflies for primes below
+// 2^50, in ntt.cu.)
 // Canonical residues live in [0, p); the transforms keep Harvey's lazy
 // ranges [0, 2p) / [0, 4p) internally and reduce at the end.
 //
@@ -40,8 +42,12 @@ struct PrimeConst {
     uint64_t r64_sh;  // Shoup companion of r64
     uint64_t ninv;    // N^-1 mod p
     uint64_t ninv_sh;
-    uint64_t pad;
+    uint64_t pinv_f64;  // bit pattern of the double 1/p rounded up (p < 2^50; 0 otherwise)
 };
+
+// Forward transforms of primes below this bound run their butterflies on the
+// FP64 pipes (residues held exactly as doubles, see ntt.cu).
+constexpr uint64_t kFpPrimeBound = 1ull << 50;
 
 // floor(w * 2^64 / p), host only (needs a 128-bit division).
 inline uint64_t shoup_precompute(uint64_t w, uint64_t p) {

@@ -24,6 +24,12 @@
 //     one dependent load per butterfly.
 //   * Harvey lazy butterflies: values stay in [0,4p) (forward) or [0,2p)
 //     (inverse) and are reduced once at the end.
+//   * For primes below 2^50 the butterflies can instead run on the FP64
+//     pipes with residues held exactly as integer-valued doubles (products
+//     split into h + l by an FMA, quotients from a precomputed w / p); the
+//     integer pipes are the bottleneck of the 64-bit Shoup butterflies and
+//     the FP64 pipes would otherwise stay idle.  Results are the same
+//     canonical residues; the autotuner picks the arithmetic per context.
 //   * Prologues/epilogues fuse the surrounding element-wise work (products of
 //     two inputs, ModDown/Rescale combinations, per-limb CRT scalings).  The
 //     mode is a per-segment field, so one launch can mix limbs with different
@@ -52,6 +58,78 @@ __device__ __forceinline__ uint64_t mulhi64_approx(uint64_t a, uint64_t b) {
     h += __umulhi(a1, b0);
     h += __umulhi(a0, b1);
     return h;
+}
+
+// ---- double-precision butterflies (MODE 4, primes below 2^50) ----
+// Residues are held exactly as signed integer-valued doubles (bit patterns in
+// the uint64_t registers) and every product runs on the FP64 pipes, which the
+// integer butterflies leave idle.  With w < p and wq = fl(w / p):
+//   h = fl(y w), l = fma(y, w, -h)          y w = h + l exactly
+//   q = rint(y wq)                          |q - y w / p| <= 1/2 + |y| 2^-54
+//   t = fma(-q, p, h) + l = y w - q p       exact, |t| <= p (1/2 + |y| 2^-54)
+// (rint through the 1.5 * 2^52 shift, valid for |y wq| < 2^51; the fma of
+// the shift rounds the exact product).  Starting from residues below p,
+// alternating plain stages with stages that first centre X (x - rint(x/p) p,
+// |.| <= p/2 + 1) keeps every value below 1.7p < 2^51, so the bounds above
+// hold at every stage and all sums are exact.  The pass ends with a floor
+// reduction against 1/p rounded up, which is exact for values in (-2p, 2p).
+constexpr double kRint = 6755399441055744.0;  // 1.5 * 2^52
+constexpr double kTwo52 = 4503599627370496.0;
+constexpr uint64_t kMant52 = (1ull << 52) - 1;
+
+__device__ __forceinline__ double as_f64(uint64_t v) { return __longlong_as_double((long long)v); }
+__device__ __forceinline__ uint64_t as_u64(double v) { return (uint64_t)__double_as_longlong(v); }
+
+// residue below 2^52 -> the same integer as a double
+__device__ __forceinline__ uint64_t fp_from_u(uint64_t v) {
+    return as_u64(__dsub_rn(as_f64(v | 0x4330000000000000ull), kTwo52));
+}
+
+// y w - q p with q = rint(y w / p) to within 1/2 + |y| 2^-54 (|y| < 2^51)
+__device__ __forceinline__ double fp_mulw(double y, double w, double wq, double p) {
+    const double h = __dmul_rn(y, w);
+    const double l = __fma_rn(y, w, -h);
+    const double q = __dsub_rn(__fma_rn(y, wq, kRint), kRint);
+    return __dadd_rn(__fma_rn(-q, p, h), l);
+}
+
+// x - rint(x / p) p, magnitude <= p/2 + |x| 2^-52 (|x| < 2^51)
+__device__ __forceinline__ double fp_center(double x, double p, double pinv) {
+    const double q = __dsub_rn(__fma_rn(x, pinv, kRint), kRint);
+    return __fma_rn(-q, p, x);
+}
+
+// canonical residue of an integer-valued v in (-2p, 2p); pinv_up >= 1/p.
+// a = v + 2p lies in (0, 4p); floor(a pinv_up) = floor(a / p) because a / p
+// is at least 1/p > 2^-50 away from the next integer while the rounding of
+// 1/p moves it by at most 4 * 2^-52.
+__device__ __forceinline__ uint64_t fp_to_u(double v, double p, double pinv_up) {
+    const double two_p = __dadd_rn(p, p);
+    const double a = __dadd_rn(v, two_p);
+    const double b = __dadd_rn(v, __dadd_rn(two_p, kTwo52));  // a + 2^52, exact
+    const double q = __dsub_rn(__fma_rd(a, pinv_up, kRint), kRint);
+    return as_u64(__fma_rn(-q, p, b)) & kMant52;  // (a - q p) + 2^52 -> low 52 bits
+}
+
+// forward butterfly on doubles; RED centres X first
+template <bool RED>
+__device__ __forceinline__ void ct_bfly_fp(uint64_t& X, uint64_t& Y, const ulonglong2 w, const double p,
+                                           const double pinv) {
+    double x = as_f64(X);
+    if constexpr (RED) x = fp_center(x, p, pinv);
+    const double t = fp_mulw(as_f64(Y), as_f64(w.x), as_f64(w.y), p);
+    X = as_u64(__dadd_rn(x, t));
+    Y = as_u64(__dsub_rn(x, t));
+}
+
+// inverse (Gentleman-Sande) butterfly on doubles: the sum is centred every
+// stage, the difference goes through the product, so every value stays
+// below 0.58p and |x - y| < 1.2p keeps the product's quotient within range
+__device__ __forceinline__ void gs_bfly_fp(uint64_t& X, uint64_t& Y, const ulonglong2 w, const double p,
+                                           const double pinv) {
+    const double x = as_f64(X), y = as_f64(Y);
+    X = as_u64(fp_center(__dadd_rn(x, y), p, pinv));
+    Y = as_u64(fp_mulw(__dsub_rn(x, y), as_f64(w.x), as_f64(w.y), p));
 }
 
 template <int MODE>
@@ -114,45 +192,70 @@ __device__ __forceinline__ void load_stage_tw(ulonglong2 (&w)[15], Tab tab, int 
 // whole group up front (more loads in flight, +30 registers); PF = false
 // fetches each stage's twiddles right before the stage (fewer registers,
 // higher occupancy).  The autotuner picks per context.
-template <int KB, int KB_END, int STEP, bool PF, int MODE, class Tab>
+// p and two_p carry the prime's constants for the butterfly mode: (p, 2p) for
+// the integer modes, the bit patterns of the doubles (p, 1/p rounded up) for
+// MODE 4.  POS counts the stages of the group (MODE 4 centres X on odd ones).
+template <int MODE, int POS>
+__device__ __forceinline__ void bfly(uint64_t& X, uint64_t& Y, const ulonglong2 w, uint64_t p, uint64_t two_p) {
+    if constexpr (MODE == 4)
+        ct_bfly_fp<(POS & 1) != 0>(X, Y, w, as_f64(p), as_f64(two_p));
+    else if constexpr (MODE == 5)
+        gs_bfly_fp(X, Y, w, as_f64(p), as_f64(two_p));
+    else if constexpr (MODE != 2)
+        ct_bfly<MODE>(X, Y, w, p, two_p);
+    else
+        gs_bfly(X, Y, w, p, two_p);
+}
+
+template <int KB, int KB_END, int STEP, bool PF, int MODE, int POS, class Tab>
 __device__ __forceinline__ void run_stages(uint64_t (&x)[16], ulonglong2 (&w)[15], Tab tab, int t_of_kb0, size_t B,
                                            int th_hi, uint64_t p, uint64_t two_p) {
     if constexpr (!PF) load_stage_tw<KB>(w, tab, t_of_kb0, B, th_hi);
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
         if (k & (1 << KB)) continue;
-        if constexpr (MODE != 2)
-            ct_bfly<MODE>(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
-        else
-            gs_bfly(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
+        bfly<MODE, POS>(x[k], x[k | (1 << KB)], w[tw_off(KB) + (k >> (KB + 1))], p, two_p);
     }
-    if constexpr (KB != KB_END) run_stages<KB + STEP, KB_END, STEP, PF, MODE>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
+    if constexpr (KB != KB_END)
+        run_stages<KB + STEP, KB_END, STEP, PF, MODE, POS + 1>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
+}
+
+// All twiddles of a group (stages with partner bits KB_FIRST..KB_LAST) into
+// registers.
+template <int KB_FIRST, int KB_LAST, class Tab>
+__device__ __forceinline__ void load_group_tw(ulonglong2 (&w)[15], Tab tab, int t_of_kb0, size_t B, int th_hi) {
+#pragma unroll
+    for (int kb = 0; kb < 4; ++kb) {
+        if ((kb < KB_FIRST && kb < KB_LAST) || (kb > KB_FIRST && kb > KB_LAST)) continue;
+        const int t = t_of_kb0 - kb;
+        const size_t base = (B << t) + ((size_t)th_hi << (3 - kb));
+#pragma unroll
+        for (int g = 0; g < (8 >> kb); ++g) w[tw_off(kb) + g] = tab(base + g);
+    }
 }
 
 // MODE: 0 forward, 1 forward without the per-butterfly reduction, 2 inverse,
-// 3 forward lazy with the approximate Shoup quotient
+// 3 forward lazy with the approximate Shoup quotient, 4 forward on doubles,
+// 5 inverse on doubles
 template <int KB_FIRST, int KB_LAST, bool PF, int MODE, class Tab>
 __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi, uint64_t p,
                                           uint64_t two_p) {
     ulonglong2 w[15];
     constexpr int STEP = KB_FIRST > KB_LAST ? -1 : 1;
-    if constexpr (PF) {
-#pragma unroll
-        for (int kb = 0; kb < 4; ++kb) {
-            if ((kb < KB_FIRST && kb < KB_LAST) || (kb > KB_FIRST && kb > KB_LAST)) continue;
-            const int t = t_of_kb0 - kb;
-            const size_t base = (B << t) + ((size_t)th_hi << (3 - kb));
-#pragma unroll
-            for (int g = 0; g < (8 >> kb); ++g) w[tw_off(kb) + g] = tab(base + g);
-        }
-    }
-    run_stages<KB_FIRST, KB_LAST, STEP, PF, MODE>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
+    if constexpr (PF) load_group_tw<KB_FIRST, KB_LAST>(w, tab, t_of_kb0, B, th_hi);
+    run_stages<KB_FIRST, KB_LAST, STEP, PF, MODE, 0>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
 }
 
 // Forward group in the mode of this limb's prime (uniform per CTA).
-template <int KF, int KL, bool PF, bool AQ, class Tab>
+template <int KF, int KL, bool PF, bool AQ, bool FP, class Tab>
 __device__ __forceinline__ void fwd_group(int fmode, uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi,
                                           uint64_t p, uint64_t two_p) {
+    if constexpr (FP) {
+        if (fmode == 4) {
+            run_group<KF, KL, PF, 4>(x, tab, t_of_kb0, B, th_hi, p, two_p);
+            return;
+        }
+    }
     if constexpr (AQ) {
         if (fmode == 3) {
             run_group<KF, KL, PF, 3>(x, tab, t_of_kb0, B, th_hi, p, two_p);
@@ -167,10 +270,38 @@ __device__ __forceinline__ void fwd_group(int fmode, uint64_t (&x)[16], Tab tab,
     run_group<KF, KL, PF, 0>(x, tab, t_of_kb0, B, th_hi, p, two_p);
 }
 
-template <bool AQ>
+template <bool AQ, bool FP>
 __device__ __forceinline__ int fwd_mode(uint64_t p) {
+    if constexpr (FP)
+        if (p < kFpPrimeBound) return 4;
     if constexpr (AQ) return p < kApproxPrimeBound ? 3 : 0;
     return p < kLazyPrimeBound ? 1 : 0;
+}
+
+// Per-prime butterfly constants of a mode (see run_stages).
+struct FwdK {
+    uint64_t k0, k1;
+};
+__device__ __forceinline__ FwdK fwd_consts(int mode, const PrimeConst& pc) {
+    if (mode == 4 || mode == 5) return {as_u64(__ull2double_rn(pc.p)), pc.pinv_f64};
+    return {pc.p, pc.two_p};
+}
+
+template <bool FP>
+__device__ __forceinline__ int inv_mode(uint64_t p) {
+    if constexpr (FP)
+        if (p < kFpPrimeBound) return 5;
+    return 2;
+}
+
+// Inverse group in the mode of this limb's prime (uniform per CTA).
+template <int KF, int KL, bool PF, bool FP, class Tab>
+__device__ __forceinline__ void inv_group(int imode, uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi,
+                                          uint64_t k0, uint64_t k1) {
+    if (FP && imode == 5)
+        run_group<KF, KL, PF, 5>(x, tab, t_of_kb0, B, th_hi, k0, k1);
+    else
+        run_group<KF, KL, PF, 2>(x, tab, t_of_kb0, B, th_hi, k0, k1);
 }
 
 // Tile geometry shared by kernels and launchers.
@@ -189,7 +320,7 @@ struct Geo {
 // ---------------------------------------------------------------------------
 // forward, pass 1: column stages 0..LR-1
 // ---------------------------------------------------------------------------
-template <int LR, int LC, int MINB, bool PF, bool AQ>
+template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP>
 __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
@@ -199,7 +330,10 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
-    const ulonglong2* twg = reinterpret_cast<const ulonglong2*>(ctx.fwd_tw) + (size_t)lr.prime * ctx.N;
+    const int fmode = fwd_mode<AQ, FP>(pc.p);
+    const FwdK kk = fwd_consts(fmode, pc);
+    const ulonglong2* twg =
+        reinterpret_cast<const ulonglong2*>(fmode == 4 ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)lr.prime * ctx.N;
     for (int i = threadIdx.x; i < G::R; i += G::NTC) tws[i] = twg[i];
 
     const int c = threadIdx.x % TC, th = threadIdx.x / TC;
@@ -215,9 +349,12 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
     }
     __syncthreads();
     auto tab = [&](size_t i) { return tws[i]; };
+    if (FP && fmode == 4) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = fp_from_u(x[k]);
+    }
     // stages 0..3: r = th + (k << (LR - 4)), twiddle (1 << t) + (k >> (4 - t))
-    const int fmode = fwd_mode<AQ>(pc.p);
-    fwd_group<3, 0, PF, AQ>(fmode, x, tab, 3, 1, 0, pc.p, pc.two_p);
+    fwd_group<3, 0, PF, AQ, FP>(fmode, x, tab, 3, 1, 0, kk.k0, kk.k1);
     if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) sm[(th + (k << (LR - 4))) * TC + c] = x[k];
@@ -225,7 +362,13 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = sm[((th << 4) + k) * TC + c];
         // stages 4..LR-1: r = 16 th + k
-        fwd_group<LR - 5, 0, PF, AQ>(fmode, x, tab, LR - 1, 1, th, pc.p, pc.two_p);
+        fwd_group<LR - 5, 0, PF, AQ, FP>(fmode, x, tab, LR - 1, 1, th, kk.k0, kk.k1);
+    }
+    if (FP && fmode == 4) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
+    }
+    if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) lr.out[(size_t)((th << 4) + k) * C + col] = x[k];
     } else {
@@ -237,9 +380,12 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
 // ---------------------------------------------------------------------------
 // forward, pass 2: row stages LR..logN-1, with fused epilogue
 // ---------------------------------------------------------------------------
+// v is the lazy butterfly output (canonical already when CANON, the
+// double-precision path)
+template <bool CANON>
 __device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRef& lr, const PrimeConst& pc, size_t g,
                                                  uint64_t v) {
-    v = reduce_fwd(v, pc);
+    if constexpr (!CANON) v = reduce_fwd(v, pc);
     switch (lr.smode) {
         case FS_MODDOWN: {
             const ulonglong2 pinv = ldg2(ctx.md_pinv, lr.prime);
@@ -267,7 +413,7 @@ __device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRe
 // mappings hit 16 distinct bank pairs.
 __device__ __forceinline__ int padi(int r) { return r + (r >> 4); }
 
-template <int LR, int LC, int MINB, bool PF, bool AQ>
+template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP>
 __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
@@ -276,7 +422,9 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
-    const uint64_t* twg = ctx.fwd_tw + (size_t)lr.prime * 2 * ctx.N;
+    const int fmode = fwd_mode<AQ, FP>(pc.p);
+    const FwdK kk = fwd_consts(fmode, pc);
+    const uint64_t* twg = (fmode == 4 ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)lr.prime * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
 
     const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
@@ -285,8 +433,11 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
     uint64_t x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
-    const int fmode = fwd_mode<AQ>(pc.p);
-    fwd_group<3, 0, PF, AQ>(fmode, x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
+    if (FP && fmode == 4) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = fp_from_u(x[k]);
+    }
+    fwd_group<3, 0, PF, AQ, FP>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
 #pragma unroll
@@ -294,23 +445,42 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        fwd_group<LC - 5, 0, PF, AQ>(fmode, x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
+        fwd_group<LC - 5, 0, PF, AQ, FP>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
+        if (FP && fmode == 4) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
+        }
         // each thread rewrites exactly the slots it read
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
     } else {
+        if (FP && fmode == 4) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
+        }
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi(th + k)] = x[k];
     }
     __syncthreads();
     const size_t base = (size_t)blockIdx.x * TR * C;
+    if (FP && fmode == 4) {
 #pragma unroll 4
-    for (int i = threadIdx.x * 2; i < TR * C; i += NT * 2) {
-        const int wi = (i / C) * CP + padi(i % C);
-        ulonglong2 o;
-        o.x = fwd_epilogue(ctx, lr, pc, base + i, sm[wi]);
-        o.y = fwd_epilogue(ctx, lr, pc, base + i + 1, sm[wi + 1]);
-        *reinterpret_cast<ulonglong2*>(lr.out + base + i) = o;
+        for (int i = threadIdx.x * 2; i < TR * C; i += NT * 2) {
+            const int wi = (i / C) * CP + padi(i % C);
+            ulonglong2 o;
+            o.x = fwd_epilogue<true>(ctx, lr, pc, base + i, sm[wi]);
+            o.y = fwd_epilogue<true>(ctx, lr, pc, base + i + 1, sm[wi + 1]);
+            *reinterpret_cast<ulonglong2*>(lr.out + base + i) = o;
+        }
+    } else {
+#pragma unroll 4
+        for (int i = threadIdx.x * 2; i < TR * C; i += NT * 2) {
+            const int wi = (i / C) * CP + padi(i % C);
+            ulonglong2 o;
+            o.x = fwd_epilogue<false>(ctx, lr, pc, base + i, sm[wi]);
+            o.y = fwd_epilogue<false>(ctx, lr, pc, base + i + 1, sm[wi + 1]);
+            *reinterpret_cast<ulonglong2*>(lr.out + base + i) = o;
+        }
     }
 }
 
@@ -319,7 +489,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
 // ---------------------------------------------------------------------------
 // Prologue modes of the inverse row pass (per segment): IL_PLAIN reads `in`,
 // IL_MUL the product in*in2, IL_AXPY_PINV in + in2*P^-1.
-template <int LR, int LC, int MINB, bool PF>
+template <int LR, int LC, int MINB, bool PF, bool FP>
 __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
@@ -328,7 +498,9 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
-    const uint64_t* twg = ctx.inv_tw + (size_t)lr.prime * 2 * ctx.N;
+    const int imode = inv_mode<FP>(pc.p);
+    const FwdK kk = fwd_consts(imode, pc);
+    const uint64_t* twg = (imode == 5 ? ctx.inv_twf : ctx.inv_tw) + (size_t)lr.prime * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
 
     const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
@@ -352,6 +524,10 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
             for (int q = 0; q < PER; ++q)
                 v[q] = add_mod(v[q], mul_shoup(lr.in2[base + threadIdx.x + q * NT], pinv.x, pinv.y, pc.p), pc.p);
         }
+        if (FP && imode == 5) {
+#pragma unroll
+            for (int q = 0; q < PER; ++q) v[q] = fp_from_u(v[q]);
+        }
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
             const int i = threadIdx.x + q * NT;
@@ -364,14 +540,18 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
     if constexpr (LC > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        run_group<0, LC - 5, PF, 2>(x, tab, LC - 1, (size_t)(R + row), th, pc.p, pc.two_p);
+        inv_group<0, LC - 5, PF, FP>(imode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
         __syncthreads();
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = srow[padi(th + (k << (LC - 4)))];
-    run_group<0, 3, PF, 2>(x, tab, 3, (size_t)(R + row), 0, pc.p, pc.two_p);
+    inv_group<0, 3, PF, FP>(imode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+    if (FP && imode == 5) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
+    }
     uint64_t* dst = lr.out + (size_t)row * C;
 #pragma unroll
     for (int k = 0; k < 16; ++k) dst[th + (k << (LC - 4))] = x[k];
@@ -388,7 +568,7 @@ __device__ __forceinline__ const uint64_t* inv_scale_entry(const DevCtx& ctx, co
     }
 }
 
-template <int LR, int LC, int MINB, bool PF>
+template <int LR, int LC, int MINB, bool PF, bool FP>
 __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
@@ -398,7 +578,10 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
-    const ulonglong2* twg = reinterpret_cast<const ulonglong2*>(ctx.inv_tw) + (size_t)lr.prime * ctx.N;
+    const int imode = inv_mode<FP>(pc.p);
+    const FwdK kk = fwd_consts(imode, pc);
+    const ulonglong2* twg =
+        reinterpret_cast<const ulonglong2*>(imode == 5 ? ctx.inv_twf : ctx.inv_tw) + (size_t)lr.prime * ctx.N;
     for (int i = threadIdx.x; i < G::R; i += G::NTC) tws[i] = twg[i];
     const uint64_t* se = inv_scale_entry(ctx, lr);
     const ulonglong2 s0 = ldg2(se, 0), s1 = ldg2(se, 1);
@@ -410,8 +593,12 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
     if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = lr.out[(size_t)((th << 4) + k) * C + col];
+        if (FP && imode == 5) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) x[k] = fp_from_u(x[k]);
+        }
         __syncthreads();
-        run_group<0, LR - 5, PF, 2>(x, tab, LR - 1, 1, th, pc.p, pc.two_p);
+        inv_group<0, LR - 5, PF, FP>(imode, x, tab, LR - 1, 1, th, kk.k0, kk.k1);
 #pragma unroll
         for (int k = 0; k < 16; ++k) sm[((th << 4) + k) * TC + c] = x[k];
         __syncthreads();
@@ -420,15 +607,30 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
     } else {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = lr.out[(size_t)(th + k) * C + col];
+        if (FP && imode == 5) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) x[k] = fp_from_u(x[k]);
+        }
         __syncthreads();
     }
-    run_group<0, 2, PF, 2>(x, tab, 3, 1, 0, pc.p, pc.two_p);
+    inv_group<0, 2, PF, FP>(imode, x, tab, 3, 1, 0, kk.k0, kk.k1);
     // last stage (twiddle index 1) with the N^-1 * scale fold
+    if (FP && imode == 5) {
+        const double p = as_f64(kk.k0), a0 = (double)s0.x, a1 = (double)s1.x;
+        const double a0q = __ddiv_rn(a0, p), a1q = __ddiv_rn(a1, p);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const uint64_t X = x[k], Y = x[k + 8];
-        x[k] = mul_shoup(X + Y, s0.x, s0.y, pc.p);
-        x[k + 8] = mul_shoup(X - Y + pc.two_p, s1.x, s1.y, pc.p);
+        for (int k = 0; k < 8; ++k) {
+            const double X = as_f64(x[k]), Y = as_f64(x[k + 8]);
+            x[k] = fp_to_u(fp_mulw(__dadd_rn(X, Y), a0, a0q, p), p, as_f64(kk.k1));
+            x[k + 8] = fp_to_u(fp_mulw(__dsub_rn(X, Y), a1, a1q, p), p, as_f64(kk.k1));
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint64_t X = x[k], Y = x[k + 8];
+            x[k] = mul_shoup(X + Y, s0.x, s0.y, pc.p);
+            x[k + 8] = mul_shoup(X - Y + pc.two_p, s1.x, s1.y, pc.p);
+        }
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) lr.out[(size_t)(th + (k << (LR - 4))) * C + col] = x[k];
@@ -443,50 +645,78 @@ void count_launches(int n) { g_launches.fetch_add((uint64_t)n); }
 
 bool ntt_supported(int logN) { return logN >= 8 && logN <= 16; }
 
-// Variants: (min CTAs per SM, twiddle policy).  0: (2, group prefetch),
-// 1: (3, per-stage), 2: (4, per-stage).
-int ntt_num_variants() { return 5; }
+// Forward variants: (min CTAs per SM, twiddle policy, butterflies).
+// 0: (2, group prefetch, Harvey / lazy), 1: (3, per-stage, lazy),
+// 2: (4, per-stage, lazy), 3: (3, per-stage, approximate quotient),
+// 4: (2, group prefetch, approximate quotient), 5 and 6: as 3 and 4 with the
+// double-precision butterflies for primes below 2^50, 7: column pass of 5
+// with the row pass of 6, 8: column pass of 5 with a row pass at 4 CTAs per
+// SM.  Inverse configurations: 0 (2, group prefetch),
+// 1 (3, per-stage), 2 (4, per-stage), 3 and 4: as 1 and 0 with
+// double-precision butterflies for primes below 2^50; ntt_inverse_of(v)
+// pairs each forward variant with an inverse configuration of the same
+// arithmetic.
+int ntt_num_variants() { return 9; }
+int ntt_num_inverse_variants() { return 5; }
+int ntt_inverse_of(int v) {
+    static const int inv[9] = {0, 1, 2, 1, 0, 3, 4, 3, 3};
+    return v >= 0 && v < 9 ? inv[v] : 0;
+}
 
-template <int LR, int LC, int MINB, bool PF, bool AQ>
+template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP>
 static void launch_fwd_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
     // grid (tiles, batch element, limb): CTAs run x fastest, then y, so the
     // elements of a batch that share a prime run together and its twiddle
     // table is fetched from HBM once per launch rather than once per element
     dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
-    k_ntt_fwd_cols<LR, LC, MINB, PF, AQ><<<g1, G::NTC, 0, st>>>(ctx, map);
-    k_ntt_fwd_rows<LR, LC, MINB, PF, AQ><<<g2, G::NTR, 0, st>>>(ctx, map);
+    k_ntt_fwd_cols<LR, LC, MINB, PF, AQ, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
+    k_ntt_fwd_rows<LR, LC, MINB, PF, AQ, FP><<<g2, G::NTR, 0, st>>>(ctx, map);
 }
 
-template <int LR, int LC, int MINB, bool PF>
+template <int LR, int LC, int MINB, bool PF, bool FP>
 static void launch_inv_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
     // grid (tiles, batch element, limb): CTAs run x fastest, then y, so the
     // elements of a batch that share a prime run together and its twiddle
     // table is fetched from HBM once per launch rather than once per element
     dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
-    k_ntt_inv_rows<LR, LC, MINB, PF><<<g2, G::NTR, 0, st>>>(ctx, map);
-    k_ntt_inv_cols<LR, LC, MINB, PF><<<g1, G::NTC, 0, st>>>(ctx, map);
+    k_ntt_inv_rows<LR, LC, MINB, PF, FP><<<g2, G::NTR, 0, st>>>(ctx, map);
+    k_ntt_inv_cols<LR, LC, MINB, PF, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
+}
+
+// column pass with one configuration, row pass with another
+template <int LR, int LC, int MB1, bool PF1, int MB2, bool PF2, bool AQ, bool FP>
+static void launch_fwd_mix(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
+    using G = Geo<LR, LC>;
+    dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
+    k_ntt_fwd_cols<LR, LC, MB1, PF1, AQ, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
+    k_ntt_fwd_rows<LR, LC, MB2, PF2, AQ, FP><<<g2, G::NTR, 0, st>>>(ctx, map);
 }
 
 template <int LR, int LC>
 static void launch_fwd(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     switch (ctx.ntt_variant) {
-        case 1: launch_fwd_v<LR, LC, 3, false, false>(ctx, map, st); break;
-        case 2: launch_fwd_v<LR, LC, 4, false, false>(ctx, map, st); break;
-        case 3: launch_fwd_v<LR, LC, 3, false, true>(ctx, map, st); break;
-        case 4: launch_fwd_v<LR, LC, 2, true, true>(ctx, map, st); break;
-        default: launch_fwd_v<LR, LC, 2, true, false>(ctx, map, st); break;
+        case 1: launch_fwd_v<LR, LC, 3, false, false, false>(ctx, map, st); break;
+        case 2: launch_fwd_v<LR, LC, 4, false, false, false>(ctx, map, st); break;
+        case 3: launch_fwd_v<LR, LC, 3, false, true, false>(ctx, map, st); break;
+        case 4: launch_fwd_v<LR, LC, 2, true, true, false>(ctx, map, st); break;
+        case 5: launch_fwd_v<LR, LC, 3, false, true, true>(ctx, map, st); break;
+        case 6: launch_fwd_v<LR, LC, 2, true, true, true>(ctx, map, st); break;
+        case 7: launch_fwd_mix<LR, LC, 3, false, 2, true, true, true>(ctx, map, st); break;
+        case 8: launch_fwd_mix<LR, LC, 3, false, 4, false, true, true>(ctx, map, st); break;
+        default: launch_fwd_v<LR, LC, 2, true, false, false>(ctx, map, st); break;
     }
 }
 
 template <int LR, int LC>
 static void launch_inv(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
-    switch (ctx.ntt_variant) {
-        case 1:
-        case 3: launch_inv_v<LR, LC, 3, false>(ctx, map, st); break;
-        case 2: launch_inv_v<LR, LC, 4, false>(ctx, map, st); break;
-        default: launch_inv_v<LR, LC, 2, true>(ctx, map, st); break;
+    switch (ctx.intt_variant) {
+        case 1: launch_inv_v<LR, LC, 3, false, false>(ctx, map, st); break;
+        case 2: launch_inv_v<LR, LC, 4, false, false>(ctx, map, st); break;
+        case 3: launch_inv_v<LR, LC, 3, false, true>(ctx, map, st); break;
+        case 4: launch_inv_v<LR, LC, 2, true, true>(ctx, map, st); break;
+        default: launch_inv_v<LR, LC, 2, true, false>(ctx, map, st); break;
     }
 }
 

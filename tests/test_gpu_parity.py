@@ -44,6 +44,11 @@ def test_every_ntt_variant_bitexact(logN):
     want = oc.ntt(x, pid)
     xs = np.stack([x, oc.random(pid, 901 + logN)])
     want_b = [want, oc.ntt(xs[1], pid)]
+    pm1 = np.array([oc.primes[i] - 1 for i in pid], dtype=np.uint64)
+    x_max = np.ascontiguousarray(np.broadcast_to(pm1[:, None], x.shape))
+    x_alt = x_max.copy()
+    x_alt[:, ::2] = 0
+    extremes = [(x_max, oc.ntt(x_max, pid)), (x_alt, oc.ntt(x_alt, pid))]
     nv = C.c_int()
     lib.fides_autotune(cc._h, None, None, C.byref(nv))
     for v in range(nv.value):
@@ -57,6 +62,14 @@ def test_every_ntt_variant_bitexact(logN):
         cc.ntt_batch(db.data_ptr(), nl * cc.N, 2, 0, nl)
         got = from_dev(db)
         assert np.array_equal(got[0], want_b[0]) and np.array_equal(got[1], want_b[1]), v
+        # the largest residues everywhere and alternating 0 / p-1 drive the
+        # lazy and double-precision bounds to their worst cases
+        for xe, we in extremes:
+            d = to_dev(xe)
+            cc.ntt(d.data_ptr(), 0, nl)
+            assert np.array_equal(from_dev(d), we), v
+            cc.ntt(d.data_ptr(), 0, nl, inverse=True)
+            assert np.array_equal(from_dev(d), xe), v
     cc.set_ntt_variant(-1)
 
 
@@ -137,9 +150,9 @@ def test_rotate_and_hoisted_parity():
 
 def test_every_conversion_variant_bitexact():
     """Every base-conversion variant (two coefficients per thread with 128-bit
-    or split 32-bit-product sums, one coefficient per thread) gives the
-    oracle's residues (HMult with rescale and a rotation at two levels, moduli
-    below 2^60)."""
+    or split 32-bit-product sums, one coefficient per thread, the int8-split
+    tensor-core ModUp) gives the oracle's residues (HMult with rescale and a
+    rotation at two levels, moduli below 2^60)."""
     from pyfideslib_b200._capi import lib
 
     cc, oc = make_pair(12, 9, 3, 3)
@@ -148,7 +161,7 @@ def test_every_conversion_variant_bitexact():
     g = cc.rotation_galois(3)
     rk = rand_key(oc, 63)
     cc.upload_galois_key(g, *rk)
-    for acc in (0, 1, 2):
+    for acc in (0, 1, 2, 3, 4):
         assert lib.fides_set_conv_accumulator(cc._h, acc) == 0
         for level in (8, 4):
             a0, a1 = rand_ct(oc, level, 70 + level)
@@ -161,6 +174,32 @@ def test_every_conversion_variant_bitexact():
             want = oc.rotate(level, a0, a1, pow(g, -1, 2 * oc.N), *rk)
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (acc, level)
     assert lib.fides_set_conv_accumulator(cc._h, -1) == 0
+    assert lib.fides_tensor_conv_status() == 0
+
+
+@pytest.mark.parametrize("dnum,variant", [(3, 3), (3, 4), (2, 3)])
+def test_tensor_conversion_c2_shape_bitexact(dnum, variant):
+    """The tensor-core ModUp conversion at N=2^16, L=30, K=10 (digits of 10
+    and 15 moduli, 60-bit special primes, the largest residues) gives the
+    oracle's HMult residues at the top, a middle and a low level."""
+    from pyfideslib_b200._capi import lib
+
+    cc, oc = make_pair(16, 30, 10, dnum)
+    kb, ka = rand_key(oc, 1300 + dnum)
+    cc.upload_relin_key(kb, ka)
+    assert lib.fides_set_conv_accumulator(cc._h, variant) == 0
+    for level in (29, 17, 2):
+        a0, a1 = rand_ct(oc, level, 11 + level)
+        b0, b1 = rand_ct(oc, level, 13 + level)
+        if level == 29:
+            pm1 = np.array([q - 1 for q in oc.primes[:level + 1]], dtype=np.uint64)[:, None]
+            a0 = np.ascontiguousarray(np.broadcast_to(pm1, a0.shape))
+            b1 = a0.copy()
+        got = cc.EvalMult(cc.upload(a0, a1), cc.upload(b0, b1), rescale=True).download()
+        want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=True)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), level
+    assert lib.fides_set_conv_accumulator(cc._h, -1) == 0
+    assert lib.fides_tensor_conv_status() == 0
 
 
 def test_hmult_c2_shape_bitexact():
