@@ -129,31 +129,65 @@ __device__ __forceinline__ int target_prime(int m, int lo, int cnt, int n, int L
     return jj < n ? jj : L + (jj - n);
 }
 
-// CK: K = 32*CK bytes of A per row, digits of up to 4*CK limbs.  CHUNK:
-// targets per MMA (N = 16*CHUNK), which is also the tensor-memory columns a
-// CTA holds / 16 (16 targets: two CTAs per SM, 8 targets: up to four).
-template <int CK, int CHUNK>
-__global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 1) k_modup_conv_tc(const __grid_constant__ DevCtx ctx, int level,
-                                                                const uint64_t* __restrict__ xt,
-                                                                uint64_t* __restrict__ dig, size_t dig_stride,
-                                                                size_t bstride) {
+// One conversion launch: ModUp (blockIdx.y = element * digits + digit) or
+// ModDown (blockIdx.y = 2 * element + half).
+struct TcArgs {
+    const uint64_t* xt;  // ModUp: scaled limbs of element 0
+    uint64_t* dig;       // ModUp: digit outputs of element 0
+    size_t dig_stride;   // ModUp: limbs per digit
+    size_t bstride;      // words between batch elements
+    MdArgs md;           // ModDown
+};
+
+// CK: K = 32*CK bytes of A per row, up to 4*CK input limbs.  CHUNK: targets
+// per MMA (N = 16*CHUNK), also the tensor-memory columns a CTA holds / 16
+// (16 targets: two CTAs per SM, 8 targets: up to three; registers bounded to match).  MD: the ModDown
+// conversion, K special limbs -> the Q primes of the level, with the fused
+// Rescale of the top limb when md.ttop is set:
+//   tl = ttop - P^-1 conv_l (mod q_l),  w_q = P^-1 conv_q + SwitchModulus(tl).
+template <int CK, int CHUNK, bool MD>
+__global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 2)
+    k_conv_tc(const __grid_constant__ DevCtx ctx, int level, const __grid_constant__ TcArgs args) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    const int ndig = level / ctx.alpha + 1;
-    const int d = blockIdx.y % ndig;
-    const size_t boff = (size_t)(blockIdx.y / ndig) * bstride;
-    xt += boff;
-    dig += boff;
     const int n = level + 1;
-    const int lo = d * ctx.alpha;
-    const int hi = min(lo + ctx.alpha - 1, level);
-    const int cnt = hi - lo + 1;
-    const int ntar = n - cnt + ctx.K;
+    const uint64_t* in;   // input limb i at in + i * N
+    int lo = 0, cnt, ntar, d = 0, half = 0;
+    size_t boff;
+    bool fused = false;   // ModDown with the top limb (target 0 = prime `level`)
+    if (MD) {
+        half = blockIdx.y & 1;
+        boff = (size_t)(blockIdx.y >> 1) * args.md.bstride;
+        in = args.md.y[half] + boff;
+        cnt = ctx.K;
+        fused = args.md.ttop[half] != nullptr;
+        ntar = n;  // level targets (+ the top limb) or level + 1 targets
+    } else {
+        const int ndig = level / ctx.alpha + 1;
+        d = blockIdx.y % ndig;
+        boff = (size_t)(blockIdx.y / ndig) * args.bstride;
+        lo = d * ctx.alpha;
+        cnt = min(lo + ctx.alpha - 1, level) - lo + 1;
+        ntar = n - cnt + ctx.K;
+        in = args.xt + boff + (size_t)lo * ctx.N;
+    }
+    // prime and matrix column of target m
+    auto tprime = [&](int m) {
+        if (MD) return fused ? (m == 0 ? level : m - 1) : m;
+        return target_prime(m, lo, cnt, n, ctx.L);
+    };
+    const int NP = ctx.L + ctx.K;
+    auto matrix = [&](int i, int m) -> uint64_t {
+        if (MD) return ctx.md_mat[(size_t)i * ctx.L + tprime(m)];
+        return ctx.modup_mat[((size_t)level * ctx.L + lo + i) * NP + tprime(m)];
+    };
     const uint32_t lbo_b = (uint32_t)ntar * kTcCols / 8 * 128;
 
     uint8_t* sA = smem;                                   // 2*CK chunks x kTcLboA
     uint8_t* sB = smem + 2 * CK * kTcLboA;                // 2*CK chunks x lbo_b
     PrimeConst* sP = reinterpret_cast<PrimeConst*>(sB + 2 * CK * lbo_b);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sP + ntar);
+    ulonglong2* sPinv = reinterpret_cast<ulonglong2*>(sP + ntar);  // ModDown: P^-1 mod target
+    uint64_t* sTL = reinterpret_cast<uint64_t*>(sPinv + (MD ? ntar : 0));  // ModDown: tl per row
+    uint64_t* bar = sTL + (MD ? kTcRows : 0);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
 
     // A: zero once (limbs cnt..4*CK-1 stay zero)
@@ -161,19 +195,16 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 1) k_modup_conv_t
         reinterpret_cast<uint4*>(sA)[i] = make_uint4(0, 0, 0, 0);
     // B: 16-byte unit (chunk c, column nn = 16 m + s) holds K bytes 16c..16c+15,
     // i.e. bytes a of limbs 2c and 2c+1 against byte s-a of M[i][m]
-    const int NP = ctx.L + ctx.K;
-    const uint64_t* mat = ctx.modup_mat + (size_t)level * ctx.L * NP;
     const int ncol = ntar * kTcCols;
     for (int u = threadIdx.x; u < 2 * CK * ncol; u += kTcThreads) {
         const int c = u / ncol, nn = u % ncol;
         const int m = nn / kTcCols, s = nn % kTcCols;
-        const int t = target_prime(m, lo, cnt, n, ctx.L);
         uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int i = 2 * c + h;
             if (i >= cnt || s > 14) continue;
-            const uint64_t M = mat[(size_t)(lo + i) * NP + t];
+            const uint64_t M = matrix(i, m);
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
                 const int b = s - a;
@@ -185,7 +216,10 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 1) k_modup_conv_t
         *reinterpret_cast<uint4*>(sB + (size_t)c * lbo_b + (nn >> 3) * 128 + (nn & 7) * 16) =
             make_uint4(w[0], w[1], w[2], w[3]);
     }
-    for (int m = threadIdx.x; m < ntar; m += kTcThreads) sP[m] = ctx.pc[target_prime(m, lo, cnt, n, ctx.L)];
+    for (int m = threadIdx.x; m < ntar; m += kTcThreads) {
+        sP[m] = ctx.pc[tprime(m)];
+        if (MD) sPinv[m] = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[tprime(m)];
+    }
 
     const uint32_t bar_a = smem_u32(bar);
     if (threadIdx.x == 0) {
@@ -205,7 +239,7 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 1) k_modup_conv_t
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = *tslot;
 
-    const int quarter = warp & 3, half = warp >> 2;
+    const int quarter = warp & 3, wh = warp >> 2;
     const int row = quarter * 32 + lane;
     const uint32_t t_lane = tmem + ((uint32_t)(quarter * 32) << 16);
     const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
@@ -220,8 +254,22 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 1) k_modup_conv_t
 #pragma unroll
         for (int q = 0; q < kPer; ++q) {
             const int e = threadIdx.x + q * kTcThreads;
-            if (e < cnt * kTcRows)
-                pre[q] = xt[(size_t)(lo + e / kTcRows) * ctx.N + (size_t)tile * kTcRows + e % kTcRows];
+            if (e < cnt * kTcRows) pre[q] = in[(size_t)(e / kTcRows) * ctx.N + (size_t)tile * kTcRows + e % kTcRows];
+        }
+    };
+    // output of target m for this thread's row (v = conversion value mod p_m)
+    auto finish = [&](int m, uint64_t v, size_t j) {
+        if (MD) {
+            if (fused) {
+                const PrimeConst pc = sP[m];
+                const ulonglong2 pinv = sPinv[m];
+                v = add_mod(mul_shoup(v, pinv.x, pinv.y, pc.p), switch_modulus(sTL[row], sP[0].p, pc), pc.p);
+                args.md.w[half][boff + (size_t)(m - 1) * ctx.N + j] = v;
+            } else {
+                args.md.w[half][boff + (size_t)m * ctx.N + j] = v;
+            }
+        } else {
+            args.dig[boff + ((size_t)d * args.dig_stride + m) * ctx.N + j] = v;
         }
     };
     if (blockIdx.x < ntiles) fetch(blockIdx.x);
@@ -262,9 +310,25 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 1) k_modup_conv_t
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             // the next tile's limbs load while this chunk's outputs are formed
             if (m0 + CHUNK >= ntar && tile + (int)gridDim.x < ntiles) fetch(tile + gridDim.x);
-            uint64_t* out = dig + ((size_t)d * dig_stride + m0) * ctx.N + j0 + row;
+            int first = wh;
+            if (MD && fused && m0 == 0) {
+                // the top limb's value first: every row's tl, shared through smem
+                if (wh == 0) {
+                    uint32_t c[16];
+                    tmem_ld16(t_lane, c);
+                    tmem_wait_ld();
+                    uint64_t vh, vl;
+                    recombine(c, vh, vl);
+                    const PrimeConst pl = sP[0];
+                    const ulonglong2 pinv = sPinv[0];
+                    const uint64_t conv = reduce128(vh, vl, pl);
+                    sTL[row] = sub_mod(args.md.ttop[half][boff + j0 + row], mul_shoup(conv, pinv.x, pinv.y, pl.p), pl.p);
+                }
+                __syncthreads();
+                if (wh == 0) first = 2;
+            }
             // two targets per step (warp-uniform), one wait for both loads
-            for (int mm = half; mm < nt; mm += 4) {
+            for (int mm = first; mm < nt; mm += 4) {
                 const bool two = mm + 2 < nt;
                 uint32_t c0[16], c1[16];
                 tmem_ld16(t_lane + (uint32_t)(mm * kTcCols), c0);
@@ -272,10 +336,10 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 1) k_modup_conv_t
                 tmem_wait_ld();
                 uint64_t vh, vl;
                 recombine(c0, vh, vl);
-                out[(size_t)mm * ctx.N] = reduce128(vh, vl, sP[m0 + mm]);
+                finish(m0 + mm, reduce128(vh, vl, sP[m0 + mm]), j0 + row);
                 if (two) {
                     recombine(c1, vh, vl);
-                    out[(size_t)(mm + 2) * ctx.N] = reduce128(vh, vl, sP[m0 + mm + 2]);
+                    finish(m0 + mm + 2, reduce128(vh, vl, sP[m0 + mm + 2]), j0 + row);
                 }
             }
         }
@@ -290,59 +354,70 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 1) k_modup_conv_t
 }
 
 // dynamic shared memory of one CTA for ntar targets
-size_t tc_smem_bytes(int ck, int ntar) {
-    return (size_t)2 * ck * kTcLboA + (size_t)2 * ck * ntar * kTcCols / 8 * 128 + (size_t)ntar * sizeof(PrimeConst) + 16;
+size_t tc_smem_bytes(int ck, int ntar, bool md) {
+    return (size_t)2 * ck * kTcLboA + (size_t)2 * ck * ntar * kTcCols / 8 * 128 + (size_t)ntar * sizeof(PrimeConst) +
+           (md ? (size_t)ntar * 16 + (size_t)kTcRows * 8 : 0) + 16;
 }
 
 constexpr int kTcMaxTargets = 48;
 constexpr size_t kTcSmemCap = 160 * 1024;
 
-template <int CK, int CHUNK>
+template <int CK, int CHUNK, bool MD>
 void set_smem_attr() {
     static std::once_flag once;
     std::call_once(once, [] {
-        cudaFuncSetAttribute(k_modup_conv_tc<CK, CHUNK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kTcSmemCap);
+        cudaFuncSetAttribute(k_conv_tc<CK, CHUNK, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemCap);
     });
 }
 
-template <int CHUNK>
-void launch_tc(int ck, dim3 g, size_t smem, const DevCtx& ctx, int level, const uint64_t* xt, uint64_t* dig,
-               size_t dig_stride, size_t bstride, cudaStream_t st) {
+template <int CHUNK, bool MD>
+void launch_ck(int ck, dim3 g, size_t smem, const DevCtx& ctx, int level, const TcArgs& a, cudaStream_t st) {
     switch (ck) {
         case 1:
-            set_smem_attr<1, CHUNK>();
-            k_modup_conv_tc<1, CHUNK><<<g, kTcThreads, smem, st>>>(ctx, level, xt, dig, dig_stride, bstride);
+            set_smem_attr<1, CHUNK, MD>();
+            k_conv_tc<1, CHUNK, MD><<<g, kTcThreads, smem, st>>>(ctx, level, a);
             break;
         case 2:
-            set_smem_attr<2, CHUNK>();
-            k_modup_conv_tc<2, CHUNK><<<g, kTcThreads, smem, st>>>(ctx, level, xt, dig, dig_stride, bstride);
+            set_smem_attr<2, CHUNK, MD>();
+            k_conv_tc<2, CHUNK, MD><<<g, kTcThreads, smem, st>>>(ctx, level, a);
             break;
         case 3:
-            set_smem_attr<3, CHUNK>();
-            k_modup_conv_tc<3, CHUNK><<<g, kTcThreads, smem, st>>>(ctx, level, xt, dig, dig_stride, bstride);
+            set_smem_attr<3, CHUNK, MD>();
+            k_conv_tc<3, CHUNK, MD><<<g, kTcThreads, smem, st>>>(ctx, level, a);
             break;
         default:
-            set_smem_attr<4, CHUNK>();
-            k_modup_conv_tc<4, CHUNK><<<g, kTcThreads, smem, st>>>(ctx, level, xt, dig, dig_stride, bstride);
+            set_smem_attr<4, CHUNK, MD>();
+            k_conv_tc<4, CHUNK, MD><<<g, kTcThreads, smem, st>>>(ctx, level, a);
             break;
     }
 }
 
-// largest target count over the digits of a level
-int tc_max_targets(const DevCtx& ctx, int level) {
-    const int n = level + 1, nd = level / ctx.alpha + 1;
-    const int last = n - (nd - 1) * ctx.alpha;
-    return n - std::min(last, ctx.alpha) + ctx.K;
+// grid, shared memory and launch; a floor on the shared memory keeps the
+// CTAs of an SM within its 512 tensor-memory columns (80 KB: at most two
+// CTAs of 256 columns; 58 KB: at most three of 128)
+template <bool MD>
+void launch_tc(const DevCtx& ctx, int level, int groups, int ck, int ntar, const TcArgs& a, cudaStream_t st,
+               int chunk) {
+    const size_t floor_bytes = chunk == 16 ? (size_t)80 * 1024 : (size_t)58 * 1024;
+    const size_t smem = std::max(tc_smem_bytes(ck, ntar, MD), floor_bytes);
+    const int ctas = chunk == 16 ? 2 * 148 : 3 * 148;
+    const int per = std::max(1, std::min(ctx.N / kTcRows, ctas / std::max(1, groups)));
+    const dim3 g(per, groups);
+    count_launches(1);
+    if (chunk == 16)
+        launch_ck<16, MD>(ck, g, smem, ctx, level, a, st);
+    else
+        launch_ck<8, MD>(ck, g, smem, ctx, level, a, st);
 }
 
 }  // namespace
 
 bool conv_tc_supported(const DevCtx& ctx) {
-    if (ctx.alpha > 16) return false;
-    const int ck = (ctx.alpha + 3) / 4;
-    const int nt = ctx.L - 1 + ctx.K;  // any level: at most L-1 other Q primes plus K
-    return nt <= kTcMaxTargets && tc_smem_bytes(ck, nt) <= kTcSmemCap;
+    if (ctx.alpha > 16 || ctx.K > 16) return false;
+    const int up = ctx.L - 1 + ctx.K;  // ModUp: at most L-1 other Q primes plus K
+    return up <= kTcMaxTargets && ctx.L <= kTcMaxTargets &&
+           tc_smem_bytes((ctx.alpha + 3) / 4, up, false) <= kTcSmemCap &&
+           tc_smem_bytes((ctx.K + 3) / 4, ctx.L, true) <= kTcSmemCap;
 }
 
 int conv_tc_error() {
@@ -354,21 +429,20 @@ int conv_tc_error() {
 void launch_modup_conv_tc(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
                           size_t bstride, cudaStream_t st, int chunk) {
     const int nd = level / ctx.alpha + 1;
-    const int ck = (ctx.alpha + 3) / 4;
-    const int ntar = tc_max_targets(ctx, level);
-    // a floor on the shared memory keeps the CTAs of an SM within its 512
-    // tensor-memory columns: 80 KB -> at most two CTAs of 256 columns,
-    // 58 KB -> at most three of 128
-    const size_t floor_bytes = chunk == 16 ? (size_t)80 * 1024 : (size_t)58 * 1024;
-    const size_t smem = std::max(tc_smem_bytes(ck, ntar), floor_bytes);
-    const int ctas = chunk == 16 ? 2 * 148 : 3 * 148;
-    const int per = std::max(1, std::min(ctx.N / kTcRows, ctas / std::max(1, nd * nb)));
-    const dim3 g(per, nd * nb);
-    count_launches(1);
-    if (chunk == 16)
-        launch_tc<16>(ck, g, smem, ctx, level, xt, dig, dig_stride, bstride, st);
-    else
-        launch_tc<8>(ck, g, smem, ctx, level, xt, dig, dig_stride, bstride, st);
+    const int n = level + 1, last = n - (nd - 1) * ctx.alpha;
+    const int ntar = n - std::min(last, ctx.alpha) + ctx.K;  // largest over the digits
+    TcArgs a{};
+    a.xt = xt;
+    a.dig = dig;
+    a.dig_stride = dig_stride;
+    a.bstride = bstride;
+    launch_tc<false>(ctx, level, nd * nb, (ctx.alpha + 3) / 4, ntar, a, st, chunk);
+}
+
+void launch_moddown_conv_tc(const DevCtx& ctx, int level, int nb, const MdArgs& md, cudaStream_t st, int chunk) {
+    TcArgs a{};
+    a.md = md;
+    launch_tc<true>(ctx, level, 2 * nb, (ctx.K + 3) / 4, level + 1, a, st, chunk);
 }
 
 }  // namespace fides

@@ -75,11 +75,12 @@ void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& arg
 // the conversion kernels keep up to 16 inputs (digit moduli / special moduli) in registers
 bool conv_supported(const DevCtx& ctx);
 constexpr int kConvVariants = 5;  // see DevCtx::conv_variant
-// ModUp conversion as an exact int8-split tcgen05 contraction (conv_tc.cu);
-// chunk = targets per MMA (16 or 8)
+// ModUp and ModDown conversions as exact int8-split tcgen05 contractions
+// (conv_tc.cu); chunk = targets per MMA (16 or 8)
 bool conv_tc_supported(const DevCtx& ctx);
 void launch_modup_conv_tc(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
                           size_t bstride, cudaStream_t st, int chunk);
+void launch_moddown_conv_tc(const DevCtx& ctx, int level, int nb, const MdArgs& md, cudaStream_t st, int chunk);
 int conv_tc_error();  // 1 once a tensor-core conversion timed out waiting for its MMAs
 // override every segment's prologue / epilogue mode (-1 keeps the segment's own)
 void set_modes(LimbMap& map, int lmode, int smode);

@@ -357,13 +357,6 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
 //   conv_l = sum_k y_k [P/p_k]_{q_l};  tl = ttop - P^-1 conv_l  (mod q_l)
 //   w_j = P^-1 conv_j + SwitchModulus(tl, q_l -> q_j)  for j < level.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t switch_modulus_d(uint64_t a, uint64_t om, const PrimeConst& nc) {
-    const uint64_t nm = nc.p;
-    if (nm > om) return a > (om >> 1) ? a + (nm - om) : a;
-    const uint64_t om_mod = csub(reduce64_lazy(om, nc), nm);
-    uint64_t v = a > (om >> 1) ? a + (nm - om_mod) : a;
-    return csub(reduce64_lazy(v, nc), nm);
-}
 
 
 template <int MAXIN, class ACC>
@@ -427,8 +420,8 @@ __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_cons
         o.y = b.reduce(pc);
         if (ttop) {
             const ulonglong2 pinv = sPinv[qq];
-            o.x = add_mod(mul_shoup(o.x, pinv.x, pinv.y, pc.p), switch_modulus_d(tl0, ql, pc), pc.p);
-            o.y = add_mod(mul_shoup(o.y, pinv.x, pinv.y, pc.p), switch_modulus_d(tl1, ql, pc), pc.p);
+            o.x = add_mod(mul_shoup(o.x, pinv.x, pinv.y, pc.p), switch_modulus(tl0, ql, pc), pc.p);
+            o.y = add_mod(mul_shoup(o.y, pinv.x, pinv.y, pc.p), switch_modulus(tl1, ql, pc), pc.p);
         }
         *reinterpret_cast<ulonglong2*>(w + (size_t)(q0 + qq) * ctx.N + j) = o;
     };
@@ -454,6 +447,10 @@ __global__ void __launch_bounds__(kConvThreads) k_moddown_conv(const __grid_cons
 void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& a, cudaStream_t st) {
     const int nout = a.ttop[0] ? level : level + 1;
     if (nout <= 0) return;
+    if ((ctx.conv_variant == 3 || ctx.conv_variant == 4) && conv_tc_supported(ctx)) {
+        launch_moddown_conv_tc(ctx, level, nb, a, st, ctx.conv_variant == 3 ? 16 : 8);
+        return;
+    }
     dim3 g(ctx.N / (2 * kConvThreads), (nout + kConvTargets - 1) / kConvTargets, 2 * nb);
     count_launches(1);
 #define FIDES_MODDOWN(M)                                                      \

@@ -83,6 +83,16 @@ FHD uint64_t reduce128(uint64_t hi, uint64_t lo, const PrimeConst& c) {
     return csub(s, c.p);
 }
 
+// Centred lift of a residue a mod om into the modulus of nc
+// (src/CKKS/Rescale.cuh:45-62): a > om/2 stands for a - om.
+FHD uint64_t switch_modulus(uint64_t a, uint64_t om, const PrimeConst& nc) {
+    const uint64_t nm = nc.p;
+    if (nm > om) return a > (om >> 1) ? a + (nm - om) : a;
+    const uint64_t om_mod = csub(reduce64_lazy(om, nc), nm);
+    uint64_t v = a > (om >> 1) ? a + (nm - om_mod) : a;
+    return csub(reduce64_lazy(v, nc), nm);
+}
+
 // 128-bit accumulator of 64x64 products.
 struct Acc128 {
     uint64_t lo, hi;

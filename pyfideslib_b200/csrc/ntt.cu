@@ -162,15 +162,6 @@ __device__ __forceinline__ uint64_t reduce_fwd(uint64_t v, const PrimeConst& c) 
     return csub(reduce64_lazy(v, c), c.p);
 }
 
-// Centred lift of a residue mod om into nm (src/CKKS/Rescale.cuh:45-62).
-__device__ __forceinline__ uint64_t switch_modulus(uint64_t a, uint64_t om, const PrimeConst& nc) {
-    const uint64_t nm = nc.p;
-    if (nm > om) return a > (om >> 1) ? a + (nm - om) : a;
-    const uint64_t om_mod = csub(reduce64_lazy(om, nc), nm);
-    uint64_t v = a > (om >> 1) ? a + (nm - om_mod) : a;
-    return csub(reduce64_lazy(v, nc), nm);
-}
-
 __device__ __forceinline__ ulonglong2 ldg2(const uint64_t* base, size_t idx) {
     return __ldg(reinterpret_cast<const ulonglong2*>(base) + idx);
 }

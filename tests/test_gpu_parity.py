@@ -151,7 +151,8 @@ def test_rotate_and_hoisted_parity():
 def test_every_conversion_variant_bitexact():
     """Every base-conversion variant (two coefficients per thread with 128-bit
     or split 32-bit-product sums, one coefficient per thread, the int8-split
-    tensor-core ModUp) gives the oracle's residues (HMult with rescale and a
+    tensor-core ModUp and ModDown with 16 or 8 targets per MMA) gives the
+    oracle's residues (HMult with and without the fused rescale and a
     rotation at two levels, moduli below 2^60)."""
     from pyfideslib_b200._capi import lib
 
@@ -167,9 +168,10 @@ def test_every_conversion_variant_bitexact():
             a0, a1 = rand_ct(oc, level, 70 + level)
             b0, b1 = rand_ct(oc, level, 80 + level)
             A, B = cc.upload(a0, a1), cc.upload(b0, b1)
-            got = cc.EvalMult(A, B, rescale=True).download()
-            want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=True)
-            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (acc, level)
+            for rs in (True, False):
+                got = cc.EvalMult(A, B, rescale=rs).download()
+                want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=rs)
+                assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (acc, level, rs)
             got = cc.EvalRotate(A, 3).download()
             want = oc.rotate(level, a0, a1, pow(g, -1, 2 * oc.N), *rk)
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (acc, level)
@@ -179,9 +181,9 @@ def test_every_conversion_variant_bitexact():
 
 @pytest.mark.parametrize("dnum,variant", [(3, 3), (3, 4), (2, 3)])
 def test_tensor_conversion_c2_shape_bitexact(dnum, variant):
-    """The tensor-core ModUp conversion at N=2^16, L=30, K=10 (digits of 10
-    and 15 moduli, 60-bit special primes, the largest residues) gives the
-    oracle's HMult residues at the top, a middle and a low level."""
+    """The tensor-core ModUp and ModDown conversions at N=2^16, L=30, K=10
+    (digits of 10 and 15 moduli, 60-bit special primes, the largest residues)
+    give the oracle's HMult residues at the top, a middle and a low level."""
     from pyfideslib_b200._capi import lib
 
     cc, oc = make_pair(16, 30, 10, dnum)
