@@ -436,8 +436,8 @@ def run_ours(args):
     autotune = {"ntt_variant": tv.value,
                 "fwd_inv_us_3x40_limbs": [round(1e3 * tms[i], 2) for i in range(nv.value)],
                 "conv_variant": ["2 coefficients/thread, 128-bit sums", "2 coefficients/thread, split 32-bit products",
-                                 "1 coefficient/thread, 128-bit sums", "tensor cores (int8 split), 16 targets/MMA",
-                                 "tensor cores (int8 split), 8 targets/MMA"][cacc.value],
+                                 "1 coefficient/thread, 128-bit sums", "tensor cores (int8 split), 32 targets/MMA",
+                                 "tensor cores (int8 split), 16 targets/MMA"][cacc.value],
                 "modup_conv_4_elements_us": [round(1e3 * cms[i], 2) for i in range(5)]}
     stream_ptr = C.c_void_p()
     lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))

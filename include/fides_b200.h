@@ -89,13 +89,13 @@ fides_status fides_autotune(fides_ctx* ctx, int* variant, float* times_ms, int* 
 /* The base-conversion variant the autotuner chose (0: two coefficients per
  * thread with 128-bit sums, 1: the same with split 32-bit partial products,
  * for moduli below 2^60, 2: one coefficient per thread, 3 and 4: ModUp on
- * the tensor cores as an exact int8-split contraction with 16 or 8 targets
+ * the tensor cores as an exact int8-split contraction with 32 or 16 targets
  * per matrix product) and the time of each on the ModUp conversion of four
  * top-level elements (times_ms: 5 entries, 0 when not eligible). */
 fides_status fides_autotune_conv_info(const fides_ctx* ctx, int* accumulator, float* times_ms);
 /* Force the conversion variant (0..4, for measurements and tests; 3 and 4
  * run the ModUp conversion on the tensor cores as an exact int8-split
- * contraction with 16 or 8 targets per matrix product, digits of at most 16
+ * contraction with 32 or 16 targets per matrix product, digits of at most 16
  * moduli); -1 restores the tuned choice. */
 fides_status fides_set_conv_accumulator(fides_ctx* ctx, int accumulator);
 /* 1 once a tensor-core conversion gave up waiting for its matrix products

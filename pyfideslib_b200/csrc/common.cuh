@@ -22,8 +22,8 @@ struct DevCtx {
     int intt_variant;            // inverse NTT kernel configuration (0..2)
     int conv_variant;            // base conversions: 0 2 coefficients/thread 128-bit sums, 1 the same with
                                  // split 32-bit products (moduli < 2^60), 2 one coefficient/thread,
-                                 // 3 and 4 ModUp and ModDown on the tensor cores (int8 split, 16
-                                 // or 8 targets per MMA)
+                                 // 3 and 4 ModUp and ModDown on the tensor cores (int8 split, 32
+                                 // or 16 targets per MMA)
     const PrimeConst* pc;        // [L+K]
     const uint64_t* fwd_tw;      // [L+K][N][2]  psi^{bitrev(i)}, companion
     const uint64_t* inv_tw;      // [L+K][N][2]  psi^{-bitrev(i)}, companion

@@ -6,18 +6,22 @@
 // over the cnt limbs i of one digit and the ntar target primes m.
 //
 // Exact int8 split (this file's own design): with x_i = sum_a x_{i,a} 2^{8a}
-// and M[i][m] = sum_b M_{i,m,b} 2^{8b} (bytes), the value before reduction is
-//   V[j][m] = sum_s c_s 2^{8s},  c_s = sum_i sum_{a+b=s} x_{i,a} M_{i,m,b},
-// and every c_s (s = 0..14) is one entry of an unsigned 8-bit matrix product
-//   A[j][(i,a)] = x_{i,a},   B[(i,a)][(m,s)] = M_{i,m,s-a} (0 outside 0..7),
-// accumulated exactly in 32 bits (at most 8 products per limb, each below
-// 2^16, for at most 16 limbs).
+// (bytes) and the pre-shifted constants M'_{i,m,a} = M[i][m] 2^{8a} mod p_m
+// = sum_s M'_{i,m,a,s} 2^{8s} (bytes), the value
+//   V'[j][m] = sum_i sum_a x_{i,a} M'_{i,m,a} = sum_{s<8} c_s 2^{8s},
+//   c_s = sum_i sum_a x_{i,a} M'_{i,m,a,s},
+// is congruent to V mod p_m, and every c_s is one entry of an unsigned 8-bit
+// matrix product A[j][(i,a)] = x_{i,a}, B[(i,a)][(m,s)] = M'_{i,m,a,s},
+// accumulated exactly in 32 bits (c_s < 16 * 8 * 255^2 < 2^23).  Folding the
+// byte position of x into the constants keeps V' below 2^80 and needs 8
+// columns per target, against 2^128 and 15 columns for the plain split.
 // A tile of 128 coefficients is multiplied by B with tcgen05.mma kind::i8
-// (M = 128, N = 16 columns per target, K = 32 bytes per instruction) into
-// tensor memory; the epilogue reads each coefficient's 16 column sums with
-// tcgen05.ld, recombines them into the 128-bit V and reduces it mod p_m.  The
-// tensor cores take the 64x64-bit products off the integer pipes; what is
-// left there is one recombination and one 128-bit reduction per output.
+// (M = 128, N = 8 columns per target, K = 32 bytes per instruction) into
+// tensor memory; the epilogue reads each coefficient's column sums with
+// tcgen05.ld, reassembles V' and reduces it with one Barrett step
+// (q = floor(floor(V'/2^16) floor(2^80/p) / 2^64), remainder in [0, 3p)).
+// The tensor cores take the 64x64-bit products off the integer pipes; what
+// is left there is a few shifts and adds and one 64-bit quotient per output.
 //
 // Operands sit in shared memory in the canonical K-major layout without
 // swizzle: core matrices of 8 rows x 16 bytes stored contiguously, 8-row
@@ -36,7 +40,7 @@ namespace {
 
 constexpr int kTcThreads = 256;     // 8 warps: two per tensor-memory lane quarter
 constexpr int kTcRows = 128;        // coefficients per tile (MMA M)
-constexpr int kTcCols = 16;         // accumulator columns per target (15 byte shifts, 1 zero)
+constexpr int kTcCols = 8;          // accumulator columns per target (byte positions 0..7 of V')
 constexpr uint32_t kTcLboA = (kTcRows / 8) * 128;  // A: K-chunk stride in bytes
 constexpr uint32_t kSpinLimit = 1u << 20;
 
@@ -94,33 +98,27 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&c)[16]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
-__device__ __forceinline__ uint64_t mad_wide(uint32_t a, uint32_t b, uint64_t c) {
-    uint64_t d;
-    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"(b), "l"(c));
-    return d;
+// V' = sum_{s<8} c_s 2^{8s} as (hi, lo), V' < 2^80.  With c_s < 2^23 the
+// pairs w_k = c_{2k} + c_{2k+1} 2^8 fit 32 bits and
+// V' = (w_0 + w_2 2^32) + (w_1 + w_3 2^32) 2^16.
+__device__ __forceinline__ void recombine8(const uint32_t* c, uint64_t& hi, uint64_t& lo) {
+    const uint32_t w0 = c[0] + (c[1] << 8), w1 = c[2] + (c[3] << 8);
+    const uint32_t w2 = c[4] + (c[5] << 8), w3 = c[6] + (c[7] << 8);
+    const uint64_t e = ((uint64_t)w2 << 32) | w0;
+    const uint64_t o = ((uint64_t)w3 << 32) | w1;
+    lo = e + (o << 16);
+    hi = (o >> 48) + (lo < e ? 1 : 0);
 }
 
-// V = sum_s c_s 2^{8s} as (hi, lo).  Every c_s < 2^23, so the four groups
-// g_k = c_{4k} + c_{4k+1} 2^8 + c_{4k+2} 2^16 + c_{4k+3} 2^24 are below 2^48
-// and V = g_0 + g_1 2^32 + g_2 2^64 + g_3 2^96 is assembled word by word.
-// V < 2^128 (at most 16 products of values below 2^62), so the high word of
-// g_3 and the last carry are zero.
-__device__ __forceinline__ void recombine(const uint32_t (&c)[16], uint64_t& hi, uint64_t& lo) {
-    uint64_t g[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t t = c[4 * k] + (c[4 * k + 1] << 8);  // < 2^32
-        g[k] = mad_wide(c[4 * k + 3], 1u << 24, mad_wide(c[4 * k + 2], 1u << 16, (uint64_t)t));
-    }
-    uint32_t w1, w2, w3;
-    asm("add.cc.u32 %0, %3, %4;\n\t"
-        "addc.cc.u32 %1, %5, %6;\n\t"
-        "addc.u32 %2, %7, %8;"
-        : "=r"(w1), "=r"(w2), "=r"(w3)
-        : "r"((uint32_t)(g[0] >> 32)), "r"((uint32_t)g[1]), "r"((uint32_t)(g[1] >> 32)), "r"((uint32_t)g[2]),
-          "r"((uint32_t)(g[2] >> 32)), "r"((uint32_t)g[3]));
-    lo = ((uint64_t)w1 << 32) | (uint32_t)g[0];
-    hi = ((uint64_t)w3 << 32) | w2;
+// V' mod p for V' = hi 2^64 + lo < 2^80 and 2^17 <= p < 2^62, mu = floor(2^80/p):
+// q = floor(floor(V'/2^16) mu / 2^64) lies in [floor(V'/p) - 2, floor(V'/p)],
+// so V' - q p, formed modulo 2^64, is the remainder plus 0, p or 2p.
+__device__ __forceinline__ uint64_t reduce80(uint64_t hi, uint64_t lo, uint64_t mu, uint64_t p) {
+    const uint64_t t = (hi << 48) | (lo >> 16);
+    const uint64_t q = __umul64hi(t, mu);
+    uint64_t r = lo - q * p;
+    r = r >= 2 * p ? r - 2 * p : r;
+    return r >= p ? r - p : r;
 }
 
 // target index m of a digit -> prime id (the other Q primes, then the special ones)
@@ -140,13 +138,13 @@ struct TcArgs {
 };
 
 // CK: K = 32*CK bytes of A per row, up to 4*CK input limbs.  CHUNK: targets
-// per MMA (N = 16*CHUNK), also the tensor-memory columns a CTA holds / 16
-// (16 targets: two CTAs per SM, 8 targets: up to three; registers bounded to match).  MD: the ModDown
-// conversion, K special limbs -> the Q primes of the level, with the fused
-// Rescale of the top limb when md.ttop is set:
+// per MMA (N = 8*CHUNK), also the tensor-memory columns a CTA holds / 8 (32
+// targets: 256 columns, two CTAs per SM; 16 targets: 128 columns, up to three).
+// MD: the ModDown conversion, K special limbs -> the Q primes of the level,
+// with the fused Rescale of the top limb when md.ttop is set:
 //   tl = ttop - P^-1 conv_l (mod q_l),  w_q = P^-1 conv_q + SwitchModulus(tl).
 template <int CK, int CHUNK, bool MD>
-__global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 2)
+__global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
     k_conv_tc(const __grid_constant__ DevCtx ctx, int level, const __grid_constant__ TcArgs args) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int n = level + 1;
@@ -170,6 +168,8 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 2)
         ntar = n - cnt + ctx.K;
         in = args.xt + boff + (size_t)lo * ctx.N;
     }
+    // MMA widths are multiples of 16 columns: targets padded to an even count
+    const int ntar2 = (ntar + 1) & ~1;
     // prime and matrix column of target m
     auto tprime = [&](int m) {
         if (MD) return fused ? (m == 0 ? level : m - 1) : m;
@@ -180,45 +180,53 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 2)
         if (MD) return ctx.md_mat[(size_t)i * ctx.L + tprime(m)];
         return ctx.modup_mat[((size_t)level * ctx.L + lo + i) * NP + tprime(m)];
     };
-    const uint32_t lbo_b = (uint32_t)ntar * kTcCols / 8 * 128;
+    const uint32_t lbo_b = (uint32_t)ntar2 * kTcCols / 8 * 128;
 
     uint8_t* sA = smem;                                   // 2*CK chunks x kTcLboA
     uint8_t* sB = smem + 2 * CK * kTcLboA;                // 2*CK chunks x lbo_b
     PrimeConst* sP = reinterpret_cast<PrimeConst*>(sB + 2 * CK * lbo_b);
-    ulonglong2* sPinv = reinterpret_cast<ulonglong2*>(sP + ntar);  // ModDown: P^-1 mod target
-    uint64_t* sTL = reinterpret_cast<uint64_t*>(sPinv + (MD ? ntar : 0));  // ModDown: tl per row
+    uint64_t* sMu = reinterpret_cast<uint64_t*>(sP + ntar2);       // floor(2^80 / p) per target
+    ulonglong2* sPinv = reinterpret_cast<ulonglong2*>(sMu + ntar2);  // ModDown: P^-1 mod target
+    uint64_t* sTL = reinterpret_cast<uint64_t*>(sPinv + (MD ? ntar2 : 0));  // ModDown: tl per row
     uint64_t* bar = sTL + (MD ? kTcRows : 0);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
 
+    for (int m = threadIdx.x; m < ntar; m += kTcThreads) {
+        const PrimeConst pc = ctx.pc[tprime(m)];
+        sP[m] = pc;
+        sMu[m] = (uint64_t)(((unsigned __int128)1 << 80) / pc.p);
+        if (MD) sPinv[m] = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[tprime(m)];
+    }
     // A: zero once (limbs cnt..4*CK-1 stay zero)
     for (int i = threadIdx.x; i < 2 * CK * (int)kTcLboA / 16; i += kTcThreads)
         reinterpret_cast<uint4*>(sA)[i] = make_uint4(0, 0, 0, 0);
-    // B: 16-byte unit (chunk c, column nn = 16 m + s) holds K bytes 16c..16c+15,
-    // i.e. bytes a of limbs 2c and 2c+1 against byte s-a of M[i][m]
-    const int ncol = ntar * kTcCols;
-    for (int u = threadIdx.x; u < 2 * CK * ncol; u += kTcThreads) {
-        const int c = u / ncol, nn = u % ncol;
-        const int m = nn / kTcCols, s = nn % kTcCols;
-        uint32_t w[4] = {0, 0, 0, 0};
+    // B: for K chunk c (limbs 2c, 2c+1) and target m, the 16 constants
+    // M'_{i,m,a} = M[i][m] 2^{8a} mod p_m; column 8m + s of the chunk holds
+    // their bytes s (16 bytes: a of limb 2c, then a of limb 2c+1)
+    for (int u = threadIdx.x; u < 2 * CK * ntar2; u += kTcThreads) {
+        const int c = u / ntar2, m = u % ntar2;
+        uint64_t mp[16];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int i = 2 * c + h;
-            if (i >= cnt || s > 14) continue;
-            const uint64_t M = matrix(i, m);
+            const bool live = i < cnt && m < ntar;
+            const PrimeConst pc = ctx.pc[live ? tprime(m) : 0];
+            uint64_t v = live ? matrix(i, m) : 0;
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
-                const int b = s - a;
-                if (b < 0 || b > 7) continue;
-                const int pos = 8 * h + a;
-                w[pos >> 2] |= (uint32_t)((M >> (8 * b)) & 0xFF) << (8 * (pos & 3));
+                mp[8 * h + a] = v;
+                if (live && a < 7) v = reduce128(v >> 56, v << 8, pc);  // v 2^8 mod p
             }
         }
-        *reinterpret_cast<uint4*>(sB + (size_t)c * lbo_b + (nn >> 3) * 128 + (nn & 7) * 16) =
-            make_uint4(w[0], w[1], w[2], w[3]);
-    }
-    for (int m = threadIdx.x; m < ntar; m += kTcThreads) {
-        sP[m] = ctx.pc[tprime(m)];
-        if (MD) sPinv[m] = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[tprime(m)];
+#pragma unroll
+        for (int sb = 0; sb < kTcCols; ++sb) {
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int pos = 0; pos < 16; ++pos) w[pos >> 2] |= (uint32_t)((mp[pos] >> (8 * sb)) & 0xFF) << (8 * (pos & 3));
+            const int nn = m * kTcCols + sb;
+            *reinterpret_cast<uint4*>(sB + (size_t)c * lbo_b + (nn >> 3) * 128 + (nn & 7) * 16) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+        }
     }
 
     const uint32_t bar_a = smem_u32(bar);
@@ -272,6 +280,11 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 2)
             args.dig[boff + ((size_t)d * args.dig_stride + m) * ctx.N + j] = v;
         }
     };
+    auto value = [&](const uint32_t* c, int m) {
+        uint64_t vh, vl;
+        recombine8(c, vh, vl);
+        return reduce80(vh, vl, sMu[m], sP[m].p);
+    };
     if (blockIdx.x < ntiles) fetch(blockIdx.x);
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const size_t j0 = (size_t)tile * kTcRows;
@@ -285,8 +298,8 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 2)
             }
         }
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        for (int m0 = 0; m0 < ntar && ok; m0 += CHUNK) {
-            const int nt = min(CHUNK, ntar - m0);
+        for (int m0 = 0; m0 < ntar2 && ok; m0 += CHUNK) {
+            const int nt = min(CHUNK, ntar2 - m0);  // even
             // the A tile is written and the previous chunk's accumulators are read
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
             __syncthreads();
@@ -309,37 +322,42 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 2)
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             // the next tile's limbs load while this chunk's outputs are formed
-            if (m0 + CHUNK >= ntar && tile + (int)gridDim.x < ntiles) fetch(tile + gridDim.x);
+            if (m0 + CHUNK >= ntar2 && tile + (int)gridDim.x < ntiles) fetch(tile + gridDim.x);
+            // target pairs (2p, 2p+1) share one 16-column load; warps of half
+            // wh take pairs wh, wh+2, ... two at a time
             int first = wh;
             if (MD && fused && m0 == 0) {
-                // the top limb's value first: every row's tl, shared through smem
+                // pair 0 holds the top limb: every row's tl first, shared through smem
+                uint32_t c[16];
+                uint64_t v1 = 0;
                 if (wh == 0) {
-                    uint32_t c[16];
                     tmem_ld16(t_lane, c);
                     tmem_wait_ld();
-                    uint64_t vh, vl;
-                    recombine(c, vh, vl);
                     const PrimeConst pl = sP[0];
                     const ulonglong2 pinv = sPinv[0];
-                    const uint64_t conv = reduce128(vh, vl, pl);
+                    const uint64_t conv = value(c, 0);
                     sTL[row] = sub_mod(args.md.ttop[half][boff + j0 + row], mul_shoup(conv, pinv.x, pinv.y, pl.p), pl.p);
+                    if (ntar > 1) v1 = value(c + 8, 1);
                 }
                 __syncthreads();
-                if (wh == 0) first = 2;
+                if (wh == 0) {
+                    if (ntar > 1) finish(1, v1, j0 + row);
+                    first = 2;
+                }
             }
-            // two targets per step (warp-uniform), one wait for both loads
-            for (int mm = first; mm < nt; mm += 4) {
-                const bool two = mm + 2 < nt;
+            for (int pp = first; 2 * pp < nt; pp += 4) {
+                const bool two = 2 * (pp + 2) < nt;
                 uint32_t c0[16], c1[16];
-                tmem_ld16(t_lane + (uint32_t)(mm * kTcCols), c0);
-                if (two) tmem_ld16(t_lane + (uint32_t)((mm + 2) * kTcCols), c1);
+                tmem_ld16(t_lane + (uint32_t)(2 * pp * kTcCols), c0);
+                if (two) tmem_ld16(t_lane + (uint32_t)(2 * (pp + 2) * kTcCols), c1);
                 tmem_wait_ld();
-                uint64_t vh, vl;
-                recombine(c0, vh, vl);
-                finish(m0 + mm, reduce128(vh, vl, sP[m0 + mm]), j0 + row);
+                const int m = m0 + 2 * pp;
+                finish(m, value(c0, m), j0 + row);
+                if (m + 1 < ntar) finish(m + 1, value(c0 + 8, m + 1), j0 + row);
                 if (two) {
-                    recombine(c1, vh, vl);
-                    finish(m0 + mm + 2, reduce128(vh, vl, sP[m0 + mm + 2]), j0 + row);
+                    const int m2 = m + 4;
+                    finish(m2, value(c1, m2), j0 + row);
+                    if (m2 + 1 < ntar) finish(m2 + 1, value(c1 + 8, m2 + 1), j0 + row);
                 }
             }
         }
@@ -355,8 +373,9 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 8 ? 3 : 2)
 
 // dynamic shared memory of one CTA for ntar targets
 size_t tc_smem_bytes(int ck, int ntar, bool md) {
-    return (size_t)2 * ck * kTcLboA + (size_t)2 * ck * ntar * kTcCols / 8 * 128 + (size_t)ntar * sizeof(PrimeConst) +
-           (md ? (size_t)ntar * 16 + (size_t)kTcRows * 8 : 0) + 16;
+    const size_t t2 = (size_t)((ntar + 1) & ~1);
+    return (size_t)2 * ck * kTcLboA + (size_t)2 * ck * t2 * kTcCols / 8 * 128 + t2 * (sizeof(PrimeConst) + 8) +
+           (md ? t2 * 16 + (size_t)kTcRows * 8 : 0) + 16;
 }
 
 constexpr int kTcMaxTargets = 48;
@@ -398,16 +417,16 @@ void launch_ck(int ck, dim3 g, size_t smem, const DevCtx& ctx, int level, const 
 template <bool MD>
 void launch_tc(const DevCtx& ctx, int level, int groups, int ck, int ntar, const TcArgs& a, cudaStream_t st,
                int chunk) {
-    const size_t floor_bytes = chunk == 16 ? (size_t)80 * 1024 : (size_t)58 * 1024;
+    const size_t floor_bytes = chunk == 32 ? (size_t)80 * 1024 : (size_t)58 * 1024;
     const size_t smem = std::max(tc_smem_bytes(ck, ntar, MD), floor_bytes);
-    const int ctas = chunk == 16 ? 2 * 148 : 3 * 148;
+    const int ctas = chunk == 32 ? 2 * 148 : 3 * 148;
     const int per = std::max(1, std::min(ctx.N / kTcRows, ctas / std::max(1, groups)));
     const dim3 g(per, groups);
     count_launches(1);
-    if (chunk == 16)
-        launch_ck<16, MD>(ck, g, smem, ctx, level, a, st);
+    if (chunk == 32)
+        launch_ck<32, MD>(ck, g, smem, ctx, level, a, st);
     else
-        launch_ck<8, MD>(ck, g, smem, ctx, level, a, st);
+        launch_ck<16, MD>(ck, g, smem, ctx, level, a, st);
 }
 
 }  // namespace

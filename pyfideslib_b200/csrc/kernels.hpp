@@ -76,7 +76,7 @@ void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& arg
 bool conv_supported(const DevCtx& ctx);
 constexpr int kConvVariants = 5;  // see DevCtx::conv_variant
 // ModUp and ModDown conversions as exact int8-split tcgen05 contractions
-// (conv_tc.cu); chunk = targets per MMA (16 or 8)
+// (conv_tc.cu); chunk = targets per MMA (32 or 16)
 bool conv_tc_supported(const DevCtx& ctx);
 void launch_modup_conv_tc(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
                           size_t bstride, cudaStream_t st, int chunk);

@@ -216,7 +216,7 @@ bool conv_supported(const DevCtx& ctx) { return ctx.alpha <= kMaxConvIn && ctx.K
 void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
                        size_t bstride, cudaStream_t st) {
     if ((ctx.conv_variant == 3 || ctx.conv_variant == 4) && conv_tc_supported(ctx)) {
-        launch_modup_conv_tc(ctx, level, nb, xt, dig, dig_stride, bstride, st, ctx.conv_variant == 3 ? 16 : 8);
+        launch_modup_conv_tc(ctx, level, nb, xt, dig, dig_stride, bstride, st, ctx.conv_variant == 3 ? 32 : 16);
         return;
     }
     const int nd = level / ctx.alpha + 1;
@@ -448,7 +448,7 @@ void launch_moddown_conv(const DevCtx& ctx, int level, int nb, const MdArgs& a, 
     const int nout = a.ttop[0] ? level : level + 1;
     if (nout <= 0) return;
     if ((ctx.conv_variant == 3 || ctx.conv_variant == 4) && conv_tc_supported(ctx)) {
-        launch_moddown_conv_tc(ctx, level, nb, a, st, ctx.conv_variant == 3 ? 16 : 8);
+        launch_moddown_conv_tc(ctx, level, nb, a, st, ctx.conv_variant == 3 ? 32 : 16);
         return;
     }
     dim3 g(ctx.N / (2 * kConvThreads), (nout + kConvTargets - 1) / kConvTargets, 2 * nb);

@@ -151,7 +151,7 @@ def test_rotate_and_hoisted_parity():
 def test_every_conversion_variant_bitexact():
     """Every base-conversion variant (two coefficients per thread with 128-bit
     or split 32-bit-product sums, one coefficient per thread, the int8-split
-    tensor-core ModUp and ModDown with 16 or 8 targets per MMA) gives the
+    tensor-core ModUp and ModDown with 32 or 16 targets per MMA) gives the
     oracle's residues (HMult with and without the fused rescale and a
     rotation at two levels, moduli below 2^60)."""
     from pyfideslib_b200._capi import lib
