@@ -439,6 +439,14 @@ def run_ours(args):
                                  "1 coefficient/thread, 128-bit sums", "tensor cores (int8 split), 32 targets/MMA",
                                  "tensor cores (int8 split), 16 targets/MMA"][cacc.value],
                 "modup_conv_4_elements_us": [round(1e3 * cms[i], 2) for i in range(5)]}
+    # forced choices (reproducible profiler runs, where the serialised
+    # launches would skew the autotuner's timings)
+    if args.ntt_variant >= 0:
+        lib.fides_set_ntt_variant(cc._h, args.ntt_variant)
+        autotune["forced_ntt_variant"] = args.ntt_variant
+    if args.conv_variant >= 0:
+        lib.fides_set_conv_accumulator(cc._h, args.conv_variant)
+        autotune["forced_conv_variant"] = args.conv_variant
     stream_ptr = C.c_void_p()
     lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))
     st = torch.cuda.ExternalStream(stream_ptr.value, device=local)
@@ -660,6 +668,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-c3", action="store_true", help="skip the config-3 hoisted/BSGS measurement")
     ap.add_argument("--no-boot", action="store_true", help="skip the bootstrap measurement")
+    ap.add_argument("--ntt-variant", type=int, default=-1, help="force a forward NTT variant (default: tuned)")
+    ap.add_argument("--conv-variant", type=int, default=-1, help="force a base-conversion variant (default: tuned)")
     ap.add_argument("--profile-roofline", action="store_true",
                     help="mark the roofline NTT loop for ncu --profile-from-start off")
     args = ap.parse_args()

@@ -19,7 +19,7 @@
 // (M = 128, N = 8 columns per target, K = 32 bytes per instruction) into
 // tensor memory; the epilogue reads each coefficient's column sums with
 // tcgen05.ld, reassembles V' and reduces it with one Barrett step
-// (q = floor(floor(V'/2^16) floor(2^80/p) / 2^64), remainder in [0, 3p)).
+// (q = floor(floor(V'/2^16) floor(2^80/p) / 2^64), remainder in [0, 2p)).
 // The tensor cores take the 64x64-bit products off the integer pipes; what
 // is left there is a few shifts and adds and one 64-bit quotient per output.
 //
@@ -98,26 +98,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&c)[16]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
-// V' = sum_{s<8} c_s 2^{8s} as (hi, lo), V' < 2^80.  With c_s < 2^23 the
-// pairs w_k = c_{2k} + c_{2k+1} 2^8 fit 32 bits and
-// V' = (w_0 + w_2 2^32) + (w_1 + w_3 2^32) 2^16.
-__device__ __forceinline__ void recombine8(const uint32_t* c, uint64_t& hi, uint64_t& lo) {
+// V' mod p for V' = sum_{s<8} c_s 2^{8s}, c_s < 2^23, 2^17 <= p < 2^62.
+// The pairs w_k = c_{2k} + c_{2k+1} 2^8 fit 32 bits, and with
+// e = w_0 + w_2 2^32, o = w_1 + w_3 2^32:  V' = e + o 2^16,
+// floor(V'/2^16) = floor(e/2^16) + o  and  V' mod 2^64 = e + (o << 16).
+// V' < 2^79.01, so with mu = floor(2^80/p) the Barrett quotient
+// q = floor(floor(V'/2^16) mu / 2^64) is floor(V'/p) or one less, and
+// V' - q p (formed modulo 2^64) lies in [0, 2p).
+__device__ __forceinline__ uint64_t reduce_cols(const uint32_t* c, uint64_t mu, uint64_t p) {
     const uint32_t w0 = c[0] + (c[1] << 8), w1 = c[2] + (c[3] << 8);
     const uint32_t w2 = c[4] + (c[5] << 8), w3 = c[6] + (c[7] << 8);
     const uint64_t e = ((uint64_t)w2 << 32) | w0;
     const uint64_t o = ((uint64_t)w3 << 32) | w1;
-    lo = e + (o << 16);
-    hi = (o >> 48) + (lo < e ? 1 : 0);
-}
-
-// V' mod p for V' = hi 2^64 + lo < 2^80 and 2^17 <= p < 2^62, mu = floor(2^80/p):
-// q = floor(floor(V'/2^16) mu / 2^64) lies in [floor(V'/p) - 2, floor(V'/p)],
-// so V' - q p, formed modulo 2^64, is the remainder plus 0, p or 2p.
-__device__ __forceinline__ uint64_t reduce80(uint64_t hi, uint64_t lo, uint64_t mu, uint64_t p) {
-    const uint64_t t = (hi << 48) | (lo >> 16);
-    const uint64_t q = __umul64hi(t, mu);
-    uint64_t r = lo - q * p;
-    r = r >= 2 * p ? r - 2 * p : r;
+    const uint64_t q = __umul64hi((e >> 16) + o, mu);
+    const uint64_t r = e + (o << 16) - q * p;
     return r >= p ? r - p : r;
 }
 
@@ -133,7 +127,8 @@ struct TcArgs {
     const uint64_t* xt;  // ModUp: scaled limbs of element 0
     uint64_t* dig;       // ModUp: digit outputs of element 0
     size_t dig_stride;   // ModUp: limbs per digit
-    size_t bstride;      // words between batch elements
+    size_t bstride;      // ModUp: words between batch elements
+    int nb;              // batch elements
     MdArgs md;           // ModDown
 };
 
@@ -148,26 +143,39 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
     k_conv_tc(const __grid_constant__ DevCtx ctx, int level, const __grid_constant__ TcArgs args) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const int n = level + 1;
-    const uint64_t* in;   // input limb i at in + i * N
-    int lo = 0, cnt, ntar, d = 0, half = 0;
-    size_t boff;
-    bool fused = false;   // ModDown with the top limb (target 0 = prime `level`)
+    const int ntiles = ctx.N / kTcRows;
+    int lo = 0, cnt, ntar, d = 0;
+    // ModDown with the top limb (target 0 = prime `level`); both halves alike
+    const bool fused = MD && args.md.ttop[0] != nullptr;
     if (MD) {
-        half = blockIdx.y & 1;
-        boff = (size_t)(blockIdx.y >> 1) * args.md.bstride;
-        in = args.md.y[half] + boff;
         cnt = ctx.K;
-        fused = args.md.ttop[half] != nullptr;
         ntar = n;  // level targets (+ the top limb) or level + 1 targets
     } else {
-        const int ndig = level / ctx.alpha + 1;
-        d = blockIdx.y % ndig;
-        boff = (size_t)(blockIdx.y / ndig) * args.bstride;
+        d = blockIdx.y;
         lo = d * ctx.alpha;
         cnt = min(lo + ctx.alpha - 1, level) - lo + 1;
         ntar = n - cnt + ctx.K;
-        in = args.xt + boff + (size_t)lo * ctx.N;
     }
+    // work items: (element, tile) of digit d (ModUp) or (element, half, tile)
+    // (ModDown), split evenly over the CTAs of the row
+    const int nitems = (MD ? 2 : 1) * args.nb * ntiles;
+    const int it_begin = (int)((long long)blockIdx.x * nitems / gridDim.x);
+    const int it_end = (int)((long long)(blockIdx.x + 1) * nitems / gridDim.x);
+    // element offset (words) and half of item `it`
+    auto item_off = [&](int it, int& half) -> size_t {
+        if (MD) {
+            const int bh = it / ntiles;
+            half = bh & 1;
+            return (size_t)(bh >> 1) * args.md.bstride;
+        }
+        half = 0;
+        return (size_t)(it / ntiles) * args.bstride;
+    };
+    auto item_in = [&](int it) -> const uint64_t* {
+        int h;
+        const size_t off = item_off(it, h) + (size_t)(it % ntiles) * kTcRows;
+        return MD ? args.md.y[h] + off : args.xt + off + (size_t)lo * ctx.N;
+    };
     // MMA widths are multiples of 16 columns: targets padded to an even count
     const int ntar2 = (ntar + 1) & ~1;
     // prime and matrix column of target m
@@ -176,8 +184,16 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
         return target_prime(m, lo, cnt, n, ctx.L);
     };
     const int NP = ctx.L + ctx.K;
+    // ModDown with the fused rescale converts P^-1 x directly: its constants
+    // carry the factor P^-1 mod q (the conversion is linear)
     auto matrix = [&](int i, int m) -> uint64_t {
-        if (MD) return ctx.md_mat[(size_t)i * ctx.L + tprime(m)];
+        if (MD) {
+            const int t = tprime(m);
+            const uint64_t M = ctx.md_mat[(size_t)i * ctx.L + t];
+            if (!fused) return M;
+            const ulonglong2 pinv = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[t];
+            return mul_shoup(M, pinv.x, pinv.y, ctx.pc[t].p);
+        }
         return ctx.modup_mat[((size_t)level * ctx.L + lo + i) * NP + tprime(m)];
     };
     const uint32_t lbo_b = (uint32_t)ntar2 * kTcCols / 8 * 128;
@@ -186,8 +202,8 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
     uint8_t* sB = smem + 2 * CK * kTcLboA;                // 2*CK chunks x lbo_b
     PrimeConst* sP = reinterpret_cast<PrimeConst*>(sB + 2 * CK * lbo_b);
     uint64_t* sMu = reinterpret_cast<uint64_t*>(sP + ntar2);       // floor(2^80 / p) per target
-    ulonglong2* sPinv = reinterpret_cast<ulonglong2*>(sMu + ntar2);  // ModDown: P^-1 mod target
-    uint64_t* sTL = reinterpret_cast<uint64_t*>(sPinv + (MD ? ntar2 : 0));  // ModDown: tl per row
+    uint64_t* sOm = sMu + ntar2;                         // ModDown: q_level mod target
+    uint64_t* sTL = sOm + (MD ? ntar2 : 0);               // ModDown: tl per row
     uint64_t* bar = sTL + (MD ? kTcRows : 0);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
 
@@ -195,7 +211,7 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
         const PrimeConst pc = ctx.pc[tprime(m)];
         sP[m] = pc;
         sMu[m] = (uint64_t)(((unsigned __int128)1 << 80) / pc.p);
-        if (MD) sPinv[m] = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[tprime(m)];
+        if (MD) sOm[m] = csub(reduce64_lazy(ctx.pc[level].p, pc), pc.p);
     }
     // A: zero once (limbs cnt..4*CK-1 stay zero)
     for (int i = threadIdx.x; i < 2 * CK * (int)kTcLboA / 16; i += kTcThreads)
@@ -253,41 +269,42 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
     const uint32_t a_base = smem_u32(sA), b_base = smem_u32(sB);
     uint32_t phase = 0;
     bool ok = true;
-    const int ntiles = ctx.N / kTcRows;
     // this thread's share of an A tile: element e = threadIdx.x + q * kTcThreads
     // is limb e / kTcRows, row e % kTcRows (at most 2*CK elements)
     constexpr int kPer = 2 * CK;
     uint64_t pre[kPer];
-    auto fetch = [&](int tile) {
+    auto fetch = [&](int it) {
+        const uint64_t* src = item_in(it);
 #pragma unroll
         for (int q = 0; q < kPer; ++q) {
             const int e = threadIdx.x + q * kTcThreads;
-            if (e < cnt * kTcRows) pre[q] = in[(size_t)(e / kTcRows) * ctx.N + (size_t)tile * kTcRows + e % kTcRows];
+            if (e < cnt * kTcRows) pre[q] = src[(size_t)(e / kTcRows) * ctx.N + e % kTcRows];
         }
     };
-    // output of target m for this thread's row (v = conversion value mod p_m)
-    auto finish = [&](int m, uint64_t v, size_t j) {
-        if (MD) {
-            if (fused) {
-                const PrimeConst pc = sP[m];
-                const ulonglong2 pinv = sPinv[m];
-                v = add_mod(mul_shoup(v, pinv.x, pinv.y, pc.p), switch_modulus(sTL[row], sP[0].p, pc), pc.p);
-                args.md.w[half][boff + (size_t)(m - 1) * ctx.N + j] = v;
+    auto value = [&](const uint32_t* c, int m) { return reduce_cols(c, sMu[m], sP[m].p); };
+    if (it_begin < it_end) fetch(it_begin);
+    for (int it = it_begin; it < it_end && ok; ++it) {
+        int half;
+        const size_t boff = item_off(it, half);
+        const size_t j = (size_t)(it % ntiles) * kTcRows + row;  // this thread's coefficient
+        // output of target m for this thread's row (v = conversion value mod p_m)
+        auto finish = [&](int m, uint64_t v) {
+            if (MD) {
+                if (fused) {
+                    // v = P^-1 conv_q (folded into the constants)
+                    // SwitchModulus(tl, q_l -> q) with q_l mod q precomputed
+                    const PrimeConst pc = sP[m];
+                    const uint64_t tl = sTL[row], ql = sP[0].p;
+                    uint64_t sw = tl > (ql >> 1) ? tl + (pc.p - sOm[m]) : tl;
+                    if (pc.p < ql) sw = csub(reduce64_lazy(sw, pc), pc.p);
+                    args.md.w[half][boff + (size_t)(m - 1) * ctx.N + j] = add_mod(v, sw, pc.p);
+                } else {
+                    args.md.w[half][boff + (size_t)m * ctx.N + j] = v;
+                }
             } else {
-                args.md.w[half][boff + (size_t)m * ctx.N + j] = v;
+                args.dig[boff + ((size_t)d * args.dig_stride + m) * ctx.N + j] = v;
             }
-        } else {
-            args.dig[boff + ((size_t)d * args.dig_stride + m) * ctx.N + j] = v;
-        }
-    };
-    auto value = [&](const uint32_t* c, int m) {
-        uint64_t vh, vl;
-        recombine8(c, vh, vl);
-        return reduce80(vh, vl, sMu[m], sP[m].p);
-    };
-    if (blockIdx.x < ntiles) fetch(blockIdx.x);
-    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const size_t j0 = (size_t)tile * kTcRows;
+        };
 #pragma unroll
         for (int q = 0; q < kPer; ++q) {
             const int e = threadIdx.x + q * kTcThreads;
@@ -321,8 +338,8 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
             ok = __syncthreads_and(got) != 0;
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            // the next tile's limbs load while this chunk's outputs are formed
-            if (m0 + CHUNK >= ntar2 && tile + (int)gridDim.x < ntiles) fetch(tile + gridDim.x);
+            // the next item's limbs load while this chunk's outputs are formed
+            if (m0 + CHUNK >= ntar2 && it + 1 < it_end) fetch(it + 1);
             // target pairs (2p, 2p+1) share one 16-column load; warps of half
             // wh take pairs wh, wh+2, ... two at a time
             int first = wh;
@@ -333,15 +350,13 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
                 if (wh == 0) {
                     tmem_ld16(t_lane, c);
                     tmem_wait_ld();
-                    const PrimeConst pl = sP[0];
-                    const ulonglong2 pinv = sPinv[0];
-                    const uint64_t conv = value(c, 0);
-                    sTL[row] = sub_mod(args.md.ttop[half][boff + j0 + row], mul_shoup(conv, pinv.x, pinv.y, pl.p), pl.p);
+                    const uint64_t ql = sP[0].p;
+                    sTL[row] = sub_mod(args.md.ttop[half][boff + j], value(c, 0), ql);  // ttop - P^-1 conv_l
                     if (ntar > 1) v1 = value(c + 8, 1);
                 }
                 __syncthreads();
                 if (wh == 0) {
-                    if (ntar > 1) finish(1, v1, j0 + row);
+                    if (ntar > 1) finish(1, v1);
                     first = 2;
                 }
             }
@@ -352,12 +367,12 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
                 if (two) tmem_ld16(t_lane + (uint32_t)(2 * (pp + 2) * kTcCols), c1);
                 tmem_wait_ld();
                 const int m = m0 + 2 * pp;
-                finish(m, value(c0, m), j0 + row);
-                if (m + 1 < ntar) finish(m + 1, value(c0 + 8, m + 1), j0 + row);
+                finish(m, value(c0, m));
+                if (m + 1 < ntar) finish(m + 1, value(c0 + 8, m + 1));
                 if (two) {
                     const int m2 = m + 4;
-                    finish(m2, value(c1, m2), j0 + row);
-                    if (m2 + 1 < ntar) finish(m2 + 1, value(c1 + 8, m2 + 1), j0 + row);
+                    finish(m2, value(c1, m2));
+                    if (m2 + 1 < ntar) finish(m2 + 1, value(c1 + 8, m2 + 1));
                 }
             }
         }
@@ -375,7 +390,7 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
 size_t tc_smem_bytes(int ck, int ntar, bool md) {
     const size_t t2 = (size_t)((ntar + 1) & ~1);
     return (size_t)2 * ck * kTcLboA + (size_t)2 * ck * t2 * kTcCols / 8 * 128 + t2 * (sizeof(PrimeConst) + 8) +
-           (md ? t2 * 16 + (size_t)kTcRows * 8 : 0) + 16;
+           (md ? t2 * 8 + (size_t)kTcRows * 8 : 0) + 16;
 }
 
 constexpr int kTcMaxTargets = 48;
@@ -415,13 +430,13 @@ void launch_ck(int ck, dim3 g, size_t smem, const DevCtx& ctx, int level, const 
 // CTAs of an SM within its 512 tensor-memory columns (80 KB: at most two
 // CTAs of 256 columns; 58 KB: at most three of 128)
 template <bool MD>
-void launch_tc(const DevCtx& ctx, int level, int groups, int ck, int ntar, const TcArgs& a, cudaStream_t st,
-               int chunk) {
+void launch_tc(const DevCtx& ctx, int level, int groups, int items, int ck, int ntar, const TcArgs& a,
+               cudaStream_t st, int chunk) {
     const size_t floor_bytes = chunk == 32 ? (size_t)80 * 1024 : (size_t)58 * 1024;
     const size_t smem = std::max(tc_smem_bytes(ck, ntar, MD), floor_bytes);
+    // one wave: the CTAs of all rows fill the SMs at the occupancy above
     const int ctas = chunk == 32 ? 2 * 148 : 3 * 148;
-    const int per = std::max(1, std::min(ctx.N / kTcRows, ctas / std::max(1, groups)));
-    const dim3 g(per, groups);
+    const dim3 g(std::max(1, std::min(items, ctas / groups)), groups);
     count_launches(1);
     if (chunk == 32)
         launch_ck<32, MD>(ck, g, smem, ctx, level, a, st);
@@ -455,13 +470,15 @@ void launch_modup_conv_tc(const DevCtx& ctx, int level, int nb, const uint64_t* 
     a.dig = dig;
     a.dig_stride = dig_stride;
     a.bstride = bstride;
-    launch_tc<false>(ctx, level, nd * nb, (ctx.alpha + 3) / 4, ntar, a, st, chunk);
+    a.nb = nb;
+    launch_tc<false>(ctx, level, nd, nb * (ctx.N / kTcRows), (ctx.alpha + 3) / 4, ntar, a, st, chunk);
 }
 
 void launch_moddown_conv_tc(const DevCtx& ctx, int level, int nb, const MdArgs& md, cudaStream_t st, int chunk) {
     TcArgs a{};
     a.md = md;
-    launch_tc<true>(ctx, level, 2 * nb, (ctx.K + 3) / 4, level + 1, a, st, chunk);
+    a.nb = nb;
+    launch_tc<true>(ctx, level, 1, 2 * nb * (ctx.N / kTcRows), (ctx.K + 3) / 4, level + 1, a, st, chunk);
 }
 
 }  // namespace fides
