@@ -98,6 +98,10 @@ fides_status fides_autotune_conv_info(const fides_ctx* ctx, int* accumulator, fl
  * contraction with 32 or 16 targets per matrix product, digits of at most 16
  * moduli); -1 restores the tuned choice. */
 fides_status fides_set_conv_accumulator(fides_ctx* ctx, int accumulator);
+/* Key-switch inner product arithmetic: 1 (default) sums the digit products
+ * of primes below 2^50 exactly on the FP64 pipes, 0 uses 128-bit integer
+ * sums everywhere (identical results; for measurements and tests). */
+fides_status fides_set_keyswitch_variant(fides_ctx* ctx, int variant);
 /* 1 once a tensor-core conversion gave up waiting for its matrix products
  * (bounded wait; its outputs are then invalid), else 0.  Process-wide. */
 int fides_tensor_conv_status(void);

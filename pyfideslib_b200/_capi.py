@@ -63,6 +63,7 @@ EXPORTS = {
     "fides_autotune_conv_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_float)], C.c_int),
     "fides_set_conv_accumulator": ([vp, C.c_int], C.c_int),
     "fides_tensor_conv_status": ([], C.c_int),
+    "fides_set_keyswitch_variant": ([vp, C.c_int], C.c_int),
     "fides_set_ntt_variant": ([vp, C.c_int], C.c_int),
     "fides_key_upload_relin": ([vp, u64p, u64p], C.c_int),
     "fides_key_upload_galois": ([vp, C.c_uint32, u64p, u64p], C.c_int),

@@ -261,6 +261,13 @@ fides_status fides_set_conv_accumulator(fides_ctx* c, int accumulator) {
 
 int fides_tensor_conv_status(void) { return conv_tc_error(); }
 
+fides_status fides_set_keyswitch_variant(fides_ctx* c, int variant) {
+    if (!c || variant < 0 || variant > 1) return FIDES_BAD_ARG;
+    Guard g(c);
+    c->dev.ks_variant = variant;
+    return FIDES_OK;
+}
+
 fides_status fides_set_ntt_variant(fides_ctx* c, int variant) {
     if (!c || variant >= ntt_num_variants() || variant < -1) return FIDES_BAD_ARG;
     Guard g(c);

@@ -451,6 +451,7 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.dnum = c->dnum;
     d.alpha = c->alpha;
     d.ntt_variant = d.intt_variant = d.conv_variant = 0;  // chosen by the autotuner
+    d.ks_variant = 1;
     d.pc = (const PrimeConst*)(base + parts[i_pc].off);
     d.fwd_tw = (const uint64_t*)(base + parts[i_fwd].off);
     d.inv_tw = (const uint64_t*)(base + parts[i_inv].off);

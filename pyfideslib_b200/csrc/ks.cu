@@ -13,6 +13,7 @@
 //     halves in 128-bit registers, reducing once per output;
 //   * rotations fold the automorphism into the inner product as a gather, so
 //     stores stay coalesced.
+#include "fp64.cuh"
 #include "kernels.hpp"
 
 namespace fides {
@@ -255,7 +256,11 @@ void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt,
 // Batch element b = blockIdx.x % nb varies fastest, so the blocks that read
 // one key tile for the different elements run back to back and the key is
 // fetched from HBM once and served from L2 to the rest of the batch.
-template <int VEC, class ACC>
+// FPK: limbs of primes below 2^50 accumulate on the FP64 pipes (fp64.cuh):
+// each product x k is reduced to |r| <= 0.875p, the sum of up to 8 digits
+// stays below 7p < 2^53, and one centring plus a floor reduction give the
+// canonical residue -- the same values as the 128-bit integer sums.
+template <int VEC, class ACC, bool FPK>
 __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx ctx, int level, int nb,
                                                   const __grid_constant__ KsArgs args) {
     const int n = level + 1;
@@ -287,6 +292,34 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
     }
     uint64_t* xb = args.xb + boff + (size_t)m * ctx.N;
     uint64_t* xa = args.xa + boff + (size_t)m * ctx.N;
+    if constexpr (VEC && FPK) {
+        if (pc.p < kFpPrimeBound) {
+            const size_t j = ((size_t)bx * blockDim.x + threadIdx.x) * 2;
+            const double p = __ull2double_rn(pc.p), pinv = as_f64(pc.pinv_f64);
+            double sb0 = 0, sb1 = 0, sa0 = 0, sa1 = 0;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                if (d < nd) {
+                    const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(srcs[d] + j);
+                    const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(kb + d * kstride + (size_t)t * ctx.N + j);
+                    const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(ka + d * kstride + (size_t)t * ctx.N + j);
+                    const double x0 = as_f64(fp_from_u(x.x)), x1 = as_f64(fp_from_u(x.y));
+                    sb0 = __dadd_rn(sb0, fp_mulmod(x0, as_f64(fp_from_u(b.x)), p, pinv));
+                    sb1 = __dadd_rn(sb1, fp_mulmod(x1, as_f64(fp_from_u(b.y)), p, pinv));
+                    sa0 = __dadd_rn(sa0, fp_mulmod(x0, as_f64(fp_from_u(a.x)), p, pinv));
+                    sa1 = __dadd_rn(sa1, fp_mulmod(x1, as_f64(fp_from_u(a.y)), p, pinv));
+                }
+            }
+            ulonglong2 ob, oa;
+            ob.x = fp_to_u(fp_center(sb0, p, pinv), p, pinv);
+            ob.y = fp_to_u(fp_center(sb1, p, pinv), p, pinv);
+            oa.x = fp_to_u(fp_center(sa0, p, pinv), p, pinv);
+            oa.y = fp_to_u(fp_center(sa1, p, pinv), p, pinv);
+            *reinterpret_cast<ulonglong2*>(xb + j) = ob;
+            *reinterpret_cast<ulonglong2*>(xa + j) = oa;
+            return;
+        }
+    }
     if constexpr (VEC) {
         const size_t j = ((size_t)bx * blockDim.x + threadIdx.x) * 2;
         ACC sb0, sb1, sa0, sa1;
@@ -336,16 +369,18 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
     count_launches(1);
     if (plain) {
         dim3 g(ctx.N / 512 * nb, level + 1 + ctx.K);
-        if (ctx.conv_variant == 1)
-            k_ks_inner<1, AccSplit><<<g, 256, 0, st>>>(ctx, level, nb, args);
+        if (ctx.ks_variant == 1)
+            k_ks_inner<1, Acc128, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
+        else if (ctx.conv_variant == 1)
+            k_ks_inner<1, AccSplit, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
         else
-            k_ks_inner<1, Acc128><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            k_ks_inner<1, Acc128, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
     } else {
         dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
         if (ctx.conv_variant == 1)
-            k_ks_inner<0, AccSplit><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            k_ks_inner<0, AccSplit, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
         else
-            k_ks_inner<0, Acc128><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            k_ks_inner<0, Acc128, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
     }
 }
 

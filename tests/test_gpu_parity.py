@@ -204,6 +204,32 @@ def test_tensor_conversion_c2_shape_bitexact(dnum, variant):
     assert lib.fides_tensor_conv_status() == 0
 
 
+@pytest.mark.parametrize("logN,L,K,dnum", [(12, 9, 3, 3), (16, 30, 10, 3)])
+def test_keyswitch_variants_bitexact(logN, L, K, dnum):
+    """The key-switch inner product with 128-bit integer sums and with exact
+    FP64 sums (primes below 2^50) gives the oracle's HMult residues, on random
+    ciphertexts and on the largest residues with the largest key values."""
+    from pyfideslib_b200._capi import lib
+
+    cc, oc = make_pair(logN, L, K, dnum)
+    kb, ka = rand_key(oc, 1400 + logN)
+    pm1_all = np.array([q - 1 for q in oc.primes], dtype=np.uint64)
+    kbx = np.ascontiguousarray(np.broadcast_to(pm1_all[None, :, None], kb.shape))
+    level = L - 1
+    a0, a1 = rand_ct(oc, level, 21)
+    b0, b1 = rand_ct(oc, level, 23)
+    pm1 = np.array([q - 1 for q in oc.primes[:level + 1]], dtype=np.uint64)[:, None]
+    e1 = np.ascontiguousarray(np.broadcast_to(pm1, a1.shape))
+    for keys, (x0, x1, y0, y1) in (((kb, ka), (a0, a1, b0, b1)), ((kbx, kbx), (a0, e1, b0, e1))):
+        cc.upload_relin_key(*keys)
+        want = oc.hmult(level, x0, x1, y0, y1, keys[0], keys[1], rescale=True)
+        for v in (0, 1):
+            assert lib.fides_set_keyswitch_variant(cc._h, v) == 0
+            got = cc.EvalMult(cc.upload(x0, x1), cc.upload(y0, y1), rescale=True).download()
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), v
+    assert lib.fides_set_keyswitch_variant(cc._h, 1) == 0
+
+
 def test_hmult_c2_shape_bitexact():
     """HMult+Relin+Rescale at N=2^16, L=30, K=10, dnum=3, top level, one pair."""
     cc, oc = make_pair(16, 30, 10, 3)
