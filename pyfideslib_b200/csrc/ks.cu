@@ -346,6 +346,31 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
         const int j = bx * blockDim.x + threadIdx.x;
         const uint32_t g = args.galois[bi];
         const uint32_t src = g ? automorph_slot(ctx.logN, g, j) : (uint32_t)j;
+        if constexpr (FPK) {
+            // up to 6 digits: |sum| <= 6 * 0.875p + p (the P c0 term) < 2^53
+            if (pc.p < kFpPrimeBound && nd <= 6) {
+                const double p = __ull2double_rn(pc.p), pinv = as_f64(pc.pinv_f64);
+                double sb = 0, sa = 0;
+#pragma unroll
+                for (int d = 0; d < 6; ++d) {
+                    if (d < nd) {
+                        const double x = as_f64(fp_from_u(srcs[d][src]));
+                        sb = __dadd_rn(sb, fp_mulmod(x, as_f64(fp_from_u(kb[d * kstride + (size_t)t * ctx.N + src])),
+                                                     p, pinv));
+                        sa = __dadd_rn(sa, fp_mulmod(x, as_f64(fp_from_u(ka[d * kstride + (size_t)t * ctx.N + src])),
+                                                     p, pinv));
+                    }
+                }
+                const uint64_t* c0 = args.c0[bi];
+                if (c0 && m < n) {
+                    const ulonglong2 pm = __ldg(reinterpret_cast<const ulonglong2*>(ctx.md_pmod) + t);
+                    sb = __dadd_rn(sb, as_f64(fp_from_u(mul_shoup(c0[(size_t)m * ctx.N + src], pm.x, pm.y, pc.p))));
+                }
+                xb[j] = fp_to_u(fp_center(sb, p, pinv), p, pinv);
+                xa[j] = fp_to_u(fp_center(sa, p, pinv), p, pinv);
+                return;
+            }
+        }
         ACC sb, sa;
 #pragma unroll
         for (int d = 0; d < 8; ++d) {
@@ -377,7 +402,9 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
             k_ks_inner<1, Acc128, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
     } else {
         dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
-        if (ctx.conv_variant == 1)
+        if (ctx.ks_variant == 1)
+            k_ks_inner<0, Acc128, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
+        else if (ctx.conv_variant == 1)
             k_ks_inner<0, AccSplit, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
         else
             k_ks_inner<0, Acc128, false><<<g, 256, 0, st>>>(ctx, level, nb, args);

@@ -123,8 +123,14 @@ def test_rescale_parity():
         assert np.array_equal(got[1], oc.rescale(level, c1))
 
 
-def test_rotate_and_hoisted_parity():
+@pytest.mark.parametrize("ks_variant", [0, 1])
+def test_rotate_and_hoisted_parity(ks_variant):
+    """Rotations and hoisted rotations, with the inner product's integer and
+    FP64 sums."""
+    from pyfideslib_b200._capi import lib
+
     cc, oc = make_pair(12, 8, 3, 3)
+    assert lib.fides_set_keyswitch_variant(cc._h, ks_variant) == 0
     idx = [1, -1, 5, 100]
     keys = {}
     for i, r in enumerate(idx):
