@@ -40,6 +40,8 @@ struct DevCtx {
     const uint64_t* md_pinv;     // [L][2]       P^-1 mod q_j
     const uint64_t* md_pmod;     // [L][2]       P mod q_j
     const uint64_t* rs_qinv;     // [L][L][2]    q_l^-1 mod q_j (row l, column j < l)
+    const uint8_t* tc_btab;      // tensor-core conversions: byte matrices B per (level, digit) and
+    const uint64_t* tc_boff;     //   per (level, fused) for ModDown, and their byte offsets (or null)
 };
 
 // A launch covers up to kMaxSeg segments of contiguous limbs.  Within a

@@ -465,6 +465,27 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.md_pinv = (const uint64_t*)(base + parts[i_dp].off);
     d.md_pmod = (const uint64_t*)(base + parts[i_dq].off);
     d.rs_qinv = (const uint64_t*)(base + parts[i_rq].off);
+    d.tc_btab = nullptr;
+    d.tc_boff = nullptr;
+    if (conv_tc_eligible(d)) {
+        // byte matrices of the tensor-core conversions, one per (level, digit)
+        // and per (level, fused) ModDown (a few MB); without them the
+        // conversions run on the integer pipes
+        std::vector<uint64_t> offs;
+        const size_t bytes = conv_tc_table_layout(d, offs);
+        const size_t obytes = offs.size() * sizeof(uint64_t);
+        if (cudaMalloc(&c->tc_mem, bytes + obytes) == cudaSuccess) {
+            uint8_t* tb = (uint8_t*)c->tc_mem;
+            if (cudaMemcpy(tb + bytes, offs.data(), obytes, cudaMemcpyHostToDevice) == cudaSuccess) {
+                d.tc_btab = tb;
+                d.tc_boff = (const uint64_t*)(tb + bytes);
+                conv_tc_build_tables(d, c->st);
+                if (cudaStreamSynchronize(c->st) != cudaSuccess) return set_err(c, FIDES_CUDA_ERR, "table build failed");
+            }
+        } else {
+            cudaGetLastError();
+        }
+    }
 
     // ---- key-switch workspace for single operations ----
     return ws_reserve(c, c->ws1, 1);
@@ -525,6 +546,8 @@ void free_context(fides_ctx* c) {
     ws_free(c->ws1);
     ws_free(c->wsb);
     if (c->table_mem) cudaFree(c->table_mem);
+    if (c->tc_mem) cudaFree(c->tc_mem);
+    c->tc_mem = nullptr;
     if (c->st) cudaStreamDestroy(c->st);
     if (c->h2d) cudaStreamSynchronize(c->h2d), cudaStreamDestroy(c->h2d);
     if (c->d2h) cudaStreamSynchronize(c->d2h), cudaStreamDestroy(c->d2h);

@@ -96,6 +96,7 @@ struct fides_ctx {
     fides::HostTables host;
     fides::DevCtx dev{};
     void* table_mem = nullptr;
+    void* tc_mem = nullptr;  // tensor-core conversion tables
     size_t table_bytes = 0;
 
     // key-switch workspaces: one element for single operations, a larger one

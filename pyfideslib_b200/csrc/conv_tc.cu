@@ -31,6 +31,7 @@
 // and the CTA releases its tensor memory and returns.
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "kernels.hpp"
 
@@ -121,6 +122,93 @@ __device__ __forceinline__ int target_prime(int m, int lo, int cnt, int n, int L
     return jj < n ? jj : L + (jj - n);
 }
 
+// Geometry of one conversion: the digit's limbs (ModUp) or the K special
+// limbs (ModDown) against the target primes of a level.
+struct TcShape {
+    int level, n, lo, cnt, ntar, ntar2;
+    bool md, fused;
+    __device__ TcShape(const DevCtx& ctx, int lev, bool is_md, bool is_fused, int d)
+        : level(lev), n(lev + 1), lo(0), md(is_md), fused(is_md && is_fused) {
+        if (md) {
+            cnt = ctx.K;
+            ntar = n;  // level targets (+ the top limb) or level + 1 targets
+        } else {
+            lo = d * ctx.alpha;
+            cnt = min(lo + ctx.alpha - 1, level) - lo + 1;
+            ntar = n - cnt + ctx.K;
+        }
+        ntar2 = (ntar + 1) & ~1;  // MMA widths are multiples of 16 columns
+    }
+    // prime of target m
+    __device__ int tprime(const DevCtx& ctx, int m) const {
+        if (md) return fused ? (m == 0 ? level : m - 1) : m;
+        return target_prime(m, lo, cnt, n, ctx.L);
+    }
+    // conversion constant of input limb i for target m; ModDown with the fused
+    // rescale converts P^-1 x directly, so its constants carry P^-1 mod q
+    __device__ uint64_t matrix(const DevCtx& ctx, int i, int m) const {
+        const int t = tprime(ctx, m);
+        if (md) {
+            const uint64_t M = ctx.md_mat[(size_t)i * ctx.L + t];
+            if (!fused) return M;
+            const ulonglong2 pinv = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[t];
+            return mul_shoup(M, pinv.x, pinv.y, ctx.pc[t].p);
+        }
+        return ctx.modup_mat[((size_t)level * ctx.L + lo + i) * (ctx.L + ctx.K) + t];
+    }
+    __device__ uint32_t lbo_b() const { return (uint32_t)ntar2 * kTcCols / 8 * 128; }
+};
+
+// B of a conversion in its shared-memory layout: for K chunk c (limbs 2c,
+// 2c+1) and target m, the 16 constants M'_{i,m,a} = M[i][m] 2^{8a} mod p_m;
+// column 8m + s of the chunk holds their bytes s (16 bytes: a of limb 2c,
+// then a of limb 2c+1), 2*CK chunks lbo_b bytes apart.
+template <int CK>
+__device__ void tc_build_b(const DevCtx& ctx, const TcShape& sh, uint8_t* dst) {
+    const uint32_t lbo_b = sh.lbo_b();
+    for (int u = threadIdx.x; u < 2 * CK * sh.ntar2; u += blockDim.x) {
+        const int c = u / sh.ntar2, m = u % sh.ntar2;
+        uint64_t mp[16];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = 2 * c + h;
+            const bool live = i < sh.cnt && m < sh.ntar;
+            const PrimeConst pc = ctx.pc[live ? sh.tprime(ctx, m) : 0];
+            uint64_t v = live ? sh.matrix(ctx, i, m) : 0;
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                mp[8 * h + a] = v;
+                if (live && a < 7) v = reduce128(v >> 56, v << 8, pc);  // v 2^8 mod p
+            }
+        }
+#pragma unroll
+        for (int sb = 0; sb < kTcCols; ++sb) {
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int pos = 0; pos < 16; ++pos) w[pos >> 2] |= (uint32_t)((mp[pos] >> (8 * sb)) & 0xFF) << (8 * (pos & 3));
+            const int nn = m * kTcCols + sb;
+            *reinterpret_cast<uint4*>(dst + (size_t)c * lbo_b + (nn >> 3) * 128 + (nn & 7) * 16) =
+                make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+}
+
+// index of a conversion's B in the context table
+__host__ __device__ inline int tc_table_index(int L, int dnum, bool md, int level, int d_or_fused) {
+    return md ? L * dnum + 2 * level + d_or_fused : level * dnum + d_or_fused;
+}
+
+// One CTA per table entry of one kind (blockIdx.x = level, blockIdx.y =
+// digit or fused flag); entries that do not exist at a level are skipped.
+template <int CK, bool MD>
+__global__ void __launch_bounds__(256) k_conv_tc_table(const __grid_constant__ DevCtx ctx, uint8_t* tab,
+                                                      const uint64_t* __restrict__ offs) {
+    const int level = blockIdx.x, y = blockIdx.y;
+    if (!MD && y > level / ctx.alpha) return;
+    const TcShape sh(ctx, level, MD, y != 0, y);
+    tc_build_b<CK>(ctx, sh, tab + offs[tc_table_index(ctx.L, ctx.dnum, MD, level, y)]);
+}
+
 // One conversion launch: ModUp (blockIdx.y = element * digits + digit) or
 // ModDown (blockIdx.y = 2 * element + half).
 struct TcArgs {
@@ -142,20 +230,12 @@ template <int CK, int CHUNK, bool MD>
 __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
     k_conv_tc(const __grid_constant__ DevCtx ctx, int level, const __grid_constant__ TcArgs args) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    const int n = level + 1;
     const int ntiles = ctx.N / kTcRows;
-    int lo = 0, cnt, ntar, d = 0;
     // ModDown with the top limb (target 0 = prime `level`); both halves alike
     const bool fused = MD && args.md.ttop[0] != nullptr;
-    if (MD) {
-        cnt = ctx.K;
-        ntar = n;  // level targets (+ the top limb) or level + 1 targets
-    } else {
-        d = blockIdx.y;
-        lo = d * ctx.alpha;
-        cnt = min(lo + ctx.alpha - 1, level) - lo + 1;
-        ntar = n - cnt + ctx.K;
-    }
+    const int d = MD ? 0 : blockIdx.y;
+    const TcShape sh(ctx, level, MD, fused, d);
+    const int lo = sh.lo, cnt = sh.cnt, ntar = sh.ntar, ntar2 = sh.ntar2;
     // work items: (element, tile) of digit d (ModUp) or (element, half, tile)
     // (ModDown), split evenly over the CTAs of the row
     const int nitems = (MD ? 2 : 1) * args.nb * ntiles;
@@ -176,27 +256,7 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
         const size_t off = item_off(it, h) + (size_t)(it % ntiles) * kTcRows;
         return MD ? args.md.y[h] + off : args.xt + off + (size_t)lo * ctx.N;
     };
-    // MMA widths are multiples of 16 columns: targets padded to an even count
-    const int ntar2 = (ntar + 1) & ~1;
-    // prime and matrix column of target m
-    auto tprime = [&](int m) {
-        if (MD) return fused ? (m == 0 ? level : m - 1) : m;
-        return target_prime(m, lo, cnt, n, ctx.L);
-    };
-    const int NP = ctx.L + ctx.K;
-    // ModDown with the fused rescale converts P^-1 x directly: its constants
-    // carry the factor P^-1 mod q (the conversion is linear)
-    auto matrix = [&](int i, int m) -> uint64_t {
-        if (MD) {
-            const int t = tprime(m);
-            const uint64_t M = ctx.md_mat[(size_t)i * ctx.L + t];
-            if (!fused) return M;
-            const ulonglong2 pinv = reinterpret_cast<const ulonglong2*>(ctx.md_pinv)[t];
-            return mul_shoup(M, pinv.x, pinv.y, ctx.pc[t].p);
-        }
-        return ctx.modup_mat[((size_t)level * ctx.L + lo + i) * NP + tprime(m)];
-    };
-    const uint32_t lbo_b = (uint32_t)ntar2 * kTcCols / 8 * 128;
+    const uint32_t lbo_b = sh.lbo_b();
 
     uint8_t* sA = smem;                                   // 2*CK chunks x kTcLboA
     uint8_t* sB = smem + 2 * CK * kTcLboA;                // 2*CK chunks x lbo_b
@@ -208,7 +268,7 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
 
     for (int m = threadIdx.x; m < ntar; m += kTcThreads) {
-        const PrimeConst pc = ctx.pc[tprime(m)];
+        const PrimeConst pc = ctx.pc[sh.tprime(ctx, m)];
         sP[m] = pc;
         sMu[m] = (uint64_t)(((unsigned __int128)1 << 80) / pc.p);
         if (MD) sOm[m] = csub(reduce64_lazy(ctx.pc[level].p, pc), pc.p);
@@ -216,33 +276,12 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
     // A: zero once (limbs cnt..4*CK-1 stay zero)
     for (int i = threadIdx.x; i < 2 * CK * (int)kTcLboA / 16; i += kTcThreads)
         reinterpret_cast<uint4*>(sA)[i] = make_uint4(0, 0, 0, 0);
-    // B: for K chunk c (limbs 2c, 2c+1) and target m, the 16 constants
-    // M'_{i,m,a} = M[i][m] 2^{8a} mod p_m; column 8m + s of the chunk holds
-    // their bytes s (16 bytes: a of limb 2c, then a of limb 2c+1)
-    for (int u = threadIdx.x; u < 2 * CK * ntar2; u += kTcThreads) {
-        const int c = u / ntar2, m = u % ntar2;
-        uint64_t mp[16];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int i = 2 * c + h;
-            const bool live = i < cnt && m < ntar;
-            const PrimeConst pc = ctx.pc[live ? tprime(m) : 0];
-            uint64_t v = live ? matrix(i, m) : 0;
-#pragma unroll
-            for (int a = 0; a < 8; ++a) {
-                mp[8 * h + a] = v;
-                if (live && a < 7) v = reduce128(v >> 56, v << 8, pc);  // v 2^8 mod p
-            }
-        }
-#pragma unroll
-        for (int sb = 0; sb < kTcCols; ++sb) {
-            uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (int pos = 0; pos < 16; ++pos) w[pos >> 2] |= (uint32_t)((mp[pos] >> (8 * sb)) & 0xFF) << (8 * (pos & 3));
-            const int nn = m * kTcCols + sb;
-            *reinterpret_cast<uint4*>(sB + (size_t)c * lbo_b + (nn >> 3) * 128 + (nn & 7) * 16) =
-                make_uint4(w[0], w[1], w[2], w[3]);
-        }
+    // B from the context's table (built once per level and digit)
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(
+            ctx.tc_btab + ctx.tc_boff[tc_table_index(ctx.L, ctx.dnum, MD, level, MD ? (fused ? 1 : 0) : d)]);
+        for (int i = threadIdx.x; i < 2 * CK * (int)lbo_b / 16; i += kTcThreads)
+            reinterpret_cast<uint4*>(sB)[i] = __ldg(src + i);
     }
 
     const uint32_t bar_a = smem_u32(bar);
@@ -446,12 +485,51 @@ void launch_tc(const DevCtx& ctx, int level, int groups, int items, int ck, int 
 
 }  // namespace
 
-bool conv_tc_supported(const DevCtx& ctx) {
+bool conv_tc_eligible(const DevCtx& ctx) {
     if (ctx.alpha > 16 || ctx.K > 16) return false;
     const int up = ctx.L - 1 + ctx.K;  // ModUp: at most L-1 other Q primes plus K
     return up <= kTcMaxTargets && ctx.L <= kTcMaxTargets &&
            tc_smem_bytes((ctx.alpha + 3) / 4, up, false) <= kTcSmemCap &&
            tc_smem_bytes((ctx.K + 3) / 4, ctx.L, true) <= kTcSmemCap;
+}
+
+bool conv_tc_supported(const DevCtx& ctx) { return ctx.tc_btab != nullptr && conv_tc_eligible(ctx); }
+
+size_t conv_tc_table_layout(const DevCtx& ctx, std::vector<uint64_t>& offs) {
+    const int L = ctx.L, K = ctx.K, dn = ctx.dnum;
+    offs.assign((size_t)L * dn + 2 * L, 0);
+    size_t off = 0;
+    auto add = [&](int idx, int ck, int ntar) {
+        offs[idx] = off;
+        off += (size_t)2 * ck * (size_t)((ntar + 1) & ~1) * kTcCols / 8 * 128;
+    };
+    for (int level = 0; level < L; ++level) {
+        const int n = level + 1;
+        for (int d = 0; d <= level / ctx.alpha && d < dn; ++d) {
+            const int lo = d * ctx.alpha, cnt = std::min(lo + ctx.alpha - 1, level) - lo + 1;
+            add(tc_table_index(L, dn, false, level, d), (ctx.alpha + 3) / 4, n - cnt + K);
+        }
+        for (int f = 0; f < 2; ++f) add(tc_table_index(L, dn, true, level, f), (K + 3) / 4, n);
+    }
+    return off;
+}
+
+void conv_tc_build_tables(const DevCtx& ctx, cudaStream_t st) {
+    const dim3 gu(ctx.L, ctx.dnum), gd(ctx.L, 2);
+    uint8_t* tab = const_cast<uint8_t*>(ctx.tc_btab);
+    switch ((ctx.alpha + 3) / 4) {
+        case 1: k_conv_tc_table<1, false><<<gu, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
+        case 2: k_conv_tc_table<2, false><<<gu, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
+        case 3: k_conv_tc_table<3, false><<<gu, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
+        default: k_conv_tc_table<4, false><<<gu, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
+    }
+    switch ((ctx.K + 3) / 4) {
+        case 1: k_conv_tc_table<1, true><<<gd, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
+        case 2: k_conv_tc_table<2, true><<<gd, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
+        case 3: k_conv_tc_table<3, true><<<gd, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
+        default: k_conv_tc_table<4, true><<<gd, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
+    }
+    count_launches(2);
 }
 
 int conv_tc_error() {

@@ -1,5 +1,7 @@
 // kernels.hpp -- host-side launchers of the sm_100a kernels.
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace fides {
@@ -77,7 +79,11 @@ bool conv_supported(const DevCtx& ctx);
 constexpr int kConvVariants = 5;  // see DevCtx::conv_variant
 // ModUp and ModDown conversions as exact int8-split tcgen05 contractions
 // (conv_tc.cu); chunk = targets per MMA (32 or 16)
-bool conv_tc_supported(const DevCtx& ctx);
+bool conv_tc_eligible(const DevCtx& ctx);   // shapes the kernels handle
+bool conv_tc_supported(const DevCtx& ctx);  // eligible and the B tables built
+// byte offsets of the per-(level, digit) and per-(level, fused) B matrices
+size_t conv_tc_table_layout(const DevCtx& ctx, std::vector<uint64_t>& offs);
+void conv_tc_build_tables(const DevCtx& ctx, cudaStream_t st);
 void launch_modup_conv_tc(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
                           size_t bstride, cudaStream_t st, int chunk);
 void launch_moddown_conv_tc(const DevCtx& ctx, int level, int nb, const MdArgs& md, cudaStream_t st, int chunk);
