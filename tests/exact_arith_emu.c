@@ -1,0 +1,207 @@
+/* Host emulation of the exact double-precision arithmetic of the CUDA kernels
+ * (pyfideslib_b200/csrc/fp64.cuh) -- test infrastructure only.
+ *
+ * The device routines are restated with C99 fma() (exactly rounded, like the
+ * GPU's __fma_rn) and, for the one round-down FMA, fesetround(FE_DOWNWARD).
+ * Built by tests/test_exact_arith.py with -ffp-contract=off so that no other
+ * operation is fused.  The drivers run the forward and inverse transforms
+ * with the kernels' stage schedule (N = 2^16 as two passes of two radix-16
+ * groups) and the key-switch sums against exact 128-bit integer arithmetic.
+ */
+#include <fenv.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef unsigned __int128 u128;
+
+static const double kRint = 6755399441055744.0; /* 1.5 * 2^52 */
+static const double kTwo52 = 4503599627370496.0;
+static const uint64_t kMant52 = (1ull << 52) - 1;
+
+static double fp_mulw(double y, double w, double wq, double p) {
+    const double h = y * w;
+    const double l = fma(y, w, -h);
+    const double q = fma(y, wq, kRint) - kRint;
+    return fma(-q, p, h) + l;
+}
+
+static double fp_center(double x, double p, double pinv) {
+    const double q = fma(x, pinv, kRint) - kRint;
+    return fma(-q, p, x);
+}
+
+static double fma_rd(double a, double b, double c) {
+    fesetround(FE_DOWNWARD);
+    volatile double r = fma(a, b, c);
+    fesetround(FE_TONEAREST);
+    return r;
+}
+
+static uint64_t fp_to_u(double v, double p, double pinv_up) {
+    const double two_p = p + p;
+    const double a = v + two_p;
+    const double b = v + (two_p + kTwo52);
+    const double q = fma_rd(a, pinv_up, kRint) - kRint;
+    const double r = fma(-q, p, b);
+    uint64_t u;
+    memcpy(&u, &r, 8);
+    return u & kMant52;
+}
+
+static double fp_mulmod(double x, double y, double p, double pinv) {
+    const double h = x * y;
+    const double l = fma(x, y, -h);
+    const double q = fma(h, pinv, kRint) - kRint;
+    return fma(-q, p, h) + l;
+}
+
+/* the double nearest above 1/p (context.cpp recip_up) */
+static double recip_up(uint64_t p) {
+    double x = 1.0 / (double)p;
+    int e = 0;
+    const double f = frexp(x, &e);
+    const uint64_t m = (uint64_t)ldexp(f, 53);
+    const int sh = 53 - e;
+    if (sh < 128 && (u128)m * p < ((u128)1 << sh)) x = nextafter(x, 1.0);
+    return x;
+}
+
+static uint64_t mulmod(uint64_t a, uint64_t b, uint64_t p) { return (uint64_t)((u128)a * b % p); }
+
+static uint64_t powmod(uint64_t a, uint64_t e, uint64_t p) {
+    uint64_t r = 1;
+    while (e) {
+        if (e & 1) r = mulmod(r, a, p);
+        a = mulmod(a, a, p);
+        e >>= 1;
+    }
+    return r;
+}
+
+static uint32_t bitrev(uint32_t x, int bits) {
+    uint32_t r = 0;
+    for (int b = 0; b < bits; ++b)
+        if (x >> b & 1) r |= 1u << (bits - 1 - b);
+    return r;
+}
+
+static uint64_t splitmix(uint64_t* s) {
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* Forward transform with the kernels' schedule: stage s (0..15) centres X
+ * first when s % 4 is odd, each pass of 8 stages ends with fp_to_u; then the
+ * inverse (Gentleman-Sande, sum centred every stage, N^-1 folded into the
+ * last stage).  psi: primitive 2N-th root mod p < 2^50.  pattern 0: random
+ * residues, 1: p - 1 everywhere, 2: alternating 0 / p - 1.  Returns the number
+ * of coefficients that differ from exact arithmetic (forward) plus those
+ * that do not come back (inverse), or -1 if a value left its proven range. */
+int emu_ntt_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
+    const int logN = 16, N = 1 << logN;
+    uint64_t *a = malloc(8 * N), *e = malloc(8 * N), *tw = malloc(8 * N), *itw = malloc(8 * N);
+    double *d = malloc(8 * (size_t)N), *W = malloc(8 * (size_t)N), *WQ = malloc(8 * (size_t)N);
+    double *IW = malloc(8 * (size_t)N), *IWQ = malloc(8 * (size_t)N);
+    const uint64_t ipsi = powmod(psi, 2 * (uint64_t)N - 1, p);
+    uint64_t pw = 1, ipw = 1;
+    uint64_t *pows = malloc(8 * N), *ipows = malloc(8 * N);
+    for (int j = 0; j < N; ++j) {
+        pows[j] = pw;
+        ipows[j] = ipw;
+        pw = mulmod(pw, psi, p);
+        ipw = mulmod(ipw, ipsi, p);
+    }
+    for (int j = 0; j < N; ++j) {
+        tw[j] = pows[bitrev(j, logN)];
+        itw[j] = ipows[bitrev(j, logN)];
+        W[j] = (double)tw[j];
+        WQ[j] = W[j] / (double)p;
+        IW[j] = (double)itw[j];
+        IWQ[j] = IW[j] / (double)p;
+    }
+    uint64_t s = seed;
+    for (int j = 0; j < N; ++j)
+        a[j] = pattern == 1 ? p - 1 : pattern == 2 ? ((j & 1) ? p - 1 : 0) : splitmix(&s) % p;
+    /* exact forward */
+    memcpy(e, a, 8 * N);
+    for (int m = 1, t = N / 2; m < N; m <<= 1, t >>= 1)
+        for (int i = 0; i < m; ++i)
+            for (int j = 2 * i * t; j < 2 * i * t + t; ++j) {
+                const uint64_t X = e[j], Y = mulmod(e[j + t], tw[m + i], p);
+                e[j] = (X + Y) % p;
+                e[j + t] = (X + p - Y) % p;
+            }
+    const double pd = (double)p, pinv = recip_up(p);
+    int bad = 0;
+    for (int j = 0; j < N; ++j) d[j] = (double)a[j];
+    int st = 0;
+    for (int m = 1, t = N / 2; m < N; m <<= 1, t >>= 1, ++st) {
+        const int red = (st % 4) & 1;
+        for (int i = 0; i < m; ++i)
+            for (int j = 2 * i * t; j < 2 * i * t + t; ++j) {
+                double x = d[j];
+                const double y = d[j + t];
+                if (fabs(y) >= 2251799813685248.0) bad = -1; /* |y| < 2^51 */
+                if (red) x = fp_center(x, pd, pinv);
+                const double tt = fp_mulw(y, W[m + i], WQ[m + i], pd);
+                d[j] = x + tt;
+                d[j + t] = x - tt;
+            }
+        if (st == 7 || st == 15)
+            for (int j = 0; j < N; ++j) d[j] = (double)fp_to_u(d[j], pd, pinv);
+    }
+    if (bad < 0) goto done;
+    for (int j = 0; j < N; ++j) bad += (uint64_t)d[j] != e[j];
+    /* inverse from the exact forward values */
+    {
+        const uint64_t ninv = powmod(N, p - 2, p), w1 = itw[1], s1 = mulmod(ninv, w1, p);
+        for (int j = 0; j < N; ++j) d[j] = (double)e[j];
+        int stg = 0;
+        for (int m = N / 2, t = 1; m > 1; m >>= 1, t <<= 1, ++stg) {
+            if (stg == 8)
+                for (int j = 0; j < N; ++j) d[j] = (double)fp_to_u(d[j], pd, pinv);
+            for (int i = 0; i < m; ++i)
+                for (int j = 2 * i * t; j < 2 * i * t + t; ++j) {
+                    const double x = d[j], y = d[j + t];
+                    if (fabs(x - y) >= 2251799813685248.0) { bad = -1; goto done; }
+                    d[j] = fp_center(x + y, pd, pinv);
+                    d[j + t] = fp_mulw(x - y, IW[m + i], IWQ[m + i], pd);
+                }
+        }
+        const double a0 = (double)ninv, a1 = (double)s1, a0q = a0 / pd, a1q = a1 / pd;
+        for (int j = 0; j < N / 2; ++j) {
+            const double x = d[j], y = d[j + N / 2];
+            d[j] = (double)fp_to_u(fp_mulw(x + y, a0, a0q, pd), pd, pinv);
+            d[j + N / 2] = (double)fp_to_u(fp_mulw(x - y, a1, a1q, pd), pd, pinv);
+        }
+        for (int j = 0; j < N; ++j) bad += (uint64_t)d[j] != a[j];
+    }
+done:
+    free(a); free(e); free(tw); free(itw); free(d); free(W); free(WQ); free(IW); free(IWQ); free(pows); free(ipows);
+    return bad;
+}
+
+/* Key-switch sums: sum of nd products x k reduced by fp_mulmod, centred and
+ * floor-reduced, against exact arithmetic, for `trials` random (or, with
+ * extreme != 0, maximal) operands.  Returns the number of mismatches. */
+int emu_ks_check(uint64_t p, int nd, uint64_t seed, int trials, int extreme) {
+    const double pd = (double)p, pinv = recip_up(p);
+    uint64_t s = seed;
+    int bad = 0;
+    for (int t = 0; t < trials; ++t) {
+        double acc = 0;
+        u128 exact = 0;
+        for (int dd = 0; dd < nd; ++dd) {
+            const uint64_t x = extreme ? p - 1 : splitmix(&s) % p;
+            const uint64_t k = extreme ? p - 1 - (uint64_t)(t & 1) : splitmix(&s) % p;
+            acc += fp_mulmod((double)x, (double)k, pd, pinv);
+            exact += (u128)x * k;
+        }
+        bad += fp_to_u(fp_center(acc, pd, pinv), pd, pinv) != (uint64_t)(exact % p);
+    }
+    return bad;
+}
