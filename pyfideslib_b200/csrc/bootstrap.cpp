@@ -416,7 +416,10 @@ class Chebyshev {
         return std::min({L.at(n) - 1, feasible(L, d - n) - 1, feasible(L, n - 1)});
     }
 
-    Lanes eval(const std::vector<double>& coeffs, int level, double scale) { return rec(coeffs, level, scale); }
+    Lanes eval(const std::vector<double>& coeffs, int level, double scale) {
+        powers((int)coeffs.size() - 1);
+        return rec(coeffs, level, scale);
+    }
 
    private:
     Arith& A;
@@ -424,34 +427,94 @@ class Chebyshev {
     std::map<int, Lanes> T;
     std::map<int, int> lvl;
 
+    // T_k for k < kBaby and the giant steps kBaby 2^j up to the degree,
+    // computed in rounds of equal dependency depth: every round's products
+    // go out as one batched HMult (T_2; T_3, T_4; T_5..T_8; T_16; ...)
+    void powers(int d) {
+        std::vector<int> ks;
+        for (int k = 2; k < std::min(kBaby, d + 1); ++k) ks.push_back(k);
+        for (int n = kBaby; n <= d; n <<= 1) ks.push_back(n);
+        std::map<int, int> depth;
+        depth[1] = 0;
+        auto dep = [&](auto&& self, int k) -> int {
+            auto it = depth.find(k);
+            if (it != depth.end()) return it->second;
+            const int v = k % 2 == 0 ? self(self, k / 2) + 1 : std::max(self(self, k / 2), self(self, k / 2 + 1)) + 1;
+            depth[k] = v;
+            return v;
+        };
+        std::map<int, std::vector<int>> rounds;
+        for (int k : ks) {
+            // odd k needs T_{k/2} and T_{k/2+1}, even k needs T_{k/2}: both in ks or 1
+            rounds[dep(dep, k)].push_back(k);
+        }
+        for (auto& kv : rounds) {
+            std::vector<int> todo;
+            for (int k : kv.second)
+                if (!T.count(k)) todo.push_back(k);
+            // operands of lower depth may not be in ks (a leaf-only power): build them lazily
+            for (int k : todo) {
+                get(k / 2);
+                if (k % 2) get(k / 2 + 1);
+            }
+            products(todo);
+        }
+    }
+
+    // T_k for every k in ks (operands present), one batched HMult for all
+    void products(const std::vector<int>& ks) {
+        if (ks.empty()) return;
+        Lanes xa, xb;
+        for (int k : ks) {
+            const Lanes& a = T.at(k / 2);
+            const Lanes& b = k % 2 == 0 ? a : T.at(k / 2 + 1);
+            xa.insert(xa.end(), a.begin(), a.end());
+            xb.insert(xb.end(), b.begin(), b.end());
+        }
+        const Lanes all = A.mul(xa, xb);
+        const size_t nl = T.at(1).size();
+        for (size_t i = 0; i < ks.size(); ++i) T[ks[i]] = finish(ks[i], Lanes(all.begin() + i * nl, all.begin() + (i + 1) * nl));
+    }
+
+    // 2 T_{k/2}^2 - 1 (even k) or 2 T_{k/2} T_{k/2+1} - T_1 (odd k) from the product p
+    Lanes finish(int k, const Lanes& p) {
+        if (k % 2 == 0) return A.ilin({{&p, 2}}, -1.0, p[0]->level);
+        // T_1 brought to the product's (level, scale)
+        Lanes t1 = A.lin({{&T[1], 1.0}}, 0.0, p[0]->level + 1, p[0]->scale, p);
+        return A.ilin({{&p, 2}, {&t1, -1}}, 0.0, p[0]->level);
+    }
+
     const Lanes& get(int k) {
         auto it = T.find(k);
         if (it != T.end()) return it->second;
-        Lanes r;
-        if (k % 2 == 0) {
-            const Lanes& h = get(k / 2);
-            Lanes sq = A.mul(h, h);
-            // 2 T_{k/2}^2 - 1
-            r = A.ilin({{&sq, 2}}, -1.0, sq[0]->level);
-        } else {
-            const Lanes& a = get(k / 2);
-            const Lanes& b = get(k / 2 + 1);
-            Lanes p = A.mul(a, b);
-            // T_1 brought to the product's (level, scale)
-            Lanes t1 = A.lin({{&T[1], 1.0}}, 0.0, p[0]->level + 1, p[0]->scale, p);
-            r = A.ilin({{&p, 2}, {&t1, -1}}, 0.0, p[0]->level);
-        }
-        T[k] = r;
-        return T[k];
+        get(k / 2);
+        if (k % 2) get(k / 2 + 1);
+        products({k});
+        return T.at(k);
     }
 
-    Lanes rec(const std::vector<double>& c, int level, double scale) {
+    // The recursion p = T_n Q + R as a tree: leaves (degree < kBaby) are
+    // linear combinations of T_1..T_7, every inner node one product T_n Q.
+    // Nodes of equal depth are independent, so their products go out as one
+    // batched HMult, deepest level first.
+    struct Node {
+        Lanes val;
+        int n = 0, q = -1, r = -1, level = 0, depth = 0;
+    };
+    std::vector<Node> nodes;
+
+    int build(const std::vector<double>& c, int level, double scale, int depth) {
         const int d = (int)c.size() - 1;
+        Node nd;
+        nd.level = level;
+        nd.depth = depth;
         if (d < kBaby) {
             std::vector<std::pair<const Lanes*, double>> terms;
             for (int k = 1; k <= d; ++k)
                 if (c[k] != 0.0) terms.push_back({&get(k), c[k]});
-            return A.lin(terms, c[0], level + 1, scale, T[1]);
+            nd.val = A.lin(terms, c[0], level + 1, scale, T[1]);
+            nodes.push_back(nd);
+            return (int)nodes.size() - 1;
         }
         int n = kBaby;
         while (2 * n <= d) n <<= 1;
@@ -463,10 +526,39 @@ class Chebyshev {
         }
         const Lanes& Tn = get(n);
         const double sq = scale * (double)A.c->host.prime[level + 1] / Tn[0]->scale;
-        Lanes Q = rec(q, level + 1, sq);
-        Lanes P = A.mul(Tn, Q);
-        Lanes R = rec(r, level, scale);
-        return A.ilin({{&P, 1}, {&R, 1}}, 0.0, level);
+        nd.n = n;
+        nd.q = build(q, level + 1, sq, depth + 1);
+        nd.r = build(r, level, scale, depth + 1);
+        nodes.push_back(nd);
+        return (int)nodes.size() - 1;
+    }
+
+    Lanes rec(const std::vector<double>& c, int level, double scale) {
+        nodes.clear();
+        const int root = build(c, level, scale, 0);
+        int maxd = 0;
+        for (const Node& nd : nodes) maxd = std::max(maxd, nd.depth);
+        const size_t nl = T.at(1).size();
+        for (int dd = maxd; dd >= 0; --dd) {
+            std::vector<int> idx;
+            Lanes xa, xb;
+            for (int i = 0; i < (int)nodes.size(); ++i)
+                if (nodes[i].depth == dd && nodes[i].q >= 0) {
+                    idx.push_back(i);
+                    const Lanes& tn = T.at(nodes[i].n);
+                    const Lanes& qv = nodes[nodes[i].q].val;
+                    xa.insert(xa.end(), tn.begin(), tn.end());
+                    xb.insert(xb.end(), qv.begin(), qv.end());
+                }
+            if (idx.empty()) continue;
+            const Lanes all = A.mul(xa, xb);
+            for (size_t j = 0; j < idx.size(); ++j) {
+                Node& nd = nodes[idx[j]];
+                const Lanes p(all.begin() + j * nl, all.begin() + (j + 1) * nl);
+                nd.val = A.ilin({{&p, 1}, {&nodes[nd.r].val, 1}}, 0.0, nd.level);
+            }
+        }
+        return nodes[root].val;
     }
 };
 
