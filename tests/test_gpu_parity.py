@@ -30,7 +30,7 @@ def test_ntt_roundtrip_and_parity(logN):
     assert np.array_equal(from_dev(d), x)
 
 
-@pytest.mark.parametrize("logN", [12, 16])
+@pytest.mark.parametrize("logN", [10, 12, 15, 16])
 def test_every_ntt_variant_bitexact(logN):
     """Every autotuner variant (occupancy, twiddle fetch, lazy or approximate
     quotient butterflies) gives the oracle's residues, forward and inverse,
@@ -181,6 +181,29 @@ def test_every_conversion_variant_bitexact():
             got = cc.EvalRotate(A, 3).download()
             want = oc.rotate(level, a0, a1, pow(g, -1, 2 * oc.N), *rk)
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (acc, level)
+    assert lib.fides_set_conv_accumulator(cc._h, -1) == 0
+    assert lib.fides_tensor_conv_status() == 0
+
+
+@pytest.mark.parametrize("variant", [3, 4])
+def test_tensor_conversion_every_level(variant):
+    """The tensor-core conversions at every level of a small context (digits
+    of 1 to 3 moduli, ModDown with and without the fused rescale, level 0
+    included)."""
+    from pyfideslib_b200._capi import lib
+
+    cc, oc = make_pair(12, 8, 3, 3)
+    kb, ka = rand_key(oc, 70 + variant)
+    cc.upload_relin_key(kb, ka)
+    assert lib.fides_set_conv_accumulator(cc._h, variant) == 0
+    for level in range(0, 8):
+        a0, a1 = rand_ct(oc, level, 90 + level)
+        b0, b1 = rand_ct(oc, level, 95 + level)
+        A, B = cc.upload(a0, a1), cc.upload(b0, b1)
+        for rs in ([False, True] if level > 0 else [False]):
+            got = cc.EvalMult(A, B, rescale=rs).download()
+            want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=rs)
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (level, rs)
     assert lib.fides_set_conv_accumulator(cc._h, -1) == 0
     assert lib.fides_tensor_conv_status() == 0
 
