@@ -1,9 +1,11 @@
-// conv_tc.cu -- ModUp base conversion on the 5th-generation tensor cores.
+// conv_tc.cu -- ModUp and ModDown base conversions on the 5th-generation
+// tensor cores.
 //
-// Role in the reference: DecompAndModUpConv (src/CKKS/Conv.cu), the same
-// contraction as k_modup_conv in ks.cu:
-//   out[m][j] = sum_i x_i[j] * M[i][m]  (mod p_m),  M[i][m] = (Q'/q_i) mod p_m,
-// over the cnt limbs i of one digit and the ntar target primes m.
+// Role in the reference: DecompAndModUpConv and ModDown2 (src/CKKS/Conv.cu),
+// the same contractions as k_modup_conv / k_moddown_conv in ks.cu:
+//   out[m][j] = sum_i x_i[j] * M[i][m]  (mod p_m),
+// with M[i][m] = (Q'/q_i) mod p_m over the cnt limbs i of one digit (ModUp),
+// or (P/p_k) mod q_m over the K special limbs (ModDown), for ntar targets m.
 //
 // Exact int8 split (this file's own design): with x_i = sum_a x_{i,a} 2^{8a}
 // (bytes) and the pre-shifted constants M'_{i,m,a} = M[i][m] 2^{8a} mod p_m
@@ -26,9 +28,10 @@
 // Operands sit in shared memory in the canonical K-major layout without
 // swizzle: core matrices of 8 rows x 16 bytes stored contiguously, 8-row
 // groups 128 bytes apart (SBO) and 16-byte K chunks LBO bytes apart.  A is
-// rebuilt per tile from coalesced limb loads; B is built once per CTA.  Every
-// wait on the MMA completion barrier is bounded; a timeout sets an error flag
-// and the CTA releases its tensor memory and returns.
+// rebuilt per tile from coalesced limb loads; every B (per level and digit,
+// per level for ModDown) is built once per context and copied in by each
+// CTA.  Every wait on the MMA completion barrier is bounded; a timeout sets an
+// error flag and the CTA releases its tensor memory and returns.
 #include <algorithm>
 #include <mutex>
 #include <vector>
