@@ -72,8 +72,10 @@ __device__ __forceinline__ uint64_t mulhi64_approx(uint64_t a, uint64_t b) {
 // the shift rounds the exact product).  Starting from residues below p,
 // alternating plain stages with stages that first centre X (x - rint(x/p) p,
 // |.| <= p/2 + 1) keeps every value below 1.7p < 2^51, so the bounds above
-// hold at every stage and all sums are exact.  The pass ends with a floor
-// reduction against 1/p rounded up, which is exact for values in (-2p, 2p).
+// hold at every stage and all sums are exact.  The column pass hands these
+// doubles to the row pass as they are; the row pass centres on the other
+// stage parity (MODE 6) and ends with a floor reduction against 1/p rounded
+// up, which is exact for values in (-2p, 2p).
 // forward butterfly on doubles; RED centres X first
 template <bool RED>
 __device__ __forceinline__ void ct_bfly_fp(uint64_t& X, uint64_t& Y, const ulonglong2 w, const double p,
@@ -148,11 +150,17 @@ __device__ __forceinline__ void load_stage_tw(ulonglong2 (&w)[15], Tab tab, int 
 // higher occupancy).  The autotuner picks per context.
 // p and two_p carry the prime's constants for the butterfly mode: (p, 2p) for
 // the integer modes, the bit patterns of the doubles (p, 1/p rounded up) for
-// MODE 4.  POS counts the stages of the group (MODE 4 centres X on odd ones).
+// MODEs 4 to 6.  POS counts the stages of the group: MODE 4 (column pass, fed
+// residues below p) centres X on odd ones and leaves values below 1.7p;
+// MODE 6 (row pass, fed those doubles unconverted) centres X on even ones,
+// so that its first stage already brings X down to p/2 and every value stays
+// below 1.7p < 2^51.
 template <int MODE, int POS>
 __device__ __forceinline__ void bfly(uint64_t& X, uint64_t& Y, const ulonglong2 w, uint64_t p, uint64_t two_p) {
     if constexpr (MODE == 4)
         ct_bfly_fp<(POS & 1) != 0>(X, Y, w, as_f64(p), as_f64(two_p));
+    else if constexpr (MODE == 6)
+        ct_bfly_fp<(POS & 1) == 0>(X, Y, w, as_f64(p), as_f64(two_p));
     else if constexpr (MODE == 5)
         gs_bfly_fp(X, Y, w, as_f64(p), as_f64(two_p));
     else if constexpr (MODE != 2)
@@ -189,8 +197,8 @@ __device__ __forceinline__ void load_group_tw(ulonglong2 (&w)[15], Tab tab, int 
 }
 
 // MODE: 0 forward, 1 forward without the per-butterfly reduction, 2 inverse,
-// 3 forward lazy with the approximate Shoup quotient, 4 forward on doubles,
-// 5 inverse on doubles
+// 3 forward lazy with the approximate Shoup quotient, 4 forward on doubles
+// (column pass), 5 inverse on doubles, 6 forward on doubles (row pass)
 template <int KB_FIRST, int KB_LAST, bool PF, int MODE, class Tab>
 __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi, uint64_t p,
                                           uint64_t two_p) {
@@ -200,13 +208,14 @@ __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_k
     run_stages<KB_FIRST, KB_LAST, STEP, PF, MODE, 0>(x, w, tab, t_of_kb0, B, th_hi, p, two_p);
 }
 
-// Forward group in the mode of this limb's prime (uniform per CTA).
-template <int KF, int KL, bool PF, bool AQ, bool FP, class Tab>
+// Forward group in the mode of this limb's prime (uniform per CTA); ROWS
+// selects the row pass's centring schedule for the double-precision mode.
+template <int KF, int KL, bool PF, bool AQ, bool FP, bool ROWS, class Tab>
 __device__ __forceinline__ void fwd_group(int fmode, uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi,
                                           uint64_t p, uint64_t two_p) {
     if constexpr (FP) {
         if (fmode == 4) {
-            run_group<KF, KL, PF, 4>(x, tab, t_of_kb0, B, th_hi, p, two_p);
+            run_group<KF, KL, PF, ROWS ? 6 : 4>(x, tab, t_of_kb0, B, th_hi, p, two_p);
             return;
         }
     }
@@ -308,7 +317,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
         for (int k = 0; k < 16; ++k) x[k] = fp_from_u(x[k]);
     }
     // stages 0..3: r = th + (k << (LR - 4)), twiddle (1 << t) + (k >> (4 - t))
-    fwd_group<3, 0, PF, AQ, FP>(fmode, x, tab, 3, 1, 0, kk.k0, kk.k1);
+    fwd_group<3, 0, PF, AQ, FP, false>(fmode, x, tab, 3, 1, 0, kk.k0, kk.k1);
     if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) sm[(th + (k << (LR - 4))) * TC + c] = x[k];
@@ -316,12 +325,10 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = sm[((th << 4) + k) * TC + c];
         // stages 4..LR-1: r = 16 th + k
-        fwd_group<LR - 5, 0, PF, AQ, FP>(fmode, x, tab, LR - 1, 1, th, kk.k0, kk.k1);
+        fwd_group<LR - 5, 0, PF, AQ, FP, false>(fmode, x, tab, LR - 1, 1, th, kk.k0, kk.k1);
     }
-    if (FP && fmode == 4) {
-#pragma unroll
-        for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
-    }
+    // double-precision limbs leave as doubles below 1.7p; the row pass
+    // continues on them without converting
     if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) lr.out[(size_t)((th << 4) + k) * C + col] = x[k];
@@ -387,11 +394,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
     uint64_t x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
-    if (FP && fmode == 4) {
-#pragma unroll
-        for (int k = 0; k < 16; ++k) x[k] = fp_from_u(x[k]);
-    }
-    fwd_group<3, 0, PF, AQ, FP>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+    fwd_group<3, 0, PF, AQ, FP, true>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
 #pragma unroll
@@ -399,7 +402,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        fwd_group<LC - 5, 0, PF, AQ, FP>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
+        fwd_group<LC - 5, 0, PF, AQ, FP, true>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
         if (FP && fmode == 4) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
@@ -502,10 +505,8 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = srow[padi(th + (k << (LC - 4)))];
     inv_group<0, 3, PF, FP>(imode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
-    if (FP && imode == 5) {
-#pragma unroll
-        for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
-    }
+    // double-precision limbs leave as doubles below 0.6p in magnitude; the
+    // column pass continues on them without converting
     uint64_t* dst = lr.out + (size_t)row * C;
 #pragma unroll
     for (int k = 0; k < 16; ++k) dst[th + (k << (LC - 4))] = x[k];
@@ -547,10 +548,6 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
     if constexpr (LR > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = lr.out[(size_t)((th << 4) + k) * C + col];
-        if (FP && imode == 5) {
-#pragma unroll
-            for (int k = 0; k < 16; ++k) x[k] = fp_from_u(x[k]);
-        }
         __syncthreads();
         inv_group<0, LR - 5, PF, FP>(imode, x, tab, LR - 1, 1, th, kk.k0, kk.k1);
 #pragma unroll
@@ -561,10 +558,6 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
     } else {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = lr.out[(size_t)(th + k) * C + col];
-        if (FP && imode == 5) {
-#pragma unroll
-            for (int k = 0; k < 16; ++k) x[k] = fp_from_u(x[k]);
-        }
         __syncthreads();
     }
     inv_group<0, 2, PF, FP>(imode, x, tab, 3, 1, 0, kk.k0, kk.k1);

@@ -94,10 +94,12 @@ static uint64_t splitmix(uint64_t* s) {
     return z ^ (z >> 31);
 }
 
-/* Forward transform with the kernels' schedule: stage s (0..15) centres X
- * first when s % 4 is odd, each pass of 8 stages ends with fp_to_u; then the
- * inverse (Gentleman-Sande, sum centred every stage, N^-1 folded into the
- * last stage).  psi: primitive 2N-th root mod p < 2^50.  pattern 0: random
+/* Forward transform with the kernels' schedule: the column pass (stages
+ * 0..7) centres X first when s % 4 is odd, the row pass (stages 8..15) when
+ * s % 4 is even (its inputs are the column pass's doubles, below 1.7p), and
+ * only the row pass ends with fp_to_u; then the inverse (Gentleman-Sande, sum
+ * centred every stage, N^-1 folded into the last stage, doubles passed
+ * between its two passes).  psi: primitive 2N-th root mod p < 2^50.  pattern 0: random
  * residues, 1: p - 1 everywhere, 2: alternating 0 / p - 1.  Returns the number
  * of coefficients that differ from exact arithmetic (forward) plus those
  * that do not come back (inverse), or -1 if a value left its proven range. */
@@ -140,7 +142,7 @@ int emu_ntt_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
     for (int j = 0; j < N; ++j) d[j] = (double)a[j];
     int st = 0;
     for (int m = 1, t = N / 2; m < N; m <<= 1, t >>= 1, ++st) {
-        const int red = (st % 4) & 1;
+        const int red = st < 8 ? (st % 4) & 1 : !((st % 4) & 1);
         for (int i = 0; i < m; ++i)
             for (int j = 2 * i * t; j < 2 * i * t + t; ++j) {
                 double x = d[j];
@@ -151,7 +153,7 @@ int emu_ntt_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
                 d[j] = x + tt;
                 d[j + t] = x - tt;
             }
-        if (st == 7 || st == 15)
+        if (st == 15)
             for (int j = 0; j < N; ++j) d[j] = (double)fp_to_u(d[j], pd, pinv);
     }
     if (bad < 0) goto done;
@@ -162,8 +164,6 @@ int emu_ntt_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
         for (int j = 0; j < N; ++j) d[j] = (double)e[j];
         int stg = 0;
         for (int m = N / 2, t = 1; m > 1; m >>= 1, t <<= 1, ++stg) {
-            if (stg == 8)
-                for (int j = 0; j < N; ++j) d[j] = (double)fp_to_u(d[j], pd, pinv);
             for (int i = 0; i < m; ++i)
                 for (int j = 2 * i * t; j < 2 * i * t + t; ++j) {
                     const double x = d[j], y = d[j + t];

@@ -5,8 +5,9 @@ because of value bounds (fp64.cuh, ntt.cu, conv_tc.cu).  These tests restate
 the device arithmetic on the host and run it against exact integer
 arithmetic on the cases the bounds are tight for:
 
-* the double-precision NTT with the kernels' stage schedule (centring on odd
-  stages, floor reductions at pass ends; inverse with centred sums) on primes
+* the double-precision NTT with the kernels' stage schedule (column pass
+  centring on odd stages, row pass on even ones, doubles passed between the
+  passes, one floor reduction at the end; inverse with centred sums) on primes
   just below 2^50, random residues, p-1 everywhere and alternating 0/p-1
   (tests/exact_arith_emu.c, C99 fma);
 * the FP64 key-switch sums of up to 8 digit products, including maximal
