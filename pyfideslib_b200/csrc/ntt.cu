@@ -127,6 +127,8 @@ __device__ __forceinline__ uint64_t reduce_fwd(uint64_t v, const PrimeConst& c) 
     return csub(reduce64_lazy(v, c), c.p);
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ ulonglong2 ldg2(const uint64_t* base, size_t idx) {
     return __ldg(reinterpret_cast<const ulonglong2*>(base) + idx);
 }
@@ -394,6 +396,18 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
     uint64_t x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
+    if (lr.smode != FS_PLAIN && lr.in2 && gridDim.y > 1) {
+        // the epilogue's operands for this tile (one 128-byte line per thread
+        // and operand): start their HBM reads now, under the butterflies.
+        // Batched launches only: a single element's grid is about two waves,
+        // where the early reads only compete with the row loads (measured
+        // 1.5% slower per operation, 0.5% faster batched)
+        const size_t tile = (size_t)blockIdx.x * TR * C;
+        for (int i = threadIdx.x * 16; i < TR * C; i += NT * 16) {
+            prefetch_l2(lr.in2 + tile + i);
+            if (lr.in3) prefetch_l2(lr.in3 + tile + i);
+        }
+    }
     fwd_group<3, 0, PF, AQ, FP, true>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
