@@ -447,6 +447,9 @@ def run_ours(args):
     if args.conv_variant >= 0:
         lib.fides_set_conv_accumulator(cc._h, args.conv_variant)
         autotune["forced_conv_variant"] = args.conv_variant
+    if args.ks_variant >= 0:
+        lib.fides_set_keyswitch_variant(cc._h, args.ks_variant)
+        autotune["forced_keyswitch_variant"] = args.ks_variant
     stream_ptr = C.c_void_p()
     lib.fides_ctx_stream(cc._h, C.byref(stream_ptr))
     st = torch.cuda.ExternalStream(stream_ptr.value, device=local)
@@ -670,6 +673,8 @@ def main():
     ap.add_argument("--no-boot", action="store_true", help="skip the bootstrap measurement")
     ap.add_argument("--ntt-variant", type=int, default=-1, help="force a forward NTT variant (default: tuned)")
     ap.add_argument("--conv-variant", type=int, default=-1, help="force a base-conversion variant (default: tuned)")
+    ap.add_argument("--ks-variant", type=int, default=-1,
+                    help="force the key-switch inner-product arithmetic: 0 integer, 1 FP64 (default: the context's)")
     ap.add_argument("--profile-roofline", action="store_true",
                     help="mark the roofline NTT loop for ncu --profile-from-start off")
     args = ap.parse_args()
