@@ -30,7 +30,7 @@ def test_ntt_roundtrip_and_parity(logN):
     assert np.array_equal(from_dev(d), x)
 
 
-@pytest.mark.parametrize("logN", [10, 12, 15, 16])
+@pytest.mark.parametrize("logN", [10, 12, 13, 14, 15, 16])
 def test_every_ntt_variant_bitexact(logN):
     """Every autotuner variant (occupancy, twiddle fetch, lazy or approximate
     quotient butterflies) gives the oracle's residues, forward and inverse,
