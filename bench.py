@@ -404,6 +404,25 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def max_over_ranks(ms, pg, device="cuda"):
+    """The job's time for one timed region: the slowest rank's (an all-reduce
+    MAX over the process group; the identity on one rank)."""
+    if pg is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank, world, ms):
+    """Whole-job throughput: the units every rank processed over the job's
+    (max-over-ranks) time in ms.  Ranks are independent replicas with the
+    same per-rank work, so the job processes world x units_per_rank."""
+    return units_per_rank * world / (ms * 1e-3)
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -533,11 +552,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         launches = lib.fides_kernel_launches() - n0
-        if pg:
-            t = torch.tensor([ms], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms, launches
+        return max_over_ranks(ms, pg), launches
 
     with ClockSampler(local) as clk:
         ms, launches = timed(step_batched, args.steps, args.warmup)
@@ -614,11 +629,10 @@ def run_ours(args):
                                           boot_inputs=boot_cts)}
     if not args.no_c3:
         c3 = measure_c3()
-    total = B * args.steps * world
-    value = total / (ms * 1e-3)
-    per_op_value = B * max(1, args.steps // 2) * world / (ms_op * 1e-3)
+    value = job_throughput(B * args.steps, world, ms)
+    per_op_value = job_throughput(B * max(1, args.steps // 2), world, ms_op)
     e2e_steps = max(1, args.steps // 2)
-    e2e_val = B * e2e_steps * world / (ms_e2e * 1e-3)
+    e2e_val = job_throughput(B * e2e_steps, world, ms_e2e)
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
