@@ -41,8 +41,25 @@ __global__ void k_tensor(const __grid_constant__ DevCtx ctx, const __grid_consta
     const ulonglong2 y0 = *reinterpret_cast<const ulonglong2*>(args.b0[bi] + i);
     const ulonglong2 y1 = *reinterpret_cast<const ulonglong2*>(args.b1[bi] + i);
     ulonglong2 r0, r1, r2;
-    r0.x = mul_mod(x0.x, y0.x, pc);
-    r0.y = mul_mod(x0.y, y0.y, pc);
+    if (pc.p < kFpPrimeBound) {
+        // e0 and e2 on the FP64 pipes (fp64.cuh: each product reduced to
+        // |r| <= 0.875p, then the floor reduction, exact), e1 on the integer
+        // pipes: the 128-bit products alone keep the IMAD pipe busier than
+        // HBM at this kernel's bytes per coefficient
+        const double p = __ull2double_rn(pc.p), pinv = as_f64(pc.pinv_f64);
+        auto fmul = [&](uint64_t a, uint64_t b) {
+            return fp_to_u(fp_mulmod(as_f64(fp_from_u(a)), as_f64(fp_from_u(b)), p, pinv), p, pinv);
+        };
+        r0.x = fmul(x0.x, y0.x);
+        r0.y = fmul(x0.y, y0.y);
+        r2.x = fmul(x1.x, y1.x);
+        r2.y = fmul(x1.y, y1.y);
+    } else {
+        r0.x = mul_mod(x0.x, y0.x, pc);
+        r0.y = mul_mod(x0.y, y0.y, pc);
+        r2.x = mul_mod(x1.x, y1.x, pc);
+        r2.y = mul_mod(x1.y, y1.y, pc);
+    }
     {
         Acc128 s;
         s.mac(x0.x, y1.x);
@@ -53,8 +70,6 @@ __global__ void k_tensor(const __grid_constant__ DevCtx ctx, const __grid_consta
         t.mac(x1.y, y0.y);
         r1.y = t.reduce(pc);
     }
-    r2.x = mul_mod(x1.x, y1.x, pc);
-    r2.y = mul_mod(x1.y, y1.y, pc);
     *reinterpret_cast<ulonglong2*>(args.e0 + o) = r0;
     *reinterpret_cast<ulonglong2*>(args.e1 + o) = r1;
     *reinterpret_cast<ulonglong2*>(args.e2 + o) = r2;
