@@ -42,10 +42,10 @@ __global__ void k_tensor(const __grid_constant__ DevCtx ctx, const __grid_consta
     const ulonglong2 y1 = *reinterpret_cast<const ulonglong2*>(args.b1[bi] + i);
     ulonglong2 r0, r1, r2;
     if (pc.p < kFpPrimeBound) {
-        // e0 and e2 on the FP64 pipes (fp64.cuh: each product reduced to
-        // |r| <= 0.875p, then the floor reduction, exact), e1 on the integer
-        // pipes: the 128-bit products alone keep the IMAD pipe busier than
-        // HBM at this kernel's bytes per coefficient
+        // all three on the FP64 pipes (fp64.cuh: each product reduced to
+        // |r| <= 0.875p, e1's sum of two below 1.75p, then the floor
+        // reduction, exact for (-2p, 2p)): with 128-bit integer products the
+        // IMAD pipe, not HBM, bounds this kernel
         const double p = __ull2double_rn(pc.p), pinv = as_f64(pc.pinv_f64);
         auto fmul = [&](uint64_t a, uint64_t b) {
             return fp_to_u(fp_mulmod(as_f64(fp_from_u(a)), as_f64(fp_from_u(b)), p, pinv), p, pinv);
@@ -54,13 +54,18 @@ __global__ void k_tensor(const __grid_constant__ DevCtx ctx, const __grid_consta
         r0.y = fmul(x0.y, y0.y);
         r2.x = fmul(x1.x, y1.x);
         r2.y = fmul(x1.y, y1.y);
+        auto fsum = [&](uint64_t a, uint64_t b, uint64_t c, uint64_t d) {
+            const double s = __dadd_rn(fp_mulmod(as_f64(fp_from_u(a)), as_f64(fp_from_u(b)), p, pinv),
+                                       fp_mulmod(as_f64(fp_from_u(c)), as_f64(fp_from_u(d)), p, pinv));
+            return fp_to_u(s, p, pinv);
+        };
+        r1.x = fsum(x0.x, y1.x, x1.x, y0.x);
+        r1.y = fsum(x0.y, y1.y, x1.y, y0.y);
     } else {
         r0.x = mul_mod(x0.x, y0.x, pc);
         r0.y = mul_mod(x0.y, y0.y, pc);
         r2.x = mul_mod(x1.x, y1.x, pc);
         r2.y = mul_mod(x1.y, y1.y, pc);
-    }
-    {
         Acc128 s;
         s.mac(x0.x, y1.x);
         s.mac(x1.x, y0.x);
