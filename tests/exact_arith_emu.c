@@ -205,3 +205,23 @@ int emu_ks_check(uint64_t p, int nd, uint64_t seed, int trials, int extreme) {
     }
     return bad;
 }
+
+/* Tensor product (k_tensor, double-precision branch): one product (e0, e2)
+ * or the sum of two (e1) reduced by fp_mulmod and floor-reduced directly, no
+ * centring (|value| < 1.75p lies inside fp_to_u's exact range (-2p, 2p)),
+ * against exact arithmetic; extreme != 0 uses p - 1 and p - 2 operands.
+ * Returns the number of mismatches. */
+int emu_tensor_check(uint64_t p, uint64_t seed, int trials, int extreme) {
+    const double pd = (double)p, pinv = recip_up(p);
+    uint64_t s = seed;
+    int bad = 0;
+    for (int t = 0; t < trials; ++t) {
+        const uint64_t a0 = extreme ? p - 1 : splitmix(&s) % p, a1 = extreme ? p - 1 - (t & 1) : splitmix(&s) % p;
+        const uint64_t b0 = extreme ? p - 1 - (t >> 1 & 1) : splitmix(&s) % p, b1 = extreme ? p - 1 : splitmix(&s) % p;
+        const double e0 = fp_mulmod((double)a0, (double)b0, pd, pinv);
+        const double e1 = fp_mulmod((double)a0, (double)b1, pd, pinv) + fp_mulmod((double)a1, (double)b0, pd, pinv);
+        bad += fp_to_u(e0, pd, pinv) != (uint64_t)((u128)a0 * b0 % p);
+        bad += fp_to_u(e1, pd, pinv) != (uint64_t)(((u128)a0 * b1 + (u128)a1 * b0) % p);
+    }
+    return bad;
+}

@@ -11,7 +11,8 @@ arithmetic on the cases the bounds are tight for:
   just below 2^50, random residues, p-1 everywhere and alternating 0/p-1
   (tests/exact_arith_emu.c, C99 fma);
 * the FP64 key-switch sums of up to 8 digit products, including maximal
-  operands;
+  operands, and the tensor product's single products and sums of two
+  (floor-reduced without centring);
 * the int8-split conversion: byte layout of A and B in the canonical K-major
   shared-memory form, the matrix product of the tensor-core MMAs, the
   reassembly of V' and its one-correction Barrett step (numpy / Python ints).
@@ -76,6 +77,7 @@ def emu(tmp_path_factory):
     lib = ctypes.CDLL(out)
     lib.emu_ntt_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
     lib.emu_ks_check.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+    lib.emu_tensor_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
     return lib
 
 
@@ -94,6 +96,14 @@ def test_fp64_keyswitch_sums_exact(emu, p):
     for nd in range(1, 9):
         assert emu.emu_ks_check(p, nd, nd, 20000, 0) == 0, nd
         assert emu.emu_ks_check(p, nd, nd, 4, 1) == 0, nd
+
+
+@pytest.mark.parametrize("p", PRIMES_50)
+def test_fp64_tensor_products_exact(emu, p):
+    """e0 = a0 b0 and e1 = a0 b1 + a1 b0 as k_tensor forms them on the FP64
+    pipes: products reduced to |r| <= 0.875p, floor-reduced without centring."""
+    assert emu.emu_tensor_check(p, 7, 100000, 0) == 0
+    assert emu.emu_tensor_check(p, 7, 4, 1) == 0
 
 
 def _conv_tc_emulate(ck, cnt, ntar, bits, seed):
