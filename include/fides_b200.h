@@ -114,7 +114,8 @@ uint64_t fides_kernel_launches(void);
 /* ---- keys (replaces KeySwitchingKey::Initialize, src/CKKS/KeySwitchingKey.cu:20-35,
  *      and the GetEvalKeySwitchKey / GetRotationKeySwitchKey imports,
  *      RawCiphertext.cu:468-602) ---- */
-/* Relinearisation key: b, a are dnum*(L+K)*N words each (host memory). */
+/* Relinearisation key: b, a are dnum*(L+K)*N words each (host memory),
+ * canonical residues like every uploaded operand. */
 fides_status fides_key_upload_relin(fides_ctx* ctx, const uint64_t* b, const uint64_t* a);
 /* Rotation / conjugation key for the automorphism X -> X^galois (galois odd, < 2N). */
 fides_status fides_key_upload_galois(fides_ctx* ctx, uint32_t galois, const uint64_t* b, const uint64_t* a);
@@ -124,9 +125,13 @@ fides_status fides_key_upload_galois(fides_ctx* ctx, uint32_t galois, const uint
 uint32_t fides_rotation_galois(const fides_ctx* ctx, int32_t index, int slots);
 
 /* ---- ciphertexts (replaces Ciphertext::load / store, Ciphertext.cpp:270-309) ----
- * Uploads run on a copy stream beside the kernels already queued (the host
- * buffers must stay unchanged until fides_ctx_synchronize; pinned memory lets
- * the copy overlap); later operations on the ciphertext wait for them. */
+ * Residues are limb-major, (level+1)*N words per component, each one
+ * canonical (below its modulus), as OpenFHE's raw ciphertexts hold them; the
+ * exact double-precision kernels rely on that and the upload does not scan
+ * for it.  Uploads run on a copy stream beside the kernels already queued
+ * (the host buffers must stay unchanged until fides_ctx_synchronize; pinned
+ * memory lets the copy overlap); later operations on the ciphertext wait for
+ * them. */
 fides_status fides_ct_upload(fides_ctx* ctx, const uint64_t* c0, const uint64_t* c1, int level, double scale,
                              int noise_deg, int slots, fides_ct** out);
 fides_status fides_ct_download(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1);
