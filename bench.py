@@ -47,7 +47,7 @@ LOGN, L, K, DNUM = 16, 30, 10, 3
 # algorithmic bytes: the column pass writes the 960 intermediate limbs
 # (480 MB, more than L2) and the row pass reads them back; twiddles add 32 MB
 # (read once per prime for the whole batch).
-NTT_BATCH_TRAFFIC_BYTES = 1941.7e6
+NTT_BATCH_TRAFFIC_BYTES = 1930.1e6  # profiles/ntt_fwd_batch32x30_n16.md (503.5 + 443.6 + 534.8 + 448.2 MB)
 
 
 def peaks():
