@@ -102,9 +102,16 @@ fides_status fides_set_conv_accumulator(fides_ctx* ctx, int accumulator);
  * of primes below 2^50 exactly on the FP64 pipes, 0 uses 128-bit integer
  * sums everywhere (identical results; for measurements and tests). */
 fides_status fides_set_keyswitch_variant(fides_ctx* ctx, int variant);
-/* 1 once a tensor-core conversion gave up waiting for its matrix products
- * (bounded wait; its outputs are then invalid), else 0.  Process-wide. */
-int fides_tensor_conv_status(void);
+/* Device error word of this context, read after the work queued so far
+ * without clearing it: bit 0 is set once a tensor-core conversion gave up its
+ * bounded wait for its matrix products (its outputs are then invalid).  The
+ * next synchronising call (fides_ctx_synchronize, fides_ct_download, a
+ * serving completion) reports a set word as FIDES_TIMEOUT with a message and
+ * clears it.  No counterpart in the reference, whose kernels do not wait. */
+fides_status fides_ctx_device_status(fides_ctx* ctx, uint32_t* flags);
+/* Write `flags` into the device error word from the host (ordered after the
+ * queued work): exercises the reporting path without any kernel failing. */
+fides_status fides_ctx_inject_device_error(fides_ctx* ctx, uint32_t flags);
 /* Force forward NTT variant `variant` with its paired inverse configuration
  * (for measurements and tests); -1 restores the tuned choices. */
 fides_status fides_set_ntt_variant(fides_ctx* ctx, int variant);
@@ -309,8 +316,8 @@ fides_status fides_polymul(fides_ctx* ctx, const uint64_t* a, const uint64_t* b,
 
 /* Same product as fides_polymul, but allocating nothing and asking for no
  * scratch: for callers that cannot obtain device memory when they multiply
- * (inside CUDA stream capture, under a host allocator that owns the device,
- * in loops that must not call cudaMalloc/cudaFree).  No counterpart in the
+ * (hosts whose own allocator owns the whole device, loops that must not call
+ * cudaMalloc/cudaFree because those synchronise the device).  No counterpart in the
  * reference.  The scratch is a fixed 8 MiB device array inside the library
  * (2^19 words per operand): nlimbs * N must not exceed 2^19, larger calls
  * return FIDES_BAD_ARG.  The first call on a device looks the array up

@@ -113,6 +113,21 @@ def find_primes(logN, bits, count, upper=0):
     return [int(x) for x in out[:n]]
 
 
+def moduli(logN, L, K=0, dnum=3, q0_bits=60, qi_bits=50, p_bits=60):
+    """The (q, p) moduli of a context with these parameters, restated from the
+    reference's parameter rules: one q0_bits prime and L-1 qi_bits primes by
+    descending search for p = 1 mod 2N, then K special p_bits primes continuing
+    the search and skipping the q's; K = 0 derives it from the widest digit
+    (Parameters / computeK, src/CKKS/Context.cu:275-295)."""
+    q = find_primes(logN, q0_bits, 1) + find_primes(logN, qi_bits, L - 1)
+    if K <= 0:
+        alpha = (L + dnum - 1) // dnum
+        widest = max(sum(int(x).bit_length() for x in q[d * alpha:min(L, (d + 1) * alpha)]) for d in range(dnum))
+        K = (widest + p_bits - 2) // (p_bits - 1)
+    p = [x for x in find_primes(logN, p_bits, K + L + 2) if x not in q][:K]
+    return q, p
+
+
 def nega_fft2(a: np.ndarray, logN, p, psi, invert=False):
     a = np.ascontiguousarray(a, dtype=np.uint64).copy()
     lib().or_nega_fft2(_p(a), logN, p, psi, int(invert))

@@ -62,7 +62,8 @@ EXPORTS = {
     "fides_autotune": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_float), C.POINTER(C.c_int)], C.c_int),
     "fides_autotune_conv_info": ([vp, C.POINTER(C.c_int), C.POINTER(C.c_float)], C.c_int),
     "fides_set_conv_accumulator": ([vp, C.c_int], C.c_int),
-    "fides_tensor_conv_status": ([], C.c_int),
+    "fides_ctx_device_status": ([vp, C.POINTER(C.c_uint32)], C.c_int),
+    "fides_ctx_inject_device_error": ([vp, C.c_uint32], C.c_int),
     "fides_set_keyswitch_variant": ([vp, C.c_int], C.c_int),
     "fides_set_ntt_variant": ([vp, C.c_int], C.c_int),
     "fides_key_upload_relin": ([vp, u64p, u64p], C.c_int),

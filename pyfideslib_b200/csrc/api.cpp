@@ -118,7 +118,8 @@ fides_status fides_ctx_synchronize(fides_ctx* ctx) {
     if (cudaStreamSynchronize(ctx->st) != cudaSuccess || cudaStreamSynchronize(ctx->h2d) != cudaSuccess ||
         cudaStreamSynchronize(ctx->d2h) != cudaSuccess)
         return check_cuda(ctx, "synchronize");
-    return check_cuda(ctx, "synchronize");
+    const fides_status s = check_cuda(ctx, "synchronize");
+    return s != FIDES_OK ? s : consume_device_error(ctx);
 }
 
 const char* fides_ctx_last_error(const fides_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
@@ -259,7 +260,23 @@ fides_status fides_set_conv_accumulator(fides_ctx* c, int accumulator) {
     return FIDES_OK;
 }
 
-int fides_tensor_conv_status(void) { return conv_tc_error(); }
+fides_status fides_ctx_device_status(fides_ctx* ctx, uint32_t* flags) {
+    if (!ctx || !flags) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    *flags = read_device_error(ctx, nullptr, false);
+    return check_cuda(ctx, "device status");
+}
+
+fides_status fides_ctx_inject_device_error(fides_ctx* ctx, uint32_t flags) {
+    if (!ctx || !ctx->dev.err) return FIDES_BAD_ARG;
+    Guard g(ctx);
+    // a host-side write into the word, ordered after the work already queued:
+    // exercises the reporting path without any kernel failing
+    const uint32_t w = flags;
+    cudaMemcpyAsync(ctx->dev.err, &w, sizeof(w), cudaMemcpyHostToDevice, ctx->st);
+    cudaStreamSynchronize(ctx->st);
+    return check_cuda(ctx, "inject device error");
+}
 
 fides_status fides_set_keyswitch_variant(fides_ctx* c, int variant) {
     if (!c || variant < 0 || variant > 1) return FIDES_BAD_ARG;
@@ -357,7 +374,8 @@ fides_status fides_ct_download(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0,
     if (c0) cudaMemcpyAsync(c0, ct->c0(), bytes, cudaMemcpyDeviceToHost, ctx->st);
     if (c1) cudaMemcpyAsync(c1, ct->c1(ctx->N), bytes, cudaMemcpyDeviceToHost, ctx->st);
     cudaStreamSynchronize(ctx->st);
-    return check_cuda(ctx, "ct download");
+    const fides_status s = check_cuda(ctx, "ct download");
+    return s != FIDES_OK ? s : consume_device_error(ctx);
 }
 
 fides_status fides_ct_download_async(fides_ctx* ctx, const fides_ct* ct, uint64_t* c0, uint64_t* c1) {

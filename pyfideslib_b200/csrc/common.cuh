@@ -12,6 +12,11 @@ constexpr int kMaxPrimes = 128;
 constexpr int kMaxSeg = 8;
 constexpr int kMaxBatch = 32;  // ciphertexts per batched launch (blockIdx.z)
 
+// Bits of a context's device error word (DevCtx::err).  A kernel whose
+// bounded wait gives up sets its bit and leaves invalid outputs; the next
+// synchronising call of the context reports FIDES_TIMEOUT and clears the word.
+constexpr uint32_t kDevErrTensorWait = 1u;  // a tensor-core conversion stopped waiting for its MMAs
+
 // Read-only view of the context tables in HBM, passed by value to kernels.
 // Index conventions: prime ids 0..L-1 are the Q primes, L..L+K-1 the special
 // primes.  Every table entry with a Shoup companion stores (value, companion)
@@ -42,6 +47,7 @@ struct DevCtx {
     const uint64_t* rs_qinv;     // [L][L][2]    q_l^-1 mod q_j (row l, column j < l)
     const uint8_t* tc_btab;      // tensor-core conversions: byte matrices B per (level, digit) and
     const uint64_t* tc_boff;     //   per (level, fused) for ModDown, and their byte offsets (or null)
+    uint32_t* err;               // the context's device error word (kDevErr* bits)
 };
 
 // A launch covers up to kMaxSeg segments of contiguous limbs.  Within a

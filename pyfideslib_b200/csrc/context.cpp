@@ -182,6 +182,30 @@ fides_status check_cuda(fides_ctx* c, const char* where) {
     return FIDES_OK;
 }
 
+uint32_t read_device_error(fides_ctx* c, cudaStream_t st, bool clear) {
+    if (!c->dev.err) return 0;
+    if (!st) st = c->st;
+    uint32_t w = 0;
+    if (cudaMemcpyAsync(&w, c->dev.err, sizeof(w), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return 0;  // the CUDA error itself is reported by check_cuda
+    if (w && clear) {
+        cudaMemsetAsync(c->dev.err, 0, sizeof(uint32_t), st);
+        cudaStreamSynchronize(st);
+    }
+    return w;
+}
+
+fides_status consume_device_error(fides_ctx* c, cudaStream_t st) {
+    const uint32_t w = read_device_error(c, st, true);
+    if (w & kDevErrTensorWait)
+        return set_err(c, FIDES_TIMEOUT,
+                       "a tensor-core base conversion stopped waiting for its matrix products: results computed "
+                       "since the previous synchronising call are invalid");
+    if (w) return set_err(c, FIDES_TIMEOUT, "device error word " + std::to_string(w));
+    return FIDES_OK;
+}
+
 LimbMap map_single(const uint64_t* in, uint64_t* out, int count, int nq, int q0, int level, const uint64_t* in2,
                    const uint64_t* in3) {
     LimbMap m{};
@@ -437,6 +461,8 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     size_t i_dp = add(md_pinv.data(), md_pinv.size() * 8);
     size_t i_dq = add(md_pmod.data(), md_pmod.size() * 8);
     size_t i_rq = add(rs_qinv.data(), rs_qinv.size() * 8);
+    const uint64_t zero_word = 0;
+    size_t i_err = add(&zero_word, sizeof(zero_word));
     c->table_bytes = off;
     if (cudaMalloc(&c->table_mem, off) != cudaSuccess) return set_err(c, FIDES_OOM, "table allocation failed");
     char* base = (char*)c->table_mem;
@@ -465,6 +491,7 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.md_pinv = (const uint64_t*)(base + parts[i_dp].off);
     d.md_pmod = (const uint64_t*)(base + parts[i_dq].off);
     d.rs_qinv = (const uint64_t*)(base + parts[i_rq].off);
+    d.err = (uint32_t*)(base + parts[i_err].off);
     d.tc_btab = nullptr;
     d.tc_boff = nullptr;
     if (conv_tc_eligible(d)) {

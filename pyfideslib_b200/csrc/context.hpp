@@ -127,6 +127,11 @@ namespace fides {
 // helpers shared by api.cpp / client.cpp
 fides_status set_err(fides_ctx* c, fides_status s, const std::string& msg);
 fides_status check_cuda(fides_ctx* c, const char* where);
+// The context's device error word (kDevErr* bits), read after the work queued
+// on `st` (default: the context stream); cleared when `clear`.
+uint32_t read_device_error(fides_ctx* c, cudaStream_t st = nullptr, bool clear = false);
+// FIDES_TIMEOUT with a message when the word is set (and clears it), else OK.
+fides_status consume_device_error(fides_ctx* c, cudaStream_t st = nullptr);
 // Canonical-embedding encode of `slots` complex values (interleaved re, im)
 // at `scale` into level+1 evaluation limbs at dm (device), on the context stream.
 fides_status encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm);

@@ -48,8 +48,6 @@ constexpr int kTcCols = 8;          // accumulator columns per target (byte posi
 constexpr uint32_t kTcLboA = (kTcRows / 8) * 128;  // A: K-chunk stride in bytes
 constexpr uint32_t kSpinLimit = 1u << 20;
 
-__device__ int g_tc_error;
-
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // shared-memory matrix descriptor (canonical K-major, no swizzle)
@@ -419,7 +417,9 @@ __global__ void __launch_bounds__(kTcThreads, CHUNK == 16 ? 3 : 2)
             }
         }
     }
-    if (!ok && threadIdx.x == 0) atomicExch(&g_tc_error, 1);
+    // a gave-up wait invalidates this launch's outputs: flagged in the
+    // context's error word, which the next synchronising call reports
+    if (!ok && threadIdx.x == 0 && ctx.err) atomicOr(ctx.err, kDevErrTensorWait);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -533,12 +533,6 @@ void conv_tc_build_tables(const DevCtx& ctx, cudaStream_t st) {
         default: k_conv_tc_table<4, true><<<gd, 256, 0, st>>>(ctx, tab, ctx.tc_boff); break;
     }
     count_launches(2);
-}
-
-int conv_tc_error() {
-    int e = 0;
-    cudaMemcpyFromSymbol(&e, g_tc_error, sizeof(int));
-    return e;
 }
 
 void launch_modup_conv_tc(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,

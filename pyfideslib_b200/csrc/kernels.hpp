@@ -87,7 +87,6 @@ void conv_tc_build_tables(const DevCtx& ctx, cudaStream_t st);
 void launch_modup_conv_tc(const DevCtx& ctx, int level, int nb, const uint64_t* xt, uint64_t* dig, size_t dig_stride,
                           size_t bstride, cudaStream_t st, int chunk);
 void launch_moddown_conv_tc(const DevCtx& ctx, int level, int nb, const MdArgs& md, cudaStream_t st, int chunk);
-int conv_tc_error();  // 1 once a tensor-core conversion timed out waiting for its MMAs
 // override every segment's prologue / epilogue mode (-1 keeps the segment's own)
 void set_modes(LimbMap& map, int lmode, int smode);
 

@@ -3,8 +3,6 @@
 // fides_polymul needs two scratch buffers for the forward transforms of its
 // operands and asks the caller for them.  Some callers cannot obtain device
 // memory at the point where they multiply:
-//   * code that runs while a CUDA stream is being captured into a graph, where
-//     cudaMalloc is not permitted;
 //   * hosts that hand the whole device to their own allocator at start-up and
 //     forbid later allocations (fixed-budget serving processes);
 //   * latency-critical loops that must not call cudaMalloc / cudaFree, which

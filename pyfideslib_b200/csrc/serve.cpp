@@ -139,8 +139,12 @@ void launch_batch(fides_server* s, Lane& ln) {
 
 void finish_lane(fides_server* s, Lane& ln, clk::time_point now, cudaError_t q) {
     const cudaError_t e = cudaGetLastError();
+    // a kernel that gave up a bounded wait flags the context's error word:
+    // the batch that completes next fails with FIDES_TIMEOUT
+    const uint32_t dev_err = (e == cudaSuccess && q == cudaSuccess) ? read_device_error(s->c, ln.st, true) : 0;
     for (Request* r : ln.batch) {
         if (e != cudaSuccess || q != cudaSuccess) r->status = FIDES_CUDA_ERR;
+        else if (dev_err && r->status == FIDES_OK) r->status = FIDES_TIMEOUT;
         const fides_ct* a = r->a;
         if (r->status != FIDES_OK || r->op == FIDES_OP_BOOTSTRAP) {
             // failed, or metadata set by fides_bootstrap

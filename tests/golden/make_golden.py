@@ -1,8 +1,8 @@
 """Extract the known-answer data FIDESlib's own test suite holds for this path
 into tests/golden/reference_vectors.json.
 
-Run in a container where the reference tree is mounted (default path below, or
-pass it as argv[1]).  Sources read (as text, nothing is executed):
+Usage: python make_golden.py <path of the reference source tree>.  Sources
+read (as text, nothing is executed):
   test/ParametrizedTest.cuh:42-76   prime lists p64 / sp64 (NTT-friendly for logN <= 16)
   test/MathTest.cu:14-39            modpow / modinv known answers
   test/NegacyclicNTTtests.cu:25-125 N=8, p=17 negacyclic convolution vectors
@@ -14,7 +14,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python make_golden.py <path of the reference source tree>")
+REF = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
 
 

@@ -43,3 +43,14 @@ def to_dev(arr):
 
 def from_dev(t):
     return t.cpu().numpy().view(np.uint64)
+
+
+def device_status(cc):
+    """The context's device error word (0 when no kernel gave up a wait)."""
+    import ctypes as C
+
+    from pyfideslib_b200._capi import lib
+
+    w = C.c_uint32()
+    assert lib.fides_ctx_device_status(cc._h, C.byref(w)) == 0
+    return w.value

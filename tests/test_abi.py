@@ -119,3 +119,30 @@ def test_generated_moduli_match_oracle_search():
         assert O.is_prime(x) and (x - 1) % (1 << 17) == 0
     q2, p2 = generated_moduli(16, 30, 0, 3)  # K derived from the widest digit
     assert len(p2) == 9
+
+
+@pytest.mark.parametrize("args", [dict(logN=16, L=30, K=10), dict(logN=16, L=20, K=0, qi_bits=40),
+                                  dict(logN=12, L=8, K=3), dict(logN=16, L=30, K=0)])
+def test_oracle_moduli_match_library(args):
+    """The oracle's restated parameter rule gives the library's moduli, so the
+    CPU reference arm of bench.py needs no product code to build its context."""
+    from oracle import oracle as O
+    from pyfideslib_b200.host_params import generated_moduli
+
+    q, p = O.moduli(args["logN"], args["L"], args["K"], 3, qi_bits=args.get("qi_bits", 50))
+    gq, gp = generated_moduli(args["logN"], args["L"], args["K"], 3, qi_bits=args.get("qi_bits", 50))
+    assert (q, p) == (gq, gp)
+
+
+def test_reference_arm_loads_no_product_code():
+    """bench.py --impl reference maps only oracle/ libraries (checked in a
+    child process on a tiny run: the import graph, not the timing)."""
+    code = ("import sys, runpy; sys.argv=['bench.py','--impl','reference','--steps','1','--warmup','0','--batch','1'];"
+            "import bench; bench.LOGN=12; bench.L=6; bench.K=2;"
+            "bench.run_reference(bench.argparse.Namespace(steps=1, warmup=0, batch=1, gpus=1));"
+            "maps=open('/proc/self/maps').read(); print('LOADED' if 'libfidesb200' in maps else 'CLEAN');"
+            "print('MOD' if any(m.startswith('pyfideslib_b200') for m in sys.modules) else 'NOMOD')")
+    r = subprocess.run([os.environ.get("PYTHON", "python"), "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "CLEAN" in r.stdout and "NOMOD" in r.stdout, r.stdout

@@ -10,7 +10,7 @@ from pyfideslib_b200._capi import FidesError
 
 pytestmark = pytest.mark.gpu
 
-BAD_ARG, KEY_MISSING, UNSUPPORTED = 1, 4, 7
+BAD_ARG, KEY_MISSING, TIMEOUT, UNSUPPORTED = 1, 4, 5, 7
 
 
 @pytest.fixture(scope="module")
@@ -69,3 +69,40 @@ def test_bad_arguments(ctx):
     assert _status(lambda: srv.submit(F.Server.HMULT, ct, other)) == BAD_ARG  # levels differ
     assert _status(lambda: srv.submit(F.Server.BOOTSTRAP, ct)) == BAD_ARG  # not set up
     srv.close()
+
+
+def test_device_error_word_is_reported_once(ctx):
+    """A kernel that gives up a bounded wait sets the context's device error
+    word.  The word is set here from the host (no kernel fails): the next
+    synchronising call returns FIDES_TIMEOUT with a message, clears the word,
+    and the call after it is clean; downloads and serving completions report
+    it the same way."""
+    import ctypes as C
+
+    from pyfideslib_b200._capi import lib
+
+    cc, sk = ctx
+    cc.EvalMultKeyGen(sk)
+    w = C.c_uint32()
+    assert lib.fides_ctx_device_status(cc._h, C.byref(w)) == 0 and w.value == 0
+    assert lib.fides_ctx_inject_device_error(cc._h, 1) == 0
+    assert lib.fides_ctx_device_status(cc._h, C.byref(w)) == 0 and w.value == 1  # reading does not clear
+    assert lib.fides_ctx_synchronize(cc._h) == TIMEOUT
+    assert b"tensor-core" in lib.fides_ctx_last_error(cc._h)
+    assert lib.fides_ctx_synchronize(cc._h) == 0
+    assert lib.fides_ctx_device_status(cc._h, C.byref(w)) == 0 and w.value == 0
+    # a download reports it too, and the next download is clean
+    ct = cc.Encrypt(sk, np.ones(cc.N // 2))
+    assert lib.fides_ctx_inject_device_error(cc._h, 1) == 0
+    assert _status(lambda: ct.download()) == TIMEOUT
+    c0, c1 = ct.download()
+    assert c0.shape == (ct.level + 1, cc.N)
+    # a serving completion fails the batch that completes next, not later ones
+    srv = F.Server(cc, hbm_budget=4 << 30, max_batch=2, num_streams=1)
+    assert lib.fides_ctx_inject_device_error(cc._h, 1) == 0
+    rid, _ = srv.submit(F.Server.HMULT, ct, ct)
+    assert _status(lambda: srv.wait(rid, 60.0)) == TIMEOUT
+    rid, _ = srv.submit(F.Server.HMULT, ct, ct)
+    srv.wait(rid, 60.0)
+    srv.close()
+    assert lib.fides_ctx_synchronize(cc._h) == 0

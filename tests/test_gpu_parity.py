@@ -11,7 +11,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from gpu_helpers import from_dev, make_pair, rand_ct, rand_key, to_dev
+from gpu_helpers import device_status, from_dev, make_pair, rand_ct, rand_key, to_dev
 
 pytestmark = pytest.mark.gpu
 
@@ -182,7 +182,7 @@ def test_every_conversion_variant_bitexact():
             want = oc.rotate(level, a0, a1, pow(g, -1, 2 * oc.N), *rk)
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (acc, level)
     assert lib.fides_set_conv_accumulator(cc._h, -1) == 0
-    assert lib.fides_tensor_conv_status() == 0
+    assert device_status(cc) == 0
 
 
 @pytest.mark.parametrize("variant", [3, 4])
@@ -205,7 +205,7 @@ def test_tensor_conversion_every_level(variant):
             want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=rs)
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (level, rs)
     assert lib.fides_set_conv_accumulator(cc._h, -1) == 0
-    assert lib.fides_tensor_conv_status() == 0
+    assert device_status(cc) == 0
 
 
 @pytest.mark.parametrize("dnum,variant", [(3, 3), (3, 4), (2, 3)])
@@ -230,7 +230,7 @@ def test_tensor_conversion_c2_shape_bitexact(dnum, variant):
         want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=True)
         assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), level
     assert lib.fides_set_conv_accumulator(cc._h, -1) == 0
-    assert lib.fides_tensor_conv_status() == 0
+    assert device_status(cc) == 0
 
 
 @pytest.mark.parametrize("logN,L,K,dnum", [(12, 9, 3, 3), (16, 30, 10, 3)])

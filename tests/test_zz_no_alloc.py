@@ -1,7 +1,7 @@
 """fides_polymul_noalloc: the polynomial multiply for callers that cannot
-allocate device memory when they multiply (inside stream capture, under a
-host allocator that owns the device, in loops that must not hit
-cudaMalloc/cudaFree).  Its scratch is a fixed device array inside the
+allocate device memory when they multiply (hosts whose own allocator owns the
+whole device, loops that must not hit cudaMalloc/cudaFree, which synchronise
+the device).  Its scratch is a fixed device array inside the
 library, so its output must equal fides_polymul's, which takes caller
 scratch — bit for bit, on two calls in a row, and sizes beyond the fixed
 scratch must be refused.
