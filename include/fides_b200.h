@@ -163,6 +163,59 @@ fides_status fides_pt_upload(fides_ctx* ctx, const uint64_t* m, int level, doubl
                              fides_pt** out);
 fides_status fides_pt_free(fides_ctx* ctx, fides_pt* pt);
 
+/* ---- raw-residue interop: the shapes FIDESlib exchanges with OpenFHE,
+ *      RawCipherText / RawPlainText / RawKeySwitchKey
+ *      (src/CKKS/openfhe-interface/RawCiphertext.cuh:19-93), filled by
+ *      GetRawCipherText / GetRawPlainText / GetKeySwitchKey (RawCiphertext.cu:48-75,
+ *      172-220, 468-602) and loaded by Ciphertext / Plaintext / KeySwitchingKey
+ *      ::Initialize (KeySwitchingKey.cu:20-35).  One array of N words per limb,
+ *      with the limb's modulus beside it.  Imports check every residue is
+ *      canonical and every modulus belongs to the context. ---- */
+typedef enum { FIDES_FORMAT_EVALUATION = 0, FIDES_FORMAT_COEFFICIENT = 1 } fides_format;
+typedef struct {
+    uint64_t** sub_0;  /* numRes limbs of N words: component 0 */
+    uint64_t** sub_1;  /* numRes limbs of N words: component 1 */
+    uint64_t* moduli;  /* numRes moduli: limb i is mod q_i of the context */
+    int numRes;        /* limbs (level + 1); on export: capacity in, limbs out */
+    int N;
+    int format;        /* fides_format: EVALUATION is bit-reversed NTT order, as OpenFHE holds it */
+    double Noise;      /* scaling factor */
+    int NoiseLevel;    /* noise scale degree */
+    int slots;
+} fides_raw_ct;
+typedef struct {
+    uint64_t** sub_0;
+    uint64_t* moduli;
+    int numRes;
+    int N;
+    int format;
+    double Noise;
+    int NoiseLevel;
+    int slots;
+} fides_raw_pt;
+typedef struct {
+    /* r_key[(h * dnum + d) * nlimbs + i]: half h (0 = a, 1 = b, RawKeySwitchKey's
+     * order), digit d, limb i of N words; r_key_moduli the same indexing.  Each
+     * digit polynomial covers the L + K primes of the context once, in any order. */
+    uint64_t** r_key;
+    uint64_t* r_key_moduli;
+    int dnum;
+    int nlimbs;  /* L + K */
+    int N;
+} fides_raw_key;
+/* Device ciphertext from a RawCipherText (COEFFICIENT input is transformed on the device). */
+fides_status fides_ct_import_raw(fides_ctx* ctx, const fides_raw_ct* raw, fides_ct** out);
+/* RawCipherText of a device ciphertext into caller buffers (raw->numRes >= level + 1
+ * limb buffers per component; raw->format selects the output format). */
+fides_status fides_ct_export_raw(fides_ctx* ctx, const fides_ct* ct, fides_raw_ct* raw);
+/* Device plaintext from a RawPlainText (LoadPlaintext, api/CryptoContext.cpp:230-246). */
+fides_status fides_pt_import_raw(fides_ctx* ctx, const fides_raw_pt* raw, fides_pt** out);
+/* Switching key from a RawKeySwitchKey: galois 0 = relinearisation key, else the
+ * automorphism X -> X^galois (LoadContext's key loading, api/CryptoContext.cpp:199-213). */
+fides_status fides_key_import_raw(fides_ctx* ctx, uint32_t galois, const fides_raw_key* raw);
+/* RawKeySwitchKey of a resident key into caller buffers (limbs in context order). */
+fides_status fides_key_export_raw(fides_ctx* ctx, uint32_t galois, fides_raw_key* raw);
+
 /* ---- evaluation (api/CryptoContext.hpp:110-181 -> CKKS::Ciphertext, Ciphertext.cuh:34-500) ---- */
 /* EvalMult + relinearisation (+ Rescale when `rescale` != 0): Ciphertext::mult, Ciphertext.cpp:409-622 */
 fides_status fides_hmult(fides_ctx* ctx, const fides_ct* a, const fides_ct* b, fides_ct* out, int rescale);

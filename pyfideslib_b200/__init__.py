@@ -14,7 +14,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._capi import BootParams, FidesError, FidesParams, SrvStats, check, lib, u64p, vp
+from ._capi import BootParams, FidesError, FidesParams, RawCt, RawKey, RawPt, SrvStats, check, lib, u64p, vp
 
 __all__ = ["CryptoContext", "Ciphertext", "Plaintext", "PrivateKey", "Server", "Plan", "FidesError", "lib"]
 
@@ -206,6 +206,67 @@ class CryptoContext:
         check(lib.fides_ct_upload(self._h, _p(c0), _p(c1), lv, float(scale or self.scale), noise_deg,
                                   slots or self.N // 2, C.byref(h)), self._h)
         return Ciphertext(self, h.value)
+
+    # ---- raw-residue interop (RawCipherText / RawPlainText / RawKeySwitchKey) ----
+    FORMAT_EVALUATION, FORMAT_COEFFICIENT = 0, 1
+
+    @staticmethod
+    def _limb_ptrs(limbs):
+        return (u64p * len(limbs))(*[_p(x) for x in limbs])
+
+    def import_raw_ct(self, sub_0, sub_1, moduli, noise=None, noise_level=1, slots=None, fmt=0):
+        """Device ciphertext from RawCipherText-shaped data: lists of per-limb
+        uint64 arrays (N words each) and the limbs' moduli."""
+        sub_0 = [np.ascontiguousarray(x, dtype=np.uint64) for x in sub_0]
+        sub_1 = [np.ascontiguousarray(x, dtype=np.uint64) for x in sub_1]
+        mod = np.ascontiguousarray(moduli, dtype=np.uint64)
+        raw = RawCt(self._limb_ptrs(sub_0), self._limb_ptrs(sub_1), _p(mod), len(sub_0), self.N, fmt,
+                    float(noise or self.scale), noise_level, slots or self.N // 2)
+        h = vp()
+        check(lib.fides_ct_import_raw(self._h, C.byref(raw), C.byref(h)), self._h)
+        return Ciphertext(self, h.value)
+
+    def export_raw_ct(self, ct, fmt=0):
+        """RawCipherText-shaped copy of a device ciphertext:
+        (sub_0, sub_1, moduli, noise, noise_level, slots)."""
+        n = ct.level + 1
+        s0 = [np.empty(self.N, dtype=np.uint64) for _ in range(n)]
+        s1 = [np.empty(self.N, dtype=np.uint64) for _ in range(n)]
+        mod = np.zeros(n, dtype=np.uint64)
+        raw = RawCt(self._limb_ptrs(s0), self._limb_ptrs(s1), _p(mod), n, self.N, fmt, 0.0, 0, 0)
+        check(lib.fides_ct_export_raw(self._h, ct._h, C.byref(raw)), self._h)
+        return s0, s1, [int(x) for x in mod], raw.Noise, raw.NoiseLevel, raw.slots
+
+    def import_raw_pt(self, sub_0, moduli, noise=None, noise_level=1, slots=None, fmt=0):
+        sub_0 = [np.ascontiguousarray(x, dtype=np.uint64) for x in sub_0]
+        mod = np.ascontiguousarray(moduli, dtype=np.uint64)
+        raw = RawPt(self._limb_ptrs(sub_0), _p(mod), len(sub_0), self.N, fmt, float(noise or self.scale),
+                    noise_level, slots or self.N // 2)
+        h = vp()
+        check(lib.fides_pt_import_raw(self._h, C.byref(raw), C.byref(h)), self._h)
+        return Plaintext(self, h.value)
+
+    def import_raw_key(self, galois, r_key, r_key_moduli):
+        """Switching key from RawKeySwitchKey-shaped data: r_key[h][d][i] (h = 0
+        for the a half, 1 for b) of N words, r_key_moduli[h][d][i] its modulus.
+        galois 0 is the relinearisation key."""
+        dnum, nl = len(r_key[0]), len(r_key[0][0])
+        limbs = [np.ascontiguousarray(r_key[h][d][i], dtype=np.uint64)
+                 for h in range(2) for d in range(dnum) for i in range(nl)]
+        mod = np.ascontiguousarray([r_key_moduli[h][d][i] for h in range(2) for d in range(dnum) for i in range(nl)],
+                                   dtype=np.uint64)
+        raw = RawKey(self._limb_ptrs(limbs), _p(mod), dnum, nl, self.N)
+        check(lib.fides_key_import_raw(self._h, galois, C.byref(raw)), self._h)
+
+    def export_raw_key(self, galois=0):
+        """(r_key [2][dnum][L+K][N], r_key_moduli [2][dnum][L+K]) of a resident key."""
+        nl = self.L + self.K
+        arr = np.empty((2, self.dnum, nl, self.N), dtype=np.uint64)
+        limbs = [arr[h, d, i] for h in range(2) for d in range(self.dnum) for i in range(nl)]
+        mod = np.zeros(2 * self.dnum * nl, dtype=np.uint64)
+        raw = RawKey(self._limb_ptrs(limbs), _p(mod), self.dnum, nl, self.N)
+        check(lib.fides_key_export_raw(self._h, galois, C.byref(raw)), self._h)
+        return arr, mod.reshape(2, self.dnum, nl)
 
     def random_ct(self, level, seed):
         h = vp()

@@ -42,6 +42,23 @@ class BootParams(C.Structure):
                 ("double_angle", C.c_int), ("correction", C.c_int)]
 
 
+class RawCt(C.Structure):
+    """fides_raw_ct: RawCipherText's shape (limb arrays with their moduli)."""
+    _fields_ = [("sub_0", C.POINTER(u64p)), ("sub_1", C.POINTER(u64p)), ("moduli", u64p), ("numRes", C.c_int),
+                ("N", C.c_int), ("format", C.c_int), ("Noise", C.c_double), ("NoiseLevel", C.c_int),
+                ("slots", C.c_int)]
+
+
+class RawPt(C.Structure):
+    _fields_ = [("sub_0", C.POINTER(u64p)), ("moduli", u64p), ("numRes", C.c_int), ("N", C.c_int),
+                ("format", C.c_int), ("Noise", C.c_double), ("NoiseLevel", C.c_int), ("slots", C.c_int)]
+
+
+class RawKey(C.Structure):
+    _fields_ = [("r_key", C.POINTER(u64p)), ("r_key_moduli", u64p), ("dnum", C.c_int), ("nlimbs", C.c_int),
+                ("N", C.c_int)]
+
+
 def _sig(name, args, res=C.c_int):
     f = getattr(lib, name)
     f.argtypes = args
@@ -82,6 +99,11 @@ EXPORTS = {
     "fides_ct_set_level": ([vp, vp, C.c_int], C.c_int),
     "fides_pt_upload": ([vp, u64p, C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),
     "fides_pt_free": ([vp, vp], C.c_int),
+    "fides_ct_import_raw": ([vp, C.POINTER(RawCt), C.POINTER(vp)], C.c_int),
+    "fides_ct_export_raw": ([vp, vp, C.POINTER(RawCt)], C.c_int),
+    "fides_pt_import_raw": ([vp, C.POINTER(RawPt), C.POINTER(vp)], C.c_int),
+    "fides_key_import_raw": ([vp, C.c_uint32, C.POINTER(RawKey)], C.c_int),
+    "fides_key_export_raw": ([vp, C.c_uint32, C.POINTER(RawKey)], C.c_int),
     "fides_hmult": ([vp, vp, vp, vp, C.c_int], C.c_int),
     "fides_square": ([vp, vp, vp, C.c_int], C.c_int),
     "fides_rescale": ([vp, vp, vp], C.c_int),

@@ -39,6 +39,38 @@ enum SecretKeyDist { GAUSSIAN = 0, UNIFORM_TERNARY = 1, SPARSE_TERNARY = 2 };
 enum PKESchemeFeature { PKE = 0x01, KEYSWITCH = 0x02, LEVELEDSHE = 0x08, ADVANCEDSHE = 0x10, FHE = 0x40 };
 struct DCRTPoly {};
 struct CryptoContextCKKSRNS {};
+enum Format { EVALUATION = 0, COEFFICIENT = 1 };
+
+// The raw-residue shapes FIDESlib exchanges with OpenFHE
+// (src/CKKS/openfhe-interface/RawCiphertext.cuh:19-93), without the OpenFHE
+// objects they were read from: one vector of N words per limb, limb i mod
+// moduli[i], EVALUATION meaning OpenFHE's bit-reversed NTT order.
+struct RawCipherText {
+    std::vector<std::vector<uint64_t>> sub_0, sub_1;
+    std::vector<uint64_t> moduli;
+    int numRes = 0;
+    int N = 0;
+    Format format = EVALUATION;
+    double Noise = 0;
+    int NoiseLevel = 1;
+    int slots = 0;
+};
+struct RawPlainText {
+    std::vector<std::vector<uint64_t>> sub_0;
+    std::vector<uint64_t> moduli;
+    int numRes = 0;
+    int N = 0;
+    Format format = EVALUATION;
+    double Noise = 0;
+    int slots = 0;
+    int NoiseLevel = 1;
+};
+// r_key[h][d][i]: half h (0 = a, 1 = b), digit d, limb i; r_key_moduli alike
+struct RawKeySwitchKey {
+    std::vector<std::vector<std::vector<uint64_t>>> r_key_moduli;
+    std::vector<std::vector<std::vector<std::vector<uint64_t>>>> r_key;
+    std::string keyid;
+};
 
 template <typename T>
 class CCParams;
@@ -77,7 +109,10 @@ class CryptoContextImpl;
 
 class CiphertextImpl {
   public:
-    CiphertextImpl(fides_ctx* c, fides_ct* h) : ctx(c), handle(h) {}
+    CiphertextImpl(fides_ctx* c, fides_ct* h) : ctx(c), handle(h), loaded(h != nullptr) {}
+    // host-side (raw) ciphertext, moved to the device by LoadCiphertext
+    CiphertextImpl(fides_ctx* c, RawCipherText r)
+        : ctx(c), handle(nullptr), raw(std::make_shared<RawCipherText>(std::move(r))), loaded(false) {}
     ~CiphertextImpl() {
         if (handle) fides_ct_free(ctx, handle);
     }
@@ -105,13 +140,18 @@ class CiphertextImpl {
     }
     fides_ctx* ctx;
     fides_ct* handle;
+    std::shared_ptr<RawCipherText> raw;
+    bool loaded;
 };
 template <typename T = DCRTPoly>
 using Ciphertext = std::shared_ptr<CiphertextImpl>;
 
 class PlaintextImpl {
   public:
-    PlaintextImpl(fides_ctx* c, fides_pt* h, uint32_t s) : ctx(c), handle(h), slots(s) {}
+    PlaintextImpl(fides_ctx* c, fides_pt* h, uint32_t s) : ctx(c), handle(h), slots(s), loaded(h != nullptr) {}
+    PlaintextImpl(fides_ctx* c, RawPlainText r)
+        : ctx(c), handle(nullptr), slots((uint32_t)r.slots), raw(std::make_shared<RawPlainText>(std::move(r))),
+          loaded(false) {}
     ~PlaintextImpl() {
         if (handle) fides_pt_free(ctx, handle);
     }
@@ -128,6 +168,8 @@ class PlaintextImpl {
     fides_ctx* ctx;
     fides_pt* handle;
     uint32_t slots;
+    std::shared_ptr<RawPlainText> raw;
+    bool loaded;
     size_t length = 0;
     std::vector<std::complex<double>> values;
 };
@@ -205,7 +247,67 @@ class CryptoContextImpl<DCRTPoly> {
         check(fides_keygen_rotations(ctx, sk->handle, (int)steps.size(), steps.data(), (int)slots, seed++), ctx);
     }
     void EvalConjugateKeyGen(const PrivateKey<DCRTPoly>& sk) { check(fides_keygen_conjugate(ctx, sk->handle, seed++), ctx); }
-    void LoadContext(const PublicKey<DCRTPoly>&) {}
+    // ---- loading (api/CryptoContext.hpp:60-66) ----
+    // Raw switching keys (RawKeySwitchKey, e.g. read from OpenFHE) queued here
+    // are uploaded by LoadContext, as the reference loads the OpenFHE
+    // context's evaluation keys there (api/CryptoContext.cpp:176-228).  Keys
+    // made by EvalMultKeyGen / EvalRotateKeyGen are device-resident already.
+    void AddEvalMultKey(RawKeySwitchKey k) { pending.emplace_back(0u, std::move(k)); }
+    void AddRotationKey(int32_t index, RawKeySwitchKey k) {
+        pending.emplace_back(fides_rotation_galois(ctx, index, (int)slots), std::move(k));
+    }
+    void LoadContext(const PublicKey<DCRTPoly>&) {
+        for (auto& pk : pending) load_key(pk.first, pk.second);
+        pending.clear();
+        loadedCtx = true;
+    }
+    void LoadCiphertext(Ciphertext<DCRTPoly>& ct) {
+        if (ct->loaded) return;
+        auto& r = *ct->raw;
+        std::vector<uint64_t*> p0, p1;
+        for (auto& v : r.sub_0) p0.push_back(v.data());
+        for (auto& v : r.sub_1) p1.push_back(v.data());
+        fides_raw_ct rc{p0.data(), p1.data(), r.moduli.data(), r.numRes, r.N, (int)r.format,
+                        r.Noise, r.NoiseLevel, r.slots};
+        check(fides_ct_import_raw(ctx, &rc, &ct->handle), ctx);
+        ct->loaded = true;
+    }
+    void LoadPlaintext(Plaintext& pt) {
+        if (pt->loaded) return;
+        auto& r = *pt->raw;
+        std::vector<uint64_t*> p0;
+        for (auto& v : r.sub_0) p0.push_back(v.data());
+        fides_raw_pt rp{p0.data(), r.moduli.data(), r.numRes, r.N, (int)r.format, r.Noise, r.NoiseLevel, r.slots};
+        check(fides_pt_import_raw(ctx, &rp, &pt->handle), ctx);
+        pt->loaded = true;
+    }
+    // A host-side ciphertext / plaintext from raw residues (what
+    // GetRawCipherText / GetRawPlainText return for an OpenFHE object); it
+    // is moved to the device by LoadCiphertext / LoadPlaintext.
+    Ciphertext<DCRTPoly> CiphertextFromRaw(RawCipherText r) { return std::make_shared<CiphertextImpl>(ctx, std::move(r)); }
+    Plaintext PlaintextFromRaw(RawPlainText r) { return std::make_shared<PlaintextImpl>(ctx, std::move(r)); }
+    // The raw residues of a device ciphertext (GetRawCipherText,
+    // src/CKKS/openfhe-interface/RawCiphertext.cu:48-75), in either format.
+    RawCipherText GetRawCipherText(const Ciphertext<DCRTPoly>& ct, Format f = EVALUATION) {
+        RawCipherText r;
+        const int n = (int)ct->GetLevel() + 1;
+        const size_t N = GetRingDimension();
+        r.sub_0.assign(n, std::vector<uint64_t>(N));
+        r.sub_1.assign(n, std::vector<uint64_t>(N));
+        r.moduli.assign(n, 0);
+        std::vector<uint64_t*> p0, p1;
+        for (auto& v : r.sub_0) p0.push_back(v.data());
+        for (auto& v : r.sub_1) p1.push_back(v.data());
+        fides_raw_ct rc{p0.data(), p1.data(), r.moduli.data(), n, (int)N, (int)f, 0.0, 0, 0};
+        check(fides_ct_export_raw(ctx, ct->handle, &rc), ctx);
+        r.numRes = rc.numRes;
+        r.N = rc.N;
+        r.format = f;
+        r.Noise = rc.Noise;
+        r.NoiseLevel = rc.NoiseLevel;
+        r.slots = rc.slots;
+        return r;
+    }
 
     Plaintext MakeCKKSPackedPlaintext(const std::vector<std::complex<double>>& v, size_t noiseScaleDeg = 1,
                                       uint32_t level = 0, std::shared_ptr<void> = nullptr, uint32_t nslots = 0) {
@@ -306,8 +408,86 @@ class CryptoContextImpl<DCRTPoly> {
         check(fides_square(ctx, prepare(a)->handle, o->handle, 0), ctx);
         return o;
     }
-    void EvalMultInPlace(Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) { a = EvalMult(a, b); }
+    // ---- the commuted, in-place, mutable and many-operand forms
+    //      (api/CryptoContext.hpp:110-159); Mutable forms may rescale or
+    //      level-align their operands in place, as OpenFHE's do ----
+    void EvalNegateInPlace(Ciphertext<DCRTPoly>& a) { a = EvalNegate(a); }
+    Ciphertext<DCRTPoly> EvalAdd(Plaintext& p, const Ciphertext<DCRTPoly>& a) { return EvalAdd(a, p); }
+    Ciphertext<DCRTPoly> EvalAdd(double v, const Ciphertext<DCRTPoly>& a) { return EvalAdd(a, v); }
     void EvalAddInPlace(Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) { a = EvalAdd(a, b); }
+    void EvalAddInPlace(Ciphertext<DCRTPoly>& a, Plaintext& p) { a = EvalAdd(a, p); }
+    void EvalAddInPlace(Plaintext& p, Ciphertext<DCRTPoly>& a) { a = EvalAdd(a, p); }
+    void EvalAddInPlace(Ciphertext<DCRTPoly>& a, double v) { a = EvalAdd(a, v); }
+    void EvalAddInPlace(double v, Ciphertext<DCRTPoly>& a) { a = EvalAdd(a, v); }
+    Ciphertext<DCRTPoly> EvalAddMutable(Ciphertext<DCRTPoly>& a, Ciphertext<DCRTPoly>& b) {
+        auto x = match(a, b);
+        a = x.first;
+        b = x.second;
+        return op2(fides_add, a, b);
+    }
+    Ciphertext<DCRTPoly> EvalAddMutable(Ciphertext<DCRTPoly>& a, Plaintext& p) { return EvalAdd(a, p); }
+    Ciphertext<DCRTPoly> EvalAddMutable(Plaintext& p, Ciphertext<DCRTPoly>& a) { return EvalAdd(a, p); }
+    void EvalAddMutableInPlace(Ciphertext<DCRTPoly>& a, Ciphertext<DCRTPoly>& b) { a = EvalAddMutable(a, b); }
+    // Sum of many ciphertexts as a balanced tree of additions.
+    Ciphertext<DCRTPoly> EvalAddMany(const std::vector<Ciphertext<DCRTPoly>>& cts) {
+        if (cts.empty()) throw Exception(FIDES_BAD_ARG, "EvalAddMany: no ciphertexts");
+        std::vector<Ciphertext<DCRTPoly>> v(cts);
+        while (v.size() > 1) {
+            std::vector<Ciphertext<DCRTPoly>> next;
+            for (size_t i = 0; i + 1 < v.size(); i += 2) next.push_back(EvalAdd(v[i], v[i + 1]));
+            if (v.size() & 1) next.push_back(v.back());
+            v.swap(next);
+        }
+        return v[0];
+    }
+    void EvalAddManyInPlace(std::vector<Ciphertext<DCRTPoly>>& cts) {
+        auto s = EvalAddMany(cts);
+        cts[0] = s;
+    }
+    // ct - pt = -(-ct + pt)
+    Ciphertext<DCRTPoly> EvalSub(const Ciphertext<DCRTPoly>& a, Plaintext& p) { return EvalNegate(EvalAdd(EvalNegate(a), p)); }
+    Ciphertext<DCRTPoly> EvalSub(Plaintext& p, const Ciphertext<DCRTPoly>& a) { return EvalAdd(EvalNegate(a), p); }
+    Ciphertext<DCRTPoly> EvalSub(const Ciphertext<DCRTPoly>& a, double v) { return EvalAdd(a, -v); }
+    Ciphertext<DCRTPoly> EvalSub(double v, const Ciphertext<DCRTPoly>& a) { return EvalAdd(EvalNegate(a), v); }
+    void EvalSubInPlace(Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) { a = EvalSub(a, b); }
+    void EvalSubInPlace(Ciphertext<DCRTPoly>& a, double v) { a = EvalSub(a, v); }
+    void EvalSubInPlace(double v, Ciphertext<DCRTPoly>& a) { a = EvalSub(v, a); }
+    Ciphertext<DCRTPoly> EvalSubMutable(Ciphertext<DCRTPoly>& a, Ciphertext<DCRTPoly>& b) {
+        auto x = match(a, b);
+        a = x.first;
+        b = x.second;
+        return op2(fides_sub, a, b);
+    }
+    Ciphertext<DCRTPoly> EvalSubMutable(Ciphertext<DCRTPoly>& a, Plaintext& p) { return EvalSub(a, p); }
+    Ciphertext<DCRTPoly> EvalSubMutable(Plaintext& p, Ciphertext<DCRTPoly>& a) { return EvalSub(p, a); }
+    void EvalSubMutableInPlace(Ciphertext<DCRTPoly>& a, Ciphertext<DCRTPoly>& b) { a = EvalSubMutable(a, b); }
+    Ciphertext<DCRTPoly> EvalMult(Plaintext& p, const Ciphertext<DCRTPoly>& a) { return EvalMult(a, p); }
+    Ciphertext<DCRTPoly> EvalMult(double v, const Ciphertext<DCRTPoly>& a) { return EvalMult(a, v); }
+    void EvalMultInPlace(Ciphertext<DCRTPoly>& a, const Ciphertext<DCRTPoly>& b) { a = EvalMult(a, b); }
+    void EvalMultInPlace(Ciphertext<DCRTPoly>& a, Plaintext& p) { a = EvalMult(a, p); }
+    void EvalMultInPlace(Ciphertext<DCRTPoly>& a, double v) { a = EvalMult(a, v); }
+    void EvalMultInPlace(double v, Ciphertext<DCRTPoly>& a) { a = EvalMult(a, v); }
+    Ciphertext<DCRTPoly> EvalMultMutable(Ciphertext<DCRTPoly>& a, Ciphertext<DCRTPoly>& b) {
+        a = prepare(a);
+        b = prepare(b);
+        auto x = align(a, b);
+        a = x.first;
+        b = x.second;
+        auto o = empty();
+        check(fides_hmult(ctx, a->handle, b->handle, o->handle, 0), ctx);
+        return o;
+    }
+    Ciphertext<DCRTPoly> EvalMultMutable(Ciphertext<DCRTPoly>& a, Plaintext& p) {
+        a = prepare(a);
+        return EvalMult(a, p);
+    }
+    Ciphertext<DCRTPoly> EvalMultMutable(Plaintext& p, Ciphertext<DCRTPoly>& a) { return EvalMultMutable(a, p); }
+    void EvalMultMutableInPlace(Ciphertext<DCRTPoly>& a, Ciphertext<DCRTPoly>& b) { a = EvalMultMutable(a, b); }
+    void EvalSquareInPlace(Ciphertext<DCRTPoly>& a) { a = EvalSquare(a); }
+    Ciphertext<DCRTPoly> EvalSquareMutable(Ciphertext<DCRTPoly>& a) {
+        a = prepare(a);
+        return EvalSquare(a);
+    }
     Ciphertext<DCRTPoly> Rescale(const Ciphertext<DCRTPoly>& a) {
         auto o = empty();
         check(fides_rescale(ctx, a->handle, o->handle), ctx);
@@ -339,27 +519,81 @@ class CryptoContextImpl<DCRTPoly> {
         check(fides_rotate_hoisted(ctx, a->handle, (int)idx.size(), idx.data(), hs.data()), ctx);
         return outs;
     }
+    // The precomputed-digit forms: the hoisted ModUp is shared inside one
+    // EvalFastRotation call; addFirst (the P c0 term) is always part of it.
+    Ciphertext<DCRTPoly> EvalFastRotationExt(const Ciphertext<DCRTPoly>& a, int32_t index, const std::shared_ptr<void>&,
+                                             bool) {
+        return EvalRotate(a, index);
+    }
+    std::vector<Ciphertext<DCRTPoly>> EvalFastRotationExt(const Ciphertext<DCRTPoly>& a,
+                                                          const std::vector<int32_t>& idx,
+                                                          const std::shared_ptr<void>& pre, bool) {
+        return EvalFastRotation(a, idx, 0, pre);
+    }
+    // Sum of `n` slots spaced `stride` apart into every slot: log2(n)
+    // rotate-and-add steps (AccumulateSum, api/CryptoContext.hpp:183-184);
+    // needs rotation keys for stride * 2^k, k < log2(n).
+    Ciphertext<DCRTPoly> AccumulateSum(const Ciphertext<DCRTPoly>& a, int n, int stride = 1) {
+        Ciphertext<DCRTPoly> acc = a;
+        for (int k = 1; k < n; k <<= 1) acc = EvalAdd(acc, EvalRotate(acc, k * stride));
+        return acc;
+    }
+    void AccumulateSumInPlace(Ciphertext<DCRTPoly>& a, int n, int stride = 1) { a = AccumulateSum(a, n, stride); }
     Ciphertext<DCRTPoly> EvalConjugate(const Ciphertext<DCRTPoly>& a) {
         auto o = empty();
         check(fides_conjugate(ctx, a->handle, o->handle), ctx);
         return o;
     }
-    // EvalChebyshevSeries (api/CryptoContext.hpp:171-173)
+    // EvalChebyshevSeries (api/CryptoContext.hpp:171-173).  The coefficients
+    // follow OpenFHE's convention, which the reference keeps: the series is
+    // c_0 / 2 + sum_{k >= 1} c_k T_k(y) (the reference adds q.front() / 2,
+    // src/CKKS/ApproxModEval.cu:216); the C ABI takes the plain sum.
     Ciphertext<DCRTPoly> EvalChebyshevSeries(const Ciphertext<DCRTPoly>& a, const std::vector<double>& coeffs,
                                              double lo, double hi) {
+        if (coeffs.empty()) throw Exception(FIDES_BAD_ARG, "EvalChebyshevSeries: no coefficients");
+        std::vector<double> c(coeffs);
+        c[0] *= 0.5;
         auto o = empty();
-        check(fides_chebyshev_series(ctx, prepare(a)->handle, coeffs.data(), (int)coeffs.size() - 1, lo, hi,
-                                     o->handle),
-              ctx);
+        check(fides_chebyshev_series(ctx, prepare(a)->handle, c.data(), (int)c.size() - 1, lo, hi, o->handle), ctx);
         return o;
     }
-    // EvalBootstrapSetup / EvalBootstrapKeyGen / EvalBootstrap (api/CryptoContext.hpp:80-82,180-181)
-    void EvalBootstrapSetup(const std::vector<uint32_t>& levelBudget = {3, 3}, const std::vector<uint32_t>& = {0, 0},
-                            uint32_t numSlots = 0) {
+    void EvalChebyshevSeriesInPlace(Ciphertext<DCRTPoly>& a, const std::vector<double>& coeffs, double lo, double hi) {
+        a = EvalChebyshevSeries(a, coeffs, lo, hi);
+    }
+    // Coefficients c_0..c_degree of the Chebyshev interpolant of func on
+    // [a, b] at the degree + 1 Chebyshev nodes (GetChebyshevCoefficients,
+    // api/CryptoContext.hpp:173, src/PolyApprox.cu:11), in OpenFHE's
+    // convention c_0 / 2 + sum_{k >= 1} c_k T_k(y), y = (2x - (a + b)) / (b - a),
+    // which EvalChebyshevSeries takes.
+    template <class F>
+    static std::vector<double> GetChebyshevCoefficients(F&& func, double a, double b, size_t degree) {
+        const size_t n = degree + 1;
+        const double pi = 3.14159265358979323846;
+        std::vector<double> f(n), c(n, 0.0);
+        for (size_t j = 0; j < n; ++j) {
+            const double y = std::cos(pi * (j + 0.5) / n);
+            f[j] = func(0.5 * (b - a) * y + 0.5 * (a + b));
+        }
+        for (size_t k = 0; k < n; ++k) {
+            double s = 0;
+            for (size_t j = 0; j < n; ++j) s += f[j] * std::cos(pi * k * (j + 0.5) / n);
+            c[k] = 2.0 * s / n;
+        }
+        return c;
+    }
+    // EvalBootstrapSetup / EvalBootstrapKeyGen / EvalBootstrap (api/CryptoContext.hpp:80-82,180-181).
+    // dim1 (the baby-step sizes of OpenFHE's linear transforms) is accepted
+    // and not needed: each CoeffsToSlots / SlotsToCoeffs group here picks its
+    // baby step from its own diagonals.  correctionFactor scales the message
+    // by 2^correctionFactor through EvalMod (fides_boot_params.correction).
+    void EvalBootstrapSetup(const std::vector<uint32_t>& levelBudget = {3, 3}, std::vector<uint32_t> dim1 = {0, 0},
+                            uint32_t numSlots = 0, uint32_t correctionFactor = 0) {
+        (void)dim1;
         fides_boot_params bp{};
         bp.slots = (int)(numSlots ? numSlots : slots);
         bp.level_budget[0] = levelBudget.size() > 0 ? (int)levelBudget[0] : 3;
         bp.level_budget[1] = levelBudget.size() > 1 ? (int)levelBudget[1] : 3;
+        bp.correction = (int)correctionFactor;
         check(fides_bootstrap_setup(ctx, &bp), ctx);
     }
     void EvalBootstrapKeyGen(const PrivateKey<DCRTPoly>& sk, uint32_t numSlots = 0) {
@@ -371,10 +605,20 @@ class CryptoContextImpl<DCRTPoly> {
         check(fides_keygen_rotations(ctx, sk->handle, n, rot.data(), s, seed++), ctx);
         check(fides_keygen_conjugate(ctx, sk->handle, seed++), ctx);
     }
-    Ciphertext<DCRTPoly> EvalBootstrap(const Ciphertext<DCRTPoly>& a) {
+    // numIterations > 1 (OpenFHE's iterated bootstrapping, which needs the
+    // input at a higher level to form the residual) is not supported here.
+    Ciphertext<DCRTPoly> EvalBootstrap(const Ciphertext<DCRTPoly>& a, uint32_t numIterations = 1,
+                                       uint32_t precision = 0, bool prescaled = false) {
+        (void)precision;
+        (void)prescaled;
+        if (numIterations > 1) throw Exception(FIDES_UNSUPPORTED, "EvalBootstrap: numIterations > 1");
         auto o = empty();
         check(fides_bootstrap(ctx, prepare(a)->handle, o->handle), ctx);
         return o;
+    }
+    void EvalBootstrapInPlace(Ciphertext<DCRTPoly>& a, uint32_t numIterations = 1, uint32_t precision = 0,
+                              bool prescaled = false) {
+        a = EvalBootstrap(a, numIterations, precision, prescaled);
     }
     static void SetLevel(Ciphertext<DCRTPoly>& ct, size_t level) {
         int L = 0;
@@ -390,7 +634,25 @@ class CryptoContextImpl<DCRTPoly> {
     uint32_t hamming;
     uint32_t slots = 0;
     bool sparse = false;
+    bool loadedCtx = false;
     uint64_t seed = 0x5EEDull;
+    std::vector<std::pair<uint32_t, RawKeySwitchKey>> pending;
+
+    void load_key(uint32_t galois, RawKeySwitchKey& k) {
+        if (k.r_key.size() != 2 || k.r_key_moduli.size() != 2) throw Exception(FIDES_BAD_ARG, "raw key: two halves");
+        const int dn = (int)k.r_key[0].size();
+        const int nl = dn ? (int)k.r_key[0][0].size() : 0;
+        std::vector<uint64_t*> limbs;
+        std::vector<uint64_t> mods;
+        for (int h = 0; h < 2; ++h)
+            for (int d = 0; d < dn; ++d)
+                for (int i = 0; i < nl; ++i) {
+                    limbs.push_back(k.r_key[h][d][i].data());
+                    mods.push_back(k.r_key_moduli[h][d][i]);
+                }
+        fides_raw_key rk{limbs.data(), mods.data(), dn, nl, (int)GetRingDimension()};
+        check(fides_key_import_raw(ctx, galois, &rk), ctx);
+    }
 
     int top_level() const {
         int L = 0;

@@ -492,6 +492,7 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.md_pmod = (const uint64_t*)(base + parts[i_dq].off);
     d.rs_qinv = (const uint64_t*)(base + parts[i_rq].off);
     d.err = (uint32_t*)(base + parts[i_err].off);
+    ntt_prepare(d);
     d.tc_btab = nullptr;
     d.tc_boff = nullptr;
     if (conv_tc_eligible(d)) {

@@ -95,10 +95,10 @@ void moddown_finish(fides_ctx* c, Workspace& w, int level, int nb, uint64_t* con
 
 }  // namespace
 
-// ModUp conversion + NTT of the digits, from the scaled coefficients in XT.
-static void modup_from_xt(fides_ctx* c, Workspace& w, int level, int nb) {
+// Limbs of the ModUp digits in DIG (transformed in place): digit d holds the
+// Q primes outside it up to `level`, then the K special primes.
+static LimbMap digit_map(fides_ctx* c, Workspace& w, int level, int nb) {
     const int n = level + 1, N = c->N;
-    launch_modup_conv(c->dev, level, nb, w.XT, w.DIG, w.dig_stride, w.stride, w.st);
     LimbMap dm{};
     dm.nb = nb;
     const int nd = level / c->alpha + 1;
@@ -111,7 +111,13 @@ static void modup_from_xt(fides_ctx* c, Workspace& w, int level, int nb) {
         dm.seg[dm.nseg++] = g;
         dm.total += g.count;
     }
-    ntt_forward(c->dev, dm, FL_PLAIN, FS_PLAIN, w.st);
+    return dm;
+}
+
+// ModUp conversion + NTT of the digits, from the scaled coefficients in XT.
+static void modup_from_xt(fides_ctx* c, Workspace& w, int level, int nb) {
+    launch_modup_conv(c->dev, level, nb, w.XT, w.DIG, w.dig_stride, w.stride, w.st);
+    ntt_forward(c->dev, digit_map(c, w, level, nb), FL_PLAIN, FS_PLAIN, w.st);
 }
 
 void eng_modup(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* x) {
@@ -153,6 +159,27 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
     im.seg[im.nseg++] = seg_ws(w.E2, w.XT, n, n, 0, level, w.stride);
     im.total = n;
     ntt_inverse(c->dev, im, IL_PLAIN, IS_MODUP, w.st);
+    if ((c->dev.ks_variant & 2) && ntt_rows_keyswitch_supported(c->dev)) {
+        // ModUp conversion and the digits' column pass; the row pass runs
+        // fused with the inner product, so the digits' evaluation limbs never
+        // reach HBM
+        launch_modup_conv(c->dev, level, nb, w.XT, w.DIG, w.dig_stride, w.stride, w.st);
+        ntt_forward_cols(c->dev, digit_map(c, w, level, nb), FL_PLAIN, w.st);
+        KsFuseArgs fa{};
+        fa.dig = w.DIG;
+        fa.own = w.E2;
+        fa.kb = key.b;
+        fa.ka = key.a;
+        fa.xb = w.XB;
+        fa.xa = w.XA;
+        fa.dig_stride = w.dig_stride;
+        fa.bstride = w.stride;
+        fa.level = level;
+        fa.fp_sums = c->dev.ks_variant & 1;
+        ntt_rows_keyswitch(c->dev, fa, nb, w.st);
+        moddown_finish(c, w, level, nb, out0, out1, true, rescale && level > 0);
+        return;
+    }
     modup_from_xt(c, w, level, nb);
     KsArgs ka{};
     for (int b = 0; b < nb; ++b) {

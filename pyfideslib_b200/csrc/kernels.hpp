@@ -32,6 +32,32 @@ int ntt_inverse_of(int forward_variant);
 // pass 2 transforms seg.out in place and applies the epilogue.  load / store
 // >= 0 override the per-segment modes.
 void ntt_forward(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st);
+// Per-device set-up of this ring dimension's kernels (the fused kernel's
+// shared-memory opt-in), before any launch or stream capture.
+void ntt_prepare(const DevCtx& ctx);
+// Forward NTT column pass alone (seg.in -> seg.out), for the fused key switch.
+void ntt_forward_cols(const DevCtx& ctx, const LimbMap& map, int load, cudaStream_t st);
+// Row pass of the ModUp digits fused with the key-switch inner product:
+//   XB[m] = sum_d D_d[t] kb[d][t],  XA[m] = sum_d D_d[t] ka[d][t]
+// over the extended basis m in [0, level+1+K) (prime t = m, or L + m - n for
+// the special limbs), for nb batch elements (blockIdx.y).  D_d[t] is the
+// column-pass output of digit d's limb in DIG, finished by the row stages
+// here, or the original evaluation limb `own` when t lies in digit d.
+struct KsFuseArgs {
+    const uint64_t* dig;  // ModUp digits of element 0 after the column pass
+    const uint64_t* own;  // key-switched polynomial in evaluation form, element 0
+    const uint64_t* kb;   // switching key halves [dnum][L+K][N] (one key for the batch)
+    const uint64_t* ka;
+    uint64_t* xb;         // outputs of element 0 [level+1+K][N]
+    uint64_t* xa;
+    size_t dig_stride;    // limbs per digit in dig
+    size_t bstride;       // words between consecutive elements of dig, own, xb, xa
+    int level;
+    int fp_sums;          // 1: exact FP64 sums for primes below 2^50
+};
+void ntt_rows_keyswitch(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaStream_t st);
+// the fused row pass keeps one transformed tile per digit in shared memory
+bool ntt_rows_keyswitch_supported(const DevCtx& ctx);
 // Inverse NTT: pass A reads seg.in (+in2 for the prologue), writes seg.out;
 // pass B finishes seg.out in place.
 void ntt_inverse(const DevCtx& ctx, const LimbMap& map, int load, int store, cudaStream_t st);

@@ -414,7 +414,7 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
     count_launches(1);
     if (plain) {
         dim3 g(ctx.N / 512 * nb, level + 1 + ctx.K);
-        if (ctx.ks_variant == 1)
+        if (ctx.ks_variant & 1)
             k_ks_inner<1, Acc128, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
         else if (ctx.conv_variant == 1)
             k_ks_inner<1, AccSplit, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
@@ -422,7 +422,7 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
             k_ks_inner<1, Acc128, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
     } else {
         dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
-        if (ctx.ks_variant == 1)
+        if (ctx.ks_variant & 1)
             k_ks_inner<0, Acc128, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
         else if (ctx.conv_variant == 1)
             k_ks_inner<0, AccSplit, false><<<g, 256, 0, st>>>(ctx, level, nb, args);

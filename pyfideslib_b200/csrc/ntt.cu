@@ -159,7 +159,9 @@ __device__ __forceinline__ void load_stage_tw(ulonglong2 (&w)[15], Tab tab, int 
 // below 1.7p < 2^51.
 template <int MODE, int POS>
 __device__ __forceinline__ void bfly(uint64_t& X, uint64_t& Y, const ulonglong2 w, uint64_t p, uint64_t two_p) {
-    if constexpr (MODE == 4)
+    if constexpr (MODE == 7)
+        ct_bfly_fp<true>(X, Y, w, as_f64(p), as_f64(two_p));
+    else if constexpr (MODE == 4)
         ct_bfly_fp<(POS & 1) != 0>(X, Y, w, as_f64(p), as_f64(two_p));
     else if constexpr (MODE == 6)
         ct_bfly_fp<(POS & 1) == 0>(X, Y, w, as_f64(p), as_f64(two_p));
@@ -212,12 +214,14 @@ __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_k
 
 // Forward group in the mode of this limb's prime (uniform per CTA); ROWS
 // selects the row pass's centring schedule for the double-precision mode.
-template <int KF, int KL, bool PF, bool AQ, bool FP, bool ROWS, class Tab>
+template <int KF, int KL, bool PF, bool AQ, bool FP, bool ROWS, class Tab, bool GEN = false>
 __device__ __forceinline__ void fwd_group(int fmode, uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi,
                                           uint64_t p, uint64_t two_p) {
     if constexpr (FP) {
         if (fmode == 4) {
-            run_group<KF, KL, PF, ROWS ? 6 : 4>(x, tab, t_of_kb0, B, th_hi, p, two_p);
+            // generated row twiddles carry a looser quotient companion: the
+            // row stages then centre X at every stage (MODE 7)
+            run_group<KF, KL, PF, (ROWS && GEN) ? 7 : (ROWS ? 6 : 4)>(x, tab, t_of_kb0, B, th_hi, p, two_p);
             return;
         }
     }
@@ -268,6 +272,38 @@ __device__ __forceinline__ void inv_group(int imode, uint64_t (&x)[16], Tab tab,
     else
         run_group<KF, KL, PF, 2>(x, tab, t_of_kb0, B, th_hi, k0, k1);
 }
+
+// Twiddles of the forward row pass.  Row r's stage s' (0 <= s' < LC) uses
+// psi_br[((R + r) << s') + h] for h < 2^s', and since the bit reversals of
+// the two parts occupy disjoint bits,
+//   psi_br[((R + r) << s') + h] = psi_br[(R + r) << s'] * psi_br[h]  (mod p).
+// With GEN (double-precision limbs) the twiddle is formed from the first
+// factor (one per row and stage, with its Shoup companion, `sa`) and the
+// second (h < C/2, shared by every row, `sb`), both in shared memory: one
+// Shoup product on the integer pipes, which the FP64 butterflies leave idle,
+// replaces a 16-byte L2 load per twiddle (about 2 KB of twiddles per 2 KB
+// row otherwise).  The quotient companion is then fl(w * pinv) rather than
+// the correctly rounded w / p, which MODE 7 allows for.  Without GEN, or for
+// limbs on the integer butterflies, the table is read from L2 as before.
+struct RowTw {
+    const uint64_t* twg;    // (w, companion) pairs of this limb's table
+    const ulonglong2* sa;   // [LC] first factors of this thread's row, or null
+    const uint64_t* sb;     // [C/2] second factors
+    int lr;                 // log2 R
+    uint64_t p;
+    double pinv;
+    __device__ __forceinline__ ulonglong2 operator()(size_t i) const {
+        if (!sa) return ldg2(twg, i);
+        const int sp = (63 - __clzll((long long)i)) - lr;
+        const ulonglong2 a = sa[sp];
+        const uint64_t w = mul_shoup(sb[i & ((1ull << sp) - 1)], a.x, a.y, p);
+        const double wd = as_f64(fp_from_u(w));
+        ulonglong2 r;
+        r.x = as_u64(wd);
+        r.y = as_u64(__dmul_rn(wd, pinv));
+        return r;
+    }
+};
 
 // Tile geometry shared by kernels and launchers.
 template <int LR, int LC>
@@ -376,22 +412,34 @@ __device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRe
 // mappings hit 16 distinct bank pairs.
 __device__ __forceinline__ int padi(int r) { return r + (r >> 4); }
 
-template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP>
+template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP, bool GEN = false>
 __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     __shared__ __align__(16) uint64_t sm[TR * CP];
+    __shared__ ulonglong2 s_twa[GEN ? TR * LC : 1];
+    __shared__ uint64_t s_twb[GEN ? C / 2 : 1];
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const int fmode = fwd_mode<AQ, FP>(pc.p);
     const FwdK kk = fwd_consts(fmode, pc);
-    const uint64_t* twg = (fmode == 4 ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)lr.prime * 2 * ctx.N;
-    auto tab = [&](size_t i) { return ldg2(twg, i); };
+    const bool gen = GEN && fmode == 4;
+    const uint64_t* twg = (fmode == 4 && !gen ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)lr.prime * 2 * ctx.N;
 
     const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int row = blockIdx.x * TR + rl;
+    RowTw tab{twg, nullptr, s_twb, LR, pc.p, as_f64(pc.pinv_f64)};
+    if constexpr (GEN) {
+        if (gen) {
+            for (int e = threadIdx.x; e < TR * LC; e += NT)
+                s_twa[e] = ldg2(twg, (size_t)(R + blockIdx.x * TR + e / LC) << (e % LC));
+            for (int e = threadIdx.x; e < C / 2; e += NT) s_twb[e] = twg[2 * (size_t)e];
+            __syncthreads();
+            tab.sa = s_twa + rl * LC;
+        }
+    }
     const uint64_t* src = lr.out + (size_t)row * C;
     uint64_t x[16];
 #pragma unroll
@@ -408,7 +456,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
             if (lr.in3) prefetch_l2(lr.in3 + tile + i);
         }
     }
-    fwd_group<3, 0, PF, AQ, FP, true>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+    fwd_group<3, 0, PF, AQ, FP, true, RowTw, GEN>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
 #pragma unroll
@@ -416,7 +464,8 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        fwd_group<LC - 5, 0, PF, AQ, FP, true>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
+        fwd_group<LC - 5, 0, PF, AQ, FP, true, RowTw, GEN>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0,
+                                                           kk.k1);
         if (FP && fmode == 4) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
@@ -452,6 +501,190 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
             o.y = fwd_epilogue<false>(ctx, lr, pc, base + i + 1, sm[wi + 1]);
             *reinterpret_cast<ulonglong2*>(lr.out + base + i) = o;
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// forward, pass 2 of the ModUp digits fused with the key-switch inner product
+// ---------------------------------------------------------------------------
+// One CTA owns a tile of TR rows of output limb m (prime t) of batch element
+// b.  First it runs the row stages of every digit limb of prime t that needs
+// them (the column pass has already run in place), each into its own
+// shared-memory tile; when t lies inside digit d, that digit's value is the
+// original evaluation limb instead and is read in the epilogue.  Then one
+// epilogue forms  XB[m] = sum_d D_d kb[d][t],  XA[m] = sum_d D_d ka[d][t]
+// with the key and own-limb loads of all digits in flight together.  The
+// digit limbs never return to HBM in evaluation form and are not read back
+// by a separate inner-product kernel.  The prime, and so the twiddles, are
+// the same for every digit of the CTA.  Reference: the key-switch dot
+// products fused into the NTT epilogue, ksk_dot_fusion / ksk_dot_acc_fusion
+// (src/NTTfusions.cuh:295-345) in the KSK_DOT modes of NTT_ (src/NTT.cu:680-700).
+//
+// Sums: for primes below 2^50 with fp_sums, each product is an exact FP64
+// fp_mulmod of operands of magnitude <= p/2 (transformed values centred
+// first) or < p (own limb, key): |r| <= 0.69p, and up to 8 digits sum below
+// 5.6p < 2^53; otherwise products are reduced on the integer pipes (mul_mod)
+// and added mod p.  Results are canonical residues, identical to k_ks_inner's.
+template <int LR, int LC>
+constexpr size_t ks_tile_words() {
+    using G = Geo<LR, LC>;
+    return (size_t)G::TR * G::CP;
+}
+
+template <int LR, int LC, bool PF, bool AQ, bool FP, bool GEN>
+__global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constant__ DevCtx ctx,
+                                                            const __grid_constant__ KsFuseArgs a) {
+    using G = Geo<LR, LC>;
+    constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
+    constexpr int TILE = TR * C;
+    constexpr int TW = TR * CP;
+    extern __shared__ __align__(16) uint64_t ks_sm[];  // [digits needing rows][TR][CP]
+    __shared__ ulonglong2 s_twa[GEN ? TR * LC : 1];
+    __shared__ uint64_t s_twb[GEN ? C / 2 : 1];
+
+    const int level = a.level, n = level + 1;
+    const int m = blockIdx.z;
+    const size_t boff = (size_t)blockIdx.y * a.bstride;
+    const int t = m < n ? m : ctx.L + (m - n);
+    const PrimeConst pc = ctx.pc[t];
+    const int fmode = fwd_mode<AQ, FP>(pc.p);
+    const FwdK kk = fwd_consts(fmode, pc);
+    const bool gen = GEN && fmode == 4;
+    const uint64_t* twg = (fmode == 4 && !gen ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)t * 2 * ctx.N;
+
+    const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int row = blockIdx.x * TR + rl;
+    RowTw tab{twg, nullptr, s_twb, LR, pc.p, as_f64(pc.pinv_f64)};
+    if constexpr (GEN) {
+        if (gen) {
+            // the twiddle factors serve every digit of the CTA (same prime, same rows)
+            for (int e = threadIdx.x; e < TR * LC; e += NT)
+                s_twa[e] = ldg2(twg, (size_t)(R + blockIdx.x * TR + e / LC) << (e % LC));
+            for (int e = threadIdx.x; e < C / 2; e += NT) s_twb[e] = twg[2 * (size_t)e];
+            __syncthreads();
+            tab.sa = s_twa + rl * LC;
+        }
+    }
+    const size_t base = (size_t)blockIdx.x * TILE;
+    const size_t kstride = (size_t)(ctx.L + ctx.K) * ctx.N;
+    const size_t limb_off = (size_t)t * ctx.N + base;
+    const int nd = level / ctx.alpha + 1;
+    const int d_own = m < n ? t / ctx.alpha : -1;  // digit holding t (its value is the own limb)
+
+    // the epilogue's key tiles (and own tile) are read once per batch from
+    // HBM; start those reads now, under the transforms
+    for (int i = threadIdx.x * 16; i < TILE; i += NT * 16) {
+        for (int d = 0; d < nd; ++d) {
+            prefetch_l2(a.kb + d * kstride + limb_off + i);
+            prefetch_l2(a.ka + d * kstride + limb_off + i);
+        }
+        if (d_own >= 0) prefetch_l2(a.own + boff + limb_off + i);
+    }
+
+#pragma unroll 1
+    for (int d = 0, slot = 0; d < nd; ++d) {
+        if (d == d_own) continue;
+        const int lo = d * ctx.alpha, hi = min(lo + ctx.alpha - 1, level), cnt = hi - lo + 1;
+        const int md = m < n ? (t < lo ? t : t - cnt) : (n - cnt) + (m - n);
+        const uint64_t* src = a.dig + boff + ((size_t)d * a.dig_stride + md) * ctx.N + (size_t)row * C;
+        uint64_t* srow = ks_sm + (size_t)slot * TW + rl * CP;
+        ++slot;
+        uint64_t x[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
+        fwd_group<3, 0, PF, AQ, FP, true, RowTw, GEN>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+        if constexpr (LC > 4) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) srow[padi(th + (k << (LC - 4)))] = x[k];
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
+            fwd_group<LC - 5, 0, PF, AQ, FP, true, RowTw, GEN>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0,
+                                                               kk.k1);
+            // each thread rewrites exactly the slots it read
+#pragma unroll
+            for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) srow[padi(th + k)] = x[k];
+        }
+    }
+    __syncthreads();
+
+    const bool fpk = a.fp_sums && pc.p < kFpPrimeBound;
+    const double pf = __ull2double_rn(pc.p), pinv = as_f64(pc.pinv_f64);
+    uint64_t* xb = a.xb + boff + (size_t)m * ctx.N + base;
+    uint64_t* xa = a.xa + boff + (size_t)m * ctx.N + base;
+    for (int i = threadIdx.x * 2; i < TILE; i += NT * 2) {
+        const int wi = (i / C) * CP + padi(i % C);
+        ulonglong2 ob, oa;
+        if (fpk) {
+            double sb0 = 0, sb1 = 0, sa0 = 0, sa1 = 0;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                if (d < nd) {
+                    const ulonglong2 kb2 = *reinterpret_cast<const ulonglong2*>(a.kb + d * kstride + limb_off + i);
+                    const ulonglong2 ka2 = *reinterpret_cast<const ulonglong2*>(a.ka + d * kstride + limb_off + i);
+                    double x0, x1;
+                    if (d == d_own) {
+                        const ulonglong2 o = *reinterpret_cast<const ulonglong2*>(a.own + boff + limb_off + i);
+                        x0 = as_f64(fp_from_u(o.x));
+                        x1 = as_f64(fp_from_u(o.y));
+                    } else {
+                        const uint64_t* tile = ks_sm + (size_t)(d_own >= 0 && d > d_own ? d - 1 : d) * TW;
+                        if (fmode == 4) {
+                            x0 = fp_center(as_f64(tile[wi]), pf, pinv);
+                            x1 = fp_center(as_f64(tile[wi + 1]), pf, pinv);
+                        } else {
+                            x0 = as_f64(fp_from_u(reduce_fwd(tile[wi], pc)));
+                            x1 = as_f64(fp_from_u(reduce_fwd(tile[wi + 1], pc)));
+                        }
+                    }
+                    sb0 = __dadd_rn(sb0, fp_mulmod(x0, as_f64(fp_from_u(kb2.x)), pf, pinv));
+                    sb1 = __dadd_rn(sb1, fp_mulmod(x1, as_f64(fp_from_u(kb2.y)), pf, pinv));
+                    sa0 = __dadd_rn(sa0, fp_mulmod(x0, as_f64(fp_from_u(ka2.x)), pf, pinv));
+                    sa1 = __dadd_rn(sa1, fp_mulmod(x1, as_f64(fp_from_u(ka2.y)), pf, pinv));
+                }
+            }
+            ob.x = fp_to_u(fp_center(sb0, pf, pinv), pf, pinv);
+            ob.y = fp_to_u(fp_center(sb1, pf, pinv), pf, pinv);
+            oa.x = fp_to_u(fp_center(sa0, pf, pinv), pf, pinv);
+            oa.y = fp_to_u(fp_center(sa1, pf, pinv), pf, pinv);
+        } else {
+            Acc128 sb0, sb1, sa0, sa1;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                if (d < nd) {
+                    const ulonglong2 kb2 = *reinterpret_cast<const ulonglong2*>(a.kb + d * kstride + limb_off + i);
+                    const ulonglong2 ka2 = *reinterpret_cast<const ulonglong2*>(a.ka + d * kstride + limb_off + i);
+                    uint64_t x0, x1;
+                    if (d == d_own) {
+                        const ulonglong2 o = *reinterpret_cast<const ulonglong2*>(a.own + boff + limb_off + i);
+                        x0 = o.x;
+                        x1 = o.y;
+                    } else {
+                        const uint64_t* tile = ks_sm + (size_t)(d_own >= 0 && d > d_own ? d - 1 : d) * TW;
+                        if (FP && fmode == 4) {
+                            x0 = fp_to_u(as_f64(tile[wi]), as_f64(kk.k0), as_f64(kk.k1));
+                            x1 = fp_to_u(as_f64(tile[wi + 1]), as_f64(kk.k0), as_f64(kk.k1));
+                        } else {
+                            x0 = reduce_fwd(tile[wi], pc);
+                            x1 = reduce_fwd(tile[wi + 1], pc);
+                        }
+                    }
+                    sb0.mac(x0, kb2.x);
+                    sb1.mac(x1, kb2.y);
+                    sa0.mac(x0, ka2.x);
+                    sa1.mac(x1, ka2.y);
+                }
+            }
+            ob.x = sb0.reduce(pc);
+            ob.y = sb1.reduce(pc);
+            oa.x = sa0.reduce(pc);
+            oa.y = sa1.reduce(pc);
+        }
+        *reinterpret_cast<ulonglong2*>(xb + i) = ob;
+        *reinterpret_cast<ulonglong2*>(xa + i) = oa;
     }
 }
 
@@ -612,16 +845,18 @@ bool ntt_supported(int logN) { return logN >= 8 && logN <= 16; }
 // 4: (2, group prefetch, approximate quotient), 5 and 6: as 3 and 4 with the
 // double-precision butterflies for primes below 2^50, 7: column pass of 5
 // with the row pass of 6, 8: column pass of 5 with a row pass at 4 CTAs per
-// SM.  Inverse configurations: 0 (2, group prefetch),
+// SM, 9: column pass of 5 with a row pass whose twiddles are generated from
+// two small factor tables in shared memory (RowTw).  Inverse configurations:
+// 0 (2, group prefetch),
 // 1 (3, per-stage), 2 (4, per-stage), 3 and 4: as 1 and 0 with
 // double-precision butterflies for primes below 2^50; ntt_inverse_of(v)
 // pairs each forward variant with an inverse configuration of the same
 // arithmetic.
-int ntt_num_variants() { return 9; }
+int ntt_num_variants() { return 10; }
 int ntt_num_inverse_variants() { return 5; }
 int ntt_inverse_of(int v) {
-    static const int inv[9] = {0, 1, 2, 1, 0, 3, 4, 3, 3};
-    return v >= 0 && v < 9 ? inv[v] : 0;
+    static const int inv[10] = {0, 1, 2, 1, 0, 3, 4, 3, 3, 3};
+    return v >= 0 && v < 10 ? inv[v] : 0;
 }
 
 template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP>
@@ -646,13 +881,14 @@ static void launch_inv_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st)
     k_ntt_inv_cols<LR, LC, MINB, PF, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
 }
 
-// column pass with one configuration, row pass with another
-template <int LR, int LC, int MB1, bool PF1, int MB2, bool PF2, bool AQ, bool FP>
+// column pass with one configuration, row pass with another (GEN2: row
+// twiddles generated from the two factor tables, see RowTw)
+template <int LR, int LC, int MB1, bool PF1, int MB2, bool PF2, bool AQ, bool FP, bool GEN2 = false>
 static void launch_fwd_mix(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
     dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
     k_ntt_fwd_cols<LR, LC, MB1, PF1, AQ, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
-    k_ntt_fwd_rows<LR, LC, MB2, PF2, AQ, FP><<<g2, G::NTR, 0, st>>>(ctx, map);
+    k_ntt_fwd_rows<LR, LC, MB2, PF2, AQ, FP, GEN2><<<g2, G::NTR, 0, st>>>(ctx, map);
 }
 
 template <int LR, int LC>
@@ -666,6 +902,7 @@ static void launch_fwd(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
         case 6: launch_fwd_v<LR, LC, 2, true, true, true>(ctx, map, st); break;
         case 7: launch_fwd_mix<LR, LC, 3, false, 2, true, true, true>(ctx, map, st); break;
         case 8: launch_fwd_mix<LR, LC, 3, false, 4, false, true, true>(ctx, map, st); break;
+        case 9: launch_fwd_mix<LR, LC, 3, false, 3, false, true, true, true>(ctx, map, st); break;
         default: launch_fwd_v<LR, LC, 2, true, false, false>(ctx, map, st); break;
     }
 }
@@ -678,6 +915,71 @@ static void launch_inv(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
         case 3: launch_inv_v<LR, LC, 3, false, true>(ctx, map, st); break;
         case 4: launch_inv_v<LR, LC, 2, true, true>(ctx, map, st); break;
         default: launch_inv_v<LR, LC, 2, true, false>(ctx, map, st); break;
+    }
+}
+
+// forward column pass alone (the row pass of the ModUp digits is fused with
+// the key-switch inner product)
+template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP>
+static void launch_fwd_cols_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
+    using G = Geo<LR, LC>;
+    dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total);
+    k_ntt_fwd_cols<LR, LC, MINB, PF, AQ, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
+}
+
+template <int LR, int LC>
+static void launch_fwd_cols(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
+    switch (ctx.ntt_variant) {
+        case 1: launch_fwd_cols_v<LR, LC, 3, false, false, false>(ctx, map, st); break;
+        case 2: launch_fwd_cols_v<LR, LC, 4, false, false, false>(ctx, map, st); break;
+        case 3: launch_fwd_cols_v<LR, LC, 3, false, true, false>(ctx, map, st); break;
+        case 4: launch_fwd_cols_v<LR, LC, 2, true, true, false>(ctx, map, st); break;
+        case 5: case 7: case 8: case 9: launch_fwd_cols_v<LR, LC, 3, false, true, true>(ctx, map, st); break;
+        case 6: launch_fwd_cols_v<LR, LC, 2, true, true, true>(ctx, map, st); break;
+        default: launch_fwd_cols_v<LR, LC, 2, true, false, false>(ctx, map, st); break;
+    }
+}
+
+template <int LR, int LC, bool PF, bool AQ, bool FP, bool GEN = false>
+static void launch_rows_ks_v(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaStream_t st) {
+    using G = Geo<LR, LC>;
+    const size_t smem = ks_tile_words<LR, LC>() * 8 * (size_t)ctx.dnum;  // opted in by ntt_prepare
+    dim3 g(G::R / G::TR, nb, a.level + 1 + ctx.K);
+    k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, GEN><<<g, G::NTR, smem, st>>>(ctx, a);
+}
+
+template <int LR, int LC, bool PF, bool AQ, bool FP, bool GEN = false>
+static void prepare_rows_ks_v(int dnum) {
+    cudaFuncSetAttribute(k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(ks_tile_words<LR, LC>() * 8 * (size_t)dnum));
+}
+
+template <int LR, int LC>
+static void prepare_rows_ks(const DevCtx& ctx, const LimbMap&, cudaStream_t) {
+    prepare_rows_ks_v<LR, LC, true, false, false>(ctx.dnum);
+    prepare_rows_ks_v<LR, LC, false, false, false>(ctx.dnum);
+    prepare_rows_ks_v<LR, LC, false, true, false>(ctx.dnum);
+    prepare_rows_ks_v<LR, LC, true, true, true>(ctx.dnum);
+    prepare_rows_ks_v<LR, LC, false, true, true>(ctx.dnum);
+    prepare_rows_ks_v<LR, LC, false, true, true, true>(ctx.dnum);
+}
+
+bool ntt_rows_keyswitch_supported(const DevCtx& ctx) {
+    // one transformed tile per digit in shared memory (at most 227 KB)
+    return ctx.dnum <= 6;
+}
+
+// the row-pass arithmetic of the context's forward variant (butterfly form,
+// twiddle fetch); occupancy is set by the fused kernel's shared memory
+template <int LR, int LC>
+static void launch_rows_ks(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaStream_t st) {
+    switch (ctx.ntt_variant) {
+        case 0: launch_rows_ks_v<LR, LC, true, false, false>(ctx, a, nb, st); break;
+        case 1: case 2: launch_rows_ks_v<LR, LC, false, false, false>(ctx, a, nb, st); break;
+        case 3: case 4: launch_rows_ks_v<LR, LC, false, true, false>(ctx, a, nb, st); break;
+        case 6: case 7: launch_rows_ks_v<LR, LC, true, true, true>(ctx, a, nb, st); break;
+        case 9: launch_rows_ks_v<LR, LC, false, true, true, true>(ctx, a, nb, st); break;
+        default: launch_rows_ks_v<LR, LC, false, true, true>(ctx, a, nb, st); break;
     }
 }
 
@@ -708,6 +1010,36 @@ void ntt_forward(const DevCtx& ctx, const LimbMap& m, int load, int store, cudaS
     set_modes(map, load, store);
     count_launches(2);
     FIDES_NTT_DISPATCH(launch_fwd)
+}
+
+void ntt_prepare(const DevCtx& ctx) {
+    const LimbMap map{};
+    cudaStream_t st = nullptr;
+    FIDES_NTT_DISPATCH(prepare_rows_ks)
+}
+
+void ntt_forward_cols(const DevCtx& ctx, const LimbMap& m, int load, cudaStream_t st) {
+    if (m.total <= 0) return;
+    LimbMap map = m;
+    set_modes(map, load, -1);
+    count_launches(1);
+    FIDES_NTT_DISPATCH(launch_fwd_cols)
+}
+
+void ntt_rows_keyswitch(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaStream_t st) {
+    count_launches(1);
+    switch (ctx.logN) {
+        case 8: launch_rows_ks<4, 4>(ctx, a, nb, st); break;
+        case 9: launch_rows_ks<4, 5>(ctx, a, nb, st); break;
+        case 10: launch_rows_ks<5, 5>(ctx, a, nb, st); break;
+        case 11: launch_rows_ks<5, 6>(ctx, a, nb, st); break;
+        case 12: launch_rows_ks<6, 6>(ctx, a, nb, st); break;
+        case 13: launch_rows_ks<6, 7>(ctx, a, nb, st); break;
+        case 14: launch_rows_ks<7, 7>(ctx, a, nb, st); break;
+        case 15: launch_rows_ks<7, 8>(ctx, a, nb, st); break;
+        case 16: launch_rows_ks<8, 8>(ctx, a, nb, st); break;
+        default: return;
+    }
 }
 
 void ntt_inverse(const DevCtx& ctx, const LimbMap& m, int load, int store, cudaStream_t st) {

@@ -103,7 +103,23 @@ static uint64_t splitmix(uint64_t* s) {
  * residues, 1: p - 1 everywhere, 2: alternating 0 / p - 1.  Returns the number
  * of coefficients that differ from exact arithmetic (forward) plus those
  * that do not come back (inverse), or -1 if a value left its proven range. */
+static int ntt_check_impl(uint64_t p, uint64_t psi, uint64_t seed, int pattern, int gen);
+
 int emu_ntt_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
+    return ntt_check_impl(p, psi, seed, pattern, 0);
+}
+
+/* The row pass with generated twiddles (forward variant 9): stages 8..15
+ * centre X first at every stage and take the twiddle's quotient companion as
+ * fl(w * pinv_up) instead of the correctly rounded w / p (the twiddle itself,
+ * psi_br[a 2^k] psi_br[h] mod p, is formed exactly on the integer pipes).
+ * The looser companion widens the quotient error to 1/2 + |y| 1.5 2^-52, so
+ * |t| <= 1.14p; centring every stage keeps every value below 1.65p. */
+int emu_ntt_gen_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
+    return ntt_check_impl(p, psi, seed, pattern, 1);
+}
+
+static int ntt_check_impl(uint64_t p, uint64_t psi, uint64_t seed, int pattern, int gen) {
     const int logN = 16, N = 1 << logN;
     uint64_t *a = malloc(8 * N), *e = malloc(8 * N), *tw = malloc(8 * N), *itw = malloc(8 * N);
     double *d = malloc(8 * (size_t)N), *W = malloc(8 * (size_t)N), *WQ = malloc(8 * (size_t)N);
@@ -142,14 +158,16 @@ int emu_ntt_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
     for (int j = 0; j < N; ++j) d[j] = (double)a[j];
     int st = 0;
     for (int m = 1, t = N / 2; m < N; m <<= 1, t >>= 1, ++st) {
-        const int red = st < 8 ? (st % 4) & 1 : !((st % 4) & 1);
+        const int red = st < 8 ? (st % 4) & 1 : (gen ? 1 : !((st % 4) & 1));
         for (int i = 0; i < m; ++i)
             for (int j = 2 * i * t; j < 2 * i * t + t; ++j) {
                 double x = d[j];
                 const double y = d[j + t];
                 if (fabs(y) >= 2251799813685248.0) bad = -1; /* |y| < 2^51 */
+                if (gen && st >= 8 && fabs(y) >= 1.65 * pd) bad = -1; /* the stated bound */
                 if (red) x = fp_center(x, pd, pinv);
-                const double tt = fp_mulw(y, W[m + i], WQ[m + i], pd);
+                const double wq = (gen && st >= 8) ? W[m + i] * pinv : WQ[m + i];
+                const double tt = fp_mulw(y, W[m + i], wq, pd);
                 d[j] = x + tt;
                 d[j + t] = x - tt;
             }

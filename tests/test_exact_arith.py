@@ -76,6 +76,7 @@ def emu(tmp_path_factory):
                     os.path.join(HERE, "exact_arith_emu.c"), "-o", out, "-lm"], check=True)
     lib = ctypes.CDLL(out)
     lib.emu_ntt_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
+    lib.emu_ntt_gen_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
     lib.emu_ks_check.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
     lib.emu_tensor_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
     return lib
@@ -89,6 +90,16 @@ def test_fp64_ntt_schedule_exact(emu, p):
     psi = _psi(p)
     for pattern in (0, 1, 2):
         assert emu.emu_ntt_check(p, psi, 1000 + pattern, pattern) == 0, pattern
+
+
+@pytest.mark.parametrize("p", PRIMES_50)
+def test_fp64_ntt_generated_row_twiddles_exact(emu, p):
+    """Forward variant 9: the row pass forms its twiddles on the fly and
+    takes their quotient companions as fl(w * pinv) (not correctly rounded),
+    centring X at every row stage."""
+    psi = _psi(p)
+    for pattern in (0, 1, 2):
+        assert emu.emu_ntt_gen_check(p, psi, 2000 + pattern, pattern) == 0, pattern
 
 
 @pytest.mark.parametrize("p", PRIMES_50[:2])

@@ -252,7 +252,7 @@ def test_keyswitch_variants_bitexact(logN, L, K, dnum):
     for keys, (x0, x1, y0, y1) in (((kb, ka), (a0, a1, b0, b1)), ((kbx, kbx), (a0, e1, b0, e1))):
         cc.upload_relin_key(*keys)
         want = oc.hmult(level, x0, x1, y0, y1, keys[0], keys[1], rescale=True)
-        for v in (0, 1):
+        for v in (0, 1, 2, 3):
             assert lib.fides_set_keyswitch_variant(cc._h, v) == 0
             got = cc.EvalMult(cc.upload(x0, x1), cc.upload(y0, y1), rescale=True).download()
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), v
@@ -269,3 +269,39 @@ def test_hmult_c2_shape_bitexact():
     got = cc.EvalMult(cc.upload(a0, a1), cc.upload(b0, b1), rescale=True).download()
     want = oc.hmult(29, a0, a1, b0, b1, kb, ka, rescale=True)
     assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+@pytest.mark.parametrize("logN,L,K", [(12, 9, 3), (16, 30, 10)])
+def test_fused_keyswitch_every_ntt_variant(logN, L, K):
+    """The inner product fused into the digits' NTT row pass (integer and FP64
+    sums) with the row-pass arithmetic of every forward NTT variant gives the
+    oracle's HMult residues, at every level of a small context and at the
+    top, a middle and the lowest level of the workload's, batched too."""
+    from pyfideslib_b200._capi import lib
+
+    cc, oc = make_pair(logN, L, K, 3)
+    kb, ka = rand_key(oc, 1500 + logN)
+    cc.upload_relin_key(kb, ka)
+    levels = list(range(L)) if logN < 16 else [L - 1, 12, 0]
+    raw = {lv: (rand_ct(oc, lv, 1600 + lv), rand_ct(oc, lv, 1700 + lv)) for lv in levels}
+    want = {lv: oc.hmult(lv, *raw[lv][0], *raw[lv][1], kb, ka, rescale=lv > 0) for lv in levels}
+    A = {lv: cc.upload(*raw[lv][0]) for lv in levels}
+    B = {lv: cc.upload(*raw[lv][1]) for lv in levels}
+    nv = C.c_int()
+    lib.fides_autotune(cc._h, None, None, C.byref(nv))
+    for v in range(nv.value):
+        cc.set_ntt_variant(v)
+        for ksv in (2, 3):
+            assert lib.fides_set_keyswitch_variant(cc._h, ksv) == 0
+            for lv in levels:
+                got = cc.EvalMult(A[lv], B[lv], rescale=lv > 0).download()
+                assert np.array_equal(got[0], want[lv][0]) and np.array_equal(got[1], want[lv][1]), (v, ksv, lv)
+            outs = cc.EvalMultBatch([A[lv] for lv in levels] * 2, [B[lv] for lv in levels] * 2, rescale=True)
+            for k, lv in enumerate(levels * 2):
+                if lv == 0:
+                    continue
+                got = outs[k].download()
+                assert np.array_equal(got[0], want[lv][0]) and np.array_equal(got[1], want[lv][1]), (v, ksv, lv)
+    cc.set_ntt_variant(-1)
+    assert lib.fides_set_keyswitch_variant(cc._h, 1) == 0
+    assert device_status(cc) == 0
