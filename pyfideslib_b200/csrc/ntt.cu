@@ -214,14 +214,12 @@ __device__ __forceinline__ void run_group(uint64_t (&x)[16], Tab tab, int t_of_k
 
 // Forward group in the mode of this limb's prime (uniform per CTA); ROWS
 // selects the row pass's centring schedule for the double-precision mode.
-template <int KF, int KL, bool PF, bool AQ, bool FP, bool ROWS, class Tab, bool GEN = false>
+template <int KF, int KL, bool PF, bool AQ, bool FP, bool ROWS, class Tab>
 __device__ __forceinline__ void fwd_group(int fmode, uint64_t (&x)[16], Tab tab, int t_of_kb0, size_t B, int th_hi,
                                           uint64_t p, uint64_t two_p) {
     if constexpr (FP) {
         if (fmode == 4) {
-            // generated row twiddles carry a looser quotient companion: the
-            // row stages then centre X at every stage (MODE 7)
-            run_group<KF, KL, PF, (ROWS && GEN) ? 7 : (ROWS ? 6 : 4)>(x, tab, t_of_kb0, B, th_hi, p, two_p);
+            run_group<KF, KL, PF, ROWS ? 6 : 4>(x, tab, t_of_kb0, B, th_hi, p, two_p);
             return;
         }
     }
@@ -273,37 +271,51 @@ __device__ __forceinline__ void inv_group(int imode, uint64_t (&x)[16], Tab tab,
         run_group<KF, KL, PF, 2>(x, tab, t_of_kb0, B, th_hi, k0, k1);
 }
 
-// Twiddles of the forward row pass.  Row r's stage s' (0 <= s' < LC) uses
-// psi_br[((R + r) << s') + h] for h < 2^s', and since the bit reversals of
-// the two parts occupy disjoint bits,
-//   psi_br[((R + r) << s') + h] = psi_br[(R + r) << s'] * psi_br[h]  (mod p).
-// With GEN (double-precision limbs) the twiddle is formed from the first
-// factor (one per row and stage, with its Shoup companion, `sa`) and the
-// second (h < C/2, shared by every row, `sb`), both in shared memory: one
-// Shoup product on the integer pipes, which the FP64 butterflies leave idle,
-// replaces a 16-byte L2 load per twiddle (about 2 KB of twiddles per 2 KB
-// row otherwise).  The quotient companion is then fl(w * pinv) rather than
-// the correctly rounded w / p, which MODE 7 allows for.  Without GEN, or for
-// limbs on the integer butterflies, the table is read from L2 as before.
-struct RowTw {
-    const uint64_t* twg;    // (w, companion) pairs of this limb's table
-    const ulonglong2* sa;   // [LC] first factors of this thread's row, or null
-    const uint64_t* sb;     // [C/2] second factors
-    int lr;                 // log2 R
-    uint64_t p;
-    double pinv;
-    __device__ __forceinline__ ulonglong2 operator()(size_t i) const {
-        if (!sa) return ldg2(twg, i);
-        const int sp = (63 - __clzll((long long)i)) - lr;
-        const ulonglong2 a = sa[sp];
-        const uint64_t w = mul_shoup(sb[i & ((1ull << sp) - 1)], a.x, a.y, p);
-        const double wd = as_f64(fp_from_u(w));
-        ulonglong2 r;
-        r.x = as_u64(wd);
-        r.y = as_u64(__dmul_rn(wd, pinv));
-        return r;
+// Row-pass twiddles of forward variant 10 (double-precision limbs, C = 256).
+// Row r's stage s' (0 <= s' < 8) uses psi_br[((R + r) << s') + h], h < 2^s'.
+// The first four stages' 15 twiddles per row are the same for the 16 threads
+// of the row: they are staged in shared memory once per CTA, loaded at
+// kernel start beside the data.  In the last four, thread th needs
+// h = th 2^(s'-4) + g (g < 2^(s'-4)), and since the bit reversals of disjoint
+// bit groups add,
+//   psi_br[((R + r) << s') + (th << (s'-4)) + g] = D_s' * psi_br[g]  (mod p),
+// D_s' = psi_br[((R + r) << s') + (th << (s'-4))]: four table loads per
+// thread, issued before the row exchange, and 11 products on the
+// FP64 pipes (fp_mulmod, |w| <= 0.875p, quotient companion fl(w * pinv))
+// instead of 15 dependent L2 loads per group.  The looser companion widens
+// the butterfly's quotient error, so these stages centre X at every stage
+// (MODE 7); every value stays below 1.7p.
+template <int KB>
+__device__ __forceinline__ void sg_stage1(uint64_t (&x)[16], const ulonglong2* g1, uint64_t p, uint64_t pinv) {
+    constexpr int t = 3 - KB;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        if (k & (1 << KB)) continue;
+        bfly<6, t>(x[k], x[k | (1 << KB)], g1[(1 << t) - 1 + (k >> (KB + 1))], p, pinv);
     }
-};
+    if constexpr (KB > 0) sg_stage1<KB - 1>(x, g1, p, pinv);
+}
+
+template <int KB>
+__device__ __forceinline__ void sg_stage2(uint64_t (&x)[16], const ulonglong2 (&d)[4], const double* gw, uint64_t p,
+                                          uint64_t pinv) {
+    constexpr int t = 7 - KB, NG = 8 >> KB;
+    const ulonglong2 D = d[t - 4];
+    ulonglong2 w[NG];
+    w[0] = D;
+#pragma unroll
+    for (int g = 1; g < NG; ++g) {
+        const double wd = fp_mulmod(as_f64(D.x), gw[g], as_f64(p), as_f64(pinv));
+        w[g].x = as_u64(wd);
+        w[g].y = as_u64(__dmul_rn(wd, as_f64(pinv)));
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        if (k & (1 << KB)) continue;
+        bfly<7, 0>(x[k], x[k | (1 << KB)], w[k >> (KB + 1)], p, pinv);
+    }
+    if constexpr (KB > 0) sg_stage2<KB - 1>(x, d, gw, p, pinv);
+}
 
 // Tile geometry shared by kernels and launchers.
 template <int LR, int LC>
@@ -412,38 +424,41 @@ __device__ __forceinline__ uint64_t fwd_epilogue(const DevCtx& ctx, const LimbRe
 // mappings hit 16 distinct bank pairs.
 __device__ __forceinline__ int padi(int r) { return r + (r >> 4); }
 
-template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP, bool GEN = false>
+template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP, bool SG = false>
 __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
+    constexpr bool kSG = SG && FP && LC == 8;
     __shared__ __align__(16) uint64_t sm[TR * CP];
-    __shared__ ulonglong2 s_twa[GEN ? TR * LC : 1];
-    __shared__ uint64_t s_twb[GEN ? C / 2 : 1];
+    __shared__ ulonglong2 s_g1[kSG ? TR * 16 : 1];  // first four stages' twiddles per row, entry 2^t - 1 + g
+    __shared__ double s_gw[kSG ? 8 : 1];            // psi_br[g], g < 8
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
     const int fmode = fwd_mode<AQ, FP>(pc.p);
     const FwdK kk = fwd_consts(fmode, pc);
-    const bool gen = GEN && fmode == 4;
-    const uint64_t* twg = (fmode == 4 && !gen ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)lr.prime * 2 * ctx.N;
+    const uint64_t* twg = (fmode == 4 ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)lr.prime * 2 * ctx.N;
+    auto tab = [&](size_t i) { return ldg2(twg, i); };
 
     const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int row = blockIdx.x * TR + rl;
-    RowTw tab{twg, nullptr, s_twb, LR, pc.p, as_f64(pc.pinv_f64)};
-    if constexpr (GEN) {
-        if (gen) {
-            for (int e = threadIdx.x; e < TR * LC; e += NT)
-                s_twa[e] = ldg2(twg, (size_t)(R + blockIdx.x * TR + e / LC) << (e % LC));
-            for (int e = threadIdx.x; e < C / 2; e += NT) s_twb[e] = twg[2 * (size_t)e];
-            __syncthreads();
-            tab.sa = s_twa + rl * LC;
-        }
-    }
     const uint64_t* src = lr.out + (size_t)row * C;
     uint64_t x[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
+    if constexpr (kSG) {
+        if (fmode == 4) {
+            // the twiddle loads go out right behind the data loads
+            const ulonglong2* tw2 = reinterpret_cast<const ulonglong2*>(twg);
+            for (int e = threadIdx.x; e < TR * 15; e += NT) {
+                const int r = e / 15, j = e % 15, t = 31 - __clz(j + 1);
+                s_g1[r * 16 + j] = tw2[((size_t)(R + blockIdx.x * TR + r) << t) + (j + 1 - (1 << t))];
+            }
+            if (threadIdx.x < 8) s_gw[threadIdx.x] = as_f64(tw2[threadIdx.x].x);
+            __syncthreads();
+        }
+    }
     if (lr.smode != FS_PLAIN && lr.in2 && gridDim.y > 1) {
         // the epilogue's operands for this tile (one 128-byte line per thread
         // and operand): start their HBM reads now, under the butterflies.
@@ -456,16 +471,32 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
             if (lr.in3) prefetch_l2(lr.in3 + tile + i);
         }
     }
-    fwd_group<3, 0, PF, AQ, FP, true, RowTw, GEN>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+    if (kSG && fmode == 4) {
+        if constexpr (kSG) sg_stage1<3>(x, s_g1 + rl * 16, kk.k0, kk.k1);
+    } else {
+        fwd_group<3, 0, PF, AQ, FP, true>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+    }
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
+        // the last four stages' D_s' go out before the row exchange
+        ulonglong2 dtw[kSG ? 4 : 1];
+        if constexpr (kSG) {
+            if (fmode == 4) {
+#pragma unroll
+                for (int t = 4; t < 8; ++t)
+                    dtw[t - 4] = ldg2(twg, ((size_t)(R + row) << t) + ((size_t)th << (t - 4)));
+            }
+        }
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi(th + (k << (LC - 4)))] = x[k];
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        fwd_group<LC - 5, 0, PF, AQ, FP, true, RowTw, GEN>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0,
-                                                           kk.k1);
+        if (kSG && fmode == 4) {
+            if constexpr (kSG) sg_stage2<3>(x, dtw, s_gw, kk.k0, kk.k1);
+        } else {
+            fwd_group<LC - 5, 0, PF, AQ, FP, true>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
+        }
         if (FP && fmode == 4) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) x[k] = fp_to_u(as_f64(x[k]), as_f64(kk.k0), as_f64(kk.k1));
@@ -531,7 +562,7 @@ constexpr size_t ks_tile_words() {
     return (size_t)G::TR * G::CP;
 }
 
-template <int LR, int LC, bool PF, bool AQ, bool FP, bool GEN>
+template <int LR, int LC, bool PF, bool AQ, bool FP>
 __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ KsFuseArgs a) {
     using G = Geo<LR, LC>;
@@ -539,8 +570,6 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constan
     constexpr int TILE = TR * C;
     constexpr int TW = TR * CP;
     extern __shared__ __align__(16) uint64_t ks_sm[];  // [digits needing rows][TR][CP]
-    __shared__ ulonglong2 s_twa[GEN ? TR * LC : 1];
-    __shared__ uint64_t s_twb[GEN ? C / 2 : 1];
 
     const int level = a.level, n = level + 1;
     const int m = blockIdx.z;
@@ -549,22 +578,11 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constan
     const PrimeConst pc = ctx.pc[t];
     const int fmode = fwd_mode<AQ, FP>(pc.p);
     const FwdK kk = fwd_consts(fmode, pc);
-    const bool gen = GEN && fmode == 4;
-    const uint64_t* twg = (fmode == 4 && !gen ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)t * 2 * ctx.N;
+    const uint64_t* twg = (fmode == 4 ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)t * 2 * ctx.N;
+    auto tab = [&](size_t i) { return ldg2(twg, i); };
 
     const int th = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int row = blockIdx.x * TR + rl;
-    RowTw tab{twg, nullptr, s_twb, LR, pc.p, as_f64(pc.pinv_f64)};
-    if constexpr (GEN) {
-        if (gen) {
-            // the twiddle factors serve every digit of the CTA (same prime, same rows)
-            for (int e = threadIdx.x; e < TR * LC; e += NT)
-                s_twa[e] = ldg2(twg, (size_t)(R + blockIdx.x * TR + e / LC) << (e % LC));
-            for (int e = threadIdx.x; e < C / 2; e += NT) s_twb[e] = twg[2 * (size_t)e];
-            __syncthreads();
-            tab.sa = s_twa + rl * LC;
-        }
-    }
     const size_t base = (size_t)blockIdx.x * TILE;
     const size_t kstride = (size_t)(ctx.L + ctx.K) * ctx.N;
     const size_t limb_off = (size_t)t * ctx.N + base;
@@ -592,15 +610,14 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constan
         uint64_t x[16];
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
-        fwd_group<3, 0, PF, AQ, FP, true, RowTw, GEN>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+        fwd_group<3, 0, PF, AQ, FP, true>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
         if constexpr (LC > 4) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) srow[padi(th + (k << (LC - 4)))] = x[k];
             __syncthreads();
 #pragma unroll
             for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-            fwd_group<LC - 5, 0, PF, AQ, FP, true, RowTw, GEN>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0,
-                                                               kk.k1);
+            fwd_group<LC - 5, 0, PF, AQ, FP, true>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
             // each thread rewrites exactly the slots it read
 #pragma unroll
             for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
@@ -845,8 +862,9 @@ bool ntt_supported(int logN) { return logN >= 8 && logN <= 16; }
 // 4: (2, group prefetch, approximate quotient), 5 and 6: as 3 and 4 with the
 // double-precision butterflies for primes below 2^50, 7: column pass of 5
 // with the row pass of 6, 8: column pass of 5 with a row pass at 4 CTAs per
-// SM, 9: column pass of 5 with a row pass whose twiddles are generated from
-// two small factor tables in shared memory (RowTw).  Inverse configurations:
+// SM, 9: column pass of 5 with a row pass whose twiddles are staged in
+// shared memory or formed from a staged factor (sg_stage1 / sg_stage2, C =
+// 256 only; other sizes run variant 5's row pass).  Inverse configurations:
 // 0 (2, group prefetch),
 // 1 (3, per-stage), 2 (4, per-stage), 3 and 4: as 1 and 0 with
 // double-precision butterflies for primes below 2^50; ntt_inverse_of(v)
@@ -881,14 +899,14 @@ static void launch_inv_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st)
     k_ntt_inv_cols<LR, LC, MINB, PF, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
 }
 
-// column pass with one configuration, row pass with another (GEN2: row
-// twiddles generated from the two factor tables, see RowTw)
-template <int LR, int LC, int MB1, bool PF1, int MB2, bool PF2, bool AQ, bool FP, bool GEN2 = false>
+// column pass with one configuration, row pass with another (SG2: the row
+// pass's staged and formed twiddles, see sg_stage1 / sg_stage2)
+template <int LR, int LC, int MB1, bool PF1, int MB2, bool PF2, bool AQ, bool FP, bool SG2 = false>
 static void launch_fwd_mix(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
     dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
     k_ntt_fwd_cols<LR, LC, MB1, PF1, AQ, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
-    k_ntt_fwd_rows<LR, LC, MB2, PF2, AQ, FP, GEN2><<<g2, G::NTR, 0, st>>>(ctx, map);
+    k_ntt_fwd_rows<LR, LC, MB2, PF2, AQ, FP, SG2><<<g2, G::NTR, 0, st>>>(ctx, map);
 }
 
 template <int LR, int LC>
@@ -940,17 +958,17 @@ static void launch_fwd_cols(const DevCtx& ctx, const LimbMap& map, cudaStream_t 
     }
 }
 
-template <int LR, int LC, bool PF, bool AQ, bool FP, bool GEN = false>
+template <int LR, int LC, bool PF, bool AQ, bool FP>
 static void launch_rows_ks_v(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaStream_t st) {
     using G = Geo<LR, LC>;
     const size_t smem = ks_tile_words<LR, LC>() * 8 * (size_t)ctx.dnum;  // opted in by ntt_prepare
     dim3 g(G::R / G::TR, nb, a.level + 1 + ctx.K);
-    k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, GEN><<<g, G::NTR, smem, st>>>(ctx, a);
+    k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP><<<g, G::NTR, smem, st>>>(ctx, a);
 }
 
-template <int LR, int LC, bool PF, bool AQ, bool FP, bool GEN = false>
+template <int LR, int LC, bool PF, bool AQ, bool FP>
 static void prepare_rows_ks_v(int dnum) {
-    cudaFuncSetAttribute(k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(ks_tile_words<LR, LC>() * 8 * (size_t)dnum));
 }
 
@@ -961,7 +979,6 @@ static void prepare_rows_ks(const DevCtx& ctx, const LimbMap&, cudaStream_t) {
     prepare_rows_ks_v<LR, LC, false, true, false>(ctx.dnum);
     prepare_rows_ks_v<LR, LC, true, true, true>(ctx.dnum);
     prepare_rows_ks_v<LR, LC, false, true, true>(ctx.dnum);
-    prepare_rows_ks_v<LR, LC, false, true, true, true>(ctx.dnum);
 }
 
 bool ntt_rows_keyswitch_supported(const DevCtx& ctx) {
@@ -978,7 +995,6 @@ static void launch_rows_ks(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaS
         case 1: case 2: launch_rows_ks_v<LR, LC, false, false, false>(ctx, a, nb, st); break;
         case 3: case 4: launch_rows_ks_v<LR, LC, false, true, false>(ctx, a, nb, st); break;
         case 6: case 7: launch_rows_ks_v<LR, LC, true, true, true>(ctx, a, nb, st); break;
-        case 9: launch_rows_ks_v<LR, LC, false, true, true, true>(ctx, a, nb, st); break;
         default: launch_rows_ks_v<LR, LC, false, true, true>(ctx, a, nb, st); break;
     }
 }

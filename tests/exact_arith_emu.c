@@ -105,6 +105,16 @@ static uint64_t splitmix(uint64_t* s) {
  * that do not come back (inverse), or -1 if a value left its proven range. */
 static int ntt_check_impl(uint64_t p, uint64_t psi, uint64_t seed, int pattern, int gen);
 
+/* Forward variant 10: the row pass's first four stages (8..11) take their
+ * twiddles exactly from the table (staged in shared memory) and centre X on
+ * even positions as before; its last four (12..15) centre X at every stage
+ * and form the twiddle of group offset g > 0 as fp_mulmod(D, psi_br[g])
+ * (|w| <= 0.875p, not reduced) with the quotient companion fl(w * pinv_up),
+ * D = psi_br[index - g] exact from the table; g = 0 uses D itself. */
+int emu_ntt_sg_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
+    return ntt_check_impl(p, psi, seed, pattern, 2);
+}
+
 int emu_ntt_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
     return ntt_check_impl(p, psi, seed, pattern, 0);
 }
@@ -158,19 +168,32 @@ static int ntt_check_impl(uint64_t p, uint64_t psi, uint64_t seed, int pattern, 
     for (int j = 0; j < N; ++j) d[j] = (double)a[j];
     int st = 0;
     for (int m = 1, t = N / 2; m < N; m <<= 1, t >>= 1, ++st) {
-        const int red = st < 8 ? (st % 4) & 1 : (gen ? 1 : !((st % 4) & 1));
-        for (int i = 0; i < m; ++i)
+        const int red = st < 8 ? (st % 4) & 1
+                        : (gen == 1 ? 1 : (gen == 2 && st >= 12) ? 1 : !((st % 4) & 1));
+        for (int i = 0; i < m; ++i) {
+            double w = W[m + i], wq = WQ[m + i];
+            if (gen == 1 && st >= 8) wq = W[m + i] * pinv;
+            if (gen == 2 && st >= 12) {
+                /* row-stage index s' = st - 8; the thread's offset h has its
+                 * low s' - 4 bits as the group offset g */
+                const int g = i & ((1 << (st - 12)) - 1);
+                if (g) {
+                    w = fp_mulmod(W[m + i - g], W[g], pd, pinv);
+                    if (fabs(w) > 0.875 * pd) bad = -1;
+                    wq = w * pinv;
+                }
+            }
             for (int j = 2 * i * t; j < 2 * i * t + t; ++j) {
                 double x = d[j];
                 const double y = d[j + t];
                 if (fabs(y) >= 2251799813685248.0) bad = -1; /* |y| < 2^51 */
-                if (gen && st >= 8 && fabs(y) >= 1.65 * pd) bad = -1; /* the stated bound */
+                if (gen && st >= 8 && fabs(y) >= 1.7 * pd) bad = -1; /* the stated bound */
                 if (red) x = fp_center(x, pd, pinv);
-                const double wq = (gen && st >= 8) ? W[m + i] * pinv : WQ[m + i];
-                const double tt = fp_mulw(y, W[m + i], wq, pd);
+                const double tt = fp_mulw(y, w, wq, pd);
                 d[j] = x + tt;
                 d[j + t] = x - tt;
             }
+        }
         if (st == 15)
             for (int j = 0; j < N; ++j) d[j] = (double)fp_to_u(d[j], pd, pinv);
     }

@@ -77,6 +77,7 @@ def emu(tmp_path_factory):
     lib = ctypes.CDLL(out)
     lib.emu_ntt_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
     lib.emu_ntt_gen_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
+    lib.emu_ntt_sg_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int]
     lib.emu_ks_check.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
     lib.emu_tensor_check.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
     return lib
@@ -100,6 +101,16 @@ def test_fp64_ntt_generated_row_twiddles_exact(emu, p):
     psi = _psi(p)
     for pattern in (0, 1, 2):
         assert emu.emu_ntt_gen_check(p, psi, 2000 + pattern, pattern) == 0, pattern
+
+
+@pytest.mark.parametrize("p", PRIMES_50)
+def test_fp64_ntt_staged_generated_row_twiddles_exact(emu, p):
+    """Forward variant 10: exact staged twiddles for the row pass's first
+    four stages, products of a table entry and psi_br[g] (unreduced, sloppy
+    quotient companion) for the last four, which centre X at every stage."""
+    psi = _psi(p)
+    for pattern in (0, 1, 2):
+        assert emu.emu_ntt_sg_check(p, psi, 3000 + pattern, pattern) == 0, pattern
 
 
 @pytest.mark.parametrize("p", PRIMES_50[:2])

@@ -94,13 +94,14 @@ def test_raw_plaintext_mult():
 
     pt = cc.import_raw_pt(list(m), oc.primes[:level + 1])
 
+    ct = cc.upload(c0, c1)
     out = F.Ciphertext(cc)
-    check(lib.fides_mult_pt(cc._h, cc.upload(c0, c1)._h, pt._h, out._h, 0), cc._h)
+    check(lib.fides_mult_pt(cc._h, ct._h, pt._h, out._h, 0), cc._h)
     got = out.download()
     assert np.array_equal(got[0], oc.polymul(c0, m, pid)) and np.array_equal(got[1], oc.polymul(c1, m, pid))
     # the same limbs in COEFFICIENT form
     ptc = cc.import_raw_pt(list(oc.ntt(m, pid, inverse=True)), oc.primes[:level + 1], fmt=cc.FORMAT_COEFFICIENT)
     out2 = F.Ciphertext(cc)
-    check(lib.fides_mult_pt(cc._h, cc.upload(c0, c1)._h, ptc._h, out2._h, 0), cc._h)
+    check(lib.fides_mult_pt(cc._h, ct._h, ptc._h, out2._h, 0), cc._h)
     g2 = out2.download()
     assert np.array_equal(g2[0], got[0]) and np.array_equal(g2[1], got[1])
