@@ -79,8 +79,10 @@ const char* fides_ctx_last_error(const fides_ctx* ctx);
  * streams in ContextData, src/CKKS/Context.cuh:85-98). */
 fides_status fides_ctx_stream(const fides_ctx* ctx, void** stream);
 /* Autotuner: time every forward NTT variant (occupancy, twiddle-fetch
- * policy, integer or double-precision butterflies) and every inverse
- * configuration on this context's limb shapes and keep the fastest of each.
+ * policy, integer or double-precision butterflies, row twiddles staged or
+ * formed in the kernel) and every inverse configuration on one element's
+ * ModUp digits and on the same shape batched over four elements, and keep
+ * the fastest of each (sum of the two times).
  * Runs once in fides_ctx_create; call again to re-tune.  *variant receives
  * the forward variant, times_ms[v] (num_variants entries, at most 16) the
  * forward time of variant v plus that of its paired inverse configuration;
@@ -264,6 +266,13 @@ fides_status fides_plan_free(fides_ctx* ctx, fides_plan* plan);
  * dotProductPt_ (CKKS/ElemenwiseBatchKernels.cu:651). */
 fides_status fides_linear_transform(fides_ctx* ctx, const fides_ct* x, int n, const int32_t* offsets,
                                     const fides_pt* const* pts, int bstep, int rescale, fides_ct* out);
+/* The same transform applied to nx ciphertexts at one level (outs[u] for
+ * xs[u]): each input's baby steps share its own hoisted ModUp, the giant
+ * rotations of all inputs run as one batched key switch.  Results equal nx
+ * calls of fides_linear_transform. */
+fides_status fides_linear_transform_batch(fides_ctx* ctx, int nx, const fides_ct* const* xs, int n,
+                                          const int32_t* offsets, const fides_pt* const* pts, int bstep, int rescale,
+                                          fides_ct* const* outs);
 /* EvalConjugate: Ciphertext::conjugate, Ciphertext.cpp:933 */
 fides_status fides_conjugate(fides_ctx* ctx, const fides_ct* a, fides_ct* out);
 /* Apply an automorphism whose key was uploaded with fides_key_upload_galois */
@@ -320,6 +329,12 @@ fides_status fides_bootstrap_info(fides_ctx* ctx, int slots, int* output_level, 
 /* EvalBootstrap: refresh a ciphertext (only its limb 0 is read) to the
  * output level, same slots and message. */
 fides_status fides_bootstrap(fides_ctx* ctx, const fides_ct* in, fides_ct* out);
+/* EvalBootstrap of n ciphertexts of the same slot count together: the linear
+ * transforms batch their giant-step rotations over the inputs, and EvalMod
+ * runs the 2n real / imaginary lanes through one batched HMult per step.
+ * out[i] equals fides_bootstrap(in[i]) bit for bit.  No counterpart in the
+ * reference, which bootstraps one ciphertext per call (Bootstrap.cu:169-320). */
+fides_status fides_bootstrap_batch(fides_ctx* ctx, int n, const fides_ct* const* in, fides_ct* const* out);
 
 /* ---- serving: continuous batching over one context (no counterpart in the
  *      reference, which has no serving layer) ---- */

@@ -492,6 +492,16 @@ class CryptoContext:
         check(lib.fides_bootstrap(self._h, a._h, out._h), self._h)
         return out
 
+    def EvalBootstrapBatch(self, a_list, outs=None):
+        """EvalBootstrap of several ciphertexts together (batched EvalMod and
+        giant-step rotations); results equal one EvalBootstrap each."""
+        n = len(a_list)
+        outs = outs or [Ciphertext(self) for _ in range(n)]
+        A = (vp * n)(*[x._h for x in a_list])
+        O = (vp * n)(*[o._h for o in outs])
+        check(lib.fides_bootstrap_batch(self._h, n, A, O), self._h)
+        return outs
+
     # ---- diagonal-form linear transforms (baby-step giant-step) ----
     @staticmethod
     def linear_transform_rotations(offsets, bstep):
@@ -519,6 +529,17 @@ class CryptoContext:
             v = np.roll(np.asarray(diags[o], dtype=np.complex128), g * bstep)
             pts.append(self.MakeCKKSPackedPlaintext(v, level=level, slots=slots, scale=scale))
         return offs, pts
+
+    def EvalLinearTransformBatch(self, xs, offsets, pts, bstep, rescale=True, outs=None):
+        """The same diagonal-form transform of several ciphertexts at one level."""
+        n = len(xs)
+        outs = outs or [Ciphertext(self) for _ in range(n)]
+        X = (vp * n)(*[x._h for x in xs])
+        O = (vp * n)(*[o._h for o in outs])
+        off = (C.c_int32 * len(offsets))(*offsets)
+        P = (vp * len(pts))(*[p._h for p in pts])
+        check(lib.fides_linear_transform_batch(self._h, n, X, len(offsets), off, P, bstep, int(rescale), O), self._h)
+        return outs
 
     def EvalLinearTransform(self, x, offsets, pts, bstep, rescale=True, out=None):
         out = self._out(out)

@@ -130,6 +130,9 @@ EXPORTS = {
     "fides_bootstrap_info": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), i32p], C.c_int),
     "fides_bootstrap": ([vp, vp, vp], C.c_int),
     "fides_linear_transform": ([vp, vp, C.c_int, i32p, C.POINTER(vp), C.c_int, C.c_int, vp], C.c_int),
+    "fides_linear_transform_batch": ([vp, C.c_int, C.POINTER(vp), C.c_int, i32p, C.POINTER(vp), C.c_int, C.c_int,
+                                      C.POINTER(vp)], C.c_int),
+    "fides_bootstrap_batch": ([vp, C.c_int, C.POINTER(vp), C.POINTER(vp)], C.c_int),
     "fides_add_scalar": ([vp, vp, C.c_double, vp], C.c_int),
     "fides_mult_scalar": ([vp, vp, C.c_double, vp, C.c_int], C.c_int),
     "fides_srv_create": ([vp, C.c_size_t, C.c_int, C.c_int, C.POINTER(vp)], C.c_int),

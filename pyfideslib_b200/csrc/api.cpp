@@ -162,9 +162,31 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
         m.total += np;
     }
     // forward variants and inverse configurations are timed (and chosen)
-    // separately; tune_ms[v] reports forward v plus its paired inverse
+    // separately, each on one element's digits and on the same shape batched
+    // over four elements (the batched key switch's launches), the score being
+    // the sum; tune_ms[v] reports forward v plus its paired inverse
+    constexpr int kTuneElems = 4;
+    const size_t elem = (size_t)(c->L + c->dnum * (c->L + c->K)) * c->N;  // XT then the digits
+    uint64_t* tbuf = nullptr;
+    if (cudaMallocAsync((void**)&tbuf, kTuneElems * elem * sizeof(uint64_t), c->st) == cudaSuccess) {
+        cudaMemsetAsync(tbuf, 0, kTuneElems * elem * sizeof(uint64_t), c->st);
+    } else {
+        cudaGetLastError();
+        tbuf = nullptr;
+    }
+    LimbMap mb{};
+    if (tbuf) {
+        mb.nb = kTuneElems;
+        for (int sgi = 0; sgi < nseg; ++sgi) {
+            uint64_t* d0 = tbuf + (size_t)c->L * c->N + (size_t)sgi * np * c->N;
+            LimbMap one = map_single(d0, d0, np, np, 0);
+            one.seg[0].bstride = elem;
+            mb.seg[mb.nseg++] = one.seg[0];
+            mb.total += np;
+        }
+    }
     const int niv = ntt_num_inverse_variants();
-    std::vector<float> fwd_ms(nv, 1e30f), inv_ms(niv, 1e30f);
+    std::vector<float> fwd_ms(nv, 1e30f), inv_ms(niv, 1e30f), fwd_bms(nv, 1e30f), inv_bms(niv, 1e30f);
     for (int r = 0; r < kRounds; ++r) {
         for (int v = 0; v < nv; ++v) {
             c->dev.ntt_variant = v;
@@ -172,6 +194,10 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
             cudaEventRecord(e0, c->st);
             for (int k = 0; k < kReps; ++k) ntt_forward(c->dev, m, FL_PLAIN, FS_PLAIN, c->st);
             fwd_ms[v] = std::min(fwd_ms[v], elapsed() / kReps);
+            if (!tbuf) continue;
+            cudaEventRecord(e0, c->st);
+            for (int k = 0; k < kReps; ++k) ntt_forward(c->dev, mb, FL_PLAIN, FS_PLAIN, c->st);
+            fwd_bms[v] = std::min(fwd_bms[v], elapsed() / kReps);
         }
         for (int v = 0; v < niv; ++v) {
             c->dev.intt_variant = v;
@@ -179,7 +205,16 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
             cudaEventRecord(e0, c->st);
             for (int k = 0; k < kReps; ++k) ntt_inverse(c->dev, m, IL_PLAIN, IS_PLAIN, c->st);
             inv_ms[v] = std::min(inv_ms[v], elapsed() / kReps);
+            if (!tbuf) continue;
+            cudaEventRecord(e0, c->st);
+            for (int k = 0; k < kReps; ++k) ntt_inverse(c->dev, mb, IL_PLAIN, IS_PLAIN, c->st);
+            inv_bms[v] = std::min(inv_bms[v], elapsed() / kReps);
         }
+    }
+    if (tbuf) {
+        // the zero residues the batched timings transformed are reused below
+        for (int v = 0; v < nv; ++v) fwd_ms[v] += fwd_bms[v];
+        for (int v = 0; v < niv; ++v) inv_ms[v] += inv_bms[v];
     }
     c->tune_ms.assign(nv, 0.f);
     for (int v = 0; v < nv; ++v) c->tune_ms[v] = fwd_ms[v] + inv_ms[ntt_inverse_of(v)];
@@ -196,12 +231,8 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
     const bool tc_tune = conv_tc_supported(c->dev);  // tensor-core ModUp (int8 split)
     c->conv_ms.assign(kConvVariants, 0.f);
     int conv_best = 0;
-    constexpr int kTuneElems = 4;
     const int top = c->L - 1;
-    const size_t elem = (size_t)(c->L + c->dnum * (c->L + c->K)) * c->N;  // XT then the digits
-    uint64_t* tbuf = nullptr;
-    if (conv_supported(c->dev) &&
-        cudaMallocAsync((void**)&tbuf, kTuneElems * elem * sizeof(uint64_t), c->st) == cudaSuccess) {
+    if (conv_supported(c->dev) && tbuf) {
         cudaMemsetAsync(tbuf, 0, kTuneElems * elem * sizeof(uint64_t), c->st);
         uint64_t* xt = tbuf;
         uint64_t* dig = tbuf + (size_t)c->L * c->N;
@@ -217,14 +248,12 @@ fides_status fides_autotune(fides_ctx* c, int* variant, float* times_ms, int* nu
                 for (int k = 0; k < kReps; ++k) launch_modup_conv(c->dev, top, kTuneElems, xt, dig, dstride, elem, c->st);
                 best_ms[v] = std::min(best_ms[v], elapsed() / kReps);
             }
-        cudaFreeAsync(tbuf, c->st);
         for (int v = 0; v < kConvVariants; ++v) {
             c->conv_ms[v] = best_ms[v] < 1e29f ? best_ms[v] : 0.f;
             if (c->conv_ms[v] > 0.f && c->conv_ms[v] < c->conv_ms[conv_best]) conv_best = v;
         }
-    } else {
-        cudaGetLastError();  // no scratch for tuning: keep the default variant
     }
+    if (tbuf) cudaFreeAsync(tbuf, c->st);
     c->dev.conv_variant = conv_best;
     c->tuned_conv = conv_best;
     cudaEventDestroy(e0);
@@ -1062,9 +1091,20 @@ struct CtTemps {
 
 fides_status fides_linear_transform(fides_ctx* c, const fides_ct* x, int n, const int32_t* offsets,
                                     const fides_pt* const* pts, int bstep, int rescale, fides_ct* out) {
-    if (!c || !valid_ct(c, x) || n < 1 || !offsets || !pts || bstep < 1 || !out) return FIDES_BAD_ARG;
+    return fides_linear_transform_batch(c, 1, &x, n, offsets, pts, bstep, rescale, &out);
+}
+
+// The same transform of nx ciphertexts at one level: the baby steps are one
+// hoisted rotation group per input, the giant rotations of every input form
+// one batched key switch (nx times the elements per launch).
+fides_status fides_linear_transform_batch(fides_ctx* c, int nx, const fides_ct* const* xs, int n,
+                                          const int32_t* offsets, const fides_pt* const* pts, int bstep, int rescale,
+                                          fides_ct* const* outs) {
+    if (!c || nx < 1 || !xs || !outs || n < 1 || !offsets || !pts || bstep < 1) return FIDES_BAD_ARG;
+    for (int u = 0; u < nx; ++u)
+        if (!valid_ct(c, xs[u]) || !outs[u] || xs[u]->level != xs[0]->level) return FIDES_BAD_ARG;
     Guard g(c);
-    const int level = x->level, nl = level + 1, N = c->N;
+    const int level = xs[0]->level, nl = level + 1, N = c->N;
     for (int k = 0; k < n; ++k)
         if (!pts[k] || !pts[k]->m || pts[k]->level < level) return FIDES_BAD_ARG;
     std::vector<int> baby(n);
@@ -1077,51 +1117,57 @@ fides_status fides_linear_transform(fides_ctx* c, const fides_ct* x, int n, cons
         groups[gs].push_back(k);
     }
     CtTemps tmp{c, {}};
-    std::map<int, const fides_ct*> bct;
-    bct[0] = x;
     fides_status s = FIDES_OK;
-    if (!babies.empty()) {
-        std::vector<fides_ct*> outs;
-        for (size_t i = 0; i < babies.size(); ++i) outs.push_back(tmp.make());
-        s = fides_rotate_hoisted(c, x, (int)babies.size(), babies.data(), outs.data());
-        if (s != FIDES_OK) return s;
-        for (size_t i = 0; i < babies.size(); ++i) bct[babies[i]] = outs[i];
-    }
-    const double sc = x->scale * pts[0]->scale;
-    const int nd = x->noise_deg + pts[0]->noise_deg, sl = x->slots;
-    fides_ct* acc = tmp.make();
-    bool have_acc = false;
+    std::vector<fides_ct*> acc(nx);
+    std::vector<char> have_acc(nx, 0);
     std::vector<const fides_ct*> inner;
     std::vector<int32_t> gidx;
-    for (auto& kv : groups) {
-        const int gs = kv.first;
-        const std::vector<int>& ks = kv.second;
-        fides_ct* dst = gs == 0 ? acc : tmp.make();
-        s = ct_reserve(c, dst, level);
-        if (s != FIDES_OK) return s;
-        for (size_t k0 = 0; k0 < ks.size(); k0 += kMaxBatch) {
-            DotArgs d{};
-            d.n = (int)std::min(ks.size() - k0, (size_t)kMaxBatch);
-            d.accumulate = k0 > 0;
-            for (int j = 0; j < d.n; ++j) {
-                const fides_ct* b = bct[baby[ks[k0 + j]]];
-                d.c0[j] = b->c0();
-                d.c1[j] = b->c1(N);
-                d.p[j] = pts[ks[k0 + j]]->m;
-            }
-            d.o0 = dst->c0();
-            d.o1 = dst->c1(N);
-            launch_dot_pt(c->dev, nl, d, c->st);
+    std::vector<int> owner;  // input of each giant-step term
+    for (int u = 0; u < nx; ++u) {
+        const fides_ct* x = xs[u];
+        std::map<int, const fides_ct*> bct;
+        bct[0] = x;
+        if (!babies.empty()) {
+            std::vector<fides_ct*> bo;
+            for (size_t i = 0; i < babies.size(); ++i) bo.push_back(tmp.make());
+            s = fides_rotate_hoisted(c, x, (int)babies.size(), babies.data(), bo.data());
+            if (s != FIDES_OK) return s;
+            for (size_t i = 0; i < babies.size(); ++i) bct[babies[i]] = bo[i];
         }
-        dst->level = level;
-        dst->scale = sc;
-        dst->noise_deg = nd;
-        dst->slots = sl;
-        if (gs == 0) {
-            have_acc = true;
-        } else {
-            inner.push_back(dst);
-            gidx.push_back(gs * bstep);
+        const double sc = x->scale * pts[0]->scale;
+        const int nd = x->noise_deg + pts[0]->noise_deg, sl = x->slots;
+        acc[u] = tmp.make();
+        for (auto& kv : groups) {
+            const int gs = kv.first;
+            const std::vector<int>& ks = kv.second;
+            fides_ct* dst = gs == 0 ? acc[u] : tmp.make();
+            s = ct_reserve(c, dst, level);
+            if (s != FIDES_OK) return s;
+            for (size_t k0 = 0; k0 < ks.size(); k0 += kMaxBatch) {
+                DotArgs d{};
+                d.n = (int)std::min(ks.size() - k0, (size_t)kMaxBatch);
+                d.accumulate = k0 > 0;
+                for (int j = 0; j < d.n; ++j) {
+                    const fides_ct* b = bct[baby[ks[k0 + j]]];
+                    d.c0[j] = b->c0();
+                    d.c1[j] = b->c1(N);
+                    d.p[j] = pts[ks[k0 + j]]->m;
+                }
+                d.o0 = dst->c0();
+                d.o1 = dst->c1(N);
+                launch_dot_pt(c->dev, nl, d, c->st);
+            }
+            dst->level = level;
+            dst->scale = sc;
+            dst->noise_deg = nd;
+            dst->slots = sl;
+            if (gs == 0) {
+                have_acc[u] = 1;
+            } else {
+                inner.push_back(dst);
+                gidx.push_back(gs * bstep);
+                owner.push_back(u);
+            }
         }
     }
     if (!inner.empty()) {
@@ -1129,28 +1175,35 @@ fides_status fides_linear_transform(fides_ctx* c, const fides_ct* x, int n, cons
         for (size_t i = 0; i < inner.size(); ++i) rot.push_back(tmp.make());
         s = fides_rotate_batch(c, (int)inner.size(), inner.data(), gidx.data(), rot.data());
         if (s != FIDES_OK) return s;
-        size_t i0 = 0;
-        if (!have_acc) {
-            s = ct_reserve(c, acc, level);
-            if (s != FIDES_OK) return s;
-            const size_t bytes = (size_t)nl * c->limb_bytes();
-            cudaMemcpyAsync(acc->c0(), rot[0]->c0(), bytes, cudaMemcpyDeviceToDevice, c->st);
-            cudaMemcpyAsync(acc->c1(N), rot[0]->c1(N), bytes, cudaMemcpyDeviceToDevice, c->st);
-            i0 = 1;
-        }
-        for (size_t i = i0; i < rot.size(); ++i) {
-            launch_elementwise(c->dev, EW_ADD, nl, 0, acc->c0(), rot[i]->c0(), acc->c0(), c->st);
-            launch_elementwise(c->dev, EW_ADD, nl, 0, acc->c1(N), rot[i]->c1(N), acc->c1(N), c->st);
+        const size_t bytes = (size_t)nl * c->limb_bytes();
+        for (size_t i = 0; i < rot.size(); ++i) {
+            fides_ct* a = acc[owner[i]];
+            if (!have_acc[owner[i]]) {
+                s = ct_reserve(c, a, level);
+                if (s != FIDES_OK) return s;
+                cudaMemcpyAsync(a->c0(), rot[i]->c0(), bytes, cudaMemcpyDeviceToDevice, c->st);
+                cudaMemcpyAsync(a->c1(N), rot[i]->c1(N), bytes, cudaMemcpyDeviceToDevice, c->st);
+                have_acc[owner[i]] = 1;
+                continue;
+            }
+            launch_elementwise(c->dev, EW_ADD, nl, 0, a->c0(), rot[i]->c0(), a->c0(), c->st);
+            launch_elementwise(c->dev, EW_ADD, nl, 0, a->c1(N), rot[i]->c1(N), a->c1(N), c->st);
         }
     }
-    commit(c, out, *acc);
-    out->level = level;
-    out->scale = sc;
-    out->noise_deg = nd;
-    out->slots = sl;
-    s = check_cuda(c, "linear_transform");
-    if (s == FIDES_OK && rescale && level > 0) s = fides_rescale(c, out, out);
-    return s;
+    for (int u = 0; u < nx; ++u) {
+        const double sc = xs[u]->scale * pts[0]->scale;
+        const int nd = xs[u]->noise_deg + pts[0]->noise_deg, sl = xs[u]->slots;
+        commit(c, outs[u], *acc[u]);
+        outs[u]->level = level;
+        outs[u]->scale = sc;
+        outs[u]->noise_deg = nd;
+        outs[u]->slots = sl;
+        if (rescale && level > 0) {
+            s = fides_rescale(c, outs[u], outs[u]);
+            if (s != FIDES_OK) return s;
+        }
+    }
+    return check_cuda(c, "linear_transform");
 }
 
 }  // extern "C"

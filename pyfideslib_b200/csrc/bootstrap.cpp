@@ -691,37 +691,49 @@ fides_status fides_bootstrap_info(fides_ctx* c, int slots, int* output_level, in
 }
 
 fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
-    if (!c || !in || !in->buf || !out) return FIDES_BAD_ARG;
+    return fides_bootstrap_batch(c, 1, &in, &out);
+}
+
+fides_status fides_bootstrap_batch(fides_ctx* c, int nin, const fides_ct* const* in, fides_ct* const* out) {
+    if (!c || nin < 1 || !in || !out) return FIDES_BAD_ARG;
+    for (int u = 0; u < nin; ++u)
+        if (!in[u] || !in[u]->buf || !out[u]) return FIDES_BAD_ARG;
     Guard g(c);
-    const int n = in->slots > 0 ? in->slots : c->N / 2;
+    const int n = in[0]->slots > 0 ? in[0]->slots : c->N / 2;
+    for (int u = 1; u < nin; ++u)
+        if ((in[u]->slots > 0 ? in[u]->slots : c->N / 2) != n)
+            return set_err(c, FIDES_BAD_ARG, "batched bootstrap: inputs with different slot counts");
     auto it = c->boot.find(n);
     if (it == c->boot.end()) return set_err(c, FIDES_BAD_ARG, "bootstrapping not set up for these slots");
     const BootPrecomp& B = *it->second;
     if (!c->has_relin) return set_err(c, FIDES_KEY_MISSING, "no relinearisation key");
     const int N = c->N;
-    const double d_in = in->scale;
+    const size_t k = (size_t)nin;
     Arith A(c);
-    Lanes x = A.fresh(1);
+    Lanes x = A.fresh(k);
     fides_status s = FIDES_OK;
-    if (B.correction > 0) {
-        // message times 2^correction (exact integer product of limb 0 and up)
-        Lanes pre = A.fresh(1);
-        if ((s = fides_mult_int(c, in, (int64_t)1 << B.correction, pre[0])) != FIDES_OK) return s;
-        s = fides_mod_raise(c, pre[0], x[0]);
-    } else {
-        s = fides_mod_raise(c, in, x[0]);
+    for (size_t u = 0; u < k; ++u) {
+        if (B.correction > 0) {
+            // message times 2^correction (exact integer product of limb 0 and up)
+            Lanes pre = A.fresh(1);
+            if ((s = fides_mult_int(c, in[u], (int64_t)1 << B.correction, pre[0])) != FIDES_OK) return s;
+            s = fides_mod_raise(c, pre[0], x[u]);
+        } else {
+            s = fides_mod_raise(c, in[u], x[u]);
+        }
+        if (s != FIDES_OK) return s;
+        x[u]->scale = B.K * (double)c->host.prime[0];
+        x[u]->slots = n;
     }
-    if (s != FIDES_OK) return s;
-    x[0]->scale = B.K * (double)c->host.prime[0];
-    x[0]->slots = n;
     // CoeffsToSlots from the scale K q0 (about 2^64, growing by 2^8 per
     // transform): its rescaling and key-switching noise and the rounding of
     // its diagonals stay small against t, whose error EvalMod multiplies by
     // 2 pi K and SlotsToCoeffs by about sqrt(n) q0 / (2 pi D)
     for (const BootStage& st : B.cts) {
-        Lanes y = A.fresh(1);
-        s = fides_linear_transform(c, x[0], (int)st.offsets.size(), st.offsets.data(),
-                                   (const fides_pt* const*)st.pts.data(), st.bstep, 1, y[0]);
+        Lanes y = A.fresh(k);
+        s = fides_linear_transform_batch(c, nin, (const fides_ct* const*)x.data(), (int)st.offsets.size(),
+                                         st.offsets.data(), (const fides_pt* const*)st.pts.data(), st.bstep, 1,
+                                         y.data());
         if (s != FIDES_OK) return s;
         x = y;
     }
@@ -733,15 +745,20 @@ fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
     x = A.normalize(x, 0.5 * (double)c->host.prime[B.level_after_cts]);
     if (!A.ok()) return A.st;
     // real and imaginary parts: (x + conj x), -i (x - conj x), each twice the part
-    Lanes cj = A.fresh(1);
-    if ((s = fides_conjugate(c, x[0], cj[0])) != FIDES_OK) return s;
+    Lanes cj = A.fresh(k);
+    for (size_t u = 0; u < k; ++u)
+        if ((s = fides_conjugate(c, x[u], cj[u])) != FIDES_OK) return s;
     Lanes re = A.ilin({{&x, 1}, {&cj, 1}}, 0.0, x[0]->level);
     Lanes df = A.ilin({{&x, 1}, {&cj, -1}}, 0.0, x[0]->level);
     Lanes im = A.monomial(df, 3u * (uint32_t)N / 2u);
     if (!A.ok()) return A.st;
-    re[0]->scale *= 2.0;
-    im[0]->scale *= 2.0;
-    Lanes v = {re[0], im[0]};
+    for (size_t u = 0; u < k; ++u) {
+        re[u]->scale *= 2.0;
+        im[u]->scale *= 2.0;
+    }
+    // 2k lanes in lockstep: real parts, then imaginary parts
+    Lanes v(re);
+    v.insert(v.end(), im.begin(), im.end());
     {
         const auto Lv = Chebyshev::plan_levels(v[0]->level, B.degree);
         const int lv = Chebyshev::feasible(Lv, B.degree);
@@ -754,23 +771,32 @@ fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
     }
     if (!A.ok()) return A.st;
     if (v[0]->level != B.level_after_mod) return set_err(c, FIDES_CUDA_ERR, "bootstrap level plan mismatch");
-    Lanes y0 = {v[0]}, y1 = {v[1]};
+    Lanes y0(v.begin(), v.begin() + k), y1(v.begin() + k, v.end());
     Lanes iy = A.monomial(y1, (uint32_t)N / 2u);
     Lanes w = A.ilin({{&y0, 1}, {&iy, 1}}, 0.0, v[0]->level);
     if (!A.ok()) return A.st;
     for (const BootStage& st : B.stc) {
-        Lanes y = A.fresh(1);
-        s = fides_linear_transform(c, w[0], (int)st.offsets.size(), st.offsets.data(),
-                                   (const fides_pt* const*)st.pts.data(), st.bstep, 1, y[0]);
+        Lanes y = A.fresh(k);
+        s = fides_linear_transform_batch(c, nin, (const fides_ct* const*)w.data(), (int)st.offsets.size(),
+                                         st.offsets.data(), (const fides_pt* const*)st.pts.data(), st.bstep, 1,
+                                         y.data());
         if (s != FIDES_OK) return s;
         w = y;
     }
-    const double sc = w[0]->scale * d_in / c->default_scale * (double)(1ll << B.correction);
-    s = fides_ct_copy(c, w[0], out);
-    if (s != FIDES_OK) return s;
-    out->scale = sc;
-    out->slots = in->slots;
-    out->noise_deg = 1;
+    // outputs last: an output may alias an input
+    std::vector<double> sc(k);
+    std::vector<int> slots(k);
+    for (size_t u = 0; u < k; ++u) {
+        sc[u] = w[u]->scale * in[u]->scale / c->default_scale * (double)(1ll << B.correction);
+        slots[u] = in[u]->slots;
+    }
+    for (size_t u = 0; u < k; ++u) {
+        s = fides_ct_copy(c, w[u], out[u]);
+        if (s != FIDES_OK) return s;
+        out[u]->scale = sc[u];
+        out[u]->slots = slots[u];
+        out[u]->noise_deg = 1;
+    }
     return check_cuda(c, "bootstrap");
 }
 

@@ -317,6 +317,43 @@ __device__ __forceinline__ void sg_stage2(uint64_t (&x)[16], const ulonglong2 (&
     if constexpr (KB > 0) sg_stage2<KB - 1>(x, d, gw, p, pinv);
 }
 
+// The inverse row pass of configuration 5 takes its twiddles the same way
+// from the inverse table: its first four stages (s' = 7..4) form the
+// per-thread ones from D_s' and psi^-1_br[g], its last four (s' = 3..0)
+// read the row's 15 from shared memory.  The GS sums are centred at every
+// stage already; the differences stay below 1.6p.
+template <int KB>
+__device__ __forceinline__ void sg_inv_stageA(uint64_t (&x)[16], const ulonglong2 (&d)[4], const double* gw,
+                                              uint64_t p, uint64_t pinv) {
+    constexpr int t = 7 - KB, NG = 8 >> KB;
+    const ulonglong2 D = d[t - 4];
+    ulonglong2 w[NG];
+    w[0] = D;
+#pragma unroll
+    for (int g = 1; g < NG; ++g) {
+        const double wd = fp_mulmod(as_f64(D.x), gw[g], as_f64(p), as_f64(pinv));
+        w[g].x = as_u64(wd);
+        w[g].y = as_u64(__dmul_rn(wd, as_f64(pinv)));
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        if (k & (1 << KB)) continue;
+        bfly<5, 0>(x[k], x[k | (1 << KB)], w[k >> (KB + 1)], p, pinv);
+    }
+    if constexpr (KB < 3) sg_inv_stageA<KB + 1>(x, d, gw, p, pinv);
+}
+
+template <int KB>
+__device__ __forceinline__ void sg_inv_stageB(uint64_t (&x)[16], const ulonglong2* g1, uint64_t p, uint64_t pinv) {
+    constexpr int t = 3 - KB;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        if (k & (1 << KB)) continue;
+        bfly<5, 0>(x[k], x[k | (1 << KB)], g1[(1 << t) - 1 + (k >> (KB + 1))], p, pinv);
+    }
+    if constexpr (KB < 3) sg_inv_stageB<KB + 1>(x, g1, p, pinv);
+}
+
 // Tile geometry shared by kernels and launchers.
 template <int LR, int LC>
 struct Geo {
@@ -710,12 +747,15 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constan
 // ---------------------------------------------------------------------------
 // Prologue modes of the inverse row pass (per segment): IL_PLAIN reads `in`,
 // IL_MUL the product in*in2, IL_AXPY_PINV in + in2*P^-1.
-template <int LR, int LC, int MINB, bool PF, bool FP>
+template <int LR, int LC, int MINB, bool PF, bool FP, bool SG = false>
 __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ LimbMap map) {
     using G = Geo<LR, LC>;
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
+    constexpr bool kSG = SG && FP && LC == 8;
     __shared__ __align__(16) uint64_t sm[TR * CP];
+    __shared__ ulonglong2 s_g1[kSG ? TR * 16 : 1];  // last four stages' twiddles per row, entry 2^t - 1 + g
+    __shared__ double s_gw[kSG ? 8 : 1];            // psi^-1_br[g], g < 8
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
@@ -755,20 +795,42 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
             sm[(i / C) * CP + padi(i % C)] = v[q];
         }
     }
+    // configuration 5: this thread's D_s' and the rows' staged twiddles
+    ulonglong2 dtw[kSG ? 4 : 1];
+    if constexpr (kSG) {
+        if (imode == 5) {
+#pragma unroll
+            for (int t = 4; t < 8; ++t) dtw[t - 4] = ldg2(twg, ((size_t)(R + row) << t) + ((size_t)th << (t - 4)));
+            const ulonglong2* tw2 = reinterpret_cast<const ulonglong2*>(twg);
+            for (int e = threadIdx.x; e < TR * 15; e += NT) {
+                const int r = e / 15, j = e % 15, t = 31 - __clz(j + 1);
+                s_g1[r * 16 + j] = tw2[((size_t)(R + blockIdx.x * TR + r) << t) + (j + 1 - (1 << t))];
+            }
+            if (threadIdx.x < 8) s_gw[threadIdx.x] = as_f64(tw2[threadIdx.x].x);
+        }
+    }
     __syncthreads();
 
     uint64_t* srow = sm + rl * CP;
     if constexpr (LC > 4) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-        inv_group<0, LC - 5, PF, FP>(imode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
+        if (kSG && imode == 5) {
+            if constexpr (kSG) sg_inv_stageA<0>(x, dtw, s_gw, kk.k0, kk.k1);
+        } else {
+            inv_group<0, LC - 5, PF, FP>(imode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
+        }
 #pragma unroll
         for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
         __syncthreads();
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) x[k] = srow[padi(th + (k << (LC - 4)))];
-    inv_group<0, 3, PF, FP>(imode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+    if (kSG && imode == 5) {
+        if constexpr (kSG) sg_inv_stageB<0>(x, s_g1 + rl * 16, kk.k0, kk.k1);
+    } else {
+        inv_group<0, 3, PF, FP>(imode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+    }
     // double-precision limbs leave as doubles below 0.6p in magnitude; the
     // column pass continues on them without converting
     uint64_t* dst = lr.out + (size_t)row * C;
@@ -865,15 +927,16 @@ bool ntt_supported(int logN) { return logN >= 8 && logN <= 16; }
 // SM, 9: column pass of 5 with a row pass whose twiddles are staged in
 // shared memory or formed from a staged factor (sg_stage1 / sg_stage2, C =
 // 256 only; other sizes run variant 5's row pass).  Inverse configurations:
-// 0 (2, group prefetch),
+// 5: configuration 3 with the row pass's twiddles staged or formed the
+// same way (sg_inv_stageA / sg_inv_stageB); 0 (2, group prefetch),
 // 1 (3, per-stage), 2 (4, per-stage), 3 and 4: as 1 and 0 with
 // double-precision butterflies for primes below 2^50; ntt_inverse_of(v)
 // pairs each forward variant with an inverse configuration of the same
 // arithmetic.
 int ntt_num_variants() { return 10; }
-int ntt_num_inverse_variants() { return 5; }
+int ntt_num_inverse_variants() { return 6; }
 int ntt_inverse_of(int v) {
-    static const int inv[10] = {0, 1, 2, 1, 0, 3, 4, 3, 3, 3};
+    static const int inv[10] = {0, 1, 2, 1, 0, 3, 4, 3, 3, 5};
     return v >= 0 && v < 10 ? inv[v] : 0;
 }
 
@@ -888,14 +951,14 @@ static void launch_fwd_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st)
     k_ntt_fwd_rows<LR, LC, MINB, PF, AQ, FP><<<g2, G::NTR, 0, st>>>(ctx, map);
 }
 
-template <int LR, int LC, int MINB, bool PF, bool FP>
+template <int LR, int LC, int MINB, bool PF, bool FP, bool SG = false>
 static void launch_inv_v(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
     using G = Geo<LR, LC>;
     // grid (tiles, batch element, limb): CTAs run x fastest, then y, so the
     // elements of a batch that share a prime run together and its twiddle
     // table is fetched from HBM once per launch rather than once per element
     dim3 g1(G::C / G::TC, map.nb > 0 ? map.nb : 1, map.total), g2(G::R / G::TR, map.nb > 0 ? map.nb : 1, map.total);
-    k_ntt_inv_rows<LR, LC, MINB, PF, FP><<<g2, G::NTR, 0, st>>>(ctx, map);
+    k_ntt_inv_rows<LR, LC, MINB, PF, FP, SG><<<g2, G::NTR, 0, st>>>(ctx, map);
     k_ntt_inv_cols<LR, LC, MINB, PF, FP><<<g1, G::NTC, 0, st>>>(ctx, map);
 }
 
@@ -932,6 +995,7 @@ static void launch_inv(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
         case 2: launch_inv_v<LR, LC, 4, false, false>(ctx, map, st); break;
         case 3: launch_inv_v<LR, LC, 3, false, true>(ctx, map, st); break;
         case 4: launch_inv_v<LR, LC, 2, true, true>(ctx, map, st); break;
+        case 5: launch_inv_v<LR, LC, 3, false, true, true>(ctx, map, st); break;
         default: launch_inv_v<LR, LC, 2, true, false>(ctx, map, st); break;
     }
 }

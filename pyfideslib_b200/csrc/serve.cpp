@@ -5,8 +5,11 @@
 // -- HMult / Rotate grouped by operation and level, up to max_batch per
 // batch -- and launches each batch on the next free stream; every stream owns
 // a key-switch workspace, so a batch admitted while others are still running
-// overlaps them on the device.  Bootstraps run one at a time on their own
-// lane (the context stream and workspaces), beside the batches.  Admission is against a fixed HBM budget: the workspaces are
+// overlaps them on the device.  Bootstraps run on their own lane (the
+// context stream and workspaces), beside the batches: the pending ones, up
+// to min(max_batch, kBootBatch), go through one batched EvalBootstrap (its
+// EvalMod lanes share every HMult, its linear transforms every giant-step
+// key switch).  Admission is against a fixed HBM budget: the workspaces are
 // charged once at start-up, and every admitted request reserves its output
 // buffer until the request completes.  Completion is detected with one CUDA
 // event per batch; the caller waits on a request id.  Ciphertexts and keys
@@ -27,6 +30,9 @@
 
 using namespace fides;
 using clk = std::chrono::steady_clock;
+
+// bootstraps batched together at most (each adds two EvalMod lanes)
+constexpr int kBootBatch = 4;
 
 namespace {
 
@@ -87,10 +93,18 @@ void launch_batch(fides_server* s, Lane& ln) {
     const int op = ln.batch[0]->op;
     const int level = ln.batch[0]->level;
     if (op == FIDES_OP_BOOTSTRAP) {
-        // one request; queued on the context stream by the host-side orchestration
-        Request* r = ln.batch[0];
-        r->t_start = clk::now();
-        r->status = fides_bootstrap(c, r->a, r->out);
+        // the batch's bootstraps together (one batched EvalMod, batched
+        // giant-step rotations), queued on the context stream by the
+        // host-side orchestration
+        std::vector<const fides_ct*> in;
+        std::vector<fides_ct*> outs;
+        for (Request* r : ln.batch) {
+            r->t_start = clk::now();
+            in.push_back(r->a);
+            outs.push_back(r->out);
+        }
+        const fides_status st = fides_bootstrap_batch(c, (int)in.size(), in.data(), outs.data());
+        for (Request* r : ln.batch) r->status = st;
         cudaEventRecord(ln.ev, ln.st);
         ln.busy = true;
         return;
@@ -223,14 +237,27 @@ void scheduler(fides_server* s) {
             lk.lock();
             any_busy = true;
         }
-        // the oldest bootstrap, when its lane is free and the budget allows
+        // the oldest bootstraps, up to max_batch with the same slot count,
+        // when their lane is free and the budget allows
         if (!s->boot.busy) {
             auto hit = std::find_if(s->pending.begin(), s->pending.end(), [](Request* r) { return is_boot(r); });
             if (hit != s->pending.end() && s->reserved + (*hit)->bytes <= s->budget) {
-                Request* r = *hit;
-                s->pending.erase(hit);
-                s->reserved += r->bytes;
-                s->boot.batch = {r};
+                const int slots = (*hit)->a->slots;
+                std::vector<Request*> pick;
+                size_t need = 0;
+                const int cap = std::min(s->max_batch, kBootBatch);
+                for (auto it = hit; it != s->pending.end() && (int)pick.size() < cap;) {
+                    Request* r = *it;
+                    if (is_boot(r) && r->a->slots == slots && s->reserved + need + r->bytes <= s->budget) {
+                        need += r->bytes;
+                        pick.push_back(r);
+                        it = s->pending.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
+                s->reserved += need;
+                s->boot.batch = std::move(pick);
                 s->batches++;
                 lk.unlock();
                 {

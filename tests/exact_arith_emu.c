@@ -105,12 +105,15 @@ static uint64_t splitmix(uint64_t* s) {
  * that do not come back (inverse), or -1 if a value left its proven range. */
 static int ntt_check_impl(uint64_t p, uint64_t psi, uint64_t seed, int pattern, int gen);
 
-/* Forward variant 10: the row pass's first four stages (8..11) take their
+/* Forward variant 9 and its inverse: the row pass's first four stages (8..11) take their
  * twiddles exactly from the table (staged in shared memory) and centre X on
  * even positions as before; its last four (12..15) centre X at every stage
  * and form the twiddle of group offset g > 0 as fp_mulmod(D, psi_br[g])
  * (|w| <= 0.875p, not reduced) with the quotient companion fl(w * pinv_up),
- * D = psi_br[index - g] exact from the table; g = 0 uses D itself. */
+ * D = psi_br[index - g] exact from the table; g = 0 uses D itself.  The
+ * inverse's row pass (its first eight stages) forms its per-thread
+ * twiddles the same way from the inverse table; its sums are centred at
+ * every stage already. */
 int emu_ntt_sg_check(uint64_t p, uint64_t psi, uint64_t seed, int pattern) {
     return ntt_check_impl(p, psi, seed, pattern, 2);
 }
@@ -205,13 +208,26 @@ static int ntt_check_impl(uint64_t p, uint64_t psi, uint64_t seed, int pattern, 
         for (int j = 0; j < N; ++j) d[j] = (double)e[j];
         int stg = 0;
         for (int m = N / 2, t = 1; m > 1; m >>= 1, t <<= 1, ++stg) {
-            for (int i = 0; i < m; ++i)
+            for (int i = 0; i < m; ++i) {
+                /* variant 10's inverse row pass (m >= 2^12): the twiddles of
+                 * group offset g > 0 are fp_mulmod(D, psi^-1_br[g]) with the
+                 * companion fl(w * pinv_up), as in the forward row pass */
+                double w = IW[m + i], wq = IWQ[m + i];
+                if (gen == 2 && m >= (1 << 12)) {
+                    const int g = i & ((m >> 12) - 1);
+                    if (g) {
+                        w = fp_mulmod(IW[m + i - g], IW[g], pd, pinv);
+                        wq = w * pinv;
+                    }
+                }
                 for (int j = 2 * i * t; j < 2 * i * t + t; ++j) {
                     const double x = d[j], y = d[j + t];
                     if (fabs(x - y) >= 2251799813685248.0) { bad = -1; goto done; }
+                    if (gen == 2 && fabs(x - y) >= 1.6 * pd) { bad = -1; goto done; }
                     d[j] = fp_center(x + y, pd, pinv);
-                    d[j + t] = fp_mulw(x - y, IW[m + i], IWQ[m + i], pd);
+                    d[j + t] = fp_mulw(x - y, w, wq, pd);
                 }
+            }
         }
         const double a0 = (double)ninv, a1 = (double)s1, a0q = a0 / pd, a1q = a1 / pd;
         for (int j = 0; j < N / 2; ++j) {

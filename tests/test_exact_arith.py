@@ -105,9 +105,11 @@ def test_fp64_ntt_generated_row_twiddles_exact(emu, p):
 
 @pytest.mark.parametrize("p", PRIMES_50)
 def test_fp64_ntt_staged_generated_row_twiddles_exact(emu, p):
-    """Forward variant 10: exact staged twiddles for the row pass's first
-    four stages, products of a table entry and psi_br[g] (unreduced, sloppy
-    quotient companion) for the last four, which centre X at every stage."""
+    """Forward variant 9 and its inverse configuration: exact staged twiddles
+    for the forward row pass's first four stages, products of a table entry
+    and psi_br[g] (unreduced, sloppy quotient companion) for the last four,
+    which centre X at every stage; the inverse row pass forms its per-thread
+    twiddles the same way."""
     psi = _psi(p)
     for pattern in (0, 1, 2):
         assert emu.emu_ntt_sg_check(p, psi, 3000 + pattern, pattern) == 0, pattern

@@ -154,3 +154,50 @@ def test_bootstrap_requests_served_in_mix():
             alone = cc.EvalRotate(a, r)
         g, w = out.download(), alone.download()
         assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1]), op
+
+
+def test_bootstrap_batch_equals_single():
+    """fides_bootstrap_batch: the batched EvalMod lanes and giant-step
+    rotations give every input the residues of its own EvalBootstrap."""
+    import pyfideslib_b200 as F
+
+    cc = F.CryptoContext(log_n=12, num_q=20, dnum=4)
+    sk = cc.KeyGen(seed=12, hamming_weight=32)
+    cc.EvalMultKeyGen(sk)
+    cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=63)
+    cc.EvalBootstrapKeyGen(sk)
+    slots = cc.N // 2
+    rng = np.random.default_rng(12)
+    msgs = [rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots) for _ in range(3)]
+    cts = [cc.Encrypt(sk, m, slots=slots, level=i, seed=40 + i) for i, m in enumerate(msgs)]
+    outs = cc.EvalBootstrapBatch(cts)
+    for ct, o, m in zip(cts, outs, msgs):
+        w = cc.EvalBootstrap(ct).download()
+        g = o.download()
+        assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1])
+        assert np.max(np.abs(cc.Decrypt(sk, o, slots=slots) - m)) < 2 ** -14
+
+
+def test_bootstrap_requests_batched_in_serving():
+    """Several bootstraps submitted together are served as one batched
+    bootstrap; each result equals the call made alone."""
+    import pyfideslib_b200 as F
+
+    cc = F.CryptoContext(log_n=12, num_q=20, dnum=4)
+    sk = cc.KeyGen(seed=13, hamming_weight=32)
+    cc.EvalMultKeyGen(sk)
+    cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=63)
+    cc.EvalBootstrapKeyGen(sk)
+    slots = cc.N // 2
+    rng = np.random.default_rng(13)
+    cts = [cc.Encrypt(sk, rng.uniform(-1, 1, slots), slots=slots, level=0, seed=60 + i) for i in range(5)]
+    srv = F.Server(cc, hbm_budget=16 << 30, max_batch=4, num_streams=1)
+    outs = [srv.submit(F.Server.BOOTSTRAP, c) for c in cts]
+    for rid, _ in outs:
+        srv.wait(rid, 120.0)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == 5 and st["batches"] < 5  # some were batched
+    for c, (_, o) in zip(cts, outs):
+        g, w = o.download(), cc.EvalBootstrap(c).download()
+        assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1])

@@ -102,3 +102,21 @@ def test_linear_transform_matches_fp64(offsets, bstep):
     err = np.max(np.abs(got - want))
     assert err < 1e-6, err
     assert y.level == ct.level - 1
+
+
+def test_linear_transform_batch_equals_single():
+    """One transform of several ciphertexts (giant rotations batched over
+    the inputs) equals one call per ciphertext, bit for bit."""
+    import pyfideslib_b200 as F
+
+    cc, oc = make_pair(12, 8, 3, 3)
+    level, offsets, bstep = 6, [-7, -3, -1, 0, 2, 5, 9, 13], 4
+    for i, r in enumerate(F.CryptoContext.linear_transform_rotations(offsets, bstep)):
+        cc.upload_galois_key(cc.rotation_galois(r), *rand_key(oc, 700 + 2 * i))
+    xs = [cc.upload(*rand_ct(oc, level, 800 + 2 * u)) for u in range(3)]
+    pts = [_upload_pt(cc, oc.random(list(range(level + 1)), 850 + k), level) for k in range(len(offsets))]
+    outs = cc.EvalLinearTransformBatch(xs, offsets, pts, bstep, rescale=True)
+    for x, o in zip(xs, outs):
+        w = cc.EvalLinearTransform(x, offsets, pts, bstep, rescale=True).download()
+        g = o.download()
+        assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1])
