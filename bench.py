@@ -570,6 +570,14 @@ def run_ours(args):
 
     with ClockSampler(local) as clk:
         ms, launches = timed(step_batched, args.steps, args.warmup)
+    if args.profile_step:
+        # one more batched step between profiler marks: what an ncu capture
+        # started with --profile-from-start off sees
+        cc.Synchronize()
+        torch.cuda.profiler.start()
+        step_batched()
+        cc.Synchronize()
+        torch.cuda.profiler.stop()
     ms_op, _ = timed(step_per_op, max(1, args.steps // 2), 2)
     ms_e2e, _ = timed(step_e2e, max(1, args.steps // 2), 1)
 
@@ -705,6 +713,8 @@ def main():
                     help="force the key-switch inner-product arithmetic: 0 integer, 1 FP64 (default: the context's)")
     ap.add_argument("--profile-roofline", action="store_true",
                     help="mark the roofline NTT loop for ncu --profile-from-start off")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="mark one batched HMult step (after the timed region) for ncu --profile-from-start off")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
