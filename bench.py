@@ -282,8 +282,22 @@ def measure_bootstrap(cc, reps=3, seed=101, degree=119):
     bt6 = cc.EvalBootstrap(cts[0])
     err6 = float(np.max(np.abs(cc.Decrypt(sk, bt6, slots=slots) - msgs[0])))
     cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=degree)
+    # several bootstraps in one batched call (EvalMod lanes and giant-step
+    # rotations shared): time per call
+    batch_ms = {}
+    for nb in (2, 4):
+        ins = [cts[i % 2] for i in range(nb)]
+        cc.EvalBootstrapBatch(ins)
+        cc.Synchronize()
+        e0.record(st)
+        outs_b = cc.EvalBootstrapBatch(ins)
+        e1.record(st)
+        e1.synchronize()
+        batch_ms[nb] = e0.elapsed_time(e1)
+        del outs_b
     res = {"bootstrap_ms": ms, "wall_ms": wall_ms, "precision_bits": -float(np.log2(err)), "max_abs_err": err,
            "precision_bits_correction6": -float(np.log2(err6)),
+           "batched_bootstrap_ms": {str(k): v for k, v in batch_ms.items()},
            "output_level": out_level, "rotation_keys": len(rots), "setup_s": setup_s,
            "params": "N=2^16 L=30 K=%d dnum=3, 2^15 slots, h=32, budget {3,3}, Chebyshev degree %d, K=16, "
                      "3 double-angle steps" % (cc.K, degree)}
@@ -304,9 +318,11 @@ def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_
     import pyfideslib_b200 as F
 
     rng = np.random.default_rng(seed)
+    # inputs at every level of the valid range (1..L-1: HMult consumes one),
+    # two resident ciphertexts per level; requests draw a level uniformly
     pool = {}
-    for lv in (29, 22, 15, 8):
-        pool[lv] = [cc.random_ct(lv, 1000 * lv + i) for i in range(4)]
+    for lv in range(1, cc.L):
+        pool[lv] = [cc.random_ct(lv, 1000 * lv + i) for i in range(2)]
     out = []
     srv = F.Server(cc, hbm_budget=40 << 30, max_batch=max_batch, num_streams=num_streams)
     p_rot = (1.0 - boot_share) / 3.0
@@ -344,9 +360,9 @@ def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_
                 q.put(srv.submit(F.Server.BOOTSTRAP, boot_inputs[int(rng.integers(0, len(boot_inputs)))]))
             else:
                 lv = list(pool)[int(rng.integers(0, len(pool)))]
-                a = pool[lv][int(rng.integers(0, 4))]
+                a = pool[lv][int(rng.integers(0, 2))]
                 if u < 1.0 - p_rot:
-                    q.put(srv.submit(F.Server.HMULT, a, pool[lv][int(rng.integers(0, 4))]))
+                    q.put(srv.submit(F.Server.HMULT, a, pool[lv][int(rng.integers(0, 2))]))
                 else:
                     q.put(srv.submit(F.Server.ROTATE, a, None,
                                      rot_indices[int(rng.integers(0, len(rot_indices)))]))
@@ -364,7 +380,8 @@ def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_
     srv.close()
     mix = "%.0f%% HMult+Relin+Rescale, %.0f%% Rotate, %.0f%% EvalBootstrap" % (
         100 * (1 - boot_share - p_rot), 100 * p_rot, 100 * boot_share)
-    return {"mix": mix, "params": "N=2^16 L=30 K=10 dnum=3, levels 29/22/15/8 (bootstrap inputs at level 0)",
+    return {"mix": mix, "params": "N=2^16 L=30 K=10 dnum=3, HMult/Rotate inputs at levels uniform in 1..29, "
+                                  "bootstrap inputs at level 0",
             "streams": num_streams, "max_batch": max_batch, "sweep": out}
 
 

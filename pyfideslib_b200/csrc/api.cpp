@@ -652,6 +652,65 @@ static fides_status rotate_many(fides_ctx* c, const fides_ct* a, int n, const ui
     return check_cuda(c, "rotate");
 }
 
+// Hoisted rotations of nx ciphertexts at one level by the same n indices:
+// groups of inputs share one batched ModUp and one inner-product / ModDown
+// launch sequence (outs[u * n + r] = rotation of xs[u] by galois[r]).
+static fides_status rotate_many_groups(fides_ctx* c, int nx, const fides_ct* const* xs, int n, const uint32_t* galois,
+                                       fides_ct* const* outs) {
+    if (n < 1 || nx < 1) return FIDES_BAD_ARG;
+    if (nx == 1 || n > kMaxBatch / 2) {
+        for (int u = 0; u < nx; ++u) {
+            std::vector<fides_ct*> o(outs + (size_t)u * n, outs + (size_t)(u + 1) * n);
+            fides_status s = rotate_many(c, xs[u], n, galois, o.data());
+            if (s != FIDES_OK) return s;
+        }
+        return FIDES_OK;
+    }
+    std::vector<const SwitchKey*> keys(n);
+    for (int r = 0; r < n; ++r) {
+        auto it = c->galois_keys.find(galois[r]);
+        if (it == c->galois_keys.end())
+            return set_err(c, FIDES_KEY_MISSING, "no key for galois element " + std::to_string(galois[r]));
+        keys[r] = &it->second;
+    }
+    const int level = xs[0]->level, N = c->N;
+    fides_status s = ws_reserve(c, c->wsb, std::min(nx * n, kMaxBatch));
+    if (s != FIDES_OK) return s;
+    const int gmax = std::max(1, c->wsb.cap / n);
+    std::vector<fides_ct> tmp((size_t)nx * n);
+    for (auto& t : tmp)
+        if ((s = ct_reserve(c, &t, level)) != FIDES_OK) return s;
+    for (int u0 = 0; u0 < nx; u0 += gmax) {
+        const int ng = std::min(gmax, nx - u0), nb = ng * n;
+        std::vector<const uint64_t*> c0(ng), c1(ng);
+        for (int g = 0; g < ng; ++g) {
+            c0[g] = xs[u0 + g]->c0();
+            c1[g] = xs[u0 + g]->c1(N);
+        }
+        std::vector<const SwitchKey*> kk(nb);
+        std::vector<uint32_t> gg(nb);
+        std::vector<uint64_t*> o0(nb), o1(nb);
+        for (int b = 0; b < nb; ++b) {
+            kk[b] = keys[b % n];
+            gg[b] = galois[b % n];
+            o0[b] = tmp[(size_t)u0 * n + b].c0();
+            o1[b] = tmp[(size_t)u0 * n + b].c1(N);
+        }
+        eng_rotate_groups(c, c->wsb, level, ng, n, c0.data(), c1.data(), kk.data(), gg.data(), o0.data(), o1.data());
+    }
+    for (int u = 0; u < nx; ++u)
+        for (int r = 0; r < n; ++r) {
+            const fides_ct meta = *xs[u];
+            fides_ct* o = outs[(size_t)u * n + r];
+            commit(c, o, tmp[(size_t)u * n + r]);
+            o->level = level;
+            o->scale = meta.scale;
+            o->noise_deg = meta.noise_deg;
+            o->slots = meta.slots;
+        }
+    return check_cuda(c, "rotate groups");
+}
+
 fides_status fides_rotate(fides_ctx* ctx, const fides_ct* a, int32_t index, fides_ct* out) {
     if (!ctx || !valid_ct(ctx, a) || !out) return FIDES_BAD_ARG;
     Guard g(ctx);
@@ -1123,17 +1182,28 @@ fides_status fides_linear_transform_batch(fides_ctx* c, int nx, const fides_ct* 
     std::vector<const fides_ct*> inner;
     std::vector<int32_t> gidx;
     std::vector<int> owner;  // input of each giant-step term
+    // baby steps of every input: hoisted rotations, grouped over the inputs
+    std::vector<fides_ct*> bo((size_t)nx * babies.size());
+    if (!babies.empty()) {
+        for (auto& p : bo) p = tmp.make();
+        std::vector<uint32_t> bgal(babies.size());
+        for (size_t i = 0; i < babies.size(); ++i)
+            bgal[i] = fides_rotation_galois(c, babies[i], xs[0]->slots > 0 ? xs[0]->slots : N / 2);
+        bool grouped = std::find(bgal.begin(), bgal.end(), 1u) == bgal.end();
+        for (int u = 1; u < nx; ++u) grouped = grouped && xs[u]->slots == xs[0]->slots;
+        if (grouped) {
+            s = rotate_many_groups(c, nx, xs, (int)babies.size(), bgal.data(), bo.data());
+        } else {
+            for (int u = 0; u < nx && s == FIDES_OK; ++u)
+                s = fides_rotate_hoisted(c, xs[u], (int)babies.size(), babies.data(), bo.data() + (size_t)u * babies.size());
+        }
+        if (s != FIDES_OK) return s;
+    }
     for (int u = 0; u < nx; ++u) {
         const fides_ct* x = xs[u];
         std::map<int, const fides_ct*> bct;
         bct[0] = x;
-        if (!babies.empty()) {
-            std::vector<fides_ct*> bo;
-            for (size_t i = 0; i < babies.size(); ++i) bo.push_back(tmp.make());
-            s = fides_rotate_hoisted(c, x, (int)babies.size(), babies.data(), bo.data());
-            if (s != FIDES_OK) return s;
-            for (size_t i = 0; i < babies.size(); ++i) bct[babies[i]] = bo[i];
-        }
+        for (size_t i = 0; i < babies.size(); ++i) bct[babies[i]] = bo[(size_t)u * babies.size() + i];
         const double sc = x->scale * pts[0]->scale;
         const int nd = x->noise_deg + pts[0]->noise_deg, sl = x->slots;
         acc[u] = tmp.make();

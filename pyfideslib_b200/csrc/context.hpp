@@ -158,6 +158,13 @@ void eng_modup(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
 void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* a0, const uint64_t* const* a1,
                const uint64_t* const* b0, const uint64_t* const* b1, uint64_t* const* out0, uint64_t* const* out1,
                bool rescale, const SwitchKey& key);
+// Hoisted rotations of ngroups ciphertexts (c0[g], c1[g]) by nper Galois
+// elements each: element b = g * nper + r rotates ciphertext g by galois[b]
+// with keys[b]; the ModUps of the ngroups inputs run as one batch and every
+// element's inner product reads its group's digits.  ngroups * nper <= w.cap.
+void eng_rotate_groups(fides_ctx* c, Workspace& w, int level, int ngroups, int nper, const uint64_t* const* c0,
+                       const uint64_t* const* c1, const SwitchKey* const* keys, const uint32_t* galois,
+                       uint64_t* const* out0, uint64_t* const* out1);
 // Rotation of element b by galois[b] with keys[b]; hoisted=true: all elements
 // rotate the same ciphertext (c0[0], c1[0]) and share one ModUp.
 void eng_rotate(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* c0, const uint64_t* const* c1,

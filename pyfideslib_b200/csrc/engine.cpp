@@ -223,4 +223,28 @@ void eng_rotate(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* c
     moddown_finish(c, w, level, nb, out0, out1, false, false);
 }
 
+void eng_rotate_groups(fides_ctx* c, Workspace& w, int level, int ngroups, int nper, const uint64_t* const* c0,
+                       const uint64_t* const* c1, const SwitchKey* const* keys, const uint32_t* galois,
+                       uint64_t* const* out0, uint64_t* const* out1) {
+    eng_modup(c, w, level, ngroups, c1);
+    const int nb = ngroups * nper;
+    KsArgs ka{};
+    for (int b = 0; b < nb; ++b) {
+        ka.own[b] = c1[b / nper];
+        ka.c0[b] = c0[b / nper];
+        ka.kb[b] = keys[b]->b;
+        ka.ka[b] = keys[b]->a;
+        ka.galois[b] = galois[b];
+    }
+    ka.dig = w.DIG;
+    ka.xb = w.XB;
+    ka.xa = w.XA;
+    ka.dig_stride = w.dig_stride;
+    ka.bstride = w.stride;
+    ka.dig_bstride = w.stride;
+    ka.dig_group = nper;
+    launch_ks_inner(c->dev, level, nb, ka, false, w.st);
+    moddown_finish(c, w, level, nb, out0, out1, false, false);
+}
+
 }  // namespace fides

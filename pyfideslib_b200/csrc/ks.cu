@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                 srcs[d] = args.own[bi] + (size_t)t * ctx.N;
             } else {
                 const int md = m < n ? (t < lo ? t : t - cnt) : (n - cnt) + (m - n);
-                srcs[d] = args.dig + (size_t)bi * args.dig_bstride + ((size_t)d * args.dig_stride + md) * ctx.N;
+                const int gi = args.dig_group > 0 ? bi / args.dig_group : bi;
+                srcs[d] = args.dig + (size_t)gi * args.dig_bstride + ((size_t)d * args.dig_stride + md) * ctx.N;
             }
         }
     }

@@ -599,14 +599,17 @@ constexpr size_t ks_tile_words() {
     return (size_t)G::TR * G::CP;
 }
 
-template <int LR, int LC, bool PF, bool AQ, bool FP>
+template <int LR, int LC, bool PF, bool AQ, bool FP, bool SG = false>
 __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constant__ DevCtx ctx,
                                                             const __grid_constant__ KsFuseArgs a) {
     using G = Geo<LR, LC>;
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     constexpr int TILE = TR * C;
     constexpr int TW = TR * CP;
+    constexpr bool kSG = SG && FP && LC == 8;
     extern __shared__ __align__(16) uint64_t ks_sm[];  // [digits needing rows][TR][CP]
+    __shared__ ulonglong2 s_g1[kSG ? TR * 16 : 1];    // staged row twiddles (variant 9), shared by the digits
+    __shared__ double s_gw[kSG ? 8 : 1];
 
     const int level = a.level, n = level + 1;
     const int m = blockIdx.z;
@@ -625,6 +628,22 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constan
     const size_t limb_off = (size_t)t * ctx.N + base;
     const int nd = level / ctx.alpha + 1;
     const int d_own = m < n ? t / ctx.alpha : -1;  // digit holding t (its value is the own limb)
+    // variant 9: the row twiddles of this prime and these rows, for every digit
+    ulonglong2 dtw[kSG ? 4 : 1];
+    if constexpr (kSG) {
+        if (fmode == 4) {
+#pragma unroll
+            for (int tt = 4; tt < 8; ++tt)
+                dtw[tt - 4] = ldg2(twg, ((size_t)(R + row) << tt) + ((size_t)th << (tt - 4)));
+            const ulonglong2* tw2 = reinterpret_cast<const ulonglong2*>(twg);
+            for (int e = threadIdx.x; e < TR * 15; e += NT) {
+                const int r = e / 15, j = e % 15, tt = 31 - __clz(j + 1);
+                s_g1[r * 16 + j] = tw2[((size_t)(R + blockIdx.x * TR + r) << tt) + (j + 1 - (1 << tt))];
+            }
+            if (threadIdx.x < 8) s_gw[threadIdx.x] = as_f64(tw2[threadIdx.x].x);
+            __syncthreads();
+        }
+    }
 
     // the epilogue's key tiles (and own tile) are read once per batch from
     // HBM; start those reads now, under the transforms
@@ -647,14 +666,22 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constan
         uint64_t x[16];
 #pragma unroll
         for (int k = 0; k < 16; ++k) x[k] = src[th + (k << (LC - 4))];
-        fwd_group<3, 0, PF, AQ, FP, true>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+        if (kSG && fmode == 4) {
+            if constexpr (kSG) sg_stage1<3>(x, s_g1 + rl * 16, kk.k0, kk.k1);
+        } else {
+            fwd_group<3, 0, PF, AQ, FP, true>(fmode, x, tab, 3, (size_t)(R + row), 0, kk.k0, kk.k1);
+        }
         if constexpr (LC > 4) {
 #pragma unroll
             for (int k = 0; k < 16; ++k) srow[padi(th + (k << (LC - 4)))] = x[k];
             __syncthreads();
 #pragma unroll
             for (int k = 0; k < 16; ++k) x[k] = srow[padi((th << 4) + k)];
-            fwd_group<LC - 5, 0, PF, AQ, FP, true>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
+            if (kSG && fmode == 4) {
+                if constexpr (kSG) sg_stage2<3>(x, dtw, s_gw, kk.k0, kk.k1);
+            } else {
+                fwd_group<LC - 5, 0, PF, AQ, FP, true>(fmode, x, tab, LC - 1, (size_t)(R + row), th, kk.k0, kk.k1);
+            }
             // each thread rewrites exactly the slots it read
 #pragma unroll
             for (int k = 0; k < 16; ++k) srow[padi((th << 4) + k)] = x[k];
@@ -1022,17 +1049,17 @@ static void launch_fwd_cols(const DevCtx& ctx, const LimbMap& map, cudaStream_t 
     }
 }
 
-template <int LR, int LC, bool PF, bool AQ, bool FP>
+template <int LR, int LC, bool PF, bool AQ, bool FP, bool SG = false>
 static void launch_rows_ks_v(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaStream_t st) {
     using G = Geo<LR, LC>;
     const size_t smem = ks_tile_words<LR, LC>() * 8 * (size_t)ctx.dnum;  // opted in by ntt_prepare
     dim3 g(G::R / G::TR, nb, a.level + 1 + ctx.K);
-    k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP><<<g, G::NTR, smem, st>>>(ctx, a);
+    k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG><<<g, G::NTR, smem, st>>>(ctx, a);
 }
 
-template <int LR, int LC, bool PF, bool AQ, bool FP>
+template <int LR, int LC, bool PF, bool AQ, bool FP, bool SG = false>
 static void prepare_rows_ks_v(int dnum) {
-    cudaFuncSetAttribute(k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(ks_tile_words<LR, LC>() * 8 * (size_t)dnum));
 }
 
@@ -1043,6 +1070,7 @@ static void prepare_rows_ks(const DevCtx& ctx, const LimbMap&, cudaStream_t) {
     prepare_rows_ks_v<LR, LC, false, true, false>(ctx.dnum);
     prepare_rows_ks_v<LR, LC, true, true, true>(ctx.dnum);
     prepare_rows_ks_v<LR, LC, false, true, true>(ctx.dnum);
+    prepare_rows_ks_v<LR, LC, false, true, true, true>(ctx.dnum);
 }
 
 bool ntt_rows_keyswitch_supported(const DevCtx& ctx) {
@@ -1059,6 +1087,7 @@ static void launch_rows_ks(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaS
         case 1: case 2: launch_rows_ks_v<LR, LC, false, false, false>(ctx, a, nb, st); break;
         case 3: case 4: launch_rows_ks_v<LR, LC, false, true, false>(ctx, a, nb, st); break;
         case 6: case 7: launch_rows_ks_v<LR, LC, true, true, true>(ctx, a, nb, st); break;
+        case 9: launch_rows_ks_v<LR, LC, false, true, true, true>(ctx, a, nb, st); break;
         default: launch_rows_ks_v<LR, LC, false, true, true>(ctx, a, nb, st); break;
     }
 }
