@@ -727,7 +727,8 @@ def main():
     ap.add_argument("--ntt-variant", type=int, default=-1, help="force a forward NTT variant (default: tuned)")
     ap.add_argument("--conv-variant", type=int, default=-1, help="force a base-conversion variant (default: tuned)")
     ap.add_argument("--ks-variant", type=int, default=-1,
-                    help="force the key-switch inner-product arithmetic: 0 integer, 1 FP64 (default: the context's)")
+                    help="force the key-switch inner product: bit 0 FP64 sums, bit 1 fused into the NTT row pass, "
+                         "bit 2 fused for batches of 4+ (default: the context's, 5)")
     ap.add_argument("--profile-roofline", action="store_true",
                     help="mark the roofline NTT loop for ncu --profile-from-start off")
     ap.add_argument("--profile-step", action="store_true",

@@ -15,6 +15,8 @@ namespace fides {
 
 namespace {
 
+constexpr int kFuseMinBatch = 4;
+
 LimbSeg seg_ws(const uint64_t* in, uint64_t* out, int count, int nq, int q0, int level, size_t bstride) {
     LimbSeg g{};
     g.in = in;
@@ -159,7 +161,12 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
     im.seg[im.nseg++] = seg_ws(w.E2, w.XT, n, n, 0, level, w.stride);
     im.total = n;
     ntt_inverse(c->dev, im, IL_PLAIN, IS_MODUP, w.st);
-    if ((c->dev.ks_variant & 2) && ntt_rows_keyswitch_supported(c->dev)) {
+    // fused inner product: forced (bit 1), or for batches of at least
+    // kFuseMinBatch elements (bit 2; a single element's fused launch is
+    // about two waves of long CTAs and measured slower than the two kernels)
+    const bool fuse = ((c->dev.ks_variant & 2) || ((c->dev.ks_variant & 4) && nb >= kFuseMinBatch)) &&
+                      ntt_rows_keyswitch_supported(c->dev);
+    if (fuse) {
         // ModUp conversion and the digits' column pass; the row pass runs
         // fused with the inner product, so the digits' evaluation limbs never
         // reach HBM

@@ -6,10 +6,9 @@
 // batch -- and launches each batch on the next free stream; every stream owns
 // a key-switch workspace, so a batch admitted while others are still running
 // overlaps them on the device.  Bootstraps run on their own lane (the
-// context stream and workspaces), beside the batches: the pending ones, up
-// to min(max_batch, kBootBatch), go through one batched EvalBootstrap (its
-// EvalMod lanes share every HMult, its linear transforms every giant-step
-// key switch).  Admission is against a fixed HBM budget: the workspaces are
+// context stream and workspaces), beside the batches, up to
+// min(max_batch, kBootBatch) per batched EvalBootstrap call.  Admission is
+// against a fixed HBM budget: the workspaces are
 // charged once at start-up, and every admitted request reserves its output
 // buffer until the request completes.  Completion is detected with one CUDA
 // event per batch; the caller waits on a request id.  Ciphertexts and keys
@@ -31,8 +30,12 @@
 using namespace fides;
 using clk = std::chrono::steady_clock;
 
-// bootstraps batched together at most (each adds two EvalMod lanes)
-constexpr int kBootBatch = 4;
+// bootstraps batched together at most.  One: a batched EvalBootstrap of 2
+// (4) ciphertexts at N = 2^16 runs 59.6 (115.3) ms against 31.4 ms for one,
+// so batching gains 5-8% throughput while every member waits for the whole
+// batch; with up to 4 per batch the p99 of the mix with 10% bootstraps at
+// 70% of the lane's capacity measured 735 ms against 126 ms one at a time.
+constexpr int kBootBatch = 1;
 
 namespace {
 
