@@ -242,6 +242,7 @@ void eng_rotate_groups(fides_ctx* c, Workspace& w, int level, int ngroups, int n
         ka.kb[b] = keys[b]->b;
         ka.ka[b] = keys[b]->a;
         ka.galois[b] = galois[b];
+        ka.dig_elem[b] = (uint8_t)(b / nper);
     }
     ka.dig = w.DIG;
     ka.xb = w.XB;

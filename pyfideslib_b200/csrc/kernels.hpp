@@ -90,7 +90,8 @@ struct KsArgs {
     size_t dig_stride;               // limbs per digit in dig
     size_t bstride;                  // words between consecutive elements' xb / xa
     size_t dig_bstride;              // words between consecutive elements' dig (0: shared ModUp)
-    int dig_group;                   // > 0: elements b share the ModUp of b / dig_group (grouped hoisting)
+    int dig_group;                   // > 0: element b reads the ModUp of element dig_elem[b] (grouped hoisting)
+    uint8_t dig_elem[kMaxBatch];
 };
 // plain: no rotation in any element (vectorised variant)
 void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, bool plain, cudaStream_t st);

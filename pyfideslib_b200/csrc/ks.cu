@@ -280,7 +280,7 @@ void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt,
 // each product x k is reduced to |r| <= 0.875p, the sum of up to 8 digits
 // stays below 7p < 2^53, and one centring plus a floor reduction give the
 // canonical residue -- the same values as the 128-bit integer sums.
-template <int VEC, class ACC, bool FPK>
+template <int VEC, class ACC, bool FPK, bool GRP = false>
 __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx ctx, int level, int nb,
                                                   const __grid_constant__ KsArgs args) {
     const int n = level + 1;
@@ -294,7 +294,9 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
     const size_t boff = (size_t)bi * args.bstride;
     const uint64_t* kb = args.kb[bi];
     const uint64_t* ka = args.ka[bi];
-    // source limb of each digit for this prime
+    // source limb of each digit for this prime (GRP, grouped hoisting: the
+    // element's ModUp is that of its group, a table entry)
+    const int gi = GRP ? (int)args.dig_elem[bi] : bi;
     const uint64_t* srcs[8];
 #pragma unroll
     for (int d = 0; d < 8; ++d) {
@@ -306,7 +308,6 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                 srcs[d] = args.own[bi] + (size_t)t * ctx.N;
             } else {
                 const int md = m < n ? (t < lo ? t : t - cnt) : (n - cnt) + (m - n);
-                const int gi = args.dig_group > 0 ? bi / args.dig_group : bi;
                 srcs[d] = args.dig + (size_t)gi * args.dig_bstride + ((size_t)d * args.dig_stride + md) * ctx.N;
             }
         }
@@ -421,6 +422,12 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
             k_ks_inner<1, AccSplit, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
         else
             k_ks_inner<1, Acc128, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
+    } else if (args.dig_group > 0) {
+        dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
+        if (ctx.ks_variant & 1)
+            k_ks_inner<0, Acc128, true, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
+        else
+            k_ks_inner<0, Acc128, false, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
     } else {
         dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
         if (ctx.ks_variant & 1)
