@@ -186,7 +186,7 @@ def measure_c4(cc, lib, st, n=256, reps=3, seed=4):
             "per_op_ms": op_ms, "per_op_pairs_per_s": n / (op_ms * 1e-3), "results_equal": bool(same)}
 
 
-def measure_c3(reps=5, seed=3, ntt_variant=-1, ks_variant=-1):
+def measure_c3(reps=5, seed=3, ntt_variant=-1, ks_variant=-1, key_compression=1):
     """Config 3: N=2^16, 20 moduli (60 + 19 x 40-bit, scale 2^40), dnum=3, one
     ciphertext; 32 hoisted rotations (+-2^k, k < 15, and 3, 5) sharing one
     ModUp, and a 64-diagonal plaintext matrix (offsets 0..63, entries uniform
@@ -204,6 +204,7 @@ def measure_c3(reps=5, seed=3, ntt_variant=-1, ks_variant=-1):
         lib.fides_set_ntt_variant(cc._h, ntt_variant)
     if ks_variant >= 0:
         lib.fides_set_keyswitch_variant(cc._h, ks_variant)
+    lib.fides_set_key_compression(cc._h, key_compression)
     slots = cc.N // 2
     rng = np.random.default_rng(seed)
     idx = sorted({s * (1 << k) for k in range(15) for s in (1, -1)} | {3, 5})
@@ -483,6 +484,7 @@ def run_ours(args):
     from pyfideslib_b200._capi import lib
 
     cc = F.CryptoContext(log_n=LOGN, num_q=L, dnum=DNUM, num_p=K, device=local)
+    lib.fides_set_key_compression(cc._h, args.key_compression)
     tv, nv = C.c_int(), C.c_int()
     tms = (C.c_float * 16)()
     lib.fides_autotune(cc._h, C.byref(tv), tms, C.byref(nv))
@@ -673,7 +675,7 @@ def run_ours(args):
                 "per_op": measure_serving(cc, brates, 4.0, rot_idx, max_batch=1, num_streams=1, boot_share=0.1,
                                           boot_inputs=boot_cts)}
     if not args.no_c3:
-        c3 = measure_c3(ntt_variant=args.ntt_variant, ks_variant=args.ks_variant)
+        c3 = measure_c3(ntt_variant=args.ntt_variant, ks_variant=args.ks_variant, key_compression=args.key_compression)
     value = job_throughput(B * args.steps, world, ms)
     per_op_value = job_throughput(B * max(1, args.steps // 2), world, ms_op)
     e2e_steps = max(1, args.steps // 2)
@@ -737,6 +739,8 @@ def main():
                          "bit 2 fused for batches of 4+ (default: the context's, 5)")
     ap.add_argument("--profile-roofline", action="store_true",
                     help="mark the roofline NTT loop for ncu --profile-from-start off")
+    ap.add_argument("--key-compression", type=int, default=1, choices=[0, 1],
+                    help="rotation keys store b and the seed of a (1, default) or both halves (0)")
     ap.add_argument("--profile-step", action="store_true",
                     help="mark one batched HMult step (after the timed region) for ncu --profile-from-start off")
     args = ap.parse_args()

@@ -415,6 +415,16 @@ fides_status fides_keygen_relin(fides_ctx* ctx, const fides_sk* sk, uint64_t see
 fides_status fides_keygen_rotations(fides_ctx* ctx, const fides_sk* sk, int n, const int32_t* indices, int slots,
                                     uint64_t seed);
 fides_status fides_keygen_conjugate(fides_ctx* ctx, const fides_sk* sk, uint64_t seed);
+/* Key compression for the rotation and conjugation keys generated from here
+ * on (1, the default): each stores its b half and the seed of its uniform a
+ * half, which the key-switch kernels regenerate (a counter-based hash per
+ * coefficient) instead of reading it: half the HBM per key and half the key
+ * bytes read per rotation.  0 stores both halves.  The relinearisation key
+ * always keeps its a half (batched HMults read it once per batch), and
+ * uploaded or imported keys keep theirs.  The key layout this replaces:
+ * KeySwitchingKey a / b (src/CKKS/KeySwitchingKey.cu:20-35); the reference
+ * has no compressed form. */
+fides_status fides_set_key_compression(fides_ctx* ctx, int on);
 /* Export generated switching keys (dnum*(L+K)*N words each) for interop tests. */
 fides_status fides_key_export(fides_ctx* ctx, uint32_t galois, uint64_t* b, uint64_t* a);
 /* Encode `slots` complex values (re, im interleaved) at `level` and `scale`

@@ -153,6 +153,7 @@ EXPORTS = {
     "fides_keygen_relin": ([vp, vp, u64], C.c_int),
     "fides_keygen_rotations": ([vp, vp, C.c_int, i32p, C.c_int, u64], C.c_int),
     "fides_keygen_conjugate": ([vp, vp, u64], C.c_int),
+    "fides_set_key_compression": ([vp, C.c_int], C.c_int),
     "fides_key_export": ([vp, C.c_uint32, u64p, u64p], C.c_int),
     "fides_encode": ([vp, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_double, u64p], C.c_int),
     "fides_encrypt": ([vp, vp, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_double, u64, C.POINTER(vp)], C.c_int),

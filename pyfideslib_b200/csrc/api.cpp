@@ -324,13 +324,8 @@ fides_status fides_set_ntt_variant(fides_ctx* c, int variant) {
 
 static fides_status upload_key(fides_ctx* c, SwitchKey& k, const uint64_t* b, const uint64_t* a) {
     const size_t words = (size_t)c->dnum * (c->L + c->K) * c->N;
-    if (!k.b) {
-        if (cudaMalloc((void**)&k.b, 2 * words * sizeof(uint64_t)) != cudaSuccess) {
-            cudaGetLastError();
-            return set_err(c, FIDES_OOM, "key allocation failed");
-        }
-        k.a = k.b + words;
-    }
+    fides_status s = key_alloc(c, k, false);
+    if (s != FIDES_OK) return s;
     cudaMemcpyAsync(k.b, b, words * 8, cudaMemcpyHostToDevice, c->st);
     cudaMemcpyAsync(k.a, a, words * 8, cudaMemcpyHostToDevice, c->st);
     cudaStreamSynchronize(c->st);

@@ -85,22 +85,12 @@ __global__ void k_small_to_rns(const int64_t* __restrict__ v, uint64_t* __restri
     out[(size_t)limb * N + j] = x < 0 ? neg_mod(a, pc.p) : a;
 }
 
-__device__ __forceinline__ uint64_t hash64(uint64_t x) {
-    x ^= x >> 33;
-    x *= 0xff51afd7ed558ccdull;
-    x ^= x >> 33;
-    x *= 0xc4ceb9fe1a85ec53ull;
-    x ^= x >> 33;
-    return x;
-}
-
 __global__ void k_fill_uniform(uint64_t* __restrict__ out, int N, int q0, const PrimeConst* __restrict__ pcs,
                                uint64_t seed) {
     const int limb = blockIdx.y;
     const uint64_t p = pcs[q0 + limb].p;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t h = hash64(seed ^ hash64(((uint64_t)(q0 + limb) << 32) | (uint64_t)j));
-    out[(size_t)limb * N + j] = __umul64hi(h, p);
+    out[(size_t)limb * N + j] = uniform_mod(seed, q0 + limb, (uint32_t)j, p);
 }
 
 // b = -a * sb + e (+ pmod_i * sg on limbs with lo <= prime < hi)
@@ -199,23 +189,27 @@ fides_status upload_small(fides_ctx* c, const std::vector<int64_t>& v, uint64_t*
     return check_cuda(c, "small_to_rns");
 }
 
-fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg, uint64_t seed, SwitchKey& key) {
+// A switching key b = -a sb + e + P sg (per digit), a uniform from the seed.
+// compress: only b is stored; the a half is regenerated from the seed by the
+// key-switch kernels (key.a null, key.a_seed set).
+fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg, uint64_t seed, SwitchKey& key,
+                            bool compress) {
     const int N = c->N, NP = c->L + c->K;
-    const size_t words = (size_t)c->dnum * NP * N;
-    if (!key.b) {
-        if (cudaMalloc((void**)&key.b, 2 * words * 8) != cudaSuccess) {
-            cudaGetLastError();
-            return set_err(c, FIDES_OOM, "key allocation");
-        }
-        key.a = key.b + words;
-    }
+    fides_status st = key_alloc(c, key, compress);
+    if (st != FIDES_OK) return st;
+    key.a_seed = seed * 1315423911ull;
     uint64_t* e = nullptr;
+    uint64_t* atmp = nullptr;
     if (cudaMallocAsync((void**)&e, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "key tmp");
+    if (compress && cudaMallocAsync((void**)&atmp, (size_t)NP * N * 8, c->st) != cudaSuccess) {
+        cudaFreeAsync(e, c->st);
+        return set_err(c, FIDES_OOM, "key tmp");
+    }
     for (int d = 0; d < c->dnum; ++d) {
         uint64_t* kb = key.b + (size_t)d * NP * N;
-        uint64_t* ka = key.a + (size_t)d * NP * N;
+        uint64_t* ka = compress ? atmp : key.a + (size_t)d * NP * N;
         count_launches(1);
-        k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(ka, N, 0, c->dev.pc, seed * 1315423911ull + d + 1);
+        k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(ka, N, 0, c->dev.pc, key.a_seed + d + 1);
         fides_status s = upload_small(c, gaussian(N, seed ^ (0xABCDull + d)), e, 0, NP);
         if (s != FIDES_OK) return s;
         ntt_forward(c->dev, map_single(e, e, NP, NP, 0), FL_PLAIN, FS_PLAIN, c->st);
@@ -225,6 +219,7 @@ fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg
     }
     cudaStreamSynchronize(c->st);
     cudaFreeAsync(e, c->st);
+    if (atmp) cudaFreeAsync(atmp, c->st);
     return check_cuda(c, "switch key");
 }
 
@@ -297,7 +292,9 @@ fides_status fides_keygen_relin(fides_ctx* c, const fides_sk* sk, uint64_t seed)
     uint64_t* s2 = nullptr;
     if (cudaMallocAsync((void**)&s2, (size_t)NP * c->N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "s^2");
     launch_elementwise(c->dev, EW_MUL, NP, 0, sk->s, sk->s, s2, c->st);
-    fides_status s = gen_switch_key(c, sk->s, s2, seed, c->relin);
+    // the relinearisation key keeps its a half: batched HMults read it once
+    // per batch, where regenerating it would cost every element
+    fides_status s = gen_switch_key(c, sk->s, s2, seed, c->relin, false);
     cudaFreeAsync(s2, c->st);
     if (s == FIDES_OK) c->has_relin = true;
     return s;
@@ -324,7 +321,7 @@ static fides_status keygen_galois(fides_ctx* c, const fides_sk* sk, uint32_t g, 
     uint64_t* sr = nullptr;
     if (cudaMallocAsync((void**)&sr, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "s rot");
     launch_automorph(c->dev, NP, sk->s, sr, ginv, c->st);
-    fides_status s = gen_switch_key(c, sr, sk->s, seed ^ ((uint64_t)g << 20), c->galois_keys[g]);
+    fides_status s = gen_switch_key(c, sr, sk->s, seed ^ ((uint64_t)g << 20), c->galois_keys[g], c->compress_keys);
     cudaFreeAsync(sr, c->st);
     return s;
 }
@@ -348,6 +345,13 @@ fides_status fides_keygen_rotations(fides_ctx* c, const fides_sk* sk, int n, con
     return FIDES_OK;
 }
 
+fides_status fides_set_key_compression(fides_ctx* c, int on) {
+    if (!c || on < 0 || on > 1) return FIDES_BAD_ARG;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    c->compress_keys = on != 0;
+    return FIDES_OK;
+}
+
 fides_status fides_keygen_conjugate(fides_ctx* c, const fides_sk* sk, uint64_t seed) {
     if (!c || !sk || !sk->s) return FIDES_BAD_ARG;
     std::lock_guard<std::recursive_mutex> lk(c->mu);
@@ -368,9 +372,22 @@ fides_status fides_key_export(fides_ctx* c, uint32_t galois, uint64_t* b, uint64
         if (it == c->galois_keys.end()) return FIDES_KEY_MISSING;
         k = &it->second;
     }
-    const size_t words = (size_t)c->dnum * (c->L + c->K) * c->N;
+    const int NP = c->L + c->K, N = c->N;
+    const size_t words = (size_t)c->dnum * NP * N;
     cudaMemcpyAsync(b, k->b, words * 8, cudaMemcpyDeviceToHost, c->st);
-    cudaMemcpyAsync(a, k->a, words * 8, cudaMemcpyDeviceToHost, c->st);
+    if (k->a) {
+        cudaMemcpyAsync(a, k->a, words * 8, cudaMemcpyDeviceToHost, c->st);
+    } else {
+        // a seeded key: its a half regenerated digit by digit
+        uint64_t* t = nullptr;
+        if (cudaMallocAsync((void**)&t, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "key export");
+        for (int d = 0; d < c->dnum; ++d) {
+            count_launches(1);
+            k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(t, N, 0, c->dev.pc, k->a_seed + d + 1);
+            cudaMemcpyAsync(a + (size_t)d * NP * N, t, (size_t)NP * N * 8, cudaMemcpyDeviceToHost, c->st);
+        }
+        cudaFreeAsync(t, c->st);
+    }
     cudaStreamSynchronize(c->st);
     return check_cuda(c, "key export");
 }

@@ -17,6 +17,21 @@ constexpr int kMaxBatch = 32;  // ciphertexts per batched launch (blockIdx.z)
 // synchronising call of the context reports FIDES_TIMEOUT and clears the word.
 constexpr uint32_t kDevErrTensorWait = 1u;  // a tensor-core conversion stopped waiting for its MMAs
 
+// Counter-based hash behind every seeded uniform draw (a halves of keys and
+// public keys, synthetic ciphertexts): a 64-bit finaliser of MurmurHash3's
+// form.  uniform_mod(seed, prime, j) is residue j of the prime's limb.
+__device__ __forceinline__ uint64_t hash64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+__device__ __forceinline__ uint64_t uniform_mod(uint64_t seed, int prime, uint32_t j, uint64_t p) {
+    return __umul64hi(hash64(seed ^ hash64(((uint64_t)prime << 32) | (uint64_t)j)), p);
+}
+
 // Read-only view of the context tables in HBM, passed by value to kernels.
 // Index conventions: prime ids 0..L-1 are the Q primes, L..L+K-1 the special
 // primes.  Every table entry with a Shoup companion stores (value, companion)

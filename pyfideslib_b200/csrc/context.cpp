@@ -519,6 +519,26 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     return ws_reserve(c, c->ws1, 1);
 }
 
+fides_status key_alloc(fides_ctx* c, SwitchKey& k, bool seeded) {
+    const size_t words = (size_t)c->dnum * (c->L + c->K) * c->N;
+    if (k.b && k.seeded != seeded) {
+        cudaStreamSynchronize(c->st);  // kernels queued with the old key
+        cudaFree(k.b);
+        k.b = k.a = nullptr;
+    }
+    if (!k.b) {
+        if (cudaMalloc((void**)&k.b, (seeded ? 1 : 2) * words * sizeof(uint64_t)) != cudaSuccess) {
+            cudaGetLastError();
+            k.b = nullptr;
+            return set_err(c, FIDES_OOM, "key allocation failed");
+        }
+    }
+    k.seeded = seeded;
+    k.a = seeded ? nullptr : k.b + words;
+    if (!seeded) k.a_seed = 0;
+    return FIDES_OK;
+}
+
 fides_status ws_reserve(fides_ctx* c, Workspace& w, int cap) {
     if (!w.st) w.st = c->st;
     if (w.base && w.cap >= cap) return FIDES_OK;
@@ -567,6 +587,7 @@ void free_context(fides_ctx* c) {
     auto freek = [](SwitchKey& k) {
         if (k.b) cudaFree(k.b);
         k.b = k.a = nullptr;
+        k.seeded = false;
     };
     if (c->has_relin) freek(c->relin);
     for (auto& kv : c->galois_keys) freek(kv.second);

@@ -52,7 +52,9 @@ namespace fides {
 
 struct SwitchKey {
     uint64_t* b = nullptr;  // [dnum][L+K][N]
-    uint64_t* a = nullptr;
+    uint64_t* a = nullptr;  // null for a seeded key: digit d's a half is uniform_mod(a_seed + d + 1, prime, j)
+    uint64_t a_seed = 0;
+    bool seeded = false;
 };
 
 // Key-switch workspace for `cap` batch elements; element b's buffers sit at
@@ -117,6 +119,7 @@ struct fides_ctx {
     std::vector<float> tune_ms;
     int tuned_conv = 0;  // base-conversion accumulator: 0 128-bit, 1 split 32-bit products
     std::vector<float> conv_ms;
+    bool compress_keys = true;  // Galois keys generated here store b and a seed for a
     std::string last_error;
     std::recursive_mutex mu;
 
@@ -149,6 +152,8 @@ void free_context(fides_ctx* c);
 LimbMap map_single(const uint64_t* in, uint64_t* out, int count, int nq, int q0, int level = -1,
                    const uint64_t* in2 = nullptr, const uint64_t* in3 = nullptr);
 fides_status ws_reserve(fides_ctx* c, Workspace& w, int cap);
+// (Re)allocate a switching key's storage: b only when seeded, b and a otherwise.
+fides_status key_alloc(fides_ctx* c, SwitchKey& k, bool seeded);
 void ws_free(Workspace& w);
 
 // ---- engine (engine.cpp): batched evaluation steps over nb <= kMaxBatch elements ----

@@ -165,7 +165,7 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
     // kFuseMinBatch elements (bit 2; a single element's fused launch is
     // about two waves of long CTAs and measured slower than the two kernels)
     const bool fuse = ((c->dev.ks_variant & 2) || ((c->dev.ks_variant & 4) && nb >= kFuseMinBatch)) &&
-                      ntt_rows_keyswitch_supported(c->dev);
+                      ntt_rows_keyswitch_supported(c->dev) && key.a != nullptr;
     if (fuse) {
         // ModUp conversion and the digits' column pass; the row pass runs
         // fused with the inner product, so the digits' evaluation limbs never
@@ -193,6 +193,7 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
         ka.own[b] = w.E2 + (size_t)b * w.stride;
         ka.kb[b] = key.b;
         ka.ka[b] = key.a;
+        ka.a_seed[b] = key.a_seed;
     }
     ka.dig = w.DIG;
     ka.xb = w.XB;
@@ -218,6 +219,7 @@ void eng_rotate(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* c
         ka.c0[b] = hoisted ? c0[0] : c0[b];
         ka.kb[b] = keys[b]->b;
         ka.ka[b] = keys[b]->a;
+        ka.a_seed[b] = keys[b]->a_seed;
         ka.galois[b] = galois[b];
     }
     ka.dig = w.DIG;
@@ -241,6 +243,7 @@ void eng_rotate_groups(fides_ctx* c, Workspace& w, int level, int ngroups, int n
         ka.c0[b] = c0[b / nper];
         ka.kb[b] = keys[b]->b;
         ka.ka[b] = keys[b]->a;
+        ka.a_seed[b] = keys[b]->a_seed;
         ka.galois[b] = galois[b];
         ka.dig_elem[b] = (uint8_t)(b / nper);
     }
