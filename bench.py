@@ -739,8 +739,9 @@ def main():
                          "bit 2 fused for batches of 4+ (default: the context's, 5)")
     ap.add_argument("--profile-roofline", action="store_true",
                     help="mark the roofline NTT loop for ncu --profile-from-start off")
-    ap.add_argument("--key-compression", type=int, default=1, choices=[0, 1],
-                    help="rotation keys store b and the seed of a (1, default) or both halves (0)")
+    ap.add_argument("--key-compression", type=int, default=1, choices=[0, 1, 2, 3],
+                    help="keys generated store b and the seed of a, a bit mask: bit 0 rotation keys "
+                         "(1, the default), bit 1 the relinearisation key; 0 stores both halves")
     ap.add_argument("--profile-step", action="store_true",
                     help="mark one batched HMult step (after the timed region) for ncu --profile-from-start off")
     args = ap.parse_args()

@@ -415,16 +415,18 @@ fides_status fides_keygen_relin(fides_ctx* ctx, const fides_sk* sk, uint64_t see
 fides_status fides_keygen_rotations(fides_ctx* ctx, const fides_sk* sk, int n, const int32_t* indices, int slots,
                                     uint64_t seed);
 fides_status fides_keygen_conjugate(fides_ctx* ctx, const fides_sk* sk, uint64_t seed);
-/* Key compression for the rotation and conjugation keys generated from here
- * on (1, the default): each stores its b half and the seed of its uniform a
- * half, which the key-switch kernels regenerate (a counter-based hash per
- * coefficient) instead of reading it: half the HBM per key and half the key
- * bytes read per rotation.  0 stores both halves.  The relinearisation key
- * always keeps its a half (batched HMults read it once per batch), and
- * uploaded or imported keys keep theirs.  The key layout this replaces:
+/* Key compression for the switching keys generated from here on, a bit
+ * mask: bit 0 the rotation and conjugation keys (the default, 1), bit 1 the
+ * relinearisation key.  A compressed key stores its b half and the seed of
+ * its uniform a half, which the key-switch kernels regenerate (one
+ * counter-based hash per coefficient) instead of reading it: half the HBM per
+ * key and half the key bytes read per key switch.  A compressed
+ * relinearisation key turns off the key switch fused into the digits' NTT
+ * row pass (batched HMults read an explicit a half once per batch).
+ * Uploaded or imported keys keep both halves.  The key layout this replaces:
  * KeySwitchingKey a / b (src/CKKS/KeySwitchingKey.cu:20-35); the reference
  * has no compressed form. */
-fides_status fides_set_key_compression(fides_ctx* ctx, int on);
+fides_status fides_set_key_compression(fides_ctx* ctx, int mask);
 /* Export generated switching keys (dnum*(L+K)*N words each) for interop tests. */
 fides_status fides_key_export(fides_ctx* ctx, uint32_t galois, uint64_t* b, uint64_t* a);
 /* Encode `slots` complex values (re, im interleaved) at `level` and `scale`

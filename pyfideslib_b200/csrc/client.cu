@@ -86,11 +86,11 @@ __global__ void k_small_to_rns(const int64_t* __restrict__ v, uint64_t* __restri
 }
 
 __global__ void k_fill_uniform(uint64_t* __restrict__ out, int N, int q0, const PrimeConst* __restrict__ pcs,
-                               uint64_t seed) {
+                               uint64_t stream) {
     const int limb = blockIdx.y;
     const uint64_t p = pcs[q0 + limb].p;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    out[(size_t)limb * N + j] = uniform_mod(seed, q0 + limb, (uint32_t)j, p);
+    out[(size_t)limb * N + j] = uniform_mod(stream, q0 + limb, (uint32_t)j, p);
 }
 
 // b = -a * sb + e (+ pmod_i * sg on limbs with lo <= prime < hi)
@@ -209,7 +209,7 @@ fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg
         uint64_t* kb = key.b + (size_t)d * NP * N;
         uint64_t* ka = compress ? atmp : key.a + (size_t)d * NP * N;
         count_launches(1);
-        k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(ka, N, 0, c->dev.pc, key.a_seed + d + 1);
+        k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(ka, N, 0, c->dev.pc, uniform_stream(key.a_seed, d + 1));
         fides_status s = upload_small(c, gaussian(N, seed ^ (0xABCDull + d)), e, 0, NP);
         if (s != FIDES_OK) return s;
         ntt_forward(c->dev, map_single(e, e, NP, NP, 0), FL_PLAIN, FS_PLAIN, c->st);
@@ -292,9 +292,10 @@ fides_status fides_keygen_relin(fides_ctx* c, const fides_sk* sk, uint64_t seed)
     uint64_t* s2 = nullptr;
     if (cudaMallocAsync((void**)&s2, (size_t)NP * c->N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "s^2");
     launch_elementwise(c->dev, EW_MUL, NP, 0, sk->s, sk->s, s2, c->st);
-    // the relinearisation key keeps its a half: batched HMults read it once
-    // per batch, where regenerating it would cost every element
-    fides_status s = gen_switch_key(c, sk->s, s2, seed, c->relin, false);
+    // bit 1 of the compression mask: batched HMults read an explicit a half
+    // once per batch and serve it from L2, where a seeded one is regenerated
+    // for every element (and the fused row-pass key switch needs it stored)
+    fides_status s = gen_switch_key(c, sk->s, s2, seed, c->relin, (c->compress_keys & 2) != 0);
     cudaFreeAsync(s2, c->st);
     if (s == FIDES_OK) c->has_relin = true;
     return s;
@@ -321,7 +322,8 @@ static fides_status keygen_galois(fides_ctx* c, const fides_sk* sk, uint32_t g, 
     uint64_t* sr = nullptr;
     if (cudaMallocAsync((void**)&sr, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "s rot");
     launch_automorph(c->dev, NP, sk->s, sr, ginv, c->st);
-    fides_status s = gen_switch_key(c, sr, sk->s, seed ^ ((uint64_t)g << 20), c->galois_keys[g], c->compress_keys);
+    fides_status s = gen_switch_key(c, sr, sk->s, seed ^ ((uint64_t)g << 20), c->galois_keys[g],
+                                    (c->compress_keys & 1) != 0);
     cudaFreeAsync(sr, c->st);
     return s;
 }
@@ -345,10 +347,10 @@ fides_status fides_keygen_rotations(fides_ctx* c, const fides_sk* sk, int n, con
     return FIDES_OK;
 }
 
-fides_status fides_set_key_compression(fides_ctx* c, int on) {
-    if (!c || on < 0 || on > 1) return FIDES_BAD_ARG;
+fides_status fides_set_key_compression(fides_ctx* c, int mask) {
+    if (!c || mask < 0 || mask > 3) return FIDES_BAD_ARG;
     std::lock_guard<std::recursive_mutex> lk(c->mu);
-    c->compress_keys = on != 0;
+    c->compress_keys = mask;
     return FIDES_OK;
 }
 
@@ -383,7 +385,7 @@ fides_status fides_key_export(fides_ctx* c, uint32_t galois, uint64_t* b, uint64
         if (cudaMallocAsync((void**)&t, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "key export");
         for (int d = 0; d < c->dnum; ++d) {
             count_launches(1);
-            k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(t, N, 0, c->dev.pc, k->a_seed + d + 1);
+            k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(t, N, 0, c->dev.pc, uniform_stream(k->a_seed, d + 1));
             cudaMemcpyAsync(a + (size_t)d * NP * N, t, (size_t)NP * N * 8, cudaMemcpyDeviceToHost, c->st);
         }
         cudaFreeAsync(t, c->st);
@@ -434,7 +436,7 @@ fides_status fides_encrypt(fides_ctx* c, const fides_sk* sk, const double* value
     if (s == FIDES_OK) {
         ntt_forward(c->dev, map_single(e, e, n, n, 0), FL_PLAIN, FS_PLAIN, c->st);
         count_launches(1);
-        k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c1(N), N, 0, c->dev.pc, seed * 2654435761ull + 17);
+        k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c1(N), N, 0, c->dev.pc, uniform_stream(seed * 2654435761ull + 17, 0));
         launch_elementwise(c->dev, EW_ADD, n, 0, e, m, e, c->st);  // e + m
         // c0 = -a s + (e + m): key_combine with no gadget term
         count_launches(1);
@@ -472,7 +474,7 @@ fides_status fides_keygen_public(fides_ctx* c, const fides_sk* sk, uint64_t seed
     uint64_t* e = nullptr;
     if (cudaMallocAsync((void**)&e, (size_t)L * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "pk tmp");
     count_launches(1);
-    k_fill_uniform<<<dim3(N / 256, L), 256, 0, c->st>>>(pk->a, N, 0, c->dev.pc, seed * 0x9E3779B97F4A7C15ull + 99);
+    k_fill_uniform<<<dim3(N / 256, L), 256, 0, c->st>>>(pk->a, N, 0, c->dev.pc, uniform_stream(seed * 0x9E3779B97F4A7C15ull + 99, 0));
     fides_status s = upload_small(c, gaussian(N, seed ^ 0x7EA5), e, 0, L);
     if (s == FIDES_OK) {
         ntt_forward(c->dev, map_single(e, e, L, L, 0), FL_PLAIN, FS_PLAIN, c->st);
@@ -578,8 +580,8 @@ fides_status fides_ct_random(fides_ctx* c, int level, uint64_t seed, fides_ct** 
     }
     const int N = c->N, n = level + 1;
     count_launches(2);
-    k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c0(), N, 0, c->dev.pc, seed * 0x9E3779B97F4A7C15ull + 1);
-    k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c1(N), N, 0, c->dev.pc, seed * 0x9E3779B97F4A7C15ull + 2);
+    k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c0(), N, 0, c->dev.pc, uniform_stream(seed * 0x9E3779B97F4A7C15ull + 1, 0));
+    k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c1(N), N, 0, c->dev.pc, uniform_stream(seed * 0x9E3779B97F4A7C15ull + 2, 0));
     ct->level = level;
     ct->scale = c->default_scale;
     ct->noise_deg = 1;

@@ -17,10 +17,16 @@ constexpr int kMaxBatch = 32;  // ciphertexts per batched launch (blockIdx.z)
 // synchronising call of the context reports FIDES_TIMEOUT and clears the word.
 constexpr uint32_t kDevErrTensorWait = 1u;  // a tensor-core conversion stopped waiting for its MMAs
 
-// Counter-based hash behind every seeded uniform draw (a halves of keys and
-// public keys, synthetic ciphertexts): a 64-bit finaliser of MurmurHash3's
-// form.  uniform_mod(seed, prime, j) is residue j of the prime's limb.
-__device__ __forceinline__ uint64_t hash64(uint64_t x) {
+// Counter-based generator behind every seeded uniform draw (a halves of keys
+// and public keys, synthetic ciphertexts).  hash64 is a 64-bit finaliser of
+// MurmurHash3's form (a bijection with full avalanche).  A draw is keyed by a
+// stream word, uniform_stream(seed, tag) = hash64(seed) ^ tag << 48, mixed
+// once on the host; residue j of prime t is
+//   uniform_mod(stream, t, j, p) = floor(hash64(stream ^ t << 32 ^ j) * p / 2^64),
+// one finaliser per residue.  The counter stream ^ t << 32 ^ j is distinct for
+// every (tag, t, j) of a seed (tag, t < 2^16, j < 2^32).  Not a cryptographic
+// generator.
+__host__ __device__ __forceinline__ uint64_t hash64(uint64_t x) {
     x ^= x >> 33;
     x *= 0xff51afd7ed558ccdull;
     x ^= x >> 33;
@@ -28,8 +34,11 @@ __device__ __forceinline__ uint64_t hash64(uint64_t x) {
     x ^= x >> 33;
     return x;
 }
-__device__ __forceinline__ uint64_t uniform_mod(uint64_t seed, int prime, uint32_t j, uint64_t p) {
-    return __umul64hi(hash64(seed ^ hash64(((uint64_t)prime << 32) | (uint64_t)j)), p);
+__host__ __device__ __forceinline__ uint64_t uniform_stream(uint64_t seed, uint32_t tag) {
+    return hash64(seed) ^ ((uint64_t)tag << 48);
+}
+__device__ __forceinline__ uint64_t uniform_mod(uint64_t stream, int prime, uint32_t j, uint64_t p) {
+    return __umul64hi(hash64(stream ^ ((uint64_t)prime << 32) ^ j), p);
 }
 
 // Read-only view of the context tables in HBM, passed by value to kernels.

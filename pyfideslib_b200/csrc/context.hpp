@@ -52,7 +52,7 @@ namespace fides {
 
 struct SwitchKey {
     uint64_t* b = nullptr;  // [dnum][L+K][N]
-    uint64_t* a = nullptr;  // null for a seeded key: digit d's a half is uniform_mod(a_seed + d + 1, prime, j)
+    uint64_t* a = nullptr;  // null for a seeded key: digit d's a half is uniform_mod(uniform_stream(a_seed, d + 1), prime, j)
     uint64_t a_seed = 0;
     bool seeded = false;
 };
@@ -119,7 +119,7 @@ struct fides_ctx {
     std::vector<float> tune_ms;
     int tuned_conv = 0;  // base-conversion accumulator: 0 128-bit, 1 split 32-bit products
     std::vector<float> conv_ms;
-    bool compress_keys = true;  // Galois keys generated here store b and a seed for a
+    int compress_keys = 1;  // keys generated here that store b and a seed for a: bit 0 Galois, bit 1 relinearisation
     std::string last_error;
     std::recursive_mutex mu;
 

@@ -193,7 +193,7 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
         ka.own[b] = w.E2 + (size_t)b * w.stride;
         ka.kb[b] = key.b;
         ka.ka[b] = key.a;
-        ka.a_seed[b] = key.a_seed;
+        ka.a_seed[b] = key.a ? 0 : uniform_stream(key.a_seed, 0);
     }
     ka.dig = w.DIG;
     ka.xb = w.XB;
@@ -219,7 +219,7 @@ void eng_rotate(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* c
         ka.c0[b] = hoisted ? c0[0] : c0[b];
         ka.kb[b] = keys[b]->b;
         ka.ka[b] = keys[b]->a;
-        ka.a_seed[b] = keys[b]->a_seed;
+        ka.a_seed[b] = keys[b]->a ? 0 : uniform_stream(keys[b]->a_seed, 0);
         ka.galois[b] = galois[b];
     }
     ka.dig = w.DIG;
@@ -243,7 +243,7 @@ void eng_rotate_groups(fides_ctx* c, Workspace& w, int level, int ngroups, int n
         ka.c0[b] = c0[b / nper];
         ka.kb[b] = keys[b]->b;
         ka.ka[b] = keys[b]->a;
-        ka.a_seed[b] = keys[b]->a_seed;
+        ka.a_seed[b] = keys[b]->a ? 0 : uniform_stream(keys[b]->a_seed, 0);
         ka.galois[b] = galois[b];
         ka.dig_elem[b] = (uint8_t)(b / nper);
     }

@@ -82,7 +82,7 @@ struct KsArgs {
     const uint64_t* own[kMaxBatch];  // evaluation values of the key-switched polynomial (own-digit limbs)
     const uint64_t* kb[kMaxBatch];   // switching key halves of each element
     const uint64_t* ka[kMaxBatch];   // null: a seeded key, a half regenerated from a_seed
-    uint64_t a_seed[kMaxBatch];
+    uint64_t a_seed[kMaxBatch];      // seeded keys: uniform_stream(key seed, 0); digit d's stream is this ^ (d+1) << 48
     const uint64_t* c0[kMaxBatch];   // rotations: c0 of the input (P*c0 added), else null
     uint32_t galois[kMaxBatch];      // rotations: automorphism X -> X^g applied as a gather, else 0
     const uint64_t* dig;             // ModUp digits of element 0

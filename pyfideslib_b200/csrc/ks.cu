@@ -293,8 +293,8 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
     const size_t kstride = (size_t)(ctx.L + ctx.K) * ctx.N;
     const size_t boff = (size_t)bi * args.bstride;
     const uint64_t* kb = args.kb[bi];
-    const uint64_t* ka = args.ka[bi];  // null: seeded, digit d's a half is uniform_mod(aseed + d + 1, t, j)
-    const uint64_t aseed = args.a_seed[bi];
+    const uint64_t* ka = args.ka[bi];  // null: seeded, digit d's a half is uniform_mod(astream ^ (d+1) << 48, t, j)
+    const uint64_t astream = args.a_seed[bi];
     // source limb of each digit for this prime (GRP, grouped hoisting: the
     // element's ModUp is that of its group, a table entry)
     const int gi = GRP ? (int)args.dig_elem[bi] : bi;
@@ -329,8 +329,8 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                     if (ka) {
                         a = *reinterpret_cast<const ulonglong2*>(ka + d * kstride + (size_t)t * ctx.N + j);
                     } else {
-                        a.x = uniform_mod(aseed + d + 1, t, (uint32_t)j, pc.p);
-                        a.y = uniform_mod(aseed + d + 1, t, (uint32_t)j + 1, pc.p);
+                        a.x = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j, pc.p);
+                        a.y = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j + 1, pc.p);
                     }
                     const double x0 = as_f64(fp_from_u(x.x)), x1 = as_f64(fp_from_u(x.y));
                     sb0 = __dadd_rn(sb0, fp_mulmod(x0, as_f64(fp_from_u(b.x)), p, pinv));
@@ -361,8 +361,8 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                 if (ka) {
                     a = *reinterpret_cast<const ulonglong2*>(ka + d * kstride + (size_t)t * ctx.N + j);
                 } else {
-                    a.x = uniform_mod(aseed + d + 1, t, (uint32_t)j, pc.p);
-                    a.y = uniform_mod(aseed + d + 1, t, (uint32_t)j + 1, pc.p);
+                    a.x = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j, pc.p);
+                    a.y = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j + 1, pc.p);
                 }
                 sb0.mac(x.x, b.x);
                 sb1.mac(x.y, b.y);
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                         sb = __dadd_rn(sb, fp_mulmod(x, as_f64(fp_from_u(kb[d * kstride + (size_t)t * ctx.N + src])),
                                                      p, pinv));
                         const uint64_t av = ka ? ka[d * kstride + (size_t)t * ctx.N + src]
-                                               : uniform_mod(aseed + d + 1, t, src, pc.p);
+                                               : uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, src, pc.p);
                         sa = __dadd_rn(sa, fp_mulmod(x, as_f64(fp_from_u(av)), p, pinv));
                     }
                 }
@@ -413,7 +413,8 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
             if (d < nd) {
                 const uint64_t x = srcs[d][src];
                 sb.mac(x, kb[d * kstride + (size_t)t * ctx.N + src]);
-                sa.mac(x, ka ? ka[d * kstride + (size_t)t * ctx.N + src] : uniform_mod(aseed + d + 1, t, src, pc.p));
+                sa.mac(x, ka ? ka[d * kstride + (size_t)t * ctx.N + src]
+                             : uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, src, pc.p));
             }
         }
         const uint64_t* c0 = args.c0[bi];

@@ -64,3 +64,33 @@ def test_compressed_keys_in_batched_transform_and_bootstrap():
         outs[comp] = [o.download() for o in cc.EvalBootstrapBatch([ct, ct])]
     for x, y in zip(outs[1], outs[0]):
         assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+
+
+def test_compressed_relin_key_bitexact():
+    """A compressed relinearisation key (mask bit 1): single and batched
+    HMults (a batch of 6, which with a full key takes the key switch fused
+    into the row pass) equal the same key stored in full and the oracle's
+    HMult with the exported key."""
+    from pyfideslib_b200._capi import lib
+
+    cc, oc = make_pair(12, 8, 3, 3)
+    sk = cc.KeyGen(seed=51, hamming_weight=64)
+    level = 7
+    raw = [(rand_ct(oc, level, 5100 + 4 * i), rand_ct(oc, level, 5102 + 4 * i)) for i in range(6)]
+    A = [cc.upload(*a) for a, _ in raw]
+    B = [cc.upload(*b) for _, b in raw]
+    res = {}
+    for mask in (3, 0):
+        assert lib.fides_set_key_compression(cc._h, mask) == 0
+        cc.EvalMultKeyGen(sk, seed=9)
+        single = cc.EvalMult(A[0], B[0]).download()
+        batch = [o.download() for o in cc.EvalMultBatch(A, B)]
+        res[mask] = [single] + batch
+        if mask == 3:
+            kb, ka = cc.export_key(0)
+            (a0, a1), (b0, b1) = raw[0]
+            want = oc.hmult(level, a0, a1, b0, b1, kb, ka, rescale=False)
+            assert np.array_equal(single[0], want[0]) and np.array_equal(single[1], want[1])
+    for x, y in zip(res[3], res[0]):
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+    assert lib.fides_set_key_compression(cc._h, 1) == 0
