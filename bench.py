@@ -41,13 +41,39 @@ sys.path.insert(0, ROOT)
 METRIC = "key-switched HMult/s at N=2^16 L=30 (batched vs per-op), bootstrap ms, NTT HBM GB/s"
 LOGN, L, K, DNUM = 16, 30, 10, 3
 # DRAM bytes (read + write) of one batched forward NTT (32 polynomials x 30
-# limbs at N=2^16), from an ncu capture of that launch pair
+# limbs at N=2^16): a constant taken from one ncu capture of that launch pair
 # (dram__bytes_read.sum + dram__bytes_write.sum of k_ntt_fwd_cols and
-# k_ntt_fwd_rows; ncu flushes the caches before each kernel).  About twice the
-# algorithmic bytes: the column pass writes the 960 intermediate limbs
-# (480 MB, more than L2) and the row pass reads them back; twiddles add 32 MB
-# (read once per prime for the whole batch).
-NTT_BATCH_TRAFFIC_BYTES = 1930.1e6  # profiles/ntt_fwd_batch32x30_n16.md (503.5 + 443.6 + 534.8 + 448.2 MB)
+# k_ntt_fwd_rows, forward variant 9, caches flushed before each kernel), stale
+# after any change to those kernels; --ntt-traffic-csv reads a fresh capture
+# instead.  About twice the algorithmic bytes: the column pass writes the 960
+# intermediate limbs (480 MB, more than L2) and the row pass reads them back;
+# twiddles add 32 MB (read once per prime for the whole batch).
+NTT_BATCH_TRAFFIC_BYTES = 1926.5e6  # 503.5 + 443.6 (cols) + 534.8 + 444.6 (rows) MB
+NTT_BATCH_TRAFFIC_SOURCE = "constant from one ncu capture of the launch pair (variant 9, caches flushed)"
+_UNITS = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "Tbyte": 1e12}
+
+
+def ntt_traffic_from_csv(path):
+    """DRAM bytes of the last k_ntt_fwd_cols + k_ntt_fwd_rows launch pair in
+    an ncu --csv log of dram__bytes_read.sum and dram__bytes_write.sum."""
+    import csv
+
+    per = {}
+    for r in csv.DictReader(line for line in open(path) if line.startswith('"')):
+        name = r.get("Metric Name", "")
+        if not name.startswith("dram__bytes_"):
+            continue
+        kern = r["Kernel Name"].split("(")[0].split("<")[0].split()[-1]
+        if kern not in ("k_ntt_fwd_cols", "k_ntt_fwd_rows"):
+            continue
+        v = float(r["Metric Value"].replace(",", "")) * _UNITS.get(r["Metric Unit"], 1.0)
+        per.setdefault((int(r["ID"]), kern), 0.0)
+        per[(int(r["ID"]), kern)] += v
+    cols = [v for (i, k), v in sorted(per.items()) if k == "k_ntt_fwd_cols"]
+    rows = [v for (i, k), v in sorted(per.items()) if k == "k_ntt_fwd_rows"]
+    if not cols or not rows:
+        raise SystemExit("no k_ntt_fwd_cols / k_ntt_fwd_rows DRAM metrics in " + path)
+    return cols[-1] + rows[-1]
 
 
 def peaks():
@@ -633,6 +659,10 @@ def run_ours(args):
     if args.profile_roofline:
         torch.cuda.profiler.stop()
     ntt_ms = e0.elapsed_time(e1) / reps
+    traffic, traffic_source = NTT_BATCH_TRAFFIC_BYTES, NTT_BATCH_TRAFFIC_SOURCE
+    if args.ntt_traffic_csv:
+        traffic = ntt_traffic_from_csv(args.ntt_traffic_csv)
+        traffic_source = "ncu capture " + os.path.basename(args.ntt_traffic_csv)
     # single polynomial, 30 limbs, cycling through 10 polynomials (157 MB)
     single = bufs[0].view(-1)
     cc.Synchronize()
@@ -699,7 +729,7 @@ def run_ours(args):
                "roofline": {"kernel": "ntt_forward batched (32 polynomials x 30 limbs, k_ntt_fwd_cols + k_ntt_fwd_rows)",
                             "bound": "hbm", "achieved": achieved,
                             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                            "traffic": NTT_BATCH_TRAFFIC_BYTES, "traffic_source": "ncu capture, caches flushed",
+                            "traffic": traffic, "traffic_source": traffic_source,
                             "algorithmic_bytes": ntt_bytes, "us_per_launch": ntt_ms * 1e3,
                             "single_30limb_us": single_us,
                             "single_30limb_gbs": 16.0 * N * nl / (single_us * 1e-6) / 1e9},
@@ -742,6 +772,9 @@ def main():
     ap.add_argument("--key-compression", type=int, default=1, choices=[0, 1, 2, 3],
                     help="keys generated store b and the seed of a, a bit mask: bit 0 rotation keys "
                          "(1, the default), bit 1 the relinearisation key; 0 stores both halves")
+    ap.add_argument("--ntt-traffic-csv", default=None,
+                    help="ncu --csv log with dram__bytes_read.sum and dram__bytes_write.sum of the roofline "
+                         "NTT pair (--profile-roofline); its last pair gives roofline.traffic")
     ap.add_argument("--profile-step", action="store_true",
                     help="mark one batched HMult step (after the timed region) for ncu --profile-from-start off")
     args = ap.parse_args()

@@ -280,8 +280,13 @@ void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt,
 // each product x k is reduced to |r| <= 0.875p, the sum of up to 8 digits
 // stays below 7p < 2^53, and one centring plus a floor reduction give the
 // canonical residue -- the same values as the 128-bit integer sums.
-template <int VEC, class ACC, bool FPK, bool GRP = false>
-__global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx ctx, int level, int nb,
+// SEED: some element's key is seeded (ka null), its a half regenerated per
+// coefficient; the instantiation without it carries no generator code and
+// keeps the register count of the plain streaming loop (32-40).  Left free,
+// the unrolled digit loop with the generator takes 56-72 registers; the
+// bound holds it at 48 (FP64 sums) or 40 so that 5-6 blocks stay resident.
+template <int VEC, class ACC, bool FPK, bool GRP = false, bool SEED = false>
+__global__ void __launch_bounds__(256, SEED ? (FPK ? 5 : 6) : 0) k_ks_inner(const __grid_constant__ DevCtx ctx, int level, int nb,
                                                   const __grid_constant__ KsArgs args) {
     const int n = level + 1;
     const int m = blockIdx.y;
@@ -326,7 +331,7 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                     const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(srcs[d] + j);
                     const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(kb + d * kstride + (size_t)t * ctx.N + j);
                     ulonglong2 a;
-                    if (ka) {
+                    if (!SEED || ka) {
                         a = *reinterpret_cast<const ulonglong2*>(ka + d * kstride + (size_t)t * ctx.N + j);
                     } else {
                         a.x = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j, pc.p);
@@ -358,7 +363,7 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                 const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(srcs[d] + j);
                 const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(kb + d * kstride + (size_t)t * ctx.N + j);
                 ulonglong2 a;
-                if (ka) {
+                if (!SEED || ka) {
                     a = *reinterpret_cast<const ulonglong2*>(ka + d * kstride + (size_t)t * ctx.N + j);
                 } else {
                     a.x = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j, pc.p);
@@ -392,8 +397,8 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
                         const double x = as_f64(fp_from_u(srcs[d][src]));
                         sb = __dadd_rn(sb, fp_mulmod(x, as_f64(fp_from_u(kb[d * kstride + (size_t)t * ctx.N + src])),
                                                      p, pinv));
-                        const uint64_t av = ka ? ka[d * kstride + (size_t)t * ctx.N + src]
-                                               : uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, src, pc.p);
+                        const uint64_t av = !SEED || ka ? ka[d * kstride + (size_t)t * ctx.N + src]
+                                                        : uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, src, pc.p);
                         sa = __dadd_rn(sa, fp_mulmod(x, as_f64(fp_from_u(av)), p, pinv));
                     }
                 }
@@ -413,8 +418,8 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
             if (d < nd) {
                 const uint64_t x = srcs[d][src];
                 sb.mac(x, kb[d * kstride + (size_t)t * ctx.N + src]);
-                sa.mac(x, ka ? ka[d * kstride + (size_t)t * ctx.N + src]
-                             : uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, src, pc.p));
+                sa.mac(x, !SEED || ka ? ka[d * kstride + (size_t)t * ctx.N + src]
+                                      : uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, src, pc.p));
             }
         }
         const uint64_t* c0 = args.c0[bi];
@@ -427,30 +432,41 @@ __global__ void __launch_bounds__(256) k_ks_inner(const __grid_constant__ DevCtx
     }
 }
 
+template <int VEC, class ACC, bool FPK, bool GRP>
+static void ks_inner_go(const DevCtx& ctx, int level, int nb, const KsArgs& args, bool seeded, dim3 g,
+                        cudaStream_t st) {
+    if (seeded)
+        k_ks_inner<VEC, ACC, FPK, GRP, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
+    else
+        k_ks_inner<VEC, ACC, FPK, GRP, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
+}
+
 void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, bool plain, cudaStream_t st) {
     count_launches(1);
+    bool seeded = false;
+    for (int b = 0; b < nb; ++b) seeded = seeded || args.ka[b] == nullptr;
     if (plain) {
         dim3 g(ctx.N / 512 * nb, level + 1 + ctx.K);
         if (ctx.ks_variant & 1)
-            k_ks_inner<1, Acc128, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            ks_inner_go<1, Acc128, true, false>(ctx, level, nb, args, seeded, g, st);
         else if (ctx.conv_variant == 1)
-            k_ks_inner<1, AccSplit, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            ks_inner_go<1, AccSplit, false, false>(ctx, level, nb, args, seeded, g, st);
         else
-            k_ks_inner<1, Acc128, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            ks_inner_go<1, Acc128, false, false>(ctx, level, nb, args, seeded, g, st);
     } else if (args.dig_group > 0) {
         dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
         if (ctx.ks_variant & 1)
-            k_ks_inner<0, Acc128, true, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            ks_inner_go<0, Acc128, true, true>(ctx, level, nb, args, seeded, g, st);
         else
-            k_ks_inner<0, Acc128, false, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            ks_inner_go<0, Acc128, false, true>(ctx, level, nb, args, seeded, g, st);
     } else {
         dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
         if (ctx.ks_variant & 1)
-            k_ks_inner<0, Acc128, true><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            ks_inner_go<0, Acc128, true, false>(ctx, level, nb, args, seeded, g, st);
         else if (ctx.conv_variant == 1)
-            k_ks_inner<0, AccSplit, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            ks_inner_go<0, AccSplit, false, false>(ctx, level, nb, args, seeded, g, st);
         else
-            k_ks_inner<0, Acc128, false><<<g, 256, 0, st>>>(ctx, level, nb, args);
+            ks_inner_go<0, Acc128, false, false>(ctx, level, nb, args, seeded, g, st);
     }
 }
 

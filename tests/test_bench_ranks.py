@@ -75,3 +75,24 @@ def test_reference_arm_nonzero_rank_exits_without_work():
                         "--steps", "1", "--warmup", "3"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_ntt_traffic_from_ncu_csv(tmp_path):
+    """roofline.traffic from a capture: the last cols + rows pair's DRAM
+    read + write bytes, units converted."""
+    import bench
+
+    hdr = '"ID","Process ID","Process Name","Host Name","Kernel Name","Context","Stream","Block Size","Grid Size",' \
+          '"Device","CC","Section Name","Metric Name","Metric Unit","Metric Value"\n'
+    rows = []
+    for i, (k, rd, wr) in enumerate([("k_ntt_fwd_cols<8, 8, 3, 0, 1, 1>", "1.0", "2.0"),
+                                     ("k_ntt_fwd_rows<8, 8, 3, 0, 1, 1, 1>", "3.0", "4.0"),
+                                     ("k_ntt_fwd_cols<8, 8, 3, 0, 1, 1>", "503.5", "443.6"),
+                                     ("k_ntt_fwd_rows<8, 8, 3, 0, 1, 1, 1>", "534,800", "444.6")]):
+        unit_r = "Kbyte" if "," in rd else "Mbyte"
+        for m, u, v in (("dram__bytes_read.sum", unit_r, rd), ("dram__bytes_write.sum", "Mbyte", wr)):
+            rows.append('"%d","1","python3","h","void %s(DevCtx, LimbMap)","1","7","(256, 1, 1)","(16, 32, 30)",'
+                        '"0","10.0","Command line profiler metrics","%s","%s","%s"\n' % (i, k, m, u, v))
+    p = tmp_path / "t.csv"
+    p.write_text("==PROF== Connected\n" + hdr + "".join(rows))
+    assert abs(bench.ntt_traffic_from_csv(str(p)) - 1926.5e6) < 1.0
