@@ -322,12 +322,29 @@ fides_status fides_set_ntt_variant(fides_ctx* c, int variant) {
     return FIDES_OK;
 }
 
-static fides_status upload_key(fides_ctx* c, SwitchKey& k, const uint64_t* b, const uint64_t* a) {
-    const size_t words = (size_t)c->dnum * (c->L + c->K) * c->N;
+// galois != 0: the key is stored permuted to the rotation's output order,
+// entry j = uploaded entry slot(galois, j) (the key-switch kernel's layout)
+static fides_status upload_key(fides_ctx* c, SwitchKey& k, const uint64_t* b, const uint64_t* a,
+                               uint32_t galois = 0) {
+    const int nlimbs = c->dnum * (c->L + c->K);
+    const size_t words = (size_t)nlimbs * c->N;
     fides_status s = key_alloc(c, k, false);
     if (s != FIDES_OK) return s;
-    cudaMemcpyAsync(k.b, b, words * 8, cudaMemcpyHostToDevice, c->st);
-    cudaMemcpyAsync(k.a, a, words * 8, cudaMemcpyHostToDevice, c->st);
+    if (!galois) {
+        cudaMemcpyAsync(k.b, b, words * 8, cudaMemcpyHostToDevice, c->st);
+        cudaMemcpyAsync(k.a, a, words * 8, cudaMemcpyHostToDevice, c->st);
+    } else {
+        uint64_t* tmp = nullptr;
+        if (cudaMallocAsync((void**)&tmp, words * 8, c->st) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(c, FIDES_OOM, "key upload scratch");
+        }
+        cudaMemcpyAsync(tmp, b, words * 8, cudaMemcpyHostToDevice, c->st);
+        launch_automorph(c->dev, nlimbs, tmp, k.b, galois, c->st);
+        cudaMemcpyAsync(tmp, a, words * 8, cudaMemcpyHostToDevice, c->st);
+        launch_automorph(c->dev, nlimbs, tmp, k.a, galois, c->st);
+        cudaFreeAsync(tmp, c->st);
+    }
     cudaStreamSynchronize(c->st);
     return check_cuda(c, "key upload");
 }
@@ -344,7 +361,7 @@ fides_status fides_key_upload_galois(fides_ctx* ctx, uint32_t galois, const uint
     if (!ctx || !b || !a || !(galois & 1) || galois >= 2u * (uint32_t)ctx->N) return FIDES_BAD_ARG;
     Guard g(ctx);
     SwitchKey& k = ctx->galois_keys[galois];
-    return upload_key(ctx, k, b, a);
+    return upload_key(ctx, k, b, a, galois);
 }
 
 uint32_t fides_rotation_galois(const fides_ctx* ctx, int32_t index, int slots) {

@@ -315,14 +315,18 @@ static uint32_t inv_mod_2n(uint32_t g, uint32_t m) {
     return (uint32_t)(t < 0 ? t + m : t);
 }
 
+// The Galois key of g in the permuted layout of the key-switch kernel: entry j
+// pairs with rotation output j, k'[j] = k[slot(g, j)] for the key k that
+// switches sigma_g^-1(s) to s.  Written out, k' = (-a' s + e' + P sigma_g(s), a')
+// with sigma_g(s)[j] = s[slot(g, j)]: a switching key from sigma_g(s) to s in
+// the plain layout, a' uniform and e' fresh noise (both distributions are
+// invariant under the permutation).
 static fides_status keygen_galois(fides_ctx* c, const fides_sk* sk, uint32_t g, uint64_t seed) {
     const int NP = c->L + c->K, N = c->N;
-    // sigma_g^-1(s) = s(X^{g^-1}): gather with the inverse element
-    const uint32_t ginv = inv_mod_2n(g, 2u * (uint32_t)N);
     uint64_t* sr = nullptr;
     if (cudaMallocAsync((void**)&sr, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "s rot");
-    launch_automorph(c->dev, NP, sk->s, sr, ginv, c->st);
-    fides_status s = gen_switch_key(c, sr, sk->s, seed ^ ((uint64_t)g << 20), c->galois_keys[g],
+    launch_automorph(c->dev, NP, sk->s, sr, g, c->st);
+    fides_status s = gen_switch_key(c, sk->s, sr, seed ^ ((uint64_t)g << 20), c->galois_keys[g],
                                     (c->compress_keys & 1) != 0);
     cudaFreeAsync(sr, c->st);
     return s;
@@ -375,21 +379,39 @@ fides_status fides_key_export(fides_ctx* c, uint32_t galois, uint64_t* b, uint64
         k = &it->second;
     }
     const int NP = c->L + c->K, N = c->N;
-    const size_t words = (size_t)c->dnum * NP * N;
-    cudaMemcpyAsync(b, k->b, words * 8, cudaMemcpyDeviceToHost, c->st);
-    if (k->a) {
-        cudaMemcpyAsync(a, k->a, words * 8, cudaMemcpyDeviceToHost, c->st);
-    } else {
+    const int nlimbs = c->dnum * NP;
+    const size_t words = (size_t)nlimbs * N;
+    // a Galois key leaves in the plain layout: entry slot(g, j) = held entry j,
+    // i.e. plain[i] = held[slot(g^-1, i)]
+    const uint32_t ginv = galois ? inv_mod_2n(galois, 2u * (uint32_t)N) : 0;
+    uint64_t* t = nullptr;
+    if ((galois || !k->a) && cudaMallocAsync((void**)&t, 2 * words * 8, c->st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FIDES_OOM, "key export");
+    }
+    const uint64_t* ka = k->a;
+    if (!ka) {
         // a seeded key: its a half regenerated digit by digit
-        uint64_t* t = nullptr;
-        if (cudaMallocAsync((void**)&t, (size_t)NP * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "key export");
+        uint64_t* ta = t + words;
         for (int d = 0; d < c->dnum; ++d) {
             count_launches(1);
-            k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(t, N, 0, c->dev.pc, uniform_stream(k->a_seed, d + 1));
-            cudaMemcpyAsync(a + (size_t)d * NP * N, t, (size_t)NP * N * 8, cudaMemcpyDeviceToHost, c->st);
+            k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(ta + (size_t)d * NP * N, N, 0, c->dev.pc,
+                                                                 uniform_stream(k->a_seed, d + 1));
         }
-        cudaFreeAsync(t, c->st);
+        ka = ta;
     }
+    if (galois) {
+        launch_automorph(c->dev, nlimbs, k->b, t, ginv, c->st);
+        cudaMemcpyAsync(b, t, words * 8, cudaMemcpyDeviceToHost, c->st);
+        // stream order: the gather below overwrites t's first half only after
+        // the copy of b has read it (a regenerated a sits in the second half)
+        launch_automorph(c->dev, nlimbs, ka, t, ginv, c->st);
+        cudaMemcpyAsync(a, t, words * 8, cudaMemcpyDeviceToHost, c->st);
+    } else {
+        cudaMemcpyAsync(b, k->b, words * 8, cudaMemcpyDeviceToHost, c->st);
+        cudaMemcpyAsync(a, ka, words * 8, cudaMemcpyDeviceToHost, c->st);
+    }
+    if (t) cudaFreeAsync(t, c->st);
     cudaStreamSynchronize(c->st);
     return check_cuda(c, "key export");
 }

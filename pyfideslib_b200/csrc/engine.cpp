@@ -15,7 +15,11 @@ namespace fides {
 
 namespace {
 
-constexpr int kFuseMinBatch = 4;
+// batch size from which the key switch fused into the digits' row pass wins
+// (B200, N=2^16, L=30, dnum=3, ms per batched step unfused / fused: 4 pairs
+// 0.986 / 0.997, 8 pairs 1.854 / 1.844, 16 pairs 3.578 / 3.529, 32 pairs
+// 7.008 / 6.886)
+constexpr int kFuseMinBatch = 8;
 
 LimbSeg seg_ws(const uint64_t* in, uint64_t* out, int count, int nq, int q0, int level, size_t bstride) {
     LimbSeg g{};
@@ -162,8 +166,8 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
     im.total = n;
     ntt_inverse(c->dev, im, IL_PLAIN, IS_MODUP, w.st);
     // fused inner product: forced (bit 1), or for batches of at least
-    // kFuseMinBatch elements (bit 2; a single element's fused launch is
-    // about two waves of long CTAs and measured slower than the two kernels)
+    // kFuseMinBatch elements (bit 2; a small batch's fused launch is a few
+    // waves of long CTAs at 2 per SM and measured slower than the two kernels)
     const bool fuse = ((c->dev.ks_variant & 2) || ((c->dev.ks_variant & 4) && nb >= kFuseMinBatch)) &&
                       ntt_rows_keyswitch_supported(c->dev) && key.a != nullptr;
     if (fuse) {

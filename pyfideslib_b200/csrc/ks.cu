@@ -11,8 +11,9 @@
 //     them, so each input limb is read from HBM once per digit;
 //   * the inner product reads each key limb once and accumulates both key
 //     halves in 128-bit registers, reducing once per output;
-//   * rotations fold the automorphism into the inner product as a gather, so
-//     stores stay coalesced.
+//   * rotations fold the automorphism into the inner product as a gather of
+//     the digit values; Galois keys are held permuted to the output order, so
+//     key loads and stores stay coalesced and vectorised.
 #include "fp64.cuh"
 #include "kernels.hpp"
 
@@ -270,8 +271,10 @@ void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt,
 //   xa[m] = sum_d D_d[t] * ka[d][t]
 // over the extended basis m in [0, n+K) (prime t = m or L + m - n).  D_d[t] is
 // the original evaluation value e2[t] when t lies in digit d, otherwise the
-// ModUp output.  With galois_inv != 0 the result is written permuted:
-// out[j] = value at slot(galois_inv, j).
+// ModUp output.  Rotations (galois g != 0): out[j] = sum_d D_d[slot(g, j)] *
+// k'_d[j] (+ P * c0[slot(g, j)]), where a Galois key is held permuted,
+// k'_d[j] = k_d[slot(g, j)] (the key that switches sigma_g(s) back to s):
+// only the digit values and c0 are gathered, the key streams in order.
 // ---------------------------------------------------------------------------
 // Batch element b = blockIdx.x % nb varies fastest, so the blocks that read
 // one key tile for the different elements run back to back and the key is
@@ -284,10 +287,16 @@ void launch_modup_conv(const DevCtx& ctx, int level, int nb, const uint64_t* xt,
 // coefficient; the instantiation without it carries no generator code and
 // keeps the register count of the plain streaming loop (32-40).  Left free,
 // the unrolled digit loop with the generator takes 56-72 registers; the
-// bound holds it at 48 (FP64 sums) or 40 so that 5-6 blocks stay resident.
+// bound holds it at 48 (FP64 sums) or 40 so that 5-6 blocks stay resident
+// (not the split-product accumulator, which would spill).
+template <class ACC>
+constexpr bool kIsSplitAcc = false;
+template <>
+constexpr bool kIsSplitAcc<AccSplit> = true;
+
 template <int VEC, class ACC, bool FPK, bool GRP = false, bool SEED = false>
-__global__ void __launch_bounds__(256, SEED ? (FPK ? 5 : 6) : 0) k_ks_inner(const __grid_constant__ DevCtx ctx, int level, int nb,
-                                                  const __grid_constant__ KsArgs args) {
+__global__ void __launch_bounds__(256, SEED ? (FPK ? 5 : (kIsSplitAcc<ACC> ? 0 : 6)) : 0)
+    k_ks_inner(const __grid_constant__ DevCtx ctx, int level, int nb, const __grid_constant__ KsArgs args) {
     const int n = level + 1;
     const int m = blockIdx.y;
     const int bi = blockIdx.x % nb;
@@ -383,52 +392,86 @@ __global__ void __launch_bounds__(256, SEED ? (FPK ? 5 : 6) : 0) k_ks_inner(cons
         *reinterpret_cast<ulonglong2*>(xb + j) = ob;
         *reinterpret_cast<ulonglong2*>(xa + j) = oa;
     } else {
-        const int j = bx * blockDim.x + threadIdx.x;
+        // rotation: outputs j, j+1 gather the digit values (and c0) at the
+        // automorphism's source slots; the key is stored permuted (entry j is
+        // the one that pairs with output j), so its loads stay vectorised
+        const size_t j = ((size_t)bx * blockDim.x + threadIdx.x) * 2;
         const uint32_t g = args.galois[bi];
-        const uint32_t src = g ? automorph_slot(ctx.logN, g, j) : (uint32_t)j;
+        const uint32_t s0 = g ? automorph_slot(ctx.logN, g, (uint32_t)j) : (uint32_t)j;
+        const uint32_t s1 = g ? automorph_slot(ctx.logN, g, (uint32_t)j + 1) : (uint32_t)j + 1;
+        const size_t koff = (size_t)t * ctx.N + j;
+        const uint64_t* c0 = args.c0[bi];
         if constexpr (FPK) {
             // up to 6 digits: |sum| <= 6 * 0.875p + p (the P c0 term) < 2^53
             if (pc.p < kFpPrimeBound && nd <= 6) {
                 const double p = __ull2double_rn(pc.p), pinv = as_f64(pc.pinv_f64);
-                double sb = 0, sa = 0;
+                double sb0 = 0, sb1 = 0, sa0 = 0, sa1 = 0;
 #pragma unroll
                 for (int d = 0; d < 6; ++d) {
                     if (d < nd) {
-                        const double x = as_f64(fp_from_u(srcs[d][src]));
-                        sb = __dadd_rn(sb, fp_mulmod(x, as_f64(fp_from_u(kb[d * kstride + (size_t)t * ctx.N + src])),
-                                                     p, pinv));
-                        const uint64_t av = !SEED || ka ? ka[d * kstride + (size_t)t * ctx.N + src]
-                                                        : uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, src, pc.p);
-                        sa = __dadd_rn(sa, fp_mulmod(x, as_f64(fp_from_u(av)), p, pinv));
+                        const double x0 = as_f64(fp_from_u(srcs[d][s0])), x1 = as_f64(fp_from_u(srcs[d][s1]));
+                        const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(kb + d * kstride + koff);
+                        ulonglong2 a;
+                        if (!SEED || ka) {
+                            a = *reinterpret_cast<const ulonglong2*>(ka + d * kstride + koff);
+                        } else {
+                            a.x = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j, pc.p);
+                            a.y = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j + 1, pc.p);
+                        }
+                        sb0 = __dadd_rn(sb0, fp_mulmod(x0, as_f64(fp_from_u(b.x)), p, pinv));
+                        sb1 = __dadd_rn(sb1, fp_mulmod(x1, as_f64(fp_from_u(b.y)), p, pinv));
+                        sa0 = __dadd_rn(sa0, fp_mulmod(x0, as_f64(fp_from_u(a.x)), p, pinv));
+                        sa1 = __dadd_rn(sa1, fp_mulmod(x1, as_f64(fp_from_u(a.y)), p, pinv));
                     }
                 }
-                const uint64_t* c0 = args.c0[bi];
                 if (c0 && m < n) {
                     const ulonglong2 pm = __ldg(reinterpret_cast<const ulonglong2*>(ctx.md_pmod) + t);
-                    sb = __dadd_rn(sb, as_f64(fp_from_u(mul_shoup(c0[(size_t)m * ctx.N + src], pm.x, pm.y, pc.p))));
+                    const uint64_t* cm = c0 + (size_t)m * ctx.N;
+                    sb0 = __dadd_rn(sb0, as_f64(fp_from_u(mul_shoup(cm[s0], pm.x, pm.y, pc.p))));
+                    sb1 = __dadd_rn(sb1, as_f64(fp_from_u(mul_shoup(cm[s1], pm.x, pm.y, pc.p))));
                 }
-                xb[j] = fp_to_u(fp_center(sb, p, pinv), p, pinv);
-                xa[j] = fp_to_u(fp_center(sa, p, pinv), p, pinv);
+                ulonglong2 ob, oa;
+                ob.x = fp_to_u(fp_center(sb0, p, pinv), p, pinv);
+                ob.y = fp_to_u(fp_center(sb1, p, pinv), p, pinv);
+                oa.x = fp_to_u(fp_center(sa0, p, pinv), p, pinv);
+                oa.y = fp_to_u(fp_center(sa1, p, pinv), p, pinv);
+                *reinterpret_cast<ulonglong2*>(xb + j) = ob;
+                *reinterpret_cast<ulonglong2*>(xa + j) = oa;
                 return;
             }
         }
-        ACC sb, sa;
+        ACC sb0, sb1, sa0, sa1;
 #pragma unroll
         for (int d = 0; d < 8; ++d) {
             if (d < nd) {
-                const uint64_t x = srcs[d][src];
-                sb.mac(x, kb[d * kstride + (size_t)t * ctx.N + src]);
-                sa.mac(x, !SEED || ka ? ka[d * kstride + (size_t)t * ctx.N + src]
-                                      : uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, src, pc.p));
+                const uint64_t x0 = srcs[d][s0], x1 = srcs[d][s1];
+                const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(kb + d * kstride + koff);
+                ulonglong2 a;
+                if (!SEED || ka) {
+                    a = *reinterpret_cast<const ulonglong2*>(ka + d * kstride + koff);
+                } else {
+                    a.x = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j, pc.p);
+                    a.y = uniform_mod(astream ^ ((uint64_t)(d + 1) << 48), t, (uint32_t)j + 1, pc.p);
+                }
+                sb0.mac(x0, b.x);
+                sb1.mac(x1, b.y);
+                sa0.mac(x0, a.x);
+                sa1.mac(x1, a.y);
             }
         }
-        const uint64_t* c0 = args.c0[bi];
         if (c0 && m < n) {
             const ulonglong2 pm = __ldg(reinterpret_cast<const ulonglong2*>(ctx.md_pmod) + t);
-            sb.mac(mul_shoup(c0[(size_t)m * ctx.N + src], pm.x, pm.y, pc.p), 1);
+            const uint64_t* cm = c0 + (size_t)m * ctx.N;
+            sb0.mac(mul_shoup(cm[s0], pm.x, pm.y, pc.p), 1);
+            sb1.mac(mul_shoup(cm[s1], pm.x, pm.y, pc.p), 1);
         }
-        xb[j] = sb.reduce(pc);
-        xa[j] = sa.reduce(pc);
+        ulonglong2 ob, oa;
+        ob.x = sb0.reduce(pc);
+        ob.y = sb1.reduce(pc);
+        oa.x = sa0.reduce(pc);
+        oa.y = sa1.reduce(pc);
+        *reinterpret_cast<ulonglong2*>(xb + j) = ob;
+        *reinterpret_cast<ulonglong2*>(xa + j) = oa;
     }
 }
 
@@ -454,13 +497,13 @@ void launch_ks_inner(const DevCtx& ctx, int level, int nb, const KsArgs& args, b
         else
             ks_inner_go<1, Acc128, false, false>(ctx, level, nb, args, seeded, g, st);
     } else if (args.dig_group > 0) {
-        dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
+        dim3 g(ctx.N / 512 * nb, level + 1 + ctx.K);
         if (ctx.ks_variant & 1)
             ks_inner_go<0, Acc128, true, true>(ctx, level, nb, args, seeded, g, st);
         else
             ks_inner_go<0, Acc128, false, true>(ctx, level, nb, args, seeded, g, st);
     } else {
-        dim3 g(ctx.N / 256 * nb, level + 1 + ctx.K);
+        dim3 g(ctx.N / 512 * nb, level + 1 + ctx.K);
         if (ctx.ks_variant & 1)
             ks_inner_go<0, Acc128, true, false>(ctx, level, nb, args, seeded, g, st);
         else if (ctx.conv_variant == 1)

@@ -68,7 +68,7 @@ def test_compressed_keys_in_batched_transform_and_bootstrap():
 
 def test_compressed_relin_key_bitexact():
     """A compressed relinearisation key (mask bit 1): single and batched
-    HMults (a batch of 6, which with a full key takes the key switch fused
+    HMults (a batch of 8, which with a full key takes the key switch fused
     into the row pass) equal the same key stored in full and the oracle's
     HMult with the exported key."""
     from pyfideslib_b200._capi import lib
@@ -76,7 +76,7 @@ def test_compressed_relin_key_bitexact():
     cc, oc = make_pair(12, 8, 3, 3)
     sk = cc.KeyGen(seed=51, hamming_weight=64)
     level = 7
-    raw = [(rand_ct(oc, level, 5100 + 4 * i), rand_ct(oc, level, 5102 + 4 * i)) for i in range(6)]
+    raw = [(rand_ct(oc, level, 5100 + 4 * i), rand_ct(oc, level, 5102 + 4 * i)) for i in range(8)]
     A = [cc.upload(*a) for a, _ in raw]
     B = [cc.upload(*b) for _, b in raw]
     res = {}
