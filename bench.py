@@ -48,7 +48,7 @@ LOGN, L, K, DNUM = 16, 30, 10, 3
 # instead.  About twice the algorithmic bytes: the column pass writes the 960
 # intermediate limbs (480 MB, more than L2) and the row pass reads them back;
 # twiddles add 32 MB (read once per prime for the whole batch).
-NTT_BATCH_TRAFFIC_BYTES = 1926.5e6  # 503.5 + 443.6 (cols) + 534.8 + 444.6 (rows) MB
+NTT_BATCH_TRAFFIC_BYTES = 1922.8e6  # 503.5 + 443.3 (cols) + 535.0 + 441.0 (rows) MB
 NTT_BATCH_TRAFFIC_SOURCE = "constant from one ncu capture of the launch pair (variant 9, caches flushed)"
 _UNITS = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "Tbyte": 1e12}
 
