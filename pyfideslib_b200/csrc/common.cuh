@@ -57,9 +57,6 @@ struct DevCtx {
                                  // split 32-bit products (moduli < 2^60), 2 one coefficient/thread,
                                  // 3 and 4 ModUp and ModDown on the tensor cores (int8 split, 32
                                  // or 16 targets per MMA)
-    int fwd_int_lanes;           // NTT launches only (set from the variant, 0 = none): the limbs of
-    int inv_int_lanes;           //   FP64-capable primes with (prime + batch index) % lanes == 0 run
-                                 //   the integer butterflies, so FP64 and integer pipes work side by side
     const PrimeConst* pc;        // [L+K]
     const uint64_t* fwd_tw;      // [L+K][N][2]  psi^{bitrev(i)}, companion
     const uint64_t* inv_tw;      // [L+K][N][2]  psi^{-bitrev(i)}, companion

@@ -477,7 +477,6 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.dnum = c->dnum;
     d.alpha = c->alpha;
     d.ntt_variant = d.intt_variant = d.conv_variant = 0;  // chosen by the autotuner
-    d.fwd_int_lanes = d.inv_int_lanes = 0;                // set per launch from the variant
     d.ks_variant = 1 | 4;  // FP64 sums; fused into the row pass for batches of 8 or more
     d.pc = (const PrimeConst*)(base + parts[i_pc].off);
     d.fwd_tw = (const uint64_t*)(base + parts[i_fwd].off);

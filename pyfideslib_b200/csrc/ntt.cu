@@ -237,19 +237,10 @@ __device__ __forceinline__ void fwd_group(int fmode, uint64_t (&x)[16], Tab tab,
     run_group<KF, KL, PF, 0>(x, tab, t_of_kb0, B, th_hi, p, two_p);
 }
 
-// Integer lanes (forward variants 10-12, inverse configurations 6-8): limb
-// (prime, batch element) runs the integer butterflies although its prime
-// allows the FP64 ones when (prime + batch) % lanes == 0.  Both passes of a
-// transform (and the fused key-switch row pass) decide alike, so the
-// representation handed from one pass to the next agrees.
-__device__ __forceinline__ bool int_lane(int lanes, int prime) {
-    return lanes > 0 && (prime + (int)blockIdx.y) % lanes == 0;
-}
-
 template <bool AQ, bool FP>
-__device__ __forceinline__ int fwd_mode(uint64_t p, bool int_lane = false) {
+__device__ __forceinline__ int fwd_mode(uint64_t p) {
     if constexpr (FP)
-        if (p < kFpPrimeBound && !int_lane) return 4;
+        if (p < kFpPrimeBound) return 4;
     if constexpr (AQ) return p < kApproxPrimeBound ? 3 : 0;
     return p < kLazyPrimeBound ? 1 : 0;
 }
@@ -264,9 +255,9 @@ __device__ __forceinline__ FwdK fwd_consts(int mode, const PrimeConst& pc) {
 }
 
 template <bool FP>
-__device__ __forceinline__ int inv_mode(uint64_t p, bool int_lane = false) {
+__device__ __forceinline__ int inv_mode(uint64_t p) {
     if constexpr (FP)
-        if (p < kFpPrimeBound && !int_lane) return 5;
+        if (p < kFpPrimeBound) return 5;
     return 2;
 }
 
@@ -389,7 +380,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_cols(const __grid_constan
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
-    const int fmode = fwd_mode<AQ, FP>(pc.p, int_lane(ctx.fwd_int_lanes, lr.prime));
+    const int fmode = fwd_mode<AQ, FP>(pc.p);
     const FwdK kk = fwd_consts(fmode, pc);
     const ulonglong2* twg =
         reinterpret_cast<const ulonglong2*>(fmode == 4 ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)lr.prime * ctx.N;
@@ -482,7 +473,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_fwd_rows(const __grid_constan
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
-    const int fmode = fwd_mode<AQ, FP>(pc.p, int_lane(ctx.fwd_int_lanes, lr.prime));
+    const int fmode = fwd_mode<AQ, FP>(pc.p);
     const FwdK kk = fwd_consts(fmode, pc);
     const uint64_t* twg = (fmode == 4 ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)lr.prime * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
@@ -625,7 +616,7 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constan
     const size_t boff = (size_t)blockIdx.y * a.bstride;
     const int t = m < n ? m : ctx.L + (m - n);
     const PrimeConst pc = ctx.pc[t];
-    const int fmode = fwd_mode<AQ, FP>(pc.p, int_lane(ctx.fwd_int_lanes, t));
+    const int fmode = fwd_mode<AQ, FP>(pc.p);
     const FwdK kk = fwd_consts(fmode, pc);
     const uint64_t* twg = (fmode == 4 ? ctx.fwd_twf : ctx.fwd_tw) + (size_t)t * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
@@ -795,7 +786,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_rows(const __grid_constan
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
-    const int imode = inv_mode<FP>(pc.p, int_lane(ctx.inv_int_lanes, lr.prime));
+    const int imode = inv_mode<FP>(pc.p);
     const FwdK kk = fwd_consts(imode, pc);
     const uint64_t* twg = (imode == 5 ? ctx.inv_twf : ctx.inv_tw) + (size_t)lr.prime * 2 * ctx.N;
     auto tab = [&](size_t i) { return ldg2(twg, i); };
@@ -895,7 +886,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_inv_cols(const __grid_constan
 
     const LimbRef lr = resolve_limb(map, blockIdx.z, blockIdx.y, ctx.N, ctx.L);
     const PrimeConst pc = ctx.pc[lr.prime];
-    const int imode = inv_mode<FP>(pc.p, int_lane(ctx.inv_int_lanes, lr.prime));
+    const int imode = inv_mode<FP>(pc.p);
     const FwdK kk = fwd_consts(imode, pc);
     const ulonglong2* twg =
         reinterpret_cast<const ulonglong2*>(imode == 5 ? ctx.inv_twf : ctx.inv_tw) + (size_t)lr.prime * ctx.N;
@@ -968,23 +959,12 @@ bool ntt_supported(int logN) { return logN >= 8 && logN <= 16; }
 // 1 (3, per-stage), 2 (4, per-stage), 3 and 4: as 1 and 0 with
 // double-precision butterflies for primes below 2^50; ntt_inverse_of(v)
 // pairs each forward variant with an inverse configuration of the same
-// arithmetic.  10, 11, 12: variant 9 with integer lanes every 4th, 3rd,
-// 2nd (prime + batch) limb (int_lane); inverse configurations 6, 7, 8: 5
-// with the same lanes.
-int ntt_num_variants() { return 13; }
-int ntt_num_inverse_variants() { return 9; }
+// arithmetic.
+int ntt_num_variants() { return 10; }
+int ntt_num_inverse_variants() { return 6; }
 int ntt_inverse_of(int v) {
-    static const int inv[13] = {0, 1, 2, 1, 0, 3, 4, 3, 3, 5, 6, 7, 8};
-    return v >= 0 && v < 13 ? inv[v] : 0;
-}
-
-// integer lanes of forward variants 10-12 / inverse configurations 6-8
-static int lanes_of(int v, int first) { return v >= first && v < first + 3 ? 4 - (v - first) : 0; }
-static DevCtx with_lanes(const DevCtx& ctx) {
-    DevCtx c = ctx;
-    c.fwd_int_lanes = lanes_of(ctx.ntt_variant, 10);
-    c.inv_int_lanes = lanes_of(ctx.intt_variant, 6);
-    return c;
+    static const int inv[10] = {0, 1, 2, 1, 0, 3, 4, 3, 3, 5};
+    return v >= 0 && v < 10 ? inv[v] : 0;
 }
 
 template <int LR, int LC, int MINB, bool PF, bool AQ, bool FP>
@@ -1031,9 +1011,6 @@ static void launch_fwd(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
         case 7: launch_fwd_mix<LR, LC, 3, false, 2, true, true, true>(ctx, map, st); break;
         case 8: launch_fwd_mix<LR, LC, 3, false, 4, false, true, true>(ctx, map, st); break;
         case 9: launch_fwd_mix<LR, LC, 3, false, 3, false, true, true, true>(ctx, map, st); break;
-        case 10: case 11: case 12:
-            launch_fwd_mix<LR, LC, 3, false, 3, false, true, true, true>(with_lanes(ctx), map, st);
-            break;
         default: launch_fwd_v<LR, LC, 2, true, false, false>(ctx, map, st); break;
     }
 }
@@ -1046,7 +1023,6 @@ static void launch_inv(const DevCtx& ctx, const LimbMap& map, cudaStream_t st) {
         case 3: launch_inv_v<LR, LC, 3, false, true>(ctx, map, st); break;
         case 4: launch_inv_v<LR, LC, 2, true, true>(ctx, map, st); break;
         case 5: launch_inv_v<LR, LC, 3, false, true, true>(ctx, map, st); break;
-        case 6: case 7: case 8: launch_inv_v<LR, LC, 3, false, true, true>(with_lanes(ctx), map, st); break;
         default: launch_inv_v<LR, LC, 2, true, false>(ctx, map, st); break;
     }
 }
@@ -1068,7 +1044,6 @@ static void launch_fwd_cols(const DevCtx& ctx, const LimbMap& map, cudaStream_t 
         case 3: launch_fwd_cols_v<LR, LC, 3, false, true, false>(ctx, map, st); break;
         case 4: launch_fwd_cols_v<LR, LC, 2, true, true, false>(ctx, map, st); break;
         case 5: case 7: case 8: case 9: launch_fwd_cols_v<LR, LC, 3, false, true, true>(ctx, map, st); break;
-        case 10: case 11: case 12: launch_fwd_cols_v<LR, LC, 3, false, true, true>(with_lanes(ctx), map, st); break;
         case 6: launch_fwd_cols_v<LR, LC, 2, true, true, true>(ctx, map, st); break;
         default: launch_fwd_cols_v<LR, LC, 2, true, false, false>(ctx, map, st); break;
     }
@@ -1113,7 +1088,6 @@ static void launch_rows_ks(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaS
         case 3: case 4: launch_rows_ks_v<LR, LC, false, true, false>(ctx, a, nb, st); break;
         case 6: case 7: launch_rows_ks_v<LR, LC, true, true, true>(ctx, a, nb, st); break;
         case 9: launch_rows_ks_v<LR, LC, false, true, true, true>(ctx, a, nb, st); break;
-        case 10: case 11: case 12: launch_rows_ks_v<LR, LC, false, true, true, true>(with_lanes(ctx), a, nb, st); break;
         default: launch_rows_ks_v<LR, LC, false, true, true>(ctx, a, nb, st); break;
     }
 }
