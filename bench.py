@@ -212,7 +212,7 @@ def measure_c4(cc, lib, st, n=256, reps=3, seed=4):
             "per_op_ms": op_ms, "per_op_pairs_per_s": n / (op_ms * 1e-3), "results_equal": bool(same)}
 
 
-def measure_c3(reps=5, seed=3, ntt_variant=-1, ks_variant=-1, key_compression=1):
+def measure_c3(reps=5, seed=3, ntt_variant=-1, ks_variant=-1, key_compression=1, profile=False):
     """Config 3: N=2^16, 20 moduli (60 + 19 x 40-bit, scale 2^40), dnum=3, one
     ciphertext; 32 hoisted rotations (+-2^k, k < 15, and 3, 5) sharing one
     ModUp, and a 64-diagonal plaintext matrix (offsets 0..63, entries uniform
@@ -260,6 +260,14 @@ def measure_c3(reps=5, seed=3, ntt_variant=-1, ks_variant=-1, key_compression=1)
         keep[0] = cc.EvalFastRotation(ct, idx)
 
     hoist_ms = timed(hoist)
+    if profile:
+        # one more hoisted call between the profiler marks, for an ncu
+        # capture started with --profile-from-start off
+        cc.Synchronize()
+        torch.cuda.profiler.start()
+        hoist()
+        cc.Synchronize()
+        torch.cuda.profiler.stop()
     lt_ms = timed(lambda: cc.EvalLinearTransform(ct, offs, pts, bstep, rescale=True))
     y = cc.EvalLinearTransform(ct, offs, pts, bstep, rescale=True)
     want = np.zeros(slots, dtype=np.complex128)
@@ -705,7 +713,8 @@ def run_ours(args):
                 "per_op": measure_serving(cc, brates, 4.0, rot_idx, max_batch=1, num_streams=1, boot_share=0.1,
                                           boot_inputs=boot_cts)}
     if not args.no_c3:
-        c3 = measure_c3(ntt_variant=args.ntt_variant, ks_variant=args.ks_variant, key_compression=args.key_compression)
+        c3 = measure_c3(ntt_variant=args.ntt_variant, ks_variant=args.ks_variant, key_compression=args.key_compression,
+                        profile=args.profile_c3)
     value = job_throughput(B * args.steps, world, ms)
     per_op_value = job_throughput(B * max(1, args.steps // 2), world, ms_op)
     e2e_steps = max(1, args.steps // 2)
@@ -775,6 +784,8 @@ def main():
     ap.add_argument("--ntt-traffic-csv", default=None,
                     help="ncu --csv log with dram__bytes_read.sum and dram__bytes_write.sum of the roofline "
                          "NTT pair (--profile-roofline); its last pair gives roofline.traffic")
+    ap.add_argument("--profile-c3", action="store_true",
+                    help="mark one call of config 3's 32 hoisted rotations for ncu --profile-from-start off")
     ap.add_argument("--profile-step", action="store_true",
                     help="mark one batched HMult step (after the timed region) for ncu --profile-from-start off")
     args = ap.parse_args()
