@@ -310,7 +310,10 @@ fides_status fides_chebyshev_series(fides_ctx* ctx, const fides_ct* a, const dou
 /* ---- bootstrapping (api/CryptoContext.hpp:80-82,180-181 EvalBootstrapSetup /
  *      EvalBootstrapKeyGen / EvalBootstrap; src/CKKS/Bootstrap.cu:169-320) ---- */
 typedef struct {
-    int slots;           /* N/2 (full packing; 0 means N/2) */
+    int slots;           /* slots of the ciphertexts bootstrapped: a power of two up to N/2
+                            (0 means N/2, full packing); below N/2 (sparse packing) the
+                            raised polynomial is first projected onto the n-slot subring
+                            by log2(N/2n) rotate-and-add steps */
     int level_budget[2]; /* levels of CoeffsToSlots and SlotsToCoeffs (0 means 3) */
     int cheb_degree;     /* degree of the EvalMod Chebyshev series (0 means 119) */
     double K;            /* EvalMod input range [-K, K] in units of q_0 (0 means 16) */
@@ -326,9 +329,17 @@ typedef struct {
  * and the rotations listed by fides_bootstrap_info. */
 fides_status fides_bootstrap_setup(fides_ctx* ctx, const fides_boot_params* params);
 /* Output level of a bootstrapped ciphertext and the rotation indices the
- * bootstrap needs keys for (rotations may be NULL to query the count). */
+ * bootstrap needs keys for (rotations may be NULL to query the count): first
+ * the CoeffsToSlots / SlotsToCoeffs rotations over `slots` slots (|index| <=
+ * slots / 2), then, for sparse packing, the indices slots, 2 slots, ..., N/4
+ * over the full N/2 slots (the subring projection).  fides_bootstrap_keygen
+ * generates them with the right slot counts. */
 fides_status fides_bootstrap_info(fides_ctx* ctx, int slots, int* output_level, int* num_rotations,
                                   int32_t* rotations);
+/* EvalBootstrapKeyGen (api/CryptoContext.hpp:181): the rotation keys
+ * fides_bootstrap_info lists and the conjugation key, for a bootstrap set up
+ * for `slots` (0: N/2). */
+fides_status fides_bootstrap_keygen(fides_ctx* ctx, const fides_sk* sk, int slots, uint64_t seed);
 /* EvalBootstrap: refresh a ciphertext (only its limb 0 is read) to the
  * output level, same slots and message. */
 fides_status fides_bootstrap(fides_ctx* ctx, const fides_ct* in, fides_ct* out);

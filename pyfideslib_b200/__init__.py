@@ -52,6 +52,10 @@ class Ciphertext:
     def level(self):
         return self.info()["level"]
 
+    @property
+    def slots(self):
+        return self.info()["slots"]
+
     def GetLevel(self):
         return self.level
 
@@ -483,9 +487,7 @@ class CryptoContext:
         return lv.value, [int(rot[i]) for i in range(n.value)]
 
     def EvalBootstrapKeyGen(self, sk, slots=None, seed=11):
-        _, rots = self.bootstrap_info(slots)
-        self.EvalRotateKeyGen(sk, rots, slots=slots, seed=seed)
-        self.EvalConjugateKeyGen(sk, seed=seed + 1)
+        check(lib.fides_bootstrap_keygen(self._h, sk._h, slots or self.N // 2, seed), self._h)
 
     def EvalBootstrap(self, a, out=None):
         out = self._out(out)

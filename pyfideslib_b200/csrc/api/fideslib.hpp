@@ -598,12 +598,8 @@ class CryptoContextImpl<DCRTPoly> {
     }
     void EvalBootstrapKeyGen(const PrivateKey<DCRTPoly>& sk, uint32_t numSlots = 0) {
         const int s = (int)(numSlots ? numSlots : slots);
-        int n = 0;
-        check(fides_bootstrap_info(ctx, s, nullptr, &n, nullptr), ctx);
-        std::vector<int32_t> rot(n);
-        check(fides_bootstrap_info(ctx, s, nullptr, nullptr, rot.data()), ctx);
-        check(fides_keygen_rotations(ctx, sk->handle, n, rot.data(), s, seed++), ctx);
-        check(fides_keygen_conjugate(ctx, sk->handle, seed++), ctx);
+        check(fides_bootstrap_keygen(ctx, sk->handle, s, seed), ctx);
+        seed += 2;
     }
     // numIterations > 1 (OpenFHE's iterated bootstrapping, which needs the
     // input at a higher level to form the residual) is not supported here.

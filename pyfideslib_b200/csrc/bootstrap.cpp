@@ -68,7 +68,8 @@ struct BootPrecomp {
     std::vector<double> cheb;
     std::vector<BootStage> cts, stc;
     int level_after_cts = 0, level_after_mod = 0, level_out = 0;
-    std::vector<int32_t> rotations;
+    std::vector<int32_t> rotations;  // CoeffsToSlots / SlotsToCoeffs, indices over `slots` slots
+    std::vector<int32_t> subsum;     // sparse packing: n, 2n, ..., N/4 over the full N/2 slots
     ~BootPrecomp() {
         for (auto* v : {&cts, &stc})
             for (auto& s : *v)
@@ -617,7 +618,8 @@ fides_status fides_bootstrap_setup(fides_ctx* c, const fides_boot_params* prm) {
     if (!c || !prm) return FIDES_BAD_ARG;
     Guard g(c);
     const int n = prm->slots > 0 ? prm->slots : c->N / 2;
-    if (n != c->N / 2) return set_err(c, FIDES_UNSUPPORTED, "bootstrapping is implemented for full packing (N/2 slots)");
+    if (n < 2 || n > c->N / 2 || (n & (n - 1)))
+        return set_err(c, FIDES_BAD_ARG, "bootstrap slots must be a power of two in [2, N/2]");
     int logn = 0;
     while ((1 << logn) < n) ++logn;
     auto bp = std::make_shared<BootPrecomp>();
@@ -674,6 +676,7 @@ fides_status fides_bootstrap_setup(fides_ctx* c, const fides_boot_params* prm) {
             }
     std::sort(rot.begin(), rot.end());
     bp->rotations = rot;
+    for (int r = n; r < c->N / 2; r <<= 1) bp->subsum.push_back(r);
     c->boot[n] = bp;
     return check_cuda(c, "bootstrap setup");
 }
@@ -685,9 +688,28 @@ fides_status fides_bootstrap_info(fides_ctx* c, int slots, int* output_level, in
     if (it == c->boot.end()) return set_err(c, FIDES_BAD_ARG, "bootstrapping not set up for these slots");
     const BootPrecomp& b = *it->second;
     if (output_level) *output_level = b.level_out;
-    if (num_rotations) *num_rotations = (int)b.rotations.size();
-    if (rotations) std::copy(b.rotations.begin(), b.rotations.end(), rotations);
+    if (num_rotations) *num_rotations = (int)(b.rotations.size() + b.subsum.size());
+    if (rotations) {
+        std::copy(b.rotations.begin(), b.rotations.end(), rotations);
+        std::copy(b.subsum.begin(), b.subsum.end(), rotations + b.rotations.size());
+    }
     return FIDES_OK;
+}
+
+fides_status fides_bootstrap_keygen(fides_ctx* c, const fides_sk* sk, int slots, uint64_t seed) {
+    if (!c || !sk) return FIDES_BAD_ARG;
+    std::shared_ptr<BootPrecomp> bp;
+    {
+        Guard g(c);
+        auto it = c->boot.find(slots > 0 ? slots : c->N / 2);
+        if (it == c->boot.end()) return set_err(c, FIDES_BAD_ARG, "bootstrapping not set up for these slots");
+        bp = it->second;
+    }
+    fides_status s = fides_keygen_rotations(c, sk, (int)bp->rotations.size(), bp->rotations.data(), bp->slots, seed);
+    if (s == FIDES_OK && !bp->subsum.empty())
+        s = fides_keygen_rotations(c, sk, (int)bp->subsum.size(), bp->subsum.data(), c->N / 2, seed + 7777);
+    if (s == FIDES_OK) s = fides_keygen_conjugate(c, sk, seed + 1);
+    return s;
 }
 
 fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
@@ -724,6 +746,23 @@ fides_status fides_bootstrap_batch(fides_ctx* c, int nin, const fides_ct* const*
         if (s != FIDES_OK) return s;
         x[u]->scale = B.K * (double)c->host.prime[0];
         x[u]->slots = n;
+    }
+    // sparse packing: the raised polynomial has coefficients everywhere (the
+    // overflow q0 I); the trace over the automorphisms X -> X^(5^(n t)),
+    // t < N / 2n (the rotations by multiples of n, which fix the subring
+    // Z[X^(N/2n)]), is N/2n times its projection onto that subring, the
+    // ring of n-slot plaintexts: log2(N/2n) rotate-and-add steps, the factor
+    // taken into the declared scale
+    for (int32_t r : B.subsum) {
+        const uint32_t gal = fides_rotation_galois(c, r, N / 2);
+        for (size_t u = 0; u < k; ++u) {
+            Lanes rt = A.fresh(2);
+            if ((s = fides_automorphism(c, x[u], gal, rt[0])) != FIDES_OK) return s;
+            if ((s = fides_add(c, x[u], rt[0], rt[1])) != FIDES_OK) return s;
+            rt[1]->scale = 2.0 * x[u]->scale;
+            rt[1]->slots = n;
+            x[u] = rt[1];
+        }
     }
     // CoeffsToSlots from the scale K q0 (about 2^64, growing by 2^8 per
     // transform): its rescaling and key-switching noise and the rounding of

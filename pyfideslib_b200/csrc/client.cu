@@ -142,26 +142,6 @@ void slot_indices(int N, std::vector<int>& pos, std::vector<int>& neg) {
     }
 }
 
-// slots (n complex) -> real coefficients (not yet scaled)
-std::vector<double> embed_inverse(int N, const double* values, int slots) {
-    std::vector<int> pos, neg;
-    slot_indices(N, pos, neg);
-    std::vector<cplx> M(N);
-    for (int j = 0; j < N / 2; ++j) {
-        const int k = j % slots;
-        const cplx z(values[2 * k], values[2 * k + 1]);
-        M[pos[j]] = z;
-        M[neg[j]] = std::conj(z);
-    }
-    fft(M, true);  // sum_t M_t w^{-t i}
-    std::vector<double> m(N);
-    for (int i = 0; i < N; ++i) {
-        const double ang = -M_PI * i / N;
-        m[i] = (M[i] * cplx(cos(ang), sin(ang))).real() / N;
-    }
-    return m;
-}
-
 // real coefficients -> slots
 void embed(int N, const std::vector<long double>& m, double* values, int slots) {
     std::vector<cplx> A(N);
@@ -225,17 +205,120 @@ fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg
 
 }  // namespace
 
-fides_status fides::encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm) {
-    const int N = c->N;
-    std::vector<double> m = embed_inverse(N, values, slots);
-    std::vector<int64_t> v(N);
-    for (int i = 0; i < N; ++i) {
-        const double x = m[i] * scale;
-        if (!(fabs(x) < 9.0e18)) return set_err(c, FIDES_BAD_ARG, "encoded coefficient exceeds 2^63");
-        v[i] = llround(x);
+// ---- encoding on the device ----
+// The canonical embedding's inverse: slot j of the N/2 (slot k = j mod slots repeated) goes to the root
+// zeta^(5^j) and its conjugate to zeta^(-5^j); an inverse complex FFT of
+// length N, the twist by exp(-i pi t / N) / N and the real part give the
+// coefficients, scaled and rounded to integers.  FP64 throughout.
+
+// M[bitrev(pos_j)] = z_(j mod slots), M[bitrev(neg_j)] = conj(z): the FFT's
+// input permutation folded into the scatter
+__global__ void k_embed_scatter(const double2* __restrict__ z, int slots, int logN, double2* __restrict__ M) {
+    const int N = 1 << logN;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N / 2) return;
+    const uint32_t mask = 2u * (uint32_t)N - 1;
+    uint32_t g = 1, b = 5;  // 5^j mod 2N by squaring
+    for (uint32_t e = (uint32_t)j; e; e >>= 1) {
+        if (e & 1) g = (uint32_t)(((uint64_t)g * b) & mask);
+        b = (uint32_t)(((uint64_t)b * b) & mask);
     }
-    fides_status s = upload_small(c, v, dm, 0, level + 1);
-    if (s != FIDES_OK) return s;
+    const double2 v = z[j & (slots - 1)];
+    const uint32_t pos = (g - 1) / 2, neg = (2u * (uint32_t)N - g - 1) / 2;
+    M[__brev(pos) >> (32 - logN)] = v;
+    M[__brev(neg) >> (32 - logN)] = make_double2(v.x, -v.y);
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(__fma_rn(a.x, b.x, -a.y * b.y), __fma_rn(a.x, b.y, a.y * b.x));
+}
+
+// inverse-FFT butterflies of blocks of length 2^s (a[i] +- w a[i + h],
+// w = exp(-2 pi i k / 2^s)): stages 1..log2(tile) in shared memory, one CTA
+// per tile of 2 blockDim.x <= 2048 elements, then one launch per further stage
+constexpr int kFftTile = 2048;
+__global__ void __launch_bounds__(1024) k_fft_tile(double2* __restrict__ M, int s_hi) {
+    __shared__ double2 t[kFftTile];
+    const int T = 2 * blockDim.x;
+    double2* base = M + (size_t)blockIdx.x * T;
+    for (int i = threadIdx.x; i < T; i += blockDim.x) t[i] = base[i];
+    __syncthreads();
+    for (int s = 1; s <= s_hi; ++s) {
+        const int h = 1 << (s - 1);
+        const int i = threadIdx.x;  // one butterfly per thread and stage
+        const int k = i & (h - 1), a = ((i >> (s - 1)) << s) + k;
+        double sn, cs;
+        sincospi(-(double)k / (double)h, &sn, &cs);
+        const double2 u = t[a], v = cmul(t[a + h], make_double2(cs, sn));
+        t[a] = make_double2(u.x + v.x, u.y + v.y);
+        t[a + h] = make_double2(u.x - v.x, u.y - v.y);
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < T; i += blockDim.x) base[i] = t[i];
+}
+
+__global__ void k_fft_stage(double2* __restrict__ M, int s, int N) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N / 2) return;
+    const int h = 1 << (s - 1);
+    const int k = i & (h - 1), a = ((i >> (s - 1)) << s) + k;
+    double sn, cs;
+    sincospi(-(double)k / (double)h, &sn, &cs);
+    const double2 u = M[a], v = cmul(M[a + h], make_double2(cs, sn));
+    M[a] = make_double2(u.x + v.x, u.y + v.y);
+    M[a + h] = make_double2(u.x - v.x, u.y - v.y);
+}
+
+// v_t = round(Re(M_t exp(-i pi t / N)) / N * scale); a magnitude at or above
+// 9e18 sets *bad and writes 0
+__global__ void k_embed_round(const double2* __restrict__ M, int N, double scale, int64_t* __restrict__ v,
+                              int* __restrict__ bad) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    double sn, cs;
+    sincospi(-(double)t / (double)N, &sn, &cs);
+    const double2 m = M[t];
+    const double x = (m.x * cs - m.y * sn) / (double)N * scale;
+    if (!(fabs(x) < 9.0e18)) {
+        *bad = 1;
+        v[t] = 0;
+        return;
+    }
+    v[t] = llround(x);
+}
+
+fides_status fides::encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm) {
+    const int N = c->N, logN = c->logN;
+    if (slots < 1 || slots > N / 2 || (slots & (slots - 1))) return set_err(c, FIDES_BAD_ARG, "encode: slots");
+    // scratch: N complex (FFT), slots complex (input), N int64, one flag
+    char* buf = nullptr;
+    const size_t b_m = (size_t)N * 16, b_z = (size_t)slots * 16, b_v = (size_t)N * 8;
+    if (cudaMallocAsync((void**)&buf, b_m + b_z + b_v + 16, c->st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FIDES_OOM, "encode scratch");
+    }
+    double2* M = (double2*)buf;
+    double2* z = (double2*)(buf + b_m);
+    int64_t* v = (int64_t*)(buf + b_m + b_z);
+    int* bad = (int*)(buf + b_m + b_z + b_v);
+    cudaMemcpyAsync(z, values, b_z, cudaMemcpyHostToDevice, c->st);
+    cudaMemsetAsync(bad, 0, sizeof(int), c->st);
+    count_launches(3);
+    k_embed_scatter<<<(N / 2 + 255) / 256, 256, 0, c->st>>>(z, slots, logN, M);
+    const int s_tile = std::min(logN, 11);  // tiles of 2^s_tile <= kFftTile elements
+    k_fft_tile<<<N >> s_tile, (1 << s_tile) / 2, 0, c->st>>>(M, s_tile);
+    for (int s = s_tile + 1; s <= logN; ++s) {
+        count_launches(1);
+        k_fft_stage<<<(N / 2 + 255) / 256, 256, 0, c->st>>>(M, s, N);
+    }
+    k_embed_round<<<(N + 255) / 256, 256, 0, c->st>>>(M, N, scale, v, bad);
+    count_launches(1);
+    k_small_to_rns<<<dim3(N / 256, level + 1), 256, 0, c->st>>>(v, dm, N, 0, c->dev.pc);
+    int hbad = 0;
+    cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->st);
+    cudaFreeAsync(buf, c->st);
+    cudaStreamSynchronize(c->st);
+    if (hbad) return set_err(c, FIDES_BAD_ARG, "encoded coefficient exceeds 2^63");
     ntt_forward(c->dev, map_single(dm, dm, level + 1, level + 1, 0), FL_PLAIN, FS_PLAIN, c->st);
     return check_cuda(c, "encode");
 }

@@ -10,7 +10,7 @@ state a precision bound the same way (test/ParametrizedTest.cuh:517-530).
 import numpy as np
 import pytest
 
-from gpu_helpers import make_pair, rand_ct
+from gpu_helpers import device_status, make_pair, rand_ct
 
 pytestmark = pytest.mark.gpu
 
@@ -201,3 +201,40 @@ def test_bootstrap_requests_queued_in_serving():
     for c, (_, o) in zip(cts, outs):
         g, w = o.download(), cc.EvalBootstrap(c).download()
         assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1])
+
+
+@pytest.mark.parametrize("slots", [8, 512])
+def test_sparse_bootstrap_precision(slots):
+    """EvalBootstrap with sparse packing (slots < N/2; the reference's
+    approxModReductionSparse path, src/CKKS/ApproxModEval.cu:94, and
+    slot-count-dependent CoeffsToSlots, src/CKKS/CoeffsToSlots.cu:26,161):
+    the raised polynomial is projected onto the n-slot subring by
+    log2(N/2n) rotate-and-add steps, then the n-slot transforms run.  The
+    refreshed ciphertext decrypts to the message, keeps its slot count, and
+    still multiplies; a full-packing set-up in the same context is unaffected."""
+    import pyfideslib_b200 as F
+
+    cc = F.CryptoContext(log_n=12, num_q=20, dnum=4)
+    sk = cc.KeyGen(seed=19, hamming_weight=32)
+    cc.EvalMultKeyGen(sk)
+    cc.EvalBootstrapSetup(level_budget=(2, 2), slots=slots, cheb_degree=63)
+    cc.EvalBootstrapKeyGen(sk, slots=slots)
+    out_level, rots = cc.bootstrap_info(slots)
+    assert any(r >= slots for r in rots)  # the subring projection's rotations
+    rng = np.random.default_rng(slots)
+    m = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+    ct = cc.Encrypt(sk, m, slots=slots, level=0)
+    bt = cc.EvalBootstrap(ct)
+    assert bt.level == out_level and bt.slots == slots
+    err = np.max(np.abs(cc.Decrypt(sk, bt, slots=slots) - m))
+    assert -np.log2(err) > 14, err
+    sq = cc.EvalMult(bt, bt, rescale=True)
+    err2 = np.max(np.abs(cc.Decrypt(sk, sq, slots=slots) - m * m))
+    assert err2 < 2 ** -10, err2
+    # batched sparse bootstraps equal single ones
+    b2 = cc.EvalBootstrapBatch([ct, ct])
+    r0, r1 = bt.download()
+    for o in b2:
+        g0, g1 = o.download()
+        assert np.array_equal(g0, r0) and np.array_equal(g1, r1)
+    assert device_status(cc) == 0
