@@ -13,7 +13,11 @@
 //     launch (src/CKKS/LimbPartitionMGPU.cu:823-832);
 //   * ModDown2<ALGO_SHOUP>, grid N/64 x (64, 2), one polynomial per launch
 //     (src/CKKS/LimbPartitionMGPU.cu:1121-1129);
-//   * fusedDotKSK_2_, grid (N/128, K + n) x 128 (src/CKKS/LimbPartitionMGPU.cu:444).
+//   * fusedDotKSK_2_, grid (N/128, K + n) x 128 (src/CKKS/LimbPartitionMGPU.cu:444);
+//   * hoistedRotateDotKSK_2_, grid (N/128, K + n) x 128, 128 num_d words of
+//     shared memory (src/CKKS/LimbPartitionMGPU.cu:553);
+//   * binomialMult_ and automorph_multi_, grid (N/128, limbs) x 128
+//     (src/CKKS/LimbPartition.cu:2592, :2004).
 //
 // The reference reads its tables from a __constant__ Constants block and a
 // device Global::Globals block that SetupConstants fills from OpenFHE
@@ -36,6 +40,7 @@
 #include "CKKS/ElemenwiseBatchKernels.cuh"
 #include "ConstantsGPU.cuh"
 #include "NTT.cuh"
+#include "Rotation.cuh"
 
 namespace FIDESlib {
 __constant__ Constants constants;
@@ -300,6 +305,10 @@ int refgpu_set_keyswitch(int L, int K, int dnum, const uint64_t* hat_inv, const 
     for (int q = 0; q < L; ++q) {
         hc.primeid_partition[0][q] = q;
         hc.primeid_digit[q] = q / alpha;
+        uint64_t P = 1;  // the special primes' product mod q
+        for (int k = 0; k < K; ++k) P = mulmod(P, hc.primes[L + k] % hc.primes[q], hc.primes[q]);
+        hc.P[q] = P;
+        hc.P_shoup[q] = shoup(P, hc.primes[q]);
     }
     for (int k = 0; k < K; ++k) hc.primeid_special_partition[k] = L + k;
     for (int d = 0; d < dnum; ++d) {
@@ -463,6 +472,133 @@ int refgpu_dot(const uint64_t* dig, const uint64_t* x, const uint64_t* ksk_b, co
     void*** tabs = (void***)(ptrs + o + 2 * NP);
     CKKS::fusedDotKSK_2_<<<dim3{(uint32_t)N / 128, (uint32_t)(K + L)}, 128, 0, st>>>(out1, sout1, out2, sout2, tabs,
                                                                                    D, 0, K, 0);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// Tensor product over nlimbs limbs (limb k: prime k; at most L once the
+// key-switch lists are set), binomialMult_ in place: c0 <- c0 d0,
+// c1 <- c0 d1 + c1 d0, c2 <- c1 d1.
+int refgpu_binomial(uint64_t* c0, uint64_t* c1, uint64_t* c2, const uint64_t* d0, const uint64_t* d1, int nlimbs,
+                    void* stream) {
+    if (!g.dglob || !c0 || !c1 || !c2 || !d0 || !d1 || nlimbs < 1 || nlimbs > (g.L ? g.L : g.np)) return 1;
+    const size_t N = g.N;
+    cudaStream_t st = (cudaStream_t)stream;
+    void** ptrs = ptr_table({"binomial", c0, c1, c2, d0, d1, (const void*)(size_t)nlimbs}, 5 * (size_t)nlimbs, st,
+                            [&](std::vector<void*>& h, void**) {
+                                for (int k = 0; k < nlimbs; ++k) {
+                                    h[k] = c0 + k * N;
+                                    h[nlimbs + k] = c1 + k * N;
+                                    h[2 * nlimbs + k] = c2 + k * N;
+                                    h[3 * nlimbs + k] = (void*)(d0 + k * N);
+                                    h[4 * nlimbs + k] = (void*)(d1 + k * N);
+                                }
+                            });
+    if (!ptrs) return 2;
+    CKKS::binomialMult_<<<dim3{(uint32_t)N / 128, (uint32_t)nlimbs}, 128, 0, st>>>(
+        0, ptrs, ptrs + nlimbs, ptrs + 2 * nlimbs, ptrs + 3 * nlimbs, ptrs + 4 * nlimbs);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// Automorphism X -> X^k of nlimbs limbs (evaluation form), automorph_multi_:
+// out[slot(k, j)] = a[j] per limb.
+int refgpu_automorph(const uint64_t* a, uint64_t* out, int nlimbs, int k, void* stream) {
+    if (!g.dglob || !a || !out || nlimbs < 1 || nlimbs > (g.L ? g.L : g.np) || !(k & 1) || k >= 2 * g.N) return 1;
+    const size_t N = g.N;
+    cudaStream_t st = (cudaStream_t)stream;
+    void** ptrs = ptr_table({"automorph", a, out, (const void*)(size_t)nlimbs}, 2 * (size_t)nlimbs, st,
+                            [&](std::vector<void*>& h, void**) {
+                                for (int l = 0; l < nlimbs; ++l) {
+                                    h[l] = (void*)(a + l * N);
+                                    h[nlimbs + l] = out + l * N;
+                                }
+                            });
+    if (!ptrs) return 2;
+    CKKS::automorph_multi_<<<dim3{(uint32_t)N / 128, (uint32_t)nlimbs}, 128, 0, st>>>(ptrs, ptrs + nlimbs, k, 1, 0);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}
+
+// Hoisted rotations' inner product at the top level, hoistedRotateDotKSK_2_:
+// for rotation r (Galois element galois[r]) and output slot j,
+//   out_b[r][slot(g, j)] = sum_d D_d[j] kb[r][d][j] (+ P c0[j] on the
+//   ciphertext primes),  out_a[r][slot(g, j)] = sum_d D_d[j] ka[r][d][j];
+// dig and x as for refgpu_dot, c0 = [L][N]; kb[r], ka[r] point to keys
+// [dnum][L + K][N] in the plain layout; out_b[r], out_a[r] to [L + K][N]
+// (ciphertext primes then special primes).  1 <= n <= 64.
+int refgpu_hoisted_dot(const uint64_t* dig, const uint64_t* x, const uint64_t* c0, int n,
+                       const uint64_t* const* kb, const uint64_t* const* ka, const int32_t* galois,
+                       uint64_t* const* out_b, uint64_t* const* out_a, void* stream) {
+    if (!g.L || !dig || !x || !c0 || n < 1 || n > 64 || !kb || !ka || !galois || !out_b || !out_a) return 1;
+    for (int r = 0; r < n; ++r)
+        if (!kb[r] || !ka[r] || !out_b[r] || !out_a[r] || !(galois[r] & 1) || galois[r] >= 2 * g.N) return 1;
+    const int L = g.L, K = g.K, D = g.dnum, NP = L + K;
+    const size_t N = g.N;
+    cudaStream_t st = (cudaStream_t)stream;
+    // layout (pointer slots): din1 tables [4 D][NP] | c0 [L] | out1, sout1,
+    // out2, sout2 tables [n][L] / [n][K] | key tables [n][6 D][NP] |
+    // table-of-tables: din1 [4 D], out1 [n], sout1 [n], out2 [n], sout2 [n],
+    // keys [n 6 D] | galois as ints [n]
+    const size_t o_din = 0, o_c0 = o_din + 4 * (size_t)D * NP, o_out = o_c0 + L;
+    const size_t o_key = o_out + (size_t)n * (2 * L + 2 * K);
+    const size_t o_tt = o_key + (size_t)n * 6 * D * NP;
+    const size_t o_tt_din = o_tt, o_tt_o1 = o_tt_din + 4 * D, o_tt_s1 = o_tt_o1 + n, o_tt_o2 = o_tt_s1 + n,
+                 o_tt_s2 = o_tt_o2 + n, o_tt_key = o_tt_s2 + n, o_idx = o_tt_key + (size_t)n * 6 * D;
+    const size_t total = o_idx + ((size_t)n + 1) / 2;
+    std::vector<const void*> key{"hoisted", dig, x, c0, (const void*)(size_t)n};
+    for (int r = 0; r < n; ++r) {
+        key.push_back(kb[r]);
+        key.push_back(ka[r]);
+        key.push_back(out_b[r]);
+        key.push_back(out_a[r]);
+        key.push_back((const void*)(size_t)galois[r]);
+    }
+    void** ptrs = ptr_table(key, total, st, [&](std::vector<void*>& h, void** base) {
+        for (int i = 0; i < D; ++i) {
+            const int lo = i * g.alpha, hi = (lo + g.alpha < L ? lo + g.alpha : L) - 1;
+            const int nt = K + L - (hi - lo + 1);
+            for (int pos = 0; pos < nt; ++pos) h[o_din + (size_t)i * NP + pos] = (void*)(dig + ((size_t)i * NP + pos) * N);
+            for (int q = 0; q < L; ++q) h[o_din + (size_t)(3 * D + i) * NP + q] = (void*)(x + (size_t)q * N);
+        }
+        for (int q = 0; q < L; ++q) h[o_c0 + q] = (void*)(c0 + (size_t)q * N);
+        for (int r = 0; r < n; ++r) {
+            const size_t b1 = o_out + (size_t)r * (2 * L + 2 * K);  // out1 [L], sout1 [K], out2 [L], sout2 [K]
+            for (int q = 0; q < L; ++q) {
+                h[b1 + q] = out_a[r] + (size_t)q * N;
+                h[b1 + L + K + q] = out_b[r] + (size_t)q * N;
+            }
+            for (int k = 0; k < K; ++k) {
+                h[b1 + L + k] = out_a[r] + (size_t)(L + k) * N;
+                h[b1 + 2 * L + K + k] = out_b[r] + (size_t)(L + k) * N;
+            }
+            h[o_tt_o1 + r] = (void*)(base + b1);
+            h[o_tt_s1 + r] = (void*)(base + b1 + L);
+            h[o_tt_o2 + r] = (void*)(base + b1 + L + K);
+            h[o_tt_s2 + r] = (void*)(base + b1 + 2 * L + K);
+            for (int i = 0; i < D; ++i) {
+                const int lo = i * g.alpha, hi = (lo + g.alpha < L ? lo + g.alpha : L) - 1;
+                const int nt = K + L - (hi - lo + 1);
+                const size_t kt = o_key + ((size_t)r * 6 * D) * NP;
+                for (int pos = 0; pos < nt; ++pos) {
+                    const int t = hc.primeid_digit_to[i][pos];
+                    h[kt + (size_t)(D + i) * NP + pos] = (void*)(ka[r] + ((size_t)i * NP + t) * N);
+                    h[kt + (size_t)(2 * D + i) * NP + pos] = (void*)(kb[r] + ((size_t)i * NP + t) * N);
+                }
+                for (int q = 0; q < L; ++q) {
+                    h[kt + (size_t)(4 * D + i) * NP + q] = (void*)(ka[r] + ((size_t)i * NP + q) * N);
+                    h[kt + (size_t)(5 * D + i) * NP + q] = (void*)(kb[r] + ((size_t)i * NP + q) * N);
+                }
+            }
+            for (int t6 = 0; t6 < 6 * D; ++t6)
+                h[o_tt_key + (size_t)r * 6 * D + t6] = (void*)(base + o_key + ((size_t)r * 6 * D + t6) * NP);
+        }
+        for (int t4 = 0; t4 < 4 * D; ++t4) h[o_tt_din + t4] = (void*)(base + o_din + (size_t)t4 * NP);
+        int32_t* idx = reinterpret_cast<int32_t*>(h.data() + o_idx);
+        for (int r = 0; r < n; ++r) idx[r] = galois[r];
+    });
+    if (!ptrs) return 2;
+    CKKS::hoistedRotateDotKSK_2_<<<dim3{(uint32_t)N / 128, (uint32_t)(K + L)}, 128, sizeof(uint64_t) * 128 * D, st>>>(
+        (void***)(ptrs + o_tt_din), ptrs + o_c0, (void***)(ptrs + o_tt_o1), (void***)(ptrs + o_tt_s1),
+        (void***)(ptrs + o_tt_o2), (void***)(ptrs + o_tt_s2), n, (const int*)(ptrs + o_idx),
+        (void***)(ptrs + o_tt_key), D, 0, K, 0, nullptr, false);
     return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }
 

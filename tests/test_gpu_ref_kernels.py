@@ -12,10 +12,13 @@ prebuilt; without it these tests skip.
   (DecompAndModUpConv) and the ModDown conversion (ModDown2) against the
   exact base-conversion sums over the oracle's CRT constants; the key-switch
   inner product (fusedDotKSK_2_) against the oracle's, at logN 12 and at the
-  HMult shape (N = 2^16, L = 30, K = 10, dnum = 3).
-* Timing at the HMult shape, CUDA events, printed for the record: each
-  reference kernel on the work one batched step gives it, and this library's
-  batched NTT / INTT on the same residues.
+  HMult shape (N = 2^16, L = 30, K = 10, dnum = 3); the tensor product
+  (binomialMult_), the automorphism (automorph_multi_) and the hoisted
+  rotations' inner product (hoistedRotateDotKSK_2_) against the oracle's, at
+  logN 12 and at config 3's shape.
+* Timing at the HMult shape and at config 3's, CUDA events, printed for the
+  record: each reference kernel on the work one batched step gives it, and
+  this library's batched NTT / INTT on the same residues.
 """
 import ctypes as C
 import os
@@ -44,8 +47,11 @@ def ref():
     lib.refgpu_modup_conv.argtypes = [vp, vp, C.c_int, C.c_int, vp]
     lib.refgpu_moddown_conv.argtypes = [vp, vp, C.c_int, vp]
     lib.refgpu_dot.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    lib.refgpu_binomial.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp]
+    lib.refgpu_automorph.argtypes = [vp, vp, C.c_int, C.c_int, vp]
+    lib.refgpu_hoisted_dot.argtypes = [vp, vp, vp, C.c_int, vp, vp, vp, vp, vp, vp]
     for f in ("refgpu_init", "refgpu_transform", "refgpu_set_keyswitch", "refgpu_modup_conv",
-              "refgpu_moddown_conv", "refgpu_dot"):
+              "refgpu_moddown_conv", "refgpu_dot", "refgpu_binomial", "refgpu_automorph", "refgpu_hoisted_dot"):
         getattr(lib, f).restype = C.c_int
     lib.refgpu_release.argtypes = []
     yield lib
@@ -267,4 +273,136 @@ def test_reference_kernel_timing_hmult_shape(ref):
                                                             t[3].data_ptr(), ob.data_ptr(), oa.data_ptr(), _stream()))
     print("\nreference kernels at N=2^16 L=30 K=10 dnum=3 (us, CUDA events): " +
           ", ".join("%s %.1f" % kv for kv in res.items()))
+    assert all(v > 0 for v in res.values())
+
+
+def _slots(logN, g):
+    """slot(g, j) for every j: the automorphism's image of evaluation slot j
+    (bit-reversed order), as the reference's automorph_slot computes it."""
+    N = 1 << logN
+    j = np.arange(N, dtype=np.uint64)
+    br = np.zeros_like(j)
+    for b in range(logN):
+        br |= ((j >> np.uint64(b)) & np.uint64(1)) << np.uint64(logN - 1 - b)
+    r = (((2 * br + 1) * np.uint64(g)) & np.uint64(2 * N - 1)) >> np.uint64(1)
+    out = np.zeros_like(r)
+    for b in range(logN):
+        out |= ((r >> np.uint64(b)) & np.uint64(1)) << np.uint64(logN - 1 - b)
+    return out.astype(np.int64)
+
+
+def _ref_ptrs(arrs):
+    return (C.c_void_p * len(arrs))(*[a.data_ptr() for a in arrs])
+
+
+def _hoisted_expected(oc, x, dig_or, c0, kbs, kas, gals):
+    """oracle inner product + P c0 on the ciphertext primes, then scattered to
+    the automorphism's slots: out[slot(g, j)] = value[j]."""
+    L = oc.L
+    _, _, p_inv = oc.moddown_consts()
+    P = np.array([pow(int(v), -1, int(q)) for v, q in zip(p_inv, oc.primes[:L])], dtype=np.uint64)
+    pc0 = oc.polymul(c0, np.ascontiguousarray(np.broadcast_to(P[:, None], c0.shape)), list(range(L)))
+    q = np.array(oc.primes[:L], dtype=np.uint64)[:, None]
+    want = []
+    for kb, ka, g in zip(kbs, kas, gals):
+        ob, oa = oc.ks_inner(L - 1, dig_or, kb, ka)
+        ob[:L] = (ob[:L] + pc0) % q
+        sl = _slots(oc.logN, g)
+        wb, wa = np.empty_like(ob), np.empty_like(oa)
+        wb[:, sl] = ob
+        wa[:, sl] = oa
+        want.append((wb, wa))
+    return want
+
+
+@pytest.mark.parametrize("logN,L,K,qi_bits", [(12, 8, 3, 50), (16, 20, 6, 40)])
+def test_reference_tensor_automorph_hoisted_equal_oracle(ref, logN, L, K, qi_bits):
+    """binomialMult_ against the oracle's tensor product, automorph_multi_
+    against its automorphism, and hoistedRotateDotKSK_2_ (4 rotations of one
+    ModUp, plain-layout keys) against the oracle's inner product permuted and
+    with P c0 added: at logN 12 and at the hoisted-rotation shape of config 3
+    (N = 2^16, L = 20 x 40-bit, K = 6)."""
+    import torch
+
+    import pyfideslib_b200 as F
+    from oracle import oracle as O
+
+    cc = F.CryptoContext(log_n=logN, num_q=L, dnum=3, num_p=K, qi_bits=qi_bits)
+    oc = O.Ctx(cc.logN, cc.q, cc.p, cc.dnum)
+    _init(ref, oc, L + K)
+    lv = L - 1
+    a0, a1, b0, b1 = (oc.random(list(range(L)), 2000 + s) for s in range(4))
+    e0, e1, e2 = oc.tensor(lv, a0, a1, b0, b1)
+    t = [to_dev(v) for v in (a0, a1, b0, b1)]
+    c2 = torch.empty_like(t[0])
+    assert ref.refgpu_binomial(t[0].data_ptr(), t[1].data_ptr(), c2.data_ptr(), t[2].data_ptr(), t[3].data_ptr(),
+                               L, _stream()) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(from_dev(t[0]), e0) and np.array_equal(from_dev(t[1]), e1)
+    assert np.array_equal(from_dev(c2), e2)
+    gals = [cc.rotation_galois(r) for r in (1, -3, 2 ** (logN - 3))] + [2 * cc.N - 1]
+    for g in gals:
+        out = torch.empty_like(t[2])
+        assert ref.refgpu_automorph(t[2].data_ptr(), out.data_ptr(), L, g, _stream()) == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(from_dev(out), oc.automorph(b0, g)), g
+    _set_keyswitch(ref, oc)
+    x, dig_or, dig_ref, _, _ = _dot_inputs(oc, 2100)
+    c0 = oc.random(list(range(L)), 2150)
+    kpid = list(range(L + K)) * oc.dnum
+    kbs = [oc.random(kpid, 2200 + 2 * r).reshape(oc.dnum, L + K, oc.N) for r in range(len(gals))]
+    kas = [oc.random(kpid, 2201 + 2 * r).reshape(oc.dnum, L + K, oc.N) for r in range(len(gals))]
+    want = _hoisted_expected(oc, x, dig_or, c0, kbs, kas, gals)
+    dd, dx, dc0 = to_dev(dig_ref), to_dev(x), to_dev(c0)
+    dkb, dka = [to_dev(k) for k in kbs], [to_dev(k) for k in kas]
+    ob = [torch.empty((L + K, oc.N), dtype=torch.int64, device="cuda") for _ in gals]
+    oa = [torch.empty_like(o) for o in ob]
+    G = (C.c_int32 * len(gals))(*gals)
+    assert ref.refgpu_hoisted_dot(dd.data_ptr(), dx.data_ptr(), dc0.data_ptr(), len(gals), _ref_ptrs(dkb),
+                                  _ref_ptrs(dka), G, _ref_ptrs(ob), _ref_ptrs(oa), _stream()) == 0
+    torch.cuda.synchronize()
+    for r, (wb, wa) in enumerate(want):
+        assert np.array_equal(from_dev(ob[r]), wb), r
+        assert np.array_equal(from_dev(oa[r]), wa), r
+
+
+def test_reference_hoisted_timing_c3_shape(ref):
+    """hoistedRotateDotKSK_2_ over the 32 rotations of config 3 (N = 2^16,
+    L = 20 x 40-bit, K = 6, dnum = 3, level 19), one launch with the
+    reference's geometry; binomialMult_ and automorph_multi_ of one
+    top-level HMult-shape element (N = 2^16, 30 limbs).  Device time, CUDA
+    events, printed for the record."""
+    import torch
+
+    import pyfideslib_b200 as F
+    from oracle import oracle as O
+
+    cc = F.CryptoContext(log_n=16, num_q=20, dnum=3, qi_bits=40)
+    oc = O.Ctx(cc.logN, cc.q, cc.p, cc.dnum)
+    L, K, N = oc.L, oc.K, oc.N
+    _init(ref, oc, L + K)
+    _set_keyswitch(ref, oc)
+    idx = sorted({s * (1 << k) for k in range(15) for s in (1, -1)} | {3, 5})
+    gals = [cc.rotation_galois(r) for r in idx]
+    x, dig_or, dig_ref, _, _ = _dot_inputs(oc, 2300)
+    dd, dx, dc0 = to_dev(dig_ref), to_dev(x), to_dev(oc.random(list(range(L)), 2350))
+    kpid = list(range(L + K)) * oc.dnum
+    keys = [to_dev(oc.random(kpid, 2400 + r).reshape(oc.dnum, L + K, N)) for r in range(2 * len(gals))]
+    kb, ka = keys[0::2], keys[1::2]
+    ob = [torch.empty((L + K, N), dtype=torch.int64, device="cuda") for _ in gals]
+    oa = [torch.empty_like(o) for o in ob]
+    G = (C.c_int32 * len(gals))(*gals)
+    P = [_ref_ptrs(kb), _ref_ptrs(ka), _ref_ptrs(ob), _ref_ptrs(oa)]
+    res = {"ref_hoisted_dot_32_rotations": _time(lambda: ref.refgpu_hoisted_dot(
+        dd.data_ptr(), dx.data_ptr(), dc0.data_ptr(), len(gals), P[0], P[1], G, P[2], P[3], _stream()), reps=5)}
+    del keys, kb, ka, ob, oa
+    cc2, oc2 = make_pair(16, 30, 10, 3)
+    _init(ref, oc2, 30)
+    t = [to_dev(oc2.random(list(range(30)), 2500 + s)) for s in range(4)]
+    c2 = torch.empty_like(t[0])
+    res["ref_binomial_1_element"] = _time(lambda: ref.refgpu_binomial(
+        t[0].data_ptr(), t[1].data_ptr(), c2.data_ptr(), t[2].data_ptr(), t[3].data_ptr(), 30, _stream()))
+    res["ref_automorph_2x30_limbs"] = _time(lambda: [ref.refgpu_automorph(
+        t[2 + h].data_ptr(), t[h].data_ptr(), 30, gals[0], _stream()) for h in (0, 1)])
+    print("\nreference kernels (us, CUDA events): " + ", ".join("%s %.1f" % kv for kv in res.items()))
     assert all(v > 0 for v in res.values())
