@@ -1,8 +1,9 @@
 // ref_gpu.cu -- a harness that runs the reference's own GPU kernels of the
 // evaluation path on this machine's GPU, for the per-kernel comparison with
 // this library.  TEST INFRASTRUCTURE ONLY: built by `make -C oracle ref-gpu`
-// from the reference tree (src/NTT.cu, src/CKKS/Conv.cu and
-// src/CKKS/ElemenwiseBatchKernels.cu compiled unmodified) into oracle/_ref/,
+// from the reference tree (src/NTT.cu, src/CKKS/Conv.cu,
+// src/CKKS/ElemenwiseBatchKernels.cu and src/Rotation.cu compiled unmodified)
+// into oracle/_ref/,
 // loaded only by tests/test_gpu_ref_kernels.py.
 //
 // Kernels and the launch geometry each entry point repeats:

@@ -503,13 +503,16 @@ class CryptoContextImpl<DCRTPoly> {
     // The hoisted ModUp happens inside EvalFastRotation; the precomputation
     // handle is kept for signature compatibility (the reference returns
     // nullptr on GPU too, api/CryptoContext.cpp:1360-1373).
+    // m is the cyclotomic order 2N (OpenFHE's argument); 0 is accepted too.
     std::shared_ptr<void> EvalFastRotationPrecompute(const Ciphertext<DCRTPoly>&) { return nullptr; }
-    Ciphertext<DCRTPoly> EvalFastRotation(const Ciphertext<DCRTPoly>& a, int32_t index, uint32_t,
+    Ciphertext<DCRTPoly> EvalFastRotation(const Ciphertext<DCRTPoly>& a, int32_t index, uint32_t m,
                                           const std::shared_ptr<void>&) {
+        check_order(m);
         return EvalRotate(a, index);
     }
     std::vector<Ciphertext<DCRTPoly>> EvalFastRotation(const Ciphertext<DCRTPoly>& a, const std::vector<int32_t>& idx,
-                                                       uint32_t, const std::shared_ptr<void>&) {
+                                                       uint32_t m, const std::shared_ptr<void>&) {
+        check_order(m);
         std::vector<Ciphertext<DCRTPoly>> outs;
         std::vector<fides_ct*> hs;
         for (size_t i = 0; i < idx.size(); ++i) {
@@ -626,6 +629,11 @@ class CryptoContextImpl<DCRTPoly> {
     fides_ctx* ctx = nullptr;
 
   private:
+    void check_order(uint32_t m) const {
+        int logN = 0;
+        fides_ctx_info(ctx, &logN, nullptr, nullptr, nullptr, nullptr, nullptr);
+        if (m != 0 && m != (2u << logN)) throw Exception(FIDES_BAD_ARG, "EvalFastRotation: m is not the cyclotomic order 2N");
+    }
     ScalingTechnique tech;
     uint32_t hamming;
     uint32_t slots = 0;

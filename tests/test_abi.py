@@ -146,3 +146,19 @@ def test_reference_arm_loads_no_product_code():
                        timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     assert "CLEAN" in r.stdout and "NOMOD" in r.stdout, r.stdout
+
+
+def test_reference_gpu_harness_loads():
+    """The reference-kernel harness (oracle/_ref/libfidesref_gpu.so, built
+    where the reference tree is mounted) resolves every symbol it links and
+    exports its entry points; loading needs no GPU."""
+    import ctypes
+
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libfidesref_gpu.so")
+    if not os.path.exists(lib_path):
+        pytest.skip("the reference's GPU kernels were not built here")
+    lib = ctypes.CDLL(lib_path)
+    for name in ("refgpu_init", "refgpu_transform", "refgpu_set_keyswitch", "refgpu_modup_conv",
+                 "refgpu_moddown_conv", "refgpu_dot", "refgpu_binomial", "refgpu_automorph",
+                 "refgpu_hoisted_dot", "refgpu_release"):
+        assert hasattr(lib, name), name

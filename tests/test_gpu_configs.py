@@ -178,3 +178,30 @@ def test_bootstrap_precision_c5_shape():
         assert device_status(cc) == 0
     finally:
         cc.close()
+
+
+def test_sparse_bootstrap_c5_shape():
+    """EvalBootstrap with sparse packing at N=2^16, L=30: 2^12 slots, h=32,
+    budget {2,2}, degree 119: the subring projection (3 rotate-and-add
+    steps) and the 2^12-slot transforms; precision asserted against the
+    FP64 message at the advertised output level."""
+    import pyfideslib_b200 as F
+
+    cc = F.CryptoContext(log_n=16, num_q=30, dnum=3)
+    try:
+        slots = 1 << 12
+        sk = cc.KeyGen(seed=103, hamming_weight=32)
+        cc.EvalMultKeyGen(sk)
+        cc.EvalBootstrapSetup(level_budget=(2, 2), slots=slots, cheb_degree=119)
+        cc.EvalBootstrapKeyGen(sk, slots=slots)
+        out_level, _ = cc.bootstrap_info(slots)
+        rng = np.random.default_rng(103)
+        m = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+        ct = cc.Encrypt(sk, m, slots=slots, level=0, seed=9)
+        bt = cc.EvalBootstrap(ct)
+        assert bt.level == out_level and bt.slots == slots
+        bits = -np.log2(np.max(np.abs(cc.Decrypt(sk, bt, slots=slots) - m)))
+        assert bits > 13.0, bits
+        assert device_status(cc) == 0
+    finally:
+        cc.close()
