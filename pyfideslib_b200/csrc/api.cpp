@@ -308,7 +308,7 @@ fides_status fides_ctx_inject_device_error(fides_ctx* ctx, uint32_t flags) {
 }
 
 fides_status fides_set_keyswitch_variant(fides_ctx* c, int variant) {
-    if (!c || variant < 0 || variant > 7) return FIDES_BAD_ARG;
+    if (!c || variant < 0 || variant > 15) return FIDES_BAD_ARG;
     Guard g(c);
     c->dev.ks_variant = variant;
     return FIDES_OK;

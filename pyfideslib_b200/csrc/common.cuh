@@ -52,7 +52,9 @@ struct DevCtx {
     int ks_variant;              // key-switch inner product: bit 0 set: FP64 sums on primes below 2^50
                                  // (else integer sums); bit 1 set: HMult's inner product runs in the
                                  // epilogue of the ModUp digits' NTT row pass (else its own kernel);
-                                 // bit 2 set: the same for HMult batches of 8 or more elements
+                                 // bit 2 set: the same for HMult batches of 8 or more elements;
+                                 // bit 3 set: that fused row pass in two launches (ciphertext-
+                                 // prime outputs at 3 CTAs per SM, special-prime outputs at 2)
     int conv_variant;            // base conversions: 0 2 coefficients/thread 128-bit sums, 1 the same with
                                  // split 32-bit products (moduli < 2^60), 2 one coefficient/thread,
                                  // 3 and 4 ModUp and ModDown on the tensor cores (int8 split, 32

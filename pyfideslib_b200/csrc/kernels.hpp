@@ -54,6 +54,7 @@ struct KsFuseArgs {
     size_t bstride;       // words between consecutive elements of dig, own, xb, xa
     int level;
     int fp_sums;          // 1: exact FP64 sums for primes below 2^50
+    int m0;               // first output limb of a launch (set by the launcher)
 };
 void ntt_rows_keyswitch(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaStream_t st);
 // the fused row pass keeps one transformed tile per digit in shared memory

@@ -599,9 +599,11 @@ constexpr size_t ks_tile_words() {
     return (size_t)G::TR * G::CP;
 }
 
-template <int LR, int LC, bool PF, bool AQ, bool FP, bool SG = false>
-__global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constant__ DevCtx ctx,
-                                                            const __grid_constant__ KsFuseArgs a) {
+// MB: CTAs per SM the register budget is cut for (2, or 3 for the launch of
+// the ciphertext-prime outputs, which hold one digit tile less)
+template <int LR, int LC, bool PF, bool AQ, bool FP, bool SG = false, int MB = 2>
+__global__ void __launch_bounds__(256, MB) k_ntt_fwd_rows_ks(const __grid_constant__ DevCtx ctx,
+                                                             const __grid_constant__ KsFuseArgs a) {
     using G = Geo<LR, LC>;
     constexpr int R = G::R, C = G::C, CP = G::CP, TPR = G::TPR, TR = G::TR, NT = G::NTR;
     constexpr int TILE = TR * C;
@@ -612,7 +614,7 @@ __global__ void __launch_bounds__(256, 2) k_ntt_fwd_rows_ks(const __grid_constan
     __shared__ double s_gw[kSG ? 8 : 1];
 
     const int level = a.level, n = level + 1;
-    const int m = blockIdx.z;
+    const int m = a.m0 + (int)blockIdx.z;
     const size_t boff = (size_t)blockIdx.y * a.bstride;
     const int t = m < n ? m : ctx.L + (m - n);
     const PrimeConst pc = ctx.pc[t];
@@ -1052,15 +1054,39 @@ static void launch_fwd_cols(const DevCtx& ctx, const LimbMap& map, cudaStream_t 
 template <int LR, int LC, bool PF, bool AQ, bool FP, bool SG = false>
 static void launch_rows_ks_v(const DevCtx& ctx, const KsFuseArgs& a, int nb, cudaStream_t st) {
     using G = Geo<LR, LC>;
-    const size_t smem = ks_tile_words<LR, LC>() * 8 * (size_t)ctx.dnum;  // opted in by ntt_prepare
-    dim3 g(G::R / G::TR, nb, a.level + 1 + ctx.K);
-    k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG><<<g, G::NTR, smem, st>>>(ctx, a);
+    const size_t tile = ks_tile_words<LR, LC>() * 8;
+    const int n = a.level + 1;
+    if constexpr (SG) {
+      if (ctx.ks_variant & 8) {
+        // split launch: the ciphertext-prime outputs need one tile less (their
+        // own digit's value is the input limb) and run at 3 CTAs per SM; the
+        // special-prime outputs keep every digit's tile at 2 per SM
+        const int nd = a.level / ctx.alpha + 1;
+        KsFuseArgs q = a, sp = a;
+        q.m0 = 0;
+        sp.m0 = n;
+        count_launches(1);
+        k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG, 3>
+            <<<dim3(G::R / G::TR, nb, n), G::NTR, tile * (size_t)(nd - 1), st>>>(ctx, q);
+        k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG, 2>
+            <<<dim3(G::R / G::TR, nb, ctx.K), G::NTR, tile * (size_t)nd, st>>>(ctx, sp);
+        return;
+      }
+    }
+    KsFuseArgs all = a;
+    all.m0 = 0;
+    const size_t smem = tile * (size_t)ctx.dnum;  // opted in by ntt_prepare
+    dim3 g(G::R / G::TR, nb, n + ctx.K);
+    k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG><<<g, G::NTR, smem, st>>>(ctx, all);
 }
 
 template <int LR, int LC, bool PF, bool AQ, bool FP, bool SG = false>
 static void prepare_rows_ks_v(int dnum) {
-    cudaFuncSetAttribute(k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(ks_tile_words<LR, LC>() * 8 * (size_t)dnum));
+    const int bytes = (int)(ks_tile_words<LR, LC>() * 8 * (size_t)dnum);
+    cudaFuncSetAttribute(k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if constexpr (SG)
+        cudaFuncSetAttribute(k_ntt_fwd_rows_ks<LR, LC, PF, AQ, FP, SG, 3>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 template <int LR, int LC>

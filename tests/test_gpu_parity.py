@@ -291,7 +291,9 @@ def test_fused_keyswitch_every_ntt_variant(logN, L, K):
     lib.fides_autotune(cc._h, None, None, C.byref(nv))
     for v in range(nv.value):
         cc.set_ntt_variant(v)
-        for ksv in (2, 3):
+        # 2 / 3: fused (integer / FP64 sums); 10 / 11: the same in the split
+        # launch (variant 9: ciphertext-prime outputs at 3 CTAs per SM)
+        for ksv in (2, 3, 10, 11):
             assert lib.fides_set_keyswitch_variant(cc._h, ksv) == 0
             for lv in levels:
                 got = cc.EvalMult(A[lv], B[lv], rescale=lv > 0).download()
