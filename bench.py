@@ -775,7 +775,7 @@ def main():
     ap.add_argument("--conv-variant", type=int, default=-1, help="force a base-conversion variant (default: tuned)")
     ap.add_argument("--ks-variant", type=int, default=-1,
                     help="force the key-switch inner product: bit 0 FP64 sums, bit 1 fused into the NTT row pass, "
-                         "bit 2 fused for batches of 8+ (default: the context's, 5)")
+                         "bit 2 fused for batches of 8+, bit 3 the fused row pass in two launches (default: the context's, 13)")
     ap.add_argument("--profile-roofline", action="store_true",
                     help="mark the roofline NTT loop for ncu --profile-from-start off")
     ap.add_argument("--key-compression", type=int, default=1, choices=[0, 1, 2, 3],

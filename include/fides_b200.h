@@ -108,7 +108,7 @@ fides_status fides_set_conv_accumulator(fides_ctx* ctx, int accumulator);
  * or more elements only.  Bit 3: that fused row pass in two launches, the
  * ciphertext-prime outputs (one digit tile less in shared memory) at 3 CTAs
  * per SM and the special-prime outputs at 2 (forward NTT variant 9 only).
- * Default 5 (FP64 sums, fused for batches of 8+). */
+ * Default 13 (FP64 sums, fused for batches of 8+, split launch). */
 fides_status fides_set_keyswitch_variant(fides_ctx* ctx, int variant);
 /* Device error word of this context, read after the work queued so far
  * without clearing it: bit 0 is set once a tensor-core conversion gave up its

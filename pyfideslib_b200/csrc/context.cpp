@@ -477,7 +477,7 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
     d.dnum = c->dnum;
     d.alpha = c->alpha;
     d.ntt_variant = d.intt_variant = d.conv_variant = 0;  // chosen by the autotuner
-    d.ks_variant = 1 | 4;  // FP64 sums; fused into the row pass for batches of 8 or more
+    d.ks_variant = 1 | 4 | 8;  // FP64 sums; fused into the row pass (split launch) for batches of 8 or more
     d.pc = (const PrimeConst*)(base + parts[i_pc].off);
     d.fwd_tw = (const uint64_t*)(base + parts[i_fwd].off);
     d.inv_tw = (const uint64_t*)(base + parts[i_inv].off);

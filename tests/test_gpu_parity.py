@@ -256,7 +256,7 @@ def test_keyswitch_variants_bitexact(logN, L, K, dnum):
             assert lib.fides_set_keyswitch_variant(cc._h, v) == 0
             got = cc.EvalMult(cc.upload(x0, x1), cc.upload(y0, y1), rescale=True).download()
             assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), v
-    assert lib.fides_set_keyswitch_variant(cc._h, 5) == 0
+    assert lib.fides_set_keyswitch_variant(cc._h, 13) == 0
 
 
 def test_hmult_c2_shape_bitexact():
@@ -305,5 +305,5 @@ def test_fused_keyswitch_every_ntt_variant(logN, L, K):
                 got = outs[k].download()
                 assert np.array_equal(got[0], want[lv][0]) and np.array_equal(got[1], want[lv][1]), (v, ksv, lv)
     cc.set_ntt_variant(-1)
-    assert lib.fides_set_keyswitch_variant(cc._h, 5) == 0
+    assert lib.fides_set_keyswitch_variant(cc._h, 13) == 0
     assert device_status(cc) == 0
