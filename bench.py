@@ -76,6 +76,28 @@ def ntt_traffic_from_csv(path):
     return cols[-1] + rows[-1]
 
 
+def measure_h2d_link(nbytes=1 << 30, reps=3):
+    """Host-to-device bandwidth of one pinned copy of nbytes (GB/s, best of
+    reps, CUDA events on a side stream): the link the end-to-end step's
+    uploads cross."""
+    import torch
+
+    src = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    dst = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s = torch.cuda.Stream()
+    best = 0.0
+    with torch.cuda.stream(s):
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            dst.copy_(src, non_blocking=True)
+            e1.record(s)
+            e1.synchronize()
+            best = max(best, nbytes / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del src, dst
+    return best
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -639,6 +661,7 @@ def run_ours(args):
         torch.cuda.profiler.stop()
     ms_op, _ = timed(step_per_op, max(1, args.steps // 2), 2)
     ms_e2e, _ = timed(step_e2e, max(1, args.steps // 2), 1)
+    h2d_link_gbs = measure_h2d_link()
 
     # roofline: the forward NTT as the key-switch pipeline launches it, batched
     # over 32 polynomials of 30 limbs (one launch pair, 1.0 GB algorithmic
@@ -734,7 +757,12 @@ def run_ours(args):
                           int(B * 2 * 2 * (lv + 1) * N * 8 / 1e6), "parallelism": "replicas%d" % world},
                "e2e": {"value": e2e_val, "unit": "HMult/s",
                        "h2d_bytes_per_step": int(B * 2 * 2 * (lv + 1) * N * 8),
-                       "d2h_bytes_per_step": int(B * 2 * lv * N * 8)},
+                       "d2h_bytes_per_step": int(B * 2 * lv * N * 8),
+                       # the step's host-to-device bytes over its time, against one plain
+                       # pinned 1 GiB copy on the same link
+                       "h2d_link_gbs": h2d_link_gbs,
+                       "h2d_frac": (B * 2 * 2 * (lv + 1) * N * 8 * e2e_steps / (ms_e2e * 1e-3) / 1e9)
+                       / h2d_link_gbs if h2d_link_gbs else None},
                "roofline": {"kernel": "ntt_forward batched (32 polynomials x 30 limbs, k_ntt_fwd_cols + k_ntt_fwd_rows)",
                             "bound": "hbm", "achieved": achieved,
                             "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
