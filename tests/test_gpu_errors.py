@@ -47,7 +47,11 @@ def test_bootstrap_preconditions(ctx):
     assert _status(lambda: cc.EvalBootstrap(ct)) == BAD_ARG  # not set up
     # six moduli are far too few levels for the default bootstrap
     assert _status(lambda: cc.EvalBootstrapSetup()) == BAD_ARG
-    assert _status(lambda: cc.EvalBootstrapSetup(slots=cc.N // 4)) == UNSUPPORTED
+    # sparse packing is set up the same way (and fails the same way here);
+    # slot counts that are not powers of two up to N/2 are refused
+    assert _status(lambda: cc.EvalBootstrapSetup(slots=cc.N // 4)) == BAD_ARG
+    assert _status(lambda: cc.EvalBootstrapSetup(slots=3)) == BAD_ARG
+    assert _status(lambda: cc.EvalBootstrapSetup(slots=cc.N)) == BAD_ARG
     # degree beyond the levels left for a Chebyshev series
     assert _status(lambda: cc.EvalChebyshevSeries(ct, np.ones(64))) == BAD_ARG
 
