@@ -346,6 +346,13 @@ fides_status fides_bootstrap_keygen(fides_ctx* ctx, const fides_sk* sk, int slot
 /* EvalBootstrap: refresh a ciphertext (only its limb 0 is read) to the
  * output level, same slots and message. */
 fides_status fides_bootstrap(fides_ctx* ctx, const fides_ct* in, fides_ct* out);
+/* EvalBootstrap with numIterations (api/CryptoContext.hpp:180-181): 1 is
+ * fides_bootstrap; 2 bootstraps again the first result's error, scaled by
+ * 2^precision (0: 12), and subtracts it (about precision more bits).  For 2
+ * the input must be at or above the bootstrap's output level; the result is
+ * one level below that output level. */
+fides_status fides_bootstrap_iter(fides_ctx* ctx, const fides_ct* in, int iterations, int precision,
+                                  fides_ct* out);
 /* EvalBootstrap of n ciphertexts of the same slot count together: the linear
  * transforms batch their giant-step rotations over the inputs, and EvalMod
  * runs the 2n real / imaginary lanes through one batched HMult per step.

@@ -489,9 +489,14 @@ class CryptoContext:
     def EvalBootstrapKeyGen(self, sk, slots=None, seed=11):
         check(lib.fides_bootstrap_keygen(self._h, sk._h, slots or self.N // 2, seed), self._h)
 
-    def EvalBootstrap(self, a, out=None):
+    def EvalBootstrap(self, a, out=None, num_iterations=1, precision=0):
+        """num_iterations 2: bootstraps the first result's error again (the
+        input must still hold the bootstrap's output level)."""
         out = self._out(out)
-        check(lib.fides_bootstrap(self._h, a._h, out._h), self._h)
+        if num_iterations == 1:
+            check(lib.fides_bootstrap(self._h, a._h, out._h), self._h)
+        else:
+            check(lib.fides_bootstrap_iter(self._h, a._h, num_iterations, precision, out._h), self._h)
         return out
 
     def EvalBootstrapBatch(self, a_list, outs=None):

@@ -129,6 +129,7 @@ EXPORTS = {
     "fides_bootstrap_setup": ([vp, C.POINTER(BootParams)], C.c_int),
     "fides_bootstrap_info": ([vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), i32p], C.c_int),
     "fides_bootstrap_keygen": ([vp, vp, C.c_int, u64], C.c_int),
+    "fides_bootstrap_iter": ([vp, vp, C.c_int, C.c_int, vp], C.c_int),
     "fides_bootstrap": ([vp, vp, vp], C.c_int),
     "fides_linear_transform": ([vp, vp, C.c_int, i32p, C.POINTER(vp), C.c_int, C.c_int, vp], C.c_int),
     "fides_linear_transform_batch": ([vp, C.c_int, C.POINTER(vp), C.c_int, i32p, C.POINTER(vp), C.c_int, C.c_int,

@@ -68,13 +68,6 @@ fides_status fides_ctx_create(const fides_params* params, fides_ctx** out) {
         if (cudaDeviceGetDefaultMemPool(&mp, params->device) == cudaSuccess) {
             uint64_t thr = UINT64_MAX;
             cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
-            // an allocation on one stream (an upload on the copy stream) must
-            // not reuse a block freed on another (inputs freed behind a
-            // computation still running) by waiting for that free: the wait
-            // would serialise the next batch's uploads behind this batch's
-            // kernels.  Blocks whose free has completed are still reused.
-            int no = 0;
-            cudaMemPoolSetAttribute(mp, cudaMemPoolReuseAllowInternalDependencies, &no);
         }
     }
     fides_status s = build_context(c, params);

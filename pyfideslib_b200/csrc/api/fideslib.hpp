@@ -604,15 +604,14 @@ class CryptoContextImpl<DCRTPoly> {
         check(fides_bootstrap_keygen(ctx, sk->handle, s, seed), ctx);
         seed += 2;
     }
-    // numIterations > 1 (OpenFHE's iterated bootstrapping, which needs the
-    // input at a higher level to form the residual) is not supported here.
+    // numIterations 2: the first result's error is bootstrapped again, scaled
+    // by 2^precision (0: 12), and subtracted; the input must still hold the
+    // bootstrap's output level (fides_bootstrap_iter).
     Ciphertext<DCRTPoly> EvalBootstrap(const Ciphertext<DCRTPoly>& a, uint32_t numIterations = 1,
                                        uint32_t precision = 0, bool prescaled = false) {
-        (void)precision;
         (void)prescaled;
-        if (numIterations > 1) throw Exception(FIDES_UNSUPPORTED, "EvalBootstrap: numIterations > 1");
         auto o = empty();
-        check(fides_bootstrap(ctx, prepare(a)->handle, o->handle), ctx);
+        check(fides_bootstrap_iter(ctx, prepare(a)->handle, (int)numIterations, (int)precision, o->handle), ctx);
         return o;
     }
     void EvalBootstrapInPlace(Ciphertext<DCRTPoly>& a, uint32_t numIterations = 1, uint32_t precision = 0,

@@ -716,6 +716,50 @@ fides_status fides_bootstrap(fides_ctx* c, const fides_ct* in, fides_ct* out) {
     return fides_bootstrap_batch(c, 1, &in, &out);
 }
 
+// Two iterations (the reference's EvalBootstrap(ct, numIterations = 2,
+// precision), api/CryptoContext.hpp:180-181, which OpenFHE implements): y =
+// the first bootstrap brought to the input's scale, r = in - y carries minus
+// the first bootstrap's error e1; r times 2^p is bootstrapped again (its
+// message 2^p e1 is of size about 1), the result's scale is taken 2^p times
+// larger (its message becomes -e1 + e2 / 2^p) and brought to y's scale, and
+// the sum leaves m + e2 / 2^p.  The input must still hold the levels of a
+// bootstrap's output; the result is one level below it.
+fides_status fides_bootstrap_iter(fides_ctx* c, const fides_ct* in, int iterations, int precision, fides_ct* out) {
+    if (!c || !in || !in->buf || !out || iterations < 1 || iterations > 2 || precision < 0 || precision > 30)
+        return FIDES_BAD_ARG;
+    if (iterations == 1) return fides_bootstrap(c, in, out);
+    Guard g(c);
+    const int n = in->slots > 0 ? in->slots : c->N / 2;
+    auto it = c->boot.find(n);
+    if (it == c->boot.end()) return set_err(c, FIDES_BAD_ARG, "bootstrapping not set up for these slots");
+    const BootPrecomp& B = *it->second;
+    if (in->level < B.level_out || B.level_out < 1)
+        return set_err(c, FIDES_BAD_ARG, "a second bootstrap iteration needs the input at the bootstrap's output level");
+    const int p = precision > 0 ? precision : 12;
+    Arith A(c);
+    Lanes bt = A.fresh(1);
+    fides_status s = fides_bootstrap(c, in, bt[0]);
+    if (s != FIDES_OK) return s;
+    Lanes y = A.normalize(bt, in->scale);  // level_out - 1, scale within 2^-50 of the input's
+    if (!A.ok()) return A.st;
+    Lanes r = A.fresh(3);
+    if ((s = fides_sub(c, in, y[0], r[0])) != FIDES_OK) return s;  // -e1 at the input's scale
+    if ((s = fides_mult_int(c, r[0], (int64_t)1 << p, r[1])) != FIDES_OK) return s;
+    r[1]->scale = in->scale;  // the message is 2^p (-e1)
+    r[1]->slots = in->slots;
+    if ((s = fides_bootstrap(c, r[1], r[2])) != FIDES_OK) return s;
+    r[2]->scale *= (double)(1ll << p);  // message -e1 + e2 / 2^p
+    Lanes rr{r[2]};
+    Lanes r4 = A.normalize(rr, y[0]->scale);
+    if (!A.ok()) return A.st;
+    const double sc = y[0]->scale;
+    if ((s = fides_add(c, y[0], r4[0], out)) != FIDES_OK) return s;
+    out->scale = sc;
+    out->slots = in->slots;
+    out->noise_deg = 1;
+    return check_cuda(c, "bootstrap iterations");
+}
+
 fides_status fides_bootstrap_batch(fides_ctx* c, int nin, const fides_ct* const* in, fides_ct* const* out) {
     if (!c || nin < 1 || !in || !out) return FIDES_BAD_ARG;
     for (int u = 0; u < nin; ++u)

@@ -238,3 +238,34 @@ def test_sparse_bootstrap_precision(slots):
         g0, g1 = o.download()
         assert np.array_equal(g0, r0) and np.array_equal(g1, r1)
     assert device_status(cc) == 0
+
+
+def test_two_iteration_bootstrap_precision():
+    """EvalBootstrap(ct, numIterations=2): the first result's error is
+    bootstrapped again at 2^12 and subtracted; the result decrypts to the
+    message with at least 8 more bits than one bootstrap, one level below a
+    single bootstrap's output.  An input below the bootstrap's output level
+    is refused for a second iteration."""
+    import pyfideslib_b200 as F
+
+    cc = F.CryptoContext(log_n=12, num_q=20, dnum=4)
+    sk = cc.KeyGen(seed=29, hamming_weight=32)
+    cc.EvalMultKeyGen(sk)
+    cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=63)
+    cc.EvalBootstrapKeyGen(sk)
+    out_level, _ = cc.bootstrap_info()
+    slots = cc.N // 2
+    rng = np.random.default_rng(29)
+    m = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+    ct = cc.Encrypt(sk, m, slots=slots, level=out_level + 2, seed=5)
+    one = cc.EvalBootstrap(ct)
+    two = cc.EvalBootstrap(ct, num_iterations=2, precision=12)
+    assert two.level == out_level - 1
+    b1 = -np.log2(np.max(np.abs(cc.Decrypt(sk, one, slots=slots) - m)))
+    b2 = -np.log2(np.max(np.abs(cc.Decrypt(sk, two, slots=slots) - m)))
+    assert b2 > b1 + 8, (b1, b2)
+    low = cc.Encrypt(sk, m, slots=slots, level=0, seed=6)
+    from pyfideslib_b200._capi import FidesError
+    with pytest.raises(FidesError):
+        cc.EvalBootstrap(low, num_iterations=2)
+    assert device_status(cc) == 0
