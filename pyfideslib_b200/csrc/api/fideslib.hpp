@@ -231,6 +231,16 @@ class CryptoContextImpl<DCRTPoly> {
         return 1u << l;
     }
     uint32_t GetCyclotomicOrder() const { return 2 * GetRingDimension(); }
+    void Enable(uint32_t) {}
+    // The bootstrap here takes its input at any scale and level (it reads the
+    // first limb and tracks the scale exactly), so no pre-scaling is needed:
+    // the factor a caller multiplies by before a `prescaled` EvalBootstrap
+    // (api/CryptoContext.cpp:148-153) is 1.
+    double GetPreScaleFactor(uint32_t) const { return 1.0; }
+    // Ciphertexts and plaintexts of this API live on the device from the
+    // start; there is nothing to load lazily (api/CryptoContext.cpp:158-165).
+    void SetAutoLoadPlaintexts(bool) {}
+    void SetAutoLoadCiphertexts(bool) {}
 
     KeyPair<DCRTPoly> KeyGen() {
         KeyPair<DCRTPoly> kp;
