@@ -370,7 +370,23 @@ def measure_bootstrap(cc, reps=3, seed=101, degree=119):
         e1.synchronize()
         batch_ms[nb] = e0.elapsed_time(e1)
         del outs_b
-    res = {"bootstrap_ms": ms, "wall_ms": wall_ms, "precision_bits": -float(np.log2(err)), "max_abs_err": err,
+    # client side, all on the device: encode + encrypt at level 29 and
+    # decrypt + decode of 2^15 slots (blocking host calls, wall clock, median
+    # of 5)
+    def wall(fn):
+        ts = []
+        for _ in range(6):
+            t = time.perf_counter()
+            fn()
+            ts.append((time.perf_counter() - t) * 1e3)
+        return float(np.median(ts[1:]))
+
+    top = cc.Encrypt(sk, msgs[0], slots=slots, seed=19)
+    client = {"encrypt_ms": wall(lambda: cc.Encrypt(sk, msgs[1], slots=slots, seed=23)),
+              "decrypt_ms": wall(lambda: cc.Decrypt(sk, top, slots=slots)),
+              "level": top.level, "slots": slots}
+    del top
+    res = {"bootstrap_ms": ms, "wall_ms": wall_ms, "client": client, "precision_bits": -float(np.log2(err)), "max_abs_err": err,
            "precision_bits_correction6": -float(np.log2(err6)),
            "two_iterations": {"ms": ms2, "precision_bits": -float(np.log2(err2)), "input_level": out_level,
                               "output_level": out_level - 1},

@@ -451,15 +451,22 @@ fides_status fides_set_key_compression(fides_ctx* ctx, int mask);
 /* Export generated switching keys (dnum*(L+K)*N words each) for interop tests. */
 fides_status fides_key_export(fides_ctx* ctx, uint32_t galois, uint64_t* b, uint64_t* a);
 /* Encode `slots` complex values (re, im interleaved) at `level` and `scale`
- * into evaluation-form residues m[(level+1)*N]. */
+ * into evaluation-form residues m[(level+1)*N] (host memory).  The FFT,
+ * rounding and NTT run on the device.  Replaces OpenFHE's
+ * MakeCKKSPackedPlaintext, which the reference calls on the CPU
+ * (api/CryptoContext.cpp:475-514). */
 fides_status fides_encode(fides_ctx* ctx, const double* values, int slots, int level, double scale, uint64_t* m);
-/* Encrypt with the secret key (symmetric CKKS encryption). */
+/* Encrypt with the secret key (symmetric CKKS encryption); the error and
+ * uniform polynomials are drawn on the device from `seed`. */
 fides_status fides_encrypt(fides_ctx* ctx, const fides_sk* sk, const double* values, int slots, int level,
                            double scale, uint64_t seed, fides_ct** out);
 /* Synthetic ciphertext with residues drawn uniformly on the device (seeded):
  * benchmark and test input without a host round trip. */
 fides_status fides_ct_random(fides_ctx* ctx, int level, uint64_t seed, fides_ct** out);
-/* Decrypt and decode into `slots` complex values (re, im interleaved). */
+/* Decrypt and decode into `slots` complex values (re, im interleaved): the
+ * CRT of the first three moduli and the decoding FFT run on the device, only
+ * the slots are copied back.  Replaces OpenFHE's Decrypt
+ * (api/CryptoContext.cpp:560-626). */
 fides_status fides_decrypt(fides_ctx* ctx, const fides_sk* sk, const fides_ct* ct, double* values, int slots);
 
 #ifdef __cplusplus

@@ -39,7 +39,6 @@
 // batched call over both.
 #include <algorithm>
 #include <cmath>
-#include <complex>
 #include <map>
 #include <memory>
 #include <new>
@@ -47,7 +46,6 @@
 #include "context.hpp"
 
 using namespace fides;
-using cplx = std::complex<double>;
 
 namespace fides {
 
@@ -105,60 +103,155 @@ uint64_t real_mod(long double x, uint64_t p) {
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal-form slot matrices: (M x)[i] = sum_o d_o[i] x[(i + o) mod n].
+// Diagonal-form slot matrices, built on the device: (M x)[i] =
+// sum_o d_o[i] x[(i + o) mod n], the live diagonals of a group held as rows
+// of an [rows][n] complex array in HBM.
 // ---------------------------------------------------------------------------
-using Diag = std::map<int, std::vector<cplx>>;
 
-// Butterfly stage s (block length 2^s) of the special FFT or its inverse.
-Diag fft_stage(int n, int s, bool inverse) {
-    const int len = 1 << s, h = len >> 1, lenq = len << 2;
-    Diag d;
-    auto& d0 = d[0];
-    d0.assign(n, 0.0);
-    std::vector<cplx> dp(n, 0.0), dm(n, 0.0), tw(h);
-    uint64_t g = 1;  // 5^j mod 4*len
-    for (int j = 0; j < h; ++j) {
-        const double ang = 2.0 * M_PI * (double)g / (double)lenq;
-        tw[j] = cplx(cos(ang), sin(ang));
-        g = (g * 5) % (uint64_t)lenq;
+// Entry i of diagonal `type` of butterfly stage s (block length 2^s,
+// h = 2^(s-1); type 0 at offset 0, 1 at +h, 2 at -h).  With jj = i mod 2^s,
+// j = jj mod h and t = exp(2 pi i (5^j mod 2^(s+2)) / 2^(s+2)), written as
+// (jj < h | jj >= h):
+//   SlotsToCoeffs A_s:     d0 = 1 | -t,           d+ = t | 0,    d- = 0 | 1
+//   CoeffsToSlots A_s^-1:  d0 = 1/2 | -conj(t)/2, d+ = 1/2 | 0,  d- = 0 | conj(t)/2
+__device__ double2 stage_entry(int type, int s, int i, bool inverse) {
+    const int len = 1 << s, h = len >> 1;
+    const int jj = i & (len - 1);
+    const bool lo = jj < h;
+    if (type == 1 && !lo) return make_double2(0, 0);
+    if (type == 2 && lo) return make_double2(0, 0);
+    if (lo && (type == 0 || inverse)) return make_double2(inverse ? 0.5 : 1.0, 0);
+    if (!lo && type == 2 && !inverse) return make_double2(1.0, 0);
+    // the twiddle t of j = jj mod h: 5^j mod 4 len, by squaring
+    const uint32_t mask = (uint32_t)(len << 2) - 1;
+    uint32_t g = 1, b = 5;
+    for (uint32_t e = (uint32_t)(jj & (h - 1)); e; e >>= 1) {
+        if (e & 1) g = (uint32_t)(((uint64_t)g * b) & mask);
+        b = (uint32_t)(((uint64_t)b * b) & mask);
     }
-    for (int p = 0; p < n; ++p) {
-        const int jj = p & (len - 1);
-        const int j = jj < h ? jj : jj - h;
-        const cplx t = tw[j];
-        if (jj < h) {
-            d0[p] += inverse ? 0.5 : 1.0;
-            dp[p] += inverse ? cplx(0.5) : t;
-        } else {
-            dm[p] += inverse ? 1.0 / (2.0 * t) : cplx(1.0);
-            d0[p] += inverse ? -1.0 / (2.0 * t) : -t;
-        }
-    }
-    auto acc = [&](int off, const std::vector<cplx>& v) {
-        auto& t = d[((off % n) + n) % n];
-        if (t.empty()) t.assign(n, 0.0);
-        for (int i = 0; i < n; ++i) t[i] += v[i];
-    };
-    acc(h, dp);
-    acc(-h, dm);
-    return d;
+    double sn, cs;
+    sincospi((double)g / (double)(len << 1), &sn, &cs);  // angle 2 pi g / (4 len)
+    if (!inverse) return type == 0 ? make_double2(-cs, -sn) : make_double2(cs, sn);  // -t (jj >= h) or t
+    return type == 0 ? make_double2(-0.5 * cs, 0.5 * sn) : make_double2(0.5 * cs, -0.5 * sn);
 }
 
-// A * B (B applied first).
-Diag diag_mul(int n, const Diag& A, const Diag& B) {
-    Diag C;
-    for (const auto& a : A)
-        for (const auto& b : B) {
-            auto& t = C[(a.first + b.first) % n];
-            if (t.empty()) t.assign(n, 0.0);
-            for (int i = 0; i < n; ++i) t[i] += a.second[i] * b.second[(i + a.first) % n];
-        }
-    for (auto it = C.begin(); it != C.end();) {
-        double mx = 0;
-        for (const cplx& v : it->second) mx = std::max(mx, std::abs(v));
-        it = mx < 1e-300 ? C.erase(it) : std::next(it);
+// C_c = A_s B: C_c[i] = sum_type d_type[i] B_b[(i + o_type) mod n], b the row
+// of offset o_c - o_type (src[3 c + type], -1 when absent)
+__global__ void k_diag_stage(const double2* __restrict__ B, double2* __restrict__ Cm, const int* __restrict__ src,
+                             int n, int s, int inverse) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (i >= n) return;
+    const int h = 1 << (s - 1);
+    const int off[3] = {0, h, n - h};
+    double2 acc = make_double2(0, 0);
+#pragma unroll
+    for (int type = 0; type < 3; ++type) {
+        const int b = src[3 * c + type];
+        if (b < 0) continue;
+        const double2 d = stage_entry(type, s, i, inverse != 0);
+        const double2 x = B[(size_t)b * n + ((i + off[type]) & (n - 1))];
+        acc.x += d.x * x.x - d.y * x.y;
+        acc.y += d.x * x.y + d.y * x.x;
     }
-    return C;
+    Cm[(size_t)c * n + i] = acc;
+}
+
+__global__ void k_diag_fill(double2* __restrict__ M, int n, double v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) M[i] = make_double2(v, 0);
+}
+
+// largest |entry| of each row (one CTA per row)
+__global__ void k_diag_absmax(const double2* __restrict__ M, int n, double* __restrict__ out) {
+    __shared__ double red[256];
+    double m = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double2 v = M[(size_t)blockIdx.x * n + i];
+        m = fmax(m, hypot(v.x, v.y));
+    }
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k; k >>= 1) {
+        if (threadIdx.x < k) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + k]);
+        __syncthreads();
+    }
+    if (!threadIdx.x) out[blockIdx.x] = red[0];
+}
+
+// The product of butterfly stages `stages` (the first applied first) in
+// diagonal form: offsets in [0, n), increasing, with row[k] the row of
+// offs[k] in buf.  Diagonals that come out exactly zero are dropped after
+// every stage.
+struct DevDiag {
+    fides_ctx* c = nullptr;
+    int n = 0;
+    std::vector<int> offs, row;
+    double2* buf = nullptr;
+    ~DevDiag() {
+        if (buf) cudaFreeAsync(buf, c->st);
+    }
+};
+
+fides_status diag_group(fides_ctx* c, int n, const std::vector<int>& stages, bool inverse, DevDiag& M) {
+    M.c = c;
+    M.n = n;
+    M.offs = {0};
+    M.row = {0};
+    if (cudaMallocAsync((void**)&M.buf, (size_t)n * 16, c->st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FIDES_OOM, "bootstrap diagonals");
+    }
+    count_launches(1);
+    k_diag_fill<<<(n + 255) / 256, 256, 0, c->st>>>(M.buf, n, 1.0);
+    for (int s : stages) {
+        const int h = 1 << (s - 1);
+        std::map<int, int> live;  // offset -> row of the current product
+        for (size_t k = 0; k < M.offs.size(); ++k) live[M.offs[k]] = M.row[k];
+        std::map<int, int> out;  // offset of the new product -> its row
+        for (const auto& kv : live)
+            for (int oa : {0, h, n - h}) out.emplace((kv.first + oa) % n, 0);
+        std::vector<int> src(3 * out.size(), -1), offs;
+        int r = 0;
+        for (auto& kv : out) {
+            kv.second = r;
+            const int oa[3] = {0, h, n - h};
+            for (int t = 0; t < 3; ++t) {
+                auto it = live.find(((kv.first - oa[t]) % n + n) % n);
+                if (it != live.end()) src[3 * r + t] = it->second;
+            }
+            offs.push_back(kv.first);
+            ++r;
+        }
+        // one allocation: the new rows, the source table, the row maxima
+        const size_t b_rows = (size_t)r * n * 16, b_src = ((size_t)3 * r * 4 + 15) / 16 * 16;
+        char* nb = nullptr;
+        if (cudaMallocAsync((void**)&nb, b_rows + b_src + (size_t)r * 8, c->st) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(c, FIDES_OOM, "bootstrap diagonals");
+        }
+        int* dsrc = (int*)(nb + b_rows);
+        double* dmax = (double*)(nb + b_rows + b_src);
+        cudaMemcpyAsync(dsrc, src.data(), src.size() * 4, cudaMemcpyHostToDevice, c->st);
+        count_launches(2);
+        k_diag_stage<<<dim3((n + 255) / 256, r), 256, 0, c->st>>>(M.buf, (double2*)nb, dsrc, n, s, inverse ? 1 : 0);
+        k_diag_absmax<<<r, 256, 0, c->st>>>((double2*)nb, n, dmax);
+        std::vector<double> mx(r);
+        cudaMemcpyAsync(mx.data(), dmax, (size_t)r * 8, cudaMemcpyDeviceToHost, c->st);
+        cudaFreeAsync(M.buf, c->st);
+        M.buf = (double2*)nb;
+        cudaStreamSynchronize(c->st);
+        fides_status e = check_cuda(c, "bootstrap diagonals");
+        if (e != FIDES_OK) return e;
+        M.offs.clear();
+        M.row.clear();
+        for (int k = 0; k < r; ++k)
+            if (mx[k] >= 1e-300) {
+                M.offs.push_back(offs[k]);
+                M.row.push_back(k);
+            }
+    }
+    return FIDES_OK;
 }
 
 // Stage groups: `budget` contiguous groups of the logn butterfly stages,
@@ -177,16 +270,18 @@ std::vector<std::vector<int>> stage_groups(int logn, int budget, bool descending
     return g;
 }
 
-// scale 0: the modulus of `level`, so the transform keeps the ciphertext's scale
-fides_status encode_stage(fides_ctx* c, int n, const Diag& M, int level, double factor, double enc_scale,
-                          BootStage& st) {
+// scale 0: the modulus of `level`, so the transform keeps the ciphertext's
+// scale.  Queued on the context stream; *bad (device) flags a coefficient at
+// or above 2^63.
+fides_status encode_stage(fides_ctx* c, int n, const DevDiag& M, int level, double factor, double enc_scale,
+                          BootStage& st, int* bad) {
     st.level = level;
     // offsets centred in (-n/2, n/2]; baby step ~ sqrt(#diagonals) in units of
     // the smallest offset step
     std::vector<int> offs;
     int unit = n;
-    for (const auto& kv : M) {
-        int o = kv.first > n / 2 ? kv.first - n : kv.first;
+    for (int raw : M.offs) {
+        int o = raw > n / 2 ? raw - n : raw;
         offs.push_back(o);
         if (o) unit = std::min(unit, std::abs(o) & -std::abs(o));
     }
@@ -196,15 +291,9 @@ fides_status encode_stage(fides_ctx* c, int n, const Diag& M, int level, double 
     while (bk * bk < nd) bk <<= 1;
     st.bstep = bk * unit;
     const double scale = enc_scale > 0 ? enc_scale : (double)c->host.prime[level];
-    std::vector<double> vals(2 * (size_t)n);
-    for (int o : offs) {
-        const auto& d = M.at(((o % n) + n) % n);
+    for (size_t k = 0; k < offs.size(); ++k) {
+        const int o = offs[k];
         const int G = floor_div(o, st.bstep) * st.bstep;
-        for (int j = 0; j < n; ++j) {
-            const cplx v = d[(size_t)((((j - G) % n) + n) % n)] * factor;
-            vals[2 * (size_t)j] = v.real();
-            vals[2 * (size_t)j + 1] = v.imag();
-        }
         fides_pt* pt = new (std::nothrow) fides_pt();
         if (!pt) return FIDES_OOM;
         pt->cap = level + 1;
@@ -215,7 +304,8 @@ fides_status encode_stage(fides_ctx* c, int n, const Diag& M, int level, double 
         }
         st.pts.push_back(pt);
         st.offsets.push_back(o);
-        fides_status s = encode_dev(c, vals.data(), n, level, scale, pt->m);
+        // slot j of the plaintext holds d_o[(j - G) mod n] * factor
+        fides_status s = encode_dev_z(c, M.buf + (size_t)M.row[k] * n, n, G, factor, level, scale, pt->m, bad);
         if (s != FIDES_OK) return s;
         pt->level = level;
         pt->scale = scale;
@@ -645,27 +735,44 @@ fides_status fides_bootstrap_setup(fides_ctx* c, const fides_boot_params* prm) {
     if (bp->level_out < 0)
         return set_err(c, FIDES_BAD_ARG, "not enough levels for bootstrapping (need " +
                                              std::to_string(top - bp->level_out) + " of " + std::to_string(top) + ")");
+    // the diagonals are generated and encoded on the device; one flag for
+    // every encoding, read once at the end
+    int* bad = nullptr;
+    if (cudaMallocAsync((void**)&bad, sizeof(int), c->st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FIDES_OOM, "bootstrap setup");
+    }
+    cudaMemsetAsync(bad, 0, sizeof(int), c->st);
+    struct FlagFree {
+        fides_ctx* c;
+        int* p;
+        ~FlagFree() { cudaFreeAsync(p, c->st); }
+    } flag_free{c, bad};
     // CoeffsToSlots: A_1^-1 ... A_logn^-1, highest stages applied first
     for (size_t b = 0; b < gc.size(); ++b) {
-        Diag M;
-        M[0] = std::vector<cplx>(n, 1.0);
-        for (int s : gc[b]) M = diag_mul(n, fft_stage(n, s, true), M);
+        DevDiag M;
+        fides_status e = diag_group(c, n, gc[b], true, M);
+        if (e != FIDES_OK) return e;
         BootStage st;
-        fides_status e = encode_stage(c, n, M, top - (int)b, 1.0, kCtsDiagScale, st);
+        e = encode_stage(c, n, M, top - (int)b, 1.0, kCtsDiagScale, st, bad);
         bp->cts.push_back(std::move(st));
         if (e != FIDES_OK) return e;
     }
     // SlotsToCoeffs: A_logn ... A_1, with q0 / (2 pi D) in the first group
     const double fac = (double)c->host.prime[0] / (2.0 * M_PI * c->default_scale);
     for (size_t b = 0; b < gs.size(); ++b) {
-        Diag M;
-        M[0] = std::vector<cplx>(n, 1.0);
-        for (int s : gs[b]) M = diag_mul(n, fft_stage(n, s, false), M);
+        DevDiag M;
+        fides_status e = diag_group(c, n, gs[b], false, M);
+        if (e != FIDES_OK) return e;
         BootStage st;
-        fides_status e = encode_stage(c, n, M, bp->level_after_mod - (int)b, b == 0 ? fac : 1.0, 0.0, st);
+        e = encode_stage(c, n, M, bp->level_after_mod - (int)b, b == 0 ? fac : 1.0, 0.0, st, bad);
         bp->stc.push_back(std::move(st));
         if (e != FIDES_OK) return e;
     }
+    int hbad = 0;
+    cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->st);
+    cudaStreamSynchronize(c->st);
+    if (hbad) return set_err(c, FIDES_BAD_ARG, "bootstrap diagonal coefficient exceeds 2^63");
     std::vector<int32_t> rot;
     for (auto* v : {&bp->cts, &bp->stc})
         for (auto& st : *v)

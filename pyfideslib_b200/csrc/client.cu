@@ -7,9 +7,10 @@
 //   * encoding: canonical embedding with slot j at the root zeta^(5^j)
 //     (zeta = e^{i pi / N}); sparse packings repeat the slots with period n.
 //     Evaluated with one complex FFT of size N over the odd powers of zeta.
-//   * secrets: ternary, uniform or with a fixed Hamming weight; errors:
-//     rounded Gaussian, sigma 3.2; uniform polynomials drawn on the device
-//     from a counter-based hash.
+//   * secrets: ternary, uniform or with a fixed Hamming weight (host, then
+//     uploaded); errors (rounded Gaussian, sigma 3.2, Box-Muller), ephemeral
+//     ternary polynomials and uniform polynomials drawn on the device from a
+//     counter-based hash.
 //   * switching keys (hybrid, digits of alpha moduli):
 //       b_d = -a_d * s_b + e_d + [P]_{q_i} * s_g   on the moduli of digit d,
 //       b_d = -a_d * s_b + e_d                    elsewhere,
@@ -17,12 +18,12 @@
 //     (sigma_g^-1(s), s) for the automorphism sigma_g: X -> X^g, matching the
 //     order in which the evaluation applies the permutation (after the inner
 //     product, before ModDown).
-//   * decryption: c0 + c1 s on the device, INTT, then a mixed-radix CRT of the
-//     first three moduli on the host (values of decryptable ciphertexts are
-//     far below q0 q1 q2 / 2).
+//   * decryption: c0 + c1 s, INTT, a mixed-radix CRT of the first three
+//     moduli (values of decryptable ciphertexts are far below q0 q1 q2 / 2)
+//     and the forward embedding FFT, all on the device; only the slots come
+//     back to the host.
 #include <algorithm>
 #include <cmath>
-#include <complex>
 #include <cstring>
 #include <new>
 #include <random>
@@ -31,7 +32,6 @@
 #include "context.hpp"
 
 using namespace fides;
-using cplx = std::complex<double>;
 
 namespace {
 
@@ -57,23 +57,8 @@ struct Xoshiro {
         s[3] = rotl(s[3], 45);
         return r;
     }
-    double uniform01() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
 };
 
-std::vector<int64_t> gaussian(int N, uint64_t seed, double sigma = 3.2) {
-    Xoshiro r(seed);
-    std::vector<int64_t> e(N);
-    for (int i = 0; i < N; i += 2) {
-        double u1 = r.uniform01(), u2 = r.uniform01();
-        if (u1 < 1e-300) u1 = 1e-300;
-        const double rad = sqrt(-2.0 * log(u1)) * sigma;
-        e[i] = llround(rad * cos(2 * M_PI * u2));
-        if (i + 1 < N) e[i + 1] = llround(rad * sin(2 * M_PI * u2));
-    }
-    return e;
-}
-
-// ---- device helpers ----
 __global__ void k_small_to_rns(const int64_t* __restrict__ v, uint64_t* __restrict__ out, int N, int q0,
                                const PrimeConst* __restrict__ pcs) {
     const int limb = blockIdx.y;
@@ -93,6 +78,39 @@ __global__ void k_fill_uniform(uint64_t* __restrict__ out, int N, int q0, const 
     out[(size_t)limb * N + j] = uniform_mod(stream, q0 + limb, (uint32_t)j, p);
 }
 
+// Small polynomials drawn on the device, coefficient form, on limbs
+// 0..nlimbs-1: KIND 0 a rounded Gaussian (Box-Muller, one pair of
+// coefficients per thread, standard deviation sigma), KIND 1 uniform ternary.
+// Pair i draws the counters stream ^ 2i and stream ^ (2i + 1).
+constexpr double kErrorSigma = 3.2;
+template <int KIND>
+__global__ void k_sample_small(uint64_t* __restrict__ out, int N, int nlimbs, const PrimeConst* __restrict__ pcs,
+                               uint64_t stream) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (2 * i >= N) return;
+    const uint64_t h0 = hash64(stream ^ (uint64_t)(2 * i)), h1 = hash64(stream ^ (uint64_t)(2 * i + 1));
+    int64_t x0, x1;
+    if (KIND == 0) {
+        const double u1 = (double)((h0 >> 11) + 1) * 0x1p-53;  // (0, 1]
+        const double u2 = (double)(h1 >> 11) * 0x1p-53;        // [0, 1)
+        const double r = sqrt(-2.0 * log(u1)) * kErrorSigma;
+        double sn, cs;
+        sincospi(2.0 * u2, &sn, &cs);
+        x0 = llrint(r * cs);
+        x1 = llrint(r * sn);
+    } else {
+        x0 = (int64_t)__umul64hi(h0, 3) - 1;
+        x1 = (int64_t)__umul64hi(h1, 3) - 1;
+    }
+    for (int limb = 0; limb < nlimbs; ++limb) {
+        const uint64_t p = pcs[limb].p;
+        ulonglong2 v;
+        v.x = x0 < 0 ? p - (uint64_t)(-x0) : (uint64_t)x0;
+        v.y = x1 < 0 ? p - (uint64_t)(-x1) : (uint64_t)x1;
+        *(ulonglong2*)(out + (size_t)limb * N + 2 * i) = v;
+    }
+}
+
 // b = -a * sb + e (+ pmod_i * sg on limbs with lo <= prime < hi)
 __global__ void k_key_combine(uint64_t* __restrict__ b, const uint64_t* __restrict__ a,
                               const uint64_t* __restrict__ sb, const uint64_t* __restrict__ e,
@@ -106,58 +124,6 @@ __global__ void k_key_combine(uint64_t* __restrict__ b, const uint64_t* __restri
     b[i] = v;
 }
 
-// ---- host FFT ----
-void fft(std::vector<cplx>& a, bool inverse) {
-    const int n = (int)a.size();
-    for (int i = 1, j = 0; i < n; ++i) {
-        int bit = n >> 1;
-        for (; j & bit; bit >>= 1) j ^= bit;
-        j ^= bit;
-        if (i < j) std::swap(a[i], a[j]);
-    }
-    for (int len = 2; len <= n; len <<= 1) {
-        const double ang = 2 * M_PI / len * (inverse ? -1 : 1);
-        const cplx wl(cos(ang), sin(ang));
-        std::vector<cplx> w(len / 2);
-        w[0] = 1;
-        for (int k = 1; k < len / 2; ++k) w[k] = (k % 64 == 0) ? cplx(cos(ang * k), sin(ang * k)) : w[k - 1] * wl;
-        for (int i = 0; i < n; i += len)
-            for (int k = 0; k < len / 2; ++k) {
-                const cplx u = a[i + k], v = a[i + k + len / 2] * w[k];
-                a[i + k] = u + v;
-                a[i + k + len / 2] = u - v;
-            }
-    }
-}
-
-// index t in [0, N) of the odd exponent 2t+1 = 5^j mod 2N (and its conjugate)
-void slot_indices(int N, std::vector<int>& pos, std::vector<int>& neg) {
-    pos.resize(N / 2);
-    neg.resize(N / 2);
-    uint64_t g = 1;
-    for (int j = 0; j < N / 2; ++j) {
-        pos[j] = (int)((g - 1) / 2);
-        neg[j] = (int)((2 * N - g - 1) / 2);
-        g = (g * 5) % (2 * N);
-    }
-}
-
-// real coefficients -> slots
-void embed(int N, const std::vector<long double>& m, double* values, int slots) {
-    std::vector<cplx> A(N);
-    for (int i = 0; i < N; ++i) {
-        const double ang = M_PI * i / N;
-        A[i] = (double)m[i] * cplx(cos(ang), sin(ang));
-    }
-    fft(A, false);  // sum_i a_i w^{t i}
-    std::vector<int> pos, neg;
-    slot_indices(N, pos, neg);
-    for (int k = 0; k < slots; ++k) {
-        values[2 * k] = A[pos[k]].real();
-        values[2 * k + 1] = A[pos[k]].imag();
-    }
-}
-
 fides_status upload_small(fides_ctx* c, const std::vector<int64_t>& v, uint64_t* out, int q0, int nlimbs) {
     int64_t* dv = nullptr;
     if (cudaMallocAsync((void**)&dv, sizeof(int64_t) * c->N, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "small");
@@ -168,6 +134,20 @@ fides_status upload_small(fides_ctx* c, const std::vector<int64_t>& v, uint64_t*
     cudaFreeAsync(dv, c->st);
     return check_cuda(c, "small_to_rns");
 }
+
+// A small polynomial on limbs 0..nlimbs-1 (coefficient form), drawn on the
+// device from the stream word: kind 0 error (Gaussian), 1 ternary.
+void sample_small(fides_ctx* c, int kind, uint64_t stream, uint64_t* out, int nlimbs) {
+    count_launches(1);
+    const int grid = (c->N / 2 + 255) / 256;
+    if (kind == 0)
+        k_sample_small<0><<<grid, 256, 0, c->st>>>(out, c->N, nlimbs, c->dev.pc, stream);
+    else
+        k_sample_small<1><<<grid, 256, 0, c->st>>>(out, c->N, nlimbs, c->dev.pc, stream);
+}
+
+// stream words of the error and ternary draws (tags above any key digit's)
+constexpr uint32_t kTagError = 0xE0, kTagTernary = 0xE1;
 
 // A switching key b = -a sb + e + P sg (per digit), a uniform from the seed.
 // compress: only b is stored; the a half is regenerated from the seed by the
@@ -190,8 +170,7 @@ fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg
         uint64_t* ka = compress ? atmp : key.a + (size_t)d * NP * N;
         count_launches(1);
         k_fill_uniform<<<dim3(N / 256, NP), 256, 0, c->st>>>(ka, N, 0, c->dev.pc, uniform_stream(key.a_seed, d + 1));
-        fides_status s = upload_small(c, gaussian(N, seed ^ (0xABCDull + d)), e, 0, NP);
-        if (s != FIDES_OK) return s;
+        sample_small(c, 0, uniform_stream(seed ^ (0xABCDull + d), kTagError), e, NP);
         ntt_forward(c->dev, map_single(e, e, NP, NP, 0), FL_PLAIN, FS_PLAIN, c->st);
         const int lo = d * c->alpha, hi = std::min(c->L, lo + c->alpha);
         count_launches(1);
@@ -213,17 +192,27 @@ fides_status gen_switch_key(fides_ctx* c, const uint64_t* sb, const uint64_t* sg
 
 // M[bitrev(pos_j)] = z_(j mod slots), M[bitrev(neg_j)] = conj(z): the FFT's
 // input permutation folded into the scatter
-__global__ void k_embed_scatter(const double2* __restrict__ z, int slots, int logN, double2* __restrict__ M) {
-    const int N = 1 << logN;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= N / 2) return;
-    const uint32_t mask = 2u * (uint32_t)N - 1;
-    uint32_t g = 1, b = 5;  // 5^j mod 2N by squaring
-    for (uint32_t e = (uint32_t)j; e; e >>= 1) {
+// 5^j mod 2N by squaring (products in 64 bits: 2N - 1 can exceed 2^16)
+__device__ __forceinline__ uint32_t pow5_mod_2n(uint32_t j, int logN) {
+    const uint32_t mask = (2u << logN) - 1;
+    uint32_t g = 1, b = 5;
+    for (uint32_t e = j; e; e >>= 1) {
         if (e & 1) g = (uint32_t)(((uint64_t)g * b) & mask);
         b = (uint32_t)(((uint64_t)b * b) & mask);
     }
-    const double2 v = z[j & (slots - 1)];
+    return g;
+}
+
+// (slot j of the N/2 takes factor * z[(j - shift) mod slots])
+__global__ void k_embed_scatter(const double2* __restrict__ z, int slots, int shift, double factor, int logN,
+                                double2* __restrict__ M) {
+    const int N = 1 << logN;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N / 2) return;
+    const uint32_t g = pow5_mod_2n((uint32_t)j, logN);
+    double2 v = z[(j - shift) & (slots - 1)];
+    v.x *= factor;
+    v.y *= factor;
     const uint32_t pos = (g - 1) / 2, neg = (2u * (uint32_t)N - g - 1) / 2;
     M[__brev(pos) >> (32 - logN)] = v;
     M[__brev(neg) >> (32 - logN)] = make_double2(v.x, -v.y);
@@ -233,11 +222,12 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(__fma_rn(a.x, b.x, -a.y * b.y), __fma_rn(a.x, b.y, a.y * b.x));
 }
 
-// inverse-FFT butterflies of blocks of length 2^s (a[i] +- w a[i + h],
-// w = exp(-2 pi i k / 2^s)): stages 1..log2(tile) in shared memory, one CTA
-// per tile of 2 blockDim.x <= 2048 elements, then one launch per further stage
+// radix-2 FFT butterflies on bit-reversed input, blocks of length 2^s
+// (a[i] +- w a[i + h], w = exp(dir 2 pi i k / 2^s); dir = -1 for encoding,
+// +1 for decoding): stages 1..log2(tile) in shared memory, one CTA per tile
+// of 2 blockDim.x <= 2048 elements, then one launch per further stage
 constexpr int kFftTile = 2048;
-__global__ void __launch_bounds__(1024) k_fft_tile(double2* __restrict__ M, int s_hi) {
+__global__ void __launch_bounds__(1024) k_fft_tile(double2* __restrict__ M, int s_hi, double dir) {
     __shared__ double2 t[kFftTile];
     const int T = 2 * blockDim.x;
     double2* base = M + (size_t)blockIdx.x * T;
@@ -248,7 +238,7 @@ __global__ void __launch_bounds__(1024) k_fft_tile(double2* __restrict__ M, int 
         const int i = threadIdx.x;  // one butterfly per thread and stage
         const int k = i & (h - 1), a = ((i >> (s - 1)) << s) + k;
         double sn, cs;
-        sincospi(-(double)k / (double)h, &sn, &cs);
+        sincospi(dir * (double)k / (double)h, &sn, &cs);
         const double2 u = t[a], v = cmul(t[a + h], make_double2(cs, sn));
         t[a] = make_double2(u.x + v.x, u.y + v.y);
         t[a + h] = make_double2(u.x - v.x, u.y - v.y);
@@ -257,13 +247,13 @@ __global__ void __launch_bounds__(1024) k_fft_tile(double2* __restrict__ M, int 
     for (int i = threadIdx.x; i < T; i += blockDim.x) base[i] = t[i];
 }
 
-__global__ void k_fft_stage(double2* __restrict__ M, int s, int N) {
+__global__ void k_fft_stage(double2* __restrict__ M, int s, int N, double dir) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N / 2) return;
     const int h = 1 << (s - 1);
     const int k = i & (h - 1), a = ((i >> (s - 1)) << s) + k;
     double sn, cs;
-    sincospi(-(double)k / (double)h, &sn, &cs);
+    sincospi(dir * (double)k / (double)h, &sn, &cs);
     const double2 u = M[a], v = cmul(M[a + h], make_double2(cs, sn));
     M[a] = make_double2(u.x + v.x, u.y + v.y);
     M[a + h] = make_double2(u.x - v.x, u.y - v.y);
@@ -287,40 +277,104 @@ __global__ void k_embed_round(const double2* __restrict__ M, int N, double scale
     v[t] = llround(x);
 }
 
-fides_status fides::encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm) {
+// the FFT of length N on M (bit-reversed input, natural-order output)
+static void fft_dev(fides_ctx* c, double2* M, double dir) {
+    const int N = c->N, logN = c->logN;
+    const int s_tile = std::min(logN, 11);  // tiles of 2^s_tile <= kFftTile elements
+    count_launches(1 + logN - s_tile);
+    k_fft_tile<<<N >> s_tile, (1 << s_tile) / 2, 0, c->st>>>(M, s_tile, dir);
+    for (int s = s_tile + 1; s <= logN; ++s) k_fft_stage<<<(N / 2 + 255) / 256, 256, 0, c->st>>>(M, s, N, dir);
+}
+
+fides_status fides::encode_dev_z(fides_ctx* c, const double2* z, int slots, int shift, double factor, int level,
+                                 double scale, uint64_t* dm, int* bad) {
     const int N = c->N, logN = c->logN;
     if (slots < 1 || slots > N / 2 || (slots & (slots - 1))) return set_err(c, FIDES_BAD_ARG, "encode: slots");
-    // scratch: N complex (FFT), slots complex (input), N int64, one flag
+    // scratch: N complex (FFT), N int64
     char* buf = nullptr;
-    const size_t b_m = (size_t)N * 16, b_z = (size_t)slots * 16, b_v = (size_t)N * 8;
-    if (cudaMallocAsync((void**)&buf, b_m + b_z + b_v + 16, c->st) != cudaSuccess) {
+    const size_t b_m = (size_t)N * 16, b_v = (size_t)N * 8;
+    if (cudaMallocAsync((void**)&buf, b_m + b_v, c->st) != cudaSuccess) {
         cudaGetLastError();
         return set_err(c, FIDES_OOM, "encode scratch");
     }
     double2* M = (double2*)buf;
-    double2* z = (double2*)(buf + b_m);
-    int64_t* v = (int64_t*)(buf + b_m + b_z);
-    int* bad = (int*)(buf + b_m + b_z + b_v);
+    int64_t* v = (int64_t*)(buf + b_m);
+    count_launches(3);
+    k_embed_scatter<<<(N / 2 + 255) / 256, 256, 0, c->st>>>(z, slots, shift & (slots - 1), factor, logN, M);
+    fft_dev(c, M, -1.0);
+    k_embed_round<<<(N + 255) / 256, 256, 0, c->st>>>(M, N, scale, v, bad);
+    k_small_to_rns<<<dim3(N / 256, level + 1), 256, 0, c->st>>>(v, dm, N, 0, c->dev.pc);
+    cudaFreeAsync(buf, c->st);
+    ntt_forward(c->dev, map_single(dm, dm, level + 1, level + 1, 0), FL_PLAIN, FS_PLAIN, c->st);
+    return FIDES_OK;
+}
+
+fides_status fides::encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm) {
+    if (slots < 1 || slots > c->N / 2 || (slots & (slots - 1))) return set_err(c, FIDES_BAD_ARG, "encode: slots");
+    // slots complex (input) and one flag
+    char* buf = nullptr;
+    const size_t b_z = (size_t)slots * 16;
+    if (cudaMallocAsync((void**)&buf, b_z + 16, c->st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FIDES_OOM, "encode scratch");
+    }
+    double2* z = (double2*)buf;
+    int* bad = (int*)(buf + b_z);
     cudaMemcpyAsync(z, values, b_z, cudaMemcpyHostToDevice, c->st);
     cudaMemsetAsync(bad, 0, sizeof(int), c->st);
-    count_launches(3);
-    k_embed_scatter<<<(N / 2 + 255) / 256, 256, 0, c->st>>>(z, slots, logN, M);
-    const int s_tile = std::min(logN, 11);  // tiles of 2^s_tile <= kFftTile elements
-    k_fft_tile<<<N >> s_tile, (1 << s_tile) / 2, 0, c->st>>>(M, s_tile);
-    for (int s = s_tile + 1; s <= logN; ++s) {
-        count_launches(1);
-        k_fft_stage<<<(N / 2 + 255) / 256, 256, 0, c->st>>>(M, s, N);
-    }
-    k_embed_round<<<(N + 255) / 256, 256, 0, c->st>>>(M, N, scale, v, bad);
-    count_launches(1);
-    k_small_to_rns<<<dim3(N / 256, level + 1), 256, 0, c->st>>>(v, dm, N, 0, c->dev.pc);
+    fides_status s = encode_dev_z(c, z, slots, 0, 1.0, level, scale, dm, bad);
     int hbad = 0;
-    cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->st);
+    if (s == FIDES_OK) cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->st);
     cudaFreeAsync(buf, c->st);
     cudaStreamSynchronize(c->st);
+    if (s != FIDES_OK) return s;
     if (hbad) return set_err(c, FIDES_BAD_ARG, "encoded coefficient exceeds 2^63");
-    ntt_forward(c->dev, map_single(dm, dm, level + 1, level + 1, 0), FL_PLAIN, FS_PLAIN, c->st);
     return check_cuda(c, "encode");
+}
+
+// ---- decoding on the device ----
+// The canonical embedding itself: the centred integer coefficients (a
+// mixed-radix CRT of the first `use` <= 3 moduli, converted to FP64 and
+// divided by the scale), twisted by exp(i pi t / N), then a forward complex
+// FFT of length N; slot j reads the transform at the index t of the root
+// zeta^(5^j), t = (5^j - 1) / 2.
+struct CrtConst {
+    uint64_t q[3];
+    uint64_t inv01, inv02, inv12;  // q0^-1 mod q1, q0^-1 mod q2, q1^-1 mod q2
+    int use;
+};
+
+// M[bitrev(t)] = x_t exp(i pi t / N), x_t the centred value of coefficient t
+// over q0..q_{use-1} divided by scale; the FFT's input permutation folded in
+__global__ void k_decode_crt(const uint64_t* __restrict__ m, int logN, CrtConst k, const PrimeConst* __restrict__ pcs,
+                             double scale, double2* __restrict__ M) {
+    const int N = 1 << logN;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N) return;
+    uint64_t v[3] = {m[t], 0, 0};
+    if (k.use > 1) v[1] = mul_mod(sub_mod(m[N + t], v[0] % k.q[1], k.q[1]), k.inv01, pcs[1]);
+    if (k.use > 2) {
+        const uint64_t u = mul_mod(sub_mod(m[2 * N + t], v[0] % k.q[2], k.q[2]), k.inv02, pcs[2]);
+        v[2] = mul_mod(sub_mod(u, v[1] % k.q[2], k.q[2]), k.inv12, pcs[2]);
+    }
+    // the value is v0 + q0 (v1 + q1 v2); above half the product it stands
+    // for a negative one, -(1 + sum (q_i - 1 - v_i) prod_{j<i} q_j)
+    const bool neg = v[k.use - 1] > k.q[k.use - 1] / 2;
+    double x = 0;
+    for (int i = k.use - 1; i >= 0; --i) {
+        const uint64_t d = neg ? k.q[i] - 1 - v[i] : v[i];
+        x = i == k.use - 1 ? (double)d : __fma_rn(x, (double)k.q[i], (double)d);
+    }
+    x = (neg ? -(x + 1.0) : x) / scale;
+    double sn, cs;
+    sincospi((double)t / (double)N, &sn, &cs);
+    M[__brev((uint32_t)t) >> (32 - logN)] = make_double2(x * cs, x * sn);
+}
+
+__global__ void k_decode_gather(const double2* __restrict__ M, int slots, int logN, double2* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= slots) return;
+    out[j] = M[(pow5_mod_2n((uint32_t)j, logN) - 1) / 2];
 }
 
 extern "C" {
@@ -537,8 +591,8 @@ fides_status fides_encrypt(fides_ctx* c, const fides_sk* sk, const double* value
     cudaMallocAsync((void**)&m, (size_t)n * N * 8, c->st);
     cudaMallocAsync((void**)&e, (size_t)n * N * 8, c->st);
     s = encode_dev(c, values, slots, level, scale, m);
-    if (s == FIDES_OK) s = upload_small(c, gaussian(N, seed ^ 0x5EED), e, 0, n);
     if (s == FIDES_OK) {
+        sample_small(c, 0, uniform_stream(seed ^ 0x5EED, kTagError), e, n);
         ntt_forward(c->dev, map_single(e, e, n, n, 0), FL_PLAIN, FS_PLAIN, c->st);
         count_launches(1);
         k_fill_uniform<<<dim3(N / 256, n), 256, 0, c->st>>>(ct->c1(N), N, 0, c->dev.pc, uniform_stream(seed * 2654435761ull + 17, 0));
@@ -580,22 +634,21 @@ fides_status fides_keygen_public(fides_ctx* c, const fides_sk* sk, uint64_t seed
     if (cudaMallocAsync((void**)&e, (size_t)L * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "pk tmp");
     count_launches(1);
     k_fill_uniform<<<dim3(N / 256, L), 256, 0, c->st>>>(pk->a, N, 0, c->dev.pc, uniform_stream(seed * 0x9E3779B97F4A7C15ull + 99, 0));
-    fides_status s = upload_small(c, gaussian(N, seed ^ 0x7EA5), e, 0, L);
-    if (s == FIDES_OK) {
-        ntt_forward(c->dev, map_single(e, e, L, L, 0), FL_PLAIN, FS_PLAIN, c->st);
-        count_launches(1);
-        k_key_combine<<<dim3(N / 256, L), 256, 0, c->st>>>(pk->b, pk->a, sk->s, e, sk->s, c->dev.pc, c->dev.md_pmod, N,
-                                                           0, 0);
-        cudaStreamSynchronize(c->st);
-    }
+    sample_small(c, 0, uniform_stream(seed ^ 0x7EA5, kTagError), e, L);
+    ntt_forward(c->dev, map_single(e, e, L, L, 0), FL_PLAIN, FS_PLAIN, c->st);
+    count_launches(1);
+    k_key_combine<<<dim3(N / 256, L), 256, 0, c->st>>>(pk->b, pk->a, sk->s, e, sk->s, c->dev.pc, c->dev.md_pmod, N, 0,
+                                                       0);
     cudaFreeAsync(e, c->st);
+    cudaStreamSynchronize(c->st);
+    fides_status s = check_cuda(c, "public key");
     if (s != FIDES_OK) {
         cudaFree(pk->b);
         delete pk;
         return s;
     }
     *out = pk;
-    return check_cuda(c, "public key");
+    return FIDES_OK;
 }
 
 fides_status fides_pk_free(fides_ctx* c, fides_pk* pk) {
@@ -629,15 +682,10 @@ fides_status fides_encrypt_pk(fides_ctx* c, const fides_pk* pk, const double* va
     }
     uint64_t *m = tmp, *v = tmp + (size_t)n * N, *e0 = tmp + 2 * (size_t)n * N, *e1 = tmp + 3 * (size_t)n * N;
     s = encode_dev(c, values, slots, level, scale, m);
-    std::vector<int64_t> vt(N);
-    {
-        Xoshiro r(seed ^ 0xC0FFEE);
-        for (int i = 0; i < N; ++i) vt[i] = (int64_t)(r.next() % 3) - 1;
-    }
-    if (s == FIDES_OK) s = upload_small(c, vt, v, 0, n);
-    if (s == FIDES_OK) s = upload_small(c, gaussian(N, seed ^ 0xE0), e0, 0, n);
-    if (s == FIDES_OK) s = upload_small(c, gaussian(N, seed ^ 0xE1), e1, 0, n);
     if (s == FIDES_OK) {
+        sample_small(c, 1, uniform_stream(seed ^ 0xC0FFEE, kTagTernary), v, n);
+        sample_small(c, 0, uniform_stream(seed ^ 0xE0, kTagError), e0, n);
+        sample_small(c, 0, uniform_stream(seed ^ 0xE1, kTagError), e1, n);
         LimbMap mm{};
         mm.nseg = 3;
         uint64_t* bufs[3] = {v, e0, e1};
@@ -700,43 +748,36 @@ fides_status fides_decrypt(fides_ctx* c, const fides_sk* sk, const fides_ct* ct,
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     cudaSetDevice(c->device);
     const int n = ct->level + 1, N = c->N;
-    uint64_t* m = nullptr;
-    if (cudaMallocAsync((void**)&m, (size_t)n * N * 8, c->st) != cudaSuccess) return set_err(c, FIDES_OOM, "decrypt");
+    // scratch: the n limbs of c0 + c1 s, N complex (FFT), slots complex (output)
+    char* buf = nullptr;
+    const size_t b_m = (size_t)n * N * 8, b_f = (size_t)N * 16, b_o = (size_t)slots * 16;
+    if (cudaMallocAsync((void**)&buf, b_m + b_f + b_o, c->st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FIDES_OOM, "decrypt");
+    }
+    uint64_t* m = (uint64_t*)buf;
+    double2* M = (double2*)(buf + b_m);
+    double2* o = (double2*)(buf + b_m + b_f);
     launch_elementwise(c->dev, EW_MUL, n, 0, ct->c1(N), sk->s, m, c->st);
     launch_elementwise(c->dev, EW_ADD, n, 0, m, ct->c0(), m, c->st);
     ntt_inverse(c->dev, map_single(m, m, n, n, 0), IL_PLAIN, IS_PLAIN, c->st);
-    const int use = std::min(n, 3);
-    std::vector<uint64_t> h((size_t)use * N);
-    cudaMemcpyAsync(h.data(), m, (size_t)use * N * 8, cudaMemcpyDeviceToHost, c->st);
-    cudaStreamSynchronize(c->st);
-    cudaFreeAsync(m, c->st);
-    fides_status s = check_cuda(c, "decrypt");
-    if (s != FIDES_OK) return s;
-    // mixed-radix CRT over q0..q_{use-1}, centred
+    CrtConst k{};
+    k.use = std::min(n, 3);
     const uint64_t* q = c->host.prime.data();
-    std::vector<long double> coef(N);
-    uint64_t inv01 = use > 1 ? invmod(q[0] % q[1], q[1]) : 0;
-    uint64_t inv02 = use > 2 ? invmod(q[0] % q[2], q[2]) : 0;
-    uint64_t inv12 = use > 2 ? invmod(q[1] % q[2], q[2]) : 0;
-    for (int i = 0; i < N; ++i) {
-        uint64_t v[3] = {h[i], 0, 0};
-        if (use > 1) v[1] = mulmod(sub_mod(h[(size_t)N + i], v[0] % q[1], q[1]), inv01, q[1]);
-        if (use > 2) {
-            uint64_t t = mulmod(sub_mod(h[(size_t)2 * N + i], v[0] % q[2], q[2]), inv02, q[2]);
-            v[2] = mulmod(sub_mod(t, v[1] % q[2], q[2]), inv12, q[2]);
-        }
-        const bool negv = v[use - 1] > q[use - 1] / 2;
-        long double acc = 0, w = 1;
-        for (int k = 0; k < use; ++k) {
-            const uint64_t dk = negv ? q[k] - 1 - v[k] : v[k];
-            acc += (long double)dk * w;
-            w *= (long double)q[k];
-        }
-        coef[i] = negv ? -(acc + 1) : acc;
-        coef[i] /= (long double)ct->scale;
+    for (int i = 0; i < k.use; ++i) k.q[i] = q[i];
+    if (k.use > 1) k.inv01 = invmod(q[0] % q[1], q[1]);
+    if (k.use > 2) {
+        k.inv02 = invmod(q[0] % q[2], q[2]);
+        k.inv12 = invmod(q[1] % q[2], q[2]);
     }
-    embed(N, coef, values, slots);
-    return FIDES_OK;
+    count_launches(2);
+    k_decode_crt<<<(N + 255) / 256, 256, 0, c->st>>>(m, c->logN, k, c->dev.pc, ct->scale, M);
+    fft_dev(c, M, 1.0);
+    k_decode_gather<<<(slots + 255) / 256, 256, 0, c->st>>>(M, slots, c->logN, o);
+    cudaMemcpyAsync(values, o, b_o, cudaMemcpyDeviceToHost, c->st);
+    cudaFreeAsync(buf, c->st);
+    cudaStreamSynchronize(c->st);
+    return check_cuda(c, "decrypt");
 }
 
 }  // extern "C"

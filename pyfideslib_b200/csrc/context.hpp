@@ -138,6 +138,11 @@ fides_status consume_device_error(fides_ctx* c, cudaStream_t st = nullptr);
 // Canonical-embedding encode of `slots` complex values (interleaved re, im)
 // at `scale` into level+1 evaluation limbs at dm (device), on the context stream.
 fides_status encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm);
+// Encoding of slot values already in HBM (z: `slots` complex), slot j taking
+// factor * z[(j - shift) mod slots]: queued on the context stream, no
+// synchronisation; a coefficient at or above 2^63 sets the device word *bad.
+fides_status encode_dev_z(fides_ctx* c, const double2* z, int slots, int shift, double factor, int level,
+                          double scale, uint64_t* dm, int* bad);
 // Per-limb integer constant z mod q_j with its Shoup companion, z of any sign.
 void int_const_limbs(const fides_ctx* c, int64_t z, int nlimbs, uint64_t (*out)[2]);
 // Output buffer of `level`+1 limbs per component, stream-ordered on `st`
