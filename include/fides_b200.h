@@ -56,6 +56,16 @@ typedef struct {
     int p_bits;
     int device;           /* CUDA device ordinal */
     double default_scale; /* encoding scale, default 2^qi_bits */
+    /* optional primitive 2N-th roots of unity psi, one per modulus (num_q and
+     * num_p entries), that fix the evaluation representation: OpenFHE's own
+     * roots, as RawParams carries them (root_of_unity / SPECIALroot_of_unity,
+     * src/CKKS/openfhe-interface/RawCiphertext.cu:235,306) and SetupConstants
+     * takes them (src/ConstantsGPU.cu:195-199).  NULL: psi = g^((p-1)/2N) with
+     * g the smallest generator, FIDESlib's rule without OpenFHE
+     * (unity_root, src/ConstantsGPU.cu:61).  A value with psi^N != -1 mod p
+     * is refused. */
+    const uint64_t* q_root;
+    const uint64_t* p_root;
 } fides_params;
 
 /* ---- context (replaces CKKS::GenCryptoContextGPU / ContextData ctor,

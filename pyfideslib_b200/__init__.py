@@ -148,13 +148,20 @@ class CryptoContext:
     """Mirror of fideslib::CryptoContextImpl<DCRTPoly> (api/CryptoContext.hpp:24-245)."""
 
     def __init__(self, log_n=16, num_q=30, dnum=3, num_p=0, q=None, p=None, q0_bits=60, qi_bits=50, p_bits=60,
-                 device=0, scale=None):
+                 device=0, scale=None, q_root=None, p_root=None):
+        """q_root / p_root: the primitive 2N-th roots of unity that fix the
+        evaluation representation (OpenFHE's RawParams root_of_unity /
+        SPECIALroot_of_unity); None for FIDESlib's smallest-generator rule."""
         prm = FidesParams()
         prm.log_n, prm.num_q, prm.num_p, prm.dnum = log_n, num_q, num_p, dnum
         self._qa = np.ascontiguousarray(q, dtype=np.uint64) if q is not None else None
         self._pa = np.ascontiguousarray(p, dtype=np.uint64) if p is not None else None
+        self._qr = np.ascontiguousarray(q_root, dtype=np.uint64) if q_root is not None else None
+        self._pr = np.ascontiguousarray(p_root, dtype=np.uint64) if p_root is not None else None
         prm.q = _p(self._qa)
         prm.p = _p(self._pa)
+        prm.q_root = _p(self._qr)
+        prm.p_root = _p(self._pr)
         if self._pa is not None:
             prm.num_p = len(self._pa)
         prm.q0_bits, prm.qi_bits, prm.p_bits = q0_bits, qi_bits, p_bits

@@ -34,7 +34,7 @@ class SrvStats(C.Structure):
 class FidesParams(C.Structure):
     _fields_ = [("log_n", C.c_int), ("num_q", C.c_int), ("num_p", C.c_int), ("dnum", C.c_int),
                 ("q", u64p), ("p", u64p), ("q0_bits", C.c_int), ("qi_bits", C.c_int), ("p_bits", C.c_int),
-                ("device", C.c_int), ("default_scale", C.c_double)]
+                ("device", C.c_int), ("default_scale", C.c_double), ("q_root", u64p), ("p_root", u64p)]
 
 
 class BootParams(C.Structure):

@@ -65,6 +65,16 @@ struct RawPlainText {
     int slots = 0;
     int NoiseLevel = 1;
 };
+// The part of the reference's RawParams (src/CKKS/openfhe-interface/
+// RawCiphertext.cuh:50-88) a context is built from when OpenFHE supplies it:
+// the moduli and the 2N-th roots of unity that fix OpenFHE's evaluation
+// representation (SetupConstants takes them, src/ConstantsGPU.cu:195-199).
+// L counts the levels: moduli holds L + 1 entries.
+struct RawParams {
+    int N = 0, L = 0, K = 0, logN = 0, dnum = 0;
+    std::vector<uint64_t> moduli, root_of_unity, SPECIALmoduli, SPECIALroot_of_unity;
+};
+
 // r_key[h][d][i]: half h (0 = a, 1 = b), digit d, limb i; r_key_moduli alike
 struct RawKeySwitchKey {
     std::vector<std::vector<std::vector<uint64_t>>> r_key_moduli;
@@ -214,6 +224,29 @@ class CryptoContextImpl<DCRTPoly> {
         prm.q0_bits = (int)p.firstBits;
         prm.qi_bits = (int)p.scaleBits;
         prm.p_bits = 60;
+        prm.device = p.devices.empty() ? 0 : p.devices[0];
+        check(fides_ctx_create(&prm, &ctx));
+        slots = p.batch ? p.batch : (1u << prm.log_n) / 2;
+        sparse = p.keyDist == SPARSE_TERNARY;
+    }
+    // A context over OpenFHE's moduli and roots (the reference builds its
+    // CKKS::Context from RawParams the same way, src/CKKS/Context.cu:37-98),
+    // so that raw ciphertexts and keys in EVALUATION format load unchanged.
+    CryptoContextImpl(const CCParams<CryptoContextCKKSRNS>& p, const RawParams& raw)
+        : tech(p.tech), hamming(p.hamming) {
+        if (raw.moduli.empty() || raw.root_of_unity.size() != raw.moduli.size() ||
+            raw.SPECIALroot_of_unity.size() != raw.SPECIALmoduli.size())
+            throw Exception(FIDES_BAD_ARG, "RawParams: moduli and roots of unity differ in count");
+        fides_params prm{};
+        prm.log_n = raw.logN;
+        prm.num_q = (int)raw.moduli.size();
+        prm.num_p = (int)raw.SPECIALmoduli.size();
+        prm.dnum = raw.dnum > 0 ? raw.dnum : (int)p.dnum;
+        prm.q = raw.moduli.data();
+        prm.p = raw.SPECIALmoduli.empty() ? nullptr : raw.SPECIALmoduli.data();
+        prm.q_root = raw.root_of_unity.data();
+        prm.p_root = raw.SPECIALroot_of_unity.empty() ? nullptr : raw.SPECIALroot_of_unity.data();
+        prm.qi_bits = (int)p.scaleBits;
         prm.device = p.devices.empty() ? 0 : p.devices[0];
         check(fides_ctx_create(&prm, &ctx));
         slots = p.batch ? p.batch : (1u << prm.log_n) / 2;
@@ -731,6 +764,10 @@ using CryptoContext = std::shared_ptr<CryptoContextImpl<DCRTPoly>>;
 
 inline CryptoContext<DCRTPoly> GenCryptoContext(const CCParams<CryptoContextCKKSRNS>& p) {
     return std::make_shared<CryptoContextImpl<DCRTPoly>>(p);
+}
+// over the moduli and roots of an OpenFHE context (RawParams from GetRawParams)
+inline CryptoContext<DCRTPoly> GenCryptoContext(const CCParams<CryptoContextCKKSRNS>& p, const RawParams& raw) {
+    return std::make_shared<CryptoContextImpl<DCRTPoly>>(p, raw);
 }
 
 }  // namespace fideslib

@@ -323,8 +323,18 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
         k.r64_sh = shoup_precompute(k.r64, pr);
         k.ninv = invmod((uint64_t)N % pr, pr);
         k.ninv_sh = shoup_precompute(k.ninv, pr);
-        const uint64_t g = smallest_generator(pr);
-        const uint64_t psi = powmod(g, (pr - 1) / (2ull * N), pr);
+        const uint64_t* given = i < L ? prm->q_root : prm->p_root;
+        uint64_t psi = 0;
+        if (given) {
+            psi = given[i < L ? i : i - L];
+            // a primitive 2N-th root: psi^N = -1 (its order divides 2N, not N)
+            if (psi == 0 || psi >= pr || powmod(psi, (uint64_t)N, pr) != pr - 1) {
+                c->host.root[i] = 0;
+                return;
+            }
+        } else {
+            psi = powmod(smallest_generator(pr), (pr - 1) / (2ull * N), pr);
+        }
         const uint64_t ipsi = invmod(psi, pr);
         c->host.root[i] = psi;
         std::vector<uint64_t> a(N), b(N);
@@ -367,7 +377,9 @@ fides_status build_context(fides_ctx* c, const fides_params* prm) {
         for (auto& x : th) x.join();
     }
     for (int i = 0; i < NP; ++i)
-        if (c->host.root[i] == 0) return set_err(c, FIDES_BAD_ARG, "no primitive root");
+        if (c->host.root[i] == 0)
+            return set_err(c, FIDES_BAD_ARG, "modulus " + std::to_string(c->host.prime[i]) +
+                                                 ": no primitive 2N-th root (or the given one is not)");
 
     // ---- CRT tables ----
     auto P = [&](int i) { return c->host.prime[i]; };
