@@ -339,6 +339,19 @@ def measure_bootstrap(cc, reps=3, seed=101, degree=119):
     ms = e0.elapsed_time(e1) / reps
     got = cc.Decrypt(sk, bt, slots=slots)
     err = float(np.max(np.abs(got - msgs[(reps - 1) % 2])))
+    # the same with one ModDown per giant-step rotation in the transforms
+    # (fides_set_giant_step_moddown scope 0) instead of one per input
+    from pyfideslib_b200._capi import lib
+    lib.fides_set_giant_step_moddown(cc._h, 0)
+    cc.EvalBootstrap(cts[0])
+    cc.Synchronize()
+    e0.record(st)
+    for r in range(reps):
+        cc.EvalBootstrap(cts[r % 2])
+    e1.record(st)
+    e1.synchronize()
+    ms_per_rot = e0.elapsed_time(e1) / reps
+    lib.fides_set_giant_step_moddown(cc._h, 1)
     # the same with the message scaled by 2^6 through EvalMod (correction
     # factor; valid for these messages, whose coefficients are below 2^-5)
     cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=degree, correction=6)
@@ -386,7 +399,8 @@ def measure_bootstrap(cc, reps=3, seed=101, degree=119):
               "decrypt_ms": wall(lambda: cc.Decrypt(sk, top, slots=slots)),
               "level": top.level, "slots": slots}
     del top
-    res = {"bootstrap_ms": ms, "wall_ms": wall_ms, "client": client, "precision_bits": -float(np.log2(err)), "max_abs_err": err,
+    res = {"bootstrap_ms": ms, "wall_ms": wall_ms, "client": client,
+           "bootstrap_ms_moddown_per_giant_rotation": ms_per_rot, "precision_bits": -float(np.log2(err)), "max_abs_err": err,
            "precision_bits_correction6": -float(np.log2(err6)),
            "two_iterations": {"ms": ms2, "precision_bits": -float(np.log2(err2)), "input_level": out_level,
                               "output_level": out_level - 1},

@@ -120,6 +120,16 @@ fides_status fides_set_conv_accumulator(fides_ctx* ctx, int accumulator);
  * per SM and the special-prime outputs at 2 (forward NTT variant 9 only).
  * Default 13 (FP64 sums, fused for batches of 8+, split launch). */
 fides_status fides_set_keyswitch_variant(fides_ctx* ctx, int variant);
+/* Giant steps of the baby-step giant-step linear transforms: each input's
+ * giant-step rotations are added in the extended basis (Q and the special
+ * moduli) and brought down by one ModDown, instead of one ModDown per
+ * rotation.  The two agree up to the rounding of the division by P.  scope 0:
+ * never; 1 (default): in the bootstrap's CoeffsToSlots / SlotsToCoeffs;
+ * 2: also in fides_linear_transform(_batch), whose default results are bit
+ * for bit those of composing rotations, products and additions.  The
+ * reference hoists the ModDown of its baby steps instead (MODDOWN_HOIST,
+ * src/CKKS/LinearTransform.cu:111-190). */
+fides_status fides_set_giant_step_moddown(fides_ctx* ctx, int scope);
 /* Device error word of this context, read after the work queued so far
  * without clearing it: bit 0 is set once a tensor-core conversion gave up its
  * bounded wait for its matrix products (its outputs are then invalid).  The

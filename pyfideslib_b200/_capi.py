@@ -82,6 +82,7 @@ EXPORTS = {
     "fides_ctx_device_status": ([vp, C.POINTER(C.c_uint32)], C.c_int),
     "fides_ctx_inject_device_error": ([vp, C.c_uint32], C.c_int),
     "fides_set_keyswitch_variant": ([vp, C.c_int], C.c_int),
+    "fides_set_giant_step_moddown": ([vp, C.c_int], C.c_int),
     "fides_set_ntt_variant": ([vp, C.c_int], C.c_int),
     "fides_key_upload_relin": ([vp, u64p, u64p], C.c_int),
     "fides_key_upload_galois": ([vp, C.c_uint32, u64p, u64p], C.c_int),

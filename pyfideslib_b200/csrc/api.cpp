@@ -307,6 +307,13 @@ fides_status fides_ctx_inject_device_error(fides_ctx* ctx, uint32_t flags) {
     return check_cuda(ctx, "inject device error");
 }
 
+fides_status fides_set_giant_step_moddown(fides_ctx* c, int scope) {
+    if (!c || scope < 0 || scope > 2) return FIDES_BAD_ARG;
+    Guard g(c);
+    c->giant_moddown = scope;
+    return FIDES_OK;
+}
+
 fides_status fides_set_keyswitch_variant(fides_ctx* c, int variant) {
     if (!c || variant < 0 || variant > 15) return FIDES_BAD_ARG;
     Guard g(c);
@@ -1165,12 +1172,104 @@ fides_status fides_linear_transform(fides_ctx* c, const fides_ct* x, int n, cons
     return fides_linear_transform_batch(c, 1, &x, n, offsets, pts, bstep, rescale, &out);
 }
 
-// The same transform of nx ciphertexts at one level: the baby steps are one
-// hoisted rotation group per input, the giant rotations of every input form
-// one batched key switch (nx times the elements per launch).
 fides_status fides_linear_transform_batch(fides_ctx* c, int nx, const fides_ct* const* xs, int n,
                                           const int32_t* offsets, const fides_pt* const* pts, int bstep, int rescale,
                                           fides_ct* const* outs) {
+    return linear_transform_batch(c, nx, xs, n, offsets, pts, bstep, rescale, outs, false);
+}
+
+}  // extern "C"
+
+namespace {
+// The giant-step rotations of the transform's inputs with one ModDown per
+// input (eng_rotate_sum): inner[i] belongs to input owner[i] (runs of equal
+// owners) and rotates by gidx[i]; each input's rotated sum is added to
+// acc[owner] (copied when have_acc is 0).
+fides_status giant_rotate_sum(fides_ctx* c, int level, const std::vector<const fides_ct*>& inner,
+                              const std::vector<int32_t>& gidx, const std::vector<int>& owner,
+                              std::vector<fides_ct*>& acc, std::vector<char>& have_acc, CtTemps& tmp) {
+    const int N = c->N, nl = level + 1;
+    const size_t bytes = (size_t)nl * c->limb_bytes();
+    auto add_into = [&](int u, const fides_ct* r) -> fides_status {
+        fides_ct* a = acc[u];
+        if (!have_acc[u]) {
+            fides_status s = ct_reserve(c, a, level);
+            if (s != FIDES_OK) return s;
+            cudaMemcpyAsync(a->c0(), r->c0(), bytes, cudaMemcpyDeviceToDevice, c->st);
+            cudaMemcpyAsync(a->c1(N), r->c1(N), bytes, cudaMemcpyDeviceToDevice, c->st);
+            have_acc[u] = 1;
+            return FIDES_OK;
+        }
+        launch_elementwise(c->dev, EW_ADD, nl, 0, a->c0(), r->c0(), a->c0(), c->st);
+        launch_elementwise(c->dev, EW_ADD, nl, 0, a->c1(N), r->c1(N), a->c1(N), c->st);
+        return FIDES_OK;
+    };
+    std::vector<int> terms;  // rotations that need a key switch, in owner order
+    std::vector<uint32_t> gal(inner.size());
+    std::vector<const SwitchKey*> keys(inner.size(), nullptr);
+    for (size_t i = 0; i < inner.size(); ++i) {
+        gal[i] = fides_rotation_galois(c, gidx[i], inner[i]->slots > 0 ? inner[i]->slots : N / 2);
+        if (gal[i] == 1) {  // a rotation by a multiple of the slot count
+            fides_status s = add_into(owner[i], inner[i]);
+            if (s != FIDES_OK) return s;
+            continue;
+        }
+        auto it = c->galois_keys.find(gal[i]);
+        if (it == c->galois_keys.end())
+            return set_err(c, FIDES_KEY_MISSING, "no key for galois element " + std::to_string(gal[i]));
+        keys[i] = &it->second;
+        terms.push_back((int)i);
+    }
+    if (terms.empty()) return FIDES_OK;
+    fides_status s = ws_reserve(c, c->wsb, std::min((int)terms.size(), kMaxBatch));
+    if (s != FIDES_OK) return s;
+    for (size_t k0 = 0; k0 < terms.size(); k0 += c->wsb.cap) {
+        const int nb = (int)std::min(terms.size() - k0, (size_t)c->wsb.cap);
+        std::vector<const uint64_t*> c0(nb), c1(nb);
+        std::vector<const SwitchKey*> kk(nb);
+        std::vector<uint32_t> gg(nb);
+        std::vector<int> start, runs;  // run r: elements start[r] .. start[r+1]-1 of input runs[r]
+        for (int j = 0; j < nb; ++j) {
+            const int i = terms[k0 + j];
+            c0[j] = inner[i]->c0();
+            c1[j] = inner[i]->c1(N);
+            kk[j] = keys[i];
+            gg[j] = gal[i];
+            if (j == 0 || owner[i] != runs.back()) {
+                start.push_back(j);
+                runs.push_back(owner[i]);
+            }
+        }
+        start.push_back(nb);
+        const int nout = (int)runs.size();
+        std::vector<fides_ct*> r(nout);
+        std::vector<uint64_t*> o0(nout), o1(nout);
+        for (int u = 0; u < nout; ++u) {
+            r[u] = tmp.make();
+            s = ct_reserve(c, r[u], level);
+            if (s != FIDES_OK) return s;
+            o0[u] = r[u]->c0();
+            o1[u] = r[u]->c1(N);
+        }
+        eng_rotate_sum(c, c->wsb, level, nb, c0.data(), c1.data(), kk.data(), gg.data(), nout, start.data(),
+                       o0.data(), o1.data());
+        for (int u = 0; u < nout; ++u) {
+            s = add_into(runs[u], r[u]);
+            if (s != FIDES_OK) return s;
+        }
+    }
+    return FIDES_OK;
+}
+}  // namespace
+
+// The same transform of nx ciphertexts at one level: the baby steps are one
+// hoisted rotation group per input, the giant rotations of every input form
+// one batched key switch (nx times the elements per launch), with one
+// ModDown per rotation or, when `boot` and the context's giant_moddown
+// select it, one per input.
+fides_status fides::linear_transform_batch(fides_ctx* c, int nx, const fides_ct* const* xs, int n,
+                                           const int32_t* offsets, const fides_pt* const* pts, int bstep,
+                                           int rescale, fides_ct* const* outs, bool boot) {
     if (!c || nx < 1 || !xs || !outs || n < 1 || !offsets || !pts || bstep < 1) return FIDES_BAD_ARG;
     for (int u = 0; u < nx; ++u)
         if (!valid_ct(c, xs[u]) || !outs[u] || xs[u]->level != xs[0]->level) return FIDES_BAD_ARG;
@@ -1252,7 +1351,10 @@ fides_status fides_linear_transform_batch(fides_ctx* c, int nx, const fides_ct* 
             }
         }
     }
-    if (!inner.empty()) {
+    if (!inner.empty() && (c->giant_moddown == 2 || (c->giant_moddown == 1 && boot))) {
+        s = giant_rotate_sum(c, level, inner, gidx, owner, acc, have_acc, tmp);
+        if (s != FIDES_OK) return s;
+    } else if (!inner.empty()) {
         std::vector<fides_ct*> rot;
         for (size_t i = 0; i < inner.size(); ++i) rot.push_back(tmp.make());
         s = fides_rotate_batch(c, (int)inner.size(), inner.data(), gidx.data(), rot.data());
@@ -1287,6 +1389,8 @@ fides_status fides_linear_transform_batch(fides_ctx* c, int nx, const fides_ct* 
     }
     return check_cuda(c, "linear_transform");
 }
+
+extern "C" {
 
 }  // extern "C"
 

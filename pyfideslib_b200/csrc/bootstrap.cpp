@@ -921,9 +921,9 @@ fides_status fides_bootstrap_batch(fides_ctx* c, int nin, const fides_ct* const*
     // 2 pi K and SlotsToCoeffs by about sqrt(n) q0 / (2 pi D)
     for (const BootStage& st : B.cts) {
         Lanes y = A.fresh(k);
-        s = fides_linear_transform_batch(c, nin, (const fides_ct* const*)x.data(), (int)st.offsets.size(),
-                                         st.offsets.data(), (const fides_pt* const*)st.pts.data(), st.bstep, 1,
-                                         y.data());
+        s = linear_transform_batch(c, nin, (const fides_ct* const*)x.data(), (int)st.offsets.size(),
+                                   st.offsets.data(), (const fides_pt* const*)st.pts.data(), st.bstep, 1, y.data(),
+                                   true);
         if (s != FIDES_OK) return s;
         x = y;
     }
@@ -967,9 +967,9 @@ fides_status fides_bootstrap_batch(fides_ctx* c, int nin, const fides_ct* const*
     if (!A.ok()) return A.st;
     for (const BootStage& st : B.stc) {
         Lanes y = A.fresh(k);
-        s = fides_linear_transform_batch(c, nin, (const fides_ct* const*)w.data(), (int)st.offsets.size(),
-                                         st.offsets.data(), (const fides_pt* const*)st.pts.data(), st.bstep, 1,
-                                         y.data());
+        s = linear_transform_batch(c, nin, (const fides_ct* const*)w.data(), (int)st.offsets.size(),
+                                   st.offsets.data(), (const fides_pt* const*)st.pts.data(), st.bstep, 1, y.data(),
+                                   true);
         if (s != FIDES_OK) return s;
         w = y;
     }

@@ -119,6 +119,10 @@ struct fides_ctx {
     std::vector<float> tune_ms;
     int tuned_conv = 0;  // base-conversion accumulator: 0 128-bit, 1 split 32-bit products
     std::vector<float> conv_ms;
+    // giant steps of linear transforms summed in the extended basis before one
+    // ModDown per input: 0 never, 1 in the bootstrap's transforms, 2 in every
+    // linear transform
+    int giant_moddown = 1;
     int compress_keys = 1;  // keys generated here that store b and a seed for a: bit 0 Galois, bit 1 relinearisation
     std::string last_error;
     std::recursive_mutex mu;
@@ -138,6 +142,11 @@ fides_status consume_device_error(fides_ctx* c, cudaStream_t st = nullptr);
 // Canonical-embedding encode of `slots` complex values (interleaved re, im)
 // at `scale` into level+1 evaluation limbs at dm (device), on the context stream.
 fides_status encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm);
+// fides_linear_transform_batch with `boot` marking the bootstrap's own
+// transforms (the context's giant_moddown decides per caller)
+fides_status linear_transform_batch(fides_ctx* c, int nx, const fides_ct* const* xs, int n, const int32_t* offsets,
+                                    const fides_pt* const* pts, int bstep, int rescale, fides_ct* const* outs,
+                                    bool boot);
 // Encoding of slot values already in HBM (z: `slots` complex), slot j taking
 // factor * z[(j - shift) mod slots]: queued on the context stream, no
 // synchronisation; a coefficient at or above 2^63 sets the device word *bad.
@@ -175,6 +184,14 @@ void eng_hmult(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* co
 void eng_rotate_groups(fides_ctx* c, Workspace& w, int level, int ngroups, int nper, const uint64_t* const* c0,
                        const uint64_t* const* c1, const SwitchKey* const* keys, const uint32_t* galois,
                        uint64_t* const* out0, uint64_t* const* out1);
+// Rotations of nb ciphertexts (element b: (c0[b], c1[b]) by galois[b] with
+// keys[b]) summed per output before ModDown: output u is the sum of elements
+// start[u] .. start[u+1]-1, brought down from the extended basis once
+// instead of once per rotation (ModDown is linear; the two differ only in
+// the rounding of the division by P, each within its usual bound).
+void eng_rotate_sum(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* c0,
+                    const uint64_t* const* c1, const SwitchKey* const* keys, const uint32_t* galois, int nout,
+                    const int* start, uint64_t* const* out0, uint64_t* const* out1);
 // Rotation of element b by galois[b] with keys[b]; hoisted=true: all elements
 // rotate the same ciphertext (c0[0], c1[0]) and share one ModUp.
 void eng_rotate(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* c0, const uint64_t* const* c1,

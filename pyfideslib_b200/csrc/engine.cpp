@@ -236,6 +236,44 @@ void eng_rotate(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* c
     moddown_finish(c, w, level, nb, out0, out1, false, false);
 }
 
+void eng_rotate_sum(fides_ctx* c, Workspace& w, int level, int nb, const uint64_t* const* c0,
+                    const uint64_t* const* c1, const SwitchKey* const* keys, const uint32_t* galois, int nout,
+                    const int* start, uint64_t* const* out0, uint64_t* const* out1) {
+    eng_modup(c, w, level, nb, c1);
+    KsArgs ka{};
+    for (int b = 0; b < nb; ++b) {
+        ka.own[b] = c1[b];
+        ka.c0[b] = c0[b];
+        ka.kb[b] = keys[b]->b;
+        ka.ka[b] = keys[b]->a;
+        ka.a_seed[b] = keys[b]->a ? 0 : uniform_stream(keys[b]->a_seed, 0);
+        ka.galois[b] = galois[b];
+    }
+    ka.dig = w.DIG;
+    ka.xb = w.XB;
+    ka.xa = w.XA;
+    ka.dig_stride = w.dig_stride;
+    ka.bstride = w.stride;
+    ka.dig_bstride = w.stride;
+    launch_ks_inner(c->dev, level, nb, ka, false, w.st);
+    ExtSumArgs sa{};
+    sa.nout = nout;
+    sa.n = level + 1;
+    for (int u = 0; u <= nout; ++u) sa.start[u] = start[u];
+    sa.x[0] = w.XB;
+    sa.x[1] = w.XA;
+    sa.bstride = w.stride;
+    launch_ext_sum(c->dev, sa, w.st);
+    // one ModDown per output, on a view of the workspace whose element 0 is
+    // the output's first element (every per-element buffer moves together)
+    for (int u = 0; u < nout; ++u) {
+        Workspace v = w;
+        const size_t off = (size_t)start[u] * w.stride;
+        for (uint64_t** p : {&v.E0, &v.E1, &v.E2, &v.XT, &v.DIG, &v.XB, &v.XA, &v.W, &v.T}) *p += off;
+        moddown_finish(c, v, level, 1, out0 + u, out1 + u, false, false);
+    }
+}
+
 void eng_rotate_groups(fides_ctx* c, Workspace& w, int level, int ngroups, int nper, const uint64_t* const* c0,
                        const uint64_t* const* c1, const SwitchKey* const* keys, const uint32_t* galois,
                        uint64_t* const* out0, uint64_t* const* out1) {

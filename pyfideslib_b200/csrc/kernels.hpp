@@ -120,6 +120,18 @@ void launch_moddown_conv_tc(const DevCtx& ctx, int level, int nb, const MdArgs& 
 // override every segment's prologue / epilogue mode (-1 keeps the segment's own)
 void set_modes(LimbMap& map, int lmode, int smode);
 
+// Sums of key-switch results in the extended basis before one ModDown: for
+// output u < nout, elements start[u] .. start[u+1]-1 of x[0] (XB) and x[1]
+// (XA) -- n ciphertext limbs then K special limbs each, element b at
+// x + b*bstride -- are added into element start[u].
+struct ExtSumArgs {
+    int start[kMaxBatch + 1];
+    int nout, n;
+    uint64_t* x[2];
+    size_t bstride;
+};
+void launch_ext_sum(const DevCtx& ctx, const ExtSumArgs& args, cudaStream_t st);
+
 // element-wise helpers; limbs 0..n-1 use primes q0..q0+n-1
 enum { EW_ADD = 0, EW_SUB = 1, EW_NEG = 2, EW_MUL = 3, EW_COPY = 4 };
 void launch_elementwise(const DevCtx& ctx, int op, int n, int q0, const uint64_t* a, const uint64_t* b,

@@ -679,6 +679,35 @@ void launch_elementwise(const DevCtx& ctx, int op, int n, int q0, const uint64_t
     }
 }
 
+// Extended-basis sums of key-switch results: for output u, the elements
+// start[u] .. start[u+1]-1 of XB and XA (n ciphertext limbs, then K special
+// limbs, at bstride) are added into element start[u].  Two coefficients per
+// thread.
+__global__ void k_ext_sum(const __grid_constant__ DevCtx ctx, const __grid_constant__ ExtSumArgs a) {
+    const int limb = blockIdx.y, u = blockIdx.z;
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) * 2;
+    if (j >= ctx.N) return;
+    const uint64_t p = ctx.pc[limb < a.n ? limb : ctx.L + (limb - a.n)].p;
+    const size_t i = (size_t)limb * ctx.N + j;
+    const int b0 = a.start[u], b1 = a.start[u + 1];
+    for (int h = 0; h < 2; ++h) {
+        ulonglong2* dst = reinterpret_cast<ulonglong2*>(a.x[h] + (size_t)b0 * a.bstride + i);
+        ulonglong2 s = *dst;
+        for (int b = b0 + 1; b < b1; ++b) {
+            const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(a.x[h] + (size_t)b * a.bstride + i);
+            s.x = add_mod(s.x, v.x, p);
+            s.y = add_mod(s.y, v.y, p);
+        }
+        *dst = s;
+    }
+}
+
+void launch_ext_sum(const DevCtx& ctx, const ExtSumArgs& a, cudaStream_t st) {
+    if (a.nout <= 0) return;
+    count_launches(1);
+    k_ext_sum<<<dim3((ctx.N + 511) / 512, a.n + ctx.K, a.nout), 256, 0, st>>>(ctx, a);
+}
+
 __global__ void k_scalar_mac(const __grid_constant__ DevCtx ctx, const uint64_t* __restrict__ a,
                              const uint64_t* __restrict__ cj, const uint64_t* __restrict__ b,
                              uint64_t* __restrict__ out) {

@@ -269,3 +269,31 @@ def test_two_iteration_bootstrap_precision():
     with pytest.raises(FidesError):
         cc.EvalBootstrap(low, num_iterations=2)
     assert device_status(cc) == 0
+
+
+def test_bootstrap_giant_step_moddown_modes():
+    """The bootstrap's transforms with one ModDown per giant-step rotation
+    (scope 0) and with each input's giant steps brought down once (scope 1,
+    the default): the same precision.  The two ModDowns differ by a few units
+    per coefficient, which the rescale after each transform divides by a
+    modulus of about 2^50, so the refreshed ciphertexts are usually
+    identical; the bound allows for the rare rounding step."""
+    import pyfideslib_b200 as F
+    from pyfideslib_b200._capi import lib
+
+    cc = F.CryptoContext(log_n=12, num_q=20, dnum=4)
+    sk = cc.KeyGen(seed=19, hamming_weight=32)
+    cc.EvalMultKeyGen(sk)
+    cc.EvalBootstrapSetup(level_budget=(3, 3), cheb_degree=63)
+    cc.EvalBootstrapKeyGen(sk)
+    slots = cc.N // 2
+    rng = np.random.default_rng(33)
+    m = rng.uniform(-1, 1, slots) + 1j * rng.uniform(-1, 1, slots)
+    ct = cc.Encrypt(sk, m, slots=slots, level=0)
+    got = {}
+    for scope in (0, 1):
+        assert lib.fides_set_giant_step_moddown(cc._h, scope) == 0
+        got[scope] = cc.Decrypt(sk, cc.EvalBootstrap(ct), slots=slots)
+        assert -np.log2(np.max(np.abs(got[scope] - m))) > 14, scope
+    d = np.max(np.abs(got[0] - got[1]))
+    assert d < 2 ** -14, d
