@@ -1223,24 +1223,40 @@ fides_status giant_rotate_sum(fides_ctx* c, int level, const std::vector<const f
     if (terms.empty()) return FIDES_OK;
     fides_status s = ws_reserve(c, c->wsb, std::min((int)terms.size(), kMaxBatch));
     if (s != FIDES_OK) return s;
-    for (size_t k0 = 0; k0 < terms.size(); k0 += c->wsb.cap) {
-        const int nb = (int)std::min(terms.size() - k0, (size_t)c->wsb.cap);
+    // batches of whole inputs, so that every input's rotations share one
+    // ModDown; only an input with more rotations than a batch holds is split
+    // (one ModDown per part)
+    const int cap = c->wsb.cap;
+    std::vector<std::pair<size_t, size_t>> pieces;  // [begin, end) in terms
+    for (size_t t0 = 0; t0 < terms.size();) {
+        size_t t1 = t0;
+        while (t1 < terms.size() && owner[terms[t1]] == owner[terms[t0]] && t1 - t0 < (size_t)cap) ++t1;
+        pieces.push_back({t0, t1});
+        t0 = t1;
+    }
+    for (size_t p0 = 0; p0 < pieces.size();) {
+        size_t p1 = p0, nbz = 0;
+        while (p1 < pieces.size() && nbz + (pieces[p1].second - pieces[p1].first) <= (size_t)cap)
+            nbz += pieces[p1].second - pieces[p1].first, ++p1;
+        const int nb = (int)nbz;
         std::vector<const uint64_t*> c0(nb), c1(nb);
         std::vector<const SwitchKey*> kk(nb);
         std::vector<uint32_t> gg(nb);
         std::vector<int> start, runs;  // run r: elements start[r] .. start[r+1]-1 of input runs[r]
-        for (int j = 0; j < nb; ++j) {
-            const int i = terms[k0 + j];
-            c0[j] = inner[i]->c0();
-            c1[j] = inner[i]->c1(N);
-            kk[j] = keys[i];
-            gg[j] = gal[i];
-            if (j == 0 || owner[i] != runs.back()) {
-                start.push_back(j);
-                runs.push_back(owner[i]);
+        int j = 0;
+        for (size_t q = p0; q < p1; ++q) {
+            start.push_back(j);
+            runs.push_back(owner[terms[pieces[q].first]]);
+            for (size_t t = pieces[q].first; t < pieces[q].second; ++t, ++j) {
+                const int i = terms[t];
+                c0[j] = inner[i]->c0();
+                c1[j] = inner[i]->c1(N);
+                kk[j] = keys[i];
+                gg[j] = gal[i];
             }
         }
         start.push_back(nb);
+        p0 = p1;
         const int nout = (int)runs.size();
         std::vector<fides_ct*> r(nout);
         std::vector<uint64_t*> o0(nout), o1(nout);

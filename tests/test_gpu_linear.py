@@ -199,3 +199,31 @@ def test_linear_transform_giant_sum_bitexact_vs_oracle(offsets, bstep):
             g = o.download()
             assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1]), (offsets, rescale, "batch")
     assert lib.fides_set_giant_step_moddown(cc._h, 3) == 1  # BAD_ARG
+
+
+@pytest.mark.parametrize("offsets,bstep,nx", [(list(range(32)), 4, 5), (list(range(0, 40)), 32, 2)])
+def test_linear_transform_giant_sum_chunks(offsets, bstep, nx):
+    """More giant-step terms than one key-switch batch holds (5 inputs x 7
+    giant steps = 35 > 32: the batches are formed of whole inputs, so each
+    input still takes one ModDown), more than four giant sums per
+    dot-product pass, and more than 16 baby steps (the per-group dot
+    products): still bit for bit the oracle composition."""
+    import pyfideslib_b200 as F
+    from pyfideslib_b200._capi import lib
+
+    cc, oc = make_pair(12, 8, 3, 3)
+    assert lib.fides_set_giant_step_moddown(cc._h, 2) == 0
+    level = 5
+    keys = {}
+    for i, r in enumerate(F.CryptoContext.linear_transform_rotations(offsets, bstep)):
+        keys[r] = rand_key(oc, 3000 + 2 * i)
+        cc.upload_galois_key(cc.rotation_galois(r), *keys[r])
+    cts = [rand_ct(oc, level, 3500 + 2 * u) for u in range(nx)]
+    xs = [cc.upload(*ct) for ct in cts]
+    pts_r = [oc.random(list(range(level + 1)), 3900 + k) for k in range(len(offsets))]
+    pts = [_upload_pt(cc, m, level) for m in pts_r]
+    outs = cc.EvalLinearTransformBatch(xs, offsets, pts, bstep, rescale=False)
+    for (c0, c1), o in zip(cts, outs):
+        w0, w1 = _oracle_bsgs_giant_sum(oc, level, c0, c1, offsets, pts_r, bstep, keys, cc.rotation_galois)
+        g = o.download()
+        assert np.array_equal(g[0], w0) and np.array_equal(g[1], w1)
