@@ -589,6 +589,12 @@ class CryptoContext:
         """Force an NTT kernel variant (-1: back to the autotuned one)."""
         check(lib.fides_set_ntt_variant(self._h, variant), self._h)
 
+    def set_giant_step_moddown(self, scope):
+        """Giant-step rotations of linear transforms summed before one ModDown
+        per input: 0 never, 1 in the bootstrap's transforms (default), 2 in
+        every transform."""
+        check(lib.fides_set_giant_step_moddown(self._h, scope), self._h)
+
     def polymul(self, a, b, c, a_ntt, b_ntt, prime0, nlimbs):
         check(lib.fides_polymul(self._h, a, b, c, a_ntt, b_ntt, prime0, nlimbs), self._h)
         self.Synchronize()
