@@ -408,7 +408,10 @@ def measure_bootstrap(cc, reps=3, seed=101, degree=119):
            "output_level": out_level, "rotation_keys": len(rots), "setup_s": setup_s,
            "params": "N=2^16 L=30 K=%d dnum=3, 2^15 slots, h=32, budget {3,3}, Chebyshev degree %d, K=16, "
                      "3 double-angle steps" % (cc.K, degree)}
-    return res, sk, cts
+    # serving's bootstrap requests: inputs at levels spread over the valid
+    # range below the bootstrap's output level (ModRaise reads limb 0 only)
+    boot_inputs = [cc.Encrypt(sk, msgs[lv % 2], slots=slots, level=lv, seed=31 + lv) for lv in range(0, out_level)]
+    return res, sk, boot_inputs
 
 
 def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_streams=2, boot_share=0.0,
@@ -487,8 +490,10 @@ def measure_serving(cc, rates, duration, rot_indices, seed=5, max_batch=16, num_
     srv.close()
     mix = "%.0f%% HMult+Relin+Rescale, %.0f%% Rotate, %.0f%% EvalBootstrap" % (
         100 * (1 - boot_share - p_rot), 100 * p_rot, 100 * boot_share)
-    return {"mix": mix, "params": "N=2^16 L=30 K=10 dnum=3, HMult/Rotate inputs at levels uniform in 1..29, "
-                                  "bootstrap inputs at level 0",
+    params = "N=2^16 L=30 K=10 dnum=3, HMult/Rotate inputs at levels uniform in 1..29"
+    if boot_share > 0 and boot_inputs:
+        params += ", bootstrap inputs at levels uniform in 0..%d" % (len(boot_inputs) - 1)
+    return {"mix": mix, "params": params,
             "streams": num_streams, "max_batch": max_batch, "sweep": out}
 
 
