@@ -577,6 +577,78 @@ fides_status fides_square(fides_ctx* ctx, const fides_ct* a, fides_ct* out, int 
     return hmult_impl(ctx, a, a, out, rescale);
 }
 
+}  // extern "C"
+
+// In-place rescale of n ciphertexts at one level, the same per-ciphertext
+// steps as fides_rescale (INTT of the top limb, then one NTT per remaining
+// limb with the switch-modulus prologue and the rescale epilogue), up to four
+// ciphertexts per launch pair: small single-ciphertext launches leave most
+// SMs idle, a batch fills them.  Results equal one fides_rescale each.
+fides_status fides::rescale_batch(fides_ctx* c, int n, fides_ct* const* cts) {
+    if (!c || n < 0) return FIDES_BAD_ARG;
+    for (int i = 0; i < n; ++i)
+        if (!valid_ct(c, cts[i]) || cts[i]->level < 1 || cts[i]->level != cts[0]->level) return FIDES_BAD_ARG;
+    if (n == 0) return FIDES_OK;
+    Guard g(c);
+    const int l = cts[0]->level, N = c->N;
+    constexpr int kPer = kMaxSeg / 2;
+    uint64_t* top = nullptr;  // INTT of the top limbs, two per ciphertext
+    if (cudaMallocAsync((void**)&top, (size_t)2 * kPer * N * 8, c->st) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, FIDES_OOM, "rescale scratch");
+    }
+    fides_status s = FIDES_OK;
+    for (int i0 = 0; i0 < n && s == FIDES_OK; i0 += kPer) {
+        const int k = std::min(kPer, n - i0);
+        std::vector<fides_ct> tmp(k);
+        LimbMap t{}, m{};
+        for (int j = 0; j < k && s == FIDES_OK; ++j) {
+            s = ct_reserve(c, &tmp[j], l - 1);
+            const uint64_t* ins[2] = {cts[i0 + j]->c0(), cts[i0 + j]->c1(N)};
+            uint64_t* os[2] = {tmp[j].c0(), tmp[j].c1(N)};
+            for (int h = 0; h < 2; ++h) {
+                uint64_t* tl = top + (size_t)(2 * j + h) * N;
+                LimbSeg& a = t.seg[t.nseg++];
+                a.in = ins[h] + (size_t)l * N;
+                a.out = tl;
+                a.count = 1;
+                a.skip_lo = 1;
+                a.nq = 1;
+                a.q0 = l;
+                a.level = l;
+                t.total += 1;
+                LimbSeg& b = m.seg[m.nseg++];
+                b.in = tl;
+                b.in_stride_zero = 1;
+                b.in2 = ins[h];
+                b.out = os[h];
+                b.count = l;
+                b.skip_lo = l;
+                b.nq = l;
+                b.level = l;
+                m.total += l;
+            }
+        }
+        if (s != FIDES_OK) break;
+        ntt_inverse(c->dev, t, IL_PLAIN, IS_PLAIN, c->st);
+        ntt_forward(c->dev, m, FL_SWITCHMOD, FS_RESCALE, c->st);
+        for (int j = 0; j < k; ++j) {
+            fides_ct* o = cts[i0 + j];
+            const double sc = o->scale / (double)c->host.prime[l];
+            const int nd = o->noise_deg - 1, sl = o->slots;
+            commit(c, o, tmp[j]);
+            o->level = l - 1;
+            o->scale = sc;
+            o->noise_deg = nd;
+            o->slots = sl;
+        }
+    }
+    cudaFreeAsync(top, c->st);
+    return s != FIDES_OK ? s : check_cuda(c, "rescale");
+}
+
+extern "C" {
+
 fides_status fides_rescale(fides_ctx* c, const fides_ct* a, fides_ct* out) {
     if (!c || !valid_ct(c, a) || !out || a->level < 1) return FIDES_BAD_ARG;
     Guard g(c);
@@ -1429,10 +1501,10 @@ fides_status fides::linear_transform_batch(fides_ctx* c, int nx, const fides_ct*
         outs[u]->scale = sc;
         outs[u]->noise_deg = nd;
         outs[u]->slots = sl;
-        if (rescale && level > 0) {
-            s = fides_rescale(c, outs[u], outs[u]);
-            if (s != FIDES_OK) return s;
-        }
+    }
+    if (rescale && level > 0) {
+        s = rescale_batch(c, nx, outs);
+        if (s != FIDES_OK) return s;
     }
     return check_cuda(c, "linear_transform");
 }

@@ -400,9 +400,10 @@ class Arith {
             if ((st = ct_reserve(c, o[l], level)) != FIDES_OK) break;
             launch(xs, level, (long double)cst * tq, o[l]);
             meta(o[l], level, (double)tq, like[l]->slots);
-            if ((st = fides_rescale(c, o[l], o[l])) != FIDES_OK) break;
-            o[l]->scale = target;
         }
+        // the lanes' rescales as one batch
+        if (ok() && (st = rescale_batch(c, (int)o.size(), o.data())) == FIDES_OK)
+            for (fides_ct* x : o) x->scale = target;
         return o;
     }
 
@@ -423,8 +424,8 @@ class Arith {
             if ((st = ct_reserve(c, o[l], level)) != FIDES_OK) break;
             launch({x[l]}, level, 0.0L, o[l]);
             meta(o[l], level, (double)((long double)x[l]->scale * (long double)z), x[l]->slots);
-            if ((st = fides_rescale(c, o[l], o[l])) != FIDES_OK) break;
         }
+        if (ok()) st = rescale_batch(c, (int)o.size(), o.data());
         return o;
     }
 

@@ -142,6 +142,9 @@ fides_status consume_device_error(fides_ctx* c, cudaStream_t st = nullptr);
 // Canonical-embedding encode of `slots` complex values (interleaved re, im)
 // at `scale` into level+1 evaluation limbs at dm (device), on the context stream.
 fides_status encode_dev(fides_ctx* c, const double* values, int slots, int level, double scale, uint64_t* dm);
+// In-place rescale of n ciphertexts at one level, batched over launches;
+// results equal one fides_rescale each
+fides_status rescale_batch(fides_ctx* c, int n, fides_ct* const* cts);
 // fides_linear_transform_batch with `boot` marking the bootstrap's own
 // transforms (the context's giant_moddown decides per caller)
 fides_status linear_transform_batch(fides_ctx* c, int nx, const fides_ct* const* xs, int n, const int32_t* offsets,
