@@ -1406,43 +1406,13 @@ fides_status fides::linear_transform_batch(fides_ctx* c, int nx, const fides_ct*
         const double sc = x->scale * pts[0]->scale;
         const int nd = x->noise_deg + pts[0]->noise_deg, sl = x->slots;
         acc[u] = tmp.make();
-        // the baby steps as a list (0 = the input itself): with at most
-        // kDotBabies of them, kDotGroups giant-step sums share one pass
-        std::vector<int> blist;
-        for (const auto& kv : bct) blist.push_back(kv.first);
-        const bool grouped_dot = (int)blist.size() <= kDotBabies;
-        std::vector<std::pair<int, fides_ct*>> pend;  // giant steps waiting for a grouped pass
-        auto flush = [&]() {
-            if (pend.empty()) return;
-            DotGroupArgs d{};
-            d.nbaby = (int)blist.size();
-            d.ngroup = (int)pend.size();
-            for (int b = 0; b < d.nbaby; ++b) {
-                d.c0[b] = bct[blist[b]]->c0();
-                d.c1[b] = bct[blist[b]]->c1(N);
-            }
-            for (int g = 0; g < d.ngroup; ++g) {
-                for (int k : groups[pend[g].first]) {
-                    const int b = (int)(std::find(blist.begin(), blist.end(), baby[k]) - blist.begin());
-                    d.p[g][b] = pts[k]->m;
-                }
-                d.o0[g] = pend[g].second->c0();
-                d.o1[g] = pend[g].second->c1(N);
-            }
-            launch_dot_pt_groups(c->dev, nl, d, c->st);
-            pend.clear();
-        };
         for (auto& kv : groups) {
             const int gs = kv.first;
             const std::vector<int>& ks = kv.second;
             fides_ct* dst = gs == 0 ? acc[u] : tmp.make();
             s = ct_reserve(c, dst, level);
             if (s != FIDES_OK) return s;
-            if (grouped_dot) {
-                pend.emplace_back(gs, dst);
-                if ((int)pend.size() == kDotGroups) flush();
-            }
-            for (size_t k0 = 0; !grouped_dot && k0 < ks.size(); k0 += kMaxBatch) {
+            for (size_t k0 = 0; k0 < ks.size(); k0 += kMaxBatch) {
                 DotArgs d{};
                 d.n = (int)std::min(ks.size() - k0, (size_t)kMaxBatch);
                 d.accumulate = k0 > 0;
@@ -1468,7 +1438,6 @@ fides_status fides::linear_transform_batch(fides_ctx* c, int nx, const fides_ct*
                 owner.push_back(u);
             }
         }
-        flush();
     }
     if (!inner.empty() && (c->giant_moddown == 2 || (c->giant_moddown == 1 && boot))) {
         s = giant_rotate_sum(c, level, inner, gidx, owner, acc, have_acc, tmp);

@@ -155,20 +155,6 @@ struct DotArgs {
     uint64_t* o1;
 };
 void launch_dot_pt(const DevCtx& ctx, int nlimbs, const DotArgs& args, cudaStream_t st);
-// Several giant-step sums of one BSGS transform from the same baby steps in
-// one pass: o0[g] = sum_b c0[b] * p[g][b], o1[g] likewise, p[g][b] null where
-// baby b has no term in group g; every baby-step value is read once for all
-// kDotGroups groups instead of once per group.
-constexpr int kDotBabies = 16, kDotGroups = 4;
-struct DotGroupArgs {
-    const uint64_t* c0[kDotBabies];
-    const uint64_t* c1[kDotBabies];
-    const uint64_t* p[kDotGroups][kDotBabies];
-    uint64_t* o0[kDotGroups];
-    uint64_t* o1[kDotGroups];
-    int nbaby, ngroup;
-};
-void launch_dot_pt_groups(const DevCtx& ctx, int nlimbs, const DotGroupArgs& args, cudaStream_t st);
 // Integer linear combination over ciphertext components, with per-limb
 // integer constants z[k][j] (value, Shoup companion) and an optional constant
 // added to component 0:

@@ -801,40 +801,6 @@ __global__ void k_dot_pt(const __grid_constant__ DevCtx ctx, const __grid_consta
     *reinterpret_cast<ulonglong2*>(args.o1 + i) = r;
 }
 
-// One coefficient per thread; at most 16 products per output (residues below
-// 2^60), so the 128-bit sums need no folding.
-__global__ void k_dot_pt_groups(const __grid_constant__ DevCtx ctx, const __grid_constant__ DotGroupArgs args) {
-    const int limb = blockIdx.y;
-    const PrimeConst pc = ctx.pc[limb];
-    const size_t i = (size_t)limb * ctx.N + blockIdx.x * blockDim.x + threadIdx.x;
-    Acc128 a[kDotGroups], b[kDotGroups];
-#pragma unroll 1
-    for (int k = 0; k < args.nbaby; ++k) {
-        const uint64_t x = args.c0[k][i], y = args.c1[k][i];
-#pragma unroll
-        for (int g = 0; g < kDotGroups; ++g) {
-            const uint64_t* p = args.p[g][k];
-            if (!p) continue;
-            const uint64_t w = __ldg(p + i);
-            a[g].mac(x, w);
-            b[g].mac(y, w);
-        }
-    }
-#pragma unroll
-    for (int g = 0; g < kDotGroups; ++g) {
-        if (g >= args.ngroup) break;
-        args.o0[g][i] = a[g].reduce(pc);
-        args.o1[g][i] = b[g].reduce(pc);
-    }
-}
-
-void launch_dot_pt_groups(const DevCtx& ctx, int nlimbs, const DotGroupArgs& args, cudaStream_t st) {
-    if (nlimbs <= 0 || args.nbaby <= 0 || args.nbaby > kDotBabies || args.ngroup <= 0 || args.ngroup > kDotGroups)
-        return;
-    count_launches(1);
-    k_dot_pt_groups<<<dim3(ctx.N / 128, nlimbs), 128, 0, st>>>(ctx, args);
-}
-
 void launch_dot_pt(const DevCtx& ctx, int nlimbs, const DotArgs& args, cudaStream_t st) {
     if (nlimbs <= 0 || args.n <= 0 || args.n > kMaxBatch) return;
     dim3 g(ctx.N / 256, nlimbs);

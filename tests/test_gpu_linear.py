@@ -205,9 +205,8 @@ def test_linear_transform_giant_sum_bitexact_vs_oracle(offsets, bstep):
 def test_linear_transform_giant_sum_chunks(offsets, bstep, nx):
     """More giant-step terms than one key-switch batch holds (5 inputs x 7
     giant steps = 35 > 32: the batches are formed of whole inputs, so each
-    input still takes one ModDown), more than four giant sums per
-    dot-product pass, and more than 16 baby steps (the per-group dot
-    products): still bit for bit the oracle composition."""
+    input still takes one ModDown), and 31 baby steps with one giant step:
+    still bit for bit the oracle composition."""
     import pyfideslib_b200 as F
     from pyfideslib_b200._capi import lib
 
